@@ -1,0 +1,196 @@
+/*
+ * its.h -- C ABI of libits, a B200 (sm_100a) implementation of the ITS thin-shell path:
+ * sparse voxel octree by triangle voxelisation, hierarchical hat-basis assembly over the
+ * octree's corner vertices, LSCG fit of the coefficients, shell iso levels, dense field
+ * evaluation and marching cubes.
+ *
+ * Conventions
+ *  - Every call returns an its_status; the message of the last failure is its_last_error().
+ *    Nothing in the library calls exit() or throws across this boundary.
+ *  - Array arguments may be host or device pointers (CUDA unified addressing tells them
+ *    apart); results are written to the memory the caller passes. Vectors of 3-D points
+ *    are row-major (x,y,z) doubles; faces are int32 triples.
+ *  - Objects (its_svo, its_op) live on the GPU of the context that made them and are used
+ *    on the context's stream. A context must not be used by two host threads at once.
+ *  - Integer outputs (Morton codes, topology, case indices) are bit-exact with the CPU
+ *    restatement of the reference in oracle/; floating-point outputs carry tolerances
+ *    stated in the tests.
+ * Each declaration names the reference interface it replaces (file:line, paths inside
+ * the Alan-Leo-Wong/ITS tree).
+ */
+#ifndef ITS_ITS_H_
+#define ITS_ITS_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum its_status {
+  ITS_OK = 0,
+  ITS_ERR_INVALID = 1,  /* bad argument, non-finite input, size out of range */
+  ITS_ERR_CUDA = 2,     /* a CUDA runtime call failed */
+  ITS_ERR_OOM = 3,      /* device allocation failed */
+  ITS_ERR_TIMEOUT = 4,  /* a bounded device wait ran out */
+  ITS_ERR_NOT_CONVERGED = 5,
+  ITS_ERR_STATE = 6     /* object used in the wrong state */
+} its_status;
+
+typedef struct its_ctx its_ctx;
+typedef struct its_svo its_svo;
+typedef struct its_op its_op;
+
+/* ---- context: owns the device, stream and allocator pool --------------------------- */
+/* Replaces the per-call device selection of DeviceQuery.cuh:41 (getMaxComputeDevice). */
+its_status its_create(its_ctx** ctx, int device);
+its_status its_destroy(its_ctx* ctx);
+const char* its_last_error(const its_ctx* ctx);
+/* Work is issued on this stream (a cudaStream_t; NULL = the context's own stream). */
+its_status its_set_stream(its_ctx* ctx, void* cuda_stream);
+its_status its_synchronize(its_ctx* ctx);
+const char* its_version(void);
+/* Number of kernels this context has launched so far (a diagnostic counter). */
+int64_t its_kernel_launches(const its_ctx* ctx);
+
+/* ---- a1-a2: model pre-processing (host) ----------------------------------------------- */
+/* BaseModel::model2UnitCube / calcUnitCubeTransformMatrix (src/BaseModel.cpp:54-92). */
+its_status its_model_to_unit_cube(double* verts, int64_t nverts, double scale_factor);
+/* BaseModel::setUniformBoundingBox (src/BaseModel.cpp:24-51). */
+its_status its_uniform_bbox(const double* verts, int64_t nverts, double origin[3], double end[3],
+                            double width[3]);
+
+/* ---- a3: triangle attributes ----------------------------------------------------------- */
+/* cuAcc::launch_modelTriAttributeKernel (src/cuAcc/CUDACompute.h:14, .cu:79-109):
+   normal = (p2-p1)x(p3-p1) (not normalised), area = |normal|/2, dir = -normal.p1.
+   Any output may be NULL. */
+its_status its_tri_attributes(its_ctx* ctx, const double* verts, int64_t nverts, const int32_t* faces,
+                              int64_t nfaces, double* normal, double* area, double* dir);
+
+/* ---- a4-a8: sparse voxel octree ----------------------------------------------------------- */
+typedef struct its_svo_info {
+  int res, depth;
+  int64_t num_voxels, num_fine_nodes, num_nodes, num_vertices, num_edges;
+  int64_t nodes_per_depth[16];
+  int64_t vertices_per_depth[16];
+  double origin[3], unit[3];
+} its_svo_info;
+/* SparseVoxelOctree::createOctree (src/SVO.h:104, src/cuAcc/SVO.cu:674-856) together with
+   constructNodeAtrributes (SVO.cu:1112-1118): voxelises the triangles at res^3 (res a power
+   of two, 1..1024) inside the box (origin, width), builds every level, the 27-neighbour
+   tables, the per-depth corner vertices and the fine-node edges. */
+its_status its_svo_build(its_ctx* ctx, const double* verts, int64_t nverts, const int32_t* faces,
+                         int64_t nfaces, int res, const double origin[3], const double width[3],
+                         its_svo** out);
+its_status its_svo_free(its_svo* svo);
+its_status its_svo_get_info(const its_svo* svo, its_svo_info* info);
+/* Surface voxels (the compacted level-0 occupancy, SVO.cu:722-749), ascending Morton. */
+its_status its_svo_get_voxels(its_svo* svo, uint32_t* morton);
+/* svoNodeArray (SVO.h:50-51): finest depth first, root last. childs is 8 per node,
+   neighbors 27 per node (slot (dx+1)+3(dy+1)+9(dz+1)); UINT32_MAX marks "none".
+   origin is 3 per node. Any output may be NULL. */
+its_status its_svo_get_nodes(its_svo* svo, uint32_t* morton, uint32_t* parent, uint32_t* childs,
+                             uint8_t* is_leaf, double* origin, double* width, uint32_t* neighbors);
+/* nodeVertexArray (SVO.h:55-62): unique corners per depth in (x,y,z) order, depths
+   concatenated; owner = lowest index of a node having the corner. */
+its_status its_svo_get_vertices(its_svo* svo, double* pos, uint32_t* owner);
+/* fineNodeEdgeArray (SVO.h:57, SVO.cu:1098-1110). */
+its_status its_svo_get_edges(its_svo* svo, double* p0, double* p1, uint32_t* owner);
+
+/* ---- a9: shell samples --------------------------------------------------------------- */
+/* ThinShells::cpIntersectionPoints (src/ThinShells.cpp:38-479): mesh-edge x fine-node-face
+   points (sorted, unique) followed by fine-node-edge x triangle points. With out_points NULL
+   only the counts are returned; otherwise up to capacity points are written. */
+its_status its_shell_samples(its_svo* svo, const double* verts, int64_t nverts, const int32_t* faces,
+                             int64_t nfaces, double* out_points, int64_t capacity, int64_t* num_points,
+                             int64_t* num_edge_points);
+
+/* ---- a10: right-hand side -------------------------------------------------------------- */
+/* ThinShells::cpSDFOfTreeNodes (src/ThinShells.cpp:481-509; libigl signed_distance with the
+   fast winding number): exact distance to the mesh, negative where the winding number
+   exceeds 1/2. */
+its_status its_signed_distance(its_ctx* ctx, const double* points, int64_t npoints, const double* verts,
+                               int64_t nverts, const int32_t* faces, int64_t nfaces, double* out);
+
+/* ---- a11: operator assembly --------------------------------------------------------------- */
+typedef enum its_op_mode { ITS_OP_FP64 = 0, ITS_OP_FP32_VALUES = 1 } its_op_mode;
+/* The sparse system of ThinShells::cpCoefficients (src/ThinShells.cpp:511-606): one row per
+   corner vertex with the diagonal 1, coincident finer vertices (1) and the non-zero hat values
+   of the corners of every ancestor of the vertex's owner node. Stored as CSR with ascending
+   columns plus its transpose; ITS_OP_FP32_VALUES also keeps float copies of the values for
+   the mixed-precision solver. */
+its_status its_operator_build(its_svo* svo, int mode, its_op** out);
+its_status its_operator_free(its_op* op);
+its_status its_operator_info(const its_op* op, int64_t* rows, int64_t* nnz);
+its_status its_operator_get_csr(its_op* op, int64_t* rowptr, int32_t* col, double* val);
+/* y = A x (transpose = 0) or y = A^T x (transpose = 1). */
+its_status its_operator_apply(its_op* op, const double* x, double* y, int transpose);
+
+/* ---- a12: least-squares conjugate gradient ----------------------------------------------- */
+typedef enum its_stop_rule {
+  ITS_STOP_NORMAL = 0,   /* Eigen LSCG: ||A^T r|| <= tol ||A^T b|| */
+  ITS_STOP_RESIDUAL = 1  /* ||b - A x|| <= tol ||b|| */
+} its_stop_rule;
+typedef enum its_precision {
+  ITS_PREC_FP64 = 0,     /* every operation in FP64 */
+  ITS_PREC_MIXED = 1     /* FP32 SpMV, FP64 dots/residual, FP64 iterative refinement */
+} its_precision;
+typedef struct its_solve_opts {
+  double tol;           /* default: DBL_EPSILON (Eigen's default) */
+  int64_t max_iters;    /* default (<= 0): 2 * columns (Eigen's default) */
+  int stop_rule;        /* its_stop_rule */
+  int precision;        /* its_precision */
+  int ir_steps;         /* mixed: outer refinement steps (default 3) */
+  double inner_tol;     /* mixed: inner relative tolerance (default 1e-3) */
+  const double* x0;     /* warm start (NULL: zero start, Eigen's solve()) */
+  int check_every;      /* iterations per convergence check / graph launch (default 8) */
+} its_solve_opts;
+typedef struct its_solve_report {
+  int64_t iterations;   /* Eigen's count: direction updates before the stop */
+  int converged, breakdown;
+  double rel_residual;         /* ||b - A x|| / ||b|| */
+  double normal_rel_residual;  /* ||A^T(b - A x)|| / ||A^T b|| */
+  double ms;                   /* device time of the solve */
+  int64_t inner_iterations;    /* mixed: CGLS iterations summed over refinement steps */
+} its_solve_report;
+its_status its_solve_opts_default(its_solve_opts* opts);
+/* Eigen::LeastSquaresConjugateGradient::compute + solve (src/ThinShells.cpp:615-617). */
+its_status its_lscg_solve(its_op* op, const double* b, double* lambda, const its_solve_opts* opts,
+                          its_solve_report* report);
+
+/* ---- a13: field at points and the shell iso levels ------------------------------------- */
+/* ThinShells::cpLatentBSplineValue (src/ThinShells.cpp:655-755): each point's fine node by
+   Morton code, then lambda times the hats of the 8 corners of that node and of every
+   ancestor. Points outside every fine node get 0 and missing[i] = 1 (missing may be NULL). */
+its_status its_eval_points(its_svo* svo, const double* lambda, const double* points, int64_t npoints,
+                           double* out, uint8_t* missing);
+/* innerShellIsoVal / outerShellIsoVal (ThinShells.cpp:743-744): min and max of the field
+   over the points, skipping points outside every fine node. */
+its_status its_shell_iso_values(its_svo* svo, const double* lambda, const double* points, int64_t npoints,
+                                double* inner, double* outer, int64_t* num_missing);
+
+/* ---- a14-a15: dense field and marching cubes -------------------------------------------- */
+/* The field of MC::launch_computSDFKernel (src/cuAcc/MarchingCubes/MarchingCubes.cu:464-536,
+   CUDACompute.cu:435-510) on the (res+1)^3 lattice origin + i*width/res, x fastest. */
+its_status its_eval_grid(its_svo* svo, const double* lambda, const double origin[3], const double width[3],
+                         int res, double* field);
+/* MC::marching_cubes (src/cuAcc/MarchingCubes/MarchingCubes.h:136-139) on a lattice field:
+   cube_index (res^3 bytes, NULL allowed) with bit i = field[corner i] < iso in the corner
+   order of MarchingCubes.cu:233-241; triangle vertices (3 doubles each) in voxel order.
+   With tri_verts NULL only num_verts is returned. */
+its_status its_marching_cubes(its_ctx* ctx, const double* field, int res, const double origin[3],
+                              const double width[3], double iso, uint8_t* cube_index, double* tri_verts,
+                              int64_t capacity, int64_t* num_verts);
+
+#ifdef __cplusplus
+}
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#endif /* ITS_ITS_H_ */

@@ -1,0 +1,282 @@
+"""Python layer over the libits C ABI: contexts, octrees, operators and the solver.
+
+Arrays may be numpy arrays (host) or torch CUDA tensors (device); results come back as
+numpy arrays unless a device output is passed. Every entry point goes through libits.so.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import ItsError, SolveOpts, SolveReport, SvoInfo, lib
+
+STOP_NORMAL, STOP_RESIDUAL = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
+OP_FP64, OP_FP32_VALUES = 0, 1
+
+
+def _ptr(a):
+    """Raw pointer of a numpy array or a torch tensor (None -> NULL)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data_as(C.c_void_p)
+    return C.c_void_p(a.data_ptr())  # torch tensor
+
+
+def _f64(a):
+    if isinstance(a, np.ndarray) or not hasattr(a, "data_ptr"):
+        return np.ascontiguousarray(a, dtype=np.float64)
+    assert str(a.dtype) == "torch.float64" and a.is_contiguous()
+    return a
+
+
+def _i32(a):
+    if isinstance(a, np.ndarray) or not hasattr(a, "data_ptr"):
+        return np.ascontiguousarray(a, dtype=np.int32)
+    assert str(a.dtype) == "torch.int32" and a.is_contiguous()
+    return a
+
+
+def _n(a):
+    return int(a.shape[0])
+
+
+class Context:
+    """An its_ctx: one GPU, one stream."""
+
+    def __init__(self, device=0):
+        h = C.c_void_p()
+        s = lib().its_create(C.byref(h), device)
+        if s != 0:
+            raise ItsError(s, "its_create(device=%d) failed" % device)
+        self.h = h
+        self.device = device
+
+    def check(self, s, what):
+        if s != 0:
+            raise ItsError(s, "%s: %s" % (what, lib().its_last_error(self.h).decode()))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().its_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def set_stream(self, stream_ptr):
+        self.check(lib().its_set_stream(self.h, C.c_void_p(stream_ptr)), "its_set_stream")
+
+    def synchronize(self):
+        self.check(lib().its_synchronize(self.h), "its_synchronize")
+
+    @property
+    def kernel_launches(self):
+        return int(lib().its_kernel_launches(self.h))
+
+    # ---- a3 / a10 / a15 -------------------------------------------------------------
+    def tri_attributes(self, V, F):
+        V, F = _f64(V), _i32(F)
+        nf = _n(F)
+        n, a, d = np.zeros((nf, 3)), np.zeros(nf), np.zeros(nf)
+        self.check(lib().its_tri_attributes(self.h, _ptr(V), _n(V), _ptr(F), nf, _ptr(n), _ptr(a), _ptr(d)),
+                   "its_tri_attributes")
+        return n, a, d
+
+    def signed_distance(self, P, V, F, out=None):
+        P, V, F = _f64(P), _f64(V), _i32(F)
+        if out is None:
+            out = np.zeros(_n(P))
+        self.check(lib().its_signed_distance(self.h, _ptr(P), _n(P), _ptr(V), _n(V), _ptr(F), _n(F), _ptr(out)),
+                   "its_signed_distance")
+        return out
+
+    def marching_cubes(self, field, res, origin, width, iso, triangles=True):
+        field = _f64(field)
+        o, w = np.ascontiguousarray(origin, np.float64), np.ascontiguousarray(width, np.float64)
+        cube = np.zeros(res ** 3, np.uint8)
+        n = C.c_int64(0)
+        self.check(lib().its_marching_cubes(self.h, _ptr(field), res, _ptr(o), _ptr(w), float(iso), _ptr(cube), None, 0,
+                                            C.byref(n)), "its_marching_cubes")
+        tri = None
+        if triangles:
+            tri = np.zeros((max(n.value, 1), 3))
+            self.check(lib().its_marching_cubes(self.h, _ptr(field), res, _ptr(o), _ptr(w), float(iso), None,
+                                                _ptr(tri), n.value, C.byref(n)), "its_marching_cubes")
+            tri = tri[:n.value]
+        return cube, tri, int(n.value)
+
+
+def model_to_unit_cube(V, scale=1.0):
+    V = np.ascontiguousarray(V, np.float64).copy()
+    s = lib().its_model_to_unit_cube(_ptr(V), _n(V), scale)
+    if s != 0:
+        raise ItsError(s, "its_model_to_unit_cube")
+    return V
+
+
+def uniform_bbox(V):
+    V = np.ascontiguousarray(V, np.float64)
+    o, e, w = np.zeros(3), np.zeros(3), np.zeros(3)
+    s = lib().its_uniform_bbox(_ptr(V), _n(V), _ptr(o), _ptr(e), _ptr(w))
+    if s != 0:
+        raise ItsError(s, "its_uniform_bbox")
+    return o, e, w
+
+
+class Svo:
+    """An its_svo: the sparse voxel octree of one mesh (SparseVoxelOctree of the reference)."""
+
+    def __init__(self, ctx, V, F, res, origin, width):
+        self.ctx = ctx
+        V, F = _f64(V), _i32(F)
+        o, w = np.ascontiguousarray(origin, np.float64), np.ascontiguousarray(width, np.float64)
+        h = C.c_void_p()
+        ctx.check(lib().its_svo_build(ctx.h, _ptr(V), _n(V), _ptr(F), _n(F), res, _ptr(o), _ptr(w), C.byref(h)),
+                  "its_svo_build")
+        self.h = h
+        info = SvoInfo()
+        ctx.check(lib().its_svo_get_info(h, C.byref(info)), "its_svo_get_info")
+        self.info = info
+        self.depth = info.depth
+        self.res = res
+        self.num_voxels, self.num_fine = info.num_voxels, info.num_fine_nodes
+        self.num_nodes, self.num_verts, self.num_edges = info.num_nodes, info.num_vertices, info.num_edges
+        self.origin, self.width = o, w
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().its_svo_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def depth_counts(self):
+        return (np.array(self.info.nodes_per_depth[:self.depth], np.int64),
+                np.array(self.info.vertices_per_depth[:self.depth], np.int64))
+
+    def voxels(self):
+        out = np.zeros(self.num_voxels, np.uint32)
+        self.ctx.check(lib().its_svo_get_voxels(self.h, _ptr(out)), "its_svo_get_voxels")
+        return out
+
+    def nodes(self):
+        N = self.num_nodes
+        r = dict(morton=np.zeros(N, np.uint32), parent=np.zeros(N, np.uint32), childs=np.zeros((N, 8), np.uint32),
+                 is_leaf=np.zeros(N, np.uint8), origin=np.zeros((N, 3)), width=np.zeros(N),
+                 neighbors=np.zeros((N, 27), np.uint32))
+        self.ctx.check(lib().its_svo_get_nodes(self.h, _ptr(r["morton"]), _ptr(r["parent"]), _ptr(r["childs"]),
+                                               _ptr(r["is_leaf"]), _ptr(r["origin"]), _ptr(r["width"]),
+                                               _ptr(r["neighbors"])), "its_svo_get_nodes")
+        return r
+
+    def vertices(self):
+        pos, own = np.zeros((self.num_verts, 3)), np.zeros(self.num_verts, np.uint32)
+        self.ctx.check(lib().its_svo_get_vertices(self.h, _ptr(pos), _ptr(own)), "its_svo_get_vertices")
+        return pos, own
+
+    def edges(self):
+        E = self.num_edges
+        p0, p1, own = np.zeros((E, 3)), np.zeros((E, 3)), np.zeros(E, np.uint32)
+        self.ctx.check(lib().its_svo_get_edges(self.h, _ptr(p0), _ptr(p1), _ptr(own)), "its_svo_get_edges")
+        return p0, p1, own
+
+    def shell_samples(self, V, F):
+        V, F = _f64(V), _i32(F)
+        n, ne = C.c_int64(0), C.c_int64(0)
+        self.ctx.check(lib().its_shell_samples(self.h, _ptr(V), _n(V), _ptr(F), _n(F), None, 0, C.byref(n),
+                                               C.byref(ne)), "its_shell_samples")
+        out = np.zeros((max(n.value, 1), 3))
+        self.ctx.check(lib().its_shell_samples(self.h, _ptr(V), _n(V), _ptr(F), _n(F), _ptr(out), n.value,
+                                               C.byref(n), C.byref(ne)), "its_shell_samples")
+        return out[:n.value], int(ne.value)
+
+    def eval_points(self, lam, P, out=None):
+        lam, P = _f64(lam), _f64(P)
+        m = _n(P)
+        if out is None:
+            out = np.zeros(m)
+        miss = np.zeros(m, np.uint8)
+        self.ctx.check(lib().its_eval_points(self.h, _ptr(lam), _ptr(P), m, _ptr(out), _ptr(miss)), "its_eval_points")
+        return out, miss
+
+    def shell_iso_values(self, lam, P):
+        lam, P = _f64(lam), _f64(P)
+        lo, hi, miss = C.c_double(0), C.c_double(0), C.c_int64(0)
+        self.ctx.check(lib().its_shell_iso_values(self.h, _ptr(lam), _ptr(P), _n(P), C.byref(lo), C.byref(hi),
+                                                  C.byref(miss)), "its_shell_iso_values")
+        return lo.value, hi.value, int(miss.value)
+
+    def eval_grid(self, lam, origin, width, res, out=None):
+        lam = _f64(lam)
+        o, w = np.ascontiguousarray(origin, np.float64), np.ascontiguousarray(width, np.float64)
+        if out is None:
+            out = np.zeros((res + 1) ** 3)
+        self.ctx.check(lib().its_eval_grid(self.h, _ptr(lam), _ptr(o), _ptr(w), res, _ptr(out)), "its_eval_grid")
+        return out
+
+    def vertex_sdf(self, V, F):
+        """Right-hand side b: signed distance of every corner vertex (ThinShells::cpSDFOfTreeNodes)."""
+        pos, _ = self.vertices()
+        return self.ctx.signed_distance(pos, V, F)
+
+
+class Operator:
+    """An its_op: the assembled basis matrix A and its transpose."""
+
+    def __init__(self, svo, mode=OP_FP64):
+        self.ctx, self.svo = svo.ctx, svo
+        h = C.c_void_p()
+        svo.ctx.check(lib().its_operator_build(svo.h, mode, C.byref(h)), "its_operator_build")
+        self.h = h
+        r, z = C.c_int64(0), C.c_int64(0)
+        svo.ctx.check(lib().its_operator_info(h, C.byref(r), C.byref(z)), "its_operator_info")
+        self.rows, self.nnz = r.value, z.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().its_operator_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def csr(self):
+        rp, col, val = np.zeros(self.rows + 1, np.int64), np.zeros(self.nnz, np.int32), np.zeros(self.nnz)
+        self.ctx.check(lib().its_operator_get_csr(self.h, _ptr(rp), _ptr(col), _ptr(val)), "its_operator_get_csr")
+        return rp, col, val
+
+    def apply(self, x, transpose=False, out=None):
+        x = _f64(x)
+        if out is None:
+            out = np.zeros(self.rows)
+        self.ctx.check(lib().its_operator_apply(self.h, _ptr(x), _ptr(out), 1 if transpose else 0), "its_operator_apply")
+        return out
+
+    def solve(self, b, tol=None, max_iters=0, stop_rule=STOP_NORMAL, precision=PREC_FP64, ir_steps=3,
+              inner_tol=None, x0=None, check_every=0, out=None):
+        """LSCG (Eigen semantics by default). Returns (lambda, report dict)."""
+        opts = SolveOpts()
+        lib().its_solve_opts_default(C.byref(opts))
+        if tol is not None:
+            opts.tol = tol
+        opts.max_iters = max_iters
+        opts.stop_rule, opts.precision, opts.ir_steps = stop_rule, precision, ir_steps
+        if inner_tol is not None:
+            opts.inner_tol = inner_tol
+        if check_every:
+            opts.check_every = check_every
+        keep = None
+        if x0 is not None:
+            keep = _f64(x0)
+            opts.x0 = _ptr(keep).value if isinstance(keep, np.ndarray) else keep.data_ptr()
+        b = _f64(b)
+        if out is None:
+            out = np.zeros(self.rows)
+        rep = SolveReport()
+        self.ctx.check(lib().its_lscg_solve(self.h, _ptr(b), _ptr(out), C.byref(opts), C.byref(rep)), "its_lscg_solve")
+        return out, dict(iterations=rep.iterations, converged=bool(rep.converged), breakdown=bool(rep.breakdown),
+                         rel_residual=rep.rel_residual, normal_rel_residual=rep.normal_rel_residual, ms=rep.ms,
+                         inner_iterations=rep.inner_iterations)

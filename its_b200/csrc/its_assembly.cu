@@ -1,0 +1,311 @@
+// Operator assembly (replaces ThinShells::cpCoefficients' triplet build and
+// SparseMatrix::setFromTriplets, ThinShells.cpp:511-606, and setInDomainPoints,
+// SVO.cu:1160-1193).
+//
+// Row v (a corner vertex at depth d, lattice point P, owner node o):
+//   * the coincident vertices at depths j0..d-1 (value 1; the chain stops at the first
+//     finer depth without that corner), found by a bit test in each depth's lattice bitmap;
+//   * the diagonal (value 1);
+//   * for every ancestor of o, the non-zero hats of its 8 corners at v, with the corner
+//     positions origin (+ w) of that ancestor, exactly as the reference computes them.
+// Columns are lattice ranks, so every row comes out sorted: chain < diagonal < ancestors,
+// corners in x-major order. Two passes (count, fill) with an exclusive scan in between.
+// The transpose is a stable radix sort of the entries by column.
+#include <cmath>
+
+#include "its_op.cuh"
+
+namespace its {
+
+struct AsmParams {
+  int depth;
+  double3 g;
+  double w0;
+  LatticeIndex lat[kMaxDepth];
+  int64_t vertStart[kMaxDepth + 1];
+  const uint32_t* parent;
+  const uint32_t* morton;
+  const uint32_t* vertLin;
+  const uint32_t* vertOwner;
+  const double* vertPos;
+};
+
+template <bool FILL>
+__global__ void kAssembleRows(const __grid_constant__ AsmParams P, int64_t n, int64_t* __restrict__ rowptrOrCount, int32_t* __restrict__ col,
+                              double* __restrict__ val, uint32_t* __restrict__ rowIdx) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  int d = 0;
+  while (d + 1 < P.depth && P.vertStart[d + 1] <= r) ++d;
+  const uint32_t M = P.lat[d].M;
+  const uint32_t lin = P.vertLin[r];
+  const uint32_t X = lin / (M * M), Y = (lin / M) % M, Z = lin % M;
+  const double qx = P.vertPos[3 * r], qy = P.vertPos[3 * r + 1], qz = P.vertPos[3 * r + 2];
+  int j0 = d;
+  for (int j = d - 1; j >= 0; --j) {
+    const int s = d - j;
+    const uint32_t Mj = P.lat[j].M;
+    const uint32_t lj = ((X << s) * Mj + (Y << s)) * Mj + (Z << s);
+    if (!latticeHas(P.lat[j], lj)) break;
+    j0 = j;
+  }
+  int64_t k = FILL ? rowptrOrCount[r] : 0;
+  for (int j = j0; j < d; ++j) {
+    if (FILL) {
+      const int s = d - j;
+      const uint32_t Mj = P.lat[j].M;
+      const uint32_t lj = ((X << s) * Mj + (Y << s)) * Mj + (Z << s);
+      col[k] = (int32_t)latticeRank(P.lat[j], lj);
+      val[k] = 1.0;
+      rowIdx[k] = (uint32_t)r;
+    }
+    ++k;
+  }
+  if (FILL) {
+    col[k] = (int32_t)r;
+    val[k] = 1.0;
+    rowIdx[k] = (uint32_t)r;
+  }
+  ++k;
+  uint32_t a = P.parent[P.vertOwner[r]];
+  for (int dd = d + 1; dd < P.depth && a != kNone; ++dd) {
+    uint32_t Xa, Ya, Za;
+    mortonDecode(P.morton[a], Xa, Ya, Za);
+    const double w = P.w0 * (double)(1u << dd);
+    const double bx = latticePos(P.g.x, w, Xa), by = latticePos(P.g.y, w, Ya), bz = latticePos(P.g.z, w, Za);
+    const LatticeIndex& L = P.lat[dd];
+#pragma unroll
+    for (int ox = 0; ox < 2; ++ox) {
+      const double hx = hat1(qx, ox ? bx + w : bx, w);
+      if (hx <= 0.0) continue;
+#pragma unroll
+      for (int oy = 0; oy < 2; ++oy) {
+        const double hy = hat1(qy, oy ? by + w : by, w);
+        if (hy <= 0.0) continue;
+#pragma unroll
+        for (int oz = 0; oz < 2; ++oz) {
+          const double hz = hat1(qz, oz ? bz + w : bz, w);
+          if (hz <= 0.0) continue;
+          const double v = hx * hy * hz;
+          if (v == 0.0) continue;
+          if (FILL) {
+            col[k] = (int32_t)latticeRank(L, ((Xa + ox) * L.M + (Ya + oy)) * L.M + (Za + oz));
+            val[k] = v;
+            rowIdx[k] = (uint32_t)r;
+          }
+          ++k;
+        }
+      }
+    }
+    a = P.parent[a];
+  }
+  if (!FILL) rowptrOrCount[r] = k;
+}
+
+__global__ void kColumnCounts(int64_t nnz, const int32_t* __restrict__ col, uint32_t* __restrict__ cnt) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k < nnz) atomicAdd(cnt + col[k], 1u);
+}
+__global__ void kGatherTranspose(int64_t nnz, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ rowIdx,
+                                 const double* __restrict__ val, int32_t* __restrict__ tcol, double* __restrict__ tval) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nnz) return;
+  const uint32_t k = perm[i];
+  tcol[i] = (int32_t)rowIdx[k];
+  tval[i] = val[k];
+}
+__global__ void kSquare(int64_t n, const double* __restrict__ a, double* __restrict__ b) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) b[i] = a[i] * a[i];
+}
+__global__ void kFill(int64_t n, double v, double* __restrict__ a) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) a[i] = v;
+}
+__global__ void kInvDiag(int64_t n, double* __restrict__ d) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) d[i] = d[i] > 0.0 ? 1.0 / d[i] : 1.0;
+}
+__global__ void kToFloat(int64_t n, const double* __restrict__ a, float* __restrict__ b) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (float)a[i];
+}
+
+static void opRelease(its_op* op) {
+  if (!op) return;
+  its_ctx* c = op->ctx;
+  releaseSolver(op);
+  void* ptrs[] = {op->rowptr, op->col, op->val, op->trowptr, op->tcol, op->tval, op->valf, op->tvalf, op->invdiag};
+  for (void* p : ptrs) devFree(c, p);
+  releasePlan(c, &op->planA);
+  releasePlan(c, &op->planT);
+}
+
+static its_status opBuild(its_op* op) {
+  its_ctx* ctx = op->ctx;
+  const SvoDevice& d = op->svo->d;
+  const int64_t n = d.numVerts;
+  op->n = n;
+  AsmParams P;
+  P.depth = d.depth;
+  P.g = make_double3(d.origin[0], d.origin[1], d.origin[2]);
+  P.w0 = d.unit[0];
+  for (int L = 0; L < kMaxDepth; ++L) P.lat[L] = L < d.depth ? d.lattice(L) : LatticeIndex{};
+  for (int L = 0; L <= kMaxDepth; ++L) P.vertStart[L] = L <= d.depth ? d.vertStart[L] : n;
+  P.parent = d.nodeParent;
+  P.morton = d.nodeMorton;
+  P.vertLin = d.vertLin;
+  P.vertOwner = d.vertOwner;
+  P.vertPos = d.vertPos;
+  its_status st;
+  if ((st = devAlloc(ctx, (void**)&op->rowptr, (n + 1) * 8)) != ITS_OK) return st;
+  kAssembleRows<false><<<gridFor(n, 128), 128, 0, ctx->stream>>>(P, n, op->rowptr, nullptr, nullptr, nullptr);
+  ITS_LAUNCHED(ctx);
+  DevBuf<int64_t> tot;
+  if ((st = tot.alloc(ctx, 1)) != ITS_OK) return st;
+  {
+    int64_t* rp = op->rowptr;
+    auto f = [rp] __device__(int64_t i) -> int64_t { return rp[i]; };
+    if ((st = scanExclusiveAlloc<int64_t>(ctx, f, n, StorePrefix<int64_t>{rp}, tot.p)) != ITS_OK) return st;
+    ITS_CU(ctx, cudaMemcpyAsync(rp + n, tot.p, 8, cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  int64_t nnz = 0;
+  if ((st = readScalar(ctx, tot.p, &nnz)) != ITS_OK) return st;
+  if (nnz >= (1ll << 32)) return setError(ctx, ITS_ERR_INVALID, "operator has more than 2^32 entries");
+  op->nnz = nnz;
+  if ((st = devAlloc(ctx, (void**)&op->col, nnz * 4)) != ITS_OK) return st;
+  if ((st = devAlloc(ctx, (void**)&op->val, nnz * 8)) != ITS_OK) return st;
+  DevBuf<uint32_t> rowIdx;
+  if ((st = rowIdx.alloc(ctx, nnz)) != ITS_OK) return st;
+  kAssembleRows<true><<<gridFor(n, 128), 128, 0, ctx->stream>>>(P, n, op->rowptr, op->col, op->val, rowIdx.p);
+  ITS_LAUNCHED(ctx);
+
+  // transpose: stable sort of the entries by column keeps rows ascending within a column
+  {
+    DevBuf<uint32_t> iota, sk, sv, tk, tv, cnt;
+    if ((st = iota.alloc(ctx, nnz)) != ITS_OK) return st;
+    if ((st = sk.alloc(ctx, nnz)) != ITS_OK) return st;
+    if ((st = sv.alloc(ctx, nnz)) != ITS_OK) return st;
+    if ((st = tk.alloc(ctx, nnz)) != ITS_OK) return st;
+    if ((st = tv.alloc(ctx, nnz)) != ITS_OK) return st;
+    uint32_t* ip = iota.p;
+    auto one = [] __device__(int64_t) -> uint32_t { return 1u; };
+    if ((st = scanExclusiveAlloc<uint32_t>(ctx, one, nnz, StorePrefix<uint32_t>{ip}, (uint32_t*)nullptr)) != ITS_OK) return st;
+    int bits = 1;
+    while (bits < 32 && (1ll << bits) < n) ++bits;
+    if ((st = radixSortPairs(ctx, (const uint32_t*)op->col, iota.p, sk.p, sv.p, tk.p, tv.p, nnz, bits)) != ITS_OK)
+      return st;
+    if ((st = devAlloc(ctx, (void**)&op->tcol, nnz * 4)) != ITS_OK) return st;
+    if ((st = devAlloc(ctx, (void**)&op->tval, nnz * 8)) != ITS_OK) return st;
+    kGatherTranspose<<<gridFor(nnz, 256), 256, 0, ctx->stream>>>(nnz, sv.p, rowIdx.p, op->val, op->tcol, op->tval);
+    ITS_LAUNCHED(ctx);
+    if ((st = cnt.zeros(ctx, n)) != ITS_OK) return st;
+    kColumnCounts<<<gridFor(nnz, 256), 256, 0, ctx->stream>>>(nnz, op->col, cnt.p);
+    ITS_LAUNCHED(ctx);
+    if ((st = devAlloc(ctx, (void**)&op->trowptr, (n + 1) * 8)) != ITS_OK) return st;
+    const uint32_t* cp = cnt.p;
+    auto f = [cp] __device__(int64_t i) -> int64_t { return (int64_t)cp[i]; };
+    if ((st = scanExclusiveAlloc<int64_t>(ctx, f, n, StorePrefix<int64_t>{op->trowptr}, tot.p)) != ITS_OK) return st;
+    ITS_CU(ctx, cudaMemcpyAsync(op->trowptr + n, tot.p, 8, cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  rowIdx.reset();
+  if ((st = buildSpmvPlan(ctx, n, op->rowptr, &op->planA)) != ITS_OK) return st;
+  if ((st = buildSpmvPlan(ctx, n, op->trowptr, &op->planT)) != ITS_OK) return st;
+
+  // Jacobi column scaling of Eigen's LeastSquareDiagonalPreconditioner
+  {
+    DevBuf<double> sq, ones;
+    if ((st = sq.alloc(ctx, nnz)) != ITS_OK) return st;
+    if ((st = ones.alloc(ctx, n)) != ITS_OK) return st;
+    if ((st = devAlloc(ctx, (void**)&op->invdiag, n * 8)) != ITS_OK) return st;
+    kSquare<<<gridFor(nnz, 256), 256, 0, ctx->stream>>>(nnz, op->tval, sq.p);
+    ITS_LAUNCHED(ctx);
+    kFill<<<gridFor(n, 256), 256, 0, ctx->stream>>>(n, 1.0, ones.p);
+    ITS_LAUNCHED(ctx);
+    CsrView<double, double> S{n, op->trowptr, op->tcol, sq.p};
+    if ((st = spmv(ctx, S, op->planT, (const double*)ones.p, op->invdiag)) != ITS_OK) return st;
+    kInvDiag<<<gridFor(n, 256), 256, 0, ctx->stream>>>(n, op->invdiag);
+    ITS_LAUNCHED(ctx);
+  }
+  if (op->mode == ITS_OP_FP32_VALUES) {
+    if ((st = devAlloc(ctx, (void**)&op->valf, nnz * 4)) != ITS_OK) return st;
+    if ((st = devAlloc(ctx, (void**)&op->tvalf, nnz * 4)) != ITS_OK) return st;
+    kToFloat<<<gridFor(nnz, 256), 256, 0, ctx->stream>>>(nnz, op->val, op->valf);
+    ITS_LAUNCHED(ctx);
+    kToFloat<<<gridFor(nnz, 256), 256, 0, ctx->stream>>>(nnz, op->tval, op->tvalf);
+    ITS_LAUNCHED(ctx);
+  }
+  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITS_OK;
+}
+
+}  // namespace its
+
+using namespace its;
+
+extern "C" {
+
+its_status its_operator_build(its_svo* svo, int mode, its_op** out) {
+  if (!svo || !out) return ITS_ERR_INVALID;
+  *out = nullptr;
+  its_ctx* ctx = svo->ctx;
+  if (mode != ITS_OP_FP64 && mode != ITS_OP_FP32_VALUES) return setError(ctx, ITS_ERR_INVALID, "unknown operator mode");
+  ITS_CU(ctx, cudaSetDevice(ctx->device));
+  its_op* op = new its_op;
+  op->ctx = ctx;
+  op->svo = svo;
+  op->mode = mode;
+  its_status st = opBuild(op);
+  if (st != ITS_OK) {
+    opRelease(op);
+    cudaStreamSynchronize(ctx->stream);
+    delete op;
+    return st;
+  }
+  *out = op;
+  return ITS_OK;
+}
+
+its_status its_operator_free(its_op* op) {
+  if (!op) return ITS_OK;
+  its_ctx* c = op->ctx;
+  opRelease(op);
+  cudaStreamSynchronize(c->stream);
+  delete op;
+  return ITS_OK;
+}
+
+its_status its_operator_info(const its_op* op, int64_t* rows, int64_t* nnz) {
+  if (!op) return ITS_ERR_INVALID;
+  if (rows) *rows = op->n;
+  if (nnz) *nnz = op->nnz;
+  return ITS_OK;
+}
+
+its_status its_operator_get_csr(its_op* op, int64_t* rowptr, int32_t* col, double* val) {
+  if (!op) return ITS_ERR_INVALID;
+  its_ctx* ctx = op->ctx;
+  if (rowptr) ITS_CU(ctx, cudaMemcpyAsync(rowptr, op->rowptr, (op->n + 1) * 8, cudaMemcpyDefault, ctx->stream));
+  if (col) ITS_CU(ctx, cudaMemcpyAsync(col, op->col, op->nnz * 4, cudaMemcpyDefault, ctx->stream));
+  if (val) ITS_CU(ctx, cudaMemcpyAsync(val, op->val, op->nnz * 8, cudaMemcpyDefault, ctx->stream));
+  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITS_OK;
+}
+
+its_status its_operator_apply(its_op* op, const double* x, double* y, int transpose) {
+  if (!op || !x || !y) return ITS_ERR_INVALID;
+  its_ctx* ctx = op->ctx;
+  InArg<double> X;
+  OutArg<double> Y;
+  its_status st;
+  if ((st = X.stage(ctx, x, op->n)) != ITS_OK) return st;
+  if ((st = Y.stage(ctx, y, op->n)) != ITS_OK) return st;
+  if (transpose) st = spmv(ctx, op->T64(), op->planT, X.d, Y.d);
+  else st = spmv(ctx, op->A64(), op->planA, X.d, Y.d);
+  if (st != ITS_OK) return st;
+  if ((st = Y.finish(ctx)) != ITS_OK) return st;
+  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,135 @@
+// Context, device buffers and host/device argument staging for the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <utility>
+
+#include "its_internal.cuh"
+
+struct its_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaStream_t ownStream = nullptr;
+  std::string lastError;
+  int64_t launches = 0;
+  int numSMs = 148;
+};
+
+namespace its {
+
+// Count and check a kernel launch on the context's stream.
+#define ITS_LAUNCHED(ctx)                                          \
+  do {                                                             \
+    (ctx)->launches++;                                             \
+    cudaError_t e__ = cudaGetLastError();                          \
+    if (e__ != cudaSuccess) return ::its::cudaFail((ctx), e__, "kernel launch"); \
+  } while (0)
+
+inline its_status devAlloc(its_ctx* ctx, void** p, size_t bytes) {
+  *p = nullptr;
+  if (bytes == 0) return ITS_OK;
+  cudaError_t e = cudaMallocAsync(p, bytes, ctx->stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return setError(ctx, e == cudaErrorMemoryAllocation ? ITS_ERR_OOM : ITS_ERR_CUDA,
+                    std::string("device allocation of ") + std::to_string(bytes) + " bytes failed: " +
+                        cudaGetErrorString(e));
+  }
+  return ITS_OK;
+}
+inline void devFree(its_ctx* ctx, void* p) {
+  if (p) cudaFreeAsync(p, ctx->stream);
+}
+
+// Stream-ordered device buffer owned by one C-ABI call (or by an object).
+template <typename T>
+struct DevBuf {
+  its_ctx* ctx = nullptr;
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  explicit DevBuf(its_ctx* c) : ctx(c) {}
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : ctx(o.ctx), p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) { reset(); ctx = o.ctx; p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    return *this;
+  }
+  ~DevBuf() { reset(); }
+  its_status alloc(its_ctx* c, size_t count) {
+    reset();
+    ctx = c;
+    n = count;
+    return devAlloc(c, (void**)&p, count * sizeof(T));
+  }
+  its_status zeros(its_ctx* c, size_t count) {
+    its_status s = alloc(c, count);
+    if (s != ITS_OK) return s;
+    if (count) ITS_CU(c, cudaMemsetAsync(p, 0, count * sizeof(T), c->stream));
+    return ITS_OK;
+  }
+  void reset() {
+    if (p && ctx) devFree(ctx, p);
+    p = nullptr;
+    n = 0;
+  }
+  T* release() { T* q = p; p = nullptr; n = 0; return q; }
+};
+
+// True when p is device (or managed) memory of some GPU.
+inline bool isDevicePtr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// A read-only argument on the device: the caller's pointer if it already is device
+// memory, else a staged copy.
+template <typename T>
+struct InArg {
+  const T* d = nullptr;
+  DevBuf<T> tmp;
+  its_status stage(its_ctx* ctx, const T* src, size_t count) {
+    if (!src || count == 0) { d = nullptr; return ITS_OK; }
+    if (isDevicePtr(src)) { d = src; return ITS_OK; }
+    its_status s = tmp.alloc(ctx, count);
+    if (s != ITS_OK) return s;
+    ITS_CU(ctx, cudaMemcpyAsync(tmp.p, src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+    d = tmp.p;
+    return ITS_OK;
+  }
+};
+// A written argument: device scratch copied back to a host destination by finish().
+template <typename T>
+struct OutArg {
+  T* d = nullptr;
+  T* host = nullptr;
+  size_t count = 0;
+  DevBuf<T> tmp;
+  its_status stage(its_ctx* ctx, T* dst, size_t n) {
+    count = n;
+    host = nullptr;
+    if (!dst || n == 0) { d = nullptr; return ITS_OK; }
+    if (isDevicePtr(dst)) { d = dst; return ITS_OK; }
+    its_status s = tmp.alloc(ctx, n);
+    if (s != ITS_OK) return s;
+    d = tmp.p;
+    host = dst;
+    return ITS_OK;
+  }
+  its_status finish(its_ctx* ctx) {
+    if (host && count) ITS_CU(ctx, cudaMemcpyAsync(host, d, count * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+    return ITS_OK;
+  }
+};
+
+inline unsigned gridFor(int64_t n, int block) { return (unsigned)((n + block - 1) / block); }
+
+}  // namespace its

@@ -1,0 +1,348 @@
+// Field evaluation and marching cubes.
+//
+// * Points (ThinShells::cpLatentBSplineValue, ThinShells.cpp:655-755): a point's fine node
+//   is found by binary search of its voxel's Morton code in the sorted depth-0 node list;
+//   the field is sum(lambda * hat) over the 8 corners of that node and of every ancestor,
+//   corners in order k = x|y<<1|z<<2, ancestors from fine to coarse (the reference's order).
+// * Lattice (the MC input of MarchingCubes.cu:464-536 / CUDACompute.cu:435-510): the
+//   reference sums lambda_j * hat_j over ALL n corner vertices for 8 duplicated corners per
+//   voxel, O(8 R^3 n). Only the 8 corners of the depth-d cell holding p can be non-zero, so
+//   each lattice point of the (R+1)^3 grid is evaluated once from at most 8 corners per depth,
+//   their existence and column read from the per-depth lattice bitmaps: O(8 D) per point.
+// * Marching cubes (MarchingCubes.cu:164-377): case index with bit i = f(corner i) < iso in
+//   the reference's corner order, vertex counts from the case table, an exclusive scan of the
+//   counts, and the triangle soup written in voxel order by the scan's own downsweep (no
+//   compaction pass, no 18 R^3 preallocation).
+#include <cfloat>
+
+#include "its_op.cuh"
+
+namespace its {
+
+__device__ __constant__ uint64_t cMcCase[256] = {
+#include "mc_tables.inc"
+};
+// corner order of MarchingCubes.cu:233-241: 0 (0,0,0) 1 (0,1,0) 2 (1,1,0) 3 (1,0,0), 4..7 at z+1
+__device__ __constant__ int8_t cMcCorner[8][3] = {{0, 0, 0}, {0, 1, 0}, {1, 1, 0}, {1, 0, 0},
+                                                 {0, 0, 1}, {0, 1, 1}, {1, 1, 1}, {1, 0, 1}};
+__device__ __constant__ int8_t cMcEdge[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
+                                               {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+
+struct EvalParams {
+  int depth, res;
+  double3 g;
+  double w0;
+  LatticeIndex lat[kMaxDepth];
+  int64_t fineCount;
+  const uint32_t* morton;
+  const uint32_t* parent;
+  const double* vertPos;
+};
+
+static EvalParams evalParams(const SvoDevice& d) {
+  EvalParams P;
+  P.depth = d.depth;
+  P.res = d.res;
+  P.g = make_double3(d.origin[0], d.origin[1], d.origin[2]);
+  P.w0 = d.unit[0];
+  for (int L = 0; L < kMaxDepth; ++L) P.lat[L] = L < d.depth ? d.lattice(L) : LatticeIndex{};
+  P.fineCount = d.levelCount[0];
+  P.morton = d.nodeMorton;
+  P.parent = d.nodeParent;
+  P.vertPos = d.vertPos;
+  return P;
+}
+
+// Chain evaluation of one point; returns false when no fine node holds it.
+__device__ inline bool evalChain(const EvalParams& P, const double* __restrict__ lambda, double px, double py,
+                                 double pz, double& out) {
+  const int dx = (int)((px - P.g.x) / P.w0), dy = (int)((py - P.g.y) / P.w0), dz = (int)((pz - P.g.z) / P.w0);
+  if (dx < 0 || dy < 0 || dz < 0 || dx >= P.res || dy >= P.res || dz >= P.res) return false;
+  const uint32_t m = mortonEncode((uint32_t)dx, (uint32_t)dy, (uint32_t)dz);
+  int64_t lo = 0, hi = P.fineCount;  // first index with morton >= m
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (P.morton[mid] < m) lo = mid + 1;
+    else hi = mid;
+  }
+  if (lo >= P.fineCount || P.morton[lo] != m) return false;
+  uint32_t t = (uint32_t)lo;
+  double sum = 0.0;
+  for (int d = 0; d < P.depth && t != kNone; ++d) {
+    uint32_t X, Y, Z;
+    mortonDecode(P.morton[t], X, Y, Z);
+    const double w = P.w0 * (double)(1u << d);
+    const double bx = latticePos(P.g.x, w, X), by = latticePos(P.g.y, w, Y), bz = latticePos(P.g.z, w, Z);
+    const LatticeIndex& L = P.lat[d];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
+      const uint32_t col = latticeRank(L, ((X + ox) * L.M + (Y + oy)) * L.M + (Z + oz));
+      sum += lambda[col] * hat3(ox ? bx + w : bx, oy ? by + w : by, oz ? bz + w : bz, w, px, py, pz);
+    }
+    t = P.parent[t];
+  }
+  out = sum;
+  return true;
+}
+
+__global__ void kEvalPoints(const __grid_constant__ EvalParams P, const double* __restrict__ lambda,
+                            const double* __restrict__ pts, int64_t m, double* __restrict__ out,
+                            uint8_t* __restrict__ missing) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  double v = 0.0;
+  const bool ok = evalChain(P, lambda, pts[3 * i], pts[3 * i + 1], pts[3 * i + 2], v);
+  out[i] = ok ? v : 0.0;
+  if (missing) missing[i] = ok ? 0 : 1;
+}
+
+// min / max over the found points, count of missing ones; one partial per block.
+__global__ void kIsoPartials(const __grid_constant__ EvalParams P, const double* __restrict__ lambda,
+                             const double* __restrict__ pts, int64_t m, double* __restrict__ pmin,
+                             double* __restrict__ pmax, unsigned long long* __restrict__ pmiss) {
+  double lo = DBL_MAX, hi = -DBL_MAX;
+  unsigned long long miss = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+    double v;
+    if (evalChain(P, lambda, pts[3 * i], pts[3 * i + 1], pts[3 * i + 2], v)) {
+      lo = fmin(lo, v);
+      hi = fmax(hi, v);
+    } else {
+      ++miss;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fmin(lo, __shfl_down_sync(0xffffffffu, lo, o));
+    hi = fmax(hi, __shfl_down_sync(0xffffffffu, hi, o));
+    miss += __shfl_down_sync(0xffffffffu, miss, o);
+  }
+  __shared__ double slo[8], shi[8];
+  __shared__ unsigned long long smiss[8];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) { slo[w] = lo; shi[w] = hi; smiss[w] = miss; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < (int)(blockDim.x >> 5); ++k) {
+      lo = fmin(lo, slo[k]);
+      hi = fmax(hi, shi[k]);
+      miss += smiss[k];
+    }
+    pmin[blockIdx.x] = lo;
+    pmax[blockIdx.x] = hi;
+    pmiss[blockIdx.x] = miss;
+  }
+}
+
+// Field on the (R+1)^3 lattice, x fastest.
+__global__ void __launch_bounds__(256) kEvalGrid(const __grid_constant__ EvalParams P, const double* __restrict__ lambda,
+                                                 double3 o, double3 vs, int R, double* __restrict__ field) {
+  const int64_t M = (int64_t)R + 1;
+  const int64_t total = M * M * M;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t xi = idx % M, yj = (idx / M) % M, zk = idx / (M * M);
+    const double px = o.x + (double)xi * vs.x, py = o.y + (double)yj * vs.y, pz = o.z + (double)zk * vs.z;
+    double sum = 0.0;
+    for (int d = 0; d < P.depth; ++d) {
+      const double w = P.w0 * (double)(1u << d);
+      const LatticeIndex& L = P.lat[d];
+      const int64_t lim = (int64_t)(P.res >> d);
+      const int64_t cx = (int64_t)floor((px - P.g.x) / w), cy = (int64_t)floor((py - P.g.y) / w),
+                    cz = (int64_t)floor((pz - P.g.z) / w);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int64_t Lx = cx + (k & 1), Ly = cy + ((k >> 1) & 1), Lz = cz + ((k >> 2) & 1);
+        if (Lx < 0 || Ly < 0 || Lz < 0 || Lx > lim || Ly > lim || Lz > lim) continue;
+        const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
+        if (!latticeHas(L, lin)) continue;
+        const uint32_t v = latticeRank(L, lin);
+        sum += lambda[v] * hat3(P.vertPos[3 * v], P.vertPos[3 * v + 1], P.vertPos[3 * v + 2], w, px, py, pz);
+      }
+    }
+    field[idx] = sum;
+  }
+}
+
+// ---- marching cubes -----------------------------------------------------------------------
+struct McCase {
+  const double* field;
+  int R;
+  double iso;
+  __device__ unsigned cube(int64_t v) const {
+    const int64_t M = (int64_t)R + 1;
+    const int64_t x = v % R, y = (v / R) % R, z = v / ((int64_t)R * R);
+    unsigned ci = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const double f = field[((z + cMcCorner[k][2]) * M + (y + cMcCorner[k][1])) * M + (x + cMcCorner[k][0])];
+      ci |= (unsigned)(f < iso) << k;
+    }
+    return ci;
+  }
+  __device__ unsigned long long operator()(int64_t v) const { return cMcCase[cube(v)] & 15ull; }
+};
+
+__device__ inline void vertexLerp(const double* p0, const double* p1, double s0, double s1, double iso, double* out) {
+  if (fabs(iso - s0) < 1e-6) { out[0] = p0[0]; out[1] = p0[1]; out[2] = p0[2]; return; }
+  if (fabs(iso - s1) < 1e-6) { out[0] = p1[0]; out[1] = p1[1]; out[2] = p1[2]; return; }
+  if (fabs(s1 - s0) < 1e-6) { out[0] = p0[0]; out[1] = p0[1]; out[2] = p0[2]; return; }
+  const double t = (iso - s0) / (s1 - s0);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) out[a] = fma(t, p1[a], fma(-t, p0[a], p0[a]));  // MCKernel::lerp
+}
+
+struct McEmit {
+  McCase mc;
+  double3 o, vs;
+  uint8_t* cubeOut;
+  double* tri;
+  unsigned long long capacity;
+  __device__ void operator()(int64_t v, unsigned long long offset, unsigned long long count) const {
+    const unsigned ci = (cubeOut || count) ? mc.cube(v) : 0u;
+    if (cubeOut) cubeOut[v] = (uint8_t)ci;
+    if (!count || !tri) return;
+    const int R = mc.R;
+    const int64_t M = (int64_t)R + 1;
+    const int64_t x = v % R, y = (v / R) % R, z = v / ((int64_t)R * R);
+    const double vp[3] = {(double)x * vs.x + o.x, (double)y * vs.y + o.y, (double)z * vs.z + o.z};
+    const double vsz[3] = {vs.x, vs.y, vs.z};
+    double corner[8][3], sdf[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      for (int a = 0; a < 3; ++a) corner[k][a] = cMcCorner[k][a] ? vp[a] + vsz[a] : vp[a];
+      sdf[k] = mc.field[((z + cMcCorner[k][2]) * M + (y + cMcCorner[k][1])) * M + (x + cMcCorner[k][0])];
+    }
+    const uint64_t cw = cMcCase[ci];
+    for (unsigned i = 0; i < (unsigned)count; ++i) {
+      const unsigned long long dst = offset + i;
+      if (dst >= capacity) break;
+      const int e = (int)((cw >> (4 * (i + 1))) & 15u);
+      double q[3];
+      vertexLerp(corner[cMcEdge[e][0]], corner[cMcEdge[e][1]], sdf[cMcEdge[e][0]], sdf[cMcEdge[e][1]], mc.iso, q);
+      tri[3 * dst] = q[0];
+      tri[3 * dst + 1] = q[1];
+      tri[3 * dst + 2] = q[2];
+    }
+  }
+};
+
+}  // namespace its
+
+using namespace its;
+
+extern "C" {
+
+its_status its_eval_points(its_svo* s, const double* lambda, const double* points, int64_t npoints, double* out,
+                           uint8_t* missing) {
+  if (!s || !lambda || (!points && npoints) || (!out && npoints) || npoints < 0) return ITS_ERR_INVALID;
+  its_ctx* ctx = s->ctx;
+  if (npoints == 0) return ITS_OK;
+  ITS_CU(ctx, cudaSetDevice(ctx->device));
+  InArg<double> L, P;
+  OutArg<double> O;
+  OutArg<uint8_t> Mi;
+  its_status st;
+  if ((st = L.stage(ctx, lambda, s->d.numVerts)) != ITS_OK) return st;
+  if ((st = P.stage(ctx, points, 3 * npoints)) != ITS_OK) return st;
+  if ((st = O.stage(ctx, out, npoints)) != ITS_OK) return st;
+  if ((st = Mi.stage(ctx, missing, npoints)) != ITS_OK) return st;
+  kEvalPoints<<<gridFor(npoints, 128), 128, 0, ctx->stream>>>(evalParams(s->d), L.d, P.d, npoints, O.d, Mi.d);
+  ITS_LAUNCHED(ctx);
+  if ((st = O.finish(ctx)) != ITS_OK) return st;
+  if ((st = Mi.finish(ctx)) != ITS_OK) return st;
+  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITS_OK;
+}
+
+its_status its_shell_iso_values(its_svo* s, const double* lambda, const double* points, int64_t npoints, double* inner,
+                                double* outer, int64_t* num_missing) {
+  if (!s || !lambda || !points || npoints <= 0 || !inner || !outer) return ITS_ERR_INVALID;
+  its_ctx* ctx = s->ctx;
+  ITS_CU(ctx, cudaSetDevice(ctx->device));
+  InArg<double> L, P;
+  its_status st;
+  if ((st = L.stage(ctx, lambda, s->d.numVerts)) != ITS_OK) return st;
+  if ((st = P.stage(ctx, points, 3 * npoints)) != ITS_OK) return st;
+  const unsigned blocks = (unsigned)std::min<int64_t>(gridFor(npoints, 256), (int64_t)ctx->numSMs * 8);
+  DevBuf<double> pmin, pmax;
+  DevBuf<unsigned long long> pmiss;
+  if ((st = pmin.alloc(ctx, blocks)) != ITS_OK) return st;
+  if ((st = pmax.alloc(ctx, blocks)) != ITS_OK) return st;
+  if ((st = pmiss.alloc(ctx, blocks)) != ITS_OK) return st;
+  kIsoPartials<<<blocks, 256, 0, ctx->stream>>>(evalParams(s->d), L.d, P.d, npoints, pmin.p, pmax.p, pmiss.p);
+  ITS_LAUNCHED(ctx);
+  std::vector<double> hmin(blocks), hmax(blocks);
+  std::vector<unsigned long long> hmiss(blocks);
+  ITS_CU(ctx, cudaMemcpyAsync(hmin.data(), pmin.p, blocks * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  ITS_CU(ctx, cudaMemcpyAsync(hmax.data(), pmax.p, blocks * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  ITS_CU(ctx, cudaMemcpyAsync(hmiss.data(), pmiss.p, blocks * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  double lo = DBL_MAX, hi = -DBL_MAX;
+  unsigned long long miss = 0;
+  for (unsigned k = 0; k < blocks; ++k) {
+    lo = std::min(lo, hmin[k]);
+    hi = std::max(hi, hmax[k]);
+    miss += hmiss[k];
+  }
+  if (miss == (unsigned long long)npoints) return setError(ctx, ITS_ERR_INVALID, "no point lies in a fine node");
+  *inner = lo;
+  *outer = hi;
+  if (num_missing) *num_missing = (int64_t)miss;
+  return ITS_OK;
+}
+
+its_status its_eval_grid(its_svo* s, const double* lambda, const double origin[3], const double width[3], int res,
+                         double* field) {
+  if (!s || !lambda || !origin || !width || !field || res < 1 || res > 2048) return ITS_ERR_INVALID;
+  its_ctx* ctx = s->ctx;
+  ITS_CU(ctx, cudaSetDevice(ctx->device));
+  const int64_t M = (int64_t)res + 1, total = M * M * M;
+  InArg<double> L;
+  OutArg<double> F;
+  its_status st;
+  if ((st = L.stage(ctx, lambda, s->d.numVerts)) != ITS_OK) return st;
+  if ((st = F.stage(ctx, field, total)) != ITS_OK) return st;
+  const double3 o = make_double3(origin[0], origin[1], origin[2]);
+  const double3 vs = make_double3(width[0] / res, width[1] / res, width[2] / res);
+  const unsigned blocks = (unsigned)std::min<int64_t>(gridFor(total, 256), (int64_t)ctx->numSMs * 64);
+  kEvalGrid<<<blocks, 256, 0, ctx->stream>>>(evalParams(s->d), L.d, o, vs, res, F.d);
+  ITS_LAUNCHED(ctx);
+  if ((st = F.finish(ctx)) != ITS_OK) return st;
+  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITS_OK;
+}
+
+its_status its_marching_cubes(its_ctx* ctx, const double* field, int res, const double origin[3],
+                              const double width[3], double iso, uint8_t* cube_index, double* tri_verts,
+                              int64_t capacity, int64_t* num_verts) {
+  if (!ctx) return ITS_ERR_INVALID;
+  if (!field || !origin || !width || res < 1 || res > 2048 || !num_verts)
+    return setError(ctx, ITS_ERR_INVALID, "its_marching_cubes: bad arguments");
+  if (tri_verts && capacity < 0) return setError(ctx, ITS_ERR_INVALID, "negative capacity");
+  ITS_CU(ctx, cudaSetDevice(ctx->device));
+  const int64_t M = (int64_t)res + 1, nvox = (int64_t)res * res * res;
+  InArg<double> F;
+  OutArg<uint8_t> Cb;
+  OutArg<double> T;
+  its_status st;
+  if ((st = F.stage(ctx, field, M * M * M)) != ITS_OK) return st;
+  if ((st = Cb.stage(ctx, cube_index, nvox)) != ITS_OK) return st;
+  if ((st = T.stage(ctx, tri_verts, tri_verts ? 3 * capacity : 0)) != ITS_OK) return st;
+  McCase mc{F.d, res, iso};
+  McEmit em{mc, make_double3(origin[0], origin[1], origin[2]),
+            make_double3(width[0] / res, width[1] / res, width[2] / res), Cb.d, T.d,
+            (unsigned long long)(tri_verts ? capacity : 0)};
+  DevBuf<unsigned long long> tot;
+  if ((st = tot.alloc(ctx, 1)) != ITS_OK) return st;
+  if ((st = scanExclusiveAlloc<unsigned long long>(ctx, mc, nvox, em, tot.p)) != ITS_OK) return st;
+  unsigned long long total = 0;
+  if ((st = readScalar(ctx, tot.p, &total)) != ITS_OK) return st;
+  *num_verts = (int64_t)total;
+  if ((st = Cb.finish(ctx)) != ITS_OK) return st;
+  if ((st = T.finish(ctx)) != ITS_OK) return st;
+  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITS_OK;
+}
+
+}  // extern "C"

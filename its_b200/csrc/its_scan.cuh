@@ -1,0 +1,133 @@
+// Exclusive prefix sums (reduce-then-scan, three launches, no inter-block waiting).
+// The input is produced by a functor so that flags, popcounts or counts need not be
+// materialised. Used for stream compaction of Morton codes, lattice ranks, CSR row
+// pointers and marching-cubes offsets.
+#pragma once
+#include "its_ctx.cuh"
+
+namespace its {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+// Block-wide exclusive scan of one value per thread; returns the block total.
+template <typename T>
+__device__ inline T blockExclusiveScan(T v, T& total) {
+  __shared__ T warpTot[kScanThreads / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  T x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warpTot[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    T t = (lane < kScanThreads / 32) ? warpTot[lane] : T(0);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      T y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
+    }
+    if (lane < kScanThreads / 32) warpTot[lane] = t;
+  }
+  __syncthreads();
+  total = warpTot[kScanThreads / 32 - 1];
+  T excl = x - v + (wid > 0 ? warpTot[wid - 1] : T(0));
+  __syncthreads();
+  return excl;
+}
+
+template <typename T, typename F>
+__global__ void kScanUpsweep(F f, int64_t n, T* blockSums) {
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  T s = 0;
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j)
+    if (base + j < n) s += f(base + j);
+  T total;
+  blockExclusiveScan<T>(s, total);
+  if (threadIdx.x == 0) blockSums[blockIdx.x] = total;
+}
+
+// Single block: exclusive scan of the block sums in place; grand total to *total.
+template <typename T>
+__global__ void kScanSpine(T* blockSums, int64_t nb, T* total) {
+  T carry = 0;
+  for (int64_t c = 0; c < nb; c += kScanThreads) {
+    const int64_t i = c + threadIdx.x;
+    const T v = (i < nb) ? blockSums[i] : T(0);
+    T t;
+    const T e = blockExclusiveScan<T>(v, t);
+    if (i < nb) blockSums[i] = carry + e;
+    carry += t;
+  }
+  if (threadIdx.x == 0 && total) *total = carry;
+}
+
+template <typename T, typename F, typename W>
+__global__ void kScanDownsweep(F f, int64_t n, const T* blockOffsets, W write) {
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  T v[kScanItems];
+  T s = 0;
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) {
+    v[j] = (base + j < n) ? f(base + j) : T(0);
+    s += v[j];
+  }
+  T total;
+  T run = blockExclusiveScan<T>(s, total) + blockOffsets[blockIdx.x];
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j)
+    if (base + j < n) {
+      write(base + j, run, v[j]);
+      run += v[j];
+    }
+}
+
+// Writes the exclusive prefix to out[i].
+template <typename T>
+struct StorePrefix {
+  T* out;
+  __device__ void operator()(int64_t i, T prefix, T) const { out[i] = prefix; }
+};
+
+// Exclusive scan of f(0..n-1); write(i, prefix, value) receives each element's prefix.
+// The total lands in *dTotal (device memory, may be NULL). scratch must hold
+// scanScratchSize(n) elements of T.
+inline int64_t scanBlocks(int64_t n) { return (n + kScanTile - 1) / kScanTile; }
+template <typename T, typename F, typename W>
+its_status scanExclusive(its_ctx* ctx, F f, int64_t n, W write, T* dTotal, T* scratch) {
+  if (n <= 0) {
+    if (dTotal) ITS_CU(ctx, cudaMemsetAsync(dTotal, 0, sizeof(T), ctx->stream));
+    return ITS_OK;
+  }
+  const int64_t nb = scanBlocks(n);
+  kScanUpsweep<T, F><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(f, n, scratch);
+  ITS_LAUNCHED(ctx);
+  kScanSpine<T><<<1, kScanThreads, 0, ctx->stream>>>(scratch, nb, dTotal);
+  ITS_LAUNCHED(ctx);
+  kScanDownsweep<T, F, W><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(f, n, scratch, write);
+  ITS_LAUNCHED(ctx);
+  return ITS_OK;
+}
+// Convenience: allocates its own spine scratch.
+template <typename T, typename F, typename W>
+its_status scanExclusiveAlloc(its_ctx* ctx, F f, int64_t n, W write, T* dTotal) {
+  DevBuf<T> spine;
+  its_status s = spine.alloc(ctx, (size_t)(scanBlocks(n > 0 ? n : 1)));
+  if (s != ITS_OK) return s;
+  return scanExclusive<T>(ctx, f, n, write, dTotal, spine.p);
+}
+
+// Read one device scalar into host memory (synchronises the stream).
+template <typename T>
+its_status readScalar(its_ctx* ctx, const T* d, T* h) {
+  ITS_CU(ctx, cudaMemcpyAsync(h, d, sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITS_OK;
+}
+
+}  // namespace its

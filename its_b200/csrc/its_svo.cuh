@@ -1,0 +1,15 @@
+// Octree object shared by the translation units of libits.
+#pragma once
+#include "its_ctx.cuh"
+
+struct its_svo {
+  its_ctx* ctx = nullptr;
+  its::SvoDevice d;
+};
+
+namespace its {
+// Checks face indices and vertex finiteness on the device.
+its_status validateMesh(its_ctx* ctx, const double* dV, int64_t nv, const int32_t* dF, int64_t nf);
+its_status svoBuild(its_ctx* ctx, const double* dV, int64_t nv, const int32_t* dF, int64_t nf, int res,
+                    const double origin[3], const double width[3], its_svo* s);
+}  // namespace its

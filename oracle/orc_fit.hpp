@@ -1,0 +1,33 @@
+// CPU oracle (test infrastructure): fit-side stages. See orc_common.hpp.
+#pragma once
+#include <vector>
+
+#include "orc_svo.hpp"
+
+namespace orc {
+
+struct Csr {
+  int64_t n = 0;
+  std::vector<int64_t> rowptr;
+  std::vector<int32_t> col;
+  std::vector<double> val;
+};
+struct CglsReport {
+  int64_t iterations = 0;
+  int converged = 0, breakdown = 0;
+  double rel_residual = 0, normal_rel_residual = 0, rhs_norm2 = 0, normal_residual_norm2 = 0;
+};
+
+std::vector<V3> intersections(const Svo& s, const double* V, int64_t nv, const int32_t* F, int64_t nf,
+                              size_t* nEdgePoints);
+void signedDistance(const double* P, int64_t m, const double* V, const int32_t* F, int64_t nf, double* out);
+Csr assemble(const Svo& s);
+Csr transpose(const Csr& A);
+CglsReport cgls(const Csr& A, const Csr& T, const double* b, double* x, double tol, int64_t maxIters, int stop);
+void evalPoints(const Svo& s, const double* lambda, const double* P, int64_t m, double* out, uint8_t* missing);
+void evalBrute(const Svo& s, const double* lambda, const double* P, int64_t m, double* out);
+void evalGrid(const Svo& s, const double* lambda, const double origin[3], const double width[3], int R, double* out);
+int64_t marchingCubes(const double* field, int R, const double origin[3], const double width[3], double iso,
+                      uint8_t* cubeIndex, double* tri, int64_t maxVerts);
+
+}  // namespace orc
