@@ -127,7 +127,8 @@ its_status its_operator_build(its_svo* svo, int mode, its_op** out);
 its_status its_operator_free(its_op* op);
 its_status its_operator_info(const its_op* op, int64_t* rows, int64_t* nnz);
 its_status its_operator_get_csr(its_op* op, int64_t* rowptr, int32_t* col, double* val);
-/* y = A x (transpose = 0) or y = A^T x (transpose = 1). */
+/* y = A x (transpose = 0) or y = A^T x (transpose = 1). With x and y in device memory the
+   call returns without waiting for the GPU (work is ordered on the context's stream). */
 its_status its_operator_apply(its_op* op, const double* x, double* y, int transpose);
 
 /* ---- a12: least-squares conjugate gradient ----------------------------------------------- */

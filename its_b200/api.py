@@ -4,6 +4,7 @@ Arrays may be numpy arrays (host) or torch CUDA tensors (device); results come b
 numpy arrays unless a device output is passed. Every entry point goes through libits.so.
 """
 import ctypes as C
+import weakref
 
 import numpy as np
 
@@ -52,13 +53,20 @@ class Context:
             raise ItsError(s, "its_create(device=%d) failed" % device)
         self.h = h
         self.device = device
+        self._children = weakref.WeakSet()  # objects that must be freed before the context
 
     def check(self, s, what):
         if s != 0:
             raise ItsError(s, "%s: %s" % (what, lib().its_last_error(self.h).decode()))
 
+    def _adopt(self, obj):
+        self._children.add(obj)
+
     def close(self):
+        """Free every octree/operator made on this context, then the context itself."""
         if getattr(self, "h", None):
+            for obj in sorted(list(self._children), key=lambda o: 0 if isinstance(o, Operator) else 1):
+                obj.close()
             lib().its_destroy(self.h)
             self.h = None
 
@@ -136,6 +144,7 @@ class Svo:
         ctx.check(lib().its_svo_build(ctx.h, _ptr(V), _n(V), _ptr(F), _n(F), res, _ptr(o), _ptr(w), C.byref(h)),
                   "its_svo_build")
         self.h = h
+        ctx._adopt(self)
         info = SvoInfo()
         ctx.check(lib().its_svo_get_info(h, C.byref(info)), "its_svo_get_info")
         self.info = info
@@ -147,7 +156,8 @@ class Svo:
 
     def close(self):
         if getattr(self, "h", None):
-            lib().its_svo_free(self.h)
+            if self.ctx.h is not None:  # a closed context has already freed its objects
+                lib().its_svo_free(self.h)
             self.h = None
 
     def __del__(self):
@@ -231,13 +241,15 @@ class Operator:
         h = C.c_void_p()
         svo.ctx.check(lib().its_operator_build(svo.h, mode, C.byref(h)), "its_operator_build")
         self.h = h
+        svo.ctx._adopt(self)
         r, z = C.c_int64(0), C.c_int64(0)
         svo.ctx.check(lib().its_operator_info(h, C.byref(r), C.byref(z)), "its_operator_info")
         self.rows, self.nnz = r.value, z.value
 
     def close(self):
         if getattr(self, "h", None):
-            lib().its_operator_free(self.h)
+            if self.ctx.h is not None:
+                lib().its_operator_free(self.h)
             self.h = None
 
     def __del__(self):

@@ -304,7 +304,8 @@ its_status its_operator_apply(its_op* op, const double* x, double* y, int transp
   else st = spmv(ctx, op->A64(), op->planA, X.d, Y.d);
   if (st != ITS_OK) return st;
   if ((st = Y.finish(ctx)) != ITS_OK) return st;
-  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  // Device-to-device applies stay asynchronous on the context stream.
+  if (Y.host || X.tmp.p) ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   return ITS_OK;
 }
 

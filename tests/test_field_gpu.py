@@ -1,0 +1,83 @@
+"""Field-path parity: point evaluation, iso levels, dense lattice field and marching cubes.
+
+Bars: point evaluation and the lattice field use the oracle's terms in the oracle's order
+and are bit-exact; marching-cubes case indices are bit-exact for the same lattice field and
+the triangle soup is identical (same lerp with explicit fma). The fit identity of the
+reference (field at corner vertices = b, ThinShells.cpp:629-652) holds to the solve
+tolerance.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import prepared_mesh
+
+
+def _fit(ctx, name="c0", res=32, tol=1e-12):
+    from its_b200 import Operator, Svo
+    V, F, o, w = prepared_mesh(name)
+    ref, gpu = oracle.Svo(V, F, res, o, w), Svo(ctx, V, F, res, o, w)
+    pos, _ = ref.vertices()
+    b = oracle.signed_distance(pos, V, F)
+    lam, rep = Operator(gpu).solve(b, tol=tol, max_iters=2000)
+    return V, F, o, w, ref, gpu, pos, b, lam
+
+
+@pytest.fixture(scope="module")
+def fitted(ctx):
+    return _fit(ctx)
+
+
+@pytest.mark.gpu
+def test_eval_points_bit_exact_and_interpolates(fitted):
+    V, F, o, w, ref, gpu, pos, b, lam = fitted
+    samples = np.vstack([V, pos])
+    f_gpu, m_gpu = gpu.eval_points(lam, samples)
+    f_ref, m_ref = ref.eval_points(lam, samples)
+    assert np.array_equal(m_gpu, m_ref)
+    assert np.array_equal(f_gpu, f_ref)
+    # interpolation identity at corner vertices that lie in a fine node
+    fv = f_gpu[len(V):]
+    inside = m_gpu[len(V):] == 0
+    assert np.abs(fv[inside] - b[inside]).max() <= 1e-9
+
+
+@pytest.mark.gpu
+def test_shell_iso_values(fitted):
+    V, F, o, w, ref, gpu, pos, b, lam = fitted
+    pts, _ = gpu.shell_samples(V, F)
+    samples = np.vstack([V, pts])
+    lo, hi, miss = gpu.shell_iso_values(lam, samples)
+    f_ref, m_ref = ref.eval_points(lam, samples)
+    assert miss == int(m_ref.sum())
+    assert lo == f_ref[m_ref == 0].min() and hi == f_ref[m_ref == 0].max()
+    assert lo < 0 < hi
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("R", [32, 64])
+def test_grid_field_bit_exact_and_matches_brute_force(fitted, R):
+    V, F, o, w, ref, gpu, pos, b, lam = fitted
+    g_gpu = gpu.eval_grid(lam, o, w, R)
+    g_ref = ref.eval_grid(lam, o, w, R)
+    assert np.array_equal(g_gpu, g_ref)
+    M = R + 1
+    idx = np.random.default_rng(0).choice(M ** 3, 500, replace=False)
+    xi, yj, zk = idx % M, (idx // M) % M, idx // (M * M)
+    P = np.stack([o[0] + xi * (w[0] / R), o[1] + yj * (w[1] / R), o[2] + zk * (w[2] / R)], 1)
+    brute = ref.eval_brute(lam, P)
+    assert np.allclose(g_gpu[idx], brute, rtol=0, atol=1e-14)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("R", [16, 48])
+def test_marching_cubes_bit_exact(ctx, fitted, R):
+    V, F, o, w, ref, gpu, pos, b, lam = fitted
+    field = gpu.eval_grid(lam, o, w, R)
+    f, miss = ref.eval_points(lam, V)
+    for iso in (f.min(), 0.0, f.max()):
+        cube_g, tri_g, n_g = ctx.marching_cubes(field, R, o, w, iso)
+        cube_r, tri_r, n_r = oracle.marching_cubes(field, R, o, w, iso)
+        assert n_g == n_r and n_g > 0
+        assert np.array_equal(cube_g, cube_r)
+        assert np.array_equal(tri_g, tri_r)
