@@ -102,9 +102,17 @@ __global__ void kAssembleRows(const __grid_constant__ AsmParams P, int64_t n, in
   if (!FILL) rowptrOrCount[r] = k;
 }
 
-__global__ void kColumnCounts(int64_t nnz, const int32_t* __restrict__ col, uint32_t* __restrict__ cnt) {
-  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (k < nnz) atomicAdd(cnt + col[k], 1u);
+// Row pointers of A^T from the column-sorted keys: entry i opens every column in
+// (key[i-1], key[i]]; the end sentinel closes the rest. Each pointer is written once, no
+// atomics (a column count by atomicAdd would pile up on the few coarse corners that touch
+// almost every row).
+__global__ void kRowptrFromSorted(int64_t nnz, const uint32_t* __restrict__ keys, int64_t n,
+                                  int64_t* __restrict__ rowptr) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i > nnz) return;
+  const int64_t c = (i < nnz) ? (int64_t)keys[i] : n;
+  const int64_t prev = (i == 0) ? -1 : (int64_t)keys[i - 1];
+  for (int64_t k = prev + 1; k <= c; ++k) rowptr[k] = i;
 }
 __global__ void kGatherTranspose(int64_t nnz, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ rowIdx,
                                  const double* __restrict__ val, int32_t* __restrict__ tcol, double* __restrict__ tval) {
@@ -182,7 +190,7 @@ static its_status opBuild(its_op* op) {
 
   // transpose: stable sort of the entries by column keeps rows ascending within a column
   {
-    DevBuf<uint32_t> iota, sk, sv, tk, tv, cnt;
+    DevBuf<uint32_t> iota, sk, sv, tk, tv;
     if ((st = iota.alloc(ctx, nnz)) != ITS_OK) return st;
     if ((st = sk.alloc(ctx, nnz)) != ITS_OK) return st;
     if ((st = sv.alloc(ctx, nnz)) != ITS_OK) return st;
@@ -199,14 +207,9 @@ static its_status opBuild(its_op* op) {
     if ((st = devAlloc(ctx, (void**)&op->tval, nnz * 8)) != ITS_OK) return st;
     kGatherTranspose<<<gridFor(nnz, 256), 256, 0, ctx->stream>>>(nnz, sv.p, rowIdx.p, op->val, op->tcol, op->tval);
     ITS_LAUNCHED(ctx);
-    if ((st = cnt.zeros(ctx, n)) != ITS_OK) return st;
-    kColumnCounts<<<gridFor(nnz, 256), 256, 0, ctx->stream>>>(nnz, op->col, cnt.p);
-    ITS_LAUNCHED(ctx);
     if ((st = devAlloc(ctx, (void**)&op->trowptr, (n + 1) * 8)) != ITS_OK) return st;
-    const uint32_t* cp = cnt.p;
-    auto f = [cp] __device__(int64_t i) -> int64_t { return (int64_t)cp[i]; };
-    if ((st = scanExclusiveAlloc<int64_t>(ctx, f, n, StorePrefix<int64_t>{op->trowptr}, tot.p)) != ITS_OK) return st;
-    ITS_CU(ctx, cudaMemcpyAsync(op->trowptr + n, tot.p, 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    kRowptrFromSorted<<<gridFor(nnz + 1, 256), 256, 0, ctx->stream>>>(nnz, sk.p, n, op->trowptr);
+    ITS_LAUNCHED(ctx);
   }
   rowIdx.reset();
   if ((st = buildSpmvPlan(ctx, n, op->rowptr, &op->planA)) != ITS_OK) return st;

@@ -1,0 +1,324 @@
+// Accelerated signed distance: a linear BVH over the triangles (Karras 2012: Morton codes of
+// centroids, radix sort, binary radix tree, bottom-up boxes) answers
+//   * the exact unsigned distance: nearest-first traversal with box lower bounds; a node is
+//     skipped only when its box is farther than the best squared distance times (1 + 1e-12),
+//     so the minimum is the same IEEE value the brute force finds (same per-triangle code);
+//   * the sign from the fast winding number (Barill et al. 2018): far nodes contribute their
+//     area-weighted normal as a dipole at their area centroid, near nodes recurse, leaves add
+//     the exact solid angle. libigl's signed_distance(FAST_WINDING_NUMBER), which the reference
+//     calls (ThinShells.cpp:501), uses the same approximation; inside if w > 1/2.
+#include <cmath>
+
+#include "its_scan.cuh"
+#include "its_sdf.cuh"
+#include "its_sparse.cuh"
+#include <vector>
+#include <algorithm>
+
+namespace its {
+
+constexpr int kBvhStack = 64;
+constexpr double kFwnBeta = 3.0;  // far-field test |q - c| > beta * r
+
+struct BvhDevice {
+  int64_t nf = 0;
+  int32_t* left = nullptr;   // internal nodes: child index; >= 0 internal, < 0 leaf -(k+1)
+  int32_t* right = nullptr;
+  int32_t* parent = nullptr; // 2F-1 entries: internal 0..F-2, leaves F-1..2F-2
+  uint32_t* leafTri = nullptr;
+  double* lo = nullptr;      // 3 per node (2F-1)
+  double* hi = nullptr;
+  double* an = nullptr;      // area-weighted normal sum (3 per node)
+  double* ac = nullptr;      // area-weighted centroid sum (3 per node)
+  double* area = nullptr;
+  unsigned* flag = nullptr;
+};
+
+__global__ void kCentroidBounds(const double* __restrict__ V, const int32_t* __restrict__ F, int64_t nf,
+                                double* __restrict__ partial) {
+  double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nf; t += (int64_t)gridDim.x * blockDim.x) {
+    for (int a = 0; a < 3; ++a) {
+      const double c = (V[3 * F[3 * t] + a] + V[3 * F[3 * t + 1] + a] + V[3 * F[3 * t + 2] + a]) / 3.0;
+      mn[a] = fmin(mn[a], c);
+      mx[a] = fmax(mx[a], c);
+    }
+  }
+  for (int a = 0; a < 3; ++a)
+    for (int o = 16; o > 0; o >>= 1) {
+      mn[a] = fmin(mn[a], __shfl_down_sync(0xffffffffu, mn[a], o));
+      mx[a] = fmax(mx[a], __shfl_down_sync(0xffffffffu, mx[a], o));
+    }
+  __shared__ double s[8][6];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0)
+    for (int a = 0; a < 3; ++a) { s[w][a] = mn[a]; s[w][3 + a] = mx[a]; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < (int)(blockDim.x >> 5); ++k)
+      for (int a = 0; a < 3; ++a) { mn[a] = fmin(mn[a], s[k][a]); mx[a] = fmax(mx[a], s[k][3 + a]); }
+    for (int a = 0; a < 3; ++a) { partial[6 * blockIdx.x + a] = mn[a]; partial[6 * blockIdx.x + 3 + a] = mx[a]; }
+  }
+}
+
+__global__ void kMortonCodes(const double* __restrict__ V, const int32_t* __restrict__ F, int64_t nf, double3 lo,
+                             double3 inv, uint32_t* __restrict__ codes, uint32_t* __restrict__ idx) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= nf) return;
+  const double c[3] = {(V[3 * F[3 * t]] + V[3 * F[3 * t + 1]] + V[3 * F[3 * t + 2]]) / 3.0,
+                       (V[3 * F[3 * t] + 1] + V[3 * F[3 * t + 1] + 1] + V[3 * F[3 * t + 2] + 1]) / 3.0,
+                       (V[3 * F[3 * t] + 2] + V[3 * F[3 * t + 1] + 2] + V[3 * F[3 * t + 2] + 2]) / 3.0};
+  const double L[3] = {lo.x, lo.y, lo.z}, I[3] = {inv.x, inv.y, inv.z};
+  uint32_t q[3];
+  for (int a = 0; a < 3; ++a) {
+    const double u = (c[a] - L[a]) * I[a];
+    q[a] = (uint32_t)fmin(fmax(u * 1024.0, 0.0), 1023.0);
+  }
+  codes[t] = mortonEncode(q[0], q[1], q[2]);
+  idx[t] = (uint32_t)t;
+}
+
+// Length of the common prefix of keys i and j (index bits break ties), -1 out of range.
+__device__ inline int delta(const uint32_t* codes, int64_t n, int64_t i, int64_t j) {
+  if (j < 0 || j >= n) return -1;
+  const uint32_t a = codes[i], b = codes[j];
+  if (a != b) return __clz(a ^ b);
+  return 32 + __clzll((unsigned long long)(i ^ j));
+}
+
+__global__ void kBuildInternal(const uint32_t* __restrict__ codes, int64_t n, int32_t* __restrict__ left,
+                               int32_t* __restrict__ right, int32_t* __restrict__ parent) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  const int d = delta(codes, n, i, i + 1) - delta(codes, n, i, i - 1) >= 0 ? 1 : -1;
+  const int dmin = delta(codes, n, i, i - d);
+  int64_t lmax = 2;
+  while (delta(codes, n, i, i + lmax * d) > dmin) lmax <<= 1;
+  int64_t l = 0;
+  for (int64_t t = lmax >> 1; t >= 1; t >>= 1)
+    if (delta(codes, n, i, i + (l + t) * d) > dmin) l += t;
+  const int64_t j = i + l * d;
+  const int dnode = delta(codes, n, i, j);
+  int64_t s = 0;
+  for (int64_t t = (l + 1) >> 1;; t = (t + 1) >> 1) {
+    if (delta(codes, n, i, i + (s + t) * d) > dnode) s += t;
+    if (t == 1) break;
+  }
+  const int64_t g = i + s * d + (d < 0 ? d : 0);
+  const int64_t lo = i < j ? i : j, hi = i < j ? j : i;
+  const int32_t L = (lo == g) ? -(int32_t)(g + 1) : (int32_t)g;
+  const int32_t R = (hi == g + 1) ? -(int32_t)(g + 2) : (int32_t)(g + 1);
+  left[i] = L;
+  right[i] = R;
+  parent[L < 0 ? (n - 1) + (-L - 1) : L] = (int32_t)i;
+  parent[R < 0 ? (n - 1) + (-R - 1) : R] = (int32_t)i;
+}
+
+// Leaf data, then climb: the second child to arrive at a node merges both children.
+__global__ void kBottomUp(const double* __restrict__ V, const int32_t* __restrict__ F, int64_t n,
+                          const uint32_t* __restrict__ leafTri, BvhDevice B) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int64_t node = (n - 1) + k;
+  {
+    const uint32_t t = leafTri[k];
+    double p[3][3];
+    for (int c = 0; c < 3; ++c)
+      for (int a = 0; a < 3; ++a) p[c][a] = V[3 * F[3 * t + c] + a];
+    const double u[3] = {p[1][0] - p[0][0], p[1][1] - p[0][1], p[1][2] - p[0][2]};
+    const double v[3] = {p[2][0] - p[0][0], p[2][1] - p[0][1], p[2][2] - p[0][2]};
+    const double nx = 0.5 * (u[1] * v[2] - u[2] * v[1]), ny = 0.5 * (u[2] * v[0] - u[0] * v[2]),
+                 nz = 0.5 * (u[0] * v[1] - u[1] * v[0]);
+    const double ar = sqrt(nx * nx + ny * ny + nz * nz);
+    for (int a = 0; a < 3; ++a) {
+      B.lo[3 * node + a] = fmin(p[0][a], fmin(p[1][a], p[2][a]));
+      B.hi[3 * node + a] = fmax(p[0][a], fmax(p[1][a], p[2][a]));
+      B.ac[3 * node + a] = ar * (p[0][a] + p[1][a] + p[2][a]) / 3.0;
+    }
+    B.an[3 * node] = nx;
+    B.an[3 * node + 1] = ny;
+    B.an[3 * node + 2] = nz;
+    B.area[node] = ar;
+  }
+  __threadfence();
+  while (true) {
+    const int32_t par = B.parent[node];
+    if (par < 0) break;
+    if (atomicAdd(B.flag + par, 1u) == 0) return;  // first arrival: the sibling finishes the merge
+    __threadfence();
+    const int32_t L = B.left[par], R = B.right[par];
+    const int64_t a = L < 0 ? (n - 1) + (-L - 1) : L, b = R < 0 ? (n - 1) + (-R - 1) : R;
+    for (int c = 0; c < 3; ++c) {
+      B.lo[3 * par + c] = fmin(((volatile double*)B.lo)[3 * a + c], ((volatile double*)B.lo)[3 * b + c]);
+      B.hi[3 * par + c] = fmax(((volatile double*)B.hi)[3 * a + c], ((volatile double*)B.hi)[3 * b + c]);
+      B.an[3 * par + c] = ((volatile double*)B.an)[3 * a + c] + ((volatile double*)B.an)[3 * b + c];
+      B.ac[3 * par + c] = ((volatile double*)B.ac)[3 * a + c] + ((volatile double*)B.ac)[3 * b + c];
+    }
+    B.area[par] = ((volatile double*)B.area)[a] + ((volatile double*)B.area)[b];
+    __threadfence();
+    node = par;
+  }
+}
+
+__device__ inline double boxDist2(const double* lo, const double* hi, const double* q) {
+  double s = 0.0;
+  for (int a = 0; a < 3; ++a) {
+    const double d = q[a] < lo[a] ? lo[a] - q[a] : (q[a] > hi[a] ? q[a] - hi[a] : 0.0);
+    s = s + d * d;
+  }
+  return s;
+}
+
+__global__ void __launch_bounds__(128) kSdfBvh(const double* __restrict__ P, int64_t m, const double* __restrict__ V,
+                                               const int32_t* __restrict__ F, BvhDevice B, double* __restrict__ out,
+                                               unsigned* __restrict__ overflow) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const int64_t n = B.nf;
+  const double q[3] = {P[3 * i], P[3 * i + 1], P[3 * i + 2]};
+  const D3 qd{q[0], q[1], q[2]};
+  auto nodeOf = [n](int32_t c) -> int64_t { return c < 0 ? (n - 1) + (-c - 1) : c; };
+  auto tri = [&](int64_t node, D3* t) {
+    const uint32_t ti = B.leafTri[node - (n - 1)];
+    for (int c = 0; c < 3; ++c) {
+      const int32_t vi = F[3 * ti + c];
+      t[c] = D3{V[3 * vi], V[3 * vi + 1], V[3 * vi + 2]};
+    }
+  };
+  // exact unsigned distance
+  double best = 1.7976931348623157e308;
+  int32_t stack[kBvhStack];
+  int sp = 0;
+  if (n == 1) {
+    D3 t[3];
+    tri(0, t);
+    best = pointTriSqDist(qd, t[0], t[1], t[2]);
+  } else {
+    stack[sp++] = 0;
+    while (sp > 0) {
+      const int64_t node = stack[--sp];
+      if (boxDist2(B.lo + 3 * node, B.hi + 3 * node, q) > best * (1.0 + 1e-12)) continue;
+      const int32_t c[2] = {B.left[node], B.right[node]};
+      double dc[2];
+      for (int k = 0; k < 2; ++k) {
+        const int64_t cn = nodeOf(c[k]);
+        dc[k] = boxDist2(B.lo + 3 * cn, B.hi + 3 * cn, q);
+      }
+      const int first = dc[1] < dc[0] ? 1 : 0;
+      for (int kk = 1; kk >= 0; --kk) {  // push the farther child first
+        const int k = kk == 1 ? 1 - first : first;
+        if (dc[k] > best * (1.0 + 1e-12)) continue;
+        if (c[k] < 0) {
+          D3 t[3];
+          tri(nodeOf(c[k]), t);
+          best = fmin(best, pointTriSqDist(qd, t[0], t[1], t[2]));
+        } else {
+          if (sp >= kBvhStack) { atomicOr(overflow, 1u); continue; }
+          stack[sp++] = c[k];
+        }
+      }
+    }
+  }
+  // fast winding number
+  double w = 0.0;
+  sp = 0;
+  stack[sp++] = n == 1 ? -1 : 0;
+  while (sp > 0) {
+    const int32_t cur = stack[--sp];
+    const int64_t node = nodeOf(cur);
+    if (cur < 0) {
+      D3 t[3];
+      tri(node, t);
+      w += solidAngle(qd, t[0], t[1], t[2]);
+      continue;
+    }
+    const double A = B.area[node];
+    const double* lo = B.lo + 3 * node;
+    const double* hi = B.hi + 3 * node;
+    if (A > 0.0) {
+      const double c[3] = {B.ac[3 * node] / A, B.ac[3 * node + 1] / A, B.ac[3 * node + 2] / A};
+      double r2 = 0.0;
+      for (int a = 0; a < 3; ++a) {
+        const double e = fmax(c[a] - lo[a], hi[a] - c[a]);
+        r2 += e * e;
+      }
+      const double d[3] = {c[0] - q[0], c[1] - q[1], c[2] - q[2]};
+      const double R2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+      if (R2 > kFwnBeta * kFwnBeta * r2) {
+        const double R = sqrt(R2);
+        w += (B.an[3 * node] * d[0] + B.an[3 * node + 1] * d[1] + B.an[3 * node + 2] * d[2]) / (R2 * R);
+        continue;
+      }
+    }
+    if (sp + 2 > kBvhStack) { atomicOr(overflow, 1u); continue; }
+    stack[sp++] = B.left[node];
+    stack[sp++] = B.right[node];
+  }
+  const double wn = w / (4.0 * 3.14159265358979323846);
+  const double dist = sqrt(best);
+  out[i] = (wn > 0.5) ? -dist : dist;
+}
+
+its_status sdfBvh(its_ctx* ctx, const double* dP, int64_t m, const double* dV, const int32_t* dF, int64_t nf, double* dOut) {
+  its_status st;
+  const int64_t nodes = 2 * nf - 1;
+  BvhDevice B;
+  B.nf = nf;
+  DevBuf<int32_t> left, right, parent;
+  DevBuf<uint32_t> codes, idx, sc, leafTri, tk, tv;
+  DevBuf<double> lo, hi, an, ac, area;
+  DevBuf<unsigned> flag, overflow;
+  if ((st = left.alloc(ctx, nf)) != ITS_OK || (st = right.alloc(ctx, nf)) != ITS_OK ||
+      (st = parent.alloc(ctx, nodes)) != ITS_OK || (st = codes.alloc(ctx, nf)) != ITS_OK ||
+      (st = idx.alloc(ctx, nf)) != ITS_OK || (st = sc.alloc(ctx, nf)) != ITS_OK ||
+      (st = leafTri.alloc(ctx, nf)) != ITS_OK || (st = tk.alloc(ctx, nf)) != ITS_OK ||
+      (st = tv.alloc(ctx, nf)) != ITS_OK || (st = lo.alloc(ctx, 3 * nodes)) != ITS_OK ||
+      (st = hi.alloc(ctx, 3 * nodes)) != ITS_OK || (st = an.alloc(ctx, 3 * nodes)) != ITS_OK ||
+      (st = ac.alloc(ctx, 3 * nodes)) != ITS_OK || (st = area.alloc(ctx, nodes)) != ITS_OK ||
+      (st = flag.zeros(ctx, nf)) != ITS_OK || (st = overflow.zeros(ctx, 1)) != ITS_OK)
+    return st;
+  // centroid bounds for the Morton quantisation
+  const unsigned pb = 256;
+  DevBuf<double> part;
+  if ((st = part.alloc(ctx, 6 * pb)) != ITS_OK) return st;
+  kCentroidBounds<<<pb, 256, 0, ctx->stream>>>(dV, dF, nf, part.p);
+  ITS_LAUNCHED(ctx);
+  std::vector<double> hp(6 * pb);
+  ITS_CU(ctx, cudaMemcpyAsync(hp.data(), part.p, 6 * pb * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  double bl[3] = {1e300, 1e300, 1e300}, bh[3] = {-1e300, -1e300, -1e300};
+  for (unsigned k = 0; k < pb; ++k)
+    for (int a = 0; a < 3; ++a) { bl[a] = std::min(bl[a], hp[6 * k + a]); bh[a] = std::max(bh[a], hp[6 * k + 3 + a]); }
+  double inv[3];
+  for (int a = 0; a < 3; ++a) inv[a] = bh[a] > bl[a] ? 1.0 / (bh[a] - bl[a]) : 0.0;
+  kMortonCodes<<<gridFor(nf, 256), 256, 0, ctx->stream>>>(dV, dF, nf, make_double3(bl[0], bl[1], bl[2]),
+                                                         make_double3(inv[0], inv[1], inv[2]), codes.p, idx.p);
+  ITS_LAUNCHED(ctx);
+  if ((st = radixSortPairs(ctx, codes.p, idx.p, sc.p, leafTri.p, tk.p, tv.p, nf, 30)) != ITS_OK) return st;
+  B.left = left.p;
+  B.right = right.p;
+  B.parent = parent.p;
+  B.leafTri = leafTri.p;
+  B.lo = lo.p;
+  B.hi = hi.p;
+  B.an = an.p;
+  B.ac = ac.p;
+  B.area = area.p;
+  B.flag = flag.p;
+  ITS_CU(ctx, cudaMemsetAsync(parent.p, 0xFF, nodes * 4, ctx->stream));
+  if (nf > 1) {
+    kBuildInternal<<<gridFor(nf - 1, 256), 256, 0, ctx->stream>>>(sc.p, nf, left.p, right.p, parent.p);
+    ITS_LAUNCHED(ctx);
+  }
+  kBottomUp<<<gridFor(nf, 256), 256, 0, ctx->stream>>>(dV, dF, nf, leafTri.p, B);
+  ITS_LAUNCHED(ctx);
+  kSdfBvh<<<gridFor(m, 128), 128, 0, ctx->stream>>>(dP, m, dV, dF, B, dOut, overflow.p);
+  ITS_LAUNCHED(ctx);
+  unsigned ov = 0;
+  ITS_CU(ctx, cudaMemcpyAsync(&ov, overflow.p, 4, cudaMemcpyDeviceToHost, ctx->stream));
+  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  if (ov) return setError(ctx, ITS_ERR_INVALID, "BVH traversal stack overflow (degenerate triangle distribution)");
+  return ITS_OK;
+}
+
+}  // namespace its

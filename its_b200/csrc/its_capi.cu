@@ -91,6 +91,27 @@ its_status its_create(its_ctx** out, int device) {
   }
   c->stream = c->ownStream;
   cudaDeviceGetAttribute(&c->numSMs, cudaDevAttrMultiProcessorCount, device);
+  // The context's own stream-ordered pool keeps freed blocks across synchronisations: with a
+  // release threshold of 0 every sync would hand memory back and the next allocation would
+  // map it again, which costs far more than the fit's kernels.
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  if (cudaMemPoolCreate(&c->pool, &props) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  } else {
+    cudaGetLastError();
+    c->pool = nullptr;
+  }
+  if (cudaMallocHost((void**)&c->pinned, 256) != cudaSuccess) {
+    cudaGetLastError();
+    if (c->pool) cudaMemPoolDestroy(c->pool);
+    cudaStreamDestroy(c->ownStream);
+    delete c;
+    return ITS_ERR_CUDA;
+  }
   *out = c;
   return ITS_OK;
 }
@@ -100,6 +121,8 @@ its_status its_destroy(its_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->ownStream) cudaStreamDestroy(c->ownStream);
+  if (c->pool) cudaMemPoolDestroy(c->pool);  // released once nothing allocated from it is live
+  if (c->pinned) cudaFreeHost(c->pinned);
   delete c;
   return ITS_OK;
 }

@@ -246,7 +246,8 @@ static its_status ensureWork(its_op* op) {
   if (!op->workf && (st = devAlloc(ctx, (void**)&op->workf, 2 * op->n * 4)) != ITS_OK) return st;
   if (!op->scalars && (st = devAlloc(ctx, &op->scalars, sizeof(CgScalars))) != ITS_OK) return st;
   if (!op->partials && (st = devAlloc(ctx, (void**)&op->partials, 2 * 8 * 4096 * 8)) != ITS_OK) return st;
-  if (!op->hostDone) ITS_CU(ctx, cudaMallocHost((void**)&op->hostDone, 64));
+  op->hostDone = ctx->pinned;
+  if (!op->hostDone) return setError(ctx, ITS_ERR_STATE, "context has no pinned scratch");
   return ITS_OK;
 }
 static Work workOf(its_op* op) {
@@ -479,7 +480,6 @@ void releaseSolver(its_op* op) {
   devFree(op->ctx, op->workf);
   devFree(op->ctx, op->scalars);
   devFree(op->ctx, op->partials);
-  if (op->hostDone) cudaFreeHost(op->hostDone);
   op->work = nullptr;
   op->workf = nullptr;
   op->scalars = nullptr;

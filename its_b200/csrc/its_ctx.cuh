@@ -14,6 +14,8 @@ struct its_ctx {
   std::string lastError;
   int64_t launches = 0;
   int numSMs = 148;
+  cudaMemPool_t pool = nullptr;  // the context's stream-ordered allocator
+  int* pinned = nullptr;         // 256 bytes of pinned host memory for small device reads
 };
 
 namespace its {
@@ -29,7 +31,8 @@ namespace its {
 inline its_status devAlloc(its_ctx* ctx, void** p, size_t bytes) {
   *p = nullptr;
   if (bytes == 0) return ITS_OK;
-  cudaError_t e = cudaMallocAsync(p, bytes, ctx->stream);
+  cudaError_t e = ctx->pool ? cudaMallocFromPoolAsync(p, bytes, ctx->pool, ctx->stream)
+                            : cudaMallocAsync(p, bytes, ctx->stream);
   if (e != cudaSuccess) {
     cudaGetLastError();
     *p = nullptr;

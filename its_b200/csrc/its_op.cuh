@@ -25,7 +25,7 @@ struct its_op {
   float* workf = nullptr;
   void* scalars = nullptr;
   double* partials = nullptr;
-  int* hostDone = nullptr;  // pinned
+  int* hostDone = nullptr;  // the context's pinned scratch
   cudaGraphExec_t graph = nullptr;
   int64_t graphLaunches = 0;  // kernels per graph launch
   int graphKey[4] = {-1, -1, -1, -1};

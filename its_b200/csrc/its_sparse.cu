@@ -6,6 +6,20 @@
 namespace its {
 
 // ---- row bins ---------------------------------------------------------------------------
+// Long row j is cut into segments first[j] .. first[j+1]-1 of kSegLen entries each.
+__global__ void kFillSegments(int64_t nLong, const uint32_t* __restrict__ longRows,
+                              const uint32_t* __restrict__ first, const int64_t* __restrict__ rowptr,
+                              uint32_t* __restrict__ segRow, int64_t* __restrict__ segBeg) {
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j >= nLong) return;
+  const uint32_t row = longRows[j];
+  const int64_t beg = rowptr[row];
+  for (uint32_t s = first[j]; s < first[j + 1]; ++s) {
+    segRow[s] = row;
+    segBeg[s] = beg + (int64_t)(s - first[j]) * kSegLen;
+  }
+}
+
 its_status buildSpmvPlan(its_ctx* ctx, int64_t n, const int64_t* rowptr, SpmvPlan* P) {
   *P = SpmvPlan();
   its_status st;
@@ -61,23 +75,9 @@ its_status buildSpmvPlan(its_ctx* ctx, int64_t n, const int64_t* rowptr, SpmvPla
     if ((st = devAlloc(ctx, (void**)&P->segRow, nseg * 4)) != ITS_OK) return st;
     if ((st = devAlloc(ctx, (void**)&P->segBeg, nseg * 8)) != ITS_OK) return st;
     if ((st = devAlloc(ctx, (void**)&P->segPartial, nseg * 8)) != ITS_OK) return st;
-    std::vector<uint32_t> hl(P->nLong), hf(P->nLong + 1);
-    ITS_CU(ctx, cudaMemcpyAsync(hl.data(), P->longRows, P->nLong * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    ITS_CU(ctx, cudaMemcpyAsync(hf.data(), P->longFirstSeg, (P->nLong + 1) * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    std::vector<int64_t> rb(P->nLong);
-    for (int64_t r = 0; r < P->nLong; ++r)
-      ITS_CU(ctx, cudaMemcpyAsync(&rb[r], rowptr + hl[r], 8, cudaMemcpyDeviceToHost, ctx->stream));
-    ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
-    std::vector<uint32_t> sr(nseg);
-    std::vector<int64_t> sb(nseg);
-    for (int64_t r = 0; r < P->nLong; ++r)
-      for (uint32_t k = hf[r]; k < hf[r + 1]; ++k) {
-        sr[k] = hl[r];
-        sb[k] = rb[r] + (int64_t)(k - hf[r]) * kSegLen;
-      }
-    ITS_CU(ctx, cudaMemcpyAsync(P->segRow, sr.data(), nseg * 4, cudaMemcpyHostToDevice, ctx->stream));
-    ITS_CU(ctx, cudaMemcpyAsync(P->segBeg, sb.data(), nseg * 8, cudaMemcpyHostToDevice, ctx->stream));
-    ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    kFillSegments<<<gridFor(P->nLong, 128), 128, 0, ctx->stream>>>(P->nLong, P->longRows, P->longFirstSeg, rowptr,
+                                                                 P->segRow, P->segBeg);
+    ITS_LAUNCHED(ctx);
   }
   return ITS_OK;
 }
