@@ -186,6 +186,15 @@ its_status its_eval_grid(its_svo* svo, const double* lambda, const double origin
 its_status its_marching_cubes(its_ctx* ctx, const double* field, int res, const double origin[3],
                               const double width[3], double iso, uint8_t* cube_index, double* tri_verts,
                               int64_t capacity, int64_t* num_verts);
+/* No counterpart in the reference. The same results as its_marching_cubes for callers that
+   cannot allocate device memory while they run (work replayed in a caller-captured CUDA
+   graph, a fixed memory budget): no cudaMalloc/cudaFree, the scan scratch is a fixed 64 KiB
+   file-scope device array. field, cube_index and tri_verts must be device memory; res <= 256
+   (ITS_ERR_INVALID beyond). Calls on one device share the array (overlapping calls race) and
+   the first call on a device looks up its address: make it before any stream capture. */
+its_status its_marching_cubes_noalloc(its_ctx* ctx, const double* field, int res, const double origin[3],
+                                      const double width[3], double iso, uint8_t* cube_index, double* tri_verts,
+                                      int64_t capacity, int64_t* num_verts);
 
 #ifdef __cplusplus
 }
