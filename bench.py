@@ -111,6 +111,29 @@ def dist_setup(args):
     return rank, world, local
 
 
+def max_over_ranks(value, dist=None, device="cuda"):
+    """Max of a per-rank time over all ranks (every rank must call it at the same point)."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def lpt_shard(costs, world):
+    """Longest-processing-time-first assignment of independent meshes to ranks.
+
+    Returns one list of item indices per rank; each list is in ascending index order."""
+    loads = [0.0] * world
+    parts = [[] for _ in range(world)]
+    for i in sorted(range(len(costs)), key=lambda k: (-costs[k], k)):
+        r = min(range(world), key=lambda k: (loads[k], k))
+        parts[r].append(i)
+        loads[r] += costs[i]
+    return [sorted(p) for p in parts]
+
+
 def run_ours(args):
     import torch
     from its_b200 import OP_FP32_VALUES, PREC_MIXED, STOP_RESIDUAL, Context, Operator, Svo, lib
@@ -127,7 +150,11 @@ def run_ours(args):
     wl = WORKLOADS[args.config]
     V, F, o, w = prepared(wl)
     ctx = Context(local)
-    stream = torch.cuda.current_stream()
+    # One non-default stream for everything: libits, torch's own ops (the L2 flush) and the
+    # timing events. (Handing libits the legacy default stream, handle 0, would select the
+    # context's own non-blocking stream and the events would not bracket its kernels.)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
 
     def barrier_sync():
@@ -144,12 +171,8 @@ def run_ours(args):
         e1.synchronize()
         return e0.elapsed_time(e1) / reps
 
-    def max_over_ranks(v):
-        if not pg:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+    def max_ranks(v):
+        return max_over_ranks(v, pg, "cuda")
 
     # ---- setup: octree and right-hand side (signed distance at the corner vertices) ------
     svo_ms = timed(lambda: Svo(ctx, V, F, wl["res"], o, w).close(), 2)
@@ -180,7 +203,7 @@ def run_ours(args):
     launches = ctx.kernel_launches - launches0
     barrier_sync()
     clk = clocks.stop()
-    fit_ms = max_over_ranks(fit_ms)
+    fit_ms = max_ranks(fit_ms)
     rep, nnz = rep_box["rep"], rep_box["nnz"]
     if args.only == "fit":
         if rank == 0:
@@ -214,7 +237,7 @@ def run_ours(args):
     for _ in range(args.steps):
         e2e_step()
     torch.cuda.synchronize()
-    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps)
+    e2e_ms = max_ranks((time.perf_counter() - t0) * 1e3 / args.steps)
 
     # ---- mixed precision fit -----------------------------------------------------------------
     rep_m = {}
@@ -227,7 +250,7 @@ def run_ours(args):
         op.close()
 
     mixed_step()
-    mixed_ms = max_over_ranks(timed(mixed_step, max(1, args.steps // 2)))
+    mixed_ms = max_ranks(timed(mixed_step, max(1, args.steps // 2)))
 
     # ---- roofline of the dominant kernel: the binned CSR SpMV ------------------------------
     op = Operator(svo)

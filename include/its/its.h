@@ -163,6 +163,16 @@ its_status its_solve_opts_default(its_solve_opts* opts);
 its_status its_lscg_solve(its_op* op, const double* b, double* lambda, const its_solve_opts* opts,
                           its_solve_report* report);
 
+/* Batched form of its_lscg_solve for many independent fits (one operator per mesh, all on one
+   context): every mesh runs Eigen's CGLS with its own scalars, stopping test and iteration
+   count, but each SpMV and reduction covers the whole batch in one launch and converged
+   meshes drop out. b[i] and lambda[i] are mesh i's vectors (host or device); opts->x0, when
+   set, points to an array of count warm-start vectors. FP64 only. reports has count entries
+   (ms is the batch's device time). No single-call counterpart in the reference, which fits
+   one mesh per ThinShells object (src/ThinShells.cpp:615-617). */
+its_status its_lscg_solve_batch(its_op* const* ops, int64_t count, const double* const* b, double* const* lambda,
+                                const its_solve_opts* opts, its_solve_report* reports);
+
 /* ---- a13: field at points and the shell iso levels ------------------------------------- */
 /* ThinShells::cpLatentBSplineValue (src/ThinShells.cpp:655-755): each point's fine node by
    Morton code, then lambda times the hats of the 8 corners of that node and of every
@@ -173,6 +183,15 @@ its_status its_eval_points(its_svo* svo, const double* lambda, const double* poi
    over the points, skipping points outside every fine node. */
 its_status its_shell_iso_values(its_svo* svo, const double* lambda, const double* points, int64_t npoints,
                                 double* inner, double* outer, int64_t* num_missing);
+
+/* ThinShells::multiPointQuery (src/ThinShells.cpp:1183-1420; CUDA branch cuAcc::cpPointQuery,
+   src/cuAcc/CUDACompute.cu:1070-1156): field at arbitrary points (the sum over all corner
+   vertices, evaluated through the lattice), points outside the model box grown by one box
+   width taking the outer iso value; label 1 (value >= outer), -1 (value <= inner) or 0
+   (between: inside the thin shell). values or labels may be NULL. */
+its_status its_point_query(its_svo* svo, const double* lambda, const double* points, int64_t npoints,
+                           const double box_origin[3], const double box_end[3], double inner, double outer,
+                           double* values, int8_t* labels);
 
 /* ---- a14-a15: dense field and marching cubes -------------------------------------------- */
 /* The field of MC::launch_computSDFKernel (src/cuAcc/MarchingCubes/MarchingCubes.cu:464-536,
@@ -186,6 +205,14 @@ its_status its_eval_grid(its_svo* svo, const double* lambda, const double origin
 its_status its_marching_cubes(its_ctx* ctx, const double* field, int res, const double origin[3],
                               const double width[3], double iso, uint8_t* cube_index, double* tri_verts,
                               int64_t capacity, int64_t* num_verts);
+/* Welded, indexed form of MC::marching_cubes' triangle soup (writeToOBJFile,
+   src/cuAcc/MarchingCubes/MarchingCubes.cu:635-661, emits 3 fresh vertices per triangle): one
+   vertex per active lattice edge (numbered in edge-id order, id = 3*((z*(res+1)+y)*(res+1)+x)+axis)
+   placed by the reference's lerp from the lower to the upper lattice point, and triangles as
+   int32 index triples in voxel order with the soup's winding. NULL outputs: counts only. */
+its_status its_marching_cubes_mesh(its_ctx* ctx, const double* field, int res, const double origin[3],
+                                   const double width[3], double iso, double* verts, int64_t vert_capacity,
+                                   int64_t* num_verts, int32_t* tris, int64_t tri_capacity, int64_t* num_tris);
 /* No counterpart in the reference. The same results as its_marching_cubes for callers that
    cannot allocate device memory while they run (work replayed in a caller-captured CUDA
    graph, a fixed memory budget): no cudaMalloc/cudaFree, the scan scratch is a fixed 64 KiB

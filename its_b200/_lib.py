@@ -60,10 +60,13 @@ SIGNATURES = {
     "its_operator_apply": (st, [vp, vp, vp, i32]),
     "its_solve_opts_default": (st, [C.POINTER(SolveOpts)]),
     "its_lscg_solve": (st, [vp, vp, vp, C.POINTER(SolveOpts), C.POINTER(SolveReport)]),
+    "its_lscg_solve_batch": (st, [vp, i64, vp, vp, C.POINTER(SolveOpts), vp]),
     "its_eval_points": (st, [vp, vp, vp, i64, vp, vp]),
     "its_shell_iso_values": (st, [vp, vp, vp, i64, C.POINTER(dbl), C.POINTER(dbl), C.POINTER(i64)]),
     "its_eval_grid": (st, [vp, vp, vp, vp, i32, vp]),
+    "its_point_query": (st, [vp, vp, vp, i64, vp, vp, dbl, dbl, vp, vp]),
     "its_marching_cubes": (st, [vp, vp, i32, vp, vp, dbl, vp, vp, i64, C.POINTER(i64)]),
+    "its_marching_cubes_mesh": (st, [vp, vp, i32, vp, vp, dbl, vp, i64, C.POINTER(i64), vp, i64, C.POINTER(i64)]),
 }
 
 _lib = None

@@ -53,6 +53,7 @@ class Context:
             raise ItsError(s, "its_create(device=%d) failed" % device)
         self.h = h
         self.device = device
+        self._L = lib()  # kept for close() at interpreter shutdown, when module globals are gone
         self._children = weakref.WeakSet()  # objects that must be freed before the context
 
     def check(self, s, what):
@@ -65,9 +66,9 @@ class Context:
     def close(self):
         """Free every octree/operator made on this context, then the context itself."""
         if getattr(self, "h", None):
-            for obj in sorted(list(self._children), key=lambda o: 0 if isinstance(o, Operator) else 1):
+            for obj in sorted(list(self._children), key=lambda o: 0 if type(o).__name__ == "Operator" else 1):
                 obj.close()
-            lib().its_destroy(self.h)
+            self._L.its_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -116,6 +117,22 @@ class Context:
         return cube, tri, int(n.value)
 
 
+def _mc_mesh(ctx, field, res, origin, width, iso):
+    field = _f64(field)
+    o, w = np.ascontiguousarray(origin, np.float64), np.ascontiguousarray(width, np.float64)
+    nv, nt = C.c_int64(0), C.c_int64(0)
+    L = lib()
+    ctx.check(L.its_marching_cubes_mesh(ctx.h, _ptr(field), res, _ptr(o), _ptr(w), float(iso), None, 0, C.byref(nv),
+                                        None, 0, C.byref(nt)), "its_marching_cubes_mesh")
+    verts, tris = np.zeros((max(nv.value, 1), 3)), np.zeros((max(nt.value, 1), 3), np.int32)
+    ctx.check(L.its_marching_cubes_mesh(ctx.h, _ptr(field), res, _ptr(o), _ptr(w), float(iso), _ptr(verts), nv.value,
+                                        C.byref(nv), _ptr(tris), nt.value, C.byref(nt)), "its_marching_cubes_mesh")
+    return verts[:nv.value], tris[:nt.value]
+
+
+Context.marching_cubes_mesh = _mc_mesh
+
+
 def model_to_unit_cube(V, scale=1.0):
     V = np.ascontiguousarray(V, np.float64).copy()
     s = lib().its_model_to_unit_cube(_ptr(V), _n(V), scale)
@@ -157,7 +174,7 @@ class Svo:
     def close(self):
         if getattr(self, "h", None):
             if self.ctx.h is not None:  # a closed context has already freed its objects
-                lib().its_svo_free(self.h)
+                self.ctx._L.its_svo_free(self.h)
             self.h = None
 
     def __del__(self):
@@ -219,6 +236,16 @@ class Svo:
                                                   C.byref(miss)), "its_shell_iso_values")
         return lo.value, hi.value, int(miss.value)
 
+    def point_query(self, lam, P, box_origin, box_end, inner, outer):
+        """Values and in/shell/out labels (1 outside, -1 inside, 0 in the shell) of points."""
+        lam, P = _f64(lam), _f64(P)
+        m = _n(P)
+        vals, labels = np.zeros(m), np.zeros(m, np.int8)
+        bo, be = np.ascontiguousarray(box_origin, np.float64), np.ascontiguousarray(box_end, np.float64)
+        self.ctx.check(lib().its_point_query(self.h, _ptr(lam), _ptr(P), m, _ptr(bo), _ptr(be), float(inner),
+                                             float(outer), _ptr(vals), _ptr(labels)), "its_point_query")
+        return vals, labels
+
     def eval_grid(self, lam, origin, width, res, out=None):
         lam = _f64(lam)
         o, w = np.ascontiguousarray(origin, np.float64), np.ascontiguousarray(width, np.float64)
@@ -249,7 +276,7 @@ class Operator:
     def close(self):
         if getattr(self, "h", None):
             if self.ctx.h is not None:
-                lib().its_operator_free(self.h)
+                self.ctx._L.its_operator_free(self.h)
             self.h = None
 
     def __del__(self):
@@ -292,3 +319,34 @@ class Operator:
         return out, dict(iterations=rep.iterations, converged=bool(rep.converged), breakdown=bool(rep.breakdown),
                          rel_residual=rep.rel_residual, normal_rel_residual=rep.normal_rel_residual, ms=rep.ms,
                          inner_iterations=rep.inner_iterations)
+
+
+def solve_batch(ops, bs, tol=None, max_iters=0, stop_rule=STOP_NORMAL, check_every=0, x0s=None, outs=None):
+    """Batched LSCG over independent operators of one context (its_lscg_solve_batch).
+
+    Returns (list of lambdas, list of report dicts)."""
+    count = len(ops)
+    ctx = ops[0].ctx
+    opts = SolveOpts()
+    lib().its_solve_opts_default(C.byref(opts))
+    if tol is not None:
+        opts.tol = tol
+    opts.max_iters, opts.stop_rule = max_iters, stop_rule
+    if check_every:
+        opts.check_every = check_every
+    bs = [_f64(b) for b in bs]
+    outs = outs if outs is not None else [np.zeros(op.rows) for op in ops]
+    keep = None
+    if x0s is not None:
+        keep = [_f64(x) for x in x0s]
+        xarr = (C.c_void_p * count)(*[_ptr(x).value if isinstance(x, np.ndarray) else x.data_ptr() for x in keep])
+        opts.x0 = C.cast(xarr, C.c_void_p).value
+    H = (C.c_void_p * count)(*[op.h.value for op in ops])
+    B = (C.c_void_p * count)(*[_ptr(b).value if isinstance(b, np.ndarray) else b.data_ptr() for b in bs])
+    X = (C.c_void_p * count)(*[_ptr(x).value if isinstance(x, np.ndarray) else x.data_ptr() for x in outs])
+    reps = (SolveReport * count)()
+    ctx.check(lib().its_lscg_solve_batch(H, count, B, X, C.byref(opts), reps), "its_lscg_solve_batch")
+    out = [dict(iterations=r.iterations, converged=bool(r.converged), breakdown=bool(r.breakdown),
+                rel_residual=r.rel_residual, normal_rel_residual=r.normal_rel_residual, ms=r.ms) for r in reps]
+    del keep
+    return outs, out

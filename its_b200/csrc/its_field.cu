@@ -126,6 +126,31 @@ __global__ void kIsoPartials(const __grid_constant__ EvalParams P, const double*
   }
 }
 
+// The field at any point: sum over every corner vertex of lambda * hat, restricted to the
+// only terms that can be non-zero -- at each depth the 8 corners of the cell holding p that
+// exist as vertices of that depth -- summed depth 0..D-1, corners k = x|y<<1|z<<2.
+__device__ inline double fieldAt(const EvalParams& P, const double* __restrict__ lambda, double px, double py,
+                                 double pz) {
+  double sum = 0.0;
+  for (int d = 0; d < P.depth; ++d) {
+    const double w = P.w0 * (double)(1u << d);
+    const LatticeIndex& L = P.lat[d];
+    const int64_t lim = (int64_t)(P.res >> d);
+    const int64_t cx = (int64_t)floor((px - P.g.x) / w), cy = (int64_t)floor((py - P.g.y) / w),
+                  cz = (int64_t)floor((pz - P.g.z) / w);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int64_t Lx = cx + (k & 1), Ly = cy + ((k >> 1) & 1), Lz = cz + ((k >> 2) & 1);
+      if (Lx < 0 || Ly < 0 || Lz < 0 || Lx > lim || Ly > lim || Lz > lim) continue;
+      const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
+      if (!latticeHas(L, lin)) continue;
+      const uint32_t v = latticeRank(L, lin);
+      sum += lambda[v] * hat3(P.vertPos[3 * v], P.vertPos[3 * v + 1], P.vertPos[3 * v + 2], w, px, py, pz);
+    }
+  }
+  return sum;
+}
+
 // Field on the (R+1)^3 lattice, x fastest.
 __global__ void __launch_bounds__(256) kEvalGrid(const __grid_constant__ EvalParams P, const double* __restrict__ lambda,
                                                  double3 o, double3 vs, int R, double* __restrict__ field) {
@@ -135,25 +160,24 @@ __global__ void __launch_bounds__(256) kEvalGrid(const __grid_constant__ EvalPar
        idx += (int64_t)gridDim.x * blockDim.x) {
     const int64_t xi = idx % M, yj = (idx / M) % M, zk = idx / (M * M);
     const double px = o.x + (double)xi * vs.x, py = o.y + (double)yj * vs.y, pz = o.z + (double)zk * vs.z;
-    double sum = 0.0;
-    for (int d = 0; d < P.depth; ++d) {
-      const double w = P.w0 * (double)(1u << d);
-      const LatticeIndex& L = P.lat[d];
-      const int64_t lim = (int64_t)(P.res >> d);
-      const int64_t cx = (int64_t)floor((px - P.g.x) / w), cy = (int64_t)floor((py - P.g.y) / w),
-                    cz = (int64_t)floor((pz - P.g.z) / w);
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const int64_t Lx = cx + (k & 1), Ly = cy + ((k >> 1) & 1), Lz = cz + ((k >> 2) & 1);
-        if (Lx < 0 || Ly < 0 || Lz < 0 || Lx > lim || Ly > lim || Lz > lim) continue;
-        const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
-        if (!latticeHas(L, lin)) continue;
-        const uint32_t v = latticeRank(L, lin);
-        sum += lambda[v] * hat3(P.vertPos[3 * v], P.vertPos[3 * v + 1], P.vertPos[3 * v + 2], w, px, py, pz);
-      }
-    }
-    field[idx] = sum;
+    field[idx] = fieldAt(P, lambda, px, py, pz);
   }
+}
+
+// Point queries (ThinShells::multiPointQuery, ThinShells.cpp:1183-1420, CUDA branch
+// cuAcc::cpPointQuery, CUDACompute.cu:1070-1156): points outside the model box grown by one
+// box width on every side take the outer iso value; the others the field. Label: 1 when the
+// value >= outer, -1 when <= inner, else 0 (inside the shell).
+__global__ void kPointQuery(const __grid_constant__ EvalParams P, const double* __restrict__ lambda,
+                            const double* __restrict__ pts, int64_t m, double3 lo, double3 hi, double inner,
+                            double outer, double* __restrict__ values, int8_t* __restrict__ labels) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const double px = pts[3 * i], py = pts[3 * i + 1], pz = pts[3 * i + 2];
+  const bool outside = px < lo.x || py < lo.y || pz < lo.z || px > hi.x || py > hi.y || pz > hi.z;
+  const double v = outside ? outer : fieldAt(P, lambda, px, py, pz);
+  if (values) values[i] = v;
+  if (labels) labels[i] = (int8_t)(v >= outer ? 1 : (v <= inner ? -1 : 0));
 }
 
 }  // namespace its
@@ -218,6 +242,38 @@ its_status its_shell_iso_values(its_svo* s, const double* lambda, const double* 
   *inner = lo;
   *outer = hi;
   if (num_missing) *num_missing = (int64_t)miss;
+  return ITS_OK;
+}
+
+its_status its_point_query(its_svo* s, const double* lambda, const double* points, int64_t npoints,
+                           const double box_origin[3], const double box_end[3], double inner, double outer,
+                           double* values, int8_t* labels) {
+  if (!s || !lambda || !box_origin || !box_end || npoints < 0 || (npoints && !points)) return ITS_ERR_INVALID;
+  its_ctx* ctx = s->ctx;
+  if (npoints == 0) return ITS_OK;
+  ITS_CU(ctx, cudaSetDevice(ctx->device));
+  InArg<double> L, P;
+  OutArg<double> Va;
+  OutArg<int8_t> La;
+  its_status st;
+  if ((st = L.stage(ctx, lambda, s->d.numVerts)) != ITS_OK) return st;
+  if ((st = P.stage(ctx, points, 3 * npoints)) != ITS_OK) return st;
+  if ((st = Va.stage(ctx, values, npoints)) != ITS_OK) return st;
+  if ((st = La.stage(ctx, labels, npoints)) != ITS_OK) return st;
+  // minRange = boxOrigin - boxWidth, maxRange = boxEnd + boxWidth (ThinShells.cpp:1198-1199)
+  double lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) {
+    const double w = box_end[a] - box_origin[a];
+    lo[a] = box_origin[a] - w;
+    hi[a] = box_end[a] + w;
+  }
+  kPointQuery<<<gridFor(npoints, 128), 128, 0, ctx->stream>>>(evalParams(s->d), L.d, P.d, npoints,
+                                                             make_double3(lo[0], lo[1], lo[2]),
+                                                             make_double3(hi[0], hi[1], hi[2]), inner, outer, Va.d, La.d);
+  ITS_LAUNCHED(ctx);
+  if ((st = Va.finish(ctx)) != ITS_OK) return st;
+  if ((st = La.finish(ctx)) != ITS_OK) return st;
+  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   return ITS_OK;
 }
 

@@ -1,11 +1,36 @@
-// SpMV row binning and the stable radix sort used to transpose the operator.
-#include <vector>
-
+// SpMV row classes and the stable radix sort used to transpose the operator.
 #include "its_sparse.cuh"
 
 namespace its {
 
-// ---- row bins ---------------------------------------------------------------------------
+// ---- row classes --------------------------------------------------------------------------
+__host__ __device__ inline uint32_t rowClass(int64_t len) {
+  for (int c = 0; c < kLongClass; ++c)
+    if (len <= classMaxLen(c)) return (uint32_t)c;
+  return kLongClass;
+}
+__global__ void kRowClass(int64_t n, const int64_t* __restrict__ rowptr, uint32_t* __restrict__ cls,
+                          uint32_t* __restrict__ ids) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  cls[r] = rowClass(rowptr[r + 1] - rowptr[r]);
+  ids[r] = (uint32_t)r;
+}
+// Class boundaries in the class-sorted list: entry i opens classes (cls[i-1], cls[i]].
+__global__ void kClassBounds(int64_t n, const uint32_t* __restrict__ cls, int64_t* __restrict__ bounds) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i > n) return;
+  const int64_t c = (i < n) ? (int64_t)cls[i] : kNumClasses;
+  const int64_t prev = (i == 0) ? -1 : (int64_t)cls[i - 1];
+  for (int64_t k = prev + 1; k <= c; ++k) bounds[k] = i;
+}
+__global__ void kSegCounts(int64_t nLong, const uint32_t* __restrict__ longRows, const int64_t* __restrict__ rowptr,
+                           uint32_t* __restrict__ cnt) {
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j >= nLong) return;
+  const int64_t l = rowptr[longRows[j] + 1] - rowptr[longRows[j]];
+  cnt[j] = (uint32_t)((l + kSegLen - 1) / kSegLen);
+}
 // Long row j is cut into segments first[j] .. first[j+1]-1 of kSegLen entries each.
 __global__ void kFillSegments(int64_t nLong, const uint32_t* __restrict__ longRows,
                               const uint32_t* __restrict__ first, const int64_t* __restrict__ rowptr,
@@ -23,67 +48,63 @@ __global__ void kFillSegments(int64_t nLong, const uint32_t* __restrict__ longRo
 its_status buildSpmvPlan(its_ctx* ctx, int64_t n, const int64_t* rowptr, SpmvPlan* P) {
   *P = SpmvPlan();
   its_status st;
-  DevBuf<uint32_t> tShort, tMid, tLong, tot;
-  DevBuf<uint32_t> segCount;  // per long row
-  if ((st = tShort.alloc(ctx, n)) != ITS_OK) return st;
-  if ((st = tMid.alloc(ctx, n)) != ITS_OK) return st;
-  if ((st = tLong.alloc(ctx, n)) != ITS_OK) return st;
-  if ((st = tot.zeros(ctx, 4)) != ITS_OK) return st;
-  const int64_t* rp = rowptr;
-  uint32_t* ps = tShort.p;
-  uint32_t* pm = tMid.p;
-  uint32_t* pl = tLong.p;
-  auto fs = [rp] __device__(int64_t i) -> uint32_t { return (rp[i + 1] - rp[i]) <= kShortMax ? 1u : 0u; };
-  auto fm = [rp] __device__(int64_t i) -> uint32_t {
-    const int64_t l = rp[i + 1] - rp[i];
-    return (l > kShortMax && l <= kMidMax) ? 1u : 0u;
-  };
-  auto fl = [rp] __device__(int64_t i) -> uint32_t { return (rp[i + 1] - rp[i]) > kMidMax ? 1u : 0u; };
-  auto ws = [ps] __device__(int64_t i, uint32_t pre, uint32_t v) { if (v) ps[pre] = (uint32_t)i; };
-  auto wm = [pm] __device__(int64_t i, uint32_t pre, uint32_t v) { if (v) pm[pre] = (uint32_t)i; };
-  auto wl = [pl] __device__(int64_t i, uint32_t pre, uint32_t v) { if (v) pl[pre] = (uint32_t)i; };
-  if ((st = scanExclusiveAlloc<uint32_t>(ctx, fs, n, ws, tot.p + 0)) != ITS_OK) return st;
-  if ((st = scanExclusiveAlloc<uint32_t>(ctx, fm, n, wm, tot.p + 1)) != ITS_OK) return st;
-  if ((st = scanExclusiveAlloc<uint32_t>(ctx, fl, n, wl, tot.p + 2)) != ITS_OK) return st;
-  uint32_t h[4] = {0, 0, 0, 0};
-  ITS_CU(ctx, cudaMemcpyAsync(h, tot.p, 16, cudaMemcpyDeviceToHost, ctx->stream));
+  DevBuf<uint32_t> cls, ids, sortedCls, tk, tv;
+  DevBuf<int64_t> bounds;
+  if ((st = cls.alloc(ctx, n)) != ITS_OK || (st = ids.alloc(ctx, n)) != ITS_OK ||
+      (st = sortedCls.alloc(ctx, n)) != ITS_OK || (st = tk.alloc(ctx, n)) != ITS_OK ||
+      (st = tv.alloc(ctx, n)) != ITS_OK || (st = bounds.alloc(ctx, kNumClasses + 1)) != ITS_OK)
+    return st;
+  if ((st = devAlloc(ctx, (void**)&P->rows, n * 4)) != ITS_OK) return st;
+  kRowClass<<<gridFor(n, 256), 256, 0, ctx->stream>>>(n, rowptr, cls.p, ids.p);
+  ITS_LAUNCHED(ctx);
+  // one stable 8-bit pass groups the rows by class, ascending inside each class
+  if ((st = radixSortPairs(ctx, cls.p, ids.p, sortedCls.p, P->rows, tk.p, tv.p, n, 3)) != ITS_OK) return st;
+  kClassBounds<<<gridFor(n + 1, 256), 256, 0, ctx->stream>>>(n, sortedCls.p, bounds.p);
+  ITS_LAUNCHED(ctx);
+  int64_t hb[kNumClasses + 1];
+  ITS_CU(ctx, cudaMemcpyAsync(hb, bounds.p, sizeof(hb), cudaMemcpyDeviceToHost, ctx->stream));
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
-  P->nShort = h[0];
-  P->nMid = h[1];
-  P->nLong = h[2];
-  if ((st = devAlloc(ctx, (void**)&P->shortRows, P->nShort * 4)) != ITS_OK) return st;
-  if ((st = devAlloc(ctx, (void**)&P->midRows, P->nMid * 4)) != ITS_OK) return st;
-  if ((st = devAlloc(ctx, (void**)&P->longRows, P->nLong * 4)) != ITS_OK) return st;
-  if (P->nShort) ITS_CU(ctx, cudaMemcpyAsync(P->shortRows, tShort.p, P->nShort * 4, cudaMemcpyDeviceToDevice, ctx->stream));
-  if (P->nMid) ITS_CU(ctx, cudaMemcpyAsync(P->midRows, tMid.p, P->nMid * 4, cudaMemcpyDeviceToDevice, ctx->stream));
-  if (P->nLong) ITS_CU(ctx, cudaMemcpyAsync(P->longRows, tLong.p, P->nLong * 4, cudaMemcpyDeviceToDevice, ctx->stream));
-  P->shortBlocks = (unsigned)((P->nShort * 8 + kSpmvThreads - 1) / kSpmvThreads);
-  P->midBlocks = (unsigned)((P->nMid + kSpmvThreads / 32 - 1) / (kSpmvThreads / 32));
-  if (P->nLong) {
-    if ((st = devAlloc(ctx, (void**)&P->longFirstSeg, (P->nLong + 1) * 4)) != ITS_OK) return st;
-    const uint32_t* lr = P->longRows;
-    uint32_t* lfs = P->longFirstSeg;
-    auto fc = [rp, lr] __device__(int64_t i) -> uint32_t {
-      const int64_t l = rp[lr[i] + 1] - rp[lr[i]];
-      return (uint32_t)((l + kSegLen - 1) / kSegLen);
-    };
-    if ((st = scanExclusiveAlloc<uint32_t>(ctx, fc, P->nLong, StorePrefix<uint32_t>{lfs}, tot.p + 3)) != ITS_OK) return st;
-    ITS_CU(ctx, cudaMemcpyAsync(lfs + P->nLong, tot.p + 3, 4, cudaMemcpyDeviceToDevice, ctx->stream));
+  unsigned blk = 0;
+  for (int c = 0; c < kNumClasses; ++c) {
+    P->offset[c] = hb[c];
+    P->count[c] = hb[c + 1] - hb[c];
+    P->blockStart[c] = blk;
+    if (c < kLongClass) {
+      P->blocks[c] = (unsigned)((P->count[c] * classLanes(c) + kSpmvThreads - 1) / kSpmvThreads);
+      blk += P->blocks[c];
+    }
+  }
+  const int64_t nLong = P->nLong();
+  if (nLong) {
+    DevBuf<uint32_t> segCnt, tot;
+    if ((st = segCnt.alloc(ctx, nLong)) != ITS_OK || (st = tot.alloc(ctx, 1)) != ITS_OK) return st;
+    if ((st = devAlloc(ctx, (void**)&P->longFirstSeg, (nLong + 1) * 4)) != ITS_OK) return st;
+    const uint32_t* longRows = P->rows + P->offset[kLongClass];
+    kSegCounts<<<gridFor(nLong, 128), 128, 0, ctx->stream>>>(nLong, longRows, rowptr, segCnt.p);
+    ITS_LAUNCHED(ctx);
+    const uint32_t* sc = segCnt.p;
+    auto fc = [sc] __device__(int64_t i) -> uint32_t { return sc[i]; };
+    if ((st = scanExclusiveAlloc<uint32_t>(ctx, fc, nLong, StorePrefix<uint32_t>{P->longFirstSeg}, tot.p)) != ITS_OK)
+      return st;
+    ITS_CU(ctx, cudaMemcpyAsync(P->longFirstSeg + nLong, tot.p, 4, cudaMemcpyDeviceToDevice, ctx->stream));
     uint32_t nseg = 0;
-    if ((st = readScalar(ctx, tot.p + 3, &nseg)) != ITS_OK) return st;
+    if ((st = readScalar(ctx, tot.p, &nseg)) != ITS_OK) return st;
     P->nSeg = nseg;
     if ((st = devAlloc(ctx, (void**)&P->segRow, nseg * 4)) != ITS_OK) return st;
     if ((st = devAlloc(ctx, (void**)&P->segBeg, nseg * 8)) != ITS_OK) return st;
     if ((st = devAlloc(ctx, (void**)&P->segPartial, nseg * 8)) != ITS_OK) return st;
-    kFillSegments<<<gridFor(P->nLong, 128), 128, 0, ctx->stream>>>(P->nLong, P->longRows, P->longFirstSeg, rowptr,
-                                                                 P->segRow, P->segBeg);
+    kFillSegments<<<gridFor(nLong, 128), 128, 0, ctx->stream>>>(nLong, longRows, P->longFirstSeg, rowptr, P->segRow,
+                                                              P->segBeg);
     ITS_LAUNCHED(ctx);
   }
+  P->blocks[kLongClass] = (unsigned)P->nSeg;
+  P->blockStart[kLongClass] = blk;
+  P->blockStart[kNumClasses] = blk + (unsigned)P->nSeg;
   return ITS_OK;
 }
 
 void releasePlan(its_ctx* ctx, SpmvPlan* P) {
-  void* ptrs[] = {P->shortRows, P->midRows, P->longRows, P->longFirstSeg, P->segRow, P->segBeg, P->segPartial};
+  void* ptrs[] = {P->rows, P->longFirstSeg, P->segRow, P->segBeg, P->segPartial};
   for (void* p : ptrs) devFree(ctx, p);
   *P = SpmvPlan();
 }
@@ -108,6 +129,8 @@ __global__ void __launch_bounds__(kRsThreads) kRadixUpsweep(const uint32_t* __re
   blockHist[(int64_t)threadIdx.x * nb + blockIdx.x] = hist[threadIdx.x];
 }
 
+// Stable scatter: items of a tile are ranked in (round, warp, lane) order, which is their
+// order in the input; warps find same-digit peers with __match_any_sync.
 __global__ void __launch_bounds__(kRsThreads) kRadixDownsweep(const uint32_t* __restrict__ keys,
                                                               const uint32_t* __restrict__ vals, int64_t n, int shift,
                                                               const uint32_t* __restrict__ offsets, int64_t nb,

@@ -63,6 +63,8 @@ def _declare(L):
         "orc_eval_brute": (None, [vp, vp, vp, i64, vp]),
         "orc_eval_grid": (None, [vp, vp, vp, vp, i32, vp]),
         "orc_marching_cubes": (i64, [vp, i32, vp, vp, dbl, vp, vp, i64]),
+        "orc_point_query": (None, [vp, vp, vp, i64, vp, vp, dbl, dbl, vp, vp]),
+        "orc_marching_cubes_mesh": (None, [vp, i32, vp, vp, dbl, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -200,6 +202,13 @@ class Svo:
         lib().orc_eval_brute(self.h, _p(lam), _p(P), P.shape[0], _p(out))
         return out
 
+    def point_query(self, lam, P, box_origin, box_end, inner, outer):
+        lam, P = _f64(lam), _f64(P)
+        vals, labels = np.zeros(P.shape[0]), np.zeros(P.shape[0], np.int8)
+        lib().orc_point_query(self.h, _p(lam), _p(P), P.shape[0], _p(_f64(box_origin)), _p(_f64(box_end)),
+                              float(inner), float(outer), _p(vals), _p(labels))
+        return vals, labels
+
     def eval_grid(self, lam, origin, width, R):
         lam = _f64(lam)
         out = np.zeros((R + 1) ** 3)
@@ -228,6 +237,16 @@ def signed_distance(P, V, F):
     out = np.zeros(P.shape[0])
     lib().orc_signed_distance(_p(P), P.shape[0], _p(V), _p(F), F.shape[0], _p(out))
     return out
+
+
+def marching_cubes_mesh(field, R, origin, width, iso):
+    field = _f64(field)
+    cnt = np.zeros(2, np.int64)
+    o, w = _f64(origin), _f64(width)
+    lib().orc_marching_cubes_mesh(_p(field), R, _p(o), _p(w), iso, None, None, _p(cnt))
+    verts, tris = np.zeros((max(cnt[0], 1), 3)), np.zeros((max(cnt[1], 1), 3), np.int32)
+    lib().orc_marching_cubes_mesh(_p(field), R, _p(o), _p(w), iso, _p(verts), _p(tris), _p(cnt))
+    return verts[:cnt[0]], tris[:cnt[1]]
 
 
 def marching_cubes(field, R, origin, width, iso, with_triangles=True):

@@ -148,6 +148,21 @@ void orc_eval_brute(void* h, const double* lambda, const double* P, int64_t m, d
 void orc_eval_grid(void* h, const double* lambda, const double* origin, const double* width, int R, double* out) {
   evalGrid(*static_cast<Svo*>(h), lambda, origin, width, R, out);
 }
+// Two calls: with verts/tris NULL the counts; then the arrays.
+void orc_marching_cubes_mesh(const double* field, int R, const double* origin, const double* width, double iso,
+                             double* verts, int32_t* tris, int64_t* counts) {
+  std::vector<double> v;
+  std::vector<int32_t> t;
+  marchingCubesMesh(field, R, origin, width, iso, v, t);
+  counts[0] = (int64_t)(v.size() / 3);
+  counts[1] = (int64_t)(t.size() / 3);
+  if (verts) std::memcpy(verts, v.data(), v.size() * sizeof(double));
+  if (tris) std::memcpy(tris, t.data(), t.size() * sizeof(int32_t));
+}
+void orc_point_query(void* h, const double* lambda, const double* P, int64_t m, const double* boxOrigin,
+                     const double* boxEnd, double inner, double outer, double* values, int8_t* labels) {
+  pointQuery(*static_cast<Svo*>(h), lambda, P, m, boxOrigin, boxEnd, inner, outer, values, labels);
+}
 int64_t orc_marching_cubes(const double* field, int R, const double* origin, const double* width, double iso,
                            uint8_t* cube, double* tri, int64_t maxVerts) {
   return marchingCubes(field, R, origin, width, iso, cube, tri, maxVerts);

@@ -480,6 +480,57 @@ void evalGrid(const Svo& s, const double* lambda, const double origin[3], const 
       }
 }
 
+// Point queries (ThinShells::multiPointQuery, ThinShells.cpp:1183-1420, CUDA branch):
+// outside [boxOrigin - boxWidth, boxEnd + boxWidth] the value is the outer iso level, else
+// the field (the sparse equivalent of the sum over all corner vertices, as in evalGrid);
+// label 1 if value >= outer, -1 if value <= inner, 0 otherwise.
+void pointQuery(const Svo& s, const double* lambda, const double* P, int64_t m, const double boxOrigin[3],
+                const double boxEnd[3], double inner, double outer, double* values, int8_t* labels) {
+  std::vector<std::unordered_map<uint64_t, size_t>> key2v(s.treeDepth);
+  for (int d = 0; d < s.treeDepth; ++d) {
+    const double w = s.unit.x * (double)(1u << d);
+    for (size_t j = 0; j < s.depthVerts[d].size(); ++j) {
+      const V3 pos = s.depthVerts[d][j].pos;
+      uint64_t key = 0;
+      for (int a = 0; a < 3; ++a) key = key * 4096 + (uint64_t)std::llround((pos[a] - s.gridOrigin[a]) / w);
+      key2v[d].emplace(key, s.esumVerts[d] + j);
+    }
+  }
+  double lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) {
+    const double w = boxEnd[a] - boxOrigin[a];
+    lo[a] = boxOrigin[a] - w;
+    hi[a] = boxEnd[a] + w;
+  }
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < m; ++i) {
+    const V3 p{P[3 * i], P[3 * i + 1], P[3 * i + 2]};
+    double v;
+    if (p.x < lo[0] || p.y < lo[1] || p.z < lo[2] || p.x > hi[0] || p.y > hi[1] || p.z > hi[2]) {
+      v = outer;
+    } else {
+      double sum = 0.0;
+      for (int d = 0; d < s.treeDepth; ++d) {
+        const double w = s.unit.x * (double)(1u << d);
+        const int64_t lim = (int64_t)(s.res >> d);
+        int64_t c[3];
+        for (int a = 0; a < 3; ++a) c[a] = (int64_t)std::floor((p[a] - s.gridOrigin[a]) / w);
+        for (int k = 0; k < 8; ++k) {
+          const int64_t L[3] = {c[0] + (k & 1), c[1] + ((k >> 1) & 1), c[2] + ((k >> 2) & 1)};
+          if (L[0] < 0 || L[1] < 0 || L[2] < 0 || L[0] > lim || L[1] > lim || L[2] > lim) continue;
+          auto it = key2v[d].find(((uint64_t)L[0] * 4096 + (uint64_t)L[1]) * 4096 + (uint64_t)L[2]);
+          if (it == key2v[d].end()) continue;
+          const VertexRec& vr = s.depthVerts[d][it->second - s.esumVerts[d]];
+          sum += lambda[it->second] * baseFunction4Point(vr.pos, w, p);
+        }
+      }
+      v = sum;
+    }
+    if (values) values[i] = v;
+    if (labels) labels[i] = (int8_t)(v >= outer ? 1 : (v <= inner ? -1 : 0));
+  }
+}
+
 // ---- marching cubes: MarchingCubes.cu:164-377 on a shared-corner lattice --------------
 static const uint64_t kMcCase[256] = {
 #include "../its_b200/csrc/mc_tables.inc"
@@ -545,6 +596,48 @@ int64_t marchingCubes(const double* field, int R, const double origin[3], const 
     }
   }
   return total;
+}
+
+// Welded marching-cubes mesh: one vertex per active lattice edge (the two end values on
+// different sides of iso), numbered in edge-id order id = 3*lin(lower end) + axis, placed by
+// the reference's lerp from the lower to the upper end point; triangles from the case table.
+void marchingCubesMesh(const double* field, int R, const double origin[3], const double width[3], double iso,
+                       std::vector<double>& verts, std::vector<int32_t>& tris) {
+  const int64_t M = R + 1;
+  const double vs[3] = {width[0] / R, width[1] / R, width[2] / R};
+  auto f = [&](int64_t x, int64_t y, int64_t z) { return field[(z * M + y) * M + x]; };
+  std::vector<int32_t> index(3 * M * M * M, -1);
+  verts.clear();
+  tris.clear();
+  for (int64_t id = 0; id < 3 * M * M * M; ++id) {
+    const int64_t lin = id / 3;
+    const int a = (int)(id % 3);
+    const int64_t x = lin % M, y = (lin / M) % M, z = lin / (M * M);
+    const int64_t x1 = x + (a == 0), y1 = y + (a == 1), z1 = z + (a == 2);
+    if (x1 >= M || y1 >= M || z1 >= M) continue;
+    if ((f(x, y, z) < iso) == (f(x1, y1, z1) < iso)) continue;
+    const V3 p0{origin[0] + (double)x * vs[0], origin[1] + (double)y * vs[1], origin[2] + (double)z * vs[2]};
+    const V3 p1{origin[0] + (double)x1 * vs[0], origin[1] + (double)y1 * vs[1], origin[2] + (double)z1 * vs[2]};
+    const V3 q = vertexLerp(p0, p1, f(x, y, z), f(x1, y1, z1), iso);
+    index[id] = (int32_t)(verts.size() / 3);
+    verts.insert(verts.end(), {q.x, q.y, q.z});
+  }
+  for (int64_t v = 0; v < (int64_t)R * R * R; ++v) {
+    const int64_t x = v % R, y = (v / R) % R, z = v / ((int64_t)R * R);
+    unsigned ci = 0;
+    for (int k = 0; k < 8; ++k)
+      ci |= (unsigned)(f(x + kMcCorner[k][0], y + kMcCorner[k][1], z + kMcCorner[k][2]) < iso) << k;
+    const uint64_t cw = kMcCase[ci];
+    const unsigned n = (unsigned)(cw & 15u);
+    for (unsigned i = 0; i < n; ++i) {
+      const int e = (int)((cw >> (4 * (i + 1))) & 15u);
+      const int* A = kMcCorner[kMcEdge[e][0]];
+      const int* B = kMcCorner[kMcEdge[e][1]];
+      const int64_t lx = x + std::min(A[0], B[0]), ly = y + std::min(A[1], B[1]), lz = z + std::min(A[2], B[2]);
+      const int axis = A[0] != B[0] ? 0 : (A[1] != B[1] ? 1 : 2);
+      tris.push_back(index[((lz * M + ly) * M + lx) * 3 + axis]);
+    }
+  }
 }
 
 }  // namespace orc

@@ -27,7 +27,11 @@ CglsReport cgls(const Csr& A, const Csr& T, const double* b, double* x, double t
 void evalPoints(const Svo& s, const double* lambda, const double* P, int64_t m, double* out, uint8_t* missing);
 void evalBrute(const Svo& s, const double* lambda, const double* P, int64_t m, double* out);
 void evalGrid(const Svo& s, const double* lambda, const double origin[3], const double width[3], int R, double* out);
+void pointQuery(const Svo& s, const double* lambda, const double* P, int64_t m, const double boxOrigin[3],
+                const double boxEnd[3], double inner, double outer, double* values, int8_t* labels);
 int64_t marchingCubes(const double* field, int R, const double origin[3], const double width[3], double iso,
                       uint8_t* cubeIndex, double* tri, int64_t maxVerts);
+void marchingCubesMesh(const double* field, int R, const double origin[3], const double width[3], double iso,
+                       std::vector<double>& verts, std::vector<int32_t>& tris);
 
 }  // namespace orc

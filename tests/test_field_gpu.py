@@ -70,6 +70,45 @@ def test_grid_field_bit_exact_and_matches_brute_force(fitted, R):
 
 
 @pytest.mark.gpu
+def test_point_query_bit_exact(fitted):
+    V, F, o, w, ref, gpu, pos, b, lam = fitted
+    pts, _ = gpu.shell_samples(V, F)
+    lo, hi, _ = gpu.shell_iso_values(lam, np.vstack([V, pts]))
+    e = o + w
+    rng = np.random.default_rng(5)
+    P = np.vstack([o - w + 3 * w * rng.random((3000, 3)),          # includes points outside the range
+                   V[:500] + rng.normal(0, 1e-3, (500, 3))])       # near the surface
+    v_gpu, l_gpu = gpu.point_query(lam, P, o, e, lo, hi)
+    v_ref, l_ref = ref.point_query(lam, P, o, e, lo, hi)
+    assert np.array_equal(v_gpu, v_ref) and np.array_equal(l_gpu, l_ref)
+    assert set(np.unique(l_gpu)) == {-1, 0, 1}
+    inside = np.all((P >= o - w) & (P <= e + w), axis=1)
+    brute = ref.eval_brute(lam, P[inside][:400])
+    assert np.allclose(v_gpu[inside][:400], brute, rtol=0, atol=1e-14)
+    assert np.all(v_gpu[~inside] == hi)
+
+
+@pytest.mark.gpu
+def test_welded_mc_mesh(ctx, fitted):
+    V, F, o, w, ref, gpu, pos, b, lam = fitted
+    R = 40
+    field = gpu.eval_grid(lam, o, w, R)
+    verts, tris = ctx.marching_cubes_mesh(field, R, o, w, 0.0)
+    rv, rt = oracle.marching_cubes_mesh(field, R, o, w, 0.0)
+    assert np.array_equal(verts, rv) and np.array_equal(tris, rt)
+    # same surface as the soup: every soup vertex is a welded vertex (up to the lerp's end
+    # point order), and the soup has 3 vertices per welded triangle
+    _, soup, n = ctx.marching_cubes(field, R, o, w, 0.0)
+    assert n == 3 * len(tris)
+    assert np.abs(verts[tris.reshape(-1)] - soup).max() <= 1e-12
+    # welded: edges are shared by two triangles (the classic table may leave a few open edges
+    # at ambiguous faces, never more than two triangles on one edge)
+    e = np.sort(np.concatenate([tris[:, [0, 1]], tris[:, [1, 2]], tris[:, [2, 0]]]), axis=1)
+    _, counts = np.unique(e, axis=0, return_counts=True)
+    assert counts.max() <= 2 and (counts == 2).mean() > 0.99
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("R", [16, 48])
 def test_marching_cubes_bit_exact(ctx, fitted, R):
     V, F, o, w, ref, gpu, pos, b, lam = fitted

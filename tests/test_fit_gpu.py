@@ -87,16 +87,18 @@ def test_lscg_matches_oracle(ctx, name, kw, res):
     rp, col, val = ref.assemble()
     A = sp.csr_matrix((val, col, rp), shape=(op.rows, op.rows))
     # Same number of iterations on both sides: the iterates agree up to rounding (GPU tree
-    # reductions vs sequential sums), which the Krylov recurrence amplifies to ~1e-10 by 15
-    # iterations; an algorithmic difference would show at O(1). A is rank-deficient
-    # (coincident vertices across depths), so lambda drifts more along near-null directions
-    # than the fitted field A lambda.
-    for iters in (5, 15):
-        x_ref, _ = oracle.cgls(rp, col, val, b, 1e-300, iters, 0)
-        x_gpu, r_gpu = op.solve(b, tol=1e-300, max_iters=iters)
-        assert r_gpu["iterations"] == iters
-        assert np.linalg.norm(x_gpu - x_ref) <= 1e-6 * np.linalg.norm(x_ref)
-        assert np.linalg.norm(A @ (x_gpu - x_ref)) <= 1e-8 * np.linalg.norm(b)
+    # reductions vs sequential sums). Mid-run iterates of this rank-deficient system are
+    # sensitive -- a 1e-16 relative change of b alone moves the oracle's own iteration-15 field
+    # by ~1e-8 on the torus before it settles again -- so the tight check is at 5 iterations;
+    # an algorithmic difference would show at O(1) there.
+    x_ref, _ = oracle.cgls(rp, col, val, b, 1e-300, 5, 0)
+    x_gpu, r_gpu = op.solve(b, tol=1e-300, max_iters=5)
+    assert r_gpu["iterations"] == 5
+    assert np.linalg.norm(x_gpu - x_ref) <= 1e-10 * np.linalg.norm(x_ref)
+    assert np.linalg.norm(A @ (x_gpu - x_ref)) <= 1e-10 * np.linalg.norm(b)
+    # The GPU solve itself is deterministic: fixed-order reductions, bit-identical reruns.
+    x_again, _ = op.solve(b, tol=1e-300, max_iters=5)
+    assert np.array_equal(x_again, x_gpu)
     # Converged runs meet the same stopping test (possibly one iteration apart at the
     # threshold): their fitted fields differ by at most the two residuals.
     for tol, stop in [(1e-10, 0), (1e-6, 1)]:
@@ -164,3 +166,31 @@ def test_shell_samples_same_point_set(ctx, name, kw, res):
     key = lambda P: P[np.lexsort((P[:, 2], P[:, 1], P[:, 0]))]  # noqa: E731
     assert np.array_equal(key(pts_gpu[:ne_gpu]), key(pts_ref[:ne_ref]))
     assert np.array_equal(key(pts_gpu[ne_gpu:]), key(pts_ref[ne_ref:]))
+
+
+@pytest.mark.gpu
+def test_batched_solve_matches_single_solves(ctx):
+    from its_b200 import Operator, Svo
+    from its_b200.api import solve_batch
+    cases = [("small", {}, 16), ("c0", {}, 32), ("torus", dict(R=0.7, r=0.25, rings=48, segs=24), 32),
+             ("superquadric", dict(e1=0.4, e2=2.5, subdiv=4), 16)]
+    ops, bs = [], []
+    for name, kw, res in cases:
+        V, F, o, w = prepared_mesh(name, **kw)
+        svo = Svo(ctx, V, F, res, o, w)
+        pos, _ = svo.vertices()
+        bs.append(ctx.signed_distance(pos, V, F))
+        ops.append(Operator(svo))
+    for tol, stop in [(1e-10, 0), (1e-6, 1)]:
+        xs, reps = solve_batch(ops, bs, tol=tol, max_iters=1000, stop_rule=stop)
+        for op, b, x, r in zip(ops, bs, xs, reps):
+            xs1, r1 = op.solve(b, tol=tol, max_iters=1000, stop_rule=stop)
+            # the same per-mesh algorithm; only the chunking of the dot products differs
+            assert r["converged"] and abs(r["iterations"] - r1["iterations"]) <= 1
+            rp, col, val = op.csr()
+            A = sp.csr_matrix((val, col, rp), shape=(op.rows, op.rows))
+            assert np.linalg.norm(A @ (x - xs1)) <= (r["rel_residual"] + r1["rel_residual"] + 1e-11) * np.linalg.norm(b)
+            assert abs(np.linalg.norm(A @ x - b) / np.linalg.norm(b) - r["rel_residual"]) <= 1e-3 * r["rel_residual"] + 1e-15
+    # a zero right-hand side in the batch finishes at once with x = 0
+    xs, reps = solve_batch(ops[:2], [bs[0], np.zeros(ops[1].rows)], tol=1e-8)
+    assert reps[1]["iterations"] == 0 and not np.any(xs[1]) and reps[0]["converged"]
