@@ -173,6 +173,21 @@ its_status its_lscg_solve(its_op* op, const double* b, double* lambda, const its
 its_status its_lscg_solve_batch(its_op* const* ops, int64_t count, const double* const* b, double* const* lambda,
                                 const its_solve_opts* opts, its_solve_report* reports);
 
+/* Exact start (hierarchical surplus). Coincident corner vertices of different depths have
+   identical rows, so A lambda = b is consistent and its exact solutions differ only in how
+   each point's value is split among its coincident vertices. This pass fixes the split
+   (vertices whose lattice coordinates are all even below the root depth take shares[v],
+   or 0 when shares is NULL) and solves every other row, coarse depths first, as
+   lambda_v = b_v - sum_{u != v} A(v,u) lambda_u: one pass over A, one launch per depth.
+   The result is an exact solution; its_lscg_solve with it as x0 stops at its residual
+   test. No counterpart in the reference (which starts Eigen's CGLS from zero,
+   src/ThinShells.cpp:615-617). Vectors may be host or device memory. */
+its_status its_exact_start(its_op* op, const double* b, const double* shares, double* lambda);
+/* The same for count operators of one context (one launch per depth for all of them);
+   shares may be NULL or hold NULL entries. */
+its_status its_exact_start_batch(its_op* const* ops, int64_t count, const double* const* b,
+                                 const double* const* shares, double* const* lambda);
+
 /* ---- a13: field at points and the shell iso levels ------------------------------------- */
 /* ThinShells::cpLatentBSplineValue (src/ThinShells.cpp:655-755): each point's fine node by
    Morton code, then lambda times the hats of the 8 corners of that node and of every

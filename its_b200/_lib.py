@@ -61,6 +61,8 @@ SIGNATURES = {
     "its_solve_opts_default": (st, [C.POINTER(SolveOpts)]),
     "its_lscg_solve": (st, [vp, vp, vp, C.POINTER(SolveOpts), C.POINTER(SolveReport)]),
     "its_lscg_solve_batch": (st, [vp, i64, vp, vp, C.POINTER(SolveOpts), vp]),
+    "its_exact_start": (st, [vp, vp, vp, vp]),
+    "its_exact_start_batch": (st, [vp, i64, vp, vp, vp]),
     "its_eval_points": (st, [vp, vp, vp, i64, vp, vp]),
     "its_shell_iso_values": (st, [vp, vp, vp, i64, C.POINTER(dbl), C.POINTER(dbl), C.POINTER(i64)]),
     "its_eval_grid": (st, [vp, vp, vp, vp, i32, vp]),

@@ -287,6 +287,15 @@ class Operator:
         self.ctx.check(lib().its_operator_get_csr(self.h, _ptr(rp), _ptr(col), _ptr(val)), "its_operator_get_csr")
         return rp, col, val
 
+    def exact_start(self, b, shares=None, out=None):
+        """Hierarchical-surplus exact solution of A lambda = b (its_exact_start)."""
+        b = _f64(b)
+        sh = None if shares is None else _f64(shares)
+        if out is None:
+            out = np.zeros(self.rows)
+        self.ctx.check(lib().its_exact_start(self.h, _ptr(b), _ptr(sh), _ptr(out)), "its_exact_start")
+        return out
+
     def apply(self, x, transpose=False, out=None):
         x = _f64(x)
         if out is None:
@@ -350,3 +359,21 @@ def solve_batch(ops, bs, tol=None, max_iters=0, stop_rule=STOP_NORMAL, check_eve
                 rel_residual=r.rel_residual, normal_rel_residual=r.normal_rel_residual, ms=r.ms) for r in reps]
     del keep
     return outs, out
+
+
+def _addr(a):
+    return None if a is None else (a.ctypes.data if isinstance(a, np.ndarray) else a.data_ptr())
+
+
+def exact_start_batch(ops, bs, shares=None, outs=None):
+    """Exact starts of many operators of one context (its_exact_start_batch)."""
+    count = len(ops)
+    bs = [_f64(b) for b in bs]
+    sh = None if shares is None else [None if x is None else _f64(x) for x in shares]
+    outs = outs if outs is not None else [np.zeros(op.rows) for op in ops]
+    H = (C.c_void_p * count)(*[op.h.value for op in ops])
+    B = (C.c_void_p * count)(*[_addr(b) for b in bs])
+    S = None if sh is None else (C.c_void_p * count)(*[_addr(x) for x in sh])
+    X = (C.c_void_p * count)(*[_addr(x) for x in outs])
+    ops[0].ctx.check(lib().its_exact_start_batch(H, count, B, S, X), "its_exact_start_batch")
+    return outs

@@ -66,7 +66,7 @@ __device__ __forceinline__ void batchClass(const BatchOp* __restrict__ ops, cons
   if (valid) {
     m = L.op[L.offset[c] + slot];
     row = L.row[L.offset[c] + slot];
-    valid = !S[m].done;
+    valid = !(S && S[m].done);
     if (valid) {
       M = tr ? ops[m].T : ops[m].A;
       off = ops[m].off;
@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(kSpmvThreads) kBatchSpmv(const BatchOp* __rest
   const int64_t seg = b - L.blockStart[6];
   if (seg >= L.nSeg) return;
   const uint32_t m = L.segOp[seg];
-  if (S[m].done) return;
+  if (S && S[m].done) return;
   const CsrView<double, double> M = tr ? ops[m].T : ops[m].A;
   const uint32_t row = L.segRow[seg];
   const int64_t beg = L.segBeg[seg], rowEnd = M.rowptr[row + 1];
@@ -121,7 +121,7 @@ __global__ void kBatchCombine(const BatchOp* __restrict__ ops, BatchList L, doub
   const int lane = threadIdx.x & 31;
   if (r >= L.nLong) return;
   const uint32_t m = L.longOp[r];
-  if (S[m].done) return;
+  if (S && S[m].done) return;
   double s = 0.0;
   for (uint32_t k = L.longFirstSeg[r] + lane; k < L.longFirstSeg[r + 1]; k += 32) s += L.segPartial[k];
   s = warpSum(s);
@@ -567,8 +567,8 @@ its_status solveBatch(its_ctx* ctx, its_op* const* ops, int64_t count, const dou
     ctx->launches += perGraph;
   }
   cudaGraphExecDestroy(ge);
-  // true residuals and results
-  if ((st = batchSpmv(ctx, R.ops, sideA, false, R.x, R.t, R.S)) != ITS_OK) return st;
+  // true residuals and results (every mesh is done: the SpMV ignores the done flags)
+  if ((st = batchSpmv(ctx, R.ops, sideA, false, R.x, R.t, nullptr)) != ITS_OK) return st;
   std::vector<CgScalars> hs(count);
   ITS_CU(ctx, cudaMemcpyAsync(hs.data(), R.S, count * sizeof(CgScalars), cudaMemcpyDeviceToHost, ctx->stream));
   // the residual reduction overwrites rr/bNorm2: read the solver state first

@@ -1,0 +1,103 @@
+// Fifth-generation tensor core (tcgen05) primitives for sm_100a: shared-memory matrix
+// descriptors, the kind::f16 MMA with its accumulator in tensor memory (TMEM), TMEM
+// allocation and loads, and bounded mbarrier waits. Inline PTX only.
+//
+// Operand layout used throughout: K-major tiles of 64 bf16 (128 bytes) per row, 128-byte
+// swizzle. A tile of R rows is R/8 atoms of 8 rows x 128 B (1024 B, 1024-aligned); inside an
+// atom, the 16-byte chunk c of row r sits at chunk position c ^ r.
+#pragma once
+#include <cstdint>
+
+#include <cuda_bf16.h>
+
+namespace its {
+namespace umma {
+
+__device__ __forceinline__ uint32_t smemAddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Byte offset of 16-byte chunk c (0..7) of row r inside a swizzled K-major 64-wide tile.
+__device__ __forceinline__ uint32_t swizzledChunk(uint32_t r, uint32_t c) {
+  return ((r >> 3) << 10) + ((r & 7u) << 7) + (((c ^ r) & 7u) << 4);
+}
+
+// Shared-memory matrix descriptor: start address, leading byte offset 16 B (not used by
+// swizzled K-major layouts), stride byte offset 1024 B (8-row atom to 8-row atom),
+// descriptor version 1, layout SWIZZLE_128B (2).
+__device__ __forceinline__ uint64_t descSw128(uint32_t saddr) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(1024u >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
+  return d;
+}
+
+// Instruction descriptor of kind::f16: F32 accumulator (bits 4-5 = 1), A and B BF16 (bits 7-9
+// and 10-12 = 1), both K-major (bits 15, 16 = 0), N/8 at bits 17-22, M/16 at bits 24-28.
+__host__ __device__ constexpr uint32_t idescBf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// D[tmem] (+)= A[desc a] * B[desc b]^T, issued by one thread.
+__device__ __forceinline__ void mma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+// Arrive on an mbarrier when every MMA issued so far by this thread has completed.
+__device__ __forceinline__ void commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
+}
+
+__device__ __forceinline__ void fenceBefore() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fenceAfter() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// Generic-proxy shared-memory writes made visible to the tensor core (async proxy).
+__device__ __forceinline__ void fenceProxyAsync() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Warp-wide TMEM allocation: the base address is written to *slot (shared memory).
+__device__ __forceinline__ void tmemAlloc(uint32_t slotAddr, uint32_t cols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slotAddr), "r"(cols));
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+}
+__device__ __forceinline__ void tmemFree(uint32_t base, uint32_t cols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(base), "r"(cols));
+}
+
+// 16 consecutive FP32 columns of this thread's TMEM lane (warp w reads lanes 32w..32w+31).
+__device__ __forceinline__ void tmemLoad16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void mbarInit(uint32_t mbar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count));
+}
+// Bounded wait for the given phase parity; false when the bound ran out.
+__device__ __forceinline__ bool mbarWait(uint32_t mbar, uint32_t parity, uint32_t maxTries = 1u << 22) {
+  for (uint32_t i = 0; i < maxTries; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+}  // namespace umma
+}  // namespace its

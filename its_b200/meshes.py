@@ -47,6 +47,31 @@ def _subdivide(V, F):
     return np.vstack([V, mid]), F2
 
 
+def _geodesic(k):
+    """Unit sphere from the bipyramid with every face split into k x k (frequency k): 10 k^2
+    faces, 5 k^2 + 2 vertices, any k >= 1."""
+    V0, F0 = _bipyramid()
+    I, J = np.meshgrid(np.arange(k + 1), np.arange(k + 1), indexing="ij")
+    keep = (I + J) <= k
+    I, J = I[keep], J[keep]
+    local = -np.ones((k + 1, k + 1), np.int64)
+    local[I, J] = np.arange(I.size)
+    i, j = np.meshgrid(np.arange(k), np.arange(k), indexing="ij")
+    up = (i + j) <= k - 1
+    dn = (i + j) <= k - 2
+    tri = np.concatenate([np.stack([local[i[up], j[up]], local[i[up] + 1, j[up]], local[i[up], j[up] + 1]], 1),
+                          np.stack([local[i[dn] + 1, j[dn]], local[i[dn] + 1, j[dn] + 1], local[i[dn], j[dn] + 1]], 1)])
+    P, T = [], []
+    for f, (a, b, c) in enumerate(F0):
+        pts = V0[a] + (V0[b] - V0[a]) * (I[:, None] / k) + (V0[c] - V0[a]) * (J[:, None] / k)
+        P.append(pts / np.linalg.norm(pts, axis=1, keepdims=True))
+        T.append(tri + f * I.size)
+    P, T = np.vstack(P), np.vstack(T)
+    # weld the copies of the shared edges
+    _, first, inv = np.unique(np.round(P * 2 ** 30).astype(np.int64), axis=0, return_index=True, return_inverse=True)
+    return P[first], inv.reshape(-1)[T]
+
+
 def _real_sh(lmax, theta, phi):
     """Real spherical harmonics up to degree lmax at (theta polar, phi azimuth)."""
     from scipy.special import lpmv
@@ -78,6 +103,14 @@ def sphere_mesh(subdiv, amp=0.1, seed=0, lmax=4):
     f = Y @ coef
     r = 1.0 + amp * f
     return V * r[:, None], F.astype(np.int32)
+
+
+def _sh_perturb(V, amp, seed, lmax=4):
+    rng = np.random.default_rng(seed)
+    theta = np.arccos(np.clip(V[:, 2], -1, 1))
+    phi = np.arctan2(V[:, 1], V[:, 0])
+    Y = _real_sh(lmax, theta, phi)
+    return V * (1.0 + amp * (Y @ rng.standard_normal(Y.shape[1])))[:, None]
 
 
 def _closed_grid_faces(rings, segs):
@@ -144,11 +177,15 @@ def torus_mesh(R=0.75, r=0.2, rings=64, segs=32):
     return V, F
 
 
-def superquadric_mesh(e1=1.0, e2=1.0, subdiv=3):
-    """Superellipsoid |x|^(2/e2)+|y|^(2/e2))^(e2/e1)+|z|^(2/e1)=1 over a geodesic sphere."""
-    V, F = _bipyramid()
-    for _ in range(subdiv):
-        V, F = _subdivide(V, F)
+def superquadric_mesh(e1=1.0, e2=1.0, subdiv=3, freq=None):
+    """Superellipsoid |x|^(2/e2)+|y|^(2/e2))^(e2/e1)+|z|^(2/e1)=1 over a geodesic sphere
+    (4-to-1 splits ``subdiv`` times, or frequency ``freq`` when given)."""
+    if freq is not None:
+        V, F = _geodesic(freq)
+    else:
+        V, F = _bipyramid()
+        for _ in range(subdiv):
+            V, F = _subdivide(V, F)
     x, y, z = V[:, 0], V[:, 1], V[:, 2]
     theta = np.arcsin(np.clip(z, -1, 1))
     phi = np.arctan2(y, x)
@@ -156,6 +193,40 @@ def superquadric_mesh(e1=1.0, e2=1.0, subdiv=3):
     cth, sth = np.cos(theta), np.sin(theta)
     V2 = np.stack([sp(cth, e1) * sp(np.cos(phi), e2), sp(cth, e1) * sp(np.sin(phi), e2), sp(sth, e1)], 1)
     return V2, F.astype(np.int32)
+
+
+def batch_meshes(count=256, seed=3, fmin=2000, fmax=200000):
+    """The uneven multi-mesh workload: face counts log-uniform in [fmin, fmax]; thirds of
+    perturbed geodesic spheres (radius 1 + 0.1 f, f a degree-4 real SH series), tori
+    (R in [0.5, 1], r in [0.1, 0.3]) and superquadrics (exponents in [0.3, 3]); octree
+    depth 7, 8 or 9 (res 64 / 128 / 256) by size, the thirds of the log range.
+
+    Returns a list of dicts (V, F, kind, res, faces) in generation order."""
+    rng = np.random.default_rng(seed)
+    out = []
+    lo, hi = math.log(fmin), math.log(fmax)
+    for i in range(count):
+        target = math.exp(rng.uniform(lo, hi))
+        kind = i % 3
+        if kind == 0:
+            k = max(2, int(round(math.sqrt(target / 10.0))))
+            V, F = _geodesic(k)
+            V = _sh_perturb(V, 0.1, seed * 100000 + i)
+        elif kind == 1:
+            R, r = rng.uniform(0.5, 1.0), rng.uniform(0.1, 0.3)
+            segs = max(8, int(round(math.sqrt(target / 2.0 * r / R))))
+            rings = max(8, int(round(target / (2.0 * segs))))
+            V, F = torus_mesh(R, r, rings, segs)
+        else:
+            e1, e2 = rng.uniform(0.3, 3.0), rng.uniform(0.3, 3.0)
+            k = max(2, int(round(math.sqrt(target / 10.0))))
+            V, F = superquadric_mesh(e1, e2, freq=k)
+        nf = F.shape[0]
+        t = (math.log(nf) - lo) / (hi - lo)
+        res = 64 if t < 1 / 3 else (128 if t < 2 / 3 else 256)
+        out.append(dict(V=np.ascontiguousarray(V, np.float64), F=np.ascontiguousarray(F, np.int32),
+                        kind=("sphere", "torus", "superquadric")[kind], res=res, faces=nf))
+    return out
 
 
 def read_off(path):

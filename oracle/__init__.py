@@ -54,6 +54,7 @@ def _declare(L):
         "orc_csr_from": (vp, [i64, vp, vp, vp]),
         "orc_csr_free": (None, [vp]),
         "orc_cgls": (i32, [vp, vp, vp, dbl, i64, i32, vp]),
+        "orc_exact_start": (None, [vp, vp, vp, vp, vp]),
         "orc_intersections": (vp, [vp, vp, i64, vp, i64]),
         "orc_points_count": (i64, [vp, vp]),
         "orc_points_get": (None, [vp, vp]),
@@ -178,6 +179,20 @@ class Svo:
         finally:
             lib().orc_csr_free(h)
         return rp, col, val
+
+    def exact_start(self, b, shares=None):
+        """Hierarchical-surplus exact solution of A lambda = b for this octree's operator
+        (shares: coefficients of the vertices coincident with a coarser corner, default 0)."""
+        rp, col, val = self.assemble()
+        b = _f64(b)
+        h = lib().orc_csr_from(rp.shape[0] - 1, _p(rp), _p(col), _p(val))
+        out = np.zeros(rp.shape[0] - 1)
+        sh = None if shares is None else _f64(shares)
+        try:
+            lib().orc_exact_start(self.h, h, _p(b), _p(sh), _p(out))
+        finally:
+            lib().orc_csr_free(h)
+        return out
 
     def intersections(self):
         h = lib().orc_intersections(self.h, _p(self.V), self.V.shape[0], _p(self.F), self.F.shape[0])

@@ -121,6 +121,10 @@ int orc_cgls(void* a, const double* b, double* x, double tol, int64_t maxIters, 
   return r.converged ? 0 : 1;
 }
 
+void orc_exact_start(void* h, void* a, const double* b, const double* shares, double* lambda) {
+  exactStart(*static_cast<Svo*>(h), *static_cast<Csr*>(a), b, shares, lambda);
+}
+
 void* orc_intersections(void* h, const double* V, int64_t nv, const int32_t* F, int64_t nf) {
   Points* p = new Points;
   p->pts = intersections(*static_cast<Svo*>(h), V, nv, F, nf, &p->nEdge);

@@ -641,3 +641,38 @@ void marchingCubesMesh(const double* field, int R, const double origin[3], const
 }
 
 }  // namespace orc
+
+namespace orc {
+
+// Exact start (hierarchical surplus) of A lambda = b, sequentially, coarse depths first.
+// A vertex of depth d below the root whose lattice coordinates (recovered from its position,
+// (p - gridOrigin) / (unit * 2^d), to the nearest integer) are all even coincides with a
+// corner of depth d + 1: it keeps its share. Every other row, coarse depths first, solves
+// lambda_v = b_v - sum_{u != v} A(v,u) lambda_u with the entries summed in column order.
+void exactStart(const Svo& s, const Csr& A, const double* b, const double* shares, double* lambda) {
+  const int depth = s.treeDepth;
+  std::vector<int64_t> start(depth + 1, 0);
+  for (int d = 0; d < depth; ++d) start[d + 1] = start[d] + (int64_t)s.depthVerts[d].size();
+  std::vector<char> coincident(A.n, 0);
+  for (int d = 0; d + 1 < depth; ++d) {
+    const double w = s.unit.x * (double)(1u << d);
+    for (size_t k = 0; k < s.depthVerts[d].size(); ++k) {
+      const V3& p = s.depthVerts[d][k].pos;
+      const long long X = std::llround((p.x - s.gridOrigin.x) / w), Y = std::llround((p.y - s.gridOrigin.y) / w),
+                      Z = std::llround((p.z - s.gridOrigin.z) / w);
+      coincident[start[d] + (int64_t)k] = ((X | Y | Z) & 1) == 0;
+    }
+  }
+  for (int64_t r = 0; r < A.n; ++r) lambda[r] = (coincident[r] && shares) ? shares[r] : 0.0;
+  for (int d = depth - 1; d >= 0; --d) {
+    for (int64_t r = start[d]; r < start[d + 1]; ++r) {
+      if (coincident[r]) continue;
+      double acc = 0.0;
+      for (int64_t k = A.rowptr[r]; k < A.rowptr[r + 1]; ++k)
+        if (A.col[k] != r) acc += A.val[k] * lambda[A.col[k]];
+      lambda[r] = b[r] - acc;
+    }
+  }
+}
+
+}  // namespace orc

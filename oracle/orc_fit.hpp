@@ -24,6 +24,7 @@ void signedDistance(const double* P, int64_t m, const double* V, const int32_t* 
 Csr assemble(const Svo& s);
 Csr transpose(const Csr& A);
 CglsReport cgls(const Csr& A, const Csr& T, const double* b, double* x, double tol, int64_t maxIters, int stop);
+void exactStart(const Svo& s, const Csr& A, const double* b, const double* shares, double* lambda);
 void evalPoints(const Svo& s, const double* lambda, const double* P, int64_t m, double* out, uint8_t* missing);
 void evalBrute(const Svo& s, const double* lambda, const double* P, int64_t m, double* out);
 void evalGrid(const Svo& s, const double* lambda, const double origin[3], const double width[3], int R, double* out);

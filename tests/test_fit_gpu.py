@@ -194,3 +194,50 @@ def test_batched_solve_matches_single_solves(ctx):
     # a zero right-hand side in the batch finishes at once with x = 0
     xs, reps = solve_batch(ops[:2], [bs[0], np.zeros(ops[1].rows)], tol=1e-8)
     assert reps[1]["iterations"] == 0 and not np.any(xs[1]) and reps[0]["converged"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,kw,res", FIT_CASES, ids=[f"{c[0]}-{c[2]}" for c in FIT_CASES])
+def test_exact_start_matches_oracle(ctx, name, kw, res):
+    from its_b200 import Operator
+    V, F, ref, gpu = _setup(ctx, name, kw, res)
+    pos, _ = ref.vertices()
+    b = oracle.signed_distance(pos, V, F)
+    op = Operator(gpu)
+    rp, col, val = ref.assemble()
+    A = sp.csr_matrix((val, col, rp), shape=(op.rows, op.rows))
+    # zero shares: an exact solution (the oracle sums each row in column order, the GPU in
+    # 8-lane partial sums, so the two agree to rounding carried through the depth levels)
+    lam_ref = ref.exact_start(b)
+    lam = op.exact_start(b)
+    assert np.abs(lam - lam_ref).max() <= 1e-12 * np.abs(lam_ref).max()
+    assert np.linalg.norm(A @ lam - b) <= 1e-14 * np.linalg.norm(b)
+    # CGLS started there stops at its residual test
+    x, rep = op.solve(b, tol=1e-6, stop_rule=1, x0=lam)
+    assert rep["iterations"] == 0 and rep["converged"] and rep["rel_residual"] <= 1e-14
+    # the shares fix the null-space component: the min-norm shares give back the (zero-start)
+    # CGLS solution, and every exact solution has the same field at the shell samples
+    x_mn, _ = oracle.cgls(rp, col, val, b, 1e-14, 20000, 1)
+    lam_mn = op.exact_start(b, shares=x_mn)
+    assert np.abs(lam_mn - x_mn).max() <= 1e-12 * np.abs(x_mn).max()
+    P = np.vstack([V, ref.intersections()[0]])
+    f0, _ = ref.eval_points(lam, P)
+    f1, _ = ref.eval_points(x_mn, P)
+    assert np.abs(f0 - f1).max() <= 1e-12 * np.abs(b).max()
+
+
+@pytest.mark.gpu
+def test_exact_start_batch_matches_single(ctx):
+    from its_b200 import Operator, Svo
+    from its_b200.api import exact_start_batch
+    ops, bs = [], []
+    for name, kw, res in FIT_CASES + [("superquadric", dict(e1=0.4, e2=2.5, subdiv=4), 64)]:
+        V, F, o, w = prepared_mesh(name, **kw)
+        svo = Svo(ctx, V, F, res, o, w)
+        bs.append(ctx.signed_distance(svo.vertices()[0], V, F))
+        ops.append(Operator(svo))
+    rng = np.random.default_rng(5)
+    shares = [None, rng.standard_normal(ops[1].rows) * 1e-3, None, None]
+    outs = exact_start_batch(ops, bs, shares)
+    for op, b, s, x in zip(ops, bs, shares, outs):
+        assert np.array_equal(x, op.exact_start(b, shares=s))
