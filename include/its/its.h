@@ -178,15 +178,21 @@ its_status its_lscg_solve_batch(its_op* const* ops, int64_t count, const double*
    each point's value is split among its coincident vertices. This pass fixes the split
    (vertices whose lattice coordinates are all even below the root depth take shares[v],
    or 0 when shares is NULL) and solves every other row, coarse depths first, as
-   lambda_v = b_v - sum_{u != v} A(v,u) lambda_u: one pass over A, one launch per depth.
-   The result is an exact solution; its_lscg_solve with it as x0 stops at its residual
-   test. No counterpart in the reference (which starts Eigen's CGLS from zero,
-   src/ThinShells.cpp:615-617). Vectors may be host or device memory. */
-its_status its_exact_start(its_op* op, const double* b, const double* shares, double* lambda);
-/* The same for count operators of one context (one launch per depth for all of them);
-   shares may be NULL or hold NULL entries. */
-its_status its_exact_start_batch(its_op* const* ops, int64_t count, const double* const* b,
+   lambda_v = b_v - sum_{u != v} A(v,u) lambda_u: one matrix-free pass over the rows of A
+   (generated from the octree), one launch per depth. The result is an exact solution;
+   its_lscg_solve with it as x0 stops at its residual test. No counterpart in the reference
+   (which starts Eigen's CGLS from zero, src/ThinShells.cpp:615-617). Vectors may be host or
+   device memory. */
+its_status its_exact_start(its_svo* svo, const double* b, const double* shares, double* lambda);
+/* The same for count octrees of one context (one launch per depth for all of them); shares
+   may be NULL or hold NULL entries. */
+its_status its_exact_start_batch(its_svo* const* svos, int64_t count, const double* const* b,
                                  const double* const* shares, double* const* lambda);
+/* ||b - A lambda|| / ||b|| without an assembled operator (rows generated from the octree,
+   summed in a fixed order). */
+its_status its_fit_residual(its_svo* svo, const double* b, const double* lambda, double* rel_residual);
+its_status its_fit_residual_batch(its_svo* const* svos, int64_t count, const double* const* b,
+                                  const double* const* lambda, double* rel_residual);
 
 /* ---- a13: field at points and the shell iso levels ------------------------------------- */
 /* ThinShells::cpLatentBSplineValue (src/ThinShells.cpp:655-755): each point's fine node by
@@ -237,6 +243,50 @@ its_status its_marching_cubes_mesh(its_ctx* ctx, const double* field, int res, c
 its_status its_marching_cubes_noalloc(its_ctx* ctx, const double* field, int res, const double origin[3],
                                       const double width[3], double iso, uint8_t* cube_index, double* tri_verts,
                                       int64_t capacity, int64_t* num_verts);
+
+/* ---- learned shares: the share network --------------------------------------------------
+   No counterpart in the reference. A 64 -> 128 -> 128 -> 128 -> 1 GELU network (BF16
+   weights and activations, FP32 accumulation, tcgen05 tensor-core GEMMs) that predicts the
+   coefficient of each corner vertex coincident with a coarser corner in the minimum-norm
+   solution, i.e. the shares of its_exact_start. Parameters: its_mlp_num_params() FP32
+   values, W1[128x64] b1 W2[128x128] b2 W3[128x128] b3 w4[128] b4 (W[out][in]). Feature rows
+   are 64 FP32 values, already normalised. Pointers may be host or device memory. */
+typedef struct its_mlp its_mlp;
+/* batch: rows per training step and per inference chunk, a multiple of 128. */
+its_status its_mlp_create(its_ctx* ctx, int64_t batch, its_mlp** out);
+its_status its_mlp_free(its_mlp* mlp);
+int64_t its_mlp_num_params(void);
+/* Loads parameters and resets the Adam state. */
+its_status its_mlp_set_params(its_mlp* mlp, const float* params);
+its_status its_mlp_get_params(its_mlp* mlp, float* params);
+its_status its_mlp_forward(its_mlp* mlp, const float* features, int64_t n, float* out);
+/* Gradient of mean((out - y)^2) over n rows (n <= batch, a multiple of 64), no update. */
+its_status its_mlp_gradient(its_mlp* mlp, const float* features, const float* y, int64_t n, float* grad,
+                            float* loss);
+/* steps Adam steps (lr, beta 0.9 / 0.999, eps 1e-8) on random batches of n resident rows;
+   loss_curve (NULL or steps entries) receives each step's mean squared error. */
+its_status its_mlp_train(its_mlp* mlp, const float* features, const float* y, int64_t n, int64_t steps, float lr,
+                         uint64_t seed, float* loss_curve);
+/* Features of the vertices coincident with a coarser corner (the shares of the exact start),
+   64 per vertex: the signed distance, zero-share surplus values of the vertex's copies and
+   lattice neighbours, neighbour presence, depth, cell width, and the face samples in the
+   owner node's 27-neighbourhood (count, mean offset, mean normal, 1 - |mean normal|).
+   V, F: the mesh of the octree. norm (NULL or 128 values: mean[64], scale[64]) normalises
+   (f - mean) * scale. features == NULL: *count only; else capacity >= *count rows, and ids
+   (NULL or capacity entries) receives the vertex of each row (ascending). */
+its_status its_share_features(its_svo* svo, const double* b, const double* V, int64_t nv, const int32_t* F,
+                              int64_t nf, const float* norm, float* features, int64_t capacity, int64_t* ids,
+                              int64_t* count);
+/* Learned start: features, the share network, then its_exact_start with the predicted
+   shares (prediction * norm[129] + norm[128]). norm: 130 values (input mean[64], input
+   scale[64], output mean, output scale). lambda: an exact solution whose null-space part is
+   the network's. */
+its_status its_learned_start(its_svo* svo, its_mlp* mlp, const double* b, const double* V, int64_t nv,
+                             const int32_t* F, int64_t nf, const float* norm, double* lambda);
+/* The same for count operators of one context (one network pass over all of them). */
+its_status its_learned_start_batch(its_svo* const* svos, int64_t count, its_mlp* mlp, const double* const* b,
+                                   const double* const* V, const int64_t* nv, const int32_t* const* F,
+                                   const int64_t* nf, const float* norm, double* const* lambda);
 
 #ifdef __cplusplus
 }

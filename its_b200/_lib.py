@@ -63,6 +63,19 @@ SIGNATURES = {
     "its_lscg_solve_batch": (st, [vp, i64, vp, vp, C.POINTER(SolveOpts), vp]),
     "its_exact_start": (st, [vp, vp, vp, vp]),
     "its_exact_start_batch": (st, [vp, i64, vp, vp, vp]),
+    "its_mlp_create": (st, [vp, i64, C.POINTER(vp)]),
+    "its_mlp_free": (st, [vp]),
+    "its_mlp_num_params": (i64, []),
+    "its_mlp_set_params": (st, [vp, vp]),
+    "its_mlp_get_params": (st, [vp, vp]),
+    "its_mlp_forward": (st, [vp, vp, i64, vp]),
+    "its_mlp_gradient": (st, [vp, vp, vp, i64, vp, vp]),
+    "its_mlp_train": (st, [vp, vp, vp, i64, i64, C.c_float, C.c_uint64, vp]),
+    "its_fit_residual": (st, [vp, vp, vp, C.POINTER(dbl)]),
+    "its_fit_residual_batch": (st, [vp, i64, vp, vp, vp]),
+    "its_share_features": (st, [vp, vp, vp, i64, vp, i64, vp, vp, i64, vp, C.POINTER(i64)]),
+    "its_learned_start": (st, [vp, vp, vp, vp, i64, vp, i64, vp, vp]),
+    "its_learned_start_batch": (st, [vp, i64, vp, vp, vp, vp, vp, vp, vp, vp]),
     "its_eval_points": (st, [vp, vp, vp, i64, vp, vp]),
     "its_shell_iso_values": (st, [vp, vp, vp, i64, C.POINTER(dbl), C.POINTER(dbl), C.POINTER(i64)]),
     "its_eval_grid": (st, [vp, vp, vp, vp, i32, vp]),

@@ -180,6 +180,36 @@ class Svo:
     def __del__(self):
         self.close()
 
+    def exact_start(self, b, shares=None, out=None):
+        """Hierarchical-surplus exact solution of A lambda = b, matrix-free (its_exact_start)."""
+        b = _f64(b)
+        sh = None if shares is None else _f64(shares)
+        if out is None:
+            out = np.zeros(self.num_verts)
+        self.ctx.check(lib().its_exact_start(self.h, _ptr(b), _ptr(sh), _ptr(out)), "its_exact_start")
+        return out
+
+    def residual(self, b, lam):
+        """||b - A lambda|| / ||b|| without an assembled operator (its_fit_residual)."""
+        b, lam = _f64(b), _f64(lam)
+        rel = C.c_double(0)
+        self.ctx.check(lib().its_fit_residual(self.h, _ptr(b), _ptr(lam), C.byref(rel)), "its_fit_residual")
+        return rel.value
+
+    def share_features(self, b, V, F, norm=None):
+        """Features of the share network (its_share_features): (features n x 64, vertex ids)."""
+        b, V, F = _f64(b), _f64(V), _i32(F)
+        nrm = None if norm is None else np.ascontiguousarray(norm, np.float32)
+        cnt = C.c_int64(0)
+        L = lib()
+        self.ctx.check(L.its_share_features(self.h, _ptr(b), _ptr(V), _n(V), _ptr(F), _n(F), _ptr(nrm), None, 0, None,
+                                            C.byref(cnt)), "its_share_features")
+        n = cnt.value
+        feats, ids = np.zeros((max(n, 1), 64), np.float32), np.zeros(max(n, 1), np.int64)
+        self.ctx.check(L.its_share_features(self.h, _ptr(b), _ptr(V), _n(V), _ptr(F), _n(F), _ptr(nrm), _ptr(feats), n,
+                                            _ptr(ids), C.byref(cnt)), "its_share_features")
+        return feats[:n], ids[:n]
+
     def depth_counts(self):
         return (np.array(self.info.nodes_per_depth[:self.depth], np.int64),
                 np.array(self.info.vertices_per_depth[:self.depth], np.int64))
@@ -288,13 +318,8 @@ class Operator:
         return rp, col, val
 
     def exact_start(self, b, shares=None, out=None):
-        """Hierarchical-surplus exact solution of A lambda = b (its_exact_start)."""
-        b = _f64(b)
-        sh = None if shares is None else _f64(shares)
-        if out is None:
-            out = np.zeros(self.rows)
-        self.ctx.check(lib().its_exact_start(self.h, _ptr(b), _ptr(sh), _ptr(out)), "its_exact_start")
-        return out
+        """Hierarchical-surplus exact solution of A lambda = b (its_exact_start on the octree)."""
+        return self.svo.exact_start(b, shares, out)
 
     def apply(self, x, transpose=False, out=None):
         x = _f64(x)
@@ -365,15 +390,110 @@ def _addr(a):
     return None if a is None else (a.ctypes.data if isinstance(a, np.ndarray) else a.data_ptr())
 
 
-def exact_start_batch(ops, bs, shares=None, outs=None):
-    """Exact starts of many operators of one context (its_exact_start_batch)."""
-    count = len(ops)
+def exact_start_batch(svos, bs, shares=None, outs=None):
+    """Exact starts of many octrees of one context (its_exact_start_batch)."""
+    count = len(svos)
     bs = [_f64(b) for b in bs]
     sh = None if shares is None else [None if x is None else _f64(x) for x in shares]
-    outs = outs if outs is not None else [np.zeros(op.rows) for op in ops]
-    H = (C.c_void_p * count)(*[op.h.value for op in ops])
+    outs = outs if outs is not None else [np.zeros(s.num_verts) for s in svos]
+    H = (C.c_void_p * count)(*[s.h.value for s in svos])
     B = (C.c_void_p * count)(*[_addr(b) for b in bs])
     S = None if sh is None else (C.c_void_p * count)(*[_addr(x) for x in sh])
     X = (C.c_void_p * count)(*[_addr(x) for x in outs])
-    ops[0].ctx.check(lib().its_exact_start_batch(H, count, B, S, X), "its_exact_start_batch")
+    svos[0].ctx.check(lib().its_exact_start_batch(H, count, B, S, X), "its_exact_start_batch")
     return outs
+
+
+def fit_residual_batch(svos, bs, lams):
+    """||b - A lambda|| / ||b|| per octree, matrix-free (its_fit_residual_batch)."""
+    count = len(svos)
+    bs, lams = [_f64(b) for b in bs], [_f64(x) for x in lams]
+    H = (C.c_void_p * count)(*[s.h.value for s in svos])
+    B = (C.c_void_p * count)(*[_addr(b) for b in bs])
+    X = (C.c_void_p * count)(*[_addr(x) for x in lams])
+    rel = np.zeros(count)
+    svos[0].ctx.check(lib().its_fit_residual_batch(H, count, B, X, _ptr(rel)), "its_fit_residual_batch")
+    return rel
+
+
+def learned_start_batch(svos, net, bs, meshes, norm, outs=None):
+    """Learned starts (its_learned_start_batch): meshes is a list of (V, F) per octree."""
+    count = len(svos)
+    bs = [_f64(b) for b in bs]
+    Vs = [_f64(V) for V, _ in meshes]
+    Fs = [_i32(F) for _, F in meshes]
+    norm = np.ascontiguousarray(norm, np.float32)
+    outs = outs if outs is not None else [np.zeros(s.num_verts) for s in svos]
+    H = (C.c_void_p * count)(*[s.h.value for s in svos])
+    B = (C.c_void_p * count)(*[_addr(b) for b in bs])
+    VV = (C.c_void_p * count)(*[_addr(v) for v in Vs])
+    FF = (C.c_void_p * count)(*[_addr(f) for f in Fs])
+    nv = np.array([_n(v) for v in Vs], np.int64)
+    nf = np.array([_n(f) for f in Fs], np.int64)
+    X = (C.c_void_p * count)(*[_addr(x) for x in outs])
+    svos[0].ctx.check(lib().its_learned_start_batch(H, count, net.h, B, VV, _ptr(nv), FF, _ptr(nf), _ptr(norm), X),
+                      "its_learned_start_batch")
+    return outs
+
+
+def _f32(a):
+    if isinstance(a, np.ndarray) or not hasattr(a, "data_ptr"):
+        return np.ascontiguousarray(a, dtype=np.float32)
+    assert str(a.dtype) == "torch.float32" and a.is_contiguous()
+    return a
+
+
+class ShareNet:
+    """The share network (its_mlp): predicts minimum-norm shares from 64 vertex features."""
+
+    def __init__(self, ctx, batch=65536, params=None):
+        self.ctx = ctx
+        h = C.c_void_p()
+        ctx.check(lib().its_mlp_create(ctx.h, batch, C.byref(h)), "its_mlp_create")
+        self.h, self.batch = h, batch
+        self.num_params = int(lib().its_mlp_num_params())
+        ctx._adopt(self)
+        if params is not None:
+            self.set_params(params)
+
+    def close(self):
+        if getattr(self, "h", None):
+            if self.ctx.h is not None:
+                self.ctx._L.its_mlp_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def set_params(self, params):
+        p = _f32(params)
+        assert p.shape[0] == self.num_params
+        self.ctx.check(lib().its_mlp_set_params(self.h, _ptr(p)), "its_mlp_set_params")
+
+    def params(self):
+        p = np.zeros(self.num_params, np.float32)
+        self.ctx.check(lib().its_mlp_get_params(self.h, _ptr(p)), "its_mlp_get_params")
+        return p
+
+    def forward(self, X, out=None):
+        X = _f32(X)
+        n = _n(X)
+        if out is None:
+            out = np.zeros(n, np.float32)
+        self.ctx.check(lib().its_mlp_forward(self.h, _ptr(X), n, _ptr(out)), "its_mlp_forward")
+        return out
+
+    def gradient(self, X, y):
+        X, y = _f32(X), _f32(y)
+        g = np.zeros(self.num_params, np.float32)
+        loss = C.c_float(0)
+        self.ctx.check(lib().its_mlp_gradient(self.h, _ptr(X), _ptr(y), _n(X), _ptr(g), C.byref(loss)),
+                       "its_mlp_gradient")
+        return g, float(loss.value)
+
+    def train(self, X, y, steps, lr=1e-3, seed=0):
+        X, y = _f32(X), _f32(y)
+        curve = np.zeros(max(steps, 1), np.float32)
+        self.ctx.check(lib().its_mlp_train(self.h, _ptr(X), _ptr(y), _n(X), steps, lr, seed, _ptr(curve)),
+                       "its_mlp_train")
+        return curve[:steps]

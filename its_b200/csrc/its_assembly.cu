@@ -2,103 +2,30 @@
 // SparseMatrix::setFromTriplets, ThinShells.cpp:511-606, and setInDomainPoints,
 // SVO.cu:1160-1193).
 //
-// Row v (a corner vertex at depth d, lattice point P, owner node o):
-//   * the coincident vertices at depths j0..d-1 (value 1; the chain stops at the first
-//     finer depth without that corner), found by a bit test in each depth's lattice bitmap;
-//   * the diagonal (value 1);
-//   * for every ancestor of o, the non-zero hats of its 8 corners at v, with the corner
-//     positions origin (+ w) of that ancestor, exactly as the reference computes them.
-// Columns are lattice ranks, so every row comes out sorted: chain < diagonal < ancestors,
-// corners in x-major order. Two passes (count, fill) with an exclusive scan in between.
-// The transpose is a stable radix sort of the entries by column.
+// Rows are generated by walkRow (its_rows.cuh): chain < diagonal < ancestors, so every row
+// comes out sorted. Two passes (count, fill) with an exclusive scan in between. The
+// transpose is a stable radix sort of the entries by column.
 #include <cmath>
 
 #include "its_op.cuh"
+#include "its_rows.cuh"
 
 namespace its {
 
-struct AsmParams {
-  int depth;
-  double3 g;
-  double w0;
-  LatticeIndex lat[kMaxDepth];
-  int64_t vertStart[kMaxDepth + 1];
-  const uint32_t* parent;
-  const uint32_t* morton;
-  const uint32_t* vertLin;
-  const uint32_t* vertOwner;
-  const double* vertPos;
-};
-
 template <bool FILL>
-__global__ void kAssembleRows(const __grid_constant__ AsmParams P, int64_t n, int64_t* __restrict__ rowptrOrCount, int32_t* __restrict__ col,
-                              double* __restrict__ val, uint32_t* __restrict__ rowIdx) {
+__global__ void kAssembleRows(const __grid_constant__ RowParams P, int64_t n, int64_t* __restrict__ rowptrOrCount,
+                              int32_t* __restrict__ col, double* __restrict__ val, uint32_t* __restrict__ rowIdx) {
   const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (r >= n) return;
-  int d = 0;
-  while (d + 1 < P.depth && P.vertStart[d + 1] <= r) ++d;
-  const uint32_t M = P.lat[d].M;
-  const uint32_t lin = P.vertLin[r];
-  const uint32_t X = lin / (M * M), Y = (lin / M) % M, Z = lin % M;
-  const double qx = P.vertPos[3 * r], qy = P.vertPos[3 * r + 1], qz = P.vertPos[3 * r + 2];
-  int j0 = d;
-  for (int j = d - 1; j >= 0; --j) {
-    const int s = d - j;
-    const uint32_t Mj = P.lat[j].M;
-    const uint32_t lj = ((X << s) * Mj + (Y << s)) * Mj + (Z << s);
-    if (!latticeHas(P.lat[j], lj)) break;
-    j0 = j;
-  }
   int64_t k = FILL ? rowptrOrCount[r] : 0;
-  for (int j = j0; j < d; ++j) {
+  walkRow(P, r, rowDepth(P, r), [&](int32_t c, double v) {
     if (FILL) {
-      const int s = d - j;
-      const uint32_t Mj = P.lat[j].M;
-      const uint32_t lj = ((X << s) * Mj + (Y << s)) * Mj + (Z << s);
-      col[k] = (int32_t)latticeRank(P.lat[j], lj);
-      val[k] = 1.0;
+      col[k] = c;
+      val[k] = v;
       rowIdx[k] = (uint32_t)r;
     }
     ++k;
-  }
-  if (FILL) {
-    col[k] = (int32_t)r;
-    val[k] = 1.0;
-    rowIdx[k] = (uint32_t)r;
-  }
-  ++k;
-  uint32_t a = P.parent[P.vertOwner[r]];
-  for (int dd = d + 1; dd < P.depth && a != kNone; ++dd) {
-    uint32_t Xa, Ya, Za;
-    mortonDecode(P.morton[a], Xa, Ya, Za);
-    const double w = P.w0 * (double)(1u << dd);
-    const double bx = latticePos(P.g.x, w, Xa), by = latticePos(P.g.y, w, Ya), bz = latticePos(P.g.z, w, Za);
-    const LatticeIndex& L = P.lat[dd];
-#pragma unroll
-    for (int ox = 0; ox < 2; ++ox) {
-      const double hx = hat1(qx, ox ? bx + w : bx, w);
-      if (hx <= 0.0) continue;
-#pragma unroll
-      for (int oy = 0; oy < 2; ++oy) {
-        const double hy = hat1(qy, oy ? by + w : by, w);
-        if (hy <= 0.0) continue;
-#pragma unroll
-        for (int oz = 0; oz < 2; ++oz) {
-          const double hz = hat1(qz, oz ? bz + w : bz, w);
-          if (hz <= 0.0) continue;
-          const double v = hx * hy * hz;
-          if (v == 0.0) continue;
-          if (FILL) {
-            col[k] = (int32_t)latticeRank(L, ((Xa + ox) * L.M + (Ya + oy)) * L.M + (Za + oz));
-            val[k] = v;
-            rowIdx[k] = (uint32_t)r;
-          }
-          ++k;
-        }
-      }
-    }
-    a = P.parent[a];
-  }
+  });
   if (!FILL) rowptrOrCount[r] = k;
 }
 
@@ -154,17 +81,7 @@ static its_status opBuild(its_op* op) {
   const SvoDevice& d = op->svo->d;
   const int64_t n = d.numVerts;
   op->n = n;
-  AsmParams P;
-  P.depth = d.depth;
-  P.g = make_double3(d.origin[0], d.origin[1], d.origin[2]);
-  P.w0 = d.unit[0];
-  for (int L = 0; L < kMaxDepth; ++L) P.lat[L] = L < d.depth ? d.lattice(L) : LatticeIndex{};
-  for (int L = 0; L <= kMaxDepth; ++L) P.vertStart[L] = L <= d.depth ? d.vertStart[L] : n;
-  P.parent = d.nodeParent;
-  P.morton = d.nodeMorton;
-  P.vertLin = d.vertLin;
-  P.vertOwner = d.vertOwner;
-  P.vertPos = d.vertPos;
+  const RowParams P = rowParams(d);
   its_status st;
   if ((st = devAlloc(ctx, (void**)&op->rowptr, (n + 1) * 8)) != ITS_OK) return st;
   kAssembleRows<false><<<gridFor(n, 128), 128, 0, ctx->stream>>>(P, n, op->rowptr, nullptr, nullptr, nullptr);

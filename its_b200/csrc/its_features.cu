@@ -1,0 +1,468 @@
+// Per-vertex features of the share network and the learned start.
+//
+// For every corner vertex v coincident with a coarser corner (lattice coordinates all even
+// below the root depth; these are the free shares of the exact start) 64 FP32 features:
+//   0  b_v (signed distance at v)            1  s: zero-share surplus of v's coarsest copy
+//   2  zero-share value of the copy one depth up
+//   3  depth / (depth count - 1)             4, 5  coarser / finer copies of v, / depth count
+//   6-11  same-depth axis neighbours present (+x -x +y -y +z -z)
+//   12-17 their b minus b_v                  18-23 their zero-share values
+//   24-29 finer-depth odd neighbours (2X +- e) present   30-35 their zero-share values
+//   36 cell width w_d                        37 b_v / w_d
+//   38 log(1 + samples in the owner node's 27-neighbourhood)
+//   39-41 mean sample offset from v / w_d    42-44 mean sample normal
+//   45 curvature proxy 1 - |mean normal|     46-63 zero
+// Samples are the mesh's face centroids with unit face normals; their per-node sums are
+// formed finest depth first (a stable sort of the samples by fine node, a segmented sum in
+// sample order, then each node sums its 8 children), so the features are deterministic.
+// Features are optionally normalised, (f - mean) * scale, as the network was trained.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "its_op.cuh"
+#include "its_scan.cuh"
+
+namespace its {
+
+constexpr int kFeat = 64;
+
+struct NodeStats {
+  float* cnt;  // per node
+  double* sp;  // 3 per node: sum of sample positions
+  double* sn;  // 3 per node: sum of unit normals
+};
+
+// Face centroid, unit normal and fine node (kNone when no fine node holds the centroid).
+__global__ void kFaceSamples(const double* __restrict__ V, const int32_t* __restrict__ F, int64_t nf, double3 g,
+                             double w0, int res, const uint32_t* __restrict__ morton, int64_t fineCount,
+                             double* __restrict__ cent, double* __restrict__ nrm, uint32_t* __restrict__ node,
+                             uint32_t* __restrict__ ids) {
+  const int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (f >= nf) return;
+  const double* a = V + 3 * (int64_t)F[3 * f];
+  const double* b = V + 3 * (int64_t)F[3 * f + 1];
+  const double* c = V + 3 * (int64_t)F[3 * f + 2];
+  const double cx = (a[0] + b[0] + c[0]) / 3.0, cy = (a[1] + b[1] + c[1]) / 3.0, cz = (a[2] + b[2] + c[2]) / 3.0;
+  const double ux = b[0] - a[0], uy = b[1] - a[1], uz = b[2] - a[2];
+  const double vx = c[0] - a[0], vy = c[1] - a[1], vz = c[2] - a[2];
+  double nx = uy * vz - uz * vy, ny = uz * vx - ux * vz, nz = ux * vy - uy * vx;
+  const double len = sqrt(nx * nx + ny * ny + nz * nz);
+  if (len > 0.0) {
+    nx /= len;
+    ny /= len;
+    nz /= len;
+  }
+  cent[3 * f] = cx;
+  cent[3 * f + 1] = cy;
+  cent[3 * f + 2] = cz;
+  nrm[3 * f] = nx;
+  nrm[3 * f + 1] = ny;
+  nrm[3 * f + 2] = nz;
+  ids[f] = (uint32_t)f;
+  uint32_t t = kNone;
+  const int dx = (int)((cx - g.x) / w0), dy = (int)((cy - g.y) / w0), dz = (int)((cz - g.z) / w0);
+  if (dx >= 0 && dy >= 0 && dz >= 0 && dx < res && dy < res && dz < res) {
+    const uint32_t m = mortonEncode((uint32_t)dx, (uint32_t)dy, (uint32_t)dz);
+    int64_t lo = 0, hi = fineCount;
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (morton[mid] < m) lo = mid + 1;
+      else hi = mid;
+    }
+    if (lo < fineCount && morton[lo] == m) t = (uint32_t)lo;
+  }
+  node[f] = t;
+}
+
+// Fine-node sums over the samples sorted by node (each node's run in sample order).
+__global__ void kFineSums(const uint32_t* __restrict__ sortedNode, const uint32_t* __restrict__ sortedId,
+                          int64_t nf, const double* __restrict__ cent, const double* __restrict__ nrm, NodeStats S) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nf) return;
+  const uint32_t t = sortedNode[i];
+  if (t == kNone || (i > 0 && sortedNode[i - 1] == t)) return;  // first sample of the run only
+  float c = 0.0f;
+  double p[3] = {0, 0, 0}, q[3] = {0, 0, 0};
+  for (int64_t k = i; k < nf && sortedNode[k] == t; ++k) {
+    const uint32_t f = sortedId[k];
+    c += 1.0f;
+    for (int a = 0; a < 3; ++a) {
+      p[a] += cent[3 * (int64_t)f + a];
+      q[a] += nrm[3 * (int64_t)f + a];
+    }
+  }
+  S.cnt[t] = c;
+  for (int a = 0; a < 3; ++a) {
+    S.sp[3 * (int64_t)t + a] = p[a];
+    S.sn[3 * (int64_t)t + a] = q[a];
+  }
+}
+
+// Nodes of one depth sum their 8 children (children 0..7 in order).
+__global__ void kParentSums(int64_t begin, int64_t count, const uint32_t* __restrict__ child0, NodeStats S) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const int64_t t = begin + i;
+  const uint32_t c0 = child0[t];
+  float c = 0.0f;
+  double p[3] = {0, 0, 0}, q[3] = {0, 0, 0};
+  if (c0 != kNone) {
+    for (int k = 0; k < 8; ++k) {
+      const int64_t ch = (int64_t)c0 + k;
+      c += S.cnt[ch];
+      for (int a = 0; a < 3; ++a) {
+        p[a] += S.sp[3 * ch + a];
+        q[a] += S.sn[3 * ch + a];
+      }
+    }
+  }
+  S.cnt[t] = c;
+  for (int a = 0; a < 3; ++a) {
+    S.sp[3 * t + a] = p[a];
+    S.sn[3 * t + a] = q[a];
+  }
+}
+
+struct FeatParams {
+  int depth, res;
+  double w0;
+  LatticeIndex lat[kMaxDepth];
+  int64_t vertStart[kMaxDepth + 1];
+  const uint32_t* vertLin;
+  const uint32_t* vertOwner;
+  const double* vertPos;
+  const uint32_t* nodeNb;
+};
+
+__device__ __forceinline__ int vertDepth(const FeatParams& P, int64_t v) {
+  int d = 0;
+  while (d + 1 < P.depth && P.vertStart[d + 1] <= v) ++d;
+  return d;
+}
+__device__ __forceinline__ bool coincidentVertex(const FeatParams& P, int64_t v, int d) {
+  if (d + 1 >= P.depth) return false;
+  const uint32_t M = P.lat[d].M, lin = P.vertLin[v];
+  return (((lin / (M * M)) | ((lin / M) % M) | (lin % M)) & 1u) == 0u;
+}
+// Vertex index of lattice point (X,Y,Z) at depth d, or -1.
+__device__ __forceinline__ int64_t latticeVertex(const FeatParams& P, int d, int64_t X, int64_t Y, int64_t Z) {
+  if (d < 0 || d >= P.depth) return -1;
+  const LatticeIndex& L = P.lat[d];
+  if (X < 0 || Y < 0 || Z < 0 || X >= L.M || Y >= L.M || Z >= L.M) return -1;
+  const uint32_t lin = (uint32_t)((X * L.M + Y) * L.M + Z);
+  return latticeHas(L, lin) ? (int64_t)latticeRank(L, lin) : -1;
+}
+
+__global__ void kMarkCoincident(const __grid_constant__ FeatParams P, int64_t n, uint32_t* __restrict__ flag) {
+  const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (v >= n) return;
+  flag[v] = coincidentVertex(P, v, vertDepth(P, v)) ? 1u : 0u;
+}
+
+__global__ void kShareFeatures(const __grid_constant__ FeatParams P, const int64_t* __restrict__ ids, int64_t count,
+                               const double* __restrict__ b, const double* __restrict__ lam0, NodeStats S,
+                               const float* __restrict__ norm, float* __restrict__ out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const int64_t v = ids[i];
+  const int d = vertDepth(P, v);
+  const uint32_t M = P.lat[d].M, lin = P.vertLin[v];
+  const int64_t X = lin / (M * M), Y = (lin / M) % M, Z = lin % M;
+  const double w = P.w0 * (double)(1u << d);
+  float f[kFeat];
+#pragma unroll
+  for (int k = 0; k < kFeat; ++k) f[k] = 0.0f;
+  const double bv = b[v];
+  // the coincident copies above and below
+  int up = 0, down = 0;
+  int64_t top = v, X1 = X, Y1 = Y, Z1 = Z;
+  double oneUp = 0.0;
+  for (int dd = d + 1; dd < P.depth; ++dd) {
+    if ((X1 | Y1 | Z1) & 1) break;
+    X1 >>= 1;
+    Y1 >>= 1;
+    Z1 >>= 1;
+    const int64_t u = latticeVertex(P, dd, X1, Y1, Z1);
+    if (u < 0) break;
+    if (dd == d + 1) oneUp = lam0[u];
+    top = u;
+    ++up;
+  }
+  for (int dd = d - 1; dd >= 0; --dd) {
+    const int s = d - dd;
+    if (latticeVertex(P, dd, X << s, Y << s, Z << s) < 0) break;
+    ++down;
+  }
+  f[0] = (float)bv;
+  f[1] = (float)lam0[top];
+  f[2] = (float)oneUp;
+  f[3] = P.depth > 1 ? (float)d / (float)(P.depth - 1) : 0.0f;
+  f[4] = (float)up / (float)P.depth;
+  f[5] = (float)down / (float)P.depth;
+  const int ex[6] = {1, -1, 0, 0, 0, 0}, ey[6] = {0, 0, 1, -1, 0, 0}, ez[6] = {0, 0, 0, 0, 1, -1};
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const int64_t u = latticeVertex(P, d, X + ex[k], Y + ey[k], Z + ez[k]);
+    if (u >= 0) {
+      f[6 + k] = 1.0f;
+      f[12 + k] = (float)(b[u] - bv);
+      f[18 + k] = (float)lam0[u];
+    }
+    if (d > 0) {
+      const int64_t q = latticeVertex(P, d - 1, 2 * X + ex[k], 2 * Y + ey[k], 2 * Z + ez[k]);
+      if (q >= 0) {
+        f[24 + k] = 1.0f;
+        f[30 + k] = (float)lam0[q];
+      }
+    }
+  }
+  f[36] = (float)w;
+  f[37] = (float)(bv / w);
+  // samples in the owner's 27-neighbourhood
+  const uint32_t o = P.vertOwner[v];
+  double c = 0.0, p[3] = {0, 0, 0}, q[3] = {0, 0, 0};
+  for (int k = 0; k < 27; ++k) {
+    const uint32_t t = P.nodeNb[27 * (int64_t)o + k];
+    if (t == kNone) continue;
+    c += (double)S.cnt[t];
+    for (int a = 0; a < 3; ++a) {
+      p[a] += S.sp[3 * (int64_t)t + a];
+      q[a] += S.sn[3 * (int64_t)t + a];
+    }
+  }
+  f[38] = (float)log1p(c);
+  if (c > 0.0) {
+    const double* x = P.vertPos + 3 * v;
+    double nn = 0.0;
+    for (int a = 0; a < 3; ++a) {
+      f[39 + a] = (float)((p[a] / c - x[a]) / w);
+      const double m = q[a] / c;
+      f[42 + a] = (float)m;
+      nn += m * m;
+    }
+    f[45] = (float)(1.0 - sqrt(nn));
+  }
+  float* row = out + i * kFeat;
+#pragma unroll
+  for (int k = 0; k < kFeat; ++k) row[k] = norm ? (f[k] - norm[k]) * norm[kFeat + k] : f[k];
+}
+
+// Learned shares into a zeroed share vector: share[ids[i]] = pred[i] * scale + mean.
+__global__ void kScatterShares(const int64_t* __restrict__ ids, int64_t count, const float* __restrict__ pred,
+                               float scale, float mean, double* __restrict__ shares) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  shares[ids[i]] = (double)pred[i] * (double)scale + (double)mean;
+}
+
+static FeatParams featParams(const SvoDevice& d) {
+  FeatParams P;
+  P.depth = d.depth;
+  P.res = d.res;
+  P.w0 = d.unit[0];
+  for (int L = 0; L < kMaxDepth; ++L) P.lat[L] = L < d.depth ? d.lattice(L) : LatticeIndex{};
+  for (int L = 0; L <= kMaxDepth; ++L) P.vertStart[L] = L <= d.depth ? d.vertStart[L] : d.numVerts;
+  P.vertLin = d.vertLin;
+  P.vertOwner = d.vertOwner;
+  P.vertPos = d.vertPos;
+  P.nodeNb = d.nodeNb;
+  return P;
+}
+
+// Coincident vertices (ascending) into ids (capacity n); *count their number.
+its_status coincidentIds(its_ctx* ctx, const SvoDevice& d, int64_t* ids, int64_t* count) {
+  const int64_t n = d.numVerts;
+  its_status st;
+  DevBuf<uint32_t> flag;
+  DevBuf<int64_t> tot;
+  if ((st = flag.alloc(ctx, n)) != ITS_OK || (st = tot.alloc(ctx, 1)) != ITS_OK) return st;
+  const FeatParams P = featParams(d);
+  kMarkCoincident<<<gridFor(n, 256), 256, 0, ctx->stream>>>(P, n, flag.p);
+  ITS_LAUNCHED(ctx);
+  const uint32_t* fl = flag.p;
+  auto fv = [fl] __device__(int64_t i) -> int64_t { return (int64_t)fl[i]; };
+  auto wr = [fl, ids] __device__(int64_t i, int64_t prefix, int64_t) {
+    if (fl[i]) ids[prefix] = i;
+  };
+  if ((st = scanExclusiveAlloc<int64_t>(ctx, fv, n, wr, tot.p)) != ITS_OK) return st;
+  return readScalar(ctx, tot.p, count);
+}
+
+// Features of the coincident vertices ids[0..count) (see the file comment).
+its_status shareFeatures(its_ctx* ctx, const SvoDevice& d, const double* b, const double* lam0, const double* V,
+                         int64_t nv, const int32_t* F, int64_t nf, const int64_t* ids, int64_t count,
+                         const float* norm, float* out) {
+  (void)nv;
+  its_status st;
+  const int64_t nn = d.numNodes;
+  DevBuf<double> cent, nrm, sp, sn;
+  DevBuf<float> cnt;
+  DevBuf<uint32_t> node, fid, sNode, sId, tk, tv;
+  if ((st = cent.alloc(ctx, 3 * nf)) != ITS_OK || (st = nrm.alloc(ctx, 3 * nf)) != ITS_OK ||
+      (st = node.alloc(ctx, nf)) != ITS_OK || (st = fid.alloc(ctx, nf)) != ITS_OK ||
+      (st = sNode.alloc(ctx, nf)) != ITS_OK || (st = sId.alloc(ctx, nf)) != ITS_OK ||
+      (st = tk.alloc(ctx, nf)) != ITS_OK || (st = tv.alloc(ctx, nf)) != ITS_OK ||
+      (st = cnt.zeros(ctx, nn)) != ITS_OK || (st = sp.zeros(ctx, 3 * nn)) != ITS_OK ||
+      (st = sn.zeros(ctx, 3 * nn)) != ITS_OK)
+    return st;
+  const int64_t fineCount = d.levelCount[0];
+  kFaceSamples<<<gridFor(nf, 256), 256, 0, ctx->stream>>>(V, F, nf, make_double3(d.origin[0], d.origin[1], d.origin[2]),
+                                                         d.unit[0], d.res, d.nodeMorton, fineCount, cent.p, nrm.p,
+                                                         node.p, fid.p);
+  ITS_LAUNCHED(ctx);
+  // stable sort by fine node (kNone sorts last: 32-bit keys)
+  if ((st = radixSortPairs(ctx, node.p, fid.p, sNode.p, sId.p, tk.p, tv.p, nf, 32)) != ITS_OK) return st;
+  NodeStats S{cnt.p, sp.p, sn.p};
+  kFineSums<<<gridFor(nf, 256), 256, 0, ctx->stream>>>(sNode.p, sId.p, nf, cent.p, nrm.p, S);
+  ITS_LAUNCHED(ctx);
+  for (int L = 1; L < d.depth; ++L) {
+    if (!d.levelCount[L]) continue;
+    kParentSums<<<gridFor(d.levelCount[L], 256), 256, 0, ctx->stream>>>(d.levelStart[L], d.levelCount[L],
+                                                                        d.nodeChild0, S);
+    ITS_LAUNCHED(ctx);
+  }
+  const FeatParams P = featParams(d);
+  if (count > 0) {
+    kShareFeatures<<<gridFor(count, 128), 128, 0, ctx->stream>>>(P, ids, count, b, lam0, S, norm, out);
+    ITS_LAUNCHED(ctx);
+  }
+  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITS_OK;
+}
+
+its_status scatterShares(its_ctx* ctx, const int64_t* ids, int64_t count, const float* pred, float scale, float mean,
+                         double* shares, int64_t n) {
+  ITS_CU(ctx, cudaMemsetAsync(shares, 0, n * 8, ctx->stream));
+  if (count > 0) {
+    kScatterShares<<<gridFor(count, 256), 256, 0, ctx->stream>>>(ids, count, pred, scale, mean, shares);
+    ITS_LAUNCHED(ctx);
+  }
+  return ITS_OK;
+}
+
+}  // namespace its
+
+namespace its {
+its_status exactStart(its_ctx* ctx, its_svo* const* svos, int64_t count, const double* const* b,
+                      const double* const* shares, double* const* lam);
+}
+
+using namespace its;
+
+extern "C" its_status its_mlp_forward(its_mlp* mlp, const float* features, int64_t n, float* out);
+
+extern "C" {
+
+its_status its_share_features(its_svo* svo, const double* b, const double* V, int64_t nv, const int32_t* F,
+                              int64_t nf, const float* norm, float* features, int64_t capacity, int64_t* ids,
+                              int64_t* count) {
+  if (!svo || !b || !V || !F || nv <= 0 || nf <= 0 || !count) return ITS_ERR_INVALID;
+  its_ctx* ctx = svo->ctx;
+  ITS_CU(ctx, cudaSetDevice(ctx->device));
+  const SvoDevice& d = svo->d;
+  const int64_t n = d.numVerts;
+  its_status st;
+  InArg<double> dV, db;
+  InArg<int32_t> dF;
+  InArg<float> dn;
+  if ((st = dV.stage(ctx, V, 3 * nv)) != ITS_OK || (st = dF.stage(ctx, F, 3 * nf)) != ITS_OK ||
+      (st = db.stage(ctx, b, n)) != ITS_OK || (st = dn.stage(ctx, norm, norm ? 2 * kFeat : 0)) != ITS_OK)
+    return st;
+  DevBuf<int64_t> dIds;
+  if ((st = dIds.alloc(ctx, n)) != ITS_OK) return st;
+  int64_t cnt = 0;
+  if ((st = coincidentIds(ctx, d, dIds.p, &cnt)) != ITS_OK) return st;
+  *count = cnt;
+  if (!features) return ITS_OK;
+  if (capacity < cnt) return setError(ctx, ITS_ERR_INVALID, "its_share_features: capacity below the count");
+  DevBuf<double> lam0;
+  if ((st = lam0.alloc(ctx, n)) != ITS_OK) return st;
+  const double* bp = db.d;
+  double* lp = lam0.p;
+  if ((st = exactStart(ctx, &svo, 1, &bp, nullptr, &lp)) != ITS_OK) return st;
+  OutArg<float> out;
+  if ((st = out.stage(ctx, features, cnt * kFeat)) != ITS_OK) return st;
+  if ((st = shareFeatures(ctx, d, db.d, lam0.p, dV.d, nv, dF.d, nf, dIds.p, cnt, dn.d, out.d)) != ITS_OK) return st;
+  if ((st = out.finish(ctx)) != ITS_OK) return st;
+  if (ids) ITS_CU(ctx, cudaMemcpyAsync(ids, dIds.p, cnt * 8, cudaMemcpyDefault, ctx->stream));
+  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITS_OK;
+}
+
+its_status its_learned_start_batch(its_svo* const* ops, int64_t count, its_mlp* mlp, const double* const* b,
+                                   const double* const* V, const int64_t* nv, const int32_t* const* F,
+                                   const int64_t* nf, const float* norm, double* const* lambda) {
+  if (!ops || count <= 0 || !mlp || !b || !V || !nv || !F || !nf || !norm || !lambda) return ITS_ERR_INVALID;
+  its_ctx* ctx = ops[0] ? ops[0]->ctx : nullptr;
+  if (!ctx) return ITS_ERR_INVALID;
+  for (int64_t m = 0; m < count; ++m)
+    if (!ops[m] || ops[m]->ctx != ctx || !b[m] || !V[m] || !F[m] || !lambda[m] || nv[m] <= 0 ||
+        nf[m] <= 0)
+      return setError(ctx, ITS_ERR_INVALID, "its_learned_start: bad operator or mesh");
+  ITS_CU(ctx, cudaSetDevice(ctx->device));
+  its_status st;
+  // host norm: input mean[64], input scale[64], output mean, output scale
+  float hn[2 * kFeat + 2];
+  ITS_CU(ctx, cudaMemcpyAsync(hn, norm, sizeof(hn), cudaMemcpyDefault, ctx->stream));
+  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  DevBuf<float> dNorm;
+  if ((st = dNorm.alloc(ctx, 2 * kFeat)) != ITS_OK) return st;
+  ITS_CU(ctx, cudaMemcpyAsync(dNorm.p, hn, 2 * kFeat * 4, cudaMemcpyHostToDevice, ctx->stream));
+  std::vector<InArg<double>> B(count), dV(count);
+  std::vector<InArg<int32_t>> dF(count);
+  std::vector<OutArg<double>> L(count);
+  std::vector<DevBuf<double>> lam0(count), shares(count);
+  std::vector<DevBuf<int64_t>> ids(count);
+  std::vector<const double*> bp(count), sp(count);
+  std::vector<double*> l0(count), lp(count);
+  std::vector<int64_t> cnt(count);
+  int64_t total = 0;
+  for (int64_t m = 0; m < count; ++m) {
+    const int64_t n = ops[m]->d.numVerts;
+    if ((st = B[m].stage(ctx, b[m], n)) != ITS_OK || (st = dV[m].stage(ctx, V[m], 3 * nv[m])) != ITS_OK ||
+        (st = dF[m].stage(ctx, F[m], 3 * nf[m])) != ITS_OK || (st = L[m].stage(ctx, lambda[m], n)) != ITS_OK ||
+        (st = lam0[m].alloc(ctx, n)) != ITS_OK || (st = shares[m].alloc(ctx, n)) != ITS_OK ||
+        (st = ids[m].alloc(ctx, n)) != ITS_OK)
+      return st;
+    bp[m] = B[m].d;
+    l0[m] = lam0[m].p;
+    lp[m] = L[m].d;
+    sp[m] = shares[m].p;
+    if ((st = coincidentIds(ctx, ops[m]->d, ids[m].p, &cnt[m])) != ITS_OK) return st;
+    total += cnt[m];
+  }
+  // zero-share starts (features), features of every mesh into one array, one network pass
+  if ((st = exactStart(ctx, ops, count, bp.data(), nullptr, l0.data())) != ITS_OK) return st;
+  DevBuf<float> feat, pred;
+  if ((st = feat.alloc(ctx, std::max<int64_t>(total, 1) * kFeat)) != ITS_OK ||
+      (st = pred.alloc(ctx, std::max<int64_t>(total, 1))) != ITS_OK)
+    return st;
+  int64_t off = 0;
+  for (int64_t m = 0; m < count; ++m) {
+    if ((st = shareFeatures(ctx, ops[m]->d, bp[m], l0[m], dV[m].d, nv[m], dF[m].d, nf[m], ids[m].p, cnt[m],
+                            dNorm.p, feat.p + off * kFeat)) != ITS_OK)
+      return st;
+    off += cnt[m];
+  }
+  if (total > 0 && (st = its_mlp_forward(mlp, feat.p, total, pred.p)) != ITS_OK) return st;
+  off = 0;
+  for (int64_t m = 0; m < count; ++m) {
+    if ((st = scatterShares(ctx, ids[m].p, cnt[m], pred.p + off, hn[2 * kFeat + 1], hn[2 * kFeat], shares[m].p,
+                            ops[m]->d.numVerts)) != ITS_OK)
+      return st;
+    off += cnt[m];
+  }
+  if ((st = exactStart(ctx, ops, count, bp.data(), sp.data(), lp.data())) != ITS_OK) return st;
+  for (int64_t m = 0; m < count; ++m)
+    if ((st = L[m].finish(ctx)) != ITS_OK) return st;
+  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITS_OK;
+}
+
+its_status its_learned_start(its_svo* svo, its_mlp* mlp, const double* b, const double* V, int64_t nv,
+                             const int32_t* F, int64_t nf, const float* norm, double* lambda) {
+  return its_learned_start_batch(&svo, 1, mlp, &b, &V, &nv, &F, &nf, norm, &lambda);
+}
+
+}  // extern "C"

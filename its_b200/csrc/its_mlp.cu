@@ -1,0 +1,589 @@
+// Share network: a small MLP that predicts, for every corner vertex coincident with a
+// coarser corner, its coefficient in the minimum-norm solution of the shell system (the
+// solution Eigen's CGLS reaches from zero). Those coefficients are exactly the free "shares"
+// of the exact start, so a good prediction puts the exact solution close to the reference's.
+//
+// Network: 64 features -> 128 GELU -> 128 GELU -> 128 GELU -> 1, BF16 weights and
+// activations, FP32 accumulation; FP32 master weights trained with Adam on a mean squared
+// error. Every layer product is one tcgen05 GEMM (kUmmaGemm): 128 rows per CTA, operands
+// staged in shared memory in the 128-byte-swizzled K-major layout, the accumulator in TMEM,
+// the epilogue (bias, GELU, output dot product, loss gradient, GELU derivative) fused and
+// read back with tcgen05.ld. Weight gradients are split-K GEMMs over the batch whose
+// partials are summed in a fixed order, so a training step is deterministic.
+//
+// Parameters (flat FP32): W1[128x64] b1[128] W2[128x128] b2[128] W3[128x128] b3[128]
+// w4[128] b4[1] (W[o][i]: output o, input i).
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "its_ctx.cuh"
+#include "its_umma.cuh"
+
+namespace its {
+
+constexpr int kIn = 64, kHid = 128;
+constexpr int64_t kOffW1 = 0, kOffB1 = kOffW1 + kHid * kIn, kOffW2 = kOffB1 + kHid, kOffB2 = kOffW2 + kHid * kHid,
+                  kOffW3 = kOffB2 + kHid, kOffB3 = kOffW3 + kHid * kHid, kOffW4 = kOffB3 + kHid,
+                  kOffB4 = kOffW4 + kHid, kNumParams = kOffB4 + 1;
+constexpr int kSplitK = 128;  // weight-gradient partial sums per layer
+
+using bf16 = __nv_bfloat16;
+
+__device__ __forceinline__ float geluF(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+__device__ __forceinline__ float geluGrad(float z) {
+  const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
+  const float pdf = 0.39894228040143268f * expf(-0.5f * z * z);
+  return cdf + z * pdf;
+}
+
+// ---- one tcgen05 GEMM: C[m][n] = sum_k A[m][k] B[n][k] over this CTA's K range -------------
+template <int N>
+struct GemmSmem {
+  static constexpr int kA = 128 * 128, kB = N * 128;
+  static constexpr int kBytes = kA + kB + 64 + 1024;  // + mbarrier, TMEM slot, alignment slack
+};
+
+template <int N, class Epi>
+__global__ void __launch_bounds__(128) kUmmaGemm(const bf16* __restrict__ A, int64_t lda, int64_t M,
+                                                 const bf16* __restrict__ B, int64_t ldb, int64_t K,
+                                                 int64_t kPerSplit, Epi epi, int* __restrict__ err) {
+  using namespace umma;
+  extern __shared__ uint8_t smemRaw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smemRaw + 1023) & ~(uintptr_t)1023);
+  uint8_t* sA = smem;
+  uint8_t* sB = smem + GemmSmem<N>::kA;
+  uint64_t* mbar = (uint64_t*)(sB + GemmSmem<N>::kB);
+  uint32_t* slot = (uint32_t*)(mbar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int64_t m0 = (int64_t)blockIdx.x * 128;
+  const int64_t k0 = (int64_t)blockIdx.z * kPerSplit;
+  const int64_t k1 = k0 + kPerSplit < K ? k0 + kPerSplit : K;
+  constexpr uint32_t kCols = N < 32 ? 32 : N;
+  if (warp == 0) tmemAlloc(smemAddr(slot), kCols);
+  if (tid == 0) mbarInit(smemAddr(mbar), 1);
+  fenceBefore();
+  __syncthreads();
+  fenceAfter();
+  const uint32_t tmem = *slot;
+  constexpr uint32_t idesc = idescBf16(128, N);
+  uint32_t phase = 0;
+  bool ok = true;
+  for (int64_t kc = k0; kc < k1; kc += 64) {
+    for (int i = tid; i < 128 * 8; i += 128) {
+      const int r = i >> 3, c = i & 7;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (m0 + r < M) v = __ldg((const uint4*)(A + (m0 + r) * lda + kc + c * 8));
+      *(uint4*)(sA + swizzledChunk(r, c)) = v;
+    }
+    for (int i = tid; i < N * 8; i += 128) {
+      const int r = i >> 3, c = i & 7;
+      *(uint4*)(sB + swizzledChunk(r, c)) = __ldg((const uint4*)(B + (int64_t)r * ldb + kc + c * 8));
+    }
+    fenceProxyAsync();
+    __syncthreads();
+    if (tid == 0) {
+      fenceAfter();
+      const uint64_t da = descSw128(smemAddr(sA)), db = descSw128(smemAddr(sB));
+#pragma unroll
+      for (int k = 0; k < 4; ++k) mma(tmem, da + 2 * k, db + 2 * k, idesc, (kc > k0 || k > 0) ? 1u : 0u);
+      commit(smemAddr(mbar));
+    }
+    ok = mbarWait(smemAddr(mbar), phase) && ok;
+    phase ^= 1u;
+  }
+  fenceAfter();
+  float acc[N];
+  const uint32_t lane = (uint32_t)(warp * 32) << 16;
+#pragma unroll
+  for (int n0 = 0; n0 < N; n0 += 16) {
+    float v[16];
+    tmemLoad16(tmem + lane + (uint32_t)n0, v);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) acc[n0 + j] = v[j];
+  }
+  if (k1 <= k0) {  // an empty split contributes zeros
+#pragma unroll
+    for (int j = 0; j < N; ++j) acc[j] = 0.0f;
+  }
+  const int64_t m = m0 + tid;
+  if (ok && m < M) epi(m, acc);
+  fenceBefore();
+  __syncthreads();
+  if (warp == 0) tmemFree(tmem, kCols);
+  if (!ok && tid == 0) atomicExch(err, 1);
+}
+
+// ---- epilogues ----------------------------------------------------------------------------
+// Hidden layer: z = acc + b, h = gelu(z); Z (FP32, for the backward pass), H row-major and
+// its transpose (the operands of the next layer and of the weight gradient).
+struct EpiHidden {
+  const float* bias;
+  float* Z;
+  bf16* H;
+  bf16* Ht;
+  int64_t ldt;
+  __device__ void operator()(int64_t m, float (&acc)[kHid]) const {
+#pragma unroll
+    for (int j = 0; j < kHid; ++j) {
+      const float z = acc[j] + bias[j];
+      const bf16 h = __float2bfloat16_rn(geluF(z));
+      if (Z) Z[m * kHid + j] = z;
+      H[m * kHid + j] = h;
+      if (Ht) Ht[(int64_t)j * ldt + m] = h;
+    }
+  }
+};
+
+// Last hidden layer plus the output unit. Inference: out = sum_j h_j w4_j + b4. Training also
+// forms the loss gradient d = scale (out - y) and dZ3 = d w4 gelu'(z3), the stored H3 (for
+// the w4 gradient) and the per-row squared error.
+struct EpiOutput {
+  const float* bias;
+  const float* w4;  // BF16-rounded values
+  const float* b4;
+  float* out;
+  // training only
+  const float* y;
+  float scale;
+  bf16* H3;
+  bf16* dZ;
+  bf16* dZt;
+  int64_t ldt;
+  float* dOut;
+  float* sqErr;
+  __device__ void operator()(int64_t m, float (&acc)[kHid]) const {
+    float o = 0.0f;
+#pragma unroll
+    for (int j = 0; j < kHid; ++j) {
+      acc[j] += bias[j];
+      const float h = __bfloat162float(__float2bfloat16_rn(geluF(acc[j])));
+      if (H3) H3[m * kHid + j] = __float2bfloat16_rn(h);
+      o += h * w4[j];
+    }
+    o += b4[0];
+    if (out) out[m] = o;
+    if (!y) return;
+    const float e = o - y[m];
+    const float d = scale * e;
+    dOut[m] = d;
+    sqErr[m] = e * e;
+#pragma unroll
+    for (int j = 0; j < kHid; ++j) {
+      const bf16 g = __float2bfloat16_rn(d * w4[j] * geluGrad(acc[j]));
+      dZ[m * kHid + j] = g;
+      dZt[(int64_t)j * ldt + m] = g;
+    }
+  }
+};
+
+// Backward through a hidden layer: dZ = acc * gelu'(Z) (acc = dH of that layer).
+struct EpiBack {
+  const float* Z;
+  bf16* dZ;
+  bf16* dZt;
+  int64_t ldt;
+  __device__ void operator()(int64_t m, float (&acc)[kHid]) const {
+#pragma unroll
+    for (int j = 0; j < kHid; ++j) {
+      const bf16 g = __float2bfloat16_rn(acc[j] * geluGrad(Z[m * kHid + j]));
+      if (dZ) dZ[m * kHid + j] = g;
+      dZt[(int64_t)j * ldt + m] = g;
+    }
+  }
+};
+
+// Split-K partial of a weight gradient: partial[split][m][n].
+template <int N>
+struct EpiPartial {
+  float* partial;
+  int64_t rows;
+  __device__ void operator()(int64_t m, float (&acc)[N]) const {
+    float* p = partial + ((int64_t)blockIdx.z * rows + m) * N;
+#pragma unroll
+    for (int j = 0; j < N; ++j) p[j] = acc[j];
+  }
+};
+
+// ---- small kernels ----------------------------------------------------------------------
+// Features (FP32, n x 64, already normalised) to BF16 rows (and columns for training).
+__global__ void kFeaturesBf16(const float* __restrict__ X, int64_t n, bf16* __restrict__ Xb, bf16* __restrict__ Xt,
+                              int64_t ldt) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n * kIn) return;
+  const int64_t m = i / kIn;
+  const int k = (int)(i % kIn);
+  const bf16 v = __float2bfloat16_rn(X[i]);
+  Xb[i] = v;
+  if (Xt) Xt[(int64_t)k * ldt + m] = v;
+}
+
+// BF16 weight copies (row-major and transposed) and the BF16-rounded output weights.
+__global__ void kCastWeights(const float* __restrict__ P, bf16* __restrict__ W1, bf16* __restrict__ W1t,
+                             bf16* __restrict__ W2, bf16* __restrict__ W2t, bf16* __restrict__ W3,
+                             bf16* __restrict__ W3t, float* __restrict__ w4r) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < kHid * kIn) {
+    const int o = i / kIn, k = i % kIn;
+    const bf16 v = __float2bfloat16_rn(P[kOffW1 + i]);
+    W1[i] = v;
+    W1t[k * kHid + o] = v;
+  }
+  if (i < kHid * kHid) {
+    const int o = i / kHid, k = i % kHid;
+    const bf16 v2 = __float2bfloat16_rn(P[kOffW2 + i]);
+    W2[i] = v2;
+    W2t[k * kHid + o] = v2;
+    const bf16 v3 = __float2bfloat16_rn(P[kOffW3 + i]);
+    W3[i] = v3;
+    W3t[k * kHid + o] = v3;
+  }
+  if (i < kHid) w4r[i] = __bfloat162float(__float2bfloat16_rn(P[kOffW4 + i]));
+}
+
+// Fixed-order block sum over a row of length n (one block per output).
+__device__ __forceinline__ float blockSum256(float v) {
+  __shared__ float sh[8];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  float t = 0.0f;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < 8; ++w) t += sh[w];
+  return t;
+}
+
+// Gradients not produced by a GEMM: biases of the hidden layers (row sums of dZ^T), the output
+// weights (H3^T dOut), the output bias (sum dOut) and the loss (mean squared error).
+// Block b: 0..383 hidden biases, 384..511 w4, 512 b4, 513 loss.
+__global__ void __launch_bounds__(256) kSmallGrads(const bf16* __restrict__ dZ1t, const bf16* __restrict__ dZ2t,
+                                                  const bf16* __restrict__ dZ3t, const bf16* __restrict__ H3,
+                                                  const float* __restrict__ dOut, const float* __restrict__ sqErr,
+                                                  int64_t n, int64_t ldt, float* __restrict__ grad,
+                                                  float* __restrict__ loss) {
+  const int b = blockIdx.x;
+  float s = 0.0f;
+  if (b < 3 * kHid) {
+    const bf16* row = (b < kHid ? dZ1t : b < 2 * kHid ? dZ2t : dZ3t) + (int64_t)(b % kHid) * ldt;
+    for (int64_t m = threadIdx.x; m < n; m += 256) s += __bfloat162float(row[m]);
+  } else if (b < 4 * kHid) {
+    const int j = b - 3 * kHid;
+    for (int64_t m = threadIdx.x; m < n; m += 256) s += dOut[m] * __bfloat162float(H3[m * kHid + j]);
+  } else if (b == 4 * kHid) {
+    for (int64_t m = threadIdx.x; m < n; m += 256) s += dOut[m];
+  } else {
+    for (int64_t m = threadIdx.x; m < n; m += 256) s += sqErr[m];
+  }
+  const float t = blockSum256(s);
+  if (threadIdx.x != 0) return;
+  if (b < 3 * kHid) {
+    const int64_t off = b < kHid ? kOffB1 : b < 2 * kHid ? kOffB2 : kOffB3;
+    grad[off + b % kHid] = t;
+  } else if (b < 4 * kHid) {
+    grad[kOffW4 + (b - 3 * kHid)] = t;
+  } else if (b == 4 * kHid) {
+    grad[kOffB4] = t;
+  } else {
+    loss[0] = t / (float)n;
+  }
+}
+
+// Weight gradients from the split-K partials (summed in split order).
+__global__ void kSumPartials(const float* __restrict__ P1, const float* __restrict__ P2, const float* __restrict__ P3,
+                             float* __restrict__ grad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < kHid * kIn) {
+    float s = 0.0f;
+    for (int k = 0; k < kSplitK; ++k) s += P1[(int64_t)k * kHid * kIn + i];
+    grad[kOffW1 + i] = s;
+  }
+  if (i < kHid * kHid) {
+    float s2 = 0.0f, s3 = 0.0f;
+    for (int k = 0; k < kSplitK; ++k) {
+      s2 += P2[(int64_t)k * kHid * kHid + i];
+      s3 += P3[(int64_t)k * kHid * kHid + i];
+    }
+    grad[kOffW2 + i] = s2;
+    grad[kOffW3 + i] = s3;
+  }
+}
+
+// Adam (Kingma & Ba): m = b1 m + (1-b1) g; v = b2 v + (1-b2) g^2; p -= lr mhat / (sqrt(vhat) + eps).
+__global__ void kAdam(float* __restrict__ P, float* __restrict__ Mo, float* __restrict__ Ve,
+                      const float* __restrict__ G, int64_t n, float lr, float b1, float b2, float eps, float c1,
+                      float c2) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float g = G[i];
+  const float m = b1 * Mo[i] + (1.0f - b1) * g;
+  const float v = b2 * Ve[i] + (1.0f - b2) * g * g;
+  Mo[i] = m;
+  Ve[i] = v;
+  P[i] -= lr * (m / c1) / (sqrtf(v / c2) + eps);
+}
+
+// Random batch: rows idx of the dataset (features n x 64 FP32, targets n).
+__global__ void kGatherBatch(const float* __restrict__ X, const float* __restrict__ y, int64_t n, uint64_t seed,
+                             uint64_t step, int64_t B, bf16* __restrict__ Xb, bf16* __restrict__ Xt,
+                             float* __restrict__ yb) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= B) return;
+  // splitmix64 of (seed, step, i)
+  uint64_t z = seed + 0x9E3779B97F4A7C15ull * (step * (uint64_t)B + (uint64_t)i + 1);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  const int64_t r = (int64_t)(z % (uint64_t)n);
+  yb[i] = y[r];
+  for (int k = 0; k < kIn; ++k) {
+    const bf16 v = __float2bfloat16_rn(X[r * kIn + k]);
+    Xb[i * kIn + k] = v;
+    Xt[(int64_t)k * B + i] = v;
+  }
+}
+
+template <int N, class Epi>
+static its_status gemm(its_ctx* ctx, const bf16* A, int64_t lda, int64_t M, const bf16* B, int64_t ldb, int64_t K,
+                       int splits, const Epi& epi, int* err) {
+  static bool configured = false;
+  if (!configured) {
+    ITS_CU(ctx, cudaFuncSetAttribute(kUmmaGemm<N, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     GemmSmem<N>::kBytes));
+    configured = true;
+  }
+  const int64_t kPer = ((K / splits + 63) / 64) * 64;
+  dim3 grid((unsigned)((M + 127) / 128), 1, (unsigned)splits);
+  kUmmaGemm<N, Epi><<<grid, 128, GemmSmem<N>::kBytes, ctx->stream>>>(A, lda, M, B, ldb, K, kPer, epi, err);
+  ITS_LAUNCHED(ctx);
+  return ITS_OK;
+}
+
+}  // namespace its
+
+using namespace its;
+
+struct its_mlp {
+  its_ctx* ctx = nullptr;
+  int64_t cap = 0;  // rows per batch
+  float* P = nullptr;
+  float* Mo = nullptr;
+  float* Ve = nullptr;
+  float* G = nullptr;
+  float* loss = nullptr;
+  int64_t step = 0;
+  bf16 *W1, *W1t, *W2, *W2t, *W3, *W3t;
+  float* w4r;
+  // batch buffers
+  bf16 *Xb, *Xt, *H1, *H1t, *H2, *H2t, *H3, *dZ3, *dZ3t, *dZ2, *dZ2t, *dZ1t;
+  float *Z1, *Z2, *yb, *dOut, *sqErr, *out, *part1, *part2, *part3;
+  int* err;
+  std::vector<void*> allocs;
+  template <typename T>
+  its_status alloc(T** p, int64_t count) {
+    its_status s = devAlloc(ctx, (void**)p, (size_t)count * sizeof(T));
+    if (s == ITS_OK) allocs.push_back((void*)*p);
+    return s;
+  }
+};
+
+namespace its {
+
+static its_status mlpCast(its_mlp* h) {
+  kCastWeights<<<gridFor(kHid * kHid, 256), 256, 0, h->ctx->stream>>>(h->P, h->W1, h->W1t, h->W2, h->W2t, h->W3,
+                                                                      h->W3t, h->w4r);
+  ITS_LAUNCHED(h->ctx);
+  return ITS_OK;
+}
+
+// Forward of n <= cap rows already in h->Xb; training forms the loss gradients too.
+static its_status mlpForward(its_mlp* h, int64_t n, bool train, const float* y, float* out) {
+  its_ctx* ctx = h->ctx;
+  its_status st;
+  const int64_t ldt = h->cap;
+  EpiHidden e1{h->P + kOffB1, train ? h->Z1 : nullptr, h->H1, train ? h->H1t : nullptr, ldt};
+  if ((st = gemm<kHid>(ctx, h->Xb, kIn, n, h->W1, kIn, kIn, 1, e1, h->err)) != ITS_OK) return st;
+  EpiHidden e2{h->P + kOffB2, train ? h->Z2 : nullptr, h->H2, train ? h->H2t : nullptr, ldt};
+  if ((st = gemm<kHid>(ctx, h->H1, kHid, n, h->W2, kHid, kHid, 1, e2, h->err)) != ITS_OK) return st;
+  EpiOutput e3{h->P + kOffB3, h->w4r, h->P + kOffB4, out, y, 2.0f / (float)n, train ? h->H3 : nullptr,
+               h->dZ3, h->dZ3t, ldt, h->dOut, h->sqErr};
+  return gemm<kHid>(ctx, h->H2, kHid, n, h->W3, kHid, kHid, 1, e3, h->err);
+}
+
+// Gradient of the mean squared error over the n rows in h->Xb/h->Xt (targets yb) into h->G.
+static its_status mlpGradient(its_mlp* h, int64_t n) {
+  its_ctx* ctx = h->ctx;
+  its_status st;
+  const int64_t ldt = h->cap;
+  if ((st = mlpForward(h, n, true, h->yb, nullptr)) != ITS_OK) return st;
+  // dH2 = dZ3 W3 -> dZ2; dH1 = dZ2 W2 -> dZ1 (transposed only)
+  EpiBack b2{h->Z2, h->dZ2, h->dZ2t, ldt};
+  if ((st = gemm<kHid>(ctx, h->dZ3, kHid, n, h->W3t, kHid, kHid, 1, b2, h->err)) != ITS_OK) return st;
+  EpiBack b1{h->Z1, nullptr, h->dZ1t, ldt};
+  if ((st = gemm<kHid>(ctx, h->dZ2, kHid, n, h->W2t, kHid, kHid, 1, b1, h->err)) != ITS_OK) return st;
+  // weight gradients dW_l = dZ_l^T H_{l-1}: split-K over the batch
+  EpiPartial<kHid> p3{h->part3, kHid};
+  if ((st = gemm<kHid>(ctx, h->dZ3t, ldt, kHid, h->H2t, ldt, n, kSplitK, p3, h->err)) != ITS_OK) return st;
+  EpiPartial<kHid> p2{h->part2, kHid};
+  if ((st = gemm<kHid>(ctx, h->dZ2t, ldt, kHid, h->H1t, ldt, n, kSplitK, p2, h->err)) != ITS_OK) return st;
+  EpiPartial<kIn> p1{h->part1, kHid};
+  if ((st = gemm<kIn>(ctx, h->dZ1t, ldt, kHid, h->Xt, ldt, n, kSplitK, p1, h->err)) != ITS_OK) return st;
+  kSumPartials<<<gridFor(kHid * kHid, 256), 256, 0, ctx->stream>>>(h->part1, h->part2, h->part3, h->G);
+  ITS_LAUNCHED(ctx);
+  kSmallGrads<<<4 * kHid + 2, 256, 0, ctx->stream>>>(h->dZ1t, h->dZ2t, h->dZ3t, h->H3, h->dOut, h->sqErr, n, ldt, h->G,
+                                                     h->loss);
+  ITS_LAUNCHED(ctx);
+  return ITS_OK;
+}
+
+static its_status mlpAdam(its_mlp* h, float lr) {
+  ++h->step;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.0f - powf(b1, (float)h->step), c2 = 1.0f - powf(b2, (float)h->step);
+  kAdam<<<gridFor(kNumParams, 256), 256, 0, h->ctx->stream>>>(h->P, h->Mo, h->Ve, h->G, kNumParams, lr, b1, b2, 1e-8f,
+                                                              c1, c2);
+  ITS_LAUNCHED(h->ctx);
+  return mlpCast(h);
+}
+
+static its_status checkErr(its_mlp* h) {
+  int e = 0;
+  ITS_CU(h->ctx, cudaMemcpyAsync(&e, h->err, 4, cudaMemcpyDeviceToHost, h->ctx->stream));
+  ITS_CU(h->ctx, cudaStreamSynchronize(h->ctx->stream));
+  if (e) return setError(h->ctx, ITS_ERR_TIMEOUT, "share network: a tensor-core wait ran out");
+  return ITS_OK;
+}
+
+}  // namespace its
+
+extern "C" {
+
+its_status its_mlp_create(its_ctx* ctx, int64_t batch, its_mlp** out) {
+  if (!ctx || !out || batch <= 0 || batch % 128) return ITS_ERR_INVALID;
+  ITS_CU(ctx, cudaSetDevice(ctx->device));
+  its_mlp* h = new its_mlp;
+  h->ctx = ctx;
+  h->cap = batch;
+  const int64_t B = batch;
+  its_status s = ITS_OK;
+  auto A = [&](auto** p, int64_t c) {
+    if (s == ITS_OK) s = h->alloc(p, c);
+  };
+  A(&h->P, kNumParams); A(&h->Mo, kNumParams); A(&h->Ve, kNumParams); A(&h->G, kNumParams); A(&h->loss, 1);
+  A(&h->W1, kHid * kIn); A(&h->W1t, kHid * kIn); A(&h->W2, kHid * kHid); A(&h->W2t, kHid * kHid);
+  A(&h->W3, kHid * kHid); A(&h->W3t, kHid * kHid); A(&h->w4r, kHid);
+  A(&h->Xb, B * kIn); A(&h->Xt, B * kIn); A(&h->H1, B * kHid); A(&h->H1t, B * kHid); A(&h->H2, B * kHid);
+  A(&h->H2t, B * kHid); A(&h->H3, B * kHid); A(&h->dZ3, B * kHid); A(&h->dZ3t, B * kHid); A(&h->dZ2, B * kHid);
+  A(&h->dZ2t, B * kHid); A(&h->dZ1t, B * kHid); A(&h->Z1, B * kHid); A(&h->Z2, B * kHid); A(&h->yb, B);
+  A(&h->dOut, B); A(&h->sqErr, B); A(&h->out, B); A(&h->part1, (int64_t)kSplitK * kHid * kIn);
+  A(&h->part2, (int64_t)kSplitK * kHid * kHid); A(&h->part3, (int64_t)kSplitK * kHid * kHid); A(&h->err, 1);
+  if (s != ITS_OK) {
+    for (void* p : h->allocs) devFree(ctx, p);
+    delete h;
+    return s;
+  }
+  cudaMemsetAsync(h->P, 0, kNumParams * 4, ctx->stream);
+  cudaMemsetAsync(h->Mo, 0, kNumParams * 4, ctx->stream);
+  cudaMemsetAsync(h->Ve, 0, kNumParams * 4, ctx->stream);
+  cudaMemsetAsync(h->err, 0, 4, ctx->stream);
+  *out = h;
+  return ITS_OK;
+}
+
+its_status its_mlp_free(its_mlp* h) {
+  if (!h) return ITS_ERR_INVALID;
+  cudaStreamSynchronize(h->ctx->stream);
+  for (void* p : h->allocs) devFree(h->ctx, p);
+  delete h;
+  return ITS_OK;
+}
+
+int64_t its_mlp_num_params(void) { return kNumParams; }
+
+its_status its_mlp_set_params(its_mlp* h, const float* params) {
+  if (!h || !params) return ITS_ERR_INVALID;
+  ITS_CU(h->ctx, cudaMemcpyAsync(h->P, params, kNumParams * 4, cudaMemcpyDefault, h->ctx->stream));
+  ITS_CU(h->ctx, cudaMemsetAsync(h->Mo, 0, kNumParams * 4, h->ctx->stream));
+  ITS_CU(h->ctx, cudaMemsetAsync(h->Ve, 0, kNumParams * 4, h->ctx->stream));
+  h->step = 0;
+  its_status s = mlpCast(h);
+  if (s != ITS_OK) return s;
+  ITS_CU(h->ctx, cudaStreamSynchronize(h->ctx->stream));
+  return ITS_OK;
+}
+
+its_status its_mlp_get_params(its_mlp* h, float* params) {
+  if (!h || !params) return ITS_ERR_INVALID;
+  ITS_CU(h->ctx, cudaMemcpyAsync(params, h->P, kNumParams * 4, cudaMemcpyDefault, h->ctx->stream));
+  ITS_CU(h->ctx, cudaStreamSynchronize(h->ctx->stream));
+  return ITS_OK;
+}
+
+// Predictions for n rows of features (n x 64 FP32, normalised), host or device memory.
+its_status its_mlp_forward(its_mlp* h, const float* X, int64_t n, float* out) {
+  if (!h || (n > 0 && (!X || !out)) || n < 0) return ITS_ERR_INVALID;
+  its_ctx* ctx = h->ctx;
+  ITS_CU(ctx, cudaSetDevice(ctx->device));
+  InArg<float> x;
+  OutArg<float> o;
+  its_status st;
+  if ((st = x.stage(ctx, X, n * kIn)) != ITS_OK) return st;
+  if ((st = o.stage(ctx, out, n)) != ITS_OK) return st;
+  for (int64_t r0 = 0; r0 < n; r0 += h->cap) {
+    const int64_t rows = n - r0 < h->cap ? n - r0 : h->cap;
+    kFeaturesBf16<<<gridFor(rows * kIn, 256), 256, 0, ctx->stream>>>(x.d + r0 * kIn, rows, h->Xb, nullptr, 0);
+    ITS_LAUNCHED(ctx);
+    if ((st = mlpForward(h, rows, false, nullptr, o.d + r0)) != ITS_OK) return st;
+  }
+  if ((st = o.finish(ctx)) != ITS_OK) return st;
+  return checkErr(h);
+}
+
+// Gradient of the mean squared error over n rows (n <= batch, a multiple of 64; no update):
+// grad has its_mlp_num_params() entries; loss may be NULL.
+its_status its_mlp_gradient(its_mlp* h, const float* X, const float* y, int64_t n, float* grad, float* loss) {
+  if (!h || !X || !y || !grad || n <= 0 || n > h->cap || n % 64) return ITS_ERR_INVALID;
+  its_ctx* ctx = h->ctx;
+  ITS_CU(ctx, cudaSetDevice(ctx->device));
+  InArg<float> x, yy;
+  its_status st;
+  if ((st = x.stage(ctx, X, n * kIn)) != ITS_OK) return st;
+  if ((st = yy.stage(ctx, y, n)) != ITS_OK) return st;
+  // columns of the transposed operands are laid out with the batch capacity as leading size
+  kFeaturesBf16<<<gridFor(n * kIn, 256), 256, 0, ctx->stream>>>(x.d, n, h->Xb, h->Xt, h->cap);
+  ITS_LAUNCHED(ctx);
+  ITS_CU(ctx, cudaMemcpyAsync(h->yb, yy.d, n * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+  if ((st = mlpGradient(h, n)) != ITS_OK) return st;
+  ITS_CU(ctx, cudaMemcpyAsync(grad, h->G, kNumParams * 4, cudaMemcpyDefault, ctx->stream));
+  if (loss) ITS_CU(ctx, cudaMemcpyAsync(loss, h->loss, 4, cudaMemcpyDefault, ctx->stream));
+  return checkErr(h);
+}
+
+// steps Adam steps on random batches (batch = capacity) of a resident dataset (n x 64
+// normalised features, n targets; host or device). loss_curve (may be NULL) gets the
+// mean squared error of every step.
+its_status its_mlp_train(its_mlp* h, const float* X, const float* y, int64_t n, int64_t steps, float lr,
+                         uint64_t seed, float* loss_curve) {
+  if (!h || !X || !y || n <= 0 || steps < 0) return ITS_ERR_INVALID;
+  its_ctx* ctx = h->ctx;
+  ITS_CU(ctx, cudaSetDevice(ctx->device));
+  InArg<float> x, yy;
+  its_status st;
+  if ((st = x.stage(ctx, X, n * kIn)) != ITS_OK) return st;
+  if ((st = yy.stage(ctx, y, n)) != ITS_OK) return st;
+  DevBuf<float> curve;
+  if ((st = curve.alloc(ctx, steps > 0 ? steps : 1)) != ITS_OK) return st;
+  for (int64_t s = 0; s < steps; ++s) {
+    kGatherBatch<<<gridFor(h->cap, 256), 256, 0, ctx->stream>>>(x.d, yy.d, n, seed, (uint64_t)s, h->cap, h->Xb, h->Xt,
+                                                               h->yb);
+    ITS_LAUNCHED(ctx);
+    if ((st = mlpGradient(h, h->cap)) != ITS_OK) return st;
+    if ((st = mlpAdam(h, lr)) != ITS_OK) return st;
+    ITS_CU(ctx, cudaMemcpyAsync(curve.p + s, h->loss, 4, cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  if (loss_curve && steps > 0)
+    ITS_CU(ctx, cudaMemcpyAsync(loss_curve, curve.p, steps * 4, cudaMemcpyDefault, ctx->stream));
+  return checkErr(h);
+}
+
+}  // extern "C"

@@ -1,0 +1,112 @@
+// The rows of the thin-shell basis matrix A, generated on the fly from the octree.
+//
+// Row v (a corner vertex at depth d, lattice point P, owner node o) evaluates the fitted
+// field at v (ThinShells::cpCoefficients, ThinShells.cpp:511-606; setInDomainPoints,
+// SVO.cu:1160-1193):
+//   * the coincident vertices at depths j0..d-1 (value 1; the chain stops at the first finer
+//     depth without that corner), found by a bit test in each depth's lattice bitmap;
+//   * the diagonal (value 1);
+//   * for every ancestor of o, the non-zero hats of its 8 corners at v, with the corner
+//     positions origin (+ w) of that ancestor, exactly as the reference computes them.
+// Columns are lattice ranks, so a row comes out sorted: chain < diagonal < ancestors, corners
+// in x-major order. The assembly writes these entries into CSR; the matrix-free kernels
+// (exact start, residual) consume them directly in the same order.
+#pragma once
+#include "its_svo.cuh"
+
+namespace its {
+
+struct RowParams {
+  int depth;
+  double3 g;
+  double w0;
+  LatticeIndex lat[kMaxDepth];
+  int64_t vertStart[kMaxDepth + 1];
+  const uint32_t* parent;
+  const uint32_t* morton;
+  const uint32_t* vertLin;
+  const uint32_t* vertOwner;
+  const double* vertPos;
+};
+
+inline RowParams rowParams(const SvoDevice& d) {
+  RowParams P;
+  P.depth = d.depth;
+  P.g = make_double3(d.origin[0], d.origin[1], d.origin[2]);
+  P.w0 = d.unit[0];
+  for (int L = 0; L < kMaxDepth; ++L) P.lat[L] = L < d.depth ? d.lattice(L) : LatticeIndex{};
+  for (int L = 0; L <= kMaxDepth; ++L) P.vertStart[L] = L <= d.depth ? d.vertStart[L] : d.numVerts;
+  P.parent = d.nodeParent;
+  P.morton = d.nodeMorton;
+  P.vertLin = d.vertLin;
+  P.vertOwner = d.vertOwner;
+  P.vertPos = d.vertPos;
+  return P;
+}
+
+__device__ __forceinline__ int rowDepth(const RowParams& P, int64_t r) {
+  int d = 0;
+  while (d + 1 < P.depth && P.vertStart[d + 1] <= r) ++d;
+  return d;
+}
+
+// A vertex whose lattice coordinates are all even below the root depth coincides with a
+// corner of the next coarser depth.
+__device__ __forceinline__ bool rowCoincident(const RowParams& P, int64_t r, int d) {
+  if (d + 1 >= P.depth) return false;
+  const uint32_t M = P.lat[d].M, lin = P.vertLin[r];
+  return (((lin / (M * M)) | ((lin / M) % M) | (lin % M)) & 1u) == 0u;
+}
+
+// visit(col, val) for every entry of row r (depth d) in column order.
+template <class Visit>
+__device__ __forceinline__ void walkRow(const RowParams& P, int64_t r, int d, Visit&& visit) {
+  const uint32_t M = P.lat[d].M;
+  const uint32_t lin = P.vertLin[r];
+  const uint32_t X = lin / (M * M), Y = (lin / M) % M, Z = lin % M;
+  const double qx = P.vertPos[3 * r], qy = P.vertPos[3 * r + 1], qz = P.vertPos[3 * r + 2];
+  int j0 = d;
+  for (int j = d - 1; j >= 0; --j) {
+    const int s = d - j;
+    const uint32_t Mj = P.lat[j].M;
+    const uint32_t lj = ((X << s) * Mj + (Y << s)) * Mj + (Z << s);
+    if (!latticeHas(P.lat[j], lj)) break;
+    j0 = j;
+  }
+  for (int j = j0; j < d; ++j) {
+    const int s = d - j;
+    const uint32_t Mj = P.lat[j].M;
+    const uint32_t lj = ((X << s) * Mj + (Y << s)) * Mj + (Z << s);
+    visit((int32_t)latticeRank(P.lat[j], lj), 1.0);
+  }
+  visit((int32_t)r, 1.0);
+  uint32_t a = P.parent[P.vertOwner[r]];
+  for (int dd = d + 1; dd < P.depth && a != kNone; ++dd) {
+    uint32_t Xa, Ya, Za;
+    mortonDecode(P.morton[a], Xa, Ya, Za);
+    const double w = P.w0 * (double)(1u << dd);
+    const double bx = latticePos(P.g.x, w, Xa), by = latticePos(P.g.y, w, Ya), bz = latticePos(P.g.z, w, Za);
+    const LatticeIndex& L = P.lat[dd];
+#pragma unroll
+    for (int ox = 0; ox < 2; ++ox) {
+      const double hx = hat1(qx, ox ? bx + w : bx, w);
+      if (hx <= 0.0) continue;
+#pragma unroll
+      for (int oy = 0; oy < 2; ++oy) {
+        const double hy = hat1(qy, oy ? by + w : by, w);
+        if (hy <= 0.0) continue;
+#pragma unroll
+        for (int oz = 0; oz < 2; ++oz) {
+          const double hz = hat1(qz, oz ? bz + w : bz, w);
+          if (hz <= 0.0) continue;
+          const double v = hx * hy * hz;
+          if (v == 0.0) continue;
+          visit((int32_t)latticeRank(L, ((Xa + ox) * L.M + (Ya + oy)) * L.M + (Za + oz)), v);
+        }
+      }
+    }
+    a = P.parent[a];
+  }
+}
+
+}  // namespace its

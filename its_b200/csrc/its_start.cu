@@ -21,35 +21,27 @@
 // inside the row space of A, the shares fix the null-space component of the final
 // coefficients. The field at the corner vertices, and hence in every finest cell, is the
 // same for every exact solution; coarser cells differ by that null-space component.
+//
+// Both passes here are matrix-free: the rows are generated from the octree by walkRow
+// (its_rows.cuh), in the assembled operator's column order, so no CSR is needed.
 #include <algorithm>
+#include <cmath>
 #include <vector>
 
 #include "its_op.cuh"
+#include "its_rows.cuh"
 
 namespace its {
 
-// One depth of one operator.
-struct StartSeg {
-  const int64_t* rowptr;
-  const int32_t* col;
-  const double* val;
+// One depth (or, for the residual, one chunk of rows) of one octree.
+struct RowSeg {
+  const RowParams* P;    // the octree's row parameters (device)
+  int d;                 // depth of the rows (exact start)
+  int64_t rowBegin, rows;
   const double* b;
   const double* shares;  // may be null (all shares 0)
   double* lam;
-  const uint32_t* vertLin;
-  int64_t rowBegin, rows;  // rows of this depth within the operator
-  uint32_t M;              // lattice points per axis at this depth
-  int root;                // the root depth: no coarser corner
 };
-
-constexpr int kStartLanes = 8;  // lanes per row (rows hold at most 1 + 9 (depth - 1) entries)
-
-__device__ __forceinline__ bool evenVertex(const StartSeg& s, int64_t r) {
-  if (s.root) return false;
-  const uint32_t lin = s.vertLin[r], M = s.M;
-  const uint32_t X = lin / (M * M), Y = (lin / M) % M, Z = lin % M;
-  return ((X | Y | Z) & 1u) == 0u;
-}
 
 __device__ __forceinline__ int findSeg(const int64_t* __restrict__ prefix, int nseg, int64_t i) {
   int lo = 0, hi = nseg - 1;  // last segment with prefix[seg] <= i
@@ -61,111 +53,204 @@ __device__ __forceinline__ int findSeg(const int64_t* __restrict__ prefix, int n
   return lo;
 }
 
-// Shares of the even vertices (every depth of every operator).
-__global__ void kStartShares(const StartSeg* __restrict__ segs, const int64_t* __restrict__ prefix, int nseg,
+// Shares of the coincident vertices, zeros elsewhere (segments: whole octrees).
+__global__ void kStartShares(const RowSeg* __restrict__ segs, const int64_t* __restrict__ prefix, int nseg,
                              int64_t total) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= total) return;
   const int g = findSeg(prefix, nseg, i);
-  const StartSeg& s = segs[g];
+  const RowSeg& s = segs[g];
   const int64_t r = s.rowBegin + (i - prefix[g]);
-  s.lam[r] = (evenVertex(s, r) && s.shares) ? s.shares[r] : 0.0;
+  const RowParams& P = *s.P;
+  s.lam[r] = (s.shares && rowCoincident(P, r, rowDepth(P, r))) ? s.shares[r] : 0.0;
 }
 
-// Surplus of the non-even rows of one depth per operator (segments = one depth each).
-__global__ void kStartLevel(const StartSeg* __restrict__ segs, const int64_t* __restrict__ prefix, int nseg,
+// Surplus of the non-coincident rows of one depth per octree, the row summed in column order.
+__global__ void kStartLevel(const RowSeg* __restrict__ segs, const int64_t* __restrict__ prefix, int nseg,
                             int64_t total) {
-  const int64_t item = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / kStartLanes;
-  const int sub = threadIdx.x & (kStartLanes - 1);
-  bool valid = item < total;
-  const StartSeg* s = nullptr;
-  int64_t r = 0, beg = 0, end = 0;
-  if (valid) {
-    const int g = findSeg(prefix, nseg, item);
-    s = &segs[g];
-    r = s->rowBegin + (item - prefix[g]);
-    valid = !evenVertex(*s, r);
-    if (valid) {
-      beg = s->rowptr[r];
-      end = s->rowptr[r + 1];
-    }
-  }
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const int g = findSeg(prefix, nseg, i);
+  const RowSeg& s = segs[g];
+  const int64_t r = s.rowBegin + (i - prefix[g]);
+  const RowParams& P = *s.P;
+  if (rowCoincident(P, r, s.d)) return;
+  const double* lam = s.lam;
   double acc = 0.0;
-  for (int64_t k = beg + sub; k < end; k += kStartLanes) {
-    const int32_t c = s->col[k];
-    if (c != (int32_t)r) acc += s->val[k] * s->lam[c];
-  }
-#pragma unroll
-  for (int o = kStartLanes / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, kStartLanes);
-  if (valid && sub == 0) s->lam[r] = s->b[r] - acc;
+  walkRow(P, r, s.d, [&](int32_t c, double v) {
+    if (c != (int32_t)r) acc += v * lam[c];
+  });
+  s.lam[r] = s.b[r] - acc;
 }
 
-// Exact starts of count operators: b[m], shares[m] (may be null) and lam[m] are device
-// vectors of operator m.
-its_status exactStart(its_ctx* ctx, its_op* const* ops, int64_t count, const double* const* b,
+constexpr int kResThreads = 256;
+constexpr int64_t kResChunk = 16384;
+
+// ||b - A lambda||^2 and ||b||^2 of one chunk of rows (segments = chunks, one block each).
+__global__ void __launch_bounds__(kResThreads) kResidualChunks(const RowSeg* __restrict__ segs, double* __restrict__ part) {
+  const RowSeg& s = segs[blockIdx.x];
+  const RowParams& P = *s.P;
+  double rr = 0.0, bb = 0.0;
+  for (int64_t i = threadIdx.x; i < s.rows; i += kResThreads) {
+    const int64_t r = s.rowBegin + i;
+    double acc = 0.0;
+    const double* lam = s.lam;
+    walkRow(P, r, rowDepth(P, r), [&](int32_t c, double v) { acc += v * lam[c]; });
+    const double e = s.b[r] - acc;
+    rr += e * e;
+    bb += s.b[r] * s.b[r];
+  }
+  __shared__ double srr[kResThreads / 32], sbb[kResThreads / 32];
+  for (int o = 16; o > 0; o >>= 1) {
+    rr += __shfl_down_sync(0xffffffffu, rr, o);
+    bb += __shfl_down_sync(0xffffffffu, bb, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    srr[threadIdx.x >> 5] = rr;
+    sbb[threadIdx.x >> 5] = bb;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, c = 0.0;
+    for (int w = 0; w < kResThreads / 32; ++w) {
+      a += srr[w];
+      c += sbb[w];
+    }
+    part[2 * blockIdx.x] = a;
+    part[2 * blockIdx.x + 1] = c;
+  }
+}
+
+__global__ void kResidualFinish(const double* __restrict__ part, const int64_t* __restrict__ first, int64_t count,
+                                double* __restrict__ rel) {
+  const int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (m >= count) return;
+  double a = 0.0, c = 0.0;
+  for (int64_t k = first[m]; k < first[m + 1]; ++k) {
+    a += part[2 * k];
+    c += part[2 * k + 1];
+  }
+  rel[m] = c > 0.0 ? sqrt(a / c) : sqrt(a);
+}
+
+// Row parameters of count octrees on the device.
+static its_status uploadParams(its_ctx* ctx, its_svo* const* svos, int64_t count, DevBuf<RowParams>& dP) {
+  its_status st;
+  std::vector<RowParams> h(count);
+  for (int64_t m = 0; m < count; ++m) h[m] = rowParams(svos[m]->d);
+  if ((st = dP.alloc(ctx, count)) != ITS_OK) return st;
+  ITS_CU(ctx, cudaMemcpyAsync(dP.p, h.data(), count * sizeof(RowParams), cudaMemcpyHostToDevice, ctx->stream));
+  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITS_OK;
+}
+
+// Exact starts of count octrees (device vectors), matrix-free: one launch for the shares and
+// one per depth (root first) for all octrees together.
+its_status exactStart(its_ctx* ctx, its_svo* const* svos, int64_t count, const double* const* b,
                       const double* const* shares, double* const* lam) {
   its_status st;
+  DevBuf<RowParams> dP;
+  if ((st = uploadParams(ctx, svos, count, dP)) != ITS_OK) return st;
   int maxDepth = 0;
-  for (int64_t m = 0; m < count; ++m) maxDepth = std::max(maxDepth, ops[m]->svo->d.depth);
-  // segments: level t (from the root down) of every operator, then all levels for the shares
-  std::vector<StartSeg> segs;
+  for (int64_t m = 0; m < count; ++m) maxDepth = std::max(maxDepth, svos[m]->d.depth);
+  std::vector<RowSeg> segs;
   std::vector<int64_t> prefix;
-  std::vector<int> levelFirst(maxDepth + 1);
-  std::vector<int64_t> levelRows(maxDepth);
-  for (int t = 0; t < maxDepth; ++t) {
-    levelFirst[t] = (int)segs.size();
+  std::vector<int> first(maxDepth + 2, 0);
+  std::vector<int64_t> rows(maxDepth + 1, 0);
+  // level 0: whole octrees (shares); level t+1: depth (depth-1-t) of every octree
+  for (int t = -1; t < maxDepth; ++t) {
+    first[t + 1] = (int)segs.size();
     int64_t acc = 0;
     for (int64_t m = 0; m < count; ++m) {
-      const SvoDevice& d = ops[m]->svo->d;
-      const int dep = d.depth - 1 - t;  // depth index (0 = finest)
-      if (dep < 0 || d.vertCount[dep] == 0) continue;
-      StartSeg s;
-      s.rowptr = ops[m]->rowptr;
-      s.col = ops[m]->col;
-      s.val = ops[m]->val;
+      const SvoDevice& d = svos[m]->d;
+      RowSeg s;
+      s.P = dP.p + m;
       s.b = b[m];
       s.shares = shares ? shares[m] : nullptr;
       s.lam = lam[m];
-      s.vertLin = d.vertLin;
-      s.rowBegin = d.vertStart[dep];
-      s.rows = d.vertCount[dep];
-      s.M = (uint32_t)(d.res >> dep) + 1u;
-      s.root = dep == d.depth - 1;
+      if (t < 0) {
+        s.d = -1;
+        s.rowBegin = 0;
+        s.rows = d.numVerts;
+      } else {
+        const int dep = d.depth - 1 - t;
+        if (dep < 0 || d.vertCount[dep] == 0) continue;
+        s.d = dep;
+        s.rowBegin = d.vertStart[dep];
+        s.rows = d.vertCount[dep];
+      }
+      if (!s.rows) continue;
       segs.push_back(s);
       prefix.push_back(acc);
       acc += s.rows;
     }
-    levelRows[t] = acc;
+    rows[t + 1] = acc;
   }
-  levelFirst[maxDepth] = (int)segs.size();
+  first[maxDepth + 1] = (int)segs.size();
   const int nseg = (int)segs.size();
   if (!nseg) return ITS_OK;
-  DevBuf<StartSeg> dSegs;
-  DevBuf<int64_t> dPrefix, dAll;
-  if ((st = dSegs.alloc(ctx, nseg)) != ITS_OK || (st = dPrefix.alloc(ctx, nseg)) != ITS_OK ||
-      (st = dAll.alloc(ctx, nseg)) != ITS_OK)
-    return st;
-  // prefix over all segments for the shares pass
-  std::vector<int64_t> all(nseg);
-  int64_t total = 0;
-  for (int g = 0; g < nseg; ++g) {
-    all[g] = total;
-    total += segs[g].rows;
-  }
-  ITS_CU(ctx, cudaMemcpyAsync(dSegs.p, segs.data(), nseg * sizeof(StartSeg), cudaMemcpyHostToDevice, ctx->stream));
+  DevBuf<RowSeg> dSegs;
+  DevBuf<int64_t> dPrefix;
+  if ((st = dSegs.alloc(ctx, nseg)) != ITS_OK || (st = dPrefix.alloc(ctx, nseg)) != ITS_OK) return st;
+  ITS_CU(ctx, cudaMemcpyAsync(dSegs.p, segs.data(), nseg * sizeof(RowSeg), cudaMemcpyHostToDevice, ctx->stream));
   ITS_CU(ctx, cudaMemcpyAsync(dPrefix.p, prefix.data(), nseg * 8, cudaMemcpyHostToDevice, ctx->stream));
-  ITS_CU(ctx, cudaMemcpyAsync(dAll.p, all.data(), nseg * 8, cudaMemcpyHostToDevice, ctx->stream));
-  kStartShares<<<gridFor(total, 256), 256, 0, ctx->stream>>>(dSegs.p, dAll.p, nseg, total);
-  ITS_LAUNCHED(ctx);
-  for (int t = 0; t < maxDepth; ++t) {
-    const int g0 = levelFirst[t], ng = levelFirst[t + 1] - g0;
-    if (!ng || !levelRows[t]) continue;
-    const int64_t threads = levelRows[t] * kStartLanes;
-    kStartLevel<<<(unsigned)((threads + 255) / 256), 256, 0, ctx->stream>>>(dSegs.p + g0, dPrefix.p + g0, ng,
-                                                                          levelRows[t]);
+  for (int t = -1; t < maxDepth; ++t) {
+    const int g0 = first[t + 1], ng = first[t + 2] - g0;
+    const int64_t total = rows[t + 1];
+    if (!ng || !total) continue;
+    if (t < 0)
+      kStartShares<<<gridFor(total, 256), 256, 0, ctx->stream>>>(dSegs.p + g0, dPrefix.p + g0, ng, total);
+    else
+      kStartLevel<<<gridFor(total, 128), 128, 0, ctx->stream>>>(dSegs.p + g0, dPrefix.p + g0, ng, total);
     ITS_LAUNCHED(ctx);
   }
-  // the host vectors above are read by the copies: wait before they go out of scope
+  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));  // the host tables above are read by the copies
+  return ITS_OK;
+}
+
+// ||b - A lambda|| / ||b|| of count octrees (device vectors), matrix-free, into rel[count]
+// (host), each mesh's sum in a fixed order.
+its_status fitResidual(its_ctx* ctx, its_svo* const* svos, int64_t count, const double* const* b,
+                       const double* const* lam, double* rel) {
+  its_status st;
+  DevBuf<RowParams> dP;
+  if ((st = uploadParams(ctx, svos, count, dP)) != ITS_OK) return st;
+  std::vector<RowSeg> segs;
+  std::vector<int64_t> first(count + 1, 0);
+  for (int64_t m = 0; m < count; ++m) {
+    first[m] = (int64_t)segs.size();
+    const int64_t n = svos[m]->d.numVerts;
+    for (int64_t r0 = 0; r0 < n; r0 += kResChunk) {
+      RowSeg s;
+      s.P = dP.p + m;
+      s.d = -1;
+      s.rowBegin = r0;
+      s.rows = std::min(kResChunk, n - r0);
+      s.b = b[m];
+      s.shares = nullptr;
+      s.lam = const_cast<double*>(lam[m]);
+      segs.push_back(s);
+    }
+  }
+  first[count] = (int64_t)segs.size();
+  const int64_t nseg = (int64_t)segs.size();
+  DevBuf<RowSeg> dSegs;
+  DevBuf<int64_t> dFirst;
+  DevBuf<double> part, dRel;
+  if ((st = dSegs.alloc(ctx, std::max<int64_t>(nseg, 1))) != ITS_OK || (st = dFirst.alloc(ctx, count + 1)) != ITS_OK ||
+      (st = part.alloc(ctx, 2 * std::max<int64_t>(nseg, 1))) != ITS_OK || (st = dRel.alloc(ctx, count)) != ITS_OK)
+    return st;
+  ITS_CU(ctx, cudaMemcpyAsync(dSegs.p, segs.data(), nseg * sizeof(RowSeg), cudaMemcpyHostToDevice, ctx->stream));
+  ITS_CU(ctx, cudaMemcpyAsync(dFirst.p, first.data(), (count + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+  if (nseg) {
+    kResidualChunks<<<(unsigned)nseg, kResThreads, 0, ctx->stream>>>(dSegs.p, part.p);
+    ITS_LAUNCHED(ctx);
+  } else {
+    ITS_CU(ctx, cudaMemsetAsync(part.p, 0, 16, ctx->stream));
+  }
+  kResidualFinish<<<gridFor(count, 128), 128, 0, ctx->stream>>>(part.p, dFirst.p, count, dRel.p);
+  ITS_LAUNCHED(ctx);
+  ITS_CU(ctx, cudaMemcpyAsync(rel, dRel.p, count * 8, cudaMemcpyDeviceToHost, ctx->stream));
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   return ITS_OK;
 }
@@ -174,25 +259,33 @@ its_status exactStart(its_ctx* ctx, its_op* const* ops, int64_t count, const dou
 
 using namespace its;
 
+namespace {
+its_status checkSvos(its_svo* const* svos, int64_t count, its_ctx** ctxOut) {
+  if (!svos || count <= 0 || !svos[0]) return ITS_ERR_INVALID;
+  its_ctx* ctx = svos[0]->ctx;
+  for (int64_t m = 0; m < count; ++m)
+    if (!svos[m] || svos[m]->ctx != ctx) return setError(ctx, ITS_ERR_INVALID, "octrees must share one context");
+  *ctxOut = ctx;
+  ITS_CU(ctx, cudaSetDevice(ctx->device));
+  return ITS_OK;
+}
+}  // namespace
+
 extern "C" {
 
-its_status its_exact_start_batch(its_op* const* ops, int64_t count, const double* const* b,
+its_status its_exact_start_batch(its_svo* const* svos, int64_t count, const double* const* b,
                                  const double* const* shares, double* const* lambda) {
-  if (!ops || count <= 0 || !b || !lambda) return ITS_ERR_INVALID;
-  its_ctx* ctx = ops[0] ? ops[0]->ctx : nullptr;
-  if (!ctx) return ITS_ERR_INVALID;
-  for (int64_t m = 0; m < count; ++m)
-    if (!ops[m] || ops[m]->ctx != ctx || !b[m] || !lambda[m] || !ops[m]->svo)
-      return setError(ctx, ITS_ERR_INVALID, "its_exact_start: operators must share one context");
-  ITS_CU(ctx, cudaSetDevice(ctx->device));
-  // stage host vectors on the device
+  its_ctx* ctx = nullptr;
+  its_status st = checkSvos(svos, count, &ctx);
+  if (st != ITS_OK) return st;
+  if (!b || !lambda) return ITS_ERR_INVALID;
   std::vector<InArg<double>> B(count), S(count);
   std::vector<OutArg<double>> L(count);
   std::vector<const double*> db(count), ds(count);
   std::vector<double*> dl(count);
-  its_status st;
   for (int64_t m = 0; m < count; ++m) {
-    const int64_t n = ops[m]->n;
+    if (!b[m] || !lambda[m]) return ITS_ERR_INVALID;
+    const int64_t n = svos[m]->d.numVerts;
     if ((st = B[m].stage(ctx, b[m], n)) != ITS_OK) return st;
     ds[m] = nullptr;
     if (shares && shares[m]) {
@@ -203,16 +296,37 @@ its_status its_exact_start_batch(its_op* const* ops, int64_t count, const double
     db[m] = B[m].d;
     dl[m] = L[m].d;
   }
-  if ((st = exactStart(ctx, ops, count, db.data(), ds.data(), dl.data())) != ITS_OK) return st;
+  if ((st = exactStart(ctx, svos, count, db.data(), ds.data(), dl.data())) != ITS_OK) return st;
   for (int64_t m = 0; m < count; ++m)
     if ((st = L[m].finish(ctx)) != ITS_OK) return st;
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   return ITS_OK;
 }
 
-its_status its_exact_start(its_op* op, const double* b, const double* shares, double* lambda) {
-  if (!op) return ITS_ERR_INVALID;
-  return its_exact_start_batch(&op, 1, &b, &shares, &lambda);
+its_status its_exact_start(its_svo* svo, const double* b, const double* shares, double* lambda) {
+  return its_exact_start_batch(&svo, 1, &b, &shares, &lambda);
+}
+
+its_status its_fit_residual_batch(its_svo* const* svos, int64_t count, const double* const* b,
+                                  const double* const* lambda, double* rel_residual) {
+  its_ctx* ctx = nullptr;
+  its_status st = checkSvos(svos, count, &ctx);
+  if (st != ITS_OK) return st;
+  if (!b || !lambda || !rel_residual) return ITS_ERR_INVALID;
+  std::vector<InArg<double>> B(count), L(count);
+  std::vector<const double*> db(count), dl(count);
+  for (int64_t m = 0; m < count; ++m) {
+    if (!b[m] || !lambda[m]) return ITS_ERR_INVALID;
+    const int64_t n = svos[m]->d.numVerts;
+    if ((st = B[m].stage(ctx, b[m], n)) != ITS_OK || (st = L[m].stage(ctx, lambda[m], n)) != ITS_OK) return st;
+    db[m] = B[m].d;
+    dl[m] = L[m].d;
+  }
+  return fitResidual(ctx, svos, count, db.data(), dl.data(), rel_residual);
+}
+
+its_status its_fit_residual(its_svo* svo, const double* b, const double* lambda, double* rel_residual) {
+  return its_fit_residual_batch(&svo, 1, &b, &lambda, rel_residual);
 }
 
 }  // extern "C"

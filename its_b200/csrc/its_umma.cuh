@@ -82,6 +82,7 @@ __device__ __forceinline__ void tmemLoad16(uint32_t taddr, float (&v)[16]) {
 
 __device__ __forceinline__ void mbarInit(uint32_t mbar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count));
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 // Bounded wait for the given phase parity; false when the bound ran out.
 __device__ __forceinline__ bool mbarWait(uint32_t mbar, uint32_t parity, uint32_t maxTries = 1u << 22) {

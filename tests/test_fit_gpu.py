@@ -206,19 +206,23 @@ def test_exact_start_matches_oracle(ctx, name, kw, res):
     op = Operator(gpu)
     rp, col, val = ref.assemble()
     A = sp.csr_matrix((val, col, rp), shape=(op.rows, op.rows))
-    # zero shares: an exact solution (the oracle sums each row in column order, the GPU in
-    # 8-lane partial sums, so the two agree to rounding carried through the depth levels)
+    # zero shares: an exact solution; the GPU generates each row from the octree and sums it
+    # in column order like the oracle, so the two are bit-identical
     lam_ref = ref.exact_start(b)
-    lam = op.exact_start(b)
-    assert np.abs(lam - lam_ref).max() <= 1e-12 * np.abs(lam_ref).max()
+    lam = gpu.exact_start(b)
+    assert np.array_equal(lam, lam_ref)
     assert np.linalg.norm(A @ lam - b) <= 1e-14 * np.linalg.norm(b)
+    # the matrix-free residual agrees with the assembled operator's
+    rel = np.linalg.norm(A @ lam - b) / np.linalg.norm(b)
+    assert abs(gpu.residual(b, lam) - rel) <= 1e-3 * rel + 1e-17
     # CGLS started there stops at its residual test
     x, rep = op.solve(b, tol=1e-6, stop_rule=1, x0=lam)
     assert rep["iterations"] == 0 and rep["converged"] and rep["rel_residual"] <= 1e-14
     # the shares fix the null-space component: the min-norm shares give back the (zero-start)
     # CGLS solution, and every exact solution has the same field at the shell samples
     x_mn, _ = oracle.cgls(rp, col, val, b, 1e-14, 20000, 1)
-    lam_mn = op.exact_start(b, shares=x_mn)
+    lam_mn = gpu.exact_start(b, shares=x_mn)
+    assert np.array_equal(lam_mn, ref.exact_start(b, shares=x_mn))
     assert np.abs(lam_mn - x_mn).max() <= 1e-12 * np.abs(x_mn).max()
     P = np.vstack([V, ref.intersections()[0]])
     f0, _ = ref.eval_points(lam, P)
@@ -228,16 +232,18 @@ def test_exact_start_matches_oracle(ctx, name, kw, res):
 
 @pytest.mark.gpu
 def test_exact_start_batch_matches_single(ctx):
-    from its_b200 import Operator, Svo
-    from its_b200.api import exact_start_batch
-    ops, bs = [], []
+    from its_b200 import Svo
+    from its_b200.api import exact_start_batch, fit_residual_batch
+    svos, bs = [], []
     for name, kw, res in FIT_CASES + [("superquadric", dict(e1=0.4, e2=2.5, subdiv=4), 64)]:
         V, F, o, w = prepared_mesh(name, **kw)
         svo = Svo(ctx, V, F, res, o, w)
         bs.append(ctx.signed_distance(svo.vertices()[0], V, F))
-        ops.append(Operator(svo))
+        svos.append(svo)
     rng = np.random.default_rng(5)
-    shares = [None, rng.standard_normal(ops[1].rows) * 1e-3, None, None]
-    outs = exact_start_batch(ops, bs, shares)
-    for op, b, s, x in zip(ops, bs, shares, outs):
-        assert np.array_equal(x, op.exact_start(b, shares=s))
+    shares = [None, rng.standard_normal(svos[1].num_verts) * 1e-3, None, None]
+    outs = exact_start_batch(svos, bs, shares)
+    rels = fit_residual_batch(svos, bs, outs)
+    for svo, b, s, x, r in zip(svos, bs, shares, outs, rels):
+        assert np.array_equal(x, svo.exact_start(b, shares=s))
+        assert r == svo.residual(b, x) and r <= 1e-14

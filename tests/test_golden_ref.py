@@ -38,3 +38,23 @@ def test_packed_mc_table_matches_reference():
         ref = [x for x in GOLD["triTable"][c] if x >= 0]
         assert n == GOLD["nVertsTable"][c]
         assert edges == ref
+
+
+def test_share_network_oracle_gradient_finite_differences():
+    # the float64 backward of the share-network oracle against central differences
+    from oracle import mlp
+    rng = np.random.default_rng(0)
+    P = mlp.init_params(1).astype(np.float64)
+    X = rng.standard_normal((16, mlp.N_IN))
+    y = rng.standard_normal(16)
+    g, _ = mlp.gradient(P, X, y, bf16_round=False)
+    idx = rng.choice(mlp.NUM_PARAMS, 40, replace=False)
+    for i in list(idx) + [mlp.NUM_PARAMS - 1]:
+        h = 1e-6
+        Pp, Pm = P.copy(), P.copy()
+        Pp[i] += h
+        Pm[i] -= h
+        lp = np.mean((mlp.forward(Pp, X, False) - y) ** 2)
+        lm = np.mean((mlp.forward(Pm, X, False) - y) ** 2)
+        fd = (lp - lm) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(fd)), (i, fd, g[i])

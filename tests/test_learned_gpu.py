@@ -1,0 +1,62 @@
+"""Learned start: share-network features against the numpy oracle, and the learned start
+as the composition features -> network -> exact start.
+
+Bars: features agree with the oracle to FP32 rounding (1e-5 relative per feature, the FP64
+sums being formed in the same order); the learned start equals the exact start with the
+network's shares bit for bit and has a residual at rounding level.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import prepared_mesh
+from oracle import features as ofeat
+from oracle import mlp as omlp
+
+CASES = [("small", {}, 16), ("c0", {}, 32), ("torus", dict(R=0.7, r=0.25, rings=48, segs=24), 32)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,kw,res", CASES, ids=[f"{c[0]}-{c[2]}" for c in CASES])
+def test_share_features_match_oracle(ctx, name, kw, res):
+    from its_b200 import Svo
+    V, F, o, w = prepared_mesh(name, **kw)
+    ref = oracle.Svo(V, F, res, o, w)
+    gpu = Svo(ctx, V, F, res, o, w)
+    b = oracle.signed_distance(ref.vertices()[0], V, F)
+    lam0 = ref.exact_start(b)
+    f_ref, ids_ref = ofeat.share_features(ref, b, V, F, lam0)
+    f_gpu, ids_gpu = gpu.share_features(b, V, F)
+    assert np.array_equal(ids_gpu, ids_ref) and len(ids_ref) > 0
+    scale = np.maximum(np.abs(f_ref).max(0), 1e-30)
+    err = (np.abs(f_gpu - f_ref) / scale).max(0)
+    assert err.max() <= 1e-5, np.argmax(err)
+    # normalisation is (f - mean) * scale
+    rng = np.random.default_rng(0)
+    norm = np.concatenate([rng.standard_normal(64), rng.uniform(0.5, 2, 64)]).astype(np.float32)
+    f_n, _ = gpu.share_features(b, V, F, norm)
+    assert np.allclose(f_n, (f_gpu - norm[:64]) * norm[64:], rtol=1e-6, atol=1e-6)
+
+
+@pytest.mark.gpu
+def test_learned_start_is_exact_start_with_predicted_shares(ctx):
+    from its_b200 import Svo
+    from its_b200.api import ShareNet, learned_start_batch
+    net = ShareNet(ctx, batch=4096, params=omlp.init_params(7) * np.float32(0.1))
+    rng = np.random.default_rng(1)
+    norm = np.concatenate([rng.standard_normal(64) * 0.01, np.ones(64), [0.001, 0.01]]).astype(np.float32)
+    svos, bs, meshes = [], [], []
+    for name, kw, res in CASES:
+        V, F, o, w = prepared_mesh(name, **kw)
+        s = Svo(ctx, V, F, res, o, w)
+        svos.append(s)
+        bs.append(ctx.signed_distance(s.vertices()[0], V, F))
+        meshes.append((V, F))
+    outs = learned_start_batch(svos, net, bs, meshes, norm)
+    for s, b, (V, F), lam in zip(svos, bs, meshes, outs):
+        feats, ids = s.share_features(b, V, F, norm[:128])
+        shares = np.zeros(s.num_verts)
+        shares[ids] = net.forward(feats).astype(np.float64) * float(norm[129]) + float(norm[128])
+        assert np.array_equal(lam, s.exact_start(b, shares))
+        assert s.residual(b, lam) <= 1e-14
+    net.close()
