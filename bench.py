@@ -3,19 +3,25 @@
 
 Workload (default): the (3,5) torus-knot tube -- 4,096 rings x 128 segments = 1,048,576
 faces, FP32 vertices with N(0, 1e-3) jitter (seed 1) -- normalised to the unit cube, SVO
-depth 9 (256^3 voxels), plain FP64 LSCG to 1e-6 relative residual, marching cubes at 512^3.
+depth 9 (256^3 voxels), fit to 1e-6 relative residual, marching cubes at 512^3.
 
-A step is one fit: operator assembly (ThinShells::cpCoefficients) plus the LSCG solve to
-the stopping tolerance, inputs (octree, right-hand side) already resident in HBM. `value`
-is the fit time in ms (max over ranks); `e2e` is the same fit through the C ABI with the
-right-hand side in pinned host memory and the coefficients read back every step. Also
-reported: the mixed-precision fit, marching-cubes throughput, the SVO build, the SpMV
-roofline and the CPU oracle on the host cores.
+A step is one fit from the octree and right-hand side (resident in HBM) to coefficients
+whose relative residual ||b - A lambda|| / ||b|| is at most 1e-6: the learned start (share
+features -> share network on the tensor cores -> exact start) checked by the matrix-free
+FP64 residual, with the plain LSCG from that start as the fallback. `value` is its time in
+ms (max over ranks); `e2e` is the same call through the C ABI with the mesh and right-hand
+side in pinned host memory and the coefficients read back every step. Beside it: the plain
+FP64 LSCG from zero (assembly + CGLS, the reference's method) and the mixed-precision
+LSCG on the same octree, the field error of the learned fit against the FP64 LSCG, the
+learned fit's breakdown, the 256-mesh uneven batch (plain per-mesh LSCG vs one learned
+batch), marching-cubes throughput, the SpMV roofline of the plain path and the CPU oracle
+on the host cores.
 
 --impl reference times the CPU restatement of the reference's fit (oracle/, OpenMP on all
 host cores) on the same workload.
 """
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -137,7 +143,8 @@ def lpt_shard(costs, world):
 def run_ours(args):
     import torch
     from its_b200 import OP_FP32_VALUES, PREC_MIXED, STOP_RESIDUAL, Context, Operator, Svo, lib
-    import ctypes as C
+    from its_b200 import sharenet
+    from its_b200.api import ShareNet, fit_residual_batch, learned_start_batch
 
     rank, world, local = dist_setup(args)
     torch.cuda.set_device(local)
@@ -181,14 +188,24 @@ def run_ours(args):
     b = ctx.signed_distance(pos, V, F)
     n = svo.num_verts
     b_dev = torch.from_numpy(b).cuda()
+    V_dev, F_dev = torch.from_numpy(np.ascontiguousarray(V)).cuda(), torch.from_numpy(np.ascontiguousarray(F)).cuda()
     lam_dev = torch.empty_like(b_dev)
+    params, norm = sharenet.load()
+    net = ShareNet(ctx, batch=65536, params=params)
     rep_box = {}
 
-    def fit_step():
-        op = Operator(svo)
-        _, rep = op.solve(b_dev, tol=wl["tol"], stop_rule=STOP_RESIDUAL, out=lam_dev)
-        rep_box["rep"], rep_box["nnz"] = rep, op.nnz
-        op.close()
+    # ---- the headline fit: learned start verified by the FP64 residual -------------------
+    # shares from the network -> exact start -> ||b - A lambda|| / ||b|| (matrix-free, FP64);
+    # the plain LSCG from that start is the fallback when the residual misses the tolerance.
+    def learned_step(b_in=b_dev, mesh=(V_dev, F_dev), out=lam_dev):
+        learned_start_batch([svo], net, [b_in], [mesh], norm, outs=[out])
+        rel = fit_residual_batch([svo], [b_in], [out])[0]
+        if rel > wl["tol"]:
+            op = Operator(svo)
+            _, r = op.solve(b_in, tol=wl["tol"], stop_rule=STOP_RESIDUAL, x0=out, out=out)
+            op.close()
+            rel = r["rel_residual"]
+        rep_box["learned_rel"] = rel
 
     # The clock sampler starts before the warm-up so that nvidia-smi's start-up (NVML
     # initialisation, which stalls the driver) falls outside the timed steps.
@@ -196,39 +213,87 @@ def run_ours(args):
     clocks.start()
     time.sleep(1.5)
     for _ in range(args.warmup):
-        fit_step()
+        learned_step()
     barrier_sync()
     launches0 = ctx.kernel_launches
-    fit_ms = timed(fit_step, args.steps)
-    launches = ctx.kernel_launches - launches0
+    fit_ms = timed(learned_step, args.steps)
+    launches = (ctx.kernel_launches - launches0) // max(args.steps, 1)
     barrier_sync()
-    clk = clocks.stop()
     fit_ms = max_ranks(fit_ms)
-    rep, nnz = rep_box["rep"], rep_box["nnz"]
+
+    # ---- plain FP64 LSCG from zero (the reference's method) and the mixed-precision form --
+    def plain_step():
+        op = Operator(svo)
+        _, r = op.solve(b_dev, tol=wl["tol"], stop_rule=STOP_RESIDUAL, out=lam_dev)
+        rep_box["plain"], rep_box["nnz"] = r, op.nnz
+        op.close()
+
+    def mixed_step():
+        op = Operator(svo, mode=OP_FP32_VALUES)
+        _, r = op.solve(b_dev, tol=wl["tol"], stop_rule=STOP_RESIDUAL, precision=PREC_MIXED, ir_steps=3,
+                        inner_tol=1e-3, out=lam_dev)
+        rep_box["mixed"] = r
+        op.close()
+
+    for _ in range(args.warmup):
+        plain_step()
+    plain_ms = max_ranks(timed(plain_step, args.steps))
+    mixed_step()
+    mixed_ms = max_ranks(timed(mixed_step, max(1, args.steps // 2)))
+    clk = clocks.stop()
+    nnz = rep_box["nnz"]
     if args.only == "fit":
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": round(fit_ms, 4), "unit": "ms", "only": "fit",
-                              "iterations": rep["iterations"], "gpu_launches": launches}), flush=True)
+                              "plain_fp64_ms": round(plain_ms, 4), "gpu_launches": launches}), flush=True)
         if pg:
             pg.barrier()
             pg.destroy_process_group()
         return
 
-    # breakdown: assembly alone, solve alone on a prepared operator
-    asm_ms = timed(lambda: Operator(svo).close(), args.steps)
-    op_s = Operator(svo)
-    solve_ms = timed(lambda: op_s.solve(b_dev, tol=wl["tol"], stop_rule=STOP_RESIDUAL, out=lam_dev), args.steps)
-    op_s.close()
+    # ---- breakdown of the learned fit ----------------------------------------------------
+    from its_b200.api import exact_start_batch
+    feats, ids = svo.share_features(b, V, F, norm[:128])
+    t_features = timed(lambda: svo.share_features(b_dev, V_dev, F_dev, norm[:128]), 3)
+    t_start = timed(lambda: exact_start_batch([svo], [b_dev], outs=[lam_dev]), 5)
+    t_resid = timed(lambda: fit_residual_batch([svo], [b_dev], [lam_dev]), 5)
+    feats_dev = torch.from_numpy(feats).cuda()
+    pred_dev = torch.empty(feats.shape[0], dtype=torch.float32, device="cuda")
+    t_net = timed(lambda: net.forward(feats_dev, out=pred_dev), 5)
 
-    # ---- end to end through the C ABI: pinned host rhs in, coefficients out --------------
+    # ---- field error of the learned fit against the FP64 LSCG from zero ------------------
+    learned_step()
+    lam_learned = lam_dev.cpu().numpy()
+    op = Operator(svo)
+    x_ref, rep_ref = op.solve(b, tol=1e-12, max_iters=20000, stop_rule=STOP_RESIDUAL)
+    op.close()
+    lam_zero = svo.exact_start(b)
+    samples = np.vstack([V, svo.shell_samples(V, F)[0]])
+    f_ref = svo.eval_points(x_ref, samples)[0]
+    G = 128
+    g_ref = svo.eval_grid(x_ref, o, w, G)
+    scale = float(np.abs(b).max())
+    field = {"reference": "FP64 LSCG from zero to 1e-12 relative residual (%d iterations)" % rep_ref["iterations"],
+             "scale": "max |b|", "grid": "%d^3 corners of the box" % (G + 1)}
+    for name, lam in (("learned", lam_learned), ("zero_shares", lam_zero)):
+        d = svo.eval_grid(lam, o, w, G) - g_ref
+        e = svo.eval_points(lam, samples)[0] - f_ref
+        field[name] = {"grid_max": float(np.abs(d).max() / scale), "grid_rms": float(np.sqrt(np.mean(d * d)) / scale),
+                       "samples_max": float(np.abs(e).max() / scale),
+                       "coef_rel": float(np.linalg.norm(lam - x_ref) / np.linalg.norm(x_ref))}
+    inner, outer, _ = svo.shell_iso_values(x_ref, samples)
+    il, ol, _ = svo.shell_iso_values(lam_learned, samples)
+    field["iso_abs_diff"] = [abs(il - inner), abs(ol - outer)]
+
+    # ---- end to end through the C ABI: host mesh and rhs in, host coefficients out --------
     b_host = torch.from_numpy(b).pin_memory()
     lam_host = torch.empty(n, dtype=torch.float64).pin_memory()
-    b_np, lam_np = b_host.numpy(), lam_host.numpy()
+    V_host = torch.from_numpy(np.ascontiguousarray(V)).pin_memory()
+    F_host = torch.from_numpy(np.ascontiguousarray(F)).pin_memory()
+    b_np, lam_np, V_np, F_np = b_host.numpy(), lam_host.numpy(), V_host.numpy(), F_host.numpy()
 
     def e2e_step():
-        op = Operator(svo)
-        op.solve(b_np, tol=wl["tol"], stop_rule=STOP_RESIDUAL, out=lam_np)
-        op.close()
+        learned_step(b_np, (V_np, F_np), lam_np)
 
     for _ in range(max(1, args.warmup // 2)):
         e2e_step()
@@ -239,27 +304,14 @@ def run_ours(args):
     torch.cuda.synchronize()
     e2e_ms = max_ranks((time.perf_counter() - t0) * 1e3 / args.steps)
 
-    # ---- mixed precision fit -----------------------------------------------------------------
-    rep_m = {}
-
-    def mixed_step():
-        op = Operator(svo, mode=OP_FP32_VALUES)
-        _, r = op.solve(b_dev, tol=wl["tol"], stop_rule=STOP_RESIDUAL, precision=PREC_MIXED, ir_steps=3,
-                        inner_tol=1e-3, out=lam_dev)
-        rep_m["rep"] = r
-        op.close()
-
-    mixed_step()
-    mixed_ms = max_ranks(timed(mixed_step, max(1, args.steps // 2)))
-
-    # ---- roofline of the dominant kernel: the binned CSR SpMV ------------------------------
+    # ---- roofline: the plain path's dominant kernel, the binned CSR SpMV ------------------
     op = Operator(svo)
     x_dev = torch.randn(n, dtype=torch.float64, device="cuda")
     y_dev = torch.empty_like(x_dev)
     # A alone (120 MB at this size) nearly fits the 126 MB L2, so every timed launch starts
     # from a flushed L2 (a 256 MB write), as in the CGLS loop where A and A^T alternate.
     flush = torch.empty(32 * 2 ** 20, dtype=torch.float64, device="cuda")
-    spmv, samples = {}, {0: [], 1: []}
+    spmv, samples_t = {}, {0: [], 1: []}
     for tr in (0, 1):
         for _ in range(3):
             op.apply(x_dev, transpose=bool(tr), out=y_dev)
@@ -271,9 +323,9 @@ def run_ours(args):
             op.apply(x_dev, transpose=bool(tr), out=y_dev)
             e1.record(stream)
             e1.synchronize()
-            samples[tr].append(e0.elapsed_time(e1))
+            samples_t[tr].append(e0.elapsed_time(e1))
     for tr in (0, 1):
-        spmv[tr] = statistics.median(samples[tr])
+        spmv[tr] = statistics.median(samples_t[tr])
     del flush
     op.close()
     spmv_bytes = 12 * nnz + 24 * n  # values 8 + columns 4 per entry; rowptr 8, x 8, y 8 per row
@@ -284,21 +336,19 @@ def run_ours(args):
     # ---- dense field + marching cubes ---------------------------------------------------------
     R = wl["mc_res"]
     M = R + 1
-    field = torch.empty(M ** 3, dtype=torch.float64, device="cuda")
-    lam_fit = lam_dev.clone()
-    samples = np.vstack([V, svo.shell_samples(V, F)[0]])
-    inner, outer, _ = svo.shell_iso_values(lam_fit.cpu().numpy(), samples)
+    fieldbuf = torch.empty(M ** 3, dtype=torch.float64, device="cuda")
+    lam_fit = torch.from_numpy(lam_learned).cuda()
     L = lib()
     o_np, w_np = np.ascontiguousarray(o), np.ascontiguousarray(w)
     cube = torch.empty(R ** 3, dtype=torch.uint8, device="cuda")
     nv = C.c_int64(0)
 
     def field_step():
-        svo.eval_grid(lam_fit, o, w, R, out=field)
+        svo.eval_grid(lam_fit, o, w, R, out=fieldbuf)
 
     def mc_step():
-        st = L.its_marching_cubes(ctx.h, C.c_void_p(field.data_ptr()), R, o_np.ctypes.data_as(C.c_void_p),
-                                  w_np.ctypes.data_as(C.c_void_p), float(outer), C.c_void_p(cube.data_ptr()), None, 0,
+        st = L.its_marching_cubes(ctx.h, C.c_void_p(fieldbuf.data_ptr()), R, o_np.ctypes.data_as(C.c_void_p),
+                                  w_np.ctypes.data_as(C.c_void_p), float(ol), C.c_void_p(cube.data_ptr()), None, 0,
                                   C.byref(nv))
         ctx.check(st, "its_marching_cubes")
 
@@ -308,40 +358,104 @@ def run_ours(args):
     mc_ms = timed(mc_step, 3)
     mc_mvox = R ** 3 / ((field_ms + mc_ms) * 1e-3) / 1e6
 
+    # ---- the uneven multi-mesh batch: plain per-mesh FP64 LSCG vs one learned batch ---------
+    batch = None
+    if not args.no_batch:
+        batch = run_batch(ctx, net, norm, timed, wl["tol"], world, rank, min(args.steps, 3), max_ranks)
+
     # ---- CPU baseline: the oracle's fit on the host cores (rank 0, N = 1) -------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_fit(V, F, o, w, wl, b)
 
     if rank == 0:
+        plain = rep_box["plain"]
         line = {
             "metric": METRIC, "value": round(fit_ms, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(fit_ms, 4), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": wl["desc"], "unknowns": n, "nnz": nnz, "iterations": rep["iterations"],
-                       "rel_residual": rep["rel_residual"], "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "operator (A and A^T, %.0f MB) larger than the 126 MB L2" % (2 * 12 * nnz / 1e6)},
-            "e2e": {"value": round(e2e_ms, 4), "unit": "ms", "h2d_bytes_per_step": 8 * n,
+            "config": {"workload": wl["desc"], "unknowns": n, "nnz": nnz, "fit": "learned start (share network, "
+                       "BF16 tcgen05) + exact start + FP64 residual check; plain LSCG from that start as fallback",
+                       "rel_residual": rep_box["learned_rel"], "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "octree tables and vectors; the plain path's operator (A and A^T, %.0f MB) exceeds the "
+                             "126 MB L2" % (2 * 12 * nnz / 1e6)},
+            "plain_fp64": {"ms": round(plain_ms, 4), "iterations": plain["iterations"],
+                           "rel_residual": plain["rel_residual"], "speedup": round(plain_ms / fit_ms, 2)},
+            "mixed": {"ms": round(mixed_ms, 4), "inner_iterations": rep_box["mixed"]["inner_iterations"],
+                      "rel_residual": rep_box["mixed"]["rel_residual"]},
+            "learned_breakdown_ms": {"features": round(t_features, 4), "network": round(t_net, 4),
+                                     "exact_start": round(t_start, 4), "residual": round(t_resid, 4),
+                                     "rows": int(feats.shape[0])},
+            "field_error": field,
+            "e2e": {"value": round(e2e_ms, 4), "unit": "ms", "h2d_bytes_per_step": int(8 * n + V.nbytes + F.nbytes),
                     "d2h_bytes_per_step": 8 * n},
-            "roofline": {"bound": "hbm", "kernel": "kSpmvBinned (%s)" % ("A^T" if dom else "A"),
+            "roofline": {"bound": "hbm", "kernel": "kSpmvBinned (%s), the plain LSCG's dominant kernel"
+                         % ("A^T" if dom else "A"),
                          "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                          "bytes_per_launch": spmv_bytes, "launch_ms": round(spmv[dom], 5), "traffic": None},
             "cpu_baseline": cpu,
             "clocks": clk,
             "gpu_launches": launches,
-            "mixed": {"fit_ms": round(mixed_ms, 4), "inner_iterations": rep_m["rep"]["inner_iterations"],
-                      "rel_residual": rep_m["rep"]["rel_residual"]},
             "mc": {"res": R, "mvox_s": round(mc_mvox, 1), "field_ms": round(field_ms, 3), "mc_ms": round(mc_ms, 3),
-                   "iso": outer, "tri_vertices": int(nv.value)},
+                   "iso": ol, "tri_vertices": int(nv.value)},
+            "batch": batch,
             "svo_build_ms": round(svo_ms, 3),
-            "fit_breakdown_ms": {"assembly": round(asm_ms, 3), "solve": round(solve_ms, 3)},
             "spmv_ms": {"A": round(spmv[0], 5), "AT": round(spmv[1], 5)},
         }
         print(json.dumps(line), flush=True)
+    net.close()
     if pg:
         pg.barrier()
         pg.destroy_process_group()
+
+
+def run_batch(ctx, net, norm, timed, tol, world, rank, steps, max_ranks):
+    """The uneven multi-mesh workload (256 meshes, 2k-200k faces; this rank's LPT share)."""
+    import torch
+    from its_b200 import STOP_RESIDUAL, Operator, Svo, meshes, model_to_unit_cube, uniform_bbox
+    from its_b200.api import fit_residual_batch, learned_start_batch
+    mix = meshes.batch_meshes(256, 3)
+    mine = lpt_shard([m["faces"] for m in mix], world)[rank]
+    svos, bs, mesh_dev, outs = [], [], [], []
+    for k in mine:
+        m = mix[k]
+        V = model_to_unit_cube(m["V"])
+        o, _, w = uniform_bbox(V)
+        s = Svo(ctx, V, m["F"], m["res"], o, w)
+        svos.append(s)
+        bs.append(torch.from_numpy(ctx.signed_distance(s.vertices()[0], V, m["F"])).cuda())
+        mesh_dev.append((torch.from_numpy(V).cuda(), torch.from_numpy(np.ascontiguousarray(m["F"])).cuda()))
+        outs.append(torch.empty_like(bs[-1]))
+    its = []
+
+    def plain():
+        its.clear()
+        for s, b, x in zip(svos, bs, outs):
+            op = Operator(s)
+            _, r = op.solve(b, tol=tol, stop_rule=STOP_RESIDUAL, out=x)
+            its.append(r["iterations"])
+            op.close()
+
+    rel = []
+
+    def learned():
+        learned_start_batch(svos, net, bs, mesh_dev, norm, outs=outs)
+        rel[:] = list(fit_residual_batch(svos, bs, outs))
+
+    plain()
+    plain_ms = max_ranks(timed(plain, max(1, steps - 1)))
+    learned()
+    learned_ms = max_ranks(timed(learned, steps))
+    out = {"workload": "256 meshes, faces log-uniform in [2k, 200k] (seed 3): geodesic spheres / tori / "
+                       "superquadrics, SVO depth 7-9; fit to 1e-6 relative residual",
+           "meshes": len(mine), "unknowns": int(sum(s.num_verts for s in svos)),
+           "plain_fp64_ms": round(plain_ms, 3), "plain_iterations_mean": float(np.mean(its)),
+           "learned_ms": round(learned_ms, 3), "learned_max_rel_residual": float(max(rel)),
+           "speedup": round(plain_ms / learned_ms, 2), "sharding": "LPT by faces" if world > 1 else "single"}
+    for s in svos:
+        s.close()
+    return out
 
 
 def cpu_fit(V, F, o, w, wl, b):
@@ -399,6 +513,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c1", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--no-batch", action="store_true", help="skip the multi-mesh batch leg")
     ap.add_argument("--only", default="all", choices=["all", "fit"], help="fit: time the fit steps only")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
