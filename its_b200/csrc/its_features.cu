@@ -33,7 +33,7 @@ struct NodeStats {
   double* sn;  // 3 per node: sum of unit normals
 };
 
-// Face centroid, unit normal and fine node (kNone when no fine node holds the centroid).
+// Face centroid, unit normal and fine node (fineCount when no fine node holds the centroid).
 __global__ void kFaceSamples(const double* __restrict__ V, const int32_t* __restrict__ F, int64_t nf, double3 g,
                              double w0, int res, const uint32_t* __restrict__ morton, int64_t fineCount,
                              double* __restrict__ cent, double* __restrict__ nrm, uint32_t* __restrict__ node,
@@ -60,7 +60,7 @@ __global__ void kFaceSamples(const double* __restrict__ V, const int32_t* __rest
   nrm[3 * f + 1] = ny;
   nrm[3 * f + 2] = nz;
   ids[f] = (uint32_t)f;
-  uint32_t t = kNone;
+  uint32_t t = (uint32_t)fineCount;  // "no fine node" sorts after every node
   const int dx = (int)((cx - g.x) / w0), dy = (int)((cy - g.y) / w0), dz = (int)((cz - g.z) / w0);
   if (dx >= 0 && dy >= 0 && dz >= 0 && dx < res && dy < res && dz < res) {
     const uint32_t m = mortonEncode((uint32_t)dx, (uint32_t)dy, (uint32_t)dz);
@@ -77,11 +77,12 @@ __global__ void kFaceSamples(const double* __restrict__ V, const int32_t* __rest
 
 // Fine-node sums over the samples sorted by node (each node's run in sample order).
 __global__ void kFineSums(const uint32_t* __restrict__ sortedNode, const uint32_t* __restrict__ sortedId,
-                          int64_t nf, const double* __restrict__ cent, const double* __restrict__ nrm, NodeStats S) {
+                          int64_t nf, int64_t fineCount, const double* __restrict__ cent, const double* __restrict__ nrm,
+                          NodeStats S) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= nf) return;
   const uint32_t t = sortedNode[i];
-  if (t == kNone || (i > 0 && sortedNode[i - 1] == t)) return;  // first sample of the run only
+  if (t >= fineCount || (i > 0 && sortedNode[i - 1] == t)) return;  // first sample of the run only
   float c = 0.0f;
   double p[3] = {0, 0, 0}, q[3] = {0, 0, 0};
   for (int64_t k = i; k < nf && sortedNode[k] == t; ++k) {
@@ -311,10 +312,12 @@ its_status shareFeatures(its_ctx* ctx, const SvoDevice& d, const double* b, cons
                                                          d.unit[0], d.res, d.nodeMorton, fineCount, cent.p, nrm.p,
                                                          node.p, fid.p);
   ITS_LAUNCHED(ctx);
-  // stable sort by fine node (kNone sorts last: 32-bit keys)
-  if ((st = radixSortPairs(ctx, node.p, fid.p, sNode.p, sId.p, tk.p, tv.p, nf, 32)) != ITS_OK) return st;
+  // stable sort by fine node ("none" = fineCount sorts last)
+  int bits = 1;
+  while (bits < 32 && (1ll << bits) <= fineCount) ++bits;
+  if ((st = radixSortPairs(ctx, node.p, fid.p, sNode.p, sId.p, tk.p, tv.p, nf, bits)) != ITS_OK) return st;
   NodeStats S{cnt.p, sp.p, sn.p};
-  kFineSums<<<gridFor(nf, 256), 256, 0, ctx->stream>>>(sNode.p, sId.p, nf, cent.p, nrm.p, S);
+  kFineSums<<<gridFor(nf, 256), 256, 0, ctx->stream>>>(sNode.p, sId.p, nf, fineCount, cent.p, nrm.p, S);
   ITS_LAUNCHED(ctx);
   for (int L = 1; L < d.depth; ++L) {
     if (!d.levelCount[L]) continue;

@@ -151,17 +151,104 @@ __device__ inline double fieldAt(const EvalParams& P, const double* __restrict__
   return sum;
 }
 
-// Field on the (R+1)^3 lattice, x fastest.
-__global__ void __launch_bounds__(256) kEvalGrid(const __grid_constant__ EvalParams P, const double* __restrict__ lambda,
-                                                 double3 o, double3 vs, int R, double* __restrict__ field) {
+// Field on the (R+1)^3 lattice in bricks of 32 x 4 x 2 points (one per thread). For each
+// depth the brick's points fall in a small box of cells; the corners of that box (presence,
+// coefficient, representative position) are staged in shared memory once, and every point
+// then sums its 8 corners from there -- the same additions in the same order as fieldAt, so
+// the result is bit-identical, without the per-point lattice lookups (bitmap, rank, vertex
+// position) that made the point-wise kernel L2-bound. Depths whose corner box exceeds the
+// tile (grids much coarser than the octree) fall back to the point-wise lookups.
+constexpr int kBrickX = 32, kBrickY = 4, kBrickZ = 2, kTileCap = 512;
+
+__global__ void __launch_bounds__(kBrickX* kBrickY* kBrickZ)
+    kEvalGridBricks(const __grid_constant__ EvalParams P, const double* __restrict__ lambda, double3 o, double3 vs,
+                    int R, double* __restrict__ field) {
+  __shared__ double tLam[kTileCap], tPx[kTileCap], tPy[kTileCap], tPz[kTileCap];
+  __shared__ unsigned char tHas[kTileCap];
   const int64_t M = (int64_t)R + 1;
-  const int64_t total = M * M * M;
-  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t xi = idx % M, yj = (idx / M) % M, zk = idx / (M * M);
-    const double px = o.x + (double)xi * vs.x, py = o.y + (double)yj * vs.y, pz = o.z + (double)zk * vs.z;
-    field[idx] = fieldAt(P, lambda, px, py, pz);
+  const int tid = threadIdx.x;
+  const int64_t x0 = (int64_t)blockIdx.x * kBrickX, y0 = (int64_t)blockIdx.y * kBrickY,
+                z0 = (int64_t)blockIdx.z * kBrickZ;
+  const int64_t xi = x0 + (tid % kBrickX), yj = y0 + ((tid / kBrickX) % kBrickY), zk = z0 + tid / (kBrickX * kBrickY);
+  const bool inside = xi < M && yj < M && zk < M;
+  const double px = o.x + (double)xi * vs.x, py = o.y + (double)yj * vs.y, pz = o.z + (double)zk * vs.z;
+  // the brick's extreme points (coordinates computed like every point's)
+  const int64_t x1 = min(x0 + kBrickX - 1, M - 1), y1 = min(y0 + kBrickY - 1, M - 1), z1 = min(z0 + kBrickZ - 1, M - 1);
+  const double ax = o.x + (double)x0 * vs.x, bx = o.x + (double)x1 * vs.x;
+  const double ay = o.y + (double)y0 * vs.y, by = o.y + (double)y1 * vs.y;
+  const double az = o.z + (double)z0 * vs.z, bz = o.z + (double)z1 * vs.z;
+  double sum = 0.0;
+  for (int d = 0; d < P.depth; ++d) {
+    const double w = P.w0 * (double)(1u << d);
+    const LatticeIndex& L = P.lat[d];
+    const int64_t lim = (int64_t)(P.res >> d);
+    const int64_t cx0 = (int64_t)floor((ax - P.g.x) / w), cy0 = (int64_t)floor((ay - P.g.y) / w),
+                  cz0 = (int64_t)floor((az - P.g.z) / w);
+    const int64_t nx = (int64_t)floor((bx - P.g.x) / w) - cx0 + 2, ny = (int64_t)floor((by - P.g.y) / w) - cy0 + 2,
+                  nz = (int64_t)floor((bz - P.g.z) / w) - cz0 + 2;
+    const int64_t cx = (int64_t)floor((px - P.g.x) / w), cy = (int64_t)floor((py - P.g.y) / w),
+                  cz = (int64_t)floor((pz - P.g.z) / w);
+    if (nx * ny * nz > kTileCap) {  // block-uniform: every thread takes this branch together
+      if (inside) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int64_t Lx = cx + (k & 1), Ly = cy + ((k >> 1) & 1), Lz = cz + ((k >> 2) & 1);
+          if (Lx < 0 || Ly < 0 || Lz < 0 || Lx > lim || Ly > lim || Lz > lim) continue;
+          const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
+          if (!latticeHas(L, lin)) continue;
+          const uint32_t v = latticeRank(L, lin);
+          sum += lambda[v] * hat3(P.vertPos[3 * v], P.vertPos[3 * v + 1], P.vertPos[3 * v + 2], w, px, py, pz);
+        }
+      }
+      continue;
+    }
+    for (int64_t t = tid; t < nx * ny * nz; t += kBrickX * kBrickY * kBrickZ) {
+      const int64_t Lx = cx0 + t / (ny * nz), Ly = cy0 + (t / nz) % ny, Lz = cz0 + t % nz;
+      unsigned char has = 0;
+      if (Lx >= 0 && Ly >= 0 && Lz >= 0 && Lx <= lim && Ly <= lim && Lz <= lim) {
+        const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
+        if (latticeHas(L, lin)) {
+          const uint32_t v = latticeRank(L, lin);
+          tLam[t] = lambda[v];
+          tPx[t] = P.vertPos[3 * v];
+          tPy[t] = P.vertPos[3 * v + 1];
+          tPz[t] = P.vertPos[3 * v + 2];
+          has = 1;
+        }
+      }
+      tHas[t] = has;
+    }
+    __syncthreads();
+    if (inside) {
+      // hat3 of each corner as the reference forms it (x, y, z factors with early exits);
+      // a factor is computed once per distinct corner coordinate: the corners sharing an
+      // offset along an axis almost always share the coordinate, and equal inputs give the
+      // same IEEE result, so reusing it changes no bit
+      double cxv[2] = {0.0, 0.0}, cyv[2] = {0.0, 0.0}, czv[2] = {0.0, 0.0};
+      double hxv[2] = {0.0, 0.0}, hyv[2] = {0.0, 0.0}, hzv[2] = {0.0, 0.0};
+      bool okx[2] = {false, false}, oky[2] = {false, false}, okz[2] = {false, false};
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
+        const int64_t t = ((cx - cx0 + ox) * ny + (cy - cy0 + oy)) * nz + (cz - cz0 + oz);
+        if (!tHas[t]) continue;
+        const double qx = tPx[t], qy = tPy[t], qz = tPz[t];
+        double hx, hy, hz;
+        if (okx[ox] && cxv[ox] == qx) hx = hxv[ox];
+        else { hx = hat1(px, qx, w); cxv[ox] = qx; hxv[ox] = hx; okx[ox] = true; }
+        if (hx <= 0.0) continue;
+        if (oky[oy] && cyv[oy] == qy) hy = hyv[oy];
+        else { hy = hat1(py, qy, w); cyv[oy] = qy; hyv[oy] = hy; oky[oy] = true; }
+        if (hy <= 0.0) continue;
+        if (okz[oz] && czv[oz] == qz) hz = hzv[oz];
+        else { hz = hat1(pz, qz, w); czv[oz] = qz; hzv[oz] = hz; okz[oz] = true; }
+        if (hz <= 0.0) continue;
+        sum += tLam[t] * (hx * hy * hz);
+      }
+    }
+    __syncthreads();
   }
+  if (inside) field[xi + M * (yj + M * zk)] = sum;
 }
 
 // Point queries (ThinShells::multiPointQuery, ThinShells.cpp:1183-1420, CUDA branch
@@ -290,8 +377,10 @@ its_status its_eval_grid(its_svo* s, const double* lambda, const double origin[3
   if ((st = F.stage(ctx, field, total)) != ITS_OK) return st;
   const double3 o = make_double3(origin[0], origin[1], origin[2]);
   const double3 vs = make_double3(width[0] / res, width[1] / res, width[2] / res);
-  const unsigned blocks = (unsigned)std::min<int64_t>(gridFor(total, 256), (int64_t)ctx->numSMs * 64);
-  kEvalGrid<<<blocks, 256, 0, ctx->stream>>>(evalParams(s->d), L.d, o, vs, res, F.d);
+  (void)total;
+  const dim3 grid((unsigned)((M + kBrickX - 1) / kBrickX), (unsigned)((M + kBrickY - 1) / kBrickY),
+                  (unsigned)((M + kBrickZ - 1) / kBrickZ));
+  kEvalGridBricks<<<grid, kBrickX * kBrickY * kBrickZ, 0, ctx->stream>>>(evalParams(s->d), L.d, o, vs, res, F.d);
   ITS_LAUNCHED(ctx);
   if ((st = F.finish(ctx)) != ITS_OK) return st;
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
