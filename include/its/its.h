@@ -56,6 +56,10 @@ its_status its_synchronize(its_ctx* ctx);
 const char* its_version(void);
 /* Number of kernels this context has launched so far (a diagnostic counter). */
 int64_t its_kernel_launches(const its_ctx* ctx);
+/* Self-check of the division the field kernels use (a multiply and two FMAs from the
+   correctly rounded reciprocal, Markstein's theorem): counts the pairs whose quotient differs
+   from the GPU's correctly rounded a[i] / b[i]. No counterpart in the reference. */
+its_status its_check_division(its_ctx* ctx, const double* a, const double* b, int64_t n, int64_t* mismatches);
 
 /* ---- a1-a2: model pre-processing (host) ----------------------------------------------- */
 /* BaseModel::model2UnitCube / calcUnitCubeTransformMatrix (src/BaseModel.cpp:54-92). */

@@ -41,6 +41,7 @@ SIGNATURES = {
     "its_synchronize": (st, [vp]),
     "its_version": (C.c_char_p, []),
     "its_kernel_launches": (i64, [vp]),
+    "its_check_division": (st, [vp, vp, vp, i64, C.POINTER(i64)]),
     "its_model_to_unit_cube": (st, [vp, i64, dbl]),
     "its_uniform_bbox": (st, [vp, i64, vp, vp, vp]),
     "its_tri_attributes": (st, [vp, vp, i64, vp, i64, vp, vp, vp]),

@@ -14,6 +14,7 @@
 //   counts, and the triangle soup written in voxel order by the scan's own downsweep (no
 //   compaction pass, no 18 R^3 preallocation).
 #include <cfloat>
+#include <vector>
 
 #include "its_mc.cuh"
 #include "its_op.cuh"
@@ -29,6 +30,7 @@ struct EvalParams {
   const uint32_t* morton;
   const uint32_t* parent;
   const double* vertPos;
+  double winv[kMaxDepth];  // RN(1 / w_d), for divRn
 };
 
 static EvalParams evalParams(const SvoDevice& d) {
@@ -42,6 +44,7 @@ static EvalParams evalParams(const SvoDevice& d) {
   P.morton = d.nodeMorton;
   P.parent = d.nodeParent;
   P.vertPos = d.vertPos;
+  for (int L = 0; L < kMaxDepth; ++L) P.winv[L] = 1.0 / (P.w0 * (double)(1u << L));
   return P;
 }
 
@@ -158,97 +161,147 @@ __device__ inline double fieldAt(const EvalParams& P, const double* __restrict__
 // the result is bit-identical, without the per-point lattice lookups (bitmap, rank, vertex
 // position) that made the point-wise kernel L2-bound. Depths whose corner box exceeds the
 // tile (grids much coarser than the octree) fall back to the point-wise lookups.
-constexpr int kBrickX = 32, kBrickY = 4, kBrickZ = 2, kTileCap = 512;
+constexpr int kBrickX = 32, kBrickY = 4, kBrickThreads = 256, kZPer = 4;
+constexpr int kBrickZ = (kBrickThreads / (kBrickX * kBrickY)) * kZPer;  // 8
+constexpr int kTileCap = 640;
 
-__global__ void __launch_bounds__(kBrickX* kBrickY* kBrickZ)
+// Field on the (R+1)^3 lattice in bricks of 32 x 4 x 8 points; a thread evaluates a column of
+// 4 points along z. For each depth the brick's points fall in a small box of cells; the
+// corners of that box (presence, coefficient, representative position) are staged in shared
+// memory once, and every point then sums its 8 corners from there -- the same additions in
+// the same order as fieldAt, so the result is bit-identical, without per-point lattice
+// lookups. The x and y hat factors of a corner are shared by the thread's 4 points (equal
+// inputs, equal IEEE results); all quotients use divRn. Depths whose corner box has no
+// corner are skipped; depths whose box exceeds the tile (grids much coarser than the octree)
+// fall back to per-point lookups.
+__global__ void __launch_bounds__(kBrickThreads, 2)
     kEvalGridBricks(const __grid_constant__ EvalParams P, const double* __restrict__ lambda, double3 o, double3 vs,
                     int R, double* __restrict__ field) {
   __shared__ double tLam[kTileCap], tPx[kTileCap], tPy[kTileCap], tPz[kTileCap];
   __shared__ unsigned char tHas[kTileCap];
+  __shared__ int64_t box[6];  // first and last cell per axis at the current depth
   const int64_t M = (int64_t)R + 1;
   const int tid = threadIdx.x;
   const int64_t x0 = (int64_t)blockIdx.x * kBrickX, y0 = (int64_t)blockIdx.y * kBrickY,
                 z0 = (int64_t)blockIdx.z * kBrickZ;
-  const int64_t xi = x0 + (tid % kBrickX), yj = y0 + ((tid / kBrickX) % kBrickY), zk = z0 + tid / (kBrickX * kBrickY);
-  const bool inside = xi < M && yj < M && zk < M;
-  const double px = o.x + (double)xi * vs.x, py = o.y + (double)yj * vs.y, pz = o.z + (double)zk * vs.z;
-  // the brick's extreme points (coordinates computed like every point's)
-  const int64_t x1 = min(x0 + kBrickX - 1, M - 1), y1 = min(y0 + kBrickY - 1, M - 1), z1 = min(z0 + kBrickZ - 1, M - 1);
-  const double ax = o.x + (double)x0 * vs.x, bx = o.x + (double)x1 * vs.x;
-  const double ay = o.y + (double)y0 * vs.y, by = o.y + (double)y1 * vs.y;
-  const double az = o.z + (double)z0 * vs.z, bz = o.z + (double)z1 * vs.z;
-  double sum = 0.0;
+  const int64_t xi = x0 + (tid % kBrickX), yj = y0 + ((tid / kBrickX) % kBrickY);
+  const int64_t zb = z0 + (int64_t)(tid / (kBrickX * kBrickY)) * kZPer;
+  const bool inXY = xi < M && yj < M;
+  const double px = o.x + (double)xi * vs.x, py = o.y + (double)yj * vs.y;
+  double pz[kZPer], sum[kZPer];
+#pragma unroll
+  for (int q = 0; q < kZPer; ++q) {
+    pz[q] = o.z + (double)(zb + q) * vs.z;
+    sum[q] = 0.0;
+  }
   for (int d = 0; d < P.depth; ++d) {
-    const double w = P.w0 * (double)(1u << d);
+    const double w = P.w0 * (double)(1u << d), wi = P.winv[d];
     const LatticeIndex& L = P.lat[d];
     const int64_t lim = (int64_t)(P.res >> d);
-    const int64_t cx0 = (int64_t)floor((ax - P.g.x) / w), cy0 = (int64_t)floor((ay - P.g.y) / w),
-                  cz0 = (int64_t)floor((az - P.g.z) / w);
-    const int64_t nx = (int64_t)floor((bx - P.g.x) / w) - cx0 + 2, ny = (int64_t)floor((by - P.g.y) / w) - cy0 + 2,
-                  nz = (int64_t)floor((bz - P.g.z) / w) - cz0 + 2;
-    const int64_t cx = (int64_t)floor((px - P.g.x) / w), cy = (int64_t)floor((py - P.g.y) / w),
-                  cz = (int64_t)floor((pz - P.g.z) / w);
-    if (nx * ny * nz > kTileCap) {  // block-uniform: every thread takes this branch together
-      if (inside) {
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          const int64_t Lx = cx + (k & 1), Ly = cy + ((k >> 1) & 1), Lz = cz + ((k >> 2) & 1);
-          if (Lx < 0 || Ly < 0 || Lz < 0 || Lx > lim || Ly > lim || Lz > lim) continue;
-          const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
-          if (!latticeHas(L, lin)) continue;
-          const uint32_t v = latticeRank(L, lin);
-          sum += lambda[v] * hat3(P.vertPos[3 * v], P.vertPos[3 * v + 1], P.vertPos[3 * v + 2], w, px, py, pz);
-        }
-      }
-      continue;
-    }
-    for (int64_t t = tid; t < nx * ny * nz; t += kBrickX * kBrickY * kBrickZ) {
-      const int64_t Lx = cx0 + t / (ny * nz), Ly = cy0 + (t / nz) % ny, Lz = cz0 + t % nz;
-      unsigned char has = 0;
-      if (Lx >= 0 && Ly >= 0 && Lz >= 0 && Lx <= lim && Ly <= lim && Lz <= lim) {
-        const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
-        if (latticeHas(L, lin)) {
-          const uint32_t v = latticeRank(L, lin);
-          tLam[t] = lambda[v];
-          tPx[t] = P.vertPos[3 * v];
-          tPy[t] = P.vertPos[3 * v + 1];
-          tPz[t] = P.vertPos[3 * v + 2];
-          has = 1;
-        }
-      }
-      tHas[t] = has;
+    if (tid < 6) {
+      const int a = tid >> 1;
+      const int64_t idx = (a == 0 ? x0 : a == 1 ? y0 : z0) +
+                          ((tid & 1) ? (a == 0 ? kBrickX : a == 1 ? kBrickY : kBrickZ) - 1 : 0);
+      const int64_t cl = idx < M ? idx : M - 1;
+      const double oa = a == 0 ? o.x : a == 1 ? o.y : o.z, va = a == 0 ? vs.x : a == 1 ? vs.y : vs.z;
+      const double ga = a == 0 ? P.g.x : a == 1 ? P.g.y : P.g.z;
+      box[tid] = (int64_t)floor(divRn((oa + (double)cl * va) - ga, w, wi));
     }
     __syncthreads();
-    if (inside) {
-      // hat3 of each corner as the reference forms it (x, y, z factors with early exits);
-      // a factor is computed once per distinct corner coordinate: the corners sharing an
-      // offset along an axis almost always share the coordinate, and equal inputs give the
-      // same IEEE result, so reusing it changes no bit
-      double cxv[2] = {0.0, 0.0}, cyv[2] = {0.0, 0.0}, czv[2] = {0.0, 0.0};
-      double hxv[2] = {0.0, 0.0}, hyv[2] = {0.0, 0.0}, hzv[2] = {0.0, 0.0};
-      bool okx[2] = {false, false}, oky[2] = {false, false}, okz[2] = {false, false};
+    const int64_t cx0 = box[0], cy0 = box[2], cz0 = box[4];
+    const int nx = (int)(box[1] - cx0 + 2), ny = (int)(box[3] - cy0 + 2), nz = (int)(box[5] - cz0 + 2);
+    const bool tiled = (int64_t)nx * ny * nz <= kTileCap;  // block-uniform
+    int any = 1;
+    if (tiled) {
+      int mine = 0;
+      for (int t = tid; t < nx * ny * nz; t += kBrickThreads) {
+        const int64_t Lx = cx0 + t / (ny * nz), Ly = cy0 + (t / nz) % ny, Lz = cz0 + t % nz;
+        unsigned char has = 0;
+        if (Lx >= 0 && Ly >= 0 && Lz >= 0 && Lx <= lim && Ly <= lim && Lz <= lim) {
+          const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
+          if (latticeHas(L, lin)) {
+            const uint32_t v = latticeRank(L, lin);
+            tLam[t] = lambda[v];
+            tPx[t] = P.vertPos[3 * v];
+            tPy[t] = P.vertPos[3 * v + 1];
+            tPz[t] = P.vertPos[3 * v + 2];
+            has = 1;
+          }
+        }
+        tHas[t] = has;
+        mine |= has;
+      }
+      any = __syncthreads_or(mine);
+    } else {
+      __syncthreads();
+    }
+    if (any && inXY) {
+      const int64_t cx = (int64_t)floor(divRn(px - P.g.x, w, wi)), cy = (int64_t)floor(divRn(py - P.g.y, w, wi));
+      // x / y hat factors per distinct corner coordinate, shared by the column's points
+      double cxv[2] = {0.0, 0.0}, cyv[2] = {0.0, 0.0}, hxv[2] = {0.0, 0.0}, hyv[2] = {0.0, 0.0};
+      bool okx[2] = {false, false}, oky[2] = {false, false};
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
-        const int64_t t = ((cx - cx0 + ox) * ny + (cy - cy0 + oy)) * nz + (cz - cz0 + oz);
-        if (!tHas[t]) continue;
-        const double qx = tPx[t], qy = tPy[t], qz = tPz[t];
-        double hx, hy, hz;
-        if (okx[ox] && cxv[ox] == qx) hx = hxv[ox];
-        else { hx = hat1(px, qx, w); cxv[ox] = qx; hxv[ox] = hx; okx[ox] = true; }
-        if (hx <= 0.0) continue;
-        if (oky[oy] && cyv[oy] == qy) hy = hyv[oy];
-        else { hy = hat1(py, qy, w); cyv[oy] = qy; hyv[oy] = hy; oky[oy] = true; }
-        if (hy <= 0.0) continue;
-        if (okz[oz] && czv[oz] == qz) hz = hzv[oz];
-        else { hz = hat1(pz, qz, w); czv[oz] = qz; hzv[oz] = hz; okz[oz] = true; }
-        if (hz <= 0.0) continue;
-        sum += tLam[t] * (hx * hy * hz);
+      for (int q = 0; q < kZPer; ++q) {
+        if (zb + q >= M) break;
+        const double pzq = pz[q];
+        const int64_t cz = (int64_t)floor(divRn(pzq - P.g.z, w, wi));
+        double czv[2] = {0.0, 0.0}, hzv[2] = {0.0, 0.0};
+        bool okz[2] = {false, false};
+        double s = sum[q];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
+          double lam, qx, qy, qz;
+          if (tiled) {
+            const int t = ((int)(cx - cx0) + ox) * ny * nz + ((int)(cy - cy0) + oy) * nz + ((int)(cz - cz0) + oz);
+            if (!tHas[t]) continue;
+            lam = tLam[t];
+            qx = tPx[t];
+            qy = tPy[t];
+            qz = tPz[t];
+          } else {
+            const int64_t Lx = cx + ox, Ly = cy + oy, Lz = cz + oz;
+            if (Lx < 0 || Ly < 0 || Lz < 0 || Lx > lim || Ly > lim || Lz > lim) continue;
+            const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
+            if (!latticeHas(L, lin)) continue;
+            const uint32_t v = latticeRank(L, lin);
+            lam = lambda[v];
+            qx = P.vertPos[3 * v];
+            qy = P.vertPos[3 * v + 1];
+            qz = P.vertPos[3 * v + 2];
+          }
+          double hx, hy, hz;
+          if (okx[ox] && cxv[ox] == qx) hx = hxv[ox];
+          else { hx = hat1r(px, qx, w, wi); cxv[ox] = qx; hxv[ox] = hx; okx[ox] = true; }
+          if (hx <= 0.0) continue;
+          if (oky[oy] && cyv[oy] == qy) hy = hyv[oy];
+          else { hy = hat1r(py, qy, w, wi); cyv[oy] = qy; hyv[oy] = hy; oky[oy] = true; }
+          if (hy <= 0.0) continue;
+          if (okz[oz] && czv[oz] == qz) hz = hzv[oz];
+          else { hz = hat1r(pzq, qz, w, wi); czv[oz] = qz; hzv[oz] = hz; okz[oz] = true; }
+          if (hz <= 0.0) continue;
+          s += lam * (hx * hy * hz);
+        }
+        sum[q] = s;
       }
     }
     __syncthreads();
   }
-  if (inside) field[xi + M * (yj + M * zk)] = sum;
+  if (inXY) {
+#pragma unroll
+    for (int q = 0; q < kZPer; ++q)
+      if (zb + q < M) field[xi + M * (yj + M * (zb + q))] = sum[q];
+  }
+}
+
+// divRn against the hardware-correct quotient (a test hook: out[i] = 1 where they differ).
+__global__ void kCheckDivRn(const double* __restrict__ a, const double* __restrict__ b, int64_t n,
+                            unsigned char* __restrict__ differ) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double y = 1.0 / b[i];
+  const double q1 = divRn(a[i], b[i], y), q2 = a[i] / b[i];
+  differ[i] = __double_as_longlong(q1) != __double_as_longlong(q2);
 }
 
 // Point queries (ThinShells::multiPointQuery, ThinShells.cpp:1183-1420, CUDA branch
@@ -380,10 +433,31 @@ its_status its_eval_grid(its_svo* s, const double* lambda, const double origin[3
   (void)total;
   const dim3 grid((unsigned)((M + kBrickX - 1) / kBrickX), (unsigned)((M + kBrickY - 1) / kBrickY),
                   (unsigned)((M + kBrickZ - 1) / kBrickZ));
-  kEvalGridBricks<<<grid, kBrickX * kBrickY * kBrickZ, 0, ctx->stream>>>(evalParams(s->d), L.d, o, vs, res, F.d);
+  kEvalGridBricks<<<grid, kBrickThreads, 0, ctx->stream>>>(evalParams(s->d), L.d, o, vs, res, F.d);
   ITS_LAUNCHED(ctx);
   if ((st = F.finish(ctx)) != ITS_OK) return st;
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITS_OK;
+}
+
+// Counts the pairs (a[i], b[i]) whose quotient by divRn differs from a[i] / b[i] (device or
+// host arrays). A self-check of the division the field kernels use.
+its_status its_check_division(its_ctx* ctx, const double* a, const double* b, int64_t n, int64_t* mismatches) {
+  if (!ctx || !a || !b || n <= 0 || !mismatches) return ITS_ERR_INVALID;
+  ITS_CU(ctx, cudaSetDevice(ctx->device));
+  InArg<double> A, B;
+  its_status st;
+  if ((st = A.stage(ctx, a, n)) != ITS_OK || (st = B.stage(ctx, b, n)) != ITS_OK) return st;
+  DevBuf<unsigned char> diff;
+  if ((st = diff.alloc(ctx, n)) != ITS_OK) return st;
+  kCheckDivRn<<<gridFor(n, 256), 256, 0, ctx->stream>>>(A.d, B.d, n, diff.p);
+  ITS_LAUNCHED(ctx);
+  std::vector<unsigned char> h(n);
+  ITS_CU(ctx, cudaMemcpyAsync(h.data(), diff.p, n, cudaMemcpyDeviceToHost, ctx->stream));
+  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  int64_t c = 0;
+  for (int64_t i = 0; i < n; ++i) c += h[i];
+  *mismatches = c;
   return ITS_OK;
 }
 

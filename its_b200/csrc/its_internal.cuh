@@ -57,6 +57,22 @@ __host__ __device__ inline double hat1(double x, double p, double w) {
   if (x <= p) return 1 + (x - p) / w;
   return 1 - (x - p) / w;
 }
+// Correctly rounded quotient a / b from y = RN(1 / b) (Markstein's theorem: with y the
+// correctly rounded reciprocal and q = RN(a y) within one ulp of a / b, the exact remainder
+// r = a - q b (one FMA) gives RN(a / b) = RN(q + r y)). Valid without overflow or underflow,
+// which the octree's coordinates (|a|, |b| in [1e-300, 1e300]) never approach. Bit-identical
+// to a / b; a multiply and two FMAs instead of a division.
+__device__ __forceinline__ double divRn(double a, double b, double y) {
+  const double q = a * y;
+  const double r = fma(-q, b, a);
+  return fma(r, y, q);
+}
+// hat1 with the quotient formed by divRn (same result bit for bit).
+__device__ __forceinline__ double hat1r(double x, double p, double w, double winv) {
+  if (fabs(x - (p - w)) < 1e-9 || x < p - w || fabs(x - (p + w)) < 1e-9 || x > p + w) return 0.0;
+  if (x <= p) return 1 + divRn(x - p, w, winv);
+  return 1 - divRn(x - p, w, winv);
+}
 __host__ __device__ inline double hat3(double px, double py, double pz, double w, double qx, double qy,
                                        double qz) {
   const double x = hat1(qx, px, w);

@@ -17,13 +17,30 @@ __device__ __constant__ int8_t cMcEdge[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0},
                                                {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
 
 // Per-voxel vertex count (the scan's input): 8 corners of the (R+1)^3 lattice field, x fastest.
+// Voxel v = x + R (y + R z) to its coordinates: 32-bit division while R^3 < 2^32 (R <= 1625),
+// 64-bit beyond (64-bit division costs several times more and dominated the scan).
+__device__ __forceinline__ void voxelXYZ(int64_t v, int R, int64_t& x, int64_t& y, int64_t& z) {
+  if ((uint64_t)R * R * R <= 0xFFFFFFFFull) {
+    const uint32_t u = (uint32_t)v, r = (uint32_t)R;
+    const uint32_t q = u / r;
+    x = u - q * r;
+    y = q % r;
+    z = q / r;
+  } else {
+    x = v % R;
+    y = (v / R) % R;
+    z = v / ((int64_t)R * R);
+  }
+}
+
 struct McCase {
   const double* field;
   int R;
   double iso;
   __device__ unsigned cube(int64_t v) const {
     const int64_t M = (int64_t)R + 1;
-    const int64_t x = v % R, y = (v / R) % R, z = v / ((int64_t)R * R);
+    int64_t x, y, z;
+    voxelXYZ(v, R, x, y, z);
     unsigned ci = 0;
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
@@ -57,7 +74,8 @@ struct McEmit {
     if (!count || !tri) return;
     const int R = mc.R;
     const int64_t M = (int64_t)R + 1;
-    const int64_t x = v % R, y = (v / R) % R, z = v / ((int64_t)R * R);
+    int64_t x, y, z;
+    voxelXYZ(v, R, x, y, z);
     const double vp[3] = {(double)x * vs.x + o.x, (double)y * vs.y + o.y, (double)z * vs.z + o.z};
     const double vsz[3] = {vs.x, vs.y, vs.z};
     double corner[8][3], sdf[8];

@@ -67,7 +67,8 @@ struct MeshTris {
     if (!count || !tris) return;
     const int R = mc.R;
     const int64_t M = (int64_t)R + 1;
-    const int64_t x = v % R, y = (v / R) % R, z = v / ((int64_t)R * R);
+    int64_t x, y, z;
+    voxelXYZ(v, R, x, y, z);
     const uint64_t cw = cMcCase[mc.cube(v)];
     for (unsigned t = 0; t < (unsigned)count; ++t) {
       if (offset + t >= capacity) break;

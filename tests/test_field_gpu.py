@@ -120,3 +120,26 @@ def test_marching_cubes_bit_exact(ctx, fitted, R):
         assert n_g == n_r and n_g > 0
         assert np.array_equal(cube_g, cube_r)
         assert np.array_equal(tri_g, tri_r)
+
+
+@pytest.mark.gpu
+def test_fast_division_is_correctly_rounded(ctx):
+    # The field kernels divide by the cell width through RN(1/w) and two FMAs (Markstein);
+    # the quotients must equal the GPU's correctly rounded division bit for bit.
+    import ctypes as C
+    from its_b200 import lib
+    rng = np.random.default_rng(0)
+    n = 1 << 22
+    a = rng.standard_normal(n) * np.exp(rng.uniform(-30, 30, n))
+    b = rng.standard_normal(n) * np.exp(rng.uniform(-30, 30, n))
+    # the kernels' own operands: offsets within two cells of widths w0 * 2^d
+    w = (1.18 / 256) * 2.0 ** rng.integers(0, 10, n)
+    a2 = rng.uniform(-2, 2, n) * w
+    # and exact multiples / neighbours of them, the ties of a floor
+    k = rng.integers(-600, 600, n).astype(np.float64)
+    a3 = np.nextafter(k * w, k * w + rng.choice([-1.0, 1.0], n))
+    for x, y in ((a, b), (a2, w), (a3, w), (k * w, w)):
+        miss = C.c_int64(-1)
+        ctx.check(lib().its_check_division(ctx.h, x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p), n,
+                                           C.byref(miss)), "its_check_division")
+        assert miss.value == 0
