@@ -41,6 +41,10 @@ WORKLOADS = {
                desc="(3,5) torus-knot tube r=0.08, 4096 rings x 128 segments = 1,048,576 faces, FP32 vertices "
                     "+ N(0,1e-3) jitter (seed 1); SVO depth 9 (256^3); FP64 LSCG to 1e-6 relative residual; "
                     "MC 512^3"),
+    "c2": dict(mesh="c2", res=512, tol=1e-6, mc_res=1024, precision=True,
+               desc="perturbed geodesic sphere subdivided 9 times, 2,621,440 faces, amplitude 0.15 (seed 2); SVO "
+                    "depth 10 (512^3); fit to 1e-6 relative residual; mixed precision (FP32 SpMV, FP64 dots and "
+                    "residual, 3 refinement steps) with its error against FP64; FP32 field at 1024^3 in bricks"),
     "c0": dict(mesh="c0", res=32, tol=1e-6, mc_res=128,
                desc="perturbed geodesic sphere, 10,240 faces (seed 0); SVO depth 6 (32^3); FP64 LSCG to 1e-6 "
                     "relative residual; MC 128^3"),
@@ -228,10 +232,12 @@ def run_ours(args):
         rep_box["plain"], rep_box["nnz"] = r, op.nnz
         op.close()
 
+    lam_mixed = torch.empty_like(b_dev)
+
     def mixed_step():
         op = Operator(svo, mode=OP_FP32_VALUES)
         _, r = op.solve(b_dev, tol=wl["tol"], stop_rule=STOP_RESIDUAL, precision=PREC_MIXED, ir_steps=3,
-                        inner_tol=1e-3, out=lam_dev)
+                        inner_tol=1e-3, out=lam_mixed)
         rep_box["mixed"] = r
         op.close()
 
@@ -240,6 +246,7 @@ def run_ours(args):
     plain_ms = max_ranks(timed(plain_step, args.steps))
     mixed_step()
     mixed_ms = max_ranks(timed(mixed_step, max(1, args.steps // 2)))
+    rep_box["mixed_x"] = lam_mixed.cpu().numpy()
     clk = clocks.stop()
     nnz = rep_box["nnz"]
     if args.only == "fit":
@@ -254,7 +261,9 @@ def run_ours(args):
     # ---- breakdown of the learned fit ----------------------------------------------------
     from its_b200.api import exact_start_batch
     feats, ids = svo.share_features(b, V, F, norm[:128])
-    t_features = timed(lambda: svo.share_features(b_dev, V_dev, F_dev, norm[:128]), 3)
+    feat_dev = torch.empty((feats.shape[0], 64), dtype=torch.float32, device="cuda")
+    ids_dev = torch.empty(feats.shape[0], dtype=torch.int64, device="cuda")
+    t_features = timed(lambda: svo.share_features(b_dev, V_dev, F_dev, norm[:128], out=feat_dev, ids=ids_dev), 3)
     t_start = timed(lambda: exact_start_batch([svo], [b_dev], outs=[lam_dev]), 5)
     t_resid = timed(lambda: fit_residual_batch([svo], [b_dev], [lam_dev]), 5)
     feats_dev = torch.from_numpy(feats).cuda()
@@ -357,6 +366,33 @@ def run_ours(args):
     field_ms = timed(field_step, 2)
     mc_ms = timed(mc_step, 3)
     mc_mvox = R ** 3 / ((field_ms + mc_ms) * 1e-3) / 1e6
+    mc_verts = int(nv.value)
+
+    # ---- FP32 field + marching cubes (the precision mode) ------------------------------------
+    field32 = torch.empty(M ** 3, dtype=torch.float32, device="cuda")
+
+    def field32_step():
+        svo.eval_grid_f32(lam_fit, o, w, R, out=field32)
+
+    def mc32_step():
+        st = L.its_marching_cubes_f32(ctx.h, C.c_void_p(field32.data_ptr()), R, o_np.ctypes.data_as(C.c_void_p),
+                                      w_np.ctypes.data_as(C.c_void_p), float(ol), C.c_void_p(cube.data_ptr()), None,
+                                      0, C.byref(nv))
+        ctx.check(st, "its_marching_cubes_f32")
+
+    field32_step()
+    mc32_step()
+    field32_ms = timed(field32_step, 2)
+    mc32_ms = timed(mc32_step, 3)
+    f32_err = float((field32.double() - fieldbuf).abs().max().item()) / scale
+    mc32 = {"res": R, "mvox_s": round(R ** 3 / ((field32_ms + mc32_ms) * 1e-3) / 1e6, 1),
+            "field_ms": round(field32_ms, 3), "mc_ms": round(mc32_ms, 3), "tri_vertices": int(nv.value),
+            "field_max_err_vs_fp64": f32_err}
+    del field32
+
+    precision = None
+    if wl.get("precision"):
+        precision = run_precision(svo, b, x_ref, rep_box["mixed_x"], samples, o, w, scale, timed)
 
     # ---- the uneven multi-mesh batch: plain per-mesh FP64 LSCG vs one learned batch ---------
     batch = None
@@ -398,7 +434,9 @@ def run_ours(args):
             "clocks": clk,
             "gpu_launches": launches,
             "mc": {"res": R, "mvox_s": round(mc_mvox, 1), "field_ms": round(field_ms, 3), "mc_ms": round(mc_ms, 3),
-                   "iso": ol, "tri_vertices": int(nv.value)},
+                   "iso": ol, "tri_vertices": mc_verts, "field": "FP64, bit-exact with the oracle"},
+            "mc_f32": mc32,
+            "precision": precision,
             "batch": batch,
             "svo_build_ms": round(svo_ms, 3),
             "spmv_ms": {"A": round(spmv[0], 5), "AT": round(spmv[1], 5)},
@@ -410,6 +448,40 @@ def run_ours(args):
         pg.destroy_process_group()
 
 
+def run_precision(svo, b, x_ref, x_mixed, samples, o, w, scale, timed):
+    """Error of the mixed-precision fit and of the FP32 field against FP64."""
+    import torch
+    out = {"reference": "FP64 LSCG from zero to 1e-12 relative residual, FP64 field"}
+    lam_scale = float(np.abs(x_ref).max())
+    d = x_mixed - x_ref
+    out["coef_max"] = float(np.abs(d).max() / lam_scale)
+    out["coef_rms"] = float(np.sqrt(np.mean(d * d)) / lam_scale)
+    e = svo.eval_points(x_mixed, samples)[0] - svo.eval_points(x_ref, samples)[0]
+    out["samples_max"] = float(np.abs(e).max() / scale)
+    out["samples_rms"] = float(np.sqrt(np.mean(e * e)) / scale)
+    # the FP32 field of the mixed fit at 1024^3 (bricked kernel) against the FP64 field of the
+    # FP64 fit, compared slab by slab on the device
+    G = 1024
+    M = G + 1
+    f32 = torch.empty(M ** 3, dtype=torch.float32, device="cuda")
+    lam_m = torch.from_numpy(x_mixed).cuda()
+    svo.eval_grid_f32(lam_m, o, w, G, out=f32)
+    out["field32_ms_1024"] = round(timed(lambda: svo.eval_grid_f32(lam_m, o, w, G, out=f32), 1), 3)
+    f64 = torch.empty(M ** 3, dtype=torch.float64, device="cuda")
+    svo.eval_grid(torch.from_numpy(x_ref).cuda(), o, w, G, out=f64)
+    mx, ss = 0.0, 0.0
+    step = M * M * 64
+    for k in range(0, M ** 3, step):
+        dd = f32[k:k + step].double() - f64[k:k + step]
+        mx = max(mx, float(dd.abs().max().item()))
+        ss += float((dd * dd).sum().item())
+    out["field1024_max"] = mx / scale
+    out["field1024_rms"] = float(np.sqrt(ss / M ** 3)) / scale
+    out["scale"] = "coefficients: max |lambda_FP64|; field: max |b|"
+    del f32, f64
+    return out
+
+
 def run_batch(ctx, net, norm, timed, tol, world, rank, steps, max_ranks):
     """The uneven multi-mesh workload (256 meshes, 2k-200k faces; this rank's LPT share)."""
     import torch
@@ -417,12 +489,13 @@ def run_batch(ctx, net, norm, timed, tol, world, rank, steps, max_ranks):
     from its_b200.api import fit_residual_batch, learned_start_batch
     mix = meshes.batch_meshes(256, 3)
     mine = lpt_shard([m["faces"] for m in mix], world)[rank]
-    svos, bs, mesh_dev, outs = [], [], [], []
+    svos, bs, mesh_dev, outs, boxes = [], [], [], [], []
     for k in mine:
         m = mix[k]
         V = model_to_unit_cube(m["V"])
         o, _, w = uniform_bbox(V)
         s = Svo(ctx, V, m["F"], m["res"], o, w)
+        boxes.append((np.ascontiguousarray(o), np.ascontiguousarray(w)))
         svos.append(s)
         bs.append(torch.from_numpy(ctx.signed_distance(s.vertices()[0], V, m["F"])).cuda())
         mesh_dev.append((torch.from_numpy(V).cuda(), torch.from_numpy(np.ascontiguousarray(m["F"])).cuda()))
@@ -447,12 +520,33 @@ def run_batch(ctx, net, norm, timed, tol, world, rank, steps, max_ranks):
     plain_ms = max_ranks(timed(plain, max(1, steps - 1)))
     learned()
     learned_ms = max_ranks(timed(learned, steps))
+    # marching cubes at 256^3 per mesh (zero level set of the learned fit; FP64 field)
+    import ctypes as C
+    from its_b200 import lib
+    R = 256
+    fld = torch.empty((R + 1) ** 3, dtype=torch.float64, device="cuda")
+    cube = torch.empty(R ** 3, dtype=torch.uint8, device="cuda")
+    nv = C.c_int64(0)
+    tris = []
+
+    def mc_all():
+        tris.clear()
+        for s, x, (o, w) in zip(svos, outs, boxes):
+            s.eval_grid(x, o, w, R, out=fld)
+            ctx.check(lib().its_marching_cubes(ctx.h, C.c_void_p(fld.data_ptr()), R, o.ctypes.data_as(C.c_void_p),
+                                               w.ctypes.data_as(C.c_void_p), 0.0, C.c_void_p(cube.data_ptr()), None, 0,
+                                               C.byref(nv)), "its_marching_cubes")
+            tris.append(nv.value // 3)
+
+    mc_ms = max_ranks(timed(mc_all, 1))
     out = {"workload": "256 meshes, faces log-uniform in [2k, 200k] (seed 3): geodesic spheres / tori / "
                        "superquadrics, SVO depth 7-9; fit to 1e-6 relative residual",
            "meshes": len(mine), "unknowns": int(sum(s.num_verts for s in svos)),
            "plain_fp64_ms": round(plain_ms, 3), "plain_iterations_mean": float(np.mean(its)),
            "learned_ms": round(learned_ms, 3), "learned_max_rel_residual": float(max(rel)),
-           "speedup": round(plain_ms / learned_ms, 2), "sharding": "LPT by faces" if world > 1 else "single"}
+           "speedup": round(plain_ms / learned_ms, 2), "sharding": "LPT by faces" if world > 1 else "single",
+           "mc_256": {"ms": round(mc_ms, 2), "mvox_s": round(len(svos) * R ** 3 / (mc_ms * 1e-3) / 1e6, 1),
+                      "triangles": int(sum(tris)), "iso": 0.0, "field": "FP64"}}
     for s in svos:
         s.close()
     return out

@@ -238,6 +238,15 @@ its_status its_marching_cubes(its_ctx* ctx, const double* field, int res, const 
 its_status its_marching_cubes_mesh(its_ctx* ctx, const double* field, int res, const double origin[3],
                                    const double width[3], double iso, double* verts, int64_t vert_capacity,
                                    int64_t* num_verts, int32_t* tris, int64_t tri_capacity, int64_t* num_tris);
+/* FP32 forms of the dense field and marching cubes (the precision mode): the field is summed in
+   FP32 from FP32 copies of the coefficients and corner positions (quotients by one reciprocal
+   multiply), 4 bytes per lattice point; marching cubes classifies and interpolates the FP32
+   values (vertex positions in FP64). No counterpart in the reference (FP64 only). */
+its_status its_eval_grid_f32(its_svo* svo, const double* lambda, const double origin[3], const double width[3],
+                             int res, float* field);
+its_status its_marching_cubes_f32(its_ctx* ctx, const float* field, int res, const double origin[3],
+                                  const double width[3], double iso, uint8_t* cube_index, double* tri_verts,
+                                  int64_t capacity, int64_t* num_verts);
 /* No counterpart in the reference. The same results as its_marching_cubes for callers that
    cannot allocate device memory while they run (work replayed in a caller-captured CUDA
    graph, a fixed memory budget): no cudaMalloc/cudaFree, the scan scratch is a fixed 64 KiB

@@ -82,6 +82,8 @@ SIGNATURES = {
     "its_eval_grid": (st, [vp, vp, vp, vp, i32, vp]),
     "its_point_query": (st, [vp, vp, vp, i64, vp, vp, dbl, dbl, vp, vp]),
     "its_marching_cubes": (st, [vp, vp, i32, vp, vp, dbl, vp, vp, i64, C.POINTER(i64)]),
+    "its_marching_cubes_f32": (st, [vp, vp, i32, vp, vp, dbl, vp, vp, i64, C.POINTER(i64)]),
+    "its_eval_grid_f32": (st, [vp, vp, vp, vp, i32, vp]),
     "its_marching_cubes_mesh": (st, [vp, vp, i32, vp, vp, dbl, vp, i64, C.POINTER(i64), vp, i64, C.POINTER(i64)]),
 }
 

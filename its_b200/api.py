@@ -196,8 +196,10 @@ class Svo:
         self.ctx.check(lib().its_fit_residual(self.h, _ptr(b), _ptr(lam), C.byref(rel)), "its_fit_residual")
         return rel.value
 
-    def share_features(self, b, V, F, norm=None):
-        """Features of the share network (its_share_features): (features n x 64, vertex ids)."""
+    def share_features(self, b, V, F, norm=None, out=None, ids=None):
+        """Features of the share network (its_share_features): (features n x 64, vertex ids).
+
+        out / ids may be preallocated (numpy or torch CUDA) with enough rows."""
         b, V, F = _f64(b), _f64(V), _i32(F)
         nrm = None if norm is None else np.ascontiguousarray(norm, np.float32)
         cnt = C.c_int64(0)
@@ -205,10 +207,12 @@ class Svo:
         self.ctx.check(L.its_share_features(self.h, _ptr(b), _ptr(V), _n(V), _ptr(F), _n(F), _ptr(nrm), None, 0, None,
                                             C.byref(cnt)), "its_share_features")
         n = cnt.value
-        feats, ids = np.zeros((max(n, 1), 64), np.float32), np.zeros(max(n, 1), np.int64)
-        self.ctx.check(L.its_share_features(self.h, _ptr(b), _ptr(V), _n(V), _ptr(F), _n(F), _ptr(nrm), _ptr(feats), n,
-                                            _ptr(ids), C.byref(cnt)), "its_share_features")
-        return feats[:n], ids[:n]
+        feats = out if out is not None else np.zeros((max(n, 1), 64), np.float32)
+        idv = ids if ids is not None else np.zeros(max(n, 1), np.int64)
+        cap = int(feats.shape[0])
+        self.ctx.check(L.its_share_features(self.h, _ptr(b), _ptr(V), _n(V), _ptr(F), _n(F), _ptr(nrm), _ptr(feats),
+                                            cap, _ptr(idv), C.byref(cnt)), "its_share_features")
+        return feats[:n], idv[:n]
 
     def depth_counts(self):
         return (np.array(self.info.nodes_per_depth[:self.depth], np.int64),
@@ -282,6 +286,16 @@ class Svo:
         if out is None:
             out = np.zeros((res + 1) ** 3)
         self.ctx.check(lib().its_eval_grid(self.h, _ptr(lam), _ptr(o), _ptr(w), res, _ptr(out)), "its_eval_grid")
+        return out
+
+    def eval_grid_f32(self, lam, origin, width, res, out=None):
+        """FP32 dense field (its_eval_grid_f32)."""
+        lam = _f64(lam)
+        o, w = np.ascontiguousarray(origin, np.float64), np.ascontiguousarray(width, np.float64)
+        if out is None:
+            out = np.zeros((res + 1) ** 3, np.float32)
+        self.ctx.check(lib().its_eval_grid_f32(self.h, _ptr(lam), _ptr(o), _ptr(w), res, _ptr(out)),
+                       "its_eval_grid_f32")
         return out
 
     def vertex_sdf(self, V, F):

@@ -174,10 +174,26 @@ constexpr int kTileCap = 640;
 // inputs, equal IEEE results); all quotients use divRn. Depths whose corner box has no
 // corner are skipped; depths whose box exceeds the tile (grids much coarser than the octree)
 // fall back to per-point lookups.
+template <typename T>
+__device__ __forceinline__ T quotT(T a, T w, T wi) {
+  if constexpr (sizeof(T) == 8) return divRn(a, w, wi);
+  else return a * wi;
+}
+template <typename T>
+__device__ __forceinline__ T hatT(T x, T p, T w, T wi) {
+  if constexpr (sizeof(T) == 8) {
+    return hat1r(x, p, w, wi);
+  } else {
+    if (x <= p - w || x >= p + w) return T(0);
+    return x <= p ? T(1) + (x - p) * wi : T(1) - (x - p) * wi;
+  }
+}
+
+template <typename T>
 __global__ void __launch_bounds__(kBrickThreads, 2)
     kEvalGridBricks(const __grid_constant__ EvalParams P, const double* __restrict__ lambda, double3 o, double3 vs,
-                    int R, double* __restrict__ field) {
-  __shared__ double tLam[kTileCap], tPx[kTileCap], tPy[kTileCap], tPz[kTileCap];
+                    int R, T* __restrict__ field) {
+  __shared__ T tLam[kTileCap], tPx[kTileCap], tPy[kTileCap], tPz[kTileCap];
   __shared__ unsigned char tHas[kTileCap];
   __shared__ int64_t box[6];  // first and last cell per axis at the current depth
   const int64_t M = (int64_t)R + 1;
@@ -187,15 +203,17 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
   const int64_t xi = x0 + (tid % kBrickX), yj = y0 + ((tid / kBrickX) % kBrickY);
   const int64_t zb = z0 + (int64_t)(tid / (kBrickX * kBrickY)) * kZPer;
   const bool inXY = xi < M && yj < M;
-  const double px = o.x + (double)xi * vs.x, py = o.y + (double)yj * vs.y;
-  double pz[kZPer], sum[kZPer];
+  const T px = (T)(o.x + (double)xi * vs.x), py = (T)(o.y + (double)yj * vs.y);
+  const T gx = (T)P.g.x, gy = (T)P.g.y, gz = (T)P.g.z;
+  T pz[kZPer], sum[kZPer];
 #pragma unroll
   for (int q = 0; q < kZPer; ++q) {
-    pz[q] = o.z + (double)(zb + q) * vs.z;
-    sum[q] = 0.0;
+    pz[q] = (T)(o.z + (double)(zb + q) * vs.z);
+    sum[q] = T(0);
   }
   for (int d = 0; d < P.depth; ++d) {
-    const double w = P.w0 * (double)(1u << d), wi = P.winv[d];
+    const double wd = P.w0 * (double)(1u << d), wid = P.winv[d];
+    const T w = (T)wd, wi = (T)wid;
     const LatticeIndex& L = P.lat[d];
     const int64_t lim = (int64_t)(P.res >> d);
     if (tid < 6) {
@@ -205,7 +223,9 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
       const int64_t cl = idx < M ? idx : M - 1;
       const double oa = a == 0 ? o.x : a == 1 ? o.y : o.z, va = a == 0 ? vs.x : a == 1 ? vs.y : vs.z;
       const double ga = a == 0 ? P.g.x : a == 1 ? P.g.y : P.g.z;
-      box[tid] = (int64_t)floor(divRn((oa + (double)cl * va) - ga, w, wi));
+      const double pa = oa + (double)cl * va;
+      box[tid] = sizeof(T) == 8 ? (int64_t)floor(divRn(pa - ga, wd, wid))
+                                : (int64_t)floorf(quotT<T>((T)pa - (T)ga, w, wi));
     }
     __syncthreads();
     const int64_t cx0 = box[0], cy0 = box[2], cz0 = box[4];
@@ -221,10 +241,10 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
           const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
           if (latticeHas(L, lin)) {
             const uint32_t v = latticeRank(L, lin);
-            tLam[t] = lambda[v];
-            tPx[t] = P.vertPos[3 * v];
-            tPy[t] = P.vertPos[3 * v + 1];
-            tPz[t] = P.vertPos[3 * v + 2];
+            tLam[t] = (T)lambda[v];
+            tPx[t] = (T)P.vertPos[3 * v];
+            tPy[t] = (T)P.vertPos[3 * v + 1];
+            tPz[t] = (T)P.vertPos[3 * v + 2];
             has = 1;
           }
         }
@@ -236,22 +256,22 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
       __syncthreads();
     }
     if (any && inXY) {
-      const int64_t cx = (int64_t)floor(divRn(px - P.g.x, w, wi)), cy = (int64_t)floor(divRn(py - P.g.y, w, wi));
+      const int64_t cx = (int64_t)floor(quotT<T>(px - gx, w, wi)), cy = (int64_t)floor(quotT<T>(py - gy, w, wi));
       // x / y hat factors per distinct corner coordinate, shared by the column's points
-      double cxv[2] = {0.0, 0.0}, cyv[2] = {0.0, 0.0}, hxv[2] = {0.0, 0.0}, hyv[2] = {0.0, 0.0};
+      T cxv[2] = {0, 0}, cyv[2] = {0, 0}, hxv[2] = {0, 0}, hyv[2] = {0, 0};
       bool okx[2] = {false, false}, oky[2] = {false, false};
 #pragma unroll
       for (int q = 0; q < kZPer; ++q) {
         if (zb + q >= M) break;
-        const double pzq = pz[q];
-        const int64_t cz = (int64_t)floor(divRn(pzq - P.g.z, w, wi));
-        double czv[2] = {0.0, 0.0}, hzv[2] = {0.0, 0.0};
+        const T pzq = pz[q];
+        const int64_t cz = (int64_t)floor(quotT<T>(pzq - gz, w, wi));
+        T czv[2] = {0, 0}, hzv[2] = {0, 0};
         bool okz[2] = {false, false};
-        double s = sum[q];
+        T s = sum[q];
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
           const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
-          double lam, qx, qy, qz;
+          T lam, qx, qy, qz;
           if (tiled) {
             const int t = ((int)(cx - cx0) + ox) * ny * nz + ((int)(cy - cy0) + oy) * nz + ((int)(cz - cz0) + oz);
             if (!tHas[t]) continue;
@@ -265,21 +285,21 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
             const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
             if (!latticeHas(L, lin)) continue;
             const uint32_t v = latticeRank(L, lin);
-            lam = lambda[v];
-            qx = P.vertPos[3 * v];
-            qy = P.vertPos[3 * v + 1];
-            qz = P.vertPos[3 * v + 2];
+            lam = (T)lambda[v];
+            qx = (T)P.vertPos[3 * v];
+            qy = (T)P.vertPos[3 * v + 1];
+            qz = (T)P.vertPos[3 * v + 2];
           }
-          double hx, hy, hz;
+          T hx, hy, hz;
           if (okx[ox] && cxv[ox] == qx) hx = hxv[ox];
-          else { hx = hat1r(px, qx, w, wi); cxv[ox] = qx; hxv[ox] = hx; okx[ox] = true; }
-          if (hx <= 0.0) continue;
+          else { hx = hatT<T>(px, qx, w, wi); cxv[ox] = qx; hxv[ox] = hx; okx[ox] = true; }
+          if (hx <= T(0)) continue;
           if (oky[oy] && cyv[oy] == qy) hy = hyv[oy];
-          else { hy = hat1r(py, qy, w, wi); cyv[oy] = qy; hyv[oy] = hy; oky[oy] = true; }
-          if (hy <= 0.0) continue;
+          else { hy = hatT<T>(py, qy, w, wi); cyv[oy] = qy; hyv[oy] = hy; oky[oy] = true; }
+          if (hy <= T(0)) continue;
           if (okz[oz] && czv[oz] == qz) hz = hzv[oz];
-          else { hz = hat1r(pzq, qz, w, wi); czv[oz] = qz; hzv[oz] = hz; okz[oz] = true; }
-          if (hz <= 0.0) continue;
+          else { hz = hatT<T>(pzq, qz, w, wi); czv[oz] = qz; hzv[oz] = hz; okz[oz] = true; }
+          if (hz <= T(0)) continue;
           s += lam * (hx * hy * hz);
         }
         sum[q] = s;
@@ -433,7 +453,29 @@ its_status its_eval_grid(its_svo* s, const double* lambda, const double origin[3
   (void)total;
   const dim3 grid((unsigned)((M + kBrickX - 1) / kBrickX), (unsigned)((M + kBrickY - 1) / kBrickY),
                   (unsigned)((M + kBrickZ - 1) / kBrickZ));
-  kEvalGridBricks<<<grid, kBrickThreads, 0, ctx->stream>>>(evalParams(s->d), L.d, o, vs, res, F.d);
+  kEvalGridBricks<double><<<grid, kBrickThreads, 0, ctx->stream>>>(evalParams(s->d), L.d, o, vs, res, F.d);
+  ITS_LAUNCHED(ctx);
+  if ((st = F.finish(ctx)) != ITS_OK) return st;
+  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITS_OK;
+}
+
+its_status its_eval_grid_f32(its_svo* s, const double* lambda, const double origin[3], const double width[3], int res,
+                             float* field) {
+  if (!s || !lambda || !origin || !width || !field || res < 1 || res > 2048) return ITS_ERR_INVALID;
+  its_ctx* ctx = s->ctx;
+  ITS_CU(ctx, cudaSetDevice(ctx->device));
+  const int64_t M = (int64_t)res + 1, total = M * M * M;
+  InArg<double> L;
+  OutArg<float> F;
+  its_status st;
+  if ((st = L.stage(ctx, lambda, s->d.numVerts)) != ITS_OK) return st;
+  if ((st = F.stage(ctx, field, total)) != ITS_OK) return st;
+  const double3 o = make_double3(origin[0], origin[1], origin[2]);
+  const double3 vs = make_double3(width[0] / res, width[1] / res, width[2] / res);
+  const dim3 grid((unsigned)((M + kBrickX - 1) / kBrickX), (unsigned)((M + kBrickY - 1) / kBrickY),
+                  (unsigned)((M + kBrickZ - 1) / kBrickZ));
+  kEvalGridBricks<float><<<grid, kBrickThreads, 0, ctx->stream>>>(evalParams(s->d), L.d, o, vs, res, F.d);
   ITS_LAUNCHED(ctx);
   if ((st = F.finish(ctx)) != ITS_OK) return st;
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
@@ -461,26 +503,29 @@ its_status its_check_division(its_ctx* ctx, const double* a, const double* b, in
   return ITS_OK;
 }
 
-its_status its_marching_cubes(its_ctx* ctx, const double* field, int res, const double origin[3],
-                              const double width[3], double iso, uint8_t* cube_index, double* tri_verts,
-                              int64_t capacity, int64_t* num_verts) {
+}  // extern "C"
+
+namespace {
+template <typename FT>
+its_status marchingCubesT(its_ctx* ctx, const FT* field, int res, const double origin[3], const double width[3],
+                          double iso, uint8_t* cube_index, double* tri_verts, int64_t capacity, int64_t* num_verts) {
   if (!ctx) return ITS_ERR_INVALID;
   if (!field || !origin || !width || res < 1 || res > 2048 || !num_verts)
     return setError(ctx, ITS_ERR_INVALID, "its_marching_cubes: bad arguments");
   if (tri_verts && capacity < 0) return setError(ctx, ITS_ERR_INVALID, "negative capacity");
   ITS_CU(ctx, cudaSetDevice(ctx->device));
   const int64_t M = (int64_t)res + 1, nvox = (int64_t)res * res * res;
-  InArg<double> F;
+  InArg<FT> F;
   OutArg<uint8_t> Cb;
   OutArg<double> T;
   its_status st;
   if ((st = F.stage(ctx, field, M * M * M)) != ITS_OK) return st;
   if ((st = Cb.stage(ctx, cube_index, nvox)) != ITS_OK) return st;
   if ((st = T.stage(ctx, tri_verts, tri_verts ? 3 * capacity : 0)) != ITS_OK) return st;
-  McCase mc{F.d, res, iso};
-  McEmit em{mc, make_double3(origin[0], origin[1], origin[2]),
-            make_double3(width[0] / res, width[1] / res, width[2] / res), Cb.d, T.d,
-            (unsigned long long)(tri_verts ? capacity : 0)};
+  McCaseT<FT> mc{F.d, res, iso};
+  McEmitT<FT> em{mc, make_double3(origin[0], origin[1], origin[2]),
+                 make_double3(width[0] / res, width[1] / res, width[2] / res), Cb.d, T.d,
+                 (unsigned long long)(tri_verts ? capacity : 0)};
   DevBuf<unsigned long long> tot;
   if ((st = tot.alloc(ctx, 1)) != ITS_OK) return st;
   if ((st = scanExclusiveAlloc<unsigned long long>(ctx, mc, nvox, em, tot.p)) != ITS_OK) return st;
@@ -491,6 +536,21 @@ its_status its_marching_cubes(its_ctx* ctx, const double* field, int res, const 
   if ((st = T.finish(ctx)) != ITS_OK) return st;
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   return ITS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+its_status its_marching_cubes(its_ctx* ctx, const double* field, int res, const double origin[3],
+                              const double width[3], double iso, uint8_t* cube_index, double* tri_verts,
+                              int64_t capacity, int64_t* num_verts) {
+  return marchingCubesT<double>(ctx, field, res, origin, width, iso, cube_index, tri_verts, capacity, num_verts);
+}
+
+its_status its_marching_cubes_f32(its_ctx* ctx, const float* field, int res, const double origin[3],
+                                  const double width[3], double iso, uint8_t* cube_index, double* tri_verts,
+                                  int64_t capacity, int64_t* num_verts) {
+  return marchingCubesT<float>(ctx, field, res, origin, width, iso, cube_index, tri_verts, capacity, num_verts);
 }
 
 }  // extern "C"

@@ -33,8 +33,9 @@ __device__ __forceinline__ void voxelXYZ(int64_t v, int R, int64_t& x, int64_t& 
   }
 }
 
-struct McCase {
-  const double* field;
+template <typename T>
+struct McCaseT {
+  const T* field;
   int R;
   double iso;
   __device__ unsigned cube(int64_t v) const {
@@ -44,13 +45,14 @@ struct McCase {
     unsigned ci = 0;
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      const double f = field[((z + cMcCorner[k][2]) * M + (y + cMcCorner[k][1])) * M + (x + cMcCorner[k][0])];
+      const double f = (double)field[((z + cMcCorner[k][2]) * M + (y + cMcCorner[k][1])) * M + (x + cMcCorner[k][0])];
       ci |= (unsigned)(f < iso) << k;
     }
     return ci;
   }
   __device__ unsigned long long operator()(int64_t v) const { return cMcCase[cube(v)] & 15ull; }
 };
+using McCase = McCaseT<double>;
 
 __device__ inline void vertexLerp(const double* p0, const double* p1, double s0, double s1, double iso, double* out) {
   if (fabs(iso - s0) < 1e-6) { out[0] = p0[0]; out[1] = p0[1]; out[2] = p0[2]; return; }
@@ -62,8 +64,9 @@ __device__ inline void vertexLerp(const double* p0, const double* p1, double s0,
 }
 
 // The scan's write step: case byte (optional) and the voxel's triangle vertices at its offset.
-struct McEmit {
-  McCase mc;
+template <typename T>
+struct McEmitT {
+  McCaseT<T> mc;
   double3 o, vs;
   uint8_t* cubeOut;
   double* tri;
@@ -82,7 +85,7 @@ struct McEmit {
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       for (int a = 0; a < 3; ++a) corner[k][a] = cMcCorner[k][a] ? vp[a] + vsz[a] : vp[a];
-      sdf[k] = mc.field[((z + cMcCorner[k][2]) * M + (y + cMcCorner[k][1])) * M + (x + cMcCorner[k][0])];
+      sdf[k] = (double)mc.field[((z + cMcCorner[k][2]) * M + (y + cMcCorner[k][1])) * M + (x + cMcCorner[k][0])];
     }
     const uint64_t cw = cMcCase[ci];
     for (unsigned i = 0; i < (unsigned)count; ++i) {
@@ -97,5 +100,6 @@ struct McEmit {
     }
   }
 };
+using McEmit = McEmitT<double>;
 
 }  // namespace its

@@ -143,3 +143,38 @@ def test_fast_division_is_correctly_rounded(ctx):
         ctx.check(lib().its_check_division(ctx.h, x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p), n,
                                            C.byref(miss)), "its_check_division")
         assert miss.value == 0
+
+
+@pytest.mark.gpu
+def test_fp32_field_and_marching_cubes(ctx):
+    # Precision mode: the FP32 field agrees with the FP64 one to FP32 rounding, and FP32
+    # marching cubes gives the same case indices outside the band where FP32 rounding can
+    # move a corner across the iso level.
+    import ctypes as C
+    from its_b200 import Operator, Svo, lib
+    V, F, o, w = prepared_mesh("c0")
+    svo = Svo(ctx, V, F, 32, o, w)
+    b = ctx.signed_distance(svo.vertices()[0], V, F)
+    lam, _ = Operator(svo).solve(b, tol=1e-10, max_iters=1000)
+    R = 96
+    f64 = svo.eval_grid(lam, o, w, R)
+    f32 = svo.eval_grid_f32(lam, o, w, R)
+    scale = np.abs(f64).max()
+    err = np.abs(f32.astype(np.float64) - f64)
+    assert err.max() <= 2e-6 * scale, err.max() / scale
+    iso = float(np.median(b[np.abs(b) < 0.05]))
+    cubes = []
+    for fld, fn in ((f64, lib().its_marching_cubes), (f32, lib().its_marching_cubes_f32)):
+        cube = np.zeros(R ** 3, np.uint8)
+        n = C.c_int64(0)
+        ctx.check(fn(ctx.h, fld.ctypes.data_as(C.c_void_p), R, o.ctypes.data_as(C.c_void_p),
+                     w.ctypes.data_as(C.c_void_p), iso, cube.ctypes.data_as(C.c_void_p), None, 0, C.byref(n)), "mc")
+        cubes.append(cube)
+    diff = np.nonzero(cubes[0] != cubes[1])[0]
+    M = R + 1
+    g = f64.reshape(M, M, M)  # [z][y][x]
+    for v in diff:
+        x, y, z = v % R, (v // R) % R, v // (R * R)
+        corners = g[z:z + 2, y:y + 2, x:x + 2]
+        assert np.abs(corners - iso).min() <= 4e-6 * scale
+    assert len(diff) <= 1e-3 * R ** 3
