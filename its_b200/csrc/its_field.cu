@@ -314,6 +314,85 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
   }
 }
 
+// ---- marching cubes in three launches -----------------------------------------------------
+// Classify: each thread takes 8 consecutive voxels (x fastest) and slides along x, loading one
+// column of 4 corner values per voxel (each field value is read about once), writes the case
+// bytes and reduces the vertex counts per block. The block sums are scanned (kScanSpine);
+// Emit re-reads only the case bytes, scans the counts inside the block and writes the
+// triangle vertices of the non-empty voxels in voxel order, as the reference's compaction does.
+template <typename T>
+__global__ void __launch_bounds__(kScanThreads) kMcClassify(const T* __restrict__ field, int R, double iso,
+                                                             uint8_t* __restrict__ cube,
+                                                             unsigned long long* __restrict__ blockSums) {
+  const int64_t nvox = (int64_t)R * R * R, M = (int64_t)R + 1;
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  unsigned long long cnt = 0;
+  if (base < nvox) {
+    int64_t x, y, z;
+    voxelXYZ(base, R, x, y, z);
+    double a = 0, b = 0, c = 0, d = 0;  // column x: (y,z) (y+1,z) (y,z+1) (y+1,z+1)
+    bool have = false;
+    for (int j = 0; j < kScanItems && base + j < nvox; ++j) {
+      const int64_t r0 = (z * M + y) * M, r1 = (z * M + y + 1) * M, r2 = ((z + 1) * M + y) * M,
+                    r3 = ((z + 1) * M + y + 1) * M;
+      if (!have) {
+        a = (double)field[r0 + x];
+        b = (double)field[r1 + x];
+        c = (double)field[r2 + x];
+        d = (double)field[r3 + x];
+      }
+      const double a1 = (double)field[r0 + x + 1], b1 = (double)field[r1 + x + 1], c1 = (double)field[r2 + x + 1],
+                   d1 = (double)field[r3 + x + 1];
+      // corner order 0 (0,0,0) 1 (0,1,0) 2 (1,1,0) 3 (1,0,0) 4 (0,0,1) 5 (0,1,1) 6 (1,1,1) 7 (1,0,1)
+      const unsigned ci = (unsigned)(a < iso) | (unsigned)(b < iso) << 1 | (unsigned)(b1 < iso) << 2 |
+                          (unsigned)(a1 < iso) << 3 | (unsigned)(c < iso) << 4 | (unsigned)(d < iso) << 5 |
+                          (unsigned)(d1 < iso) << 6 | (unsigned)(c1 < iso) << 7;
+      cube[base + j] = (uint8_t)ci;
+      cnt += cMcCase[ci] & 15ull;
+      a = a1;
+      b = b1;
+      c = c1;
+      d = d1;
+      have = true;
+      if (++x == R) {  // next row
+        x = 0;
+        have = false;
+        if (++y == R) {
+          y = 0;
+          ++z;
+        }
+      }
+    }
+  }
+  unsigned long long total;
+  blockExclusiveScan<unsigned long long>(cnt, total);
+  if (threadIdx.x == 0) blockSums[blockIdx.x] = total;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kScanThreads) kMcEmit(McCaseT<T> mc, double3 o, double3 vs,
+                                                         const uint8_t* __restrict__ cube,
+                                                         const unsigned long long* __restrict__ blockOffsets,
+                                                         double* __restrict__ tri, unsigned long long capacity) {
+  const int64_t nvox = (int64_t)mc.R * mc.R * mc.R;
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  unsigned char ci[kScanItems];
+  unsigned long long cnt = 0;
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) {
+    ci[j] = base + j < nvox ? cube[base + j] : 0;
+    cnt += cMcCase[ci[j]] & 15ull;
+  }
+  unsigned long long total;
+  unsigned long long run = blockExclusiveScan<unsigned long long>(cnt, total) + blockOffsets[blockIdx.x];
+  if (!total || !tri) return;
+  for (int j = 0; j < kScanItems; ++j) {
+    const unsigned long long c = cMcCase[ci[j]] & 15ull;
+    if (c) mcEmitVoxel(mc, o, vs, tri, capacity, base + j, ci[j], run, c);
+    run += c;
+  }
+}
+
 // divRn against the hardware-correct quotient (a test hook: out[i] = 1 where they differ).
 __global__ void kCheckDivRn(const double* __restrict__ a, const double* __restrict__ b, int64_t n,
                             unsigned char* __restrict__ differ) {
@@ -523,12 +602,26 @@ its_status marchingCubesT(its_ctx* ctx, const FT* field, int res, const double o
   if ((st = Cb.stage(ctx, cube_index, nvox)) != ITS_OK) return st;
   if ((st = T.stage(ctx, tri_verts, tri_verts ? 3 * capacity : 0)) != ITS_OK) return st;
   McCaseT<FT> mc{F.d, res, iso};
-  McEmitT<FT> em{mc, make_double3(origin[0], origin[1], origin[2]),
-                 make_double3(width[0] / res, width[1] / res, width[2] / res), Cb.d, T.d,
-                 (unsigned long long)(tri_verts ? capacity : 0)};
-  DevBuf<unsigned long long> tot;
-  if ((st = tot.alloc(ctx, 1)) != ITS_OK) return st;
-  if ((st = scanExclusiveAlloc<unsigned long long>(ctx, mc, nvox, em, tot.p)) != ITS_OK) return st;
+  // case bytes: the caller's buffer when it is on the device, else scratch copied back
+  DevBuf<uint8_t> cubeTmp;
+  uint8_t* cubeD = Cb.d;
+  if (!cubeD) {
+    if ((st = cubeTmp.alloc(ctx, nvox)) != ITS_OK) return st;
+    cubeD = cubeTmp.p;
+  }
+  const int64_t nb = scanBlocks(nvox);
+  DevBuf<unsigned long long> sums, tot;
+  if ((st = sums.alloc(ctx, nb)) != ITS_OK || (st = tot.alloc(ctx, 1)) != ITS_OK) return st;
+  kMcClassify<FT><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(F.d, res, iso, cubeD, sums.p);
+  ITS_LAUNCHED(ctx);
+  kScanSpine<unsigned long long><<<1, kScanThreads, 0, ctx->stream>>>(sums.p, nb, tot.p);
+  ITS_LAUNCHED(ctx);
+  if (T.d) {
+    kMcEmit<FT><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(
+        mc, make_double3(origin[0], origin[1], origin[2]), make_double3(width[0] / res, width[1] / res, width[2] / res),
+        cubeD, sums.p, T.d, (unsigned long long)capacity);
+    ITS_LAUNCHED(ctx);
+  }
   unsigned long long total = 0;
   if ((st = readScalar(ctx, tot.p, &total)) != ITS_OK) return st;
   *num_verts = (int64_t)total;

@@ -63,6 +63,35 @@ __device__ inline void vertexLerp(const double* p0, const double* p1, double s0,
   for (int a = 0; a < 3; ++a) out[a] = fma(t, p1[a], fma(-t, p0[a], p0[a]));  // MCKernel::lerp
 }
 
+// The triangle vertices of voxel v (case ci, count vertices) written from offset on.
+template <typename T>
+__device__ inline void mcEmitVoxel(const McCaseT<T>& mc, double3 o, double3 vs, double* tri, unsigned long long capacity,
+                                   int64_t v, unsigned ci, unsigned long long offset, unsigned long long count) {
+  const int R = mc.R;
+  const int64_t M = (int64_t)R + 1;
+  int64_t x, y, z;
+  voxelXYZ(v, R, x, y, z);
+  const double vp[3] = {(double)x * vs.x + o.x, (double)y * vs.y + o.y, (double)z * vs.z + o.z};
+  const double vsz[3] = {vs.x, vs.y, vs.z};
+  double corner[8][3], sdf[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    for (int a = 0; a < 3; ++a) corner[k][a] = cMcCorner[k][a] ? vp[a] + vsz[a] : vp[a];
+    sdf[k] = (double)mc.field[((z + cMcCorner[k][2]) * M + (y + cMcCorner[k][1])) * M + (x + cMcCorner[k][0])];
+  }
+  const uint64_t cw = cMcCase[ci];
+  for (unsigned i = 0; i < (unsigned)count; ++i) {
+    const unsigned long long dst = offset + i;
+    if (dst >= capacity) break;
+    const int e = (int)((cw >> (4 * (i + 1))) & 15u);
+    double q[3];
+    vertexLerp(corner[cMcEdge[e][0]], corner[cMcEdge[e][1]], sdf[cMcEdge[e][0]], sdf[cMcEdge[e][1]], mc.iso, q);
+    tri[3 * dst] = q[0];
+    tri[3 * dst + 1] = q[1];
+    tri[3 * dst + 2] = q[2];
+  }
+}
+
 // The scan's write step: case byte (optional) and the voxel's triangle vertices at its offset.
 template <typename T>
 struct McEmitT {
@@ -75,29 +104,7 @@ struct McEmitT {
     const unsigned ci = (cubeOut || count) ? mc.cube(v) : 0u;
     if (cubeOut) cubeOut[v] = (uint8_t)ci;
     if (!count || !tri) return;
-    const int R = mc.R;
-    const int64_t M = (int64_t)R + 1;
-    int64_t x, y, z;
-    voxelXYZ(v, R, x, y, z);
-    const double vp[3] = {(double)x * vs.x + o.x, (double)y * vs.y + o.y, (double)z * vs.z + o.z};
-    const double vsz[3] = {vs.x, vs.y, vs.z};
-    double corner[8][3], sdf[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      for (int a = 0; a < 3; ++a) corner[k][a] = cMcCorner[k][a] ? vp[a] + vsz[a] : vp[a];
-      sdf[k] = (double)mc.field[((z + cMcCorner[k][2]) * M + (y + cMcCorner[k][1])) * M + (x + cMcCorner[k][0])];
-    }
-    const uint64_t cw = cMcCase[ci];
-    for (unsigned i = 0; i < (unsigned)count; ++i) {
-      const unsigned long long dst = offset + i;
-      if (dst >= capacity) break;
-      const int e = (int)((cw >> (4 * (i + 1))) & 15u);
-      double q[3];
-      vertexLerp(corner[cMcEdge[e][0]], corner[cMcEdge[e][1]], sdf[cMcEdge[e][0]], sdf[cMcEdge[e][1]], mc.iso, q);
-      tri[3 * dst] = q[0];
-      tri[3 * dst + 1] = q[1];
-      tri[3 * dst + 2] = q[2];
-    }
+    mcEmitVoxel(mc, o, vs, tri, capacity, v, ci, offset, count);
   }
 };
 using McEmit = McEmitT<double>;
