@@ -56,6 +56,14 @@ its_status its_synchronize(its_ctx* ctx);
 const char* its_version(void);
 /* Number of kernels this context has launched so far (a diagnostic counter). */
 int64_t its_kernel_launches(const its_ctx* ctx);
+/* The autotuner. With enable = 1 the first call of a tunable launch (the dense field's brick
+   shape, the marching-cubes tile) for a given shape key times every candidate on the context's
+   stream and keeps the fastest; later calls reuse the choice. Every candidate computes the
+   same bits, so tuning changes speed only. cache_path (NULL: none) persists the choices as
+   "key value" lines and is read here. No counterpart in the reference. */
+its_status its_set_autotune(its_ctx* ctx, int enable, const char* cache_path);
+/* The choices made so far as "key value" lines (length without the terminating zero). */
+its_status its_autotune_choices(const its_ctx* ctx, char* buf, int64_t size, int64_t* length);
 /* Self-check of the division the field kernels use (a multiply and two FMAs from the
    correctly rounded reciprocal, Markstein's theorem): counts the pairs whose quotient differs
    from the GPU's correctly rounded a[i] / b[i]. No counterpart in the reference. */
@@ -217,6 +225,15 @@ its_status its_shell_iso_values(its_svo* svo, const double* lambda, const double
 its_status its_point_query(its_svo* svo, const double* lambda, const double* points, int64_t npoints,
                            const double box_origin[3], const double box_end[3], double inner, double outer,
                            double* values, int8_t* labels);
+
+/* ThinShells::getPointValGradient (src/ThinShells.cpp:1800-1866), the gradients behind the
+   point normals of ThinShells.cpp:1658-1735: a point outside the box [box_origin, box_end]
+   moves halfway towards its previous position (before, may be NULL) until inside, then the
+   field and its gradient (de_BaseFunction, BSpline.hpp:30-57) over its fine node's chain.
+   gradients: 3 per point; points in no fine node get 0 and missing[i] = 1 (may be NULL). */
+its_status its_point_value_gradient(its_svo* svo, const double* lambda, const double* points, const double* before,
+                                   int64_t npoints, const double box_origin[3], const double box_end[3], double* values,
+                                   double* gradients, uint8_t* missing);
 
 /* ---- a14-a15: dense field and marching cubes -------------------------------------------- */
 /* The field of MC::launch_computSDFKernel (src/cuAcc/MarchingCubes/MarchingCubes.cu:464-536,

@@ -42,6 +42,8 @@ SIGNATURES = {
     "its_version": (C.c_char_p, []),
     "its_kernel_launches": (i64, [vp]),
     "its_check_division": (st, [vp, vp, vp, i64, C.POINTER(i64)]),
+    "its_set_autotune": (st, [vp, i32, C.c_char_p]),
+    "its_autotune_choices": (st, [vp, C.c_char_p, i64, C.POINTER(i64)]),
     "its_model_to_unit_cube": (st, [vp, i64, dbl]),
     "its_uniform_bbox": (st, [vp, i64, vp, vp, vp]),
     "its_tri_attributes": (st, [vp, vp, i64, vp, i64, vp, vp, vp]),
@@ -81,6 +83,7 @@ SIGNATURES = {
     "its_shell_iso_values": (st, [vp, vp, vp, i64, C.POINTER(dbl), C.POINTER(dbl), C.POINTER(i64)]),
     "its_eval_grid": (st, [vp, vp, vp, vp, i32, vp]),
     "its_point_query": (st, [vp, vp, vp, i64, vp, vp, dbl, dbl, vp, vp]),
+    "its_point_value_gradient": (st, [vp, vp, vp, vp, i64, vp, vp, vp, vp, vp]),
     "its_marching_cubes": (st, [vp, vp, i32, vp, vp, dbl, vp, vp, i64, C.POINTER(i64)]),
     "its_marching_cubes_f32": (st, [vp, vp, i32, vp, vp, dbl, vp, vp, i64, C.POINTER(i64)]),
     "its_eval_grid_f32": (st, [vp, vp, vp, vp, i32, vp]),

@@ -80,6 +80,18 @@ class Context:
     def synchronize(self):
         self.check(lib().its_synchronize(self.h), "its_synchronize")
 
+    def set_autotune(self, enable=True, cache_path=None):
+        """Pick launch shapes by measurement (its_set_autotune); choices persist in cache_path."""
+        self.check(lib().its_set_autotune(self.h, 1 if enable else 0,
+                                          None if cache_path is None else cache_path.encode()), "its_set_autotune")
+
+    def autotune_choices(self):
+        n = C.c_int64(0)
+        self.check(lib().its_autotune_choices(self.h, None, 0, C.byref(n)), "its_autotune_choices")
+        buf = C.create_string_buffer(n.value + 1)
+        self.check(lib().its_autotune_choices(self.h, buf, n.value + 1, C.byref(n)), "its_autotune_choices")
+        return dict((k, int(v)) for k, v in (line.split() for line in buf.value.decode().splitlines() if line))
+
     @property
     def kernel_launches(self):
         return int(lib().its_kernel_launches(self.h))
@@ -179,6 +191,17 @@ class Svo:
 
     def __del__(self):
         self.close()
+
+    def point_gradient(self, lam, P, box_origin, box_end, before=None):
+        """Field, gradient (n x 3) and missing flags (its_point_value_gradient)."""
+        lam, P = _f64(lam), _f64(P)
+        m = _n(P)
+        val, grad, miss = np.zeros(m), np.zeros((m, 3)), np.zeros(m, np.uint8)
+        bo, be = np.ascontiguousarray(box_origin, np.float64), np.ascontiguousarray(box_end, np.float64)
+        bf = None if before is None else _f64(before)
+        self.ctx.check(lib().its_point_value_gradient(self.h, _ptr(lam), _ptr(P), _ptr(bf), m, _ptr(bo), _ptr(be),
+                                                      _ptr(val), _ptr(grad), _ptr(miss)), "its_point_value_gradient")
+        return val, grad, miss
 
     def exact_start(self, b, shares=None, out=None):
         """Hierarchical-surplus exact solution of A lambda = b, matrix-free (its_exact_start)."""

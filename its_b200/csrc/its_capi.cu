@@ -2,12 +2,22 @@
 // triangle attributes and mesh validation.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 
 #include "its_ctx.cuh"
 #include "its_svo.cuh"
 
 namespace its {
+
+void saveTuneCache(its_ctx* ctx) {
+  if (ctx->tuneCache.empty()) return;
+  if (FILE* f = std::fopen(ctx->tuneCache.c_str(), "w")) {
+    for (const auto& kv : ctx->tuned) std::fprintf(f, "%s %d\n", kv.first.c_str(), kv.second);
+    std::fclose(f);
+  }
+}
+
 
 its_status setError(its_ctx* ctx, its_status code, const std::string& msg) {
   if (ctx) ctx->lastError = msg;
@@ -142,6 +152,34 @@ its_status its_synchronize(its_ctx* c) {
 }
 
 int64_t its_kernel_launches(const its_ctx* c) { return c ? c->launches : 0; }
+
+its_status its_set_autotune(its_ctx* c, int enable, const char* cache_path) {
+  if (!c) return ITS_ERR_INVALID;
+  c->autotune = enable ? 1 : 0;
+  c->tuneCache = cache_path ? cache_path : "";
+  if (!c->tuneCache.empty()) {  // load earlier choices: one "key value" pair per line
+    if (FILE* f = std::fopen(c->tuneCache.c_str(), "r")) {
+      char key[512];
+      int v;
+      while (std::fscanf(f, "%511s %d", key, &v) == 2) c->tuned[key] = v;
+      std::fclose(f);
+    }
+  }
+  return ITS_OK;
+}
+
+its_status its_autotune_choices(const its_ctx* c, char* buf, int64_t size, int64_t* length) {
+  if (!c || !length) return ITS_ERR_INVALID;
+  std::string out;
+  for (const auto& kv : c->tuned) out += kv.first + " " + std::to_string(kv.second) + "\n";
+  *length = (int64_t)out.size();
+  if (buf && size > 0) {
+    const int64_t k = std::min<int64_t>(size - 1, (int64_t)out.size());
+    std::memcpy(buf, out.data(), (size_t)k);
+    buf[k] = 0;
+  }
+  return ITS_OK;
+}
 
 // BaseModel::calcUnitCubeTransformMatrix + model2UnitCube (BaseModel.cpp:54-92): host code in
 // the reference as well; centre the box, scale its longest side to scale_factor^-1.

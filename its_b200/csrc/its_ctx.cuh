@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <map>
 #include <string>
 #include <utility>
 
@@ -16,6 +17,10 @@ struct its_ctx {
   int numSMs = 148;
   cudaMemPool_t pool = nullptr;  // the context's stream-ordered allocator
   int* pinned = nullptr;         // 256 bytes of pinned host memory for small device reads
+  // autotuner: launch shapes chosen by measurement (its_tune.cuh)
+  int autotune = 0;                  // 0: built-in defaults, 1: measure candidates on first use
+  std::map<std::string, int> tuned;  // shape key -> chosen candidate
+  std::string tuneCache;             // file the choices persist to ("" = none)
 };
 
 namespace its {

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "its_mc.cuh"
+#include "its_tune.cuh"
 #include "its_op.cuh"
 
 namespace its {
@@ -161,9 +162,7 @@ __device__ inline double fieldAt(const EvalParams& P, const double* __restrict__
 // the result is bit-identical, without the per-point lattice lookups (bitmap, rank, vertex
 // position) that made the point-wise kernel L2-bound. Depths whose corner box exceeds the
 // tile (grids much coarser than the octree) fall back to the point-wise lookups.
-constexpr int kBrickX = 32, kBrickY = 4, kBrickThreads = 256, kZPer = 4;
-constexpr int kBrickZ = (kBrickThreads / (kBrickX * kBrickY)) * kZPer;  // 8
-constexpr int kTileCap = 640;
+constexpr int kBrickThreads = 256, kTileCap = 640;
 
 // Field on the (R+1)^3 lattice in bricks of 32 x 4 x 8 points; a thread evaluates a column of
 // 4 points along z. For each depth the brick's points fall in a small box of cells; the
@@ -189,10 +188,11 @@ __device__ __forceinline__ T hatT(T x, T p, T w, T wi) {
   }
 }
 
-template <typename T>
+template <typename T, int kBrickX, int kBrickY, int kZPer>
 __global__ void __launch_bounds__(kBrickThreads, 2)
     kEvalGridBricks(const __grid_constant__ EvalParams P, const double* __restrict__ lambda, double3 o, double3 vs,
                     int R, T* __restrict__ field) {
+  constexpr int kBrickZ = (kBrickThreads / (kBrickX * kBrickY)) * kZPer;
   __shared__ T tLam[kTileCap], tPx[kTileCap], tPy[kTileCap], tPz[kTileCap];
   __shared__ unsigned char tHas[kTileCap];
   __shared__ int64_t box[6];  // first and last cell per axis at the current depth
@@ -320,19 +320,19 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
 // bytes and reduces the vertex counts per block. The block sums are scanned (kScanSpine);
 // Emit re-reads only the case bytes, scans the counts inside the block and writes the
 // triangle vertices of the non-empty voxels in voxel order, as the reference's compaction does.
-template <typename T>
+template <typename T, int ITEMS>
 __global__ void __launch_bounds__(kScanThreads) kMcClassify(const T* __restrict__ field, int R, double iso,
                                                              uint8_t* __restrict__ cube,
                                                              unsigned long long* __restrict__ blockSums) {
   const int64_t nvox = (int64_t)R * R * R, M = (int64_t)R + 1;
-  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  const int64_t base = (int64_t)blockIdx.x * (kScanThreads * ITEMS) + (int64_t)threadIdx.x * ITEMS;
   unsigned long long cnt = 0;
   if (base < nvox) {
     int64_t x, y, z;
     voxelXYZ(base, R, x, y, z);
     double a = 0, b = 0, c = 0, d = 0;  // column x: (y,z) (y+1,z) (y,z+1) (y+1,z+1)
     bool have = false;
-    for (int j = 0; j < kScanItems && base + j < nvox; ++j) {
+    for (int j = 0; j < ITEMS && base + j < nvox; ++j) {
       const int64_t r0 = (z * M + y) * M, r1 = (z * M + y + 1) * M, r2 = ((z + 1) * M + y) * M,
                     r3 = ((z + 1) * M + y + 1) * M;
       if (!have) {
@@ -369,28 +369,61 @@ __global__ void __launch_bounds__(kScanThreads) kMcClassify(const T* __restrict_
   if (threadIdx.x == 0) blockSums[blockIdx.x] = total;
 }
 
-template <typename T>
+template <typename T, int ITEMS>
 __global__ void __launch_bounds__(kScanThreads) kMcEmit(McCaseT<T> mc, double3 o, double3 vs,
                                                          const uint8_t* __restrict__ cube,
                                                          const unsigned long long* __restrict__ blockOffsets,
                                                          double* __restrict__ tri, unsigned long long capacity) {
   const int64_t nvox = (int64_t)mc.R * mc.R * mc.R;
-  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
-  unsigned char ci[kScanItems];
+  const int64_t base = (int64_t)blockIdx.x * (kScanThreads * ITEMS) + (int64_t)threadIdx.x * ITEMS;
+  unsigned char ci[ITEMS];
   unsigned long long cnt = 0;
 #pragma unroll
-  for (int j = 0; j < kScanItems; ++j) {
+  for (int j = 0; j < ITEMS; ++j) {
     ci[j] = base + j < nvox ? cube[base + j] : 0;
     cnt += cMcCase[ci[j]] & 15ull;
   }
   unsigned long long total;
   unsigned long long run = blockExclusiveScan<unsigned long long>(cnt, total) + blockOffsets[blockIdx.x];
   if (!total || !tri) return;
-  for (int j = 0; j < kScanItems; ++j) {
+  for (int j = 0; j < ITEMS; ++j) {
     const unsigned long long c = cMcCase[ci[j]] & 15ull;
     if (c) mcEmitVoxel(mc, o, vs, tri, capacity, base + j, ci[j], run, c);
     run += c;
   }
+}
+
+// Dense-field launch shapes (bricks of BX x BY x BZ points, a thread per column of ZPER
+// points); every shape computes the same bits, the autotuner picks the fastest.
+template <typename T, int BX, int BY, int ZPER>
+static its_status launchBricks(its_ctx* ctx, const EvalParams& P, const double* lam, double3 o, double3 vs, int res,
+                               T* field) {
+  constexpr int BZ = (kBrickThreads / (BX * BY)) * ZPER;
+  const int64_t M = (int64_t)res + 1;
+  const dim3 grid((unsigned)((M + BX - 1) / BX), (unsigned)((M + BY - 1) / BY), (unsigned)((M + BZ - 1) / BZ));
+  kEvalGridBricks<T, BX, BY, ZPER><<<grid, kBrickThreads, 0, ctx->stream>>>(P, lam, o, vs, res, field);
+  ITS_LAUNCHED(ctx);
+  return ITS_OK;
+}
+
+template <typename T>
+static its_status evalGridTuned(its_ctx* ctx, const SvoDevice& d, const double* lam, double3 o, double3 vs, int res,
+                                T* field) {
+  const EvalParams P = evalParams(d);
+  auto run = [&](int i) -> its_status {
+    switch (i) {
+      case 1: return launchBricks<T, 32, 8, 2>(ctx, P, lam, o, vs, res, field);
+      case 2: return launchBricks<T, 64, 4, 2>(ctx, P, lam, o, vs, res, field);
+      case 3: return launchBricks<T, 16, 4, 4>(ctx, P, lam, o, vs, res, field);
+      default: return launchBricks<T, 32, 4, 4>(ctx, P, lam, o, vs, res, field);
+    }
+  };
+  const std::string key = std::string("eval_grid/") + (sizeof(T) == 8 ? "f64" : "f32") + "/grid=" +
+                          std::to_string(res) + "/octree=" + std::to_string(d.res) + "/depth=" + std::to_string(d.depth);
+  int choice = 0;
+  its_status st = tuneChoice(ctx, key, 4, 0, run, &choice);
+  if (st != ITS_OK) return st;
+  return run(choice);
 }
 
 // divRn against the hardware-correct quotient (a test hook: out[i] = 1 where they differ).
@@ -401,6 +434,74 @@ __global__ void kCheckDivRn(const double* __restrict__ a, const double* __restri
   const double y = 1.0 / b[i];
   const double q1 = divRn(a[i], b[i], y), q2 = a[i] / b[i];
   differ[i] = __double_as_longlong(q1) != __double_as_longlong(q2);
+}
+
+// ThinShells::getPointValGradient (ThinShells.cpp:1800-1866): a point outside the model box
+// moves halfway towards its previous position until inside (at most 64 halvings; no move
+// without previous positions), then the field and its gradient over its fine node's chain,
+// with de_BaseFunction (BSpline.hpp:30-57) for the derivative factors.
+__device__ __forceinline__ double deHat1(double x, double p, double w) {
+  if (fabs(x - (p - w)) < 1e-9 || x < p - w || fabs(x - (p + w)) < 1e-9 || x > p + w) return 0.0;
+  if (x <= p) return 1 / w;
+  return -1 / w;
+}
+
+__global__ void kPointGradient(const __grid_constant__ EvalParams P, const double* __restrict__ lambda,
+                               const double* __restrict__ pts, const double* __restrict__ before, int64_t m, double3 lo,
+                               double3 hi, double* __restrict__ val, double* __restrict__ grad,
+                               uint8_t* __restrict__ missing) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  double px = pts[3 * i], py = pts[3 * i + 1], pz = pts[3 * i + 2];
+  if (before) {
+    const double bx = before[3 * i], by = before[3 * i + 1], bz = before[3 * i + 2];
+    for (int it = 0; it < 64; ++it) {
+      if (!(px < lo.x || py < lo.y || pz < lo.z || px > hi.x || py > hi.y || pz > hi.z)) break;
+      px = (px + bx) / 2.0;
+      py = (py + by) / 2.0;
+      pz = (pz + bz) / 2.0;
+    }
+  }
+  double sum = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+  bool found = false;
+  const int dx = (int)((px - P.g.x) / P.w0), dy = (int)((py - P.g.y) / P.w0), dz = (int)((pz - P.g.z) / P.w0);
+  if (dx >= 0 && dy >= 0 && dz >= 0 && dx < P.res && dy < P.res && dz < P.res) {
+    const uint32_t mc = mortonEncode((uint32_t)dx, (uint32_t)dy, (uint32_t)dz);
+    int64_t a = 0, b = P.fineCount;
+    while (a < b) {
+      const int64_t mid = (a + b) >> 1;
+      if (P.morton[mid] < mc) a = mid + 1;
+      else b = mid;
+    }
+    if (a < P.fineCount && P.morton[a] == mc) {
+      found = true;
+      uint32_t t = (uint32_t)a;
+      for (int d = 0; d < P.depth && t != kNone; ++d) {
+        uint32_t X, Y, Z;
+        mortonDecode(P.morton[t], X, Y, Z);
+        const double w = P.w0 * (double)(1u << d);
+        const double bx = latticePos(P.g.x, w, X), by = latticePos(P.g.y, w, Y), bz = latticePos(P.g.z, w, Z);
+        const LatticeIndex& L = P.lat[d];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
+          const double cx = ox ? bx + w : bx, cy = oy ? by + w : by, cz = oz ? bz + w : bz;
+          const double lam = lambda[latticeRank(L, ((X + ox) * L.M + (Y + oy)) * L.M + (Z + oz))];
+          sum += lam * hat3(cx, cy, cz, w, px, py, pz);
+          const double hx = hat1(px, cx, w), hy = hat1(py, cy, w), hz = hat1(pz, cz, w);
+          gx += lam * (deHat1(px, cx, w) * hy * hz);
+          gy += lam * (hx * deHat1(py, cy, w) * hz);
+          gz += lam * (hx * hy * deHat1(pz, cz, w));
+        }
+        t = P.parent[t];
+      }
+    }
+  }
+  val[i] = sum;
+  grad[3 * i] = gx;
+  grad[3 * i + 1] = gy;
+  grad[3 * i + 2] = gz;
+  if (missing) missing[i] = found ? 0 : 1;
 }
 
 // Point queries (ThinShells::multiPointQuery, ThinShells.cpp:1183-1420, CUDA branch
@@ -516,6 +617,31 @@ its_status its_point_query(its_svo* s, const double* lambda, const double* point
   return ITS_OK;
 }
 
+its_status its_point_value_gradient(its_svo* s, const double* lambda, const double* points, const double* before,
+                                   int64_t npoints, const double box_origin[3], const double box_end[3], double* values,
+                                   double* gradients, uint8_t* missing) {
+  if (!s || !lambda || npoints < 0 || (npoints && (!points || !values || !gradients)) || !box_origin || !box_end)
+    return ITS_ERR_INVALID;
+  its_ctx* ctx = s->ctx;
+  if (npoints == 0) return ITS_OK;
+  ITS_CU(ctx, cudaSetDevice(ctx->device));
+  InArg<double> L, P, B;
+  OutArg<double> Vo, G;
+  OutArg<uint8_t> Mi;
+  its_status st;
+  if ((st = L.stage(ctx, lambda, s->d.numVerts)) != ITS_OK || (st = P.stage(ctx, points, 3 * npoints)) != ITS_OK ||
+      (st = B.stage(ctx, before, before ? 3 * npoints : 0)) != ITS_OK || (st = Vo.stage(ctx, values, npoints)) != ITS_OK ||
+      (st = G.stage(ctx, gradients, 3 * npoints)) != ITS_OK || (st = Mi.stage(ctx, missing, npoints)) != ITS_OK)
+    return st;
+  kPointGradient<<<gridFor(npoints, 128), 128, 0, ctx->stream>>>(
+      evalParams(s->d), L.d, P.d, B.d, npoints, make_double3(box_origin[0], box_origin[1], box_origin[2]),
+      make_double3(box_end[0], box_end[1], box_end[2]), Vo.d, G.d, Mi.d);
+  ITS_LAUNCHED(ctx);
+  if ((st = Vo.finish(ctx)) != ITS_OK || (st = G.finish(ctx)) != ITS_OK || (st = Mi.finish(ctx)) != ITS_OK) return st;
+  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITS_OK;
+}
+
 its_status its_eval_grid(its_svo* s, const double* lambda, const double origin[3], const double width[3], int res,
                          double* field) {
   if (!s || !lambda || !origin || !width || !field || res < 1 || res > 2048) return ITS_ERR_INVALID;
@@ -529,11 +655,7 @@ its_status its_eval_grid(its_svo* s, const double* lambda, const double origin[3
   if ((st = F.stage(ctx, field, total)) != ITS_OK) return st;
   const double3 o = make_double3(origin[0], origin[1], origin[2]);
   const double3 vs = make_double3(width[0] / res, width[1] / res, width[2] / res);
-  (void)total;
-  const dim3 grid((unsigned)((M + kBrickX - 1) / kBrickX), (unsigned)((M + kBrickY - 1) / kBrickY),
-                  (unsigned)((M + kBrickZ - 1) / kBrickZ));
-  kEvalGridBricks<double><<<grid, kBrickThreads, 0, ctx->stream>>>(evalParams(s->d), L.d, o, vs, res, F.d);
-  ITS_LAUNCHED(ctx);
+  if ((st = evalGridTuned<double>(ctx, s->d, L.d, o, vs, res, F.d)) != ITS_OK) return st;
   if ((st = F.finish(ctx)) != ITS_OK) return st;
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   return ITS_OK;
@@ -552,10 +674,7 @@ its_status its_eval_grid_f32(its_svo* s, const double* lambda, const double orig
   if ((st = F.stage(ctx, field, total)) != ITS_OK) return st;
   const double3 o = make_double3(origin[0], origin[1], origin[2]);
   const double3 vs = make_double3(width[0] / res, width[1] / res, width[2] / res);
-  const dim3 grid((unsigned)((M + kBrickX - 1) / kBrickX), (unsigned)((M + kBrickY - 1) / kBrickY),
-                  (unsigned)((M + kBrickZ - 1) / kBrickZ));
-  kEvalGridBricks<float><<<grid, kBrickThreads, 0, ctx->stream>>>(evalParams(s->d), L.d, o, vs, res, F.d);
-  ITS_LAUNCHED(ctx);
+  if ((st = evalGridTuned<float>(ctx, s->d, L.d, o, vs, res, F.d)) != ITS_OK) return st;
   if ((st = F.finish(ctx)) != ITS_OK) return st;
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   return ITS_OK;
@@ -609,19 +728,42 @@ its_status marchingCubesT(its_ctx* ctx, const FT* field, int res, const double o
     if ((st = cubeTmp.alloc(ctx, nvox)) != ITS_OK) return st;
     cubeD = cubeTmp.p;
   }
-  const int64_t nb = scanBlocks(nvox);
+  // tile of 256 threads x ITEMS voxels; the autotuner picks ITEMS (same bits for every choice)
+  const int itemsOf[3] = {8, 16, 4};
+  const int64_t nbMax = (nvox + kScanThreads * 4 - 1) / (kScanThreads * 4);
   DevBuf<unsigned long long> sums, tot;
-  if ((st = sums.alloc(ctx, nb)) != ITS_OK || (st = tot.alloc(ctx, 1)) != ITS_OK) return st;
-  kMcClassify<FT><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(F.d, res, iso, cubeD, sums.p);
-  ITS_LAUNCHED(ctx);
-  kScanSpine<unsigned long long><<<1, kScanThreads, 0, ctx->stream>>>(sums.p, nb, tot.p);
-  ITS_LAUNCHED(ctx);
-  if (T.d) {
-    kMcEmit<FT><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(
-        mc, make_double3(origin[0], origin[1], origin[2]), make_double3(width[0] / res, width[1] / res, width[2] / res),
-        cubeD, sums.p, T.d, (unsigned long long)capacity);
+  if ((st = sums.alloc(ctx, nbMax)) != ITS_OK || (st = tot.alloc(ctx, 1)) != ITS_OK) return st;
+  const double3 o3 = make_double3(origin[0], origin[1], origin[2]);
+  const double3 v3 = make_double3(width[0] / res, width[1] / res, width[2] / res);
+  auto run = [&](int i) -> its_status {
+    const int items = itemsOf[i];
+    const int64_t nb = (nvox + kScanThreads * items - 1) / (kScanThreads * items);
+    if (items == 16)
+      kMcClassify<FT, 16><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(F.d, res, iso, cubeD, sums.p);
+    else if (items == 4)
+      kMcClassify<FT, 4><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(F.d, res, iso, cubeD, sums.p);
+    else
+      kMcClassify<FT, 8><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(F.d, res, iso, cubeD, sums.p);
     ITS_LAUNCHED(ctx);
-  }
+    kScanSpine<unsigned long long><<<1, kScanThreads, 0, ctx->stream>>>(sums.p, nb, tot.p);
+    ITS_LAUNCHED(ctx);
+    if (T.d) {
+      const unsigned long long cap = (unsigned long long)capacity;
+      if (items == 16)
+        kMcEmit<FT, 16><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(mc, o3, v3, cubeD, sums.p, T.d, cap);
+      else if (items == 4)
+        kMcEmit<FT, 4><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(mc, o3, v3, cubeD, sums.p, T.d, cap);
+      else
+        kMcEmit<FT, 8><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(mc, o3, v3, cubeD, sums.p, T.d, cap);
+      ITS_LAUNCHED(ctx);
+    }
+    return ITS_OK;
+  };
+  const std::string key = std::string("marching_cubes/") + (sizeof(FT) == 8 ? "f64" : "f32") + "/res=" +
+                          std::to_string(res) + (T.d ? "/soup" : "/cases");
+  int choice = 0;
+  if ((st = tuneChoice(ctx, key, 3, 0, run, &choice)) != ITS_OK) return st;
+  if ((st = run(choice)) != ITS_OK) return st;
   unsigned long long total = 0;
   if ((st = readScalar(ctx, tot.p, &total)) != ITS_OK) return st;
   *num_verts = (int64_t)total;

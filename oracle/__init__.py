@@ -55,6 +55,7 @@ def _declare(L):
         "orc_csr_free": (None, [vp]),
         "orc_cgls": (i32, [vp, vp, vp, dbl, i64, i32, vp]),
         "orc_exact_start": (None, [vp, vp, vp, vp, vp]),
+        "orc_point_gradient": (None, [vp, vp, vp, vp, i64, vp, vp, vp, vp, vp]),
         "orc_intersections": (vp, [vp, vp, i64, vp, i64]),
         "orc_points_count": (i64, [vp, vp]),
         "orc_points_get": (None, [vp, vp]),
@@ -179,6 +180,16 @@ class Svo:
         finally:
             lib().orc_csr_free(h)
         return rp, col, val
+
+    def point_gradient(self, lam, P, box_origin, box_end, before=None):
+        """Field, gradient and missing flags (ThinShells::getPointValGradient)."""
+        lam, P = _f64(lam), _f64(P)
+        m = P.shape[0]
+        val, grad, miss = np.zeros(m), np.zeros((m, 3)), np.zeros(m, np.uint8)
+        bo, be = _f64(box_origin), _f64(box_end)
+        bf = None if before is None else _f64(before)
+        lib().orc_point_gradient(self.h, _p(lam), _p(P), _p(bf), m, _p(bo), _p(be), _p(val), _p(grad), _p(miss))
+        return val, grad, miss
 
     def exact_start(self, b, shares=None):
         """Hierarchical-surplus exact solution of A lambda = b for this octree's operator

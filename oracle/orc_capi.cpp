@@ -125,6 +125,11 @@ void orc_exact_start(void* h, void* a, const double* b, const double* shares, do
   exactStart(*static_cast<Svo*>(h), *static_cast<Csr*>(a), b, shares, lambda);
 }
 
+void orc_point_gradient(void* h, const double* lambda, const double* P, const double* before, int64_t m,
+                        const double* boxOrigin, const double* boxEnd, double* val, double* grad, uint8_t* missing) {
+  pointValGradient(*static_cast<Svo*>(h), lambda, P, before, m, boxOrigin, boxEnd, val, grad, missing);
+}
+
 void* orc_intersections(void* h, const double* V, int64_t nv, const int32_t* F, int64_t nf) {
   Points* p = new Points;
   p->pts = intersections(*static_cast<Svo*>(h), V, nv, F, nf, &p->nEdge);

@@ -166,6 +166,12 @@ inline double baseFunction(double x, double p, double w) {
   if (x <= p) return 1 + (x - p) / w;
   return 1 - (x - p) / w;
 }
+// de_BaseFunction (BSpline.hpp:30-35): 1/w left of the node, -1/w right of it, 0 outside.
+inline double deBaseFunction(double x, double p, double w) {
+  if (std::fabs(x - (p - w)) < 1e-9 || x < p - w || std::fabs(x - (p + w)) < 1e-9 || x > p + w) return 0.0;
+  if (x <= p) return 1 / w;
+  return -1 / w;
+}
 inline double baseFunction4Point(const V3& p, double w, const V3& q) {
   double x = baseFunction(q.x, p.x, w);
   if (x <= 0.0) return 0.0;

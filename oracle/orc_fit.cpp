@@ -420,6 +420,61 @@ void evalPoints(const Svo& s, const double* lambda, const double* P, int64_t m, 
   }
 }
 
+void pointValGradient(const Svo& s, const double* lambda, const double* P, const double* before, int64_t m,
+                      const double boxOrigin[3], const double boxEnd[3], double* val, double* grad, uint8_t* missing) {
+  const std::vector<VertMap> vm = depthVert2Idx(s);
+  std::map<uint32_t, size_t> morton2Fine;
+  for (size_t i = 0; i < s.numFineNodes; ++i) morton2Fine.emplace(s.nodes[i].morton, i);
+  const double vw = s.nodes[0].width;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t i = 0; i < m; ++i) {
+    V3 p{P[3 * i], P[3 * i + 1], P[3 * i + 2]};
+    if (before) {
+      const V3 b{before[3 * i], before[3 * i + 1], before[3 * i + 2]};
+      for (int it = 0; it < 64; ++it) {
+        bool out = false;
+        for (int a = 0; a < 3; ++a) out = out || p[a] < boxOrigin[a] || p[a] > boxEnd[a];
+        if (!out) break;
+        for (int a = 0; a < 3; ++a) p[a] = (p[a] + b[a]) / 2.0;
+      }
+    }
+    int dis[3];
+    for (int a = 0; a < 3; ++a) dis[a] = (int)((p[a] - s.gridOrigin[a]) / vw);
+    val[i] = 0.0;
+    grad[3 * i] = grad[3 * i + 1] = grad[3 * i + 2] = 0.0;
+    const bool inGrid = dis[0] >= 0 && dis[1] >= 0 && dis[2] >= 0 && dis[0] < s.res && dis[1] < s.res && dis[2] < s.res;
+    auto it = inGrid ? morton2Fine.find(mortonEncode((uint16_t)dis[0], (uint16_t)dis[1], (uint16_t)dis[2]))
+                     : morton2Fine.end();
+    if (it == morton2Fine.end()) {
+      if (missing) missing[i] = 1;
+      continue;
+    }
+    if (missing) missing[i] = 0;
+    double sum = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+    uint32_t nodeIdx = (uint32_t)it->second;
+    int depth = 0;
+    while (depth < s.treeDepth && nodeIdx != kNone) {
+      const Node& nd = s.nodes[nodeIdx];
+      const double w = nd.width;
+      for (int k = 0; k < 8; ++k) {
+        const V3 c = cornerOf(nd, k);
+        const double lam = lambda[vm[depth].at(c)];
+        sum += lam * baseFunction4Point(c, w, p);
+        const double bx = baseFunction(p.x, c.x, w), by = baseFunction(p.y, c.y, w), bz = baseFunction(p.z, c.z, w);
+        gx += lam * (deBaseFunction(p.x, c.x, w) * by * bz);
+        gy += lam * (bx * deBaseFunction(p.y, c.y, w) * bz);
+        gz += lam * (bx * by * deBaseFunction(p.z, c.z, w));
+      }
+      nodeIdx = nd.parent;
+      ++depth;
+    }
+    val[i] = sum;
+    grad[3 * i] = gx;
+    grad[3 * i + 1] = gy;
+    grad[3 * i + 2] = gz;
+  }
+}
+
 // Brute-force field (CUDACompute.cu:435-510 semantics): sum over every corner vertex,
 // in index order; width = width of the vertex's owner node.
 void evalBrute(const Svo& s, const double* lambda, const double* P, int64_t m, double* out) {

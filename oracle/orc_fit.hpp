@@ -26,6 +26,11 @@ Csr transpose(const Csr& A);
 CglsReport cgls(const Csr& A, const Csr& T, const double* b, double* x, double tol, int64_t maxIters, int stop);
 void exactStart(const Svo& s, const Csr& A, const double* b, const double* shares, double* lambda);
 void evalPoints(const Svo& s, const double* lambda, const double* P, int64_t m, double* out, uint8_t* missing);
+// ThinShells::getPointValGradient (ThinShells.cpp:1800-1866): a point outside the box is moved
+// halfway towards its previous position until inside (before may be null: no move), then the
+// field and its gradient over its fine node's chain; missing as in evalPoints.
+void pointValGradient(const Svo& s, const double* lambda, const double* P, const double* before, int64_t m,
+                      const double boxOrigin[3], const double boxEnd[3], double* val, double* grad, uint8_t* missing);
 void evalBrute(const Svo& s, const double* lambda, const double* P, int64_t m, double* out);
 void evalGrid(const Svo& s, const double* lambda, const double origin[3], const double width[3], int R, double* out);
 void pointQuery(const Svo& s, const double* lambda, const double* P, int64_t m, const double boxOrigin[3],

@@ -58,3 +58,30 @@ def test_facade_matches_oracle(tmp_path):
     for side in ("inner", "outer"):
         obj = str(tmp_path / ("c0_%s.obj" % side))
         assert os.path.getsize(obj) > 0
+
+
+@pytest.mark.gpu
+def test_facade_learned_start_and_obj_io(tmp_path):
+    # OBJ input (readObj), the learned creatShell (an exact solution, residual at rounding
+    # level) and the welded OBJ output; iso levels equal the plain fit's to 1e-9 of the range
+    exe = _compile(tmp_path)
+    V, F = meshes.config_mesh("c0")
+    obj = str(tmp_path / "c0.obj")
+    with open(obj, "w") as f:
+        for v in V:
+            f.write("v %.17g %.17g %.17g\n" % tuple(v))
+        for t in F:
+            f.write("f %d/1 %d/1 %d/1\n" % tuple(t + 1))
+    plain = json.loads(subprocess.run([exe, obj, "32", str(tmp_path / "p")], check=True, capture_output=True,
+                                      text=True).stdout.strip().splitlines()[-1])
+    net = os.path.join(ROOT, "its_b200", "share_net.f32")
+    learned = json.loads(subprocess.run([exe, obj, "32", str(tmp_path / "l"), net], check=True, capture_output=True,
+                                        text=True).stdout.strip().splitlines()[-1])
+    assert learned["rel_residual"] <= 1e-13 and learned["iterations"] == 0
+    span = plain["outer"] - plain["inner"]
+    assert abs(learned["inner"] - plain["inner"]) <= 1e-6 * span and abs(learned["outer"] - plain["outer"]) <= 1e-6 * span
+    welded = [l.split() for l in open(str(tmp_path / "l_outer_welded.obj"))]
+    nv = sum(1 for l in welded if l and l[0] == "v")
+    faces = [l for l in welded if l and l[0] == "f"]
+    assert nv > 0 and len(faces) > 0 and nv < 3 * len(faces)  # shared vertices
+    assert max(int(i) for fc in faces for i in fc[1:]) == nv

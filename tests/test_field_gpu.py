@@ -178,3 +178,59 @@ def test_fp32_field_and_marching_cubes(ctx):
         corners = g[z:z + 2, y:y + 2, x:x + 2]
         assert np.abs(corners - iso).min() <= 4e-6 * scale
     assert len(diff) <= 1e-3 * R ** 3
+
+
+@pytest.mark.gpu
+def test_autotuner_changes_speed_not_bits(tmp_path):
+    # Tuned launches (brick shape of the dense field, marching-cubes tile) compute the same
+    # bits as the defaults; the choices are recorded and persist through the cache file.
+    from its_b200 import Context, Operator, Svo
+    V, F, o, w = prepared_mesh("c0")
+    outs = {}
+    cache = str(tmp_path / "tune.txt")
+    for mode in (0, 1, 2):
+        ctx = Context(0)
+        if mode:
+            ctx.set_autotune(True, cache)
+        svo = Svo(ctx, V, F, 32, o, w)
+        b = ctx.signed_distance(svo.vertices()[0], V, F)
+        lam = svo.exact_start(b)
+        field = svo.eval_grid(lam, o, w, 80)
+        cube, tri, n = ctx.marching_cubes(field, 80, o, w, float(np.median(b)))
+        outs[mode] = (field, cube, tri, ctx.autotune_choices())
+        ctx.close()
+    for mode in (1, 2):
+        assert np.array_equal(outs[mode][0], outs[0][0])
+        assert np.array_equal(outs[mode][1], outs[0][1]) and np.array_equal(outs[mode][2], outs[0][2])
+    choices = outs[1][3]
+    assert any(k.startswith("eval_grid/f64") for k in choices) and any(k.startswith("marching_cubes/f64") for k in choices)
+    assert outs[2][3] == choices  # read back from the cache file
+
+
+@pytest.mark.gpu
+def test_point_value_gradient_matches_oracle(ctx):
+    from its_b200 import Operator, Svo, uniform_bbox
+    V, F, o, w = prepared_mesh("c0")
+    ref = oracle.Svo(V, F, 32, o, w)
+    svo = Svo(ctx, V, F, 32, o, w)
+    b = oracle.signed_distance(ref.vertices()[0], V, F)
+    lam, _ = Operator(svo).solve(b, tol=1e-10, max_iters=1000)
+    bo, be, _ = uniform_bbox(V)
+    rng = np.random.default_rng(4)
+    P = np.vstack([V + rng.normal(0, 0.01, V.shape), bo + (be - bo) * rng.uniform(-0.3, 1.3, (2000, 3))])
+    before = V[rng.integers(0, len(V), len(P))]
+    for bf in (None, before):
+        v, g, miss = svo.point_gradient(lam, P, bo, be, bf)
+        v_r, g_r, miss_r = ref.point_gradient(lam, P, bo, be, bf)
+        assert np.array_equal(miss, miss_r) and np.array_equal(v, v_r) and np.array_equal(g, g_r)
+    # the gradient is the field's derivative: central differences inside fine cells
+    h = 1e-7
+    inside = np.nonzero(miss == 0)[0][:200]
+    for a in range(3):
+        e = np.zeros(3)
+        e[a] = h
+        fp, _, mp = svo.point_gradient(lam, P[inside] + e, bo, be)
+        fm, _, mm = svo.point_gradient(lam, P[inside] - e, bo, be)
+        ok = (mp == 0) & (mm == 0)
+        fd = (fp - fm) / (2 * h)
+        assert np.median(np.abs(fd[ok] - g[inside][ok, a])) <= 1e-5 * np.abs(g[inside]).max()
