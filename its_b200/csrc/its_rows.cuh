@@ -8,6 +8,7 @@
 //   * the diagonal (value 1);
 //   * for every ancestor of o, the non-zero hats of its 8 corners at v, with the corner
 //     positions origin (+ w) of that ancestor, exactly as the reference computes them.
+//     (An ancestor exists at every coarser depth: the level build keeps every parent.)
 // Columns are lattice ranks, so a row comes out sorted: chain < diagonal < ancestors, corners
 // in x-major order. The assembly writes these entries into CSR; the matrix-free kernels
 // (exact start, residual) consume them directly in the same order.
@@ -80,10 +81,14 @@ __device__ __forceinline__ void walkRow(const RowParams& P, int64_t r, int d, Vi
     visit((int32_t)latticeRank(P.lat[j], lj), 1.0);
   }
   visit((int32_t)r, 1.0);
-  uint32_t a = P.parent[P.vertOwner[r]];
-  for (int dd = d + 1; dd < P.depth && a != kNone; ++dd) {
-    uint32_t Xa, Ya, Za;
-    mortonDecode(P.morton[a], Xa, Ya, Za);
+  // The ancestors of the owner node: the octree's levels are O_{L+1} = O_L >> 3, so the
+  // ancestor k levels up has the owner's coordinates shifted right by k -- no walk along the
+  // parent links (a chain of dependent loads), the same nodes and the same arithmetic.
+  uint32_t Xo, Yo, Zo;
+  mortonDecode(P.morton[P.vertOwner[r]], Xo, Yo, Zo);
+  for (int dd = d + 1; dd < P.depth; ++dd) {
+    const int up = dd - d;
+    const uint32_t Xa = Xo >> up, Ya = Yo >> up, Za = Zo >> up;
     const double w = P.w0 * (double)(1u << dd);
     const double bx = latticePos(P.g.x, w, Xa), by = latticePos(P.g.y, w, Ya), bz = latticePos(P.g.z, w, Za);
     const LatticeIndex& L = P.lat[dd];
@@ -105,7 +110,6 @@ __device__ __forceinline__ void walkRow(const RowParams& P, int64_t r, int d, Vi
         }
       }
     }
-    a = P.parent[a];
   }
 }
 
