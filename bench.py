@@ -9,8 +9,8 @@ A step is one fit from the octree and right-hand side (resident in HBM) to coeff
 whose relative residual ||b - A lambda|| / ||b|| is at most 1e-6: the learned start (share
 features -> share network on the tensor cores -> exact start) checked by the matrix-free
 FP64 residual, with the plain LSCG from that start as the fallback. `value` is its time in
-ms (max over ranks); `e2e` is the same call through the C ABI with the mesh and right-hand
-side in pinned host memory and the coefficients read back every step. Beside it: the plain
+ms (max over ranks); `e2e` is the same call through the C ABI with the right-hand side in
+pinned host memory and the coefficients read back every step. Beside it: the plain
 FP64 LSCG from zero (assembly + CGLS, the reference's method) and the mixed-precision
 LSCG on the same octree, the field error of the learned fit against the FP64 LSCG, the
 learned fit's breakdown, the 256-mesh uneven batch (plain per-mesh LSCG vs one learned
@@ -192,7 +192,6 @@ def run_ours(args):
     b = ctx.signed_distance(pos, V, F)
     n = svo.num_verts
     b_dev = torch.from_numpy(b).cuda()
-    V_dev, F_dev = torch.from_numpy(np.ascontiguousarray(V)).cuda(), torch.from_numpy(np.ascontiguousarray(F)).cuda()
     lam_dev = torch.empty_like(b_dev)
     params, norm = sharenet.load()
     net = ShareNet(ctx, batch=65536, params=params)
@@ -201,8 +200,8 @@ def run_ours(args):
     # ---- the headline fit: learned start verified by the FP64 residual -------------------
     # shares from the network -> exact start -> ||b - A lambda|| / ||b|| (matrix-free, FP64);
     # the plain LSCG from that start is the fallback when the residual misses the tolerance.
-    def learned_step(b_in=b_dev, mesh=(V_dev, F_dev), out=lam_dev):
-        learned_start_batch([svo], net, [b_in], [mesh], norm, outs=[out])
+    def learned_step(b_in=b_dev, out=lam_dev):
+        learned_start_batch([svo], net, [b_in], norm, outs=[out])
         rel = fit_residual_batch([svo], [b_in], [out])[0]
         if rel > wl["tol"]:
             op = Operator(svo)
@@ -260,10 +259,10 @@ def run_ours(args):
 
     # ---- breakdown of the learned fit ----------------------------------------------------
     from its_b200.api import exact_start_batch
-    feats, ids = svo.share_features(b, V, F, norm[:128])
+    feats, ids = svo.share_features(b, norm[:128])
     feat_dev = torch.empty((feats.shape[0], 64), dtype=torch.float32, device="cuda")
     ids_dev = torch.empty(feats.shape[0], dtype=torch.int64, device="cuda")
-    t_features = timed(lambda: svo.share_features(b_dev, V_dev, F_dev, norm[:128], out=feat_dev, ids=ids_dev), 3)
+    t_features = timed(lambda: svo.share_features(b_dev, norm[:128], out=feat_dev, ids=ids_dev), 3)
     t_start = timed(lambda: exact_start_batch([svo], [b_dev], outs=[lam_dev]), 5)
     t_resid = timed(lambda: fit_residual_batch([svo], [b_dev], [lam_dev]), 5)
     feats_dev = torch.from_numpy(feats).cuda()
@@ -297,12 +296,10 @@ def run_ours(args):
     # ---- end to end through the C ABI: host mesh and rhs in, host coefficients out --------
     b_host = torch.from_numpy(b).pin_memory()
     lam_host = torch.empty(n, dtype=torch.float64).pin_memory()
-    V_host = torch.from_numpy(np.ascontiguousarray(V)).pin_memory()
-    F_host = torch.from_numpy(np.ascontiguousarray(F)).pin_memory()
-    b_np, lam_np, V_np, F_np = b_host.numpy(), lam_host.numpy(), V_host.numpy(), F_host.numpy()
+    b_np, lam_np = b_host.numpy(), lam_host.numpy()
 
     def e2e_step():
-        learned_step(b_np, (V_np, F_np), lam_np)
+        learned_step(b_np, lam_np)
 
     for _ in range(max(1, args.warmup // 2)):
         e2e_step()
@@ -423,7 +420,7 @@ def run_ours(args):
                                      "exact_start": round(t_start, 4), "residual": round(t_resid, 4),
                                      "rows": int(feats.shape[0])},
             "field_error": field,
-            "e2e": {"value": round(e2e_ms, 4), "unit": "ms", "h2d_bytes_per_step": int(8 * n + V.nbytes + F.nbytes),
+            "e2e": {"value": round(e2e_ms, 4), "unit": "ms", "h2d_bytes_per_step": 8 * n,
                     "d2h_bytes_per_step": 8 * n},
             "roofline": {"bound": "hbm", "kernel": "kSpmvBinned (%s), the plain LSCG's dominant kernel"
                          % ("A^T" if dom else "A"),
@@ -489,7 +486,7 @@ def run_batch(ctx, net, norm, timed, tol, world, rank, steps, max_ranks):
     from its_b200.api import fit_residual_batch, learned_start_batch
     mix = meshes.batch_meshes(256, 3)
     mine = lpt_shard([m["faces"] for m in mix], world)[rank]
-    svos, bs, mesh_dev, outs, boxes = [], [], [], [], []
+    svos, bs, outs, boxes = [], [], [], []
     for k in mine:
         m = mix[k]
         V = model_to_unit_cube(m["V"])
@@ -498,7 +495,6 @@ def run_batch(ctx, net, norm, timed, tol, world, rank, steps, max_ranks):
         boxes.append((np.ascontiguousarray(o), np.ascontiguousarray(w)))
         svos.append(s)
         bs.append(torch.from_numpy(ctx.signed_distance(s.vertices()[0], V, m["F"])).cuda())
-        mesh_dev.append((torch.from_numpy(V).cuda(), torch.from_numpy(np.ascontiguousarray(m["F"])).cuda()))
         outs.append(torch.empty_like(bs[-1]))
     its = []
 
@@ -513,7 +509,7 @@ def run_batch(ctx, net, norm, timed, tol, world, rank, steps, max_ranks):
     rel = []
 
     def learned():
-        learned_start_batch(svos, net, bs, mesh_dev, norm, outs=outs)
+        learned_start_batch(svos, net, bs, norm, outs=outs)
         rel[:] = list(fit_residual_batch(svos, bs, outs))
 
     plain()

@@ -93,8 +93,7 @@ class ThinShells {
       if (!in) throw Error(ITS_ERR_INVALID, "cannot read share network file " + shareNetFile);
       if (!mlp_) check(its_mlp_create(ctx_, 65536, &mlp_), ctx_, "its_mlp_create");
       check(its_mlp_set_params(mlp_, params.data()), ctx_, "its_mlp_set_params");
-      check(its_learned_start(svo_, mlp_, sdfVal_.data(), V_.data(), nv, F_.data(), nf, norm.data(), lambda_.data()),
-            ctx_, "learned start");
+      check(its_learned_start(svo_, mlp_, sdfVal_.data(), norm.data(), lambda_.data()), ctx_, "learned start");
       double rel = 0;
       check(its_fit_residual(svo_, sdfVal_.data(), lambda_.data(), &rel), ctx_, "residual");
       report_.rel_residual = rel;

@@ -299,24 +299,22 @@ its_status its_mlp_train(its_mlp* mlp, const float* features, const float* y, in
                          uint64_t seed, float* loss_curve);
 /* Features of the vertices coincident with a coarser corner (the shares of the exact start),
    64 per vertex: the signed distance, zero-share surplus values of the vertex's copies and
-   lattice neighbours, neighbour presence, depth, cell width, and the face samples in the
-   owner node's 27-neighbourhood (count, mean offset, mean normal, 1 - |mean normal|).
-   V, F: the mesh of the octree. norm (NULL or 128 values: mean[64], scale[64]) normalises
-   (f - mean) * scale. features == NULL: *count only; else capacity >= *count rows, and ids
-   (NULL or capacity entries) receives the vertex of each row (ascending). */
-its_status its_share_features(its_svo* svo, const double* b, const double* V, int64_t nv, const int32_t* F,
-                              int64_t nf, const float* norm, float* features, int64_t capacity, int64_t* ids,
-                              int64_t* count);
+   lattice neighbours, neighbour presence, depth, cell width, and the face samples of the
+   octree's mesh (summed per node at its_svo_build) in the owner node's 27-neighbourhood:
+   count, mean offset, mean normal, 1 - |mean normal|. norm (NULL or 128 values: mean[64],
+   scale[64]) normalises (f - mean) * scale. features == NULL: *count only; else capacity >=
+   *count rows, and ids (NULL or capacity entries) receives the vertex of each row
+   (ascending). */
+its_status its_share_features(its_svo* svo, const double* b, const float* norm, float* features, int64_t capacity,
+                              int64_t* ids, int64_t* count);
 /* Learned start: features, the share network, then its_exact_start with the predicted
    shares (prediction * norm[129] + norm[128]). norm: 130 values (input mean[64], input
    scale[64], output mean, output scale). lambda: an exact solution whose null-space part is
    the network's. */
-its_status its_learned_start(its_svo* svo, its_mlp* mlp, const double* b, const double* V, int64_t nv,
-                             const int32_t* F, int64_t nf, const float* norm, double* lambda);
-/* The same for count operators of one context (one network pass over all of them). */
+its_status its_learned_start(its_svo* svo, its_mlp* mlp, const double* b, const float* norm, double* lambda);
+/* The same for count octrees of one context (one network pass over all of them). */
 its_status its_learned_start_batch(its_svo* const* svos, int64_t count, its_mlp* mlp, const double* const* b,
-                                   const double* const* V, const int64_t* nv, const int32_t* const* F,
-                                   const int64_t* nf, const float* norm, double* const* lambda);
+                                   const float* norm, double* const* lambda);
 
 #ifdef __cplusplus
 }

@@ -76,9 +76,9 @@ SIGNATURES = {
     "its_mlp_train": (st, [vp, vp, vp, i64, i64, C.c_float, C.c_uint64, vp]),
     "its_fit_residual": (st, [vp, vp, vp, C.POINTER(dbl)]),
     "its_fit_residual_batch": (st, [vp, i64, vp, vp, vp]),
-    "its_share_features": (st, [vp, vp, vp, i64, vp, i64, vp, vp, i64, vp, C.POINTER(i64)]),
-    "its_learned_start": (st, [vp, vp, vp, vp, i64, vp, i64, vp, vp]),
-    "its_learned_start_batch": (st, [vp, i64, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "its_share_features": (st, [vp, vp, vp, vp, i64, vp, C.POINTER(i64)]),
+    "its_learned_start": (st, [vp, vp, vp, vp, vp]),
+    "its_learned_start_batch": (st, [vp, i64, vp, vp, vp, vp]),
     "its_eval_points": (st, [vp, vp, vp, i64, vp, vp]),
     "its_shell_iso_values": (st, [vp, vp, vp, i64, C.POINTER(dbl), C.POINTER(dbl), C.POINTER(i64)]),
     "its_eval_grid": (st, [vp, vp, vp, vp, i32, vp]),

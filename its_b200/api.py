@@ -219,22 +219,22 @@ class Svo:
         self.ctx.check(lib().its_fit_residual(self.h, _ptr(b), _ptr(lam), C.byref(rel)), "its_fit_residual")
         return rel.value
 
-    def share_features(self, b, V, F, norm=None, out=None, ids=None):
+    def share_features(self, b, norm=None, out=None, ids=None):
         """Features of the share network (its_share_features): (features n x 64, vertex ids).
 
         out / ids may be preallocated (numpy or torch CUDA) with enough rows."""
-        b, V, F = _f64(b), _f64(V), _i32(F)
+        b = _f64(b)
         nrm = None if norm is None else np.ascontiguousarray(norm, np.float32)
         cnt = C.c_int64(0)
         L = lib()
-        self.ctx.check(L.its_share_features(self.h, _ptr(b), _ptr(V), _n(V), _ptr(F), _n(F), _ptr(nrm), None, 0, None,
-                                            C.byref(cnt)), "its_share_features")
+        self.ctx.check(L.its_share_features(self.h, _ptr(b), _ptr(nrm), None, 0, None, C.byref(cnt)),
+                       "its_share_features")
         n = cnt.value
         feats = out if out is not None else np.zeros((max(n, 1), 64), np.float32)
         idv = ids if ids is not None else np.zeros(max(n, 1), np.int64)
         cap = int(feats.shape[0])
-        self.ctx.check(L.its_share_features(self.h, _ptr(b), _ptr(V), _n(V), _ptr(F), _n(F), _ptr(nrm), _ptr(feats),
-                                            cap, _ptr(idv), C.byref(cnt)), "its_share_features")
+        self.ctx.check(L.its_share_features(self.h, _ptr(b), _ptr(nrm), _ptr(feats), cap, _ptr(idv), C.byref(cnt)),
+                       "its_share_features")
         return feats[:n], idv[:n]
 
     def depth_counts(self):
@@ -453,23 +453,16 @@ def fit_residual_batch(svos, bs, lams):
     return rel
 
 
-def learned_start_batch(svos, net, bs, meshes, norm, outs=None):
-    """Learned starts (its_learned_start_batch): meshes is a list of (V, F) per octree."""
+def learned_start_batch(svos, net, bs, norm, outs=None):
+    """Learned starts of many octrees of one context (its_learned_start_batch)."""
     count = len(svos)
     bs = [_f64(b) for b in bs]
-    Vs = [_f64(V) for V, _ in meshes]
-    Fs = [_i32(F) for _, F in meshes]
     norm = np.ascontiguousarray(norm, np.float32)
     outs = outs if outs is not None else [np.zeros(s.num_verts) for s in svos]
     H = (C.c_void_p * count)(*[s.h.value for s in svos])
     B = (C.c_void_p * count)(*[_addr(b) for b in bs])
-    VV = (C.c_void_p * count)(*[_addr(v) for v in Vs])
-    FF = (C.c_void_p * count)(*[_addr(f) for f in Fs])
-    nv = np.array([_n(v) for v in Vs], np.int64)
-    nf = np.array([_n(f) for f in Fs], np.int64)
     X = (C.c_void_p * count)(*[_addr(x) for x in outs])
-    svos[0].ctx.check(lib().its_learned_start_batch(H, count, net.h, B, VV, _ptr(nv), FF, _ptr(nf), _ptr(norm), X),
-                      "its_learned_start_batch")
+    svos[0].ctx.check(lib().its_learned_start_batch(H, count, net.h, B, _ptr(norm), X), "its_learned_start_batch")
     return outs
 
 

@@ -290,22 +290,23 @@ its_status coincidentIds(its_ctx* ctx, const SvoDevice& d, int64_t* ids, int64_t
   return readScalar(ctx, tot.p, count);
 }
 
-// Features of the coincident vertices ids[0..count) (see the file comment).
-its_status shareFeatures(its_ctx* ctx, const SvoDevice& d, const double* b, const double* lam0, const double* V,
-                         int64_t nv, const int32_t* F, int64_t nf, const int64_t* ids, int64_t count,
-                         const float* norm, float* out) {
-  (void)nv;
+its_status nodeSampleStats(its_ctx* ctx, SvoDevice& d, const double* V, const int32_t* F, int64_t nf) {
   its_status st;
   const int64_t nn = d.numNodes;
-  DevBuf<double> cent, nrm, sp, sn;
-  DevBuf<float> cnt;
+  if ((st = devAlloc(ctx, (void**)&d.nodeSampleCnt, std::max<int64_t>(nn, 1) * 4)) != ITS_OK ||
+      (st = devAlloc(ctx, (void**)&d.nodeSamplePos, std::max<int64_t>(nn, 1) * 24)) != ITS_OK ||
+      (st = devAlloc(ctx, (void**)&d.nodeSampleNrm, std::max<int64_t>(nn, 1) * 24)) != ITS_OK)
+    return st;
+  ITS_CU(ctx, cudaMemsetAsync(d.nodeSampleCnt, 0, nn * 4, ctx->stream));
+  ITS_CU(ctx, cudaMemsetAsync(d.nodeSamplePos, 0, nn * 24, ctx->stream));
+  ITS_CU(ctx, cudaMemsetAsync(d.nodeSampleNrm, 0, nn * 24, ctx->stream));
+  if (nf <= 0 || nn <= 0) return ITS_OK;
+  DevBuf<double> cent, nrm;
   DevBuf<uint32_t> node, fid, sNode, sId, tk, tv;
   if ((st = cent.alloc(ctx, 3 * nf)) != ITS_OK || (st = nrm.alloc(ctx, 3 * nf)) != ITS_OK ||
       (st = node.alloc(ctx, nf)) != ITS_OK || (st = fid.alloc(ctx, nf)) != ITS_OK ||
       (st = sNode.alloc(ctx, nf)) != ITS_OK || (st = sId.alloc(ctx, nf)) != ITS_OK ||
-      (st = tk.alloc(ctx, nf)) != ITS_OK || (st = tv.alloc(ctx, nf)) != ITS_OK ||
-      (st = cnt.zeros(ctx, nn)) != ITS_OK || (st = sp.zeros(ctx, 3 * nn)) != ITS_OK ||
-      (st = sn.zeros(ctx, 3 * nn)) != ITS_OK)
+      (st = tk.alloc(ctx, nf)) != ITS_OK || (st = tv.alloc(ctx, nf)) != ITS_OK)
     return st;
   const int64_t fineCount = d.levelCount[0];
   kFaceSamples<<<gridFor(nf, 256), 256, 0, ctx->stream>>>(V, F, nf, make_double3(d.origin[0], d.origin[1], d.origin[2]),
@@ -316,7 +317,7 @@ its_status shareFeatures(its_ctx* ctx, const SvoDevice& d, const double* b, cons
   int bits = 1;
   while (bits < 32 && (1ll << bits) <= fineCount) ++bits;
   if ((st = radixSortPairs(ctx, node.p, fid.p, sNode.p, sId.p, tk.p, tv.p, nf, bits)) != ITS_OK) return st;
-  NodeStats S{cnt.p, sp.p, sn.p};
+  NodeStats S{d.nodeSampleCnt, d.nodeSamplePos, d.nodeSampleNrm};
   kFineSums<<<gridFor(nf, 256), 256, 0, ctx->stream>>>(sNode.p, sId.p, nf, fineCount, cent.p, nrm.p, S);
   ITS_LAUNCHED(ctx);
   for (int L = 1; L < d.depth; ++L) {
@@ -325,12 +326,19 @@ its_status shareFeatures(its_ctx* ctx, const SvoDevice& d, const double* b, cons
                                                                         d.nodeChild0, S);
     ITS_LAUNCHED(ctx);
   }
+  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));  // the sample scratch is freed on return
+  return ITS_OK;
+}
+
+// Features of the coincident vertices ids[0..count) (see the file comment).
+its_status shareFeatures(its_ctx* ctx, const SvoDevice& d, const double* b, const double* lam0, const int64_t* ids,
+                         int64_t count, const float* norm, float* out) {
   const FeatParams P = featParams(d);
+  NodeStats S{d.nodeSampleCnt, d.nodeSamplePos, d.nodeSampleNrm};
   if (count > 0) {
     kShareFeatures<<<gridFor(count, 128), 128, 0, ctx->stream>>>(P, ids, count, b, lam0, S, norm, out);
     ITS_LAUNCHED(ctx);
   }
-  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   return ITS_OK;
 }
 
@@ -357,21 +365,17 @@ extern "C" its_status its_mlp_forward(its_mlp* mlp, const float* features, int64
 
 extern "C" {
 
-its_status its_share_features(its_svo* svo, const double* b, const double* V, int64_t nv, const int32_t* F,
-                              int64_t nf, const float* norm, float* features, int64_t capacity, int64_t* ids,
-                              int64_t* count) {
-  if (!svo || !b || !V || !F || nv <= 0 || nf <= 0 || !count) return ITS_ERR_INVALID;
+its_status its_share_features(its_svo* svo, const double* b, const float* norm, float* features, int64_t capacity,
+                              int64_t* ids, int64_t* count) {
+  if (!svo || !b || !count) return ITS_ERR_INVALID;
   its_ctx* ctx = svo->ctx;
   ITS_CU(ctx, cudaSetDevice(ctx->device));
   const SvoDevice& d = svo->d;
   const int64_t n = d.numVerts;
   its_status st;
-  InArg<double> dV, db;
-  InArg<int32_t> dF;
+  InArg<double> db;
   InArg<float> dn;
-  if ((st = dV.stage(ctx, V, 3 * nv)) != ITS_OK || (st = dF.stage(ctx, F, 3 * nf)) != ITS_OK ||
-      (st = db.stage(ctx, b, n)) != ITS_OK || (st = dn.stage(ctx, norm, norm ? 2 * kFeat : 0)) != ITS_OK)
-    return st;
+  if ((st = db.stage(ctx, b, n)) != ITS_OK || (st = dn.stage(ctx, norm, norm ? 2 * kFeat : 0)) != ITS_OK) return st;
   DevBuf<int64_t> dIds;
   if ((st = dIds.alloc(ctx, n)) != ITS_OK) return st;
   int64_t cnt = 0;
@@ -386,23 +390,21 @@ its_status its_share_features(its_svo* svo, const double* b, const double* V, in
   if ((st = exactStart(ctx, &svo, 1, &bp, nullptr, &lp)) != ITS_OK) return st;
   OutArg<float> out;
   if ((st = out.stage(ctx, features, cnt * kFeat)) != ITS_OK) return st;
-  if ((st = shareFeatures(ctx, d, db.d, lam0.p, dV.d, nv, dF.d, nf, dIds.p, cnt, dn.d, out.d)) != ITS_OK) return st;
+  if ((st = shareFeatures(ctx, d, db.d, lam0.p, dIds.p, cnt, dn.d, out.d)) != ITS_OK) return st;
   if ((st = out.finish(ctx)) != ITS_OK) return st;
   if (ids) ITS_CU(ctx, cudaMemcpyAsync(ids, dIds.p, cnt * 8, cudaMemcpyDefault, ctx->stream));
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   return ITS_OK;
 }
 
-its_status its_learned_start_batch(its_svo* const* ops, int64_t count, its_mlp* mlp, const double* const* b,
-                                   const double* const* V, const int64_t* nv, const int32_t* const* F,
-                                   const int64_t* nf, const float* norm, double* const* lambda) {
-  if (!ops || count <= 0 || !mlp || !b || !V || !nv || !F || !nf || !norm || !lambda) return ITS_ERR_INVALID;
-  its_ctx* ctx = ops[0] ? ops[0]->ctx : nullptr;
+its_status its_learned_start_batch(its_svo* const* svos, int64_t count, its_mlp* mlp, const double* const* b,
+                                   const float* norm, double* const* lambda) {
+  if (!svos || count <= 0 || !mlp || !b || !norm || !lambda) return ITS_ERR_INVALID;
+  its_ctx* ctx = svos[0] ? svos[0]->ctx : nullptr;
   if (!ctx) return ITS_ERR_INVALID;
   for (int64_t m = 0; m < count; ++m)
-    if (!ops[m] || ops[m]->ctx != ctx || !b[m] || !V[m] || !F[m] || !lambda[m] || nv[m] <= 0 ||
-        nf[m] <= 0)
-      return setError(ctx, ITS_ERR_INVALID, "its_learned_start: bad operator or mesh");
+    if (!svos[m] || svos[m]->ctx != ctx || !b[m] || !lambda[m])
+      return setError(ctx, ITS_ERR_INVALID, "its_learned_start: bad octree or vector");
   ITS_CU(ctx, cudaSetDevice(ctx->device));
   its_status st;
   // host norm: input mean[64], input scale[64], output mean, output scale
@@ -412,8 +414,7 @@ its_status its_learned_start_batch(its_svo* const* ops, int64_t count, its_mlp* 
   DevBuf<float> dNorm;
   if ((st = dNorm.alloc(ctx, 2 * kFeat)) != ITS_OK) return st;
   ITS_CU(ctx, cudaMemcpyAsync(dNorm.p, hn, 2 * kFeat * 4, cudaMemcpyHostToDevice, ctx->stream));
-  std::vector<InArg<double>> B(count), dV(count);
-  std::vector<InArg<int32_t>> dF(count);
+  std::vector<InArg<double>> B(count);
   std::vector<OutArg<double>> L(count);
   std::vector<DevBuf<double>> lam0(count), shares(count);
   std::vector<DevBuf<int64_t>> ids(count);
@@ -422,9 +423,8 @@ its_status its_learned_start_batch(its_svo* const* ops, int64_t count, its_mlp* 
   std::vector<int64_t> cnt(count);
   int64_t total = 0;
   for (int64_t m = 0; m < count; ++m) {
-    const int64_t n = ops[m]->d.numVerts;
-    if ((st = B[m].stage(ctx, b[m], n)) != ITS_OK || (st = dV[m].stage(ctx, V[m], 3 * nv[m])) != ITS_OK ||
-        (st = dF[m].stage(ctx, F[m], 3 * nf[m])) != ITS_OK || (st = L[m].stage(ctx, lambda[m], n)) != ITS_OK ||
+    const int64_t n = svos[m]->d.numVerts;
+    if ((st = B[m].stage(ctx, b[m], n)) != ITS_OK || (st = L[m].stage(ctx, lambda[m], n)) != ITS_OK ||
         (st = lam0[m].alloc(ctx, n)) != ITS_OK || (st = shares[m].alloc(ctx, n)) != ITS_OK ||
         (st = ids[m].alloc(ctx, n)) != ITS_OK)
       return st;
@@ -432,19 +432,18 @@ its_status its_learned_start_batch(its_svo* const* ops, int64_t count, its_mlp* 
     l0[m] = lam0[m].p;
     lp[m] = L[m].d;
     sp[m] = shares[m].p;
-    if ((st = coincidentIds(ctx, ops[m]->d, ids[m].p, &cnt[m])) != ITS_OK) return st;
+    if ((st = coincidentIds(ctx, svos[m]->d, ids[m].p, &cnt[m])) != ITS_OK) return st;
     total += cnt[m];
   }
   // zero-share starts (features), features of every mesh into one array, one network pass
-  if ((st = exactStart(ctx, ops, count, bp.data(), nullptr, l0.data())) != ITS_OK) return st;
+  if ((st = exactStart(ctx, svos, count, bp.data(), nullptr, l0.data())) != ITS_OK) return st;
   DevBuf<float> feat, pred;
   if ((st = feat.alloc(ctx, std::max<int64_t>(total, 1) * kFeat)) != ITS_OK ||
       (st = pred.alloc(ctx, std::max<int64_t>(total, 1))) != ITS_OK)
     return st;
   int64_t off = 0;
   for (int64_t m = 0; m < count; ++m) {
-    if ((st = shareFeatures(ctx, ops[m]->d, bp[m], l0[m], dV[m].d, nv[m], dF[m].d, nf[m], ids[m].p, cnt[m],
-                            dNorm.p, feat.p + off * kFeat)) != ITS_OK)
+    if ((st = shareFeatures(ctx, svos[m]->d, bp[m], l0[m], ids[m].p, cnt[m], dNorm.p, feat.p + off * kFeat)) != ITS_OK)
       return st;
     off += cnt[m];
   }
@@ -452,20 +451,19 @@ its_status its_learned_start_batch(its_svo* const* ops, int64_t count, its_mlp* 
   off = 0;
   for (int64_t m = 0; m < count; ++m) {
     if ((st = scatterShares(ctx, ids[m].p, cnt[m], pred.p + off, hn[2 * kFeat + 1], hn[2 * kFeat], shares[m].p,
-                            ops[m]->d.numVerts)) != ITS_OK)
+                            svos[m]->d.numVerts)) != ITS_OK)
       return st;
     off += cnt[m];
   }
-  if ((st = exactStart(ctx, ops, count, bp.data(), sp.data(), lp.data())) != ITS_OK) return st;
+  if ((st = exactStart(ctx, svos, count, bp.data(), sp.data(), lp.data())) != ITS_OK) return st;
   for (int64_t m = 0; m < count; ++m)
     if ((st = L[m].finish(ctx)) != ITS_OK) return st;
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   return ITS_OK;
 }
 
-its_status its_learned_start(its_svo* svo, its_mlp* mlp, const double* b, const double* V, int64_t nv,
-                             const int32_t* F, int64_t nf, const float* norm, double* lambda) {
-  return its_learned_start_batch(&svo, 1, mlp, &b, &V, &nv, &F, &nf, norm, &lambda);
+its_status its_learned_start(its_svo* svo, its_mlp* mlp, const double* b, const float* norm, double* lambda) {
+  return its_learned_start_batch(&svo, 1, mlp, &b, norm, &lambda);
 }
 
 }  // extern "C"

@@ -327,9 +327,34 @@ __global__ void __launch_bounds__(kScanThreads) kMcClassify(const T* __restrict_
   const int64_t nvox = (int64_t)R * R * R, M = (int64_t)R + 1;
   const int64_t base = (int64_t)blockIdx.x * (kScanThreads * ITEMS) + (int64_t)threadIdx.x * ITEMS;
   unsigned long long cnt = 0;
-  if (base < nvox) {
-    int64_t x, y, z;
-    voxelXYZ(base, R, x, y, z);
+  int64_t x = 0, y = 0, z = 0;
+  if (base < nvox) voxelXYZ(base, R, x, y, z);
+  if (base + ITEMS <= nvox && x + ITEMS <= R) {
+    // the run stays in one row: all 4 x (ITEMS + 1) corner values are loaded up front
+    const int64_t r0 = (z * M + y) * M + x, r1 = (z * M + y + 1) * M + x, r2 = ((z + 1) * M + y) * M + x,
+                  r3 = ((z + 1) * M + y + 1) * M + x;
+    double fa[ITEMS + 1], fb[ITEMS + 1], fc[ITEMS + 1], fd[ITEMS + 1];
+#pragma unroll
+    for (int j = 0; j <= ITEMS; ++j) {
+      fa[j] = (double)field[r0 + j];
+      fb[j] = (double)field[r1 + j];
+      fc[j] = (double)field[r2 + j];
+      fd[j] = (double)field[r3 + j];
+    }
+    unsigned long long packed = 0;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+      const unsigned ci = (unsigned)(fa[j] < iso) | (unsigned)(fb[j] < iso) << 1 | (unsigned)(fb[j + 1] < iso) << 2 |
+                          (unsigned)(fa[j + 1] < iso) << 3 | (unsigned)(fc[j] < iso) << 4 |
+                          (unsigned)(fd[j] < iso) << 5 | (unsigned)(fd[j + 1] < iso) << 6 |
+                          (unsigned)(fc[j + 1] < iso) << 7;
+      cnt += cMcCase[ci] & 15ull;
+      packed |= (unsigned long long)ci << (8 * (j & 7));
+      if (ITEMS != 8 || (((uintptr_t)(cube + base)) & 7u)) cube[base + j] = (uint8_t)ci;
+    }
+    // one 8-byte store when the caller's buffer allows it (base is a multiple of 8)
+    if (ITEMS == 8 && !(((uintptr_t)(cube + base)) & 7u)) *(unsigned long long*)(cube + base) = packed;
+  } else if (base < nvox) {
     double a = 0, b = 0, c = 0, d = 0;  // column x: (y,z) (y+1,z) (y,z+1) (y+1,z+1)
     bool have = false;
     for (int j = 0; j < ITEMS && base + j < nvox; ++j) {

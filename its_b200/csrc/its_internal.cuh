@@ -126,6 +126,10 @@ struct SvoDevice {
   uint32_t* edgeKey = nullptr;
   uint32_t* edgeOwner = nullptr;
   uint64_t* fineOcc = nullptr;     // res^3-bit Morton bitset of depth-0 nodes
+  // face samples (centroids, unit normals) summed per node, finest depth first
+  float* nodeSampleCnt = nullptr;  // per node
+  double* nodeSamplePos = nullptr; // 3 per node: sum of centroids
+  double* nodeSampleNrm = nullptr; // 3 per node: sum of unit normals
   LatticeIndex lattice(int d) const {
     LatticeIndex L;
     L.bits = vbits[d];

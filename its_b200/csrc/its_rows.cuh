@@ -28,6 +28,7 @@ struct RowParams {
   const uint32_t* vertLin;
   const uint32_t* vertOwner;
   const double* vertPos;
+  double winv[kMaxDepth];  // RN(1 / w_d): the hat quotients by divRn (bit-identical, no division)
 };
 
 inline RowParams rowParams(const SvoDevice& d) {
@@ -42,6 +43,7 @@ inline RowParams rowParams(const SvoDevice& d) {
   P.vertLin = d.vertLin;
   P.vertOwner = d.vertOwner;
   P.vertPos = d.vertPos;
+  for (int L = 0; L < kMaxDepth; ++L) P.winv[L] = 1.0 / (P.w0 * (double)(1u << L));
   return P;
 }
 
@@ -89,20 +91,20 @@ __device__ __forceinline__ void walkRow(const RowParams& P, int64_t r, int d, Vi
   for (int dd = d + 1; dd < P.depth; ++dd) {
     const int up = dd - d;
     const uint32_t Xa = Xo >> up, Ya = Yo >> up, Za = Zo >> up;
-    const double w = P.w0 * (double)(1u << dd);
+    const double w = P.w0 * (double)(1u << dd), wi = P.winv[dd];
     const double bx = latticePos(P.g.x, w, Xa), by = latticePos(P.g.y, w, Ya), bz = latticePos(P.g.z, w, Za);
     const LatticeIndex& L = P.lat[dd];
 #pragma unroll
     for (int ox = 0; ox < 2; ++ox) {
-      const double hx = hat1(qx, ox ? bx + w : bx, w);
+      const double hx = hat1r(qx, ox ? bx + w : bx, w, wi);
       if (hx <= 0.0) continue;
 #pragma unroll
       for (int oy = 0; oy < 2; ++oy) {
-        const double hy = hat1(qy, oy ? by + w : by, w);
+        const double hy = hat1r(qy, oy ? by + w : by, w, wi);
         if (hy <= 0.0) continue;
 #pragma unroll
         for (int oz = 0; oz < 2; ++oz) {
-          const double hz = hat1(qz, oz ? bz + w : bz, w);
+          const double hz = hat1r(qz, oz ? bz + w : bz, w, wi);
           if (hz <= 0.0) continue;
           const double v = hx * hy * hz;
           if (v == 0.0) continue;

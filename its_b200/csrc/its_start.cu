@@ -84,7 +84,7 @@ __global__ void kStartLevel(const RowSeg* __restrict__ segs, const int64_t* __re
 }
 
 constexpr int kResThreads = 256;
-constexpr int64_t kResChunk = 1024;  // rows per block: enough blocks for one mesh to fill the GPU
+constexpr int64_t kResChunk = 256;  // rows per block (one per thread): enough blocks to fill the GPU
 
 // ||b - A lambda||^2 and ||b||^2 of one chunk of rows (segments = chunks, one block each).
 __global__ void __launch_bounds__(kResThreads) kResidualChunks(const RowSeg* __restrict__ segs, double* __restrict__ part) {

@@ -308,7 +308,8 @@ static void svoRelease(its_svo* s) {
   its_ctx* c = s->ctx;
   SvoDevice& d = s->d;
   void* ptrs[] = {d.voxels, d.nodeMorton, d.nodeParent, d.nodeChild0, d.nodeLeaf, d.nodeNb, d.vertLin,
-                  d.vertOwner, d.vertPos, d.ebits, d.erank, d.edgeKey, d.edgeOwner, d.fineOcc};
+                  d.vertOwner, d.vertPos, d.ebits, d.erank, d.edgeKey, d.edgeOwner, d.fineOcc,
+                  d.nodeSampleCnt, d.nodeSamplePos, d.nodeSampleNrm};
   for (void* p : ptrs) devFree(c, p);
   for (int i = 0; i < kMaxDepth; ++i) { devFree(c, d.vbits[i]); devFree(c, d.vrank[i]); }
   d = SvoDevice();
@@ -508,6 +509,8 @@ its_status svoBuild(its_ctx* ctx, const double* dV, int64_t nv, const int32_t* d
     kMarkFine<<<gridFor(nf0, 256), 256, 0, ctx->stream>>>(nf0, d.nodeMorton, (unsigned long long*)d.fineOcc);
     ITS_LAUNCHED(ctx);
   }
+  // per-node sums of the face samples (features of the share network)
+  if ((st = nodeSampleStats(ctx, d, dV, dF, nf)) != ITS_OK) return st;
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   return ITS_OK;
 }

@@ -12,4 +12,7 @@ namespace its {
 its_status validateMesh(its_ctx* ctx, const double* dV, int64_t nv, const int32_t* dF, int64_t nf);
 its_status svoBuild(its_ctx* ctx, const double* dV, int64_t nv, const int32_t* dF, int64_t nf, int res,
                     const double origin[3], const double width[3], its_svo* s);
+// Face samples (centroid, unit normal) summed per fine node in face order, then per coarser
+// node over its 8 children in order, into d.nodeSample* (its_features.cu).
+its_status nodeSampleStats(its_ctx* ctx, SvoDevice& d, const double* dV, const int32_t* dF, int64_t nf);
 }  // namespace its

@@ -80,7 +80,7 @@ def dataset(ctx, meshes, log=None):
     for k, m in enumerate(meshes):
         svo, V, b, _, _ = prepare(ctx, m)
         x, rep = min_norm_fit(svo, b)
-        f, ids = svo.share_features(b, V, m["F"])
+        f, ids = svo.share_features(b)
         feats.append(f)
         targets.append(x[ids].astype(np.float32))
         svo.close()
@@ -130,7 +130,7 @@ def evaluate(ctx, net, norm, meshes, grid=64):
         svo, V, b, o, w = prepare(ctx, m)
         x, rep = min_norm_fit(svo, b)
         zero = svo.exact_start(b)
-        learned = learned_start_batch([svo], net, [b], [(V, m["F"])], norm)[0]
+        learned = learned_start_batch([svo], net, [b], norm)[0]
         g = svo.eval_grid(x, o, w, grid)
         scale = float(np.abs(b).max())
         r = dict(faces=m["faces"], res=m["res"], kind=m["kind"], lscg_iterations=rep["iterations"],

@@ -26,7 +26,7 @@ def test_share_features_match_oracle(ctx, name, kw, res):
     b = oracle.signed_distance(ref.vertices()[0], V, F)
     lam0 = ref.exact_start(b)
     f_ref, ids_ref = ofeat.share_features(ref, b, V, F, lam0)
-    f_gpu, ids_gpu = gpu.share_features(b, V, F)
+    f_gpu, ids_gpu = gpu.share_features(b)
     assert np.array_equal(ids_gpu, ids_ref) and len(ids_ref) > 0
     scale = np.maximum(np.abs(f_ref).max(0), 1e-30)
     err = (np.abs(f_gpu - f_ref) / scale).max(0)
@@ -34,7 +34,7 @@ def test_share_features_match_oracle(ctx, name, kw, res):
     # normalisation is (f - mean) * scale
     rng = np.random.default_rng(0)
     norm = np.concatenate([rng.standard_normal(64), rng.uniform(0.5, 2, 64)]).astype(np.float32)
-    f_n, _ = gpu.share_features(b, V, F, norm)
+    f_n, _ = gpu.share_features(b, norm)
     assert np.allclose(f_n, (f_gpu - norm[:64]) * norm[64:], rtol=1e-6, atol=1e-6)
 
 
@@ -52,9 +52,9 @@ def test_learned_start_is_exact_start_with_predicted_shares(ctx):
         svos.append(s)
         bs.append(ctx.signed_distance(s.vertices()[0], V, F))
         meshes.append((V, F))
-    outs = learned_start_batch(svos, net, bs, meshes, norm)
+    outs = learned_start_batch(svos, net, bs, norm)
     for s, b, (V, F), lam in zip(svos, bs, meshes, outs):
-        feats, ids = s.share_features(b, V, F, norm[:128])
+        feats, ids = s.share_features(b, norm[:128])
         shares = np.zeros(s.num_verts)
         shares[ids] = net.forward(feats).astype(np.float64) * float(norm[129]) + float(norm[128])
         assert np.array_equal(lam, s.exact_start(b, shares))
@@ -81,7 +81,7 @@ def test_trained_network_gain_on_held_out_meshes(ctx):
         op = Operator(svo)
         _, plain = op.solve(b, tol=1e-6, stop_rule=STOP_RESIDUAL)
         op.close()
-        learned = learned_start_batch([svo], net, [b], [(V, m["F"])], norm)[0]
+        learned = learned_start_batch([svo], net, [b], norm)[0]
         zero = svo.exact_start(b)
         assert svo.residual(b, learned) <= 1e-13 and plain["iterations"] >= 10
         g = svo.eval_grid(x, o, w, 48)
