@@ -289,7 +289,10 @@ int64_t its_mlp_num_params(void);
 /* Loads parameters and resets the Adam state. */
 its_status its_mlp_set_params(its_mlp* mlp, const float* params);
 its_status its_mlp_get_params(its_mlp* mlp, float* params);
+/* Predictions: one persistent kernel for all layers (weights and activations in shared memory). */
 its_status its_mlp_forward(its_mlp* mlp, const float* features, int64_t n, float* out);
+/* The same predictions layer by layer through the training kernels (bit-identical). */
+its_status its_mlp_forward_layers(its_mlp* mlp, const float* features, int64_t n, float* out);
 /* Gradient of mean((out - y)^2) over n rows (n <= batch, a multiple of 64), no update. */
 its_status its_mlp_gradient(its_mlp* mlp, const float* features, const float* y, int64_t n, float* grad,
                             float* loss);

@@ -72,6 +72,7 @@ SIGNATURES = {
     "its_mlp_set_params": (st, [vp, vp]),
     "its_mlp_get_params": (st, [vp, vp]),
     "its_mlp_forward": (st, [vp, vp, i64, vp]),
+    "its_mlp_forward_layers": (st, [vp, vp, i64, vp]),
     "its_mlp_gradient": (st, [vp, vp, vp, i64, vp, vp]),
     "its_mlp_train": (st, [vp, vp, vp, i64, i64, C.c_float, C.c_uint64, vp]),
     "its_fit_residual": (st, [vp, vp, vp, C.POINTER(dbl)]),

@@ -513,6 +513,14 @@ class ShareNet:
         self.ctx.check(lib().its_mlp_forward(self.h, _ptr(X), n, _ptr(out)), "its_mlp_forward")
         return out
 
+    def forward_layers(self, X, out=None):
+        X = _f32(X)
+        n = _n(X)
+        if out is None:
+            out = np.zeros(n, np.float32)
+        self.ctx.check(lib().its_mlp_forward_layers(self.h, _ptr(X), n, _ptr(out)), "its_mlp_forward_layers")
+        return out
+
     def gradient(self, X, y):
         X, y = _f32(X), _f32(y)
         g = np.zeros(self.num_params, np.float32)

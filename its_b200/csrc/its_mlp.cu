@@ -205,6 +205,121 @@ struct EpiPartial {
   }
 };
 
+// ---- fused inference ------------------------------------------------------------------------
+// The whole network for 128-row tiles in one persistent kernel: the three weight matrices
+// stay in shared memory (80 KB, loaded once per CTA), the features of a tile are converted to
+// BF16 into shared memory, and each layer's activations go from TMEM through the epilogue
+// straight back into shared memory as the next layer's A operand -- nothing but the features
+// and the outputs touches global memory. The MMA sequence and the epilogue arithmetic are
+// those of the layer-by-layer kernels, so the outputs are identical.
+constexpr int kFusedSmem = 16384 /*X*/ + 16384 /*W1*/ + 32768 /*W2*/ + 32768 /*W3*/ + 32768 /*H*/ + 64 + 1024;
+
+__device__ __forceinline__ void loadWeightTile(uint8_t* dst, const bf16* __restrict__ W, int K, int tid) {
+  // W: 128 rows x K bf16, row-major (K-major B operand); K/64 swizzled blocks of 128 x 128 B
+  for (int i = tid; i < 128 * (K / 8); i += 128) {
+    const int r = i / (K / 8), c = i % (K / 8);
+    *(uint4*)(dst + (c >> 3) * 16384 + umma::swizzledChunk(r, c & 7)) = __ldg((const uint4*)(W + (int64_t)r * K + c * 8));
+  }
+}
+
+__global__ void __launch_bounds__(128, 1) kMlpForwardFused(const float* __restrict__ X, int64_t n,
+                                                           const bf16* __restrict__ W1, const bf16* __restrict__ W2,
+                                                           const bf16* __restrict__ W3, const float* __restrict__ P,
+                                                           const float* __restrict__ w4r, float* __restrict__ out,
+                                                           int* __restrict__ err) {
+  using namespace umma;
+  extern __shared__ uint8_t smemRaw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smemRaw + 1023) & ~(uintptr_t)1023);
+  uint8_t* sX = smem;
+  uint8_t* sW1 = sX + 16384;
+  uint8_t* sW2 = sW1 + 16384;
+  uint8_t* sW3 = sW2 + 32768;
+  uint8_t* sH = sW3 + 32768;
+  uint64_t* mbar = (uint64_t*)(sH + 32768);
+  uint32_t* slot = (uint32_t*)(mbar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  if (warp == 0) tmemAlloc(smemAddr(slot), 128);
+  if (tid == 0) mbarInit(smemAddr(mbar), 1);
+  loadWeightTile(sW1, W1, kIn, tid);
+  loadWeightTile(sW2, W2, kHid, tid);
+  loadWeightTile(sW3, W3, kHid, tid);
+  fenceBefore();
+  __syncthreads();
+  fenceAfter();
+  const uint32_t tmem = *slot;
+  const uint32_t lane = (uint32_t)(warp * 32) << 16;
+  constexpr uint32_t idesc = idescBf16(128, kHid);
+  uint32_t phase = 0;
+  bool ok = true;
+  const float* b1 = P + kOffB1;
+  const float* b2 = P + kOffB2;
+  const float* b3 = P + kOffB3;
+  const int64_t tiles = (n + 127) / 128;
+  for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const int64_t m = t * 128 + tid;
+    // features -> BF16, this thread's row (8 chunks of 8 values)
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      __align__(16) bf16 v[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) v[e] = __float2bfloat16_rn(m < n ? X[m * kIn + c * 8 + e] : 0.0f);
+      *(uint4*)(sX + swizzledChunk(tid, c)) = *(const uint4*)v;
+    }
+    float acc[kHid];
+    for (int layer = 0; layer < 3; ++layer) {
+      fenceProxyAsync();
+      fenceBefore();
+      __syncthreads();
+      if (tid == 0) {
+        fenceAfter();
+        if (layer == 0) {
+          const uint64_t da = descSw128(smemAddr(sX)), db = descSw128(smemAddr(sW1));
+#pragma unroll
+          for (int k = 0; k < 4; ++k) mma(tmem, da + 2 * k, db + 2 * k, idesc, k > 0 ? 1u : 0u);
+        } else {
+          const uint8_t* sW = layer == 1 ? sW2 : sW3;
+#pragma unroll
+          for (int kb = 0; kb < 2; ++kb) {
+            const uint64_t da = descSw128(smemAddr(sH + kb * 16384)), db = descSw128(smemAddr(sW + kb * 16384));
+#pragma unroll
+            for (int k = 0; k < 4; ++k) mma(tmem, da + 2 * k, db + 2 * k, idesc, (kb > 0 || k > 0) ? 1u : 0u);
+          }
+        }
+        commit(smemAddr(mbar));
+      }
+      ok = mbarWait(smemAddr(mbar), phase) && ok;
+      phase ^= 1u;
+      fenceAfter();
+#pragma unroll
+      for (int n0 = 0; n0 < kHid; n0 += 16) {
+        float v[16];
+        tmemLoad16(tmem + lane + (uint32_t)n0, v);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) acc[n0 + j] = v[j];
+      }
+      if (layer < 2) {  // hidden layer: next layer's A operand
+        const float* bias = layer == 0 ? b1 : b2;
+#pragma unroll
+        for (int c = 0; c < 16; ++c) {
+          __align__(16) bf16 v[8];
+#pragma unroll
+          for (int e = 0; e < 8; ++e) v[e] = __float2bfloat16_rn(geluF(acc[c * 8 + e] + bias[c * 8 + e]));
+          *(uint4*)(sH + (c >> 3) * 16384 + swizzledChunk(tid, c & 7)) = *(const uint4*)v;
+        }
+      } else if (m < n && ok) {  // output unit
+        float o = 0.0f;
+#pragma unroll
+        for (int j = 0; j < kHid; ++j) o += __bfloat162float(__float2bfloat16_rn(geluF(acc[j] + b3[j]))) * w4r[j];
+        out[m] = o + P[kOffB4];
+      }
+    }
+  }
+  fenceBefore();
+  __syncthreads();
+  if (warp == 0) tmemFree(tmem, 128);
+  if (!ok && tid == 0) atomicExch(err, 1);
+}
+
 // ---- small kernels ----------------------------------------------------------------------
 // Features (FP32, n x 64, already normalised) to BF16 rows (and columns for training).
 __global__ void kFeaturesBf16(const float* __restrict__ X, int64_t n, bf16* __restrict__ Xb, bf16* __restrict__ Xt,
@@ -521,6 +636,32 @@ its_status its_mlp_get_params(its_mlp* h, float* params) {
 
 // Predictions for n rows of features (n x 64 FP32, normalised), host or device memory.
 its_status its_mlp_forward(its_mlp* h, const float* X, int64_t n, float* out) {
+  if (!h || (n > 0 && (!X || !out)) || n < 0) return ITS_ERR_INVALID;
+  its_ctx* ctx = h->ctx;
+  ITS_CU(ctx, cudaSetDevice(ctx->device));
+  InArg<float> x;
+  OutArg<float> o;
+  its_status st;
+  if ((st = x.stage(ctx, X, n * kIn)) != ITS_OK) return st;
+  if ((st = o.stage(ctx, out, n)) != ITS_OK) return st;
+  if (n > 0) {
+    static bool configured = false;
+    if (!configured) {
+      ITS_CU(ctx, cudaFuncSetAttribute(kMlpForwardFused, cudaFuncAttributeMaxDynamicSharedMemorySize, kFusedSmem));
+      configured = true;
+    }
+    const int64_t tiles = (n + 127) / 128;
+    const unsigned grid = (unsigned)(tiles < ctx->numSMs ? tiles : ctx->numSMs);
+    kMlpForwardFused<<<grid, 128, kFusedSmem, ctx->stream>>>(x.d, n, h->W1, h->W2, h->W3, h->P, h->w4r, o.d, h->err);
+    ITS_LAUNCHED(ctx);
+  }
+  if ((st = o.finish(ctx)) != ITS_OK) return st;
+  return checkErr(h);
+}
+
+// The same predictions layer by layer (the training kernels' forward); identical to
+// its_mlp_forward bit for bit (a test hook).
+its_status its_mlp_forward_layers(its_mlp* h, const float* X, int64_t n, float* out) {
   if (!h || (n > 0 && (!X || !out)) || n < 0) return ITS_ERR_INVALID;
   its_ctx* ctx = h->ctx;
   ITS_CU(ctx, cudaSetDevice(ctx->device));

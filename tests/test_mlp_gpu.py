@@ -25,6 +25,8 @@ def test_forward_matches_oracle(ctx, n):
     net = ShareNet(ctx, batch=65536, params=ref.init_params(3))
     X, _ = _data(n, 1)
     out = net.forward(X)
+    # the fused persistent kernel and the layer-by-layer training kernels agree bit for bit
+    assert np.array_equal(out, net.forward_layers(X))
     want = ref.forward(ref.init_params(3), X)
     scale = np.abs(want).max()
     assert np.abs(out - want).max() <= 1e-2 * scale, np.abs(out - want).max() / scale
