@@ -18,6 +18,7 @@
 // Features are optionally normalised, (f - mean) * scale, as the network was trained.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "its_op.cuh"
@@ -376,10 +377,8 @@ its_status its_share_features(its_svo* svo, const double* b, const float* norm, 
   InArg<double> db;
   InArg<float> dn;
   if ((st = db.stage(ctx, b, n)) != ITS_OK || (st = dn.stage(ctx, norm, norm ? 2 * kFeat : 0)) != ITS_OK) return st;
-  DevBuf<int64_t> dIds;
-  if ((st = dIds.alloc(ctx, n)) != ITS_OK) return st;
-  int64_t cnt = 0;
-  if ((st = coincidentIds(ctx, d, dIds.p, &cnt)) != ITS_OK) return st;
+  const int64_t cnt = d.numCoinc;
+  const int64_t* dIds = d.coincIds;
   *count = cnt;
   if (!features) return ITS_OK;
   if (capacity < cnt) return setError(ctx, ITS_ERR_INVALID, "its_share_features: capacity below the count");
@@ -390,9 +389,9 @@ its_status its_share_features(its_svo* svo, const double* b, const float* norm, 
   if ((st = exactStart(ctx, &svo, 1, &bp, nullptr, &lp)) != ITS_OK) return st;
   OutArg<float> out;
   if ((st = out.stage(ctx, features, cnt * kFeat)) != ITS_OK) return st;
-  if ((st = shareFeatures(ctx, d, db.d, lam0.p, dIds.p, cnt, dn.d, out.d)) != ITS_OK) return st;
+  if ((st = shareFeatures(ctx, d, db.d, lam0.p, dIds, cnt, dn.d, out.d)) != ITS_OK) return st;
   if ((st = out.finish(ctx)) != ITS_OK) return st;
-  if (ids) ITS_CU(ctx, cudaMemcpyAsync(ids, dIds.p, cnt * 8, cudaMemcpyDefault, ctx->stream));
+  if (ids) ITS_CU(ctx, cudaMemcpyAsync(ids, dIds, cnt * 8, cudaMemcpyDefault, ctx->stream));
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   return ITS_OK;
 }
@@ -409,15 +408,18 @@ its_status its_learned_start_batch(its_svo* const* svos, int64_t count, its_mlp*
   its_status st;
   // host norm: input mean[64], input scale[64], output mean, output scale
   float hn[2 * kFeat + 2];
-  ITS_CU(ctx, cudaMemcpyAsync(hn, norm, sizeof(hn), cudaMemcpyDefault, ctx->stream));
-  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  if (isDevicePtr(norm)) {
+    ITS_CU(ctx, cudaMemcpyAsync(hn, norm, sizeof(hn), cudaMemcpyDeviceToHost, ctx->stream));
+    ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  } else {
+    std::memcpy(hn, norm, sizeof(hn));
+  }
   DevBuf<float> dNorm;
   if ((st = dNorm.alloc(ctx, 2 * kFeat)) != ITS_OK) return st;
   ITS_CU(ctx, cudaMemcpyAsync(dNorm.p, hn, 2 * kFeat * 4, cudaMemcpyHostToDevice, ctx->stream));
   std::vector<InArg<double>> B(count);
   std::vector<OutArg<double>> L(count);
   std::vector<DevBuf<double>> lam0(count), shares(count);
-  std::vector<DevBuf<int64_t>> ids(count);
   std::vector<const double*> bp(count), sp(count);
   std::vector<double*> l0(count), lp(count);
   std::vector<int64_t> cnt(count);
@@ -425,14 +427,13 @@ its_status its_learned_start_batch(its_svo* const* svos, int64_t count, its_mlp*
   for (int64_t m = 0; m < count; ++m) {
     const int64_t n = svos[m]->d.numVerts;
     if ((st = B[m].stage(ctx, b[m], n)) != ITS_OK || (st = L[m].stage(ctx, lambda[m], n)) != ITS_OK ||
-        (st = lam0[m].alloc(ctx, n)) != ITS_OK || (st = shares[m].alloc(ctx, n)) != ITS_OK ||
-        (st = ids[m].alloc(ctx, n)) != ITS_OK)
+        (st = lam0[m].alloc(ctx, n)) != ITS_OK || (st = shares[m].alloc(ctx, n)) != ITS_OK)
       return st;
     bp[m] = B[m].d;
     l0[m] = lam0[m].p;
     lp[m] = L[m].d;
     sp[m] = shares[m].p;
-    if ((st = coincidentIds(ctx, svos[m]->d, ids[m].p, &cnt[m])) != ITS_OK) return st;
+    cnt[m] = svos[m]->d.numCoinc;
     total += cnt[m];
   }
   // zero-share starts (features), features of every mesh into one array, one network pass
@@ -443,22 +444,27 @@ its_status its_learned_start_batch(its_svo* const* svos, int64_t count, its_mlp*
     return st;
   int64_t off = 0;
   for (int64_t m = 0; m < count; ++m) {
-    if ((st = shareFeatures(ctx, svos[m]->d, bp[m], l0[m], ids[m].p, cnt[m], dNorm.p, feat.p + off * kFeat)) != ITS_OK)
+    if ((st = shareFeatures(ctx, svos[m]->d, bp[m], l0[m], svos[m]->d.coincIds, cnt[m], dNorm.p,
+                            feat.p + off * kFeat)) != ITS_OK)
       return st;
     off += cnt[m];
   }
   if (total > 0 && (st = its_mlp_forward(mlp, feat.p, total, pred.p)) != ITS_OK) return st;
   off = 0;
   for (int64_t m = 0; m < count; ++m) {
-    if ((st = scatterShares(ctx, ids[m].p, cnt[m], pred.p + off, hn[2 * kFeat + 1], hn[2 * kFeat], shares[m].p,
+    if ((st = scatterShares(ctx, svos[m]->d.coincIds, cnt[m], pred.p + off, hn[2 * kFeat + 1], hn[2 * kFeat], shares[m].p,
                             svos[m]->d.numVerts)) != ITS_OK)
       return st;
     off += cnt[m];
   }
   if ((st = exactStart(ctx, svos, count, bp.data(), sp.data(), lp.data())) != ITS_OK) return st;
-  for (int64_t m = 0; m < count; ++m)
+  bool host = false;
+  for (int64_t m = 0; m < count; ++m) {
+    host = host || L[m].host;
     if ((st = L[m].finish(ctx)) != ITS_OK) return st;
-  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  // device outputs: ordered on the context's stream; host outputs: complete on return
+  if (host) ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   return ITS_OK;
 }
 

@@ -130,6 +130,8 @@ struct SvoDevice {
   float* nodeSampleCnt = nullptr;  // per node
   double* nodeSamplePos = nullptr; // 3 per node: sum of centroids
   double* nodeSampleNrm = nullptr; // 3 per node: sum of unit normals
+  int64_t* coincIds = nullptr;     // vertices coincident with a coarser corner, ascending
+  int64_t numCoinc = 0;
   LatticeIndex lattice(int d) const {
     LatticeIndex L;
     L.bits = vbits[d];

@@ -139,8 +139,8 @@ static its_status uploadParams(its_ctx* ctx, its_svo* const* svos, int64_t count
   std::vector<RowParams> h(count);
   for (int64_t m = 0; m < count; ++m) h[m] = rowParams(svos[m]->d);
   if ((st = dP.alloc(ctx, count)) != ITS_OK) return st;
+  // from pageable memory: the call returns once the source is staged, so h may go away
   ITS_CU(ctx, cudaMemcpyAsync(dP.p, h.data(), count * sizeof(RowParams), cudaMemcpyHostToDevice, ctx->stream));
-  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   return ITS_OK;
 }
 
@@ -204,8 +204,7 @@ its_status exactStart(its_ctx* ctx, its_svo* const* svos, int64_t count, const d
       kStartLevel<<<gridFor(total, 128), 128, 0, ctx->stream>>>(dSegs.p + g0, dPrefix.p + g0, ng, total);
     ITS_LAUNCHED(ctx);
   }
-  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));  // the host tables above are read by the copies
-  return ITS_OK;
+  return ITS_OK;  // the tables were copied from pageable memory (staged at the call)
 }
 
 // ||b - A lambda|| / ||b|| of count octrees (device vectors), matrix-free, into rel[count]
@@ -297,9 +296,13 @@ its_status its_exact_start_batch(its_svo* const* svos, int64_t count, const doub
     dl[m] = L[m].d;
   }
   if ((st = exactStart(ctx, svos, count, db.data(), ds.data(), dl.data())) != ITS_OK) return st;
-  for (int64_t m = 0; m < count; ++m)
+  bool host = false;
+  for (int64_t m = 0; m < count; ++m) {
+    host = host || L[m].host;
     if ((st = L[m].finish(ctx)) != ITS_OK) return st;
-  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  // device outputs: ordered on the context's stream; host outputs: complete on return
+  if (host) ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   return ITS_OK;
 }
 

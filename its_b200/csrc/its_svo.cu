@@ -309,7 +309,7 @@ static void svoRelease(its_svo* s) {
   SvoDevice& d = s->d;
   void* ptrs[] = {d.voxels, d.nodeMorton, d.nodeParent, d.nodeChild0, d.nodeLeaf, d.nodeNb, d.vertLin,
                   d.vertOwner, d.vertPos, d.ebits, d.erank, d.edgeKey, d.edgeOwner, d.fineOcc,
-                  d.nodeSampleCnt, d.nodeSamplePos, d.nodeSampleNrm};
+                  d.nodeSampleCnt, d.nodeSamplePos, d.nodeSampleNrm, d.coincIds};
   for (void* p : ptrs) devFree(c, p);
   for (int i = 0; i < kMaxDepth; ++i) { devFree(c, d.vbits[i]); devFree(c, d.vrank[i]); }
   d = SvoDevice();
@@ -511,6 +511,9 @@ its_status svoBuild(its_ctx* ctx, const double* dV, int64_t nv, const int32_t* d
   }
   // per-node sums of the face samples (features of the share network)
   if ((st = nodeSampleStats(ctx, d, dV, dF, nf)) != ITS_OK) return st;
+  // the coincident vertices (the shares of the exact start)
+  if ((st = devAlloc(ctx, (void**)&d.coincIds, std::max<int64_t>(d.numVerts, 1) * 8)) != ITS_OK) return st;
+  if ((st = coincidentIds(ctx, d, d.coincIds, &d.numCoinc)) != ITS_OK) return st;
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   return ITS_OK;
 }

@@ -15,4 +15,7 @@ its_status svoBuild(its_ctx* ctx, const double* dV, int64_t nv, const int32_t* d
 // Face samples (centroid, unit normal) summed per fine node in face order, then per coarser
 // node over its 8 children in order, into d.nodeSample* (its_features.cu).
 its_status nodeSampleStats(its_ctx* ctx, SvoDevice& d, const double* dV, const int32_t* dF, int64_t nf);
+// The vertices coincident with a coarser corner (lattice coordinates all even below the
+// root depth), ascending, into ids (capacity numVerts); *count their number.
+its_status coincidentIds(its_ctx* ctx, const SvoDevice& d, int64_t* ids, int64_t* count);
 }  // namespace its
