@@ -427,6 +427,12 @@ def run_ours(args):
                          "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                          "bytes_per_launch": spmv_bytes, "launch_ms": round(spmv[dom], 5), "traffic": None},
+            "roofline_learned": {"bound": "hbm", "kernel": "kStartLevel (matrix-free exact start, all depths)",
+                                 "achieved": round(60 * n / (t_start * 1e-3) / 1e9, 1), "peak": peak, "unit": "GB/s",
+                                 "frac": round(60 * n / (t_start * 1e-3) / 1e9 / peak, 4), "peak_kind": peak_kind,
+                                 "bytes_per_launch": 60 * n, "launch_ms": round(t_start, 5), "traffic": None,
+                                 "note": "60 B per row (octree tables 36, b 8, lambda read 8 and written 8); the "
+                                         "row walks' lattice lookups hit L2: latency-bound, not HBM-bound"},
             "cpu_baseline": cpu,
             "clocks": clk,
             "gpu_launches": launches,

@@ -212,65 +212,70 @@ struct EpiPartial {
 // straight back into shared memory as the next layer's A operand -- nothing but the features
 // and the outputs touches global memory. The MMA sequence and the epilogue arithmetic are
 // those of the layer-by-layer kernels, so the outputs are identical.
-constexpr int kFusedSmem = 16384 /*X*/ + 16384 /*W1*/ + 32768 /*W2*/ + 32768 /*W3*/ + 32768 /*H*/ + 64 + 1024;
+constexpr int kFusedGroups = 2;  // two 128-row tiles in flight per CTA (one per warp group)
+constexpr int kFusedSmem = 16384 /*W1*/ + 32768 /*W2*/ + 32768 /*W3*/ + kFusedGroups * (16384 /*X*/ + 32768 /*H*/) +
+                           64 + 1024;
 
-__device__ __forceinline__ void loadWeightTile(uint8_t* dst, const bf16* __restrict__ W, int K, int tid) {
+__device__ __forceinline__ void loadWeightTile(uint8_t* dst, const bf16* __restrict__ W, int K, int tid, int nthreads) {
   // W: 128 rows x K bf16, row-major (K-major B operand); K/64 swizzled blocks of 128 x 128 B
-  for (int i = tid; i < 128 * (K / 8); i += 128) {
+  for (int i = tid; i < 128 * (K / 8); i += nthreads) {
     const int r = i / (K / 8), c = i % (K / 8);
     *(uint4*)(dst + (c >> 3) * 16384 + umma::swizzledChunk(r, c & 7)) = __ldg((const uint4*)(W + (int64_t)r * K + c * 8));
   }
 }
 
-__global__ void __launch_bounds__(128, 1) kMlpForwardFused(const float* __restrict__ X, int64_t n,
-                                                           const bf16* __restrict__ W1, const bf16* __restrict__ W2,
-                                                           const bf16* __restrict__ W3, const float* __restrict__ P,
-                                                           const float* __restrict__ w4r, float* __restrict__ out,
-                                                           int* __restrict__ err) {
+// Barrier of one warp group (128 threads), ids 1 and 2 (0 is __syncthreads').
+__device__ __forceinline__ void groupSync(int g) { asm volatile("bar.sync %0, 128;" ::"r"(1 + g) : "memory"); }
+
+__global__ void __launch_bounds__(128 * kFusedGroups, 1)
+    kMlpForwardFused(const float* __restrict__ X, int64_t n, const bf16* __restrict__ W1, const bf16* __restrict__ W2,
+                     const bf16* __restrict__ W3, const float* __restrict__ P, const float* __restrict__ w4r,
+                     float* __restrict__ out, int* __restrict__ err) {
   using namespace umma;
   extern __shared__ uint8_t smemRaw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smemRaw + 1023) & ~(uintptr_t)1023);
-  uint8_t* sX = smem;
-  uint8_t* sW1 = sX + 16384;
+  uint8_t* sW1 = smem;
   uint8_t* sW2 = sW1 + 16384;
   uint8_t* sW3 = sW2 + 32768;
-  uint8_t* sH = sW3 + 32768;
-  uint64_t* mbar = (uint64_t*)(sH + 32768);
-  uint32_t* slot = (uint32_t*)(mbar + 1);
-  const int tid = threadIdx.x, warp = tid >> 5;
-  if (warp == 0) tmemAlloc(smemAddr(slot), 128);
-  if (tid == 0) mbarInit(smemAddr(mbar), 1);
-  loadWeightTile(sW1, W1, kIn, tid);
-  loadWeightTile(sW2, W2, kHid, tid);
-  loadWeightTile(sW3, W3, kHid, tid);
+  const int tid = threadIdx.x, g = tid >> 7, row = tid & 127, warp = tid >> 5;
+  uint8_t* sX = sW3 + 32768 + g * (16384 + 32768);
+  uint8_t* sH = sX + 16384;
+  uint64_t* mbar = (uint64_t*)(sW3 + 32768 + kFusedGroups * (16384 + 32768));
+  uint32_t* slot = (uint32_t*)(mbar + kFusedGroups);
+  if (warp == 0) tmemAlloc(smemAddr(slot), 128 * kFusedGroups);
+  if (tid == 0)
+    for (int k = 0; k < kFusedGroups; ++k) mbarInit(smemAddr(mbar + k), 1);
+  loadWeightTile(sW1, W1, kIn, tid, blockDim.x);
+  loadWeightTile(sW2, W2, kHid, tid, blockDim.x);
+  loadWeightTile(sW3, W3, kHid, tid, blockDim.x);
   fenceBefore();
   __syncthreads();
   fenceAfter();
-  const uint32_t tmem = *slot;
-  const uint32_t lane = (uint32_t)(warp * 32) << 16;
+  const uint32_t tmem = *slot + 128u * g;                 // this group's 128 columns
+  const uint32_t lane = (uint32_t)((warp & 3) * 32) << 16;  // the warp's TMEM lanes
   constexpr uint32_t idesc = idescBf16(128, kHid);
+  const uint32_t bar = smemAddr(mbar + g);
   uint32_t phase = 0;
   bool ok = true;
   const float* b1 = P + kOffB1;
   const float* b2 = P + kOffB2;
   const float* b3 = P + kOffB3;
   const int64_t tiles = (n + 127) / 128;
-  for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
-    const int64_t m = t * 128 + tid;
-    // features -> BF16, this thread's row (8 chunks of 8 values)
+  for (int64_t t = (int64_t)blockIdx.x * kFusedGroups + g; t < tiles; t += (int64_t)gridDim.x * kFusedGroups) {
+    const int64_t m = t * 128 + row;
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
+    for (int c = 0; c < 8; ++c) {  // features -> BF16, this thread's row
       __align__(16) bf16 v[8];
 #pragma unroll
       for (int e = 0; e < 8; ++e) v[e] = __float2bfloat16_rn(m < n ? X[m * kIn + c * 8 + e] : 0.0f);
-      *(uint4*)(sX + swizzledChunk(tid, c)) = *(const uint4*)v;
+      *(uint4*)(sX + swizzledChunk(row, c)) = *(const uint4*)v;
     }
     float acc[kHid];
     for (int layer = 0; layer < 3; ++layer) {
       fenceProxyAsync();
       fenceBefore();
-      __syncthreads();
-      if (tid == 0) {
+      groupSync(g);
+      if (row == 0) {
         fenceAfter();
         if (layer == 0) {
           const uint64_t da = descSw128(smemAddr(sX)), db = descSw128(smemAddr(sW1));
@@ -285,9 +290,9 @@ __global__ void __launch_bounds__(128, 1) kMlpForwardFused(const float* __restri
             for (int k = 0; k < 4; ++k) mma(tmem, da + 2 * k, db + 2 * k, idesc, (kb > 0 || k > 0) ? 1u : 0u);
           }
         }
-        commit(smemAddr(mbar));
+        commit(bar);
       }
-      ok = mbarWait(smemAddr(mbar), phase) && ok;
+      ok = mbarWait(bar, phase) && ok;
       phase ^= 1u;
       fenceAfter();
 #pragma unroll
@@ -297,14 +302,14 @@ __global__ void __launch_bounds__(128, 1) kMlpForwardFused(const float* __restri
 #pragma unroll
         for (int j = 0; j < 16; ++j) acc[n0 + j] = v[j];
       }
-      if (layer < 2) {  // hidden layer: next layer's A operand
+      if (layer < 2) {  // hidden layer: the next layer's A operand
         const float* bias = layer == 0 ? b1 : b2;
 #pragma unroll
         for (int c = 0; c < 16; ++c) {
           __align__(16) bf16 v[8];
 #pragma unroll
           for (int e = 0; e < 8; ++e) v[e] = __float2bfloat16_rn(geluF(acc[c * 8 + e] + bias[c * 8 + e]));
-          *(uint4*)(sH + (c >> 3) * 16384 + swizzledChunk(tid, c & 7)) = *(const uint4*)v;
+          *(uint4*)(sH + (c >> 3) * 16384 + swizzledChunk(row, c & 7)) = *(const uint4*)v;
         }
       } else if (m < n && ok) {  // output unit
         float o = 0.0f;
@@ -313,10 +318,12 @@ __global__ void __launch_bounds__(128, 1) kMlpForwardFused(const float* __restri
         out[m] = o + P[kOffB4];
       }
     }
+    fenceBefore();
+    groupSync(g);  // every lane has read TMEM before the next tile's first MMA
   }
   fenceBefore();
   __syncthreads();
-  if (warp == 0) tmemFree(tmem, 128);
+  if (warp == 0) tmemFree(*slot, 128 * kFusedGroups);
   if (!ok && tid == 0) atomicExch(err, 1);
 }
 
@@ -650,9 +657,10 @@ its_status its_mlp_forward(its_mlp* h, const float* X, int64_t n, float* out) {
       ITS_CU(ctx, cudaFuncSetAttribute(kMlpForwardFused, cudaFuncAttributeMaxDynamicSharedMemorySize, kFusedSmem));
       configured = true;
     }
-    const int64_t tiles = (n + 127) / 128;
-    const unsigned grid = (unsigned)(tiles < ctx->numSMs ? tiles : ctx->numSMs);
-    kMlpForwardFused<<<grid, 128, kFusedSmem, ctx->stream>>>(x.d, n, h->W1, h->W2, h->W3, h->P, h->w4r, o.d, h->err);
+    const int64_t tiles = (n + 127) / 128, ctas = (tiles + kFusedGroups - 1) / kFusedGroups;
+    const unsigned grid = (unsigned)(ctas < ctx->numSMs ? ctas : ctx->numSMs);
+    kMlpForwardFused<<<grid, 128 * kFusedGroups, kFusedSmem, ctx->stream>>>(x.d, n, h->W1, h->W2, h->W3, h->P, h->w4r,
+                                                                             o.d, h->err);
     ITS_LAUNCHED(ctx);
   }
   if ((st = o.finish(ctx)) != ITS_OK) return st;

@@ -94,17 +94,21 @@ __device__ __forceinline__ void walkRow(const RowParams& P, int64_t r, int d, Vi
     const double w = P.w0 * (double)(1u << dd), wi = P.winv[dd];
     const double bx = latticePos(P.g.x, w, Xa), by = latticePos(P.g.y, w, Ya), bz = latticePos(P.g.z, w, Za);
     const LatticeIndex& L = P.lat[dd];
+    // the six axis factors once (the corners share them); visiting order and values unchanged
+    const double hxs[2] = {hat1r(qx, bx, w, wi), hat1r(qx, bx + w, w, wi)};
+    const double hys[2] = {hat1r(qy, by, w, wi), hat1r(qy, by + w, w, wi)};
+    const double hzs[2] = {hat1r(qz, bz, w, wi), hat1r(qz, bz + w, w, wi)};
 #pragma unroll
     for (int ox = 0; ox < 2; ++ox) {
-      const double hx = hat1r(qx, ox ? bx + w : bx, w, wi);
+      const double hx = hxs[ox];
       if (hx <= 0.0) continue;
 #pragma unroll
       for (int oy = 0; oy < 2; ++oy) {
-        const double hy = hat1r(qy, oy ? by + w : by, w, wi);
+        const double hy = hys[oy];
         if (hy <= 0.0) continue;
 #pragma unroll
         for (int oz = 0; oz < 2; ++oz) {
-          const double hz = hat1r(qz, oz ? bz + w : bz, w, wi);
+          const double hz = hzs[oz];
           if (hz <= 0.0) continue;
           const double v = hx * hy * hz;
           if (v == 0.0) continue;

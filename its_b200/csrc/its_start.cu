@@ -121,16 +121,29 @@ __global__ void __launch_bounds__(kResThreads) kResidualChunks(const RowSeg* __r
   }
 }
 
-__global__ void kResidualFinish(const double* __restrict__ part, const int64_t* __restrict__ first, int64_t count,
-                                double* __restrict__ rel) {
-  const int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (m >= count) return;
+// One block per mesh: the mesh's chunk partials in a fixed order (strided per thread, then a
+// fixed tree), so the result does not depend on timing.
+__global__ void __launch_bounds__(kResThreads) kResidualFinish(const double* __restrict__ part,
+                                                               const int64_t* __restrict__ first,
+                                                               double* __restrict__ rel) {
+  const int64_t m = blockIdx.x;
   double a = 0.0, c = 0.0;
-  for (int64_t k = first[m]; k < first[m + 1]; ++k) {
+  for (int64_t k = first[m] + threadIdx.x; k < first[m + 1]; k += kResThreads) {
     a += part[2 * k];
     c += part[2 * k + 1];
   }
-  rel[m] = c > 0.0 ? sqrt(a / c) : sqrt(a);
+  __shared__ double sa[kResThreads], sc[kResThreads];
+  sa[threadIdx.x] = a;
+  sc[threadIdx.x] = c;
+  __syncthreads();
+  for (int s = kResThreads / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      sa[threadIdx.x] += sa[threadIdx.x + s];
+      sc[threadIdx.x] += sc[threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) rel[m] = sc[0] > 0.0 ? sqrt(sa[0] / sc[0]) : sqrt(sa[0]);
 }
 
 // Row parameters of count octrees on the device.
@@ -247,7 +260,7 @@ its_status fitResidual(its_ctx* ctx, its_svo* const* svos, int64_t count, const 
   } else {
     ITS_CU(ctx, cudaMemsetAsync(part.p, 0, 16, ctx->stream));
   }
-  kResidualFinish<<<gridFor(count, 128), 128, 0, ctx->stream>>>(part.p, dFirst.p, count, dRel.p);
+  kResidualFinish<<<(unsigned)count, kResThreads, 0, ctx->stream>>>(part.p, dFirst.p, dRel.p);
   ITS_LAUNCHED(ctx);
   ITS_CU(ctx, cudaMemcpyAsync(rel, dRel.p, count * 8, cudaMemcpyDeviceToHost, ctx->stream));
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
