@@ -241,11 +241,16 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
           const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
           if (latticeHas(L, lin)) {
             const uint32_t v = latticeRank(L, lin);
+            const double qx = P.vertPos[3 * v], qy = P.vertPos[3 * v + 1], qz = P.vertPos[3 * v + 2];
             tLam[t] = (T)lambda[v];
-            tPx[t] = (T)P.vertPos[3 * v];
-            tPy[t] = (T)P.vertPos[3 * v + 1];
-            tPz[t] = (T)P.vertPos[3 * v + 2];
-            has = 1;
+            tPx[t] = (T)qx;
+            tPy[t] = (T)qy;
+            tPz[t] = (T)qz;
+            // bit 0: present; bits 1-3: the x / y / z coordinate is the lattice coordinate
+            // g + w X, so the column's shared factor for that axis applies (FP32: always)
+            has = (unsigned char)(1 | ((sizeof(T) == 4 || qx == latticePos(P.g.x, wd, (uint32_t)Lx)) ? 2 : 0) |
+                                  ((sizeof(T) == 4 || qy == latticePos(P.g.y, wd, (uint32_t)Ly)) ? 4 : 0) |
+                                  ((sizeof(T) == 4 || qz == latticePos(P.g.z, wd, (uint32_t)Lz)) ? 8 : 0));
           }
         }
         tHas[t] = has;
@@ -257,48 +262,51 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
     }
     if (any && inXY) {
       const int64_t cx = (int64_t)floor(quotT<T>(px - gx, w, wi)), cy = (int64_t)floor(quotT<T>(py - gy, w, wi));
-      // x / y hat factors per distinct corner coordinate, shared by the column's points
-      T cxv[2] = {0, 0}, cyv[2] = {0, 0}, hxv[2] = {0, 0}, hyv[2] = {0, 0};
-      bool okx[2] = {false, false}, oky[2] = {false, false};
+      // the lattice factors of this column's cell: x and y shared by its 4 points
+      const T fx[2] = {hatT<T>(px, (T)latticePos(P.g.x, wd, (uint32_t)cx), w, wi),
+                       hatT<T>(px, (T)latticePos(P.g.x, wd, (uint32_t)(cx + 1)), w, wi)};
+      const T fy[2] = {hatT<T>(py, (T)latticePos(P.g.y, wd, (uint32_t)cy), w, wi),
+                       hatT<T>(py, (T)latticePos(P.g.y, wd, (uint32_t)(cy + 1)), w, wi)};
 #pragma unroll
       for (int q = 0; q < kZPer; ++q) {
         if (zb + q >= M) break;
         const T pzq = pz[q];
         const int64_t cz = (int64_t)floor(quotT<T>(pzq - gz, w, wi));
-        T czv[2] = {0, 0}, hzv[2] = {0, 0};
-        bool okz[2] = {false, false};
+        const T fz[2] = {hatT<T>(pzq, (T)latticePos(P.g.z, wd, (uint32_t)cz), w, wi),
+                         hatT<T>(pzq, (T)latticePos(P.g.z, wd, (uint32_t)(cz + 1)), w, wi)};
         T s = sum[q];
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
           const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
-          T lam, qx, qy, qz;
+          T lam;
+          unsigned f;
+          int t = 0;
+          uint32_t vv = 0;
           if (tiled) {
-            const int t = ((int)(cx - cx0) + ox) * ny * nz + ((int)(cy - cy0) + oy) * nz + ((int)(cz - cz0) + oz);
-            if (!tHas[t]) continue;
+            t = ((int)(cx - cx0) + ox) * ny * nz + ((int)(cy - cy0) + oy) * nz + ((int)(cz - cz0) + oz);
+            f = tHas[t];
+            if (!f) continue;
             lam = tLam[t];
-            qx = tPx[t];
-            qy = tPy[t];
-            qz = tPz[t];
           } else {
             const int64_t Lx = cx + ox, Ly = cy + oy, Lz = cz + oz;
             if (Lx < 0 || Ly < 0 || Lz < 0 || Lx > lim || Ly > lim || Lz > lim) continue;
             const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
             if (!latticeHas(L, lin)) continue;
-            const uint32_t v = latticeRank(L, lin);
-            lam = (T)lambda[v];
-            qx = (T)P.vertPos[3 * v];
-            qy = (T)P.vertPos[3 * v + 1];
-            qz = (T)P.vertPos[3 * v + 2];
+            vv = latticeRank(L, lin);
+            lam = (T)lambda[vv];
+            f = sizeof(T) == 4 ? 15u : 1u;  // FP64: positions from the vertex array
           }
+          // hat3 as the reference forms it: x, y, z factors with early exits; a factor at the
+          // lattice coordinate is the column's shared one (equal inputs, equal IEEE result)
           T hx, hy, hz;
-          if (okx[ox] && cxv[ox] == qx) hx = hxv[ox];
-          else { hx = hatT<T>(px, qx, w, wi); cxv[ox] = qx; hxv[ox] = hx; okx[ox] = true; }
+          if (f & 2) hx = fx[ox];
+          else hx = hatT<T>(px, tiled ? tPx[t] : (T)P.vertPos[3 * (int64_t)vv], w, wi);
           if (hx <= T(0)) continue;
-          if (oky[oy] && cyv[oy] == qy) hy = hyv[oy];
-          else { hy = hatT<T>(py, qy, w, wi); cyv[oy] = qy; hyv[oy] = hy; oky[oy] = true; }
+          if (f & 4) hy = fy[oy];
+          else hy = hatT<T>(py, tiled ? tPy[t] : (T)P.vertPos[3 * (int64_t)vv + 1], w, wi);
           if (hy <= T(0)) continue;
-          if (okz[oz] && czv[oz] == qz) hz = hzv[oz];
-          else { hz = hatT<T>(pzq, qz, w, wi); czv[oz] = qz; hzv[oz] = hz; okz[oz] = true; }
+          if (f & 8) hz = fz[oz];
+          else hz = hatT<T>(pzq, tiled ? tPz[t] : (T)P.vertPos[3 * (int64_t)vv + 2], w, wi);
           if (hz <= T(0)) continue;
           s += lam * (hx * hy * hz);
         }
