@@ -276,13 +276,17 @@ its_status solve(its_op* op, const double* dB, double* dX, const its_solve_opts&
       kSetScalars<<<1, 1, 0, ctx->stream>>>(sc.S, o.tol, maxIters, o.stop_rule);
       ITS_LAUNCHED(ctx);
       if ((st = trueResidual(ctx, sc, sc.w.b, rr.p)) != ITS_OK) return st;
-      if ((st = spmv(ctx, op->T64(), op->planT, (const double*)sc.w.b, sc.w.d)) != ITS_OK) return st;
-      if ((st = reduce(ctx, sc, OpRhsNorm{sc.w.d}, 0)) != ITS_OK) return st;
-      if ((st = spmv(ctx, op->T64(), op->planT, (const double*)rr.p, sc.w.nr)) != ITS_OK) return st;
-      if ((st = reduce(ctx, sc, OpNormal{sc.w.nr, op->invdiag}, 0)) != ITS_OK) return st;
+      if (s == 0) {  // ||A^T b||^2 once
+        if ((st = spmv(ctx, op->T64(), op->planT, (const double*)sc.w.b, sc.w.d)) != ITS_OK) return st;
+        if ((st = reduce(ctx, sc, OpRhsNorm{sc.w.d}, 0)) != ITS_OK) return st;
+      }
+      if (o.stop_rule == 0) {  // the normal-equation residual only where the stopping test uses it
+        if ((st = spmv(ctx, op->T64(), op->planT, (const double*)rr.p, sc.w.nr)) != ITS_OK) return st;
+        if ((st = reduce(ctx, sc, OpNormal{sc.w.nr, op->invdiag}, 0)) != ITS_OK) return st;
+      }
       if ((st = readScalars(ctx, sc, &h)) != ITS_OK) return st;
       bNorm2 = h.bNorm2;
-      rhsNorm2 = h.rhsNorm2;
+      if (s == 0) rhsNorm2 = h.rhsNorm2;
       const double m = o.stop_rule == 0 ? h.nrr / (rhsNorm2 > 0 ? rhsNorm2 : 1.0) : h.rr / (bNorm2 > 0 ? bNorm2 : 1.0);
       rep->normal_rel_residual = rhsNorm2 > 0 ? std::sqrt(h.nrr / rhsNorm2) : 0.0;
       if (bNorm2 == 0.0 || m < o.tol * o.tol) { conv = true; break; }
@@ -301,13 +305,13 @@ its_status solve(its_op* op, const double* dB, double* dX, const its_solve_opts&
       ITS_LAUNCHED(ctx);
       ITS_CU(ctx, cudaMemcpyAsync(sc.w.x, saveX.p, n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
     }
-    if (!conv) {  // final check after the last correction
+    if (!conv || o.stop_rule != 0) {  // final check after the last correction; normal residual for the report
       if ((st = trueResidual(ctx, sc, sc.w.b, rr.p)) != ITS_OK) return st;
       if ((st = spmv(ctx, op->T64(), op->planT, (const double*)rr.p, sc.w.nr)) != ITS_OK) return st;
       if ((st = reduce(ctx, sc, OpNormal{sc.w.nr, op->invdiag}, 0)) != ITS_OK) return st;
       if ((st = readScalars(ctx, sc, &h)) != ITS_OK) return st;
       const double m = o.stop_rule == 0 ? h.nrr / (rhsNorm2 > 0 ? rhsNorm2 : 1.0) : h.rr / (bNorm2 > 0 ? bNorm2 : 1.0);
-      conv = m < o.tol * o.tol;
+      if (!conv) conv = m < o.tol * o.tol;
       rep->normal_rel_residual = rhsNorm2 > 0 ? std::sqrt(h.nrr / rhsNorm2) : 0.0;
     }
     rep->iterations = inner;

@@ -362,7 +362,10 @@ its_status exactStart(its_ctx* ctx, its_svo* const* svos, int64_t count, const d
 
 using namespace its;
 
-extern "C" its_status its_mlp_forward(its_mlp* mlp, const float* features, int64_t n, float* out);
+namespace its {
+its_status mlpInfer(its_mlp* mlp, const float* X, int64_t n, float* out);
+its_status mlpCheck(its_mlp* mlp);
+}  // namespace its
 
 extern "C" {
 
@@ -449,7 +452,7 @@ its_status its_learned_start_batch(its_svo* const* svos, int64_t count, its_mlp*
       return st;
     off += cnt[m];
   }
-  if (total > 0 && (st = its_mlp_forward(mlp, feat.p, total, pred.p)) != ITS_OK) return st;
+  if (total > 0 && (st = mlpInfer(mlp, feat.p, total, pred.p)) != ITS_OK) return st;
   off = 0;
   for (int64_t m = 0; m < count; ++m) {
     if ((st = scatterShares(ctx, svos[m]->d.coincIds, cnt[m], pred.p + off, hn[2 * kFeat + 1], hn[2 * kFeat], shares[m].p,
@@ -463,8 +466,9 @@ its_status its_learned_start_batch(its_svo* const* svos, int64_t count, its_mlp*
     host = host || L[m].host;
     if ((st = L[m].finish(ctx)) != ITS_OK) return st;
   }
-  // device outputs: ordered on the context's stream; host outputs: complete on return
-  if (host) ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  // device outputs: ordered on the context's stream (a tensor-core wait that ran out shows at
+  // the network's next checked call); host outputs: complete on return, network checked
+  if (host) return mlpCheck(mlp);
   return ITS_OK;
 }
 

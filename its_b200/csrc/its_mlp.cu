@@ -576,6 +576,26 @@ static its_status checkErr(its_mlp* h) {
   return ITS_OK;
 }
 
+// Predictions for n device rows into device out, launched on the context's stream without
+// waiting (the caller checks the error flag at its next synchronisation).
+its_status mlpInfer(its_mlp* h, const float* X, int64_t n, float* out) {
+  its_ctx* ctx = h->ctx;
+  if (n <= 0) return ITS_OK;
+  static bool configured = false;
+  if (!configured) {
+    ITS_CU(ctx, cudaFuncSetAttribute(kMlpForwardFused, cudaFuncAttributeMaxDynamicSharedMemorySize, kFusedSmem));
+    configured = true;
+  }
+  const int64_t tiles = (n + 127) / 128, ctas = (tiles + kFusedGroups - 1) / kFusedGroups;
+  const unsigned grid = (unsigned)(ctas < ctx->numSMs ? ctas : ctx->numSMs);
+  kMlpForwardFused<<<grid, 128 * kFusedGroups, kFusedSmem, ctx->stream>>>(X, n, h->W1, h->W2, h->W3, h->P, h->w4r, out,
+                                                                           h->err);
+  ITS_LAUNCHED(ctx);
+  return ITS_OK;
+}
+
+its_status mlpCheck(its_mlp* h) { return checkErr(h); }
+
 }  // namespace its
 
 extern "C" {
@@ -651,18 +671,7 @@ its_status its_mlp_forward(its_mlp* h, const float* X, int64_t n, float* out) {
   its_status st;
   if ((st = x.stage(ctx, X, n * kIn)) != ITS_OK) return st;
   if ((st = o.stage(ctx, out, n)) != ITS_OK) return st;
-  if (n > 0) {
-    static bool configured = false;
-    if (!configured) {
-      ITS_CU(ctx, cudaFuncSetAttribute(kMlpForwardFused, cudaFuncAttributeMaxDynamicSharedMemorySize, kFusedSmem));
-      configured = true;
-    }
-    const int64_t tiles = (n + 127) / 128, ctas = (tiles + kFusedGroups - 1) / kFusedGroups;
-    const unsigned grid = (unsigned)(ctas < ctx->numSMs ? ctas : ctx->numSMs);
-    kMlpForwardFused<<<grid, 128 * kFusedGroups, kFusedSmem, ctx->stream>>>(x.d, n, h->W1, h->W2, h->W3, h->P, h->w4r,
-                                                                             o.d, h->err);
-    ITS_LAUNCHED(ctx);
-  }
+  if ((st = mlpInfer(h, x.d, n, o.d)) != ITS_OK) return st;
   if ((st = o.finish(ctx)) != ITS_OK) return st;
   return checkErr(h);
 }

@@ -65,14 +65,8 @@ __global__ void kStartShares(const RowSeg* __restrict__ segs, const int64_t* __r
   s.lam[r] = (s.shares && rowCoincident(P, r, rowDepth(P, r))) ? s.shares[r] : 0.0;
 }
 
-// Surplus of the non-coincident rows of one depth per octree, the row summed in column order.
-__global__ void kStartLevel(const RowSeg* __restrict__ segs, const int64_t* __restrict__ prefix, int nseg,
-                            int64_t total) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= total) return;
-  const int g = findSeg(prefix, nseg, i);
-  const RowSeg& s = segs[g];
-  const int64_t r = s.rowBegin + (i - prefix[g]);
+// Surplus of one non-coincident row, the row summed in column order.
+__device__ __forceinline__ void startRow(const RowSeg& s, int64_t r) {
   const RowParams& P = *s.P;
   if (rowCoincident(P, r, s.d)) return;
   const double* lam = s.lam;
@@ -81,6 +75,33 @@ __global__ void kStartLevel(const RowSeg* __restrict__ segs, const int64_t* __re
     if (c != (int32_t)r) acc += v * lam[c];
   });
   s.lam[r] = s.b[r] - acc;
+}
+
+// One depth per octree (segments = that depth of every octree).
+__global__ void kStartLevel(const RowSeg* __restrict__ segs, const int64_t* __restrict__ prefix, int nseg,
+                            int64_t total) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const int g = findSeg(prefix, nseg, i);
+  startRow(segs[g], segs[g].rowBegin + (i - prefix[g]));
+}
+
+// The coarse depths, whose few rows would leave a launch per depth mostly idle: one block
+// walks depths t0..t1-1 in order (a block barrier between depths makes each depth's values
+// visible to the next), the rows of a depth spread over its threads.
+constexpr int kSmallLevelRows = 4096;
+__global__ void __launch_bounds__(1024) kStartLevelsSmall(const RowSeg* __restrict__ segs,
+                                                          const int64_t* __restrict__ prefix,
+                                                          const int* __restrict__ levelFirst,
+                                                          const int64_t* __restrict__ levelRows, int t0, int t1) {
+  for (int t = t0; t < t1; ++t) {
+    const int g0 = levelFirst[t], ng = levelFirst[t + 1] - g0;
+    for (int64_t i = threadIdx.x; i < levelRows[t]; i += blockDim.x) {
+      const int g = g0 + findSeg(prefix + g0, ng, i);
+      startRow(segs[g], segs[g].rowBegin + (i - prefix[g]));
+    }
+    __syncthreads();
+  }
 }
 
 constexpr int kResThreads = 256;
@@ -203,11 +224,27 @@ its_status exactStart(its_ctx* ctx, its_svo* const* svos, int64_t count, const d
   const int nseg = (int)segs.size();
   if (!nseg) return ITS_OK;
   DevBuf<RowSeg> dSegs;
-  DevBuf<int64_t> dPrefix;
-  if ((st = dSegs.alloc(ctx, nseg)) != ITS_OK || (st = dPrefix.alloc(ctx, nseg)) != ITS_OK) return st;
+  DevBuf<int64_t> dPrefix, dLevelRows;
+  DevBuf<int> dLevelFirst;
+  if ((st = dSegs.alloc(ctx, nseg)) != ITS_OK || (st = dPrefix.alloc(ctx, nseg)) != ITS_OK ||
+      (st = dLevelFirst.alloc(ctx, maxDepth + 1)) != ITS_OK || (st = dLevelRows.alloc(ctx, maxDepth)) != ITS_OK)
+    return st;
   ITS_CU(ctx, cudaMemcpyAsync(dSegs.p, segs.data(), nseg * sizeof(RowSeg), cudaMemcpyHostToDevice, ctx->stream));
   ITS_CU(ctx, cudaMemcpyAsync(dPrefix.p, prefix.data(), nseg * 8, cudaMemcpyHostToDevice, ctx->stream));
+  ITS_CU(ctx, cudaMemcpyAsync(dLevelFirst.p, first.data() + 1, (maxDepth + 1) * sizeof(int), cudaMemcpyHostToDevice,
+                              ctx->stream));
+  ITS_CU(ctx, cudaMemcpyAsync(dLevelRows.p, rows.data() + 1, maxDepth * 8, cudaMemcpyHostToDevice, ctx->stream));
+  // leading run of small depths (from the root): one launch for all of them
+  int tSmall = 0;
+  while (tSmall < maxDepth && rows[tSmall + 1] <= kSmallLevelRows) ++tSmall;
   for (int t = -1; t < maxDepth; ++t) {
+    if (t == 0 && tSmall >= 2) {
+      // shares first (t = -1 above), then the small depths together
+      kStartLevelsSmall<<<1, 1024, 0, ctx->stream>>>(dSegs.p, dPrefix.p, dLevelFirst.p, dLevelRows.p, 0, tSmall);
+      ITS_LAUNCHED(ctx);
+      t = tSmall - 1;
+      continue;
+    }
     const int g0 = first[t + 1], ng = first[t + 2] - g0;
     const int64_t total = rows[t + 1];
     if (!ng || !total) continue;
