@@ -261,16 +261,32 @@ __global__ void __launch_bounds__(128 * kFusedGroups, 1)
   const float* b2 = P + kOffB2;
   const float* b3 = P + kOffB3;
   const int64_t tiles = (n + 127) / 128;
+  const bool xVec = ((uintptr_t)X & 15) == 0;  // rows are 256 B apart: 16-byte loads when the base allows
   for (int64_t t = (int64_t)blockIdx.x * kFusedGroups + g; t < tiles; t += (int64_t)gridDim.x * kFusedGroups) {
     const int64_t m = t * 128 + row;
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {  // features -> BF16, this thread's row
-      __align__(16) bf16 v[8];
-#pragma unroll
-      for (int e = 0; e < 8; ++e) v[e] = __float2bfloat16_rn(m < n ? X[m * kIn + c * 8 + e] : 0.0f);
-      *(uint4*)(sX + swizzledChunk(row, c)) = *(const uint4*)v;
+    // features -> BF16: the tile's 128 rows x 256 B read in coalesced 32-byte pieces, each one
+    // 16-byte chunk of a row in the swizzled A tile
+#pragma unroll 2
+    for (int p = row; p < 128 * 8; p += 128) {
+      const int pr = p >> 3, pc = p & 7;
+      const int64_t mr = t * 128 + pr;
+      float4 f0 = make_float4(0.f, 0.f, 0.f, 0.f), f1 = f0;
+      if (mr < n) {
+        const float* src = X + mr * kIn + pc * 8;
+        if (xVec) {
+          f0 = ((const float4*)src)[0];
+          f1 = ((const float4*)src)[1];
+        } else {
+          f0 = make_float4(src[0], src[1], src[2], src[3]);
+          f1 = make_float4(src[4], src[5], src[6], src[7]);
+        }
+      }
+      __align__(16) bf16 v[8] = {__float2bfloat16_rn(f0.x), __float2bfloat16_rn(f0.y), __float2bfloat16_rn(f0.z),
+                                 __float2bfloat16_rn(f0.w), __float2bfloat16_rn(f1.x), __float2bfloat16_rn(f1.y),
+                                 __float2bfloat16_rn(f1.z), __float2bfloat16_rn(f1.w)};
+      *(uint4*)(sX + swizzledChunk(pr, pc)) = *(const uint4*)v;
     }
-    float acc[kHid];
+    float o = 0.0f;
     for (int layer = 0; layer < 3; ++layer) {
       fenceProxyAsync();
       fenceBefore();
@@ -295,29 +311,29 @@ __global__ void __launch_bounds__(128 * kFusedGroups, 1)
       ok = mbarWait(bar, phase) && ok;
       phase ^= 1u;
       fenceAfter();
-#pragma unroll
+      // epilogue, 16 accumulator columns at a time (a rolled loop keeps the code small)
+      const float* bias = layer == 0 ? b1 : (layer == 1 ? b2 : b3);
+#pragma unroll 1
       for (int n0 = 0; n0 < kHid; n0 += 16) {
         float v[16];
         tmemLoad16(tmem + lane + (uint32_t)n0, v);
+        if (layer < 2) {  // hidden layer: the next layer's A operand
 #pragma unroll
-        for (int j = 0; j < 16; ++j) acc[n0 + j] = v[j];
-      }
-      if (layer < 2) {  // hidden layer: the next layer's A operand
-        const float* bias = layer == 0 ? b1 : b2;
+          for (int h = 0; h < 2; ++h) {
+            __align__(16) bf16 q[8];
 #pragma unroll
-        for (int c = 0; c < 16; ++c) {
-          __align__(16) bf16 v[8];
+            for (int e = 0; e < 8; ++e) q[e] = __float2bfloat16_rn(geluF(v[h * 8 + e] + bias[n0 + h * 8 + e]));
+            const int c = (n0 >> 3) + h;
+            *(uint4*)(sH + (c >> 3) * 16384 + swizzledChunk(row, c & 7)) = *(const uint4*)q;
+          }
+        } else {  // output unit, columns in order
 #pragma unroll
-          for (int e = 0; e < 8; ++e) v[e] = __float2bfloat16_rn(geluF(acc[c * 8 + e] + bias[c * 8 + e]));
-          *(uint4*)(sH + (c >> 3) * 16384 + swizzledChunk(row, c & 7)) = *(const uint4*)v;
+          for (int j = 0; j < 16; ++j)
+            o += __bfloat162float(__float2bfloat16_rn(geluF(v[j] + bias[n0 + j]))) * w4r[n0 + j];
         }
-      } else if (m < n && ok) {  // output unit
-        float o = 0.0f;
-#pragma unroll
-        for (int j = 0; j < kHid; ++j) o += __bfloat162float(__float2bfloat16_rn(geluF(acc[j] + b3[j]))) * w4r[j];
-        out[m] = o + P[kOffB4];
       }
     }
+    if (m < n && ok) out[m] = o + P[kOffB4];
     fenceBefore();
     groupSync(g);  // every lane has read TMEM before the next tile's first MMA
   }

@@ -61,13 +61,12 @@ __device__ __forceinline__ bool rowCoincident(const RowParams& P, int64_t r, int
   return (((lin / (M * M)) | ((lin / M) % M) | (lin % M)) & 1u) == 0u;
 }
 
-// visit(col, val) for every entry of row r (depth d) in column order.
+// The coincident vertices of the finer depths at the point of a depth-d vertex with lattice
+// coordinates (X, Y, Z): visit(col) for depths j0..d-1, finest first (their value in the row
+// is 1). The chain stops at the first finer depth without a corner there.
 template <class Visit>
-__device__ __forceinline__ void walkRow(const RowParams& P, int64_t r, int d, Visit&& visit) {
-  const uint32_t M = P.lat[d].M;
-  const uint32_t lin = P.vertLin[r];
-  const uint32_t X = lin / (M * M), Y = (lin / M) % M, Z = lin % M;
-  const double qx = P.vertPos[3 * r], qy = P.vertPos[3 * r + 1], qz = P.vertPos[3 * r + 2];
+__device__ __forceinline__ void walkChain(const RowParams& P, int d, uint32_t X, uint32_t Y, uint32_t Z,
+                                          Visit&& visit) {
   int j0 = d;
   for (int j = d - 1; j >= 0; --j) {
     const int s = d - j;
@@ -80,43 +79,59 @@ __device__ __forceinline__ void walkRow(const RowParams& P, int64_t r, int d, Vi
     const int s = d - j;
     const uint32_t Mj = P.lat[j].M;
     const uint32_t lj = ((X << s) * Mj + (Y << s)) * Mj + (Z << s);
-    visit((int32_t)latticeRank(P.lat[j], lj), 1.0);
+    visit((int32_t)latticeRank(P.lat[j], lj));
   }
-  visit((int32_t)r, 1.0);
-  // The ancestors of the owner node: the octree's levels are O_{L+1} = O_L >> 3, so the
-  // ancestor k levels up has the owner's coordinates shifted right by k -- no walk along the
-  // parent links (a chain of dependent loads), the same nodes and the same arithmetic.
-  uint32_t Xo, Yo, Zo;
-  mortonDecode(P.morton[P.vertOwner[r]], Xo, Yo, Zo);
-  for (int dd = d + 1; dd < P.depth; ++dd) {
-    const int up = dd - d;
-    const uint32_t Xa = Xo >> up, Ya = Yo >> up, Za = Zo >> up;
-    const double w = P.w0 * (double)(1u << dd), wi = P.winv[dd];
-    const double bx = latticePos(P.g.x, w, Xa), by = latticePos(P.g.y, w, Ya), bz = latticePos(P.g.z, w, Za);
-    const LatticeIndex& L = P.lat[dd];
-    // the six axis factors once (the corners share them); visiting order and values unchanged
-    const double hxs[2] = {hat1r(qx, bx, w, wi), hat1r(qx, bx + w, w, wi)};
-    const double hys[2] = {hat1r(qy, by, w, wi), hat1r(qy, by + w, w, wi)};
-    const double hzs[2] = {hat1r(qz, bz, w, wi), hat1r(qz, bz + w, w, wi)};
+}
+
+// visit(col, val) for the non-zero hats at (qx, qy, qz) of the 8 corners of the depth-dd
+// ancestor of a depth-d node with Morton coordinates (Xo, Yo, Zo), corners in x-major order.
+// The octree's levels are O_{L+1} = O_L >> 3, so that ancestor has the node's coordinates
+// shifted right by dd - d -- no walk along the parent links (a chain of dependent loads).
+template <class Visit>
+__device__ __forceinline__ void walkAncestor(const RowParams& P, int d, int dd, uint32_t Xo, uint32_t Yo, uint32_t Zo,
+                                             double qx, double qy, double qz, Visit&& visit) {
+  const int up = dd - d;
+  const uint32_t Xa = Xo >> up, Ya = Yo >> up, Za = Zo >> up;
+  const double w = P.w0 * (double)(1u << dd), wi = P.winv[dd];
+  const double bx = latticePos(P.g.x, w, Xa), by = latticePos(P.g.y, w, Ya), bz = latticePos(P.g.z, w, Za);
+  const LatticeIndex& L = P.lat[dd];
+  // the six axis factors once (the corners share them)
+  const double hxs[2] = {hat1r(qx, bx, w, wi), hat1r(qx, bx + w, w, wi)};
+  const double hys[2] = {hat1r(qy, by, w, wi), hat1r(qy, by + w, w, wi)};
+  const double hzs[2] = {hat1r(qz, bz, w, wi), hat1r(qz, bz + w, w, wi)};
 #pragma unroll
-    for (int ox = 0; ox < 2; ++ox) {
-      const double hx = hxs[ox];
-      if (hx <= 0.0) continue;
+  for (int ox = 0; ox < 2; ++ox) {
+    const double hx = hxs[ox];
+    if (hx <= 0.0) continue;
 #pragma unroll
-      for (int oy = 0; oy < 2; ++oy) {
-        const double hy = hys[oy];
-        if (hy <= 0.0) continue;
+    for (int oy = 0; oy < 2; ++oy) {
+      const double hy = hys[oy];
+      if (hy <= 0.0) continue;
 #pragma unroll
-        for (int oz = 0; oz < 2; ++oz) {
-          const double hz = hzs[oz];
-          if (hz <= 0.0) continue;
-          const double v = hx * hy * hz;
-          if (v == 0.0) continue;
-          visit((int32_t)latticeRank(L, ((Xa + ox) * L.M + (Ya + oy)) * L.M + (Za + oz)), v);
-        }
+      for (int oz = 0; oz < 2; ++oz) {
+        const double hz = hzs[oz];
+        if (hz <= 0.0) continue;
+        const double v = hx * hy * hz;
+        if (v == 0.0) continue;
+        visit((int32_t)latticeRank(L, ((Xa + ox) * L.M + (Ya + oy)) * L.M + (Za + oz)), v);
       }
     }
   }
+}
+
+// visit(col, val) for every entry of row r (depth d) in column order: the finer coincident
+// vertices, the diagonal, then the corners of every ancestor of the owner, coarser last.
+template <class Visit>
+__device__ __forceinline__ void walkRow(const RowParams& P, int64_t r, int d, Visit&& visit) {
+  const uint32_t M = P.lat[d].M;
+  const uint32_t lin = P.vertLin[r];
+  const uint32_t X = lin / (M * M), Y = (lin / M) % M, Z = lin % M;
+  const double qx = P.vertPos[3 * r], qy = P.vertPos[3 * r + 1], qz = P.vertPos[3 * r + 2];
+  walkChain(P, d, X, Y, Z, [&](int32_t c) { visit(c, 1.0); });
+  visit((int32_t)r, 1.0);
+  uint32_t Xo, Yo, Zo;
+  mortonDecode(P.morton[P.vertOwner[r]], Xo, Yo, Zo);
+  for (int dd = d + 1; dd < P.depth; ++dd) walkAncestor(P, d, dd, Xo, Yo, Zo, qx, qy, qz, visit);
 }
 
 }  // namespace its

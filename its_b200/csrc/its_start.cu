@@ -1,4 +1,4 @@
-// Exact start of the thin-shell least-squares system (hierarchical surplus).
+// Exact start of the thin-shell least-squares system.
 //
 // Row v of A evaluates the fitted field at corner vertex v: the coincident vertices of the
 // finer depths (value 1), v itself (1), and the non-zero hats of the corners of every
@@ -10,20 +10,29 @@
 //   * a vertex whose lattice coordinates are all even (below the root depth) coincides with
 //     a corner of the next coarser depth; its coefficient is a free "share" (0 by default,
 //     or the value given, e.g. a learned prediction);
-//   * every other vertex, coarse depths first, takes the surplus
-//       lambda_v = b_v - sum_{u != v} A(v,u) lambda_u,
-//     whose terms are all known by then: coarser columns are final, and the finer columns
-//     of row v are coincident (even) vertices holding their shares.
+//   * every other vertex v takes its hierarchical surplus, the value at v minus what the
+//     coarser depths already put there.
 //
-// The result satisfies A lambda = b up to rounding for any shares: one pass over the rows of
-// A (one launch per depth), instead of the CGLS iterations. CGLS started there stops at once
-// (Eigen's solve with a guess tests the initial residual first), and because CGLS only moves
-// inside the row space of A, the shares fix the null-space component of the final
-// coefficients. The field at the corner vertices, and hence in every finest cell, is the
-// same for every exact solution; coarser cells differ by that null-space component.
+// The surplus needs no sweep over the depths. The coarser depths' part of the field,
+// F_{>d} = sum over depths dd > d of the hats of the depth-dd corners, is trilinear on the
+// cell P of depth d+1 that holds v (each depth-dd term is trilinear on its own cell, which
+// contains P), so it is the trilinear interpolant -- row v's hats of P's corners -- of its
+// values at P's corners c. Those values follow from row c alone: the row says
+// F_{>=d+1}(c) = b_c - (the finer coincident vertices at c), i.e. b_c minus shares. With
+//   G_u = b_u - sum of the shares of the finer coincident vertices at u's point,
+// every surplus is explicit:
+//   lambda_v = G_v - sum_{corners c of P} hat_c(v) G_c        (lambda_v = G_v at the root),
+// one independent row per vertex: two launches (G, then lambda) for any number of octrees,
+// one when the shares are zero (G = b). The result satisfies A lambda = b up to rounding
+// for any shares. CGLS started there stops at once (Eigen's solve with a guess tests the
+// initial residual first), and because CGLS only moves inside the row space of A, the
+// shares fix the null-space component of the final coefficients. The field at the corner
+// vertices, and hence in every finest cell, is the same for every exact solution; coarser
+// cells differ by that null-space component.
 //
-// Both passes here are matrix-free: the rows are generated from the octree by walkRow
-// (its_rows.cuh), in the assembled operator's column order, so no CSR is needed.
+// Both the start and the residual check are matrix-free: rows and their parts come from the
+// octree (walkRow, walkChain, walkAncestor in its_rows.cuh) in the assembled operator's
+// column order, so no CSR is needed.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -33,13 +42,13 @@
 
 namespace its {
 
-// One depth (or, for the residual, one chunk of rows) of one octree.
+// One octree (exact start) or one chunk of rows of an octree (residual).
 struct RowSeg {
   const RowParams* P;    // the octree's row parameters (device)
-  int d;                 // depth of the rows (exact start)
   int64_t rowBegin, rows;
   const double* b;
   const double* shares;  // may be null (all shares 0)
+  double* g;             // values less the finer shares (b itself when there are no shares)
   double* lam;
 };
 
@@ -53,55 +62,46 @@ __device__ __forceinline__ int findSeg(const int64_t* __restrict__ prefix, int n
   return lo;
 }
 
-// Shares of the coincident vertices, zeros elsewhere (segments: whole octrees).
-__global__ void kStartShares(const RowSeg* __restrict__ segs, const int64_t* __restrict__ prefix, int nseg,
+// G_r = b_r - the shares of the finer coincident vertices at r's point (finest first).
+__global__ void kStartValues(const RowSeg* __restrict__ segs, const int64_t* __restrict__ prefix, int nseg,
                              int64_t total) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= total) return;
-  const int g = findSeg(prefix, nseg, i);
-  const RowSeg& s = segs[g];
-  const int64_t r = s.rowBegin + (i - prefix[g]);
+  const int k = findSeg(prefix, nseg, i);
+  const RowSeg& s = segs[k];
+  const int64_t r = s.rowBegin + (i - prefix[k]);
   const RowParams& P = *s.P;
-  s.lam[r] = (s.shares && rowCoincident(P, r, rowDepth(P, r))) ? s.shares[r] : 0.0;
-}
-
-// Surplus of one non-coincident row, the row summed in column order.
-__device__ __forceinline__ void startRow(const RowSeg& s, int64_t r) {
-  const RowParams& P = *s.P;
-  if (rowCoincident(P, r, s.d)) return;
-  const double* lam = s.lam;
+  const int d = rowDepth(P, r);
+  const uint32_t M = P.lat[d].M, lin = P.vertLin[r];
   double acc = 0.0;
-  walkRow(P, r, s.d, [&](int32_t c, double v) {
-    if (c != (int32_t)r) acc += v * lam[c];
-  });
-  s.lam[r] = s.b[r] - acc;
+  if (s.shares) walkChain(P, d, lin / (M * M), (lin / M) % M, lin % M, [&](int32_t c) { acc += s.shares[c]; });
+  s.g[r] = s.b[r] - acc;
 }
 
-// One depth per octree (segments = that depth of every octree).
-__global__ void kStartLevel(const RowSeg* __restrict__ segs, const int64_t* __restrict__ prefix, int nseg,
-                            int64_t total) {
+// lambda_r: the share of a coincident vertex; otherwise G_r less the interpolant of G over
+// the corners of the owner's parent cell (the row's hats of that depth, in column order).
+__global__ void kStartInterp(const RowSeg* __restrict__ segs, const int64_t* __restrict__ prefix, int nseg,
+                             int64_t total) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= total) return;
-  const int g = findSeg(prefix, nseg, i);
-  startRow(segs[g], segs[g].rowBegin + (i - prefix[g]));
-}
-
-// The coarse depths, whose few rows would leave a launch per depth mostly idle: one block
-// walks depths t0..t1-1 in order (a block barrier between depths makes each depth's values
-// visible to the next), the rows of a depth spread over its threads.
-constexpr int kSmallLevelRows = 4096;
-__global__ void __launch_bounds__(1024) kStartLevelsSmall(const RowSeg* __restrict__ segs,
-                                                          const int64_t* __restrict__ prefix,
-                                                          const int* __restrict__ levelFirst,
-                                                          const int64_t* __restrict__ levelRows, int t0, int t1) {
-  for (int t = t0; t < t1; ++t) {
-    const int g0 = levelFirst[t], ng = levelFirst[t + 1] - g0;
-    for (int64_t i = threadIdx.x; i < levelRows[t]; i += blockDim.x) {
-      const int g = g0 + findSeg(prefix + g0, ng, i);
-      startRow(segs[g], segs[g].rowBegin + (i - prefix[g]));
-    }
-    __syncthreads();
+  const int k = findSeg(prefix, nseg, i);
+  const RowSeg& s = segs[k];
+  const int64_t r = s.rowBegin + (i - prefix[k]);
+  const RowParams& P = *s.P;
+  const int d = rowDepth(P, r);
+  if (rowCoincident(P, r, d)) {
+    s.lam[r] = s.shares ? s.shares[r] : 0.0;
+    return;
   }
+  const double* __restrict__ g = s.g;
+  double acc = 0.0;
+  if (d + 1 < P.depth) {
+    uint32_t Xo, Yo, Zo;
+    mortonDecode(P.morton[P.vertOwner[r]], Xo, Yo, Zo);
+    walkAncestor(P, d, d + 1, Xo, Yo, Zo, P.vertPos[3 * r], P.vertPos[3 * r + 1], P.vertPos[3 * r + 2],
+                 [&](int32_t c, double v) { acc += v * g[c]; });
+  }
+  s.lam[r] = g[r] - acc;
 }
 
 constexpr int kResThreads = 256;
@@ -178,82 +178,52 @@ static its_status uploadParams(its_ctx* ctx, its_svo* const* svos, int64_t count
   return ITS_OK;
 }
 
-// Exact starts of count octrees (device vectors), matrix-free: one launch for the shares and
-// one per depth (root first) for all octrees together.
+// Exact starts of count octrees (device vectors), matrix-free: G (when there are shares),
+// then lambda, each one launch for all octrees together.
 its_status exactStart(its_ctx* ctx, its_svo* const* svos, int64_t count, const double* const* b,
                       const double* const* shares, double* const* lam) {
   its_status st;
   DevBuf<RowParams> dP;
   if ((st = uploadParams(ctx, svos, count, dP)) != ITS_OK) return st;
-  int maxDepth = 0;
-  for (int64_t m = 0; m < count; ++m) maxDepth = std::max(maxDepth, svos[m]->d.depth);
+  bool anyShares = false;
+  int64_t total = 0;
+  for (int64_t m = 0; m < count; ++m) {
+    anyShares = anyShares || (shares && shares[m]);
+    total += svos[m]->d.numVerts;
+  }
+  DevBuf<double> G;
+  if (anyShares && (st = G.alloc(ctx, std::max<int64_t>(total, 1))) != ITS_OK) return st;
   std::vector<RowSeg> segs;
   std::vector<int64_t> prefix;
-  std::vector<int> first(maxDepth + 2, 0);
-  std::vector<int64_t> rows(maxDepth + 1, 0);
-  // level 0: whole octrees (shares); level t+1: depth (depth-1-t) of every octree
-  for (int t = -1; t < maxDepth; ++t) {
-    first[t + 1] = (int)segs.size();
-    int64_t acc = 0;
-    for (int64_t m = 0; m < count; ++m) {
-      const SvoDevice& d = svos[m]->d;
-      RowSeg s;
-      s.P = dP.p + m;
-      s.b = b[m];
-      s.shares = shares ? shares[m] : nullptr;
-      s.lam = lam[m];
-      if (t < 0) {
-        s.d = -1;
-        s.rowBegin = 0;
-        s.rows = d.numVerts;
-      } else {
-        const int dep = d.depth - 1 - t;
-        if (dep < 0 || d.vertCount[dep] == 0) continue;
-        s.d = dep;
-        s.rowBegin = d.vertStart[dep];
-        s.rows = d.vertCount[dep];
-      }
-      if (!s.rows) continue;
-      segs.push_back(s);
-      prefix.push_back(acc);
-      acc += s.rows;
-    }
-    rows[t + 1] = acc;
+  int64_t acc = 0;
+  for (int64_t m = 0; m < count; ++m) {
+    const int64_t n = svos[m]->d.numVerts;
+    if (!n) continue;
+    RowSeg s;
+    s.P = dP.p + m;
+    s.rowBegin = 0;
+    s.rows = n;
+    s.b = b[m];
+    s.shares = shares ? shares[m] : nullptr;
+    s.g = anyShares ? G.p + acc : const_cast<double*>(b[m]);  // no shares anywhere: G = b
+    s.lam = lam[m];
+    segs.push_back(s);
+    prefix.push_back(acc);
+    acc += n;
   }
-  first[maxDepth + 1] = (int)segs.size();
   const int nseg = (int)segs.size();
   if (!nseg) return ITS_OK;
   DevBuf<RowSeg> dSegs;
-  DevBuf<int64_t> dPrefix, dLevelRows;
-  DevBuf<int> dLevelFirst;
-  if ((st = dSegs.alloc(ctx, nseg)) != ITS_OK || (st = dPrefix.alloc(ctx, nseg)) != ITS_OK ||
-      (st = dLevelFirst.alloc(ctx, maxDepth + 1)) != ITS_OK || (st = dLevelRows.alloc(ctx, maxDepth)) != ITS_OK)
-    return st;
+  DevBuf<int64_t> dPrefix;
+  if ((st = dSegs.alloc(ctx, nseg)) != ITS_OK || (st = dPrefix.alloc(ctx, nseg)) != ITS_OK) return st;
   ITS_CU(ctx, cudaMemcpyAsync(dSegs.p, segs.data(), nseg * sizeof(RowSeg), cudaMemcpyHostToDevice, ctx->stream));
   ITS_CU(ctx, cudaMemcpyAsync(dPrefix.p, prefix.data(), nseg * 8, cudaMemcpyHostToDevice, ctx->stream));
-  ITS_CU(ctx, cudaMemcpyAsync(dLevelFirst.p, first.data() + 1, (maxDepth + 1) * sizeof(int), cudaMemcpyHostToDevice,
-                              ctx->stream));
-  ITS_CU(ctx, cudaMemcpyAsync(dLevelRows.p, rows.data() + 1, maxDepth * 8, cudaMemcpyHostToDevice, ctx->stream));
-  // leading run of small depths (from the root): one launch for all of them
-  int tSmall = 0;
-  while (tSmall < maxDepth && rows[tSmall + 1] <= kSmallLevelRows) ++tSmall;
-  for (int t = -1; t < maxDepth; ++t) {
-    if (t == 0 && tSmall >= 2) {
-      // shares first (t = -1 above), then the small depths together
-      kStartLevelsSmall<<<1, 1024, 0, ctx->stream>>>(dSegs.p, dPrefix.p, dLevelFirst.p, dLevelRows.p, 0, tSmall);
-      ITS_LAUNCHED(ctx);
-      t = tSmall - 1;
-      continue;
-    }
-    const int g0 = first[t + 1], ng = first[t + 2] - g0;
-    const int64_t total = rows[t + 1];
-    if (!ng || !total) continue;
-    if (t < 0)
-      kStartShares<<<gridFor(total, 256), 256, 0, ctx->stream>>>(dSegs.p + g0, dPrefix.p + g0, ng, total);
-    else
-      kStartLevel<<<gridFor(total, 128), 128, 0, ctx->stream>>>(dSegs.p + g0, dPrefix.p + g0, ng, total);
+  if (anyShares) {
+    kStartValues<<<gridFor(total, 256), 256, 0, ctx->stream>>>(dSegs.p, dPrefix.p, nseg, total);
     ITS_LAUNCHED(ctx);
   }
+  kStartInterp<<<gridFor(total, 256), 256, 0, ctx->stream>>>(dSegs.p, dPrefix.p, nseg, total);
+  ITS_LAUNCHED(ctx);
   return ITS_OK;  // the tables were copied from pageable memory (staged at the call)
 }
 
@@ -272,11 +242,11 @@ its_status fitResidual(its_ctx* ctx, its_svo* const* svos, int64_t count, const 
     for (int64_t r0 = 0; r0 < n; r0 += kResChunk) {
       RowSeg s;
       s.P = dP.p + m;
-      s.d = -1;
       s.rowBegin = r0;
       s.rows = std::min(kResChunk, n - r0);
       s.b = b[m];
       s.shares = nullptr;
+      s.g = nullptr;
       s.lam = const_cast<double*>(lam[m]);
       segs.push_back(s);
     }

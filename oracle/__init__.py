@@ -55,6 +55,7 @@ def _declare(L):
         "orc_csr_free": (None, [vp]),
         "orc_cgls": (i32, [vp, vp, vp, dbl, i64, i32, vp]),
         "orc_exact_start": (None, [vp, vp, vp, vp, vp]),
+        "orc_exact_start_surplus": (None, [vp, vp, vp, vp, vp]),
         "orc_point_gradient": (None, [vp, vp, vp, vp, i64, vp, vp, vp, vp, vp]),
         "orc_intersections": (vp, [vp, vp, i64, vp, i64]),
         "orc_points_count": (i64, [vp, vp]),
@@ -191,16 +192,19 @@ class Svo:
         lib().orc_point_gradient(self.h, _p(lam), _p(P), _p(bf), m, _p(bo), _p(be), _p(val), _p(grad), _p(miss))
         return val, grad, miss
 
-    def exact_start(self, b, shares=None):
-        """Hierarchical-surplus exact solution of A lambda = b for this octree's operator
-        (shares: coefficients of the vertices coincident with a coarser corner, default 0)."""
+    def exact_start(self, b, shares=None, form="explicit"):
+        """Exact solution of A lambda = b for this octree's operator (shares: coefficients of
+        the vertices coincident with a coarser corner, default 0). form "explicit": each
+        surplus from G = b - finer shares (orc_exact_start); "surplus": the sequential
+        coarse-to-fine definition (orc_exact_start_surplus)."""
         rp, col, val = self.assemble()
         b = _f64(b)
         h = lib().orc_csr_from(rp.shape[0] - 1, _p(rp), _p(col), _p(val))
         out = np.zeros(rp.shape[0] - 1)
         sh = None if shares is None else _f64(shares)
+        fn = lib().orc_exact_start if form == "explicit" else lib().orc_exact_start_surplus
         try:
-            lib().orc_exact_start(self.h, h, _p(b), _p(sh), _p(out))
+            fn(self.h, h, _p(b), _p(sh), _p(out))
         finally:
             lib().orc_csr_free(h)
         return out

@@ -125,6 +125,10 @@ void orc_exact_start(void* h, void* a, const double* b, const double* shares, do
   exactStart(*static_cast<Svo*>(h), *static_cast<Csr*>(a), b, shares, lambda);
 }
 
+void orc_exact_start_surplus(void* h, void* a, const double* b, const double* shares, double* lambda) {
+  exactStartSurplus(*static_cast<Svo*>(h), *static_cast<Csr*>(a), b, shares, lambda);
+}
+
 void orc_point_gradient(void* h, const double* lambda, const double* P, const double* before, int64_t m,
                         const double* boxOrigin, const double* boxEnd, double* val, double* grad, uint8_t* missing) {
   pointValGradient(*static_cast<Svo*>(h), lambda, P, before, m, boxOrigin, boxEnd, val, grad, missing);

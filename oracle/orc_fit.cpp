@@ -699,16 +699,14 @@ void marchingCubesMesh(const double* field, int R, const double origin[3], const
 
 namespace orc {
 
-// Exact start (hierarchical surplus) of A lambda = b, sequentially, coarse depths first.
-// A vertex of depth d below the root whose lattice coordinates (recovered from its position,
-// (p - gridOrigin) / (unit * 2^d), to the nearest integer) are all even coincides with a
-// corner of depth d + 1: it keeps its share. Every other row, coarse depths first, solves
-// lambda_v = b_v - sum_{u != v} A(v,u) lambda_u with the entries summed in column order.
-void exactStart(const Svo& s, const Csr& A, const double* b, const double* shares, double* lambda) {
+// Coincident flags and depth starts of the corner vertices. A vertex of depth d below the
+// root whose lattice coordinates (recovered from its position, (p - gridOrigin) /
+// (unit * 2^d), to the nearest integer) are all even coincides with a corner of depth d + 1.
+static void startTables(const Svo& s, int64_t n, std::vector<int64_t>& start, std::vector<char>& coincident) {
   const int depth = s.treeDepth;
-  std::vector<int64_t> start(depth + 1, 0);
+  start.assign(depth + 1, 0);
   for (int d = 0; d < depth; ++d) start[d + 1] = start[d] + (int64_t)s.depthVerts[d].size();
-  std::vector<char> coincident(A.n, 0);
+  coincident.assign(n, 0);
   for (int d = 0; d + 1 < depth; ++d) {
     const double w = s.unit.x * (double)(1u << d);
     for (size_t k = 0; k < s.depthVerts[d].size(); ++k) {
@@ -718,8 +716,52 @@ void exactStart(const Svo& s, const Csr& A, const double* b, const double* share
       coincident[start[d] + (int64_t)k] = ((X | Y | Z) & 1) == 0;
     }
   }
+}
+
+// Exact start of A lambda = b in explicit form, read off the assembled rows. Coincident
+// vertices keep their shares. With G_r = b_r - (row r's finer coincident columns, value 1,
+// times their shares), every other row is
+//   lambda_r = G_r - sum over row r's entries of depth d+1 (its owner's parent cell) of A(r,c) G_c,
+// both sums in column order: the coarser depths' part of the field is trilinear on that cell,
+// and its values at the cell's corners are G.
+void exactStart(const Svo& s, const Csr& A, const double* b, const double* shares, double* lambda) {
+  std::vector<int64_t> start;
+  std::vector<char> coincident;
+  startTables(s, A.n, start, coincident);
+  const int depth = s.treeDepth;
+  std::vector<double> G(A.n);
+  std::vector<int> rowDepth(A.n);
+  for (int d = 0; d < depth; ++d)
+    for (int64_t r = start[d]; r < start[d + 1]; ++r) rowDepth[r] = d;
+  for (int64_t r = 0; r < A.n; ++r) {
+    double acc = 0.0;
+    if (shares)
+      for (int64_t k = A.rowptr[r]; k < A.rowptr[r + 1]; ++k)
+        if (A.col[k] < start[rowDepth[r]]) acc += A.val[k] * shares[A.col[k]];
+    G[r] = b[r] - acc;
+  }
+  for (int64_t r = 0; r < A.n; ++r) {
+    const int d = rowDepth[r];
+    if (coincident[r]) {
+      lambda[r] = shares ? shares[r] : 0.0;
+      continue;
+    }
+    double acc = 0.0;
+    if (d + 1 < depth)
+      for (int64_t k = A.rowptr[r]; k < A.rowptr[r + 1]; ++k)
+        if (A.col[k] >= start[d + 1] && A.col[k] < start[d + 2]) acc += A.val[k] * G[A.col[k]];
+    lambda[r] = G[r] - acc;
+  }
+}
+
+// The same solution by the sequential definition, coarse depths first: every non-coincident
+// row solves lambda_v = b_v - sum_{u != v} A(v,u) lambda_u, its entries summed in column order.
+void exactStartSurplus(const Svo& s, const Csr& A, const double* b, const double* shares, double* lambda) {
+  std::vector<int64_t> start;
+  std::vector<char> coincident;
+  startTables(s, A.n, start, coincident);
   for (int64_t r = 0; r < A.n; ++r) lambda[r] = (coincident[r] && shares) ? shares[r] : 0.0;
-  for (int d = depth - 1; d >= 0; --d) {
+  for (int d = s.treeDepth - 1; d >= 0; --d) {
     for (int64_t r = start[d]; r < start[d + 1]; ++r) {
       if (coincident[r]) continue;
       double acc = 0.0;

@@ -25,6 +25,7 @@ Csr assemble(const Svo& s);
 Csr transpose(const Csr& A);
 CglsReport cgls(const Csr& A, const Csr& T, const double* b, double* x, double tol, int64_t maxIters, int stop);
 void exactStart(const Svo& s, const Csr& A, const double* b, const double* shares, double* lambda);
+void exactStartSurplus(const Svo& s, const Csr& A, const double* b, const double* shares, double* lambda);
 void evalPoints(const Svo& s, const double* lambda, const double* P, int64_t m, double* out, uint8_t* missing);
 // ThinShells::getPointValGradient (ThinShells.cpp:1800-1866): a point outside the box is moved
 // halfway towards its previous position until inside (before may be null: no move), then the

@@ -206,8 +206,8 @@ def test_exact_start_matches_oracle(ctx, name, kw, res):
     op = Operator(gpu)
     rp, col, val = ref.assemble()
     A = sp.csr_matrix((val, col, rp), shape=(op.rows, op.rows))
-    # zero shares: an exact solution; the GPU generates each row from the octree and sums it
-    # in column order like the oracle, so the two are bit-identical
+    # zero shares: an exact solution; the GPU generates each row's parent-cell hats from the
+    # octree and sums them in column order like the oracle, so the two are bit-identical
     lam_ref = ref.exact_start(b)
     lam = gpu.exact_start(b)
     assert np.array_equal(lam, lam_ref)
