@@ -18,7 +18,7 @@ __global__ void kAssembleRows(const __grid_constant__ RowParams P, int64_t n, in
   const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (r >= n) return;
   int64_t k = FILL ? rowptrOrCount[r] : 0;
-  walkRow(P, r, rowDepth(P, r), [&](int32_t c, double v) {
+  walkRow(P, r, [&](int32_t c, double v) {
     if (FILL) {
       col[k] = c;
       val[k] = v;

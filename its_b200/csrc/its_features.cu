@@ -132,6 +132,7 @@ struct FeatParams {
   LatticeIndex lat[kMaxDepth];
   int64_t vertStart[kMaxDepth + 1];
   const uint32_t* vertLin;
+  const uint64_t* vertKey;
   const uint32_t* vertOwner;
   const double* vertPos;
   const uint32_t* nodeNb;
@@ -162,95 +163,154 @@ __global__ void kMarkCoincident(const __grid_constant__ FeatParams P, int64_t n,
   flag[v] = coincidentVertex(P, v, vertDepth(P, v)) ? 1u : 0u;
 }
 
-__global__ void kShareFeatures(const __grid_constant__ FeatParams P, const int64_t* __restrict__ ids, int64_t count,
-                               const double* __restrict__ b, const double* __restrict__ lam0, NodeStats S,
-                               const float* __restrict__ norm, float* __restrict__ out) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= count) return;
-  const int64_t v = ids[i];
-  const int d = vertDepth(P, v);
-  const uint32_t M = P.lat[d].M, lin = P.vertLin[v];
-  const int64_t X = lin / (M * M), Y = (lin / M) % M, Z = lin % M;
-  const double w = P.w0 * (double)(1u << d);
-  float f[kFeat];
+// Feature normalisation (mean[64], scale[64]) passed by value with the launch.
+struct FeatNorm {
+  float v[2 * kFeat];
+  int on;
+};
+
+constexpr int kFeatLanes = 4;                       // lanes per vertex
+constexpr int kFeatThreads = 128;
+constexpr int kFeatRows = kFeatThreads / kFeatLanes;  // vertices per block
+
+// Four lanes per vertex: lane 0 the coincident copies above and the scalar features, lane 1
+// the copies below, the face neighbours split over the lanes, the owner's 27-neighbourhood
+// sample sums strided over the lanes and added by a fixed shuffle tree. The block's rows go
+// through shared memory so that the normalised features leave in coalesced stores.
+__global__ void __launch_bounds__(kFeatThreads) kShareFeatures(const __grid_constant__ FeatParams P,
+                                                               const int64_t* __restrict__ ids, int64_t count,
+                                                               const double* __restrict__ b,
+                                                               const double* __restrict__ lam0, NodeStats S,
+                                                               const __grid_constant__ FeatNorm norm,
+                                                               float* __restrict__ out) {
+  __shared__ __align__(16) float sf[kFeatRows][kFeat];
+  const int sub = threadIdx.x & (kFeatLanes - 1), slot = threadIdx.x / kFeatLanes;
+  const int64_t i0 = (int64_t)blockIdx.x * kFeatRows, i = i0 + slot;
+  float* f = sf[slot];
 #pragma unroll
-  for (int k = 0; k < kFeat; ++k) f[k] = 0.0f;
-  const double bv = b[v];
-  // the coincident copies above and below
-  int up = 0, down = 0;
-  int64_t top = v, X1 = X, Y1 = Y, Z1 = Z;
-  double oneUp = 0.0;
-  for (int dd = d + 1; dd < P.depth; ++dd) {
-    if ((X1 | Y1 | Z1) & 1) break;
-    X1 >>= 1;
-    Y1 >>= 1;
-    Z1 >>= 1;
-    const int64_t u = latticeVertex(P, dd, X1, Y1, Z1);
-    if (u < 0) break;
-    if (dd == d + 1) oneUp = lam0[u];
-    top = u;
-    ++up;
-  }
-  for (int dd = d - 1; dd >= 0; --dd) {
-    const int s = d - dd;
-    if (latticeVertex(P, dd, X << s, Y << s, Z << s) < 0) break;
-    ++down;
-  }
-  f[0] = (float)bv;
-  f[1] = (float)lam0[top];
-  f[2] = (float)oneUp;
-  f[3] = P.depth > 1 ? (float)d / (float)(P.depth - 1) : 0.0f;
-  f[4] = (float)up / (float)P.depth;
-  f[5] = (float)down / (float)P.depth;
-  const int ex[6] = {1, -1, 0, 0, 0, 0}, ey[6] = {0, 0, 1, -1, 0, 0}, ez[6] = {0, 0, 0, 0, 1, -1};
-#pragma unroll
-  for (int k = 0; k < 6; ++k) {
-    const int64_t u = latticeVertex(P, d, X + ex[k], Y + ey[k], Z + ez[k]);
-    if (u >= 0) {
-      f[6 + k] = 1.0f;
-      f[12 + k] = (float)(b[u] - bv);
-      f[18 + k] = (float)lam0[u];
+  for (int k = 0; k < kFeat / kFeatLanes; ++k) f[sub * (kFeat / kFeatLanes) + k] = 0.0f;
+  __syncwarp();
+  const bool valid = i < count;
+  double c = 0.0, p[3] = {0, 0, 0}, q[3] = {0, 0, 0};
+  int64_t v = 0;
+  int d = 0;
+  double w = 0.0;
+  if (valid) {
+    v = ids[i];
+    const VertCoord vc = decodeVertKey(P.vertKey[v]);
+    d = vc.d;
+    const int64_t X = vc.X, Y = vc.Y, Z = vc.Z;
+    w = P.w0 * (double)(1u << d);
+    const double bv = b[v];
+    if (sub == 0) {  // the coincident copies above
+      int up = 0;
+      int64_t top = v, X1 = X, Y1 = Y, Z1 = Z;
+      double oneUp = 0.0;
+      for (int dd = d + 1; dd < P.depth; ++dd) {
+        if ((X1 | Y1 | Z1) & 1) break;
+        X1 >>= 1;
+        Y1 >>= 1;
+        Z1 >>= 1;
+        const int64_t u = latticeVertex(P, dd, X1, Y1, Z1);
+        if (u < 0) break;
+        if (dd == d + 1) oneUp = lam0[u];
+        top = u;
+        ++up;
+      }
+      f[0] = (float)bv;
+      f[1] = (float)lam0[top];
+      f[2] = (float)oneUp;
+      f[3] = P.depth > 1 ? (float)d / (float)(P.depth - 1) : 0.0f;
+      f[4] = (float)up / (float)P.depth;
+      f[36] = (float)w;
+      f[37] = (float)(bv / w);
+    } else if (sub == 1) {  // the coincident copies below
+      int down = 0;
+      for (int dd = d - 1; dd >= 0; --dd) {
+        const int s = d - dd;
+        if (latticeVertex(P, dd, X << s, Y << s, Z << s) < 0) break;
+        ++down;
+      }
+      f[5] = (float)down / (float)P.depth;
     }
-    if (d > 0) {
-      const int64_t q = latticeVertex(P, d - 1, 2 * X + ex[k], 2 * Y + ey[k], 2 * Z + ez[k]);
-      if (q >= 0) {
-        f[24 + k] = 1.0f;
-        f[30 + k] = (float)lam0[q];
+    // face neighbours: lanes 0, 1 one each, lanes 2, 3 two each
+    const int ex[6] = {1, -1, 0, 0, 0, 0}, ey[6] = {0, 0, 1, -1, 0, 0}, ez[6] = {0, 0, 0, 0, 1, -1};
+    const int k0 = sub < 2 ? sub : 2 * sub - 2, k1 = sub < 2 ? sub + 1 : 2 * sub;
+    for (int k = k0; k < k1; ++k) {
+      const int64_t u = latticeVertex(P, d, X + ex[k], Y + ey[k], Z + ez[k]);
+      if (u >= 0) {
+        f[6 + k] = 1.0f;
+        f[12 + k] = (float)(b[u] - bv);
+        f[18 + k] = (float)lam0[u];
+      }
+      if (d > 0) {
+        const int64_t qv = latticeVertex(P, d - 1, 2 * X + ex[k], 2 * Y + ey[k], 2 * Z + ez[k]);
+        if (qv >= 0) {
+          f[24 + k] = 1.0f;
+          f[30 + k] = (float)lam0[qv];
+        }
+      }
+    }
+    // samples in the owner's 27-neighbourhood, strided over the lanes
+    const uint32_t o = P.vertOwner[v];
+    for (int k = sub; k < 27; k += kFeatLanes) {
+      const uint32_t t = P.nodeNb[27 * (int64_t)o + k];
+      if (t == kNone) continue;
+      c += (double)S.cnt[t];
+      for (int a = 0; a < 3; ++a) {
+        p[a] += S.sp[3 * (int64_t)t + a];
+        q[a] += S.sn[3 * (int64_t)t + a];
       }
     }
   }
-  f[36] = (float)w;
-  f[37] = (float)(bv / w);
-  // samples in the owner's 27-neighbourhood
-  const uint32_t o = P.vertOwner[v];
-  double c = 0.0, p[3] = {0, 0, 0}, q[3] = {0, 0, 0};
-  for (int k = 0; k < 27; ++k) {
-    const uint32_t t = P.nodeNb[27 * (int64_t)o + k];
-    if (t == kNone) continue;
-    c += (double)S.cnt[t];
-    for (int a = 0; a < 3; ++a) {
-      p[a] += S.sp[3 * (int64_t)t + a];
-      q[a] += S.sn[3 * (int64_t)t + a];
-    }
-  }
-  f[38] = (float)log1p(c);
-  if (c > 0.0) {
-    const double* x = P.vertPos + 3 * v;
-    double nn = 0.0;
-    for (int a = 0; a < 3; ++a) {
-      f[39 + a] = (float)((p[a] / c - x[a]) / w);
-      const double m = q[a] / c;
-      f[42 + a] = (float)m;
-      nn += m * m;
-    }
-    f[45] = (float)(1.0 - sqrt(nn));
-  }
-  float* row = out + i * kFeat;
 #pragma unroll
-  for (int k = 0; k < kFeat; ++k) row[k] = norm ? (f[k] - norm[k]) * norm[kFeat + k] : f[k];
+  for (int off = kFeatLanes / 2; off > 0; off >>= 1) {
+    c += __shfl_down_sync(0xffffffffu, c, off, kFeatLanes);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      p[a] += __shfl_down_sync(0xffffffffu, p[a], off, kFeatLanes);
+      q[a] += __shfl_down_sync(0xffffffffu, q[a], off, kFeatLanes);
+    }
+  }
+  if (valid && sub == 0) {
+    f[38] = (float)log1p(c);
+    if (c > 0.0) {
+      const double* x = P.vertPos + 3 * v;
+      double nn = 0.0;
+      for (int a = 0; a < 3; ++a) {
+        f[39 + a] = (float)((p[a] / c - x[a]) / w);
+        const double m = q[a] / c;
+        f[42 + a] = (float)m;
+        nn += m * m;
+      }
+      f[45] = (float)(1.0 - sqrt(nn));
+    }
+  }
+  __syncthreads();
+  // the block's rows are consecutive in out: float4 stores over all of them
+  const int64_t rows = count - i0 < kFeatRows ? count - i0 : kFeatRows;
+  for (int e = threadIdx.x; e < rows * (kFeat / 4); e += kFeatThreads) {
+    const int r = e / (kFeat / 4), k = 4 * (e % (kFeat / 4));
+    float4 x = *(const float4*)&sf[r][k];
+    if (norm.on) {
+      x.x = (x.x - norm.v[k]) * norm.v[kFeat + k];
+      x.y = (x.y - norm.v[k + 1]) * norm.v[kFeat + k + 1];
+      x.z = (x.z - norm.v[k + 2]) * norm.v[kFeat + k + 2];
+      x.w = (x.w - norm.v[k + 3]) * norm.v[kFeat + k + 3];
+    }
+    float* dst = out + (i0 + r) * kFeat + k;
+    if (((uintptr_t)out & 15) == 0) {
+      *(float4*)dst = x;
+    } else {
+      dst[0] = x.x;
+      dst[1] = x.y;
+      dst[2] = x.z;
+      dst[3] = x.w;
+    }
+  }
 }
 
-// Learned shares into a zeroed share vector: share[ids[i]] = pred[i] * scale + mean.
+// Learned shares of the coincident vertices: share[ids[i]] = pred[i] * scale + mean.
 __global__ void kScatterShares(const int64_t* __restrict__ ids, int64_t count, const float* __restrict__ pred,
                                float scale, float mean, double* __restrict__ shares) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -266,6 +326,7 @@ static FeatParams featParams(const SvoDevice& d) {
   for (int L = 0; L < kMaxDepth; ++L) P.lat[L] = L < d.depth ? d.lattice(L) : LatticeIndex{};
   for (int L = 0; L <= kMaxDepth; ++L) P.vertStart[L] = L <= d.depth ? d.vertStart[L] : d.numVerts;
   P.vertLin = d.vertLin;
+  P.vertKey = d.vertKey;
   P.vertOwner = d.vertOwner;
   P.vertPos = d.vertPos;
   P.nodeNb = d.nodeNb;
@@ -331,21 +392,25 @@ its_status nodeSampleStats(its_ctx* ctx, SvoDevice& d, const double* V, const in
   return ITS_OK;
 }
 
-// Features of the coincident vertices ids[0..count) (see the file comment).
+// Features of the coincident vertices ids[0..count) (see the file comment); hostNorm (host
+// memory, may be null) the normalisation.
 its_status shareFeatures(its_ctx* ctx, const SvoDevice& d, const double* b, const double* lam0, const int64_t* ids,
-                         int64_t count, const float* norm, float* out) {
+                         int64_t count, const float* hostNorm, float* out) {
   const FeatParams P = featParams(d);
   NodeStats S{d.nodeSampleCnt, d.nodeSamplePos, d.nodeSampleNrm};
+  FeatNorm norm;
+  norm.on = hostNorm != nullptr;
+  for (int k = 0; k < 2 * kFeat; ++k) norm.v[k] = hostNorm ? hostNorm[k] : 0.0f;
   if (count > 0) {
-    kShareFeatures<<<gridFor(count, 128), 128, 0, ctx->stream>>>(P, ids, count, b, lam0, S, norm, out);
+    kShareFeatures<<<gridFor(count, kFeatRows), kFeatThreads, 0, ctx->stream>>>(P, ids, count, b, lam0, S, norm, out);
     ITS_LAUNCHED(ctx);
   }
   return ITS_OK;
 }
 
+// Learned shares of the coincident vertices (the exact start reads shares nowhere else).
 its_status scatterShares(its_ctx* ctx, const int64_t* ids, int64_t count, const float* pred, float scale, float mean,
-                         double* shares, int64_t n) {
-  ITS_CU(ctx, cudaMemsetAsync(shares, 0, n * 8, ctx->stream));
+                         double* shares) {
   if (count > 0) {
     kScatterShares<<<gridFor(count, 256), 256, 0, ctx->stream>>>(ids, count, pred, scale, mean, shares);
     ITS_LAUNCHED(ctx);
@@ -378,8 +443,14 @@ its_status its_share_features(its_svo* svo, const double* b, const float* norm, 
   const int64_t n = d.numVerts;
   its_status st;
   InArg<double> db;
-  InArg<float> dn;
-  if ((st = db.stage(ctx, b, n)) != ITS_OK || (st = dn.stage(ctx, norm, norm ? 2 * kFeat : 0)) != ITS_OK) return st;
+  if ((st = db.stage(ctx, b, n)) != ITS_OK) return st;
+  float hn[2 * kFeat];
+  if (norm && isDevicePtr(norm)) {
+    ITS_CU(ctx, cudaMemcpyAsync(hn, norm, sizeof(hn), cudaMemcpyDeviceToHost, ctx->stream));
+    ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  } else if (norm) {
+    std::memcpy(hn, norm, sizeof(hn));
+  }
   const int64_t cnt = d.numCoinc;
   const int64_t* dIds = d.coincIds;
   *count = cnt;
@@ -392,7 +463,7 @@ its_status its_share_features(its_svo* svo, const double* b, const float* norm, 
   if ((st = exactStart(ctx, &svo, 1, &bp, nullptr, &lp)) != ITS_OK) return st;
   OutArg<float> out;
   if ((st = out.stage(ctx, features, cnt * kFeat)) != ITS_OK) return st;
-  if ((st = shareFeatures(ctx, d, db.d, lam0.p, dIds, cnt, dn.d, out.d)) != ITS_OK) return st;
+  if ((st = shareFeatures(ctx, d, db.d, lam0.p, dIds, cnt, norm ? hn : nullptr, out.d)) != ITS_OK) return st;
   if ((st = out.finish(ctx)) != ITS_OK) return st;
   if (ids) ITS_CU(ctx, cudaMemcpyAsync(ids, dIds, cnt * 8, cudaMemcpyDefault, ctx->stream));
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
@@ -417,9 +488,6 @@ its_status its_learned_start_batch(its_svo* const* svos, int64_t count, its_mlp*
   } else {
     std::memcpy(hn, norm, sizeof(hn));
   }
-  DevBuf<float> dNorm;
-  if ((st = dNorm.alloc(ctx, 2 * kFeat)) != ITS_OK) return st;
-  ITS_CU(ctx, cudaMemcpyAsync(dNorm.p, hn, 2 * kFeat * 4, cudaMemcpyHostToDevice, ctx->stream));
   std::vector<InArg<double>> B(count);
   std::vector<OutArg<double>> L(count);
   std::vector<DevBuf<double>> lam0(count), shares(count);
@@ -447,7 +515,7 @@ its_status its_learned_start_batch(its_svo* const* svos, int64_t count, its_mlp*
     return st;
   int64_t off = 0;
   for (int64_t m = 0; m < count; ++m) {
-    if ((st = shareFeatures(ctx, svos[m]->d, bp[m], l0[m], svos[m]->d.coincIds, cnt[m], dNorm.p,
+    if ((st = shareFeatures(ctx, svos[m]->d, bp[m], l0[m], svos[m]->d.coincIds, cnt[m], hn,
                             feat.p + off * kFeat)) != ITS_OK)
       return st;
     off += cnt[m];
@@ -455,8 +523,8 @@ its_status its_learned_start_batch(its_svo* const* svos, int64_t count, its_mlp*
   if (total > 0 && (st = mlpInfer(mlp, feat.p, total, pred.p)) != ITS_OK) return st;
   off = 0;
   for (int64_t m = 0; m < count; ++m) {
-    if ((st = scatterShares(ctx, svos[m]->d.coincIds, cnt[m], pred.p + off, hn[2 * kFeat + 1], hn[2 * kFeat], shares[m].p,
-                            svos[m]->d.numVerts)) != ITS_OK)
+    if ((st = scatterShares(ctx, svos[m]->d.coincIds, cnt[m], pred.p + off, hn[2 * kFeat + 1], hn[2 * kFeat],
+                            shares[m].p)) != ITS_OK)
       return st;
     off += cnt[m];
   }

@@ -102,6 +102,29 @@ __device__ __forceinline__ uint32_t latticeRank(const LatticeIndex& L, uint32_t 
   return L.base + L.rank[lin >> 6] + (uint32_t)__popcll(below);
 }
 
+// ---- packed vertex key: X | Y << 11 | Z << 22 | depth << 33 | owner corner bits 37-39 ----
+struct VertCoord {
+  uint32_t X, Y, Z;     // lattice coordinates at the vertex's depth
+  int d;                // depth
+  uint32_t Xo, Yo, Zo;  // the owner node's coordinates (the vertex is its corner X-Xo, Y-Yo, Z-Zo)
+};
+__host__ __device__ inline VertCoord decodeVertKey(uint64_t k) {
+  VertCoord c;
+  c.X = (uint32_t)k & 2047u;
+  c.Y = (uint32_t)(k >> 11) & 2047u;
+  c.Z = (uint32_t)(k >> 22) & 2047u;
+  c.d = (int)((k >> 33) & 15u);
+  c.Xo = c.X - ((uint32_t)(k >> 37) & 1u);
+  c.Yo = c.Y - ((uint32_t)(k >> 38) & 1u);
+  c.Zo = c.Z - ((uint32_t)(k >> 39) & 1u);
+  return c;
+}
+__host__ __device__ inline uint64_t encodeVertKey(uint32_t X, uint32_t Y, uint32_t Z, int d, uint32_t Xo, uint32_t Yo,
+                                                  uint32_t Zo) {
+  return (uint64_t)X | ((uint64_t)Y << 11) | ((uint64_t)Z << 22) | ((uint64_t)d << 33) | ((uint64_t)(X - Xo) << 37) |
+         ((uint64_t)(Y - Yo) << 38) | ((uint64_t)(Z - Zo) << 39);
+}
+
 // ---- octree on the device (structure of arrays; finest depth first, root last) ------
 struct SvoDevice {
   int res = 0, depth = 0;
@@ -119,6 +142,8 @@ struct SvoDevice {
   unsigned long long* vbits[kMaxDepth] = {nullptr};
   uint32_t* vrank[kMaxDepth] = {nullptr};
   uint32_t* vertLin = nullptr;     // lattice index within its depth
+  uint64_t* vertKey = nullptr;     // lattice coordinates, depth and the vertex's corner of its owner:
+                                   // X | Y << 11 | Z << 22 | depth << 33 | (X - Xo) << 37 | (Y - Yo) << 38 | (Z - Zo) << 39
   uint32_t* vertOwner = nullptr;   // lowest-index node having the corner
   double* vertPos = nullptr;       // 3 per vertex
   unsigned long long* ebits = nullptr;  // fine edges: bit (lin*3 + {z:0,y:1,x:2})
@@ -132,6 +157,7 @@ struct SvoDevice {
   double* nodeSampleNrm = nullptr; // 3 per node: sum of unit normals
   int64_t* coincIds = nullptr;     // vertices coincident with a coarser corner, ascending
   int64_t numCoinc = 0;
+  void* rowParams = nullptr;       // device copy of the octree's RowParams (its_rows.cuh)
   LatticeIndex lattice(int d) const {
     LatticeIndex L;
     L.bits = vbits[d];

@@ -26,6 +26,7 @@ struct RowParams {
   const uint32_t* parent;
   const uint32_t* morton;
   const uint32_t* vertLin;
+  const uint64_t* vertKey;
   const uint32_t* vertOwner;
   const double* vertPos;
   double winv[kMaxDepth];  // RN(1 / w_d): the hat quotients by divRn (bit-identical, no division)
@@ -41,24 +42,23 @@ inline RowParams rowParams(const SvoDevice& d) {
   P.parent = d.nodeParent;
   P.morton = d.nodeMorton;
   P.vertLin = d.vertLin;
+  P.vertKey = d.vertKey;
   P.vertOwner = d.vertOwner;
   P.vertPos = d.vertPos;
   for (int L = 0; L < kMaxDepth; ++L) P.winv[L] = 1.0 / (P.w0 * (double)(1u << L));
   return P;
 }
 
-__device__ __forceinline__ int rowDepth(const RowParams& P, int64_t r) {
-  int d = 0;
-  while (d + 1 < P.depth && P.vertStart[d + 1] <= r) ++d;
-  return d;
-}
+// Lattice coordinates, depth and owner coordinates of vertex r (one 8-byte load). The
+// owner (the lowest-index node with that corner) has the vertex at its corner (X - Xo,
+// Y - Yo, Z - Zo); its ancestor k depths up has coordinates (Xo, Yo, Zo) >> k, because the
+// octree's levels are O_{L+1} = O_L >> 3 -- no walk along the parent links.
+__device__ __forceinline__ VertCoord vertCoord(const RowParams& P, int64_t r) { return decodeVertKey(P.vertKey[r]); }
 
 // A vertex whose lattice coordinates are all even below the root depth coincides with a
 // corner of the next coarser depth.
-__device__ __forceinline__ bool rowCoincident(const RowParams& P, int64_t r, int d) {
-  if (d + 1 >= P.depth) return false;
-  const uint32_t M = P.lat[d].M, lin = P.vertLin[r];
-  return (((lin / (M * M)) | ((lin / M) % M) | (lin % M)) & 1u) == 0u;
+__device__ __forceinline__ bool coordCoincident(const RowParams& P, const VertCoord& v) {
+  return v.d + 1 < P.depth && ((v.X | v.Y | v.Z) & 1u) == 0u;
 }
 
 // The coincident vertices of the finer depths at the point of a depth-d vertex with lattice
@@ -84,17 +84,17 @@ __device__ __forceinline__ void walkChain(const RowParams& P, int d, uint32_t X,
 }
 
 // visit(col, val) for the non-zero hats at (qx, qy, qz) of the 8 corners of the depth-dd
-// ancestor of a depth-d node with Morton coordinates (Xo, Yo, Zo), corners in x-major order.
-// The octree's levels are O_{L+1} = O_L >> 3, so that ancestor has the node's coordinates
-// shifted right by dd - d -- no walk along the parent links (a chain of dependent loads).
+// ancestor of the depth-d vertex c's owner, corners in x-major order. (Corner positions are
+// the cell's origin (+ w), as the reference forms them, so the cell must be the owner's
+// ancestor itself: a neighbouring cell sharing the corner would place it an ulp away.)
 template <class Visit>
-__device__ __forceinline__ void walkAncestor(const RowParams& P, int d, int dd, uint32_t Xo, uint32_t Yo, uint32_t Zo,
-                                             double qx, double qy, double qz, Visit&& visit) {
-  const int up = dd - d;
-  const uint32_t Xa = Xo >> up, Ya = Yo >> up, Za = Zo >> up;
+__device__ __forceinline__ void walkAncestor(const RowParams& P, const VertCoord& c, int dd, double qx, double qy,
+                                             double qz, Visit&& visit) {
+  const int up = dd - c.d;
+  const LatticeIndex& L = P.lat[dd];
+  const uint32_t Xa = c.Xo >> up, Ya = c.Yo >> up, Za = c.Zo >> up;
   const double w = P.w0 * (double)(1u << dd), wi = P.winv[dd];
   const double bx = latticePos(P.g.x, w, Xa), by = latticePos(P.g.y, w, Ya), bz = latticePos(P.g.z, w, Za);
-  const LatticeIndex& L = P.lat[dd];
   // the six axis factors once (the corners share them)
   const double hxs[2] = {hat1r(qx, bx, w, wi), hat1r(qx, bx + w, w, wi)};
   const double hys[2] = {hat1r(qy, by, w, wi), hat1r(qy, by + w, w, wi)};
@@ -119,19 +119,15 @@ __device__ __forceinline__ void walkAncestor(const RowParams& P, int d, int dd, 
   }
 }
 
-// visit(col, val) for every entry of row r (depth d) in column order: the finer coincident
-// vertices, the diagonal, then the corners of every ancestor of the owner, coarser last.
+// visit(col, val) for every entry of row r in column order: the finer coincident vertices,
+// the diagonal, then the corners of every ancestor of the owner, coarser last.
 template <class Visit>
-__device__ __forceinline__ void walkRow(const RowParams& P, int64_t r, int d, Visit&& visit) {
-  const uint32_t M = P.lat[d].M;
-  const uint32_t lin = P.vertLin[r];
-  const uint32_t X = lin / (M * M), Y = (lin / M) % M, Z = lin % M;
+__device__ __forceinline__ void walkRow(const RowParams& P, int64_t r, Visit&& visit) {
+  const VertCoord c = vertCoord(P, r);
   const double qx = P.vertPos[3 * r], qy = P.vertPos[3 * r + 1], qz = P.vertPos[3 * r + 2];
-  walkChain(P, d, X, Y, Z, [&](int32_t c) { visit(c, 1.0); });
+  walkChain(P, c.d, c.X, c.Y, c.Z, [&](int32_t k) { visit(k, 1.0); });
   visit((int32_t)r, 1.0);
-  uint32_t Xo, Yo, Zo;
-  mortonDecode(P.morton[P.vertOwner[r]], Xo, Yo, Zo);
-  for (int dd = d + 1; dd < P.depth; ++dd) walkAncestor(P, d, dd, Xo, Yo, Zo, qx, qy, qz, visit);
+  for (int dd = c.d + 1; dd < P.depth; ++dd) walkAncestor(P, c, dd, qx, qy, qz, visit);
 }
 
 }  // namespace its

@@ -35,6 +35,7 @@
 // column order, so no CSR is needed.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "its_op.cuh"
@@ -63,63 +64,97 @@ __device__ __forceinline__ int findSeg(const int64_t* __restrict__ prefix, int n
 }
 
 // G_r = b_r - the shares of the finer coincident vertices at r's point (finest first).
-__global__ void kStartValues(const RowSeg* __restrict__ segs, const int64_t* __restrict__ prefix, int nseg,
-                             int64_t total) {
+__global__ void __launch_bounds__(256) kStartValues(const RowSeg* __restrict__ segs, const int64_t* __restrict__ prefix,
+                                                    int nseg, int64_t total) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= total) return;
   const int k = findSeg(prefix, nseg, i);
   const RowSeg& s = segs[k];
   const int64_t r = s.rowBegin + (i - prefix[k]);
   const RowParams& P = *s.P;
-  const int d = rowDepth(P, r);
-  const uint32_t M = P.lat[d].M, lin = P.vertLin[r];
   double acc = 0.0;
-  if (s.shares) walkChain(P, d, lin / (M * M), (lin / M) % M, lin % M, [&](int32_t c) { acc += s.shares[c]; });
+  if (s.shares) {
+    const VertCoord v = vertCoord(P, r);
+    walkChain(P, v.d, v.X, v.Y, v.Z, [&](int32_t c) { acc += s.shares[c]; });
+  }
   s.g[r] = s.b[r] - acc;
 }
 
 // lambda_r: the share of a coincident vertex; otherwise G_r less the interpolant of G over
 // the corners of the owner's parent cell (the row's hats of that depth, in column order).
-__global__ void kStartInterp(const RowSeg* __restrict__ segs, const int64_t* __restrict__ prefix, int nseg,
-                             int64_t total) {
+__global__ void __launch_bounds__(256) kStartInterp(const RowSeg* __restrict__ segs, const int64_t* __restrict__ prefix,
+                                                    int nseg, int64_t total) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= total) return;
   const int k = findSeg(prefix, nseg, i);
   const RowSeg& s = segs[k];
   const int64_t r = s.rowBegin + (i - prefix[k]);
   const RowParams& P = *s.P;
-  const int d = rowDepth(P, r);
-  if (rowCoincident(P, r, d)) {
+  const VertCoord v = vertCoord(P, r);
+  if (coordCoincident(P, v)) {
     s.lam[r] = s.shares ? s.shares[r] : 0.0;
     return;
   }
   const double* __restrict__ g = s.g;
   double acc = 0.0;
-  if (d + 1 < P.depth) {
-    uint32_t Xo, Yo, Zo;
-    mortonDecode(P.morton[P.vertOwner[r]], Xo, Yo, Zo);
-    walkAncestor(P, d, d + 1, Xo, Yo, Zo, P.vertPos[3 * r], P.vertPos[3 * r + 1], P.vertPos[3 * r + 2],
-                 [&](int32_t c, double v) { acc += v * g[c]; });
-  }
+  if (v.d + 1 < P.depth)
+    walkAncestor(P, v, v.d + 1, P.vertPos[3 * r], P.vertPos[3 * r + 1], P.vertPos[3 * r + 2],
+                 [&](int32_t c, double h) { acc += h * g[c]; });
   s.lam[r] = g[r] - acc;
 }
 
+// ---- residual ||b - A lambda|| ---------------------------------------------------------
+// (A lambda)_v = (the finer coincident columns: their lambdas) + H_v, where H_v = lambda_v +
+// F_{>d}(v) is the field of v's own and the coarser depths at v. For the vertices above the
+// finest depth, H_v is summed as row v has it (the hats of every ancestor's corners). For the
+// finest vertices -- most of the rows, and the most ancestors each -- F_{>0} is trilinear on
+// the owner's parent cell (the argument of the exact start), so
+//   H_v = lambda_v + sum_{corners c of the parent cell} hat_c(v) H_c:
+// the same operator with 8 hats per row instead of 8 per ancestor. Two launches (the coarse
+// band, then the finest depth) over 256-row chunks; every chunk leaves its sums of e^2 and b^2
+// in a slot of its own, a mesh's slots contiguous, and kResidualFinish adds a mesh's slots in
+// a fixed order.
 constexpr int kResThreads = 256;
-constexpr int64_t kResChunk = 256;  // rows per block (one per thread): enough blocks to fill the GPU
 
-// ||b - A lambda||^2 and ||b||^2 of one chunk of rows (segments = chunks, one block each).
-__global__ void __launch_bounds__(kResThreads) kResidualChunks(const RowSeg* __restrict__ segs, double* __restrict__ part) {
-  const RowSeg& s = segs[blockIdx.x];
+struct ResSeg {
+  const RowParams* P;
+  int64_t rowBegin, rows;  // one band of one octree
+  const double* b;
+  const double* lam;
+  double* H;
+  int64_t slot;            // slot of the segment's first chunk
+};
+
+template <bool kFine>
+__global__ void __launch_bounds__(kResThreads) kResidualBand(const ResSeg* __restrict__ segs,
+                                                            const int64_t* __restrict__ chunkFirst, int nseg,
+                                                            double* __restrict__ part) {
+  const int k = findSeg(chunkFirst, nseg, blockIdx.x);
+  const ResSeg& s = segs[k];
+  const int64_t j = blockIdx.x - chunkFirst[k];
   const RowParams& P = *s.P;
+  const int64_t i = j * kResThreads + threadIdx.x;
   double rr = 0.0, bb = 0.0;
-  for (int64_t i = threadIdx.x; i < s.rows; i += kResThreads) {
+  if (i < s.rows) {
     const int64_t r = s.rowBegin + i;
+    const VertCoord v = vertCoord(P, r);
+    const double* __restrict__ lam = s.lam;
+    const double qx = P.vertPos[3 * r], qy = P.vertPos[3 * r + 1], qz = P.vertPos[3 * r + 2];
     double acc = 0.0;
-    const double* lam = s.lam;
-    walkRow(P, r, rowDepth(P, r), [&](int32_t c, double v) { acc += v * lam[c]; });
-    const double e = s.b[r] - acc;
-    rr += e * e;
-    bb += s.b[r] * s.b[r];
+    if (kFine) {  // interpolate H from the parent cell's corners
+      const double* __restrict__ H = s.H;
+      if (v.d + 1 < P.depth) walkAncestor(P, v, v.d + 1, qx, qy, qz, [&](int32_t c, double h) { acc += h * H[c]; });
+    } else {      // the row's own ancestors
+      for (int dd = v.d + 1; dd < P.depth; ++dd)
+        walkAncestor(P, v, dd, qx, qy, qz, [&](int32_t c, double h) { acc += h * lam[c]; });
+    }
+    const double h = lam[r] + acc;
+    if (!kFine) s.H[r] = h;
+    double chain = 0.0;
+    walkChain(P, v.d, v.X, v.Y, v.Z, [&](int32_t c) { chain += lam[c]; });
+    const double e = s.b[r] - (chain + h);
+    rr = e * e;
+    bb = s.b[r] * s.b[r];
   }
   __shared__ double srr[kResThreads / 32], sbb[kResThreads / 32];
   for (int o = 16; o > 0; o >>= 1) {
@@ -137,8 +172,8 @@ __global__ void __launch_bounds__(kResThreads) kResidualChunks(const RowSeg* __r
       a += srr[w];
       c += sbb[w];
     }
-    part[2 * blockIdx.x] = a;
-    part[2 * blockIdx.x + 1] = c;
+    part[2 * (s.slot + j)] = a;
+    part[2 * (s.slot + j) + 1] = c;
   }
 }
 
@@ -167,24 +202,34 @@ __global__ void __launch_bounds__(kResThreads) kResidualFinish(const double* __r
   if (threadIdx.x == 0) rel[m] = sc[0] > 0.0 ? sqrt(sa[0] / sc[0]) : sqrt(sa[0]);
 }
 
-// Row parameters of count octrees on the device.
-static its_status uploadParams(its_ctx* ctx, its_svo* const* svos, int64_t count, DevBuf<RowParams>& dP) {
-  its_status st;
-  std::vector<RowParams> h(count);
-  for (int64_t m = 0; m < count; ++m) h[m] = rowParams(svos[m]->d);
-  if ((st = dP.alloc(ctx, count)) != ITS_OK) return st;
-  // from pageable memory: the call returns once the source is staged, so h may go away
-  ITS_CU(ctx, cudaMemcpyAsync(dP.p, h.data(), count * sizeof(RowParams), cudaMemcpyHostToDevice, ctx->stream));
-  return ITS_OK;
-}
+// A segment table and its prefix in one device buffer (one copy from pageable memory, staged
+// at the call, so the host vectors may go away on return).
+template <class Seg>
+struct SegTable {
+  DevBuf<uint8_t> buf;
+  const Seg* segs = nullptr;
+  const int64_t* prefix = nullptr;
+  its_status upload(its_ctx* ctx, const std::vector<Seg>& s, const std::vector<int64_t>& pre) {
+    const size_t a = s.size() * sizeof(Seg), b = pre.size() * sizeof(int64_t);
+    std::vector<uint8_t> h(a + b);
+    std::memcpy(h.data(), s.data(), a);
+    std::memcpy(h.data() + a, pre.data(), b);
+    its_status st;
+    if ((st = buf.alloc(ctx, std::max<size_t>(a + b, 8))) != ITS_OK) return st;
+    ITS_CU(ctx, cudaMemcpyAsync(buf.p, h.data(), a + b, cudaMemcpyHostToDevice, ctx->stream));
+    segs = (const Seg*)buf.p;
+    prefix = (const int64_t*)(buf.p + a);
+    return ITS_OK;
+  }
+};
+
+static const RowParams* rowParamsOf(its_svo* s) { return (const RowParams*)s->d.rowParams; }
 
 // Exact starts of count octrees (device vectors), matrix-free: G (when there are shares),
 // then lambda, each one launch for all octrees together.
 its_status exactStart(its_ctx* ctx, its_svo* const* svos, int64_t count, const double* const* b,
                       const double* const* shares, double* const* lam) {
   its_status st;
-  DevBuf<RowParams> dP;
-  if ((st = uploadParams(ctx, svos, count, dP)) != ITS_OK) return st;
   bool anyShares = false;
   int64_t total = 0;
   for (int64_t m = 0; m < count; ++m) {
@@ -200,7 +245,7 @@ its_status exactStart(its_ctx* ctx, its_svo* const* svos, int64_t count, const d
     const int64_t n = svos[m]->d.numVerts;
     if (!n) continue;
     RowSeg s;
-    s.P = dP.p + m;
+    s.P = rowParamsOf(svos[m]);
     s.rowBegin = 0;
     s.rows = n;
     s.b = b[m];
@@ -213,61 +258,82 @@ its_status exactStart(its_ctx* ctx, its_svo* const* svos, int64_t count, const d
   }
   const int nseg = (int)segs.size();
   if (!nseg) return ITS_OK;
-  DevBuf<RowSeg> dSegs;
-  DevBuf<int64_t> dPrefix;
-  if ((st = dSegs.alloc(ctx, nseg)) != ITS_OK || (st = dPrefix.alloc(ctx, nseg)) != ITS_OK) return st;
-  ITS_CU(ctx, cudaMemcpyAsync(dSegs.p, segs.data(), nseg * sizeof(RowSeg), cudaMemcpyHostToDevice, ctx->stream));
-  ITS_CU(ctx, cudaMemcpyAsync(dPrefix.p, prefix.data(), nseg * 8, cudaMemcpyHostToDevice, ctx->stream));
+  SegTable<RowSeg> T;
+  if ((st = T.upload(ctx, segs, prefix)) != ITS_OK) return st;
   if (anyShares) {
-    kStartValues<<<gridFor(total, 256), 256, 0, ctx->stream>>>(dSegs.p, dPrefix.p, nseg, total);
+    kStartValues<<<gridFor(total, 256), 256, 0, ctx->stream>>>(T.segs, T.prefix, nseg, total);
     ITS_LAUNCHED(ctx);
   }
-  kStartInterp<<<gridFor(total, 256), 256, 0, ctx->stream>>>(dSegs.p, dPrefix.p, nseg, total);
+  kStartInterp<<<gridFor(total, 256), 256, 0, ctx->stream>>>(T.segs, T.prefix, nseg, total);
   ITS_LAUNCHED(ctx);
   return ITS_OK;  // the tables were copied from pageable memory (staged at the call)
 }
 
 // ||b - A lambda|| / ||b|| of count octrees (device vectors), matrix-free, into rel[count]
-// (host), each mesh's sum in a fixed order.
+// (host), each mesh's sum in a fixed order: the coarse band, the finest depth, the sums.
 its_status fitResidual(its_ctx* ctx, its_svo* const* svos, int64_t count, const double* const* b,
                        const double* const* lam, double* rel) {
   its_status st;
-  DevBuf<RowParams> dP;
-  if ((st = uploadParams(ctx, svos, count, dP)) != ITS_OK) return st;
-  std::vector<RowSeg> segs;
-  std::vector<int64_t> first(count + 1, 0);
-  for (int64_t m = 0; m < count; ++m) {
-    first[m] = (int64_t)segs.size();
-    const int64_t n = svos[m]->d.numVerts;
-    for (int64_t r0 = 0; r0 < n; r0 += kResChunk) {
-      RowSeg s;
-      s.P = dP.p + m;
-      s.rowBegin = r0;
-      s.rows = std::min(kResChunk, n - r0);
+  int64_t total = 0;
+  for (int64_t m = 0; m < count; ++m) total += svos[m]->d.numVerts;
+  DevBuf<double> H;
+  if ((st = H.alloc(ctx, std::max<int64_t>(total, 1))) != ITS_OK) return st;
+  // band 0: depths 1.. (rows vertStart[1]..numVerts-1); band 1: the finest depth. Mesh m owns
+  // slots [mFirst[m], mFirst[m+1]): its coarse band's chunks, then its finest depth's.
+  std::vector<ResSeg> segs[2];
+  std::vector<int64_t> cf[2];
+  int64_t chunks[2] = {0, 0};
+  std::vector<int64_t> mFirst(count + 1, 0);
+  for (int64_t m = 0, h = 0; m < count; ++m) {
+    const SvoDevice& d = svos[m]->d;
+    int64_t slot = mFirst[m];
+    for (int band = 0; band < 2; ++band) {
+      ResSeg s;
+      s.P = rowParamsOf(svos[m]);
+      const int64_t fine = d.vertStart[1 < d.depth ? 1 : d.depth];  // rows of the finest depth
+      s.rowBegin = band == 0 ? fine : 0;
+      s.rows = band == 0 ? d.numVerts - fine : fine;
       s.b = b[m];
-      s.shares = nullptr;
-      s.g = nullptr;
-      s.lam = const_cast<double*>(lam[m]);
-      segs.push_back(s);
+      s.lam = lam[m];
+      s.H = H.p + h;
+      s.slot = slot;
+      const int64_t c = (s.rows + kResThreads - 1) / kResThreads;
+      if (!c) continue;
+      segs[band].push_back(s);
+      cf[band].push_back(chunks[band]);
+      chunks[band] += c;
+      slot += c;
     }
+    mFirst[m + 1] = slot;
+    h += d.numVerts;
   }
-  first[count] = (int64_t)segs.size();
-  const int64_t nseg = (int64_t)segs.size();
-  DevBuf<RowSeg> dSegs;
-  DevBuf<int64_t> dFirst;
+  // one upload: both bands' segments, then their chunk prefixes and the mesh slot starts
+  std::vector<ResSeg> allSegs(segs[0]);
+  allSegs.insert(allSegs.end(), segs[1].begin(), segs[1].end());
+  std::vector<int64_t> tail(cf[0]);
+  tail.push_back(chunks[0]);
+  const size_t cf1 = tail.size();
+  tail.insert(tail.end(), cf[1].begin(), cf[1].end());
+  tail.push_back(chunks[1]);
+  const size_t mfOff = tail.size();
+  tail.insert(tail.end(), mFirst.begin(), mFirst.end());
+  const int64_t slots = mFirst[count];
+  SegTable<ResSeg> T;
   DevBuf<double> part, dRel;
-  if ((st = dSegs.alloc(ctx, std::max<int64_t>(nseg, 1))) != ITS_OK || (st = dFirst.alloc(ctx, count + 1)) != ITS_OK ||
-      (st = part.alloc(ctx, 2 * std::max<int64_t>(nseg, 1))) != ITS_OK || (st = dRel.alloc(ctx, count)) != ITS_OK)
+  if ((st = T.upload(ctx, allSegs, tail)) != ITS_OK || (st = part.alloc(ctx, 2 * std::max<int64_t>(slots, 1))) != ITS_OK ||
+      (st = dRel.alloc(ctx, count)) != ITS_OK)
     return st;
-  ITS_CU(ctx, cudaMemcpyAsync(dSegs.p, segs.data(), nseg * sizeof(RowSeg), cudaMemcpyHostToDevice, ctx->stream));
-  ITS_CU(ctx, cudaMemcpyAsync(dFirst.p, first.data(), (count + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
-  if (nseg) {
-    kResidualChunks<<<(unsigned)nseg, kResThreads, 0, ctx->stream>>>(dSegs.p, part.p);
+  const int n0 = (int)segs[0].size(), n1 = (int)segs[1].size();
+  if (chunks[0]) {
+    kResidualBand<false><<<(unsigned)chunks[0], kResThreads, 0, ctx->stream>>>(T.segs, T.prefix, n0, part.p);
     ITS_LAUNCHED(ctx);
-  } else {
-    ITS_CU(ctx, cudaMemsetAsync(part.p, 0, 16, ctx->stream));
   }
-  kResidualFinish<<<(unsigned)count, kResThreads, 0, ctx->stream>>>(part.p, dFirst.p, dRel.p);
+  if (chunks[1]) {
+    kResidualBand<true><<<(unsigned)chunks[1], kResThreads, 0, ctx->stream>>>(T.segs + n0, T.prefix + cf1, n1, part.p);
+    ITS_LAUNCHED(ctx);
+  }
+  if (!slots) ITS_CU(ctx, cudaMemsetAsync(part.p, 0, 16, ctx->stream));
+  kResidualFinish<<<(unsigned)count, kResThreads, 0, ctx->stream>>>(part.p, T.prefix + mfOff, dRel.p);
   ITS_LAUNCHED(ctx);
   ITS_CU(ctx, cudaMemcpyAsync(rel, dRel.p, count * 8, cudaMemcpyDeviceToHost, ctx->stream));
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "its_scan.cuh"
+#include "its_rows.cuh"
 #include "its_svo.cuh"
 
 namespace its {
@@ -197,9 +198,11 @@ __global__ void kOwnerCorners(int64_t count, int64_t start, const uint32_t* __re
 }
 // Representative position of a corner: taken from its owner node, corner = origin (+ w),
 // origin = g + w*X (the surviving entry of the reference's stable sort + unique).
-__global__ void kVertexPositions(int64_t count, int64_t vstart, uint32_t M, double3 g, double w,
+// Also the vertex's packed key (lattice coordinates, depth, corner of the owner).
+__global__ void kVertexPositions(int64_t count, int64_t vstart, uint32_t M, int depth, double3 g, double w,
                                  const uint32_t* __restrict__ lin, const uint32_t* __restrict__ owner,
-                                 const uint32_t* __restrict__ morton, double* __restrict__ pos) {
+                                 const uint32_t* __restrict__ morton, double* __restrict__ pos,
+                                 uint64_t* __restrict__ key) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= count) return;
   const int64_t v = vstart + i;
@@ -207,6 +210,7 @@ __global__ void kVertexPositions(int64_t count, int64_t vstart, uint32_t M, doub
   const uint32_t X = l / (M * M), Y = (l / M) % M, Z = l % M;
   uint32_t Xo, Yo, Zo;
   mortonDecode(morton[owner[v]], Xo, Yo, Zo);
+  key[v] = encodeVertKey(X, Y, Z, depth, Xo, Yo, Zo);
   const double bx = latticePos(g.x, w, Xo), by = latticePos(g.y, w, Yo), bz = latticePos(g.z, w, Zo);
   pos[3 * v] = (X != Xo) ? bx + w : bx;
   pos[3 * v + 1] = (Y != Yo) ? by + w : by;
@@ -307,9 +311,9 @@ static void svoRelease(its_svo* s) {
   if (!s) return;
   its_ctx* c = s->ctx;
   SvoDevice& d = s->d;
-  void* ptrs[] = {d.voxels, d.nodeMorton, d.nodeParent, d.nodeChild0, d.nodeLeaf, d.nodeNb, d.vertLin,
+  void* ptrs[] = {d.voxels, d.nodeMorton, d.nodeParent, d.nodeChild0, d.nodeLeaf, d.nodeNb, d.vertLin, d.vertKey,
                   d.vertOwner, d.vertPos, d.ebits, d.erank, d.edgeKey, d.edgeOwner, d.fineOcc,
-                  d.nodeSampleCnt, d.nodeSamplePos, d.nodeSampleNrm, d.coincIds};
+                  d.nodeSampleCnt, d.nodeSamplePos, d.nodeSampleNrm, d.coincIds, d.rowParams};
   for (void* p : ptrs) devFree(c, p);
   for (int i = 0; i < kMaxDepth; ++i) { devFree(c, d.vbits[i]); devFree(c, d.vrank[i]); }
   d = SvoDevice();
@@ -464,6 +468,7 @@ its_status svoBuild(its_ctx* ctx, const double* dV, int64_t nv, const int32_t* d
   if ((st = devAlloc(ctx, (void**)&d.vertLin, d.numVerts * 4)) != ITS_OK) return st;
   if ((st = devAlloc(ctx, (void**)&d.vertOwner, d.numVerts * 4)) != ITS_OK) return st;
   if ((st = devAlloc(ctx, (void**)&d.vertPos, d.numVerts * 24)) != ITS_OK) return st;
+  if ((st = devAlloc(ctx, (void**)&d.vertKey, d.numVerts * 8)) != ITS_OK) return st;
   ITS_CU(ctx, cudaMemsetAsync(d.vertOwner, 0xFF, d.numVerts * 4, ctx->stream));
   for (int L = 0; L < d.depth; ++L) {
     const uint32_t M = (uint32_t)(res >> L) + 1u;
@@ -474,9 +479,9 @@ its_status svoBuild(its_ctx* ctx, const double* dV, int64_t nv, const int32_t* d
                                                                                d.nodeMorton, d.lattice(L), d.vertOwner);
     ITS_LAUNCHED(ctx);
     const double w = d.unit[0] * (double)(1u << L);
-    kVertexPositions<<<gridFor(d.vertCount[L], 256), 256, 0, ctx->stream>>>(d.vertCount[L], d.vertStart[L], M, g, w,
-                                                                             d.vertLin, d.vertOwner, d.nodeMorton,
-                                                                             d.vertPos);
+    kVertexPositions<<<gridFor(d.vertCount[L], 256), 256, 0, ctx->stream>>>(d.vertCount[L], d.vertStart[L], M, L, g,
+                                                                             w, d.vertLin, d.vertOwner, d.nodeMorton,
+                                                                             d.vertPos, d.vertKey);
     ITS_LAUNCHED(ctx);
   }
 
@@ -514,6 +519,10 @@ its_status svoBuild(its_ctx* ctx, const double* dV, int64_t nv, const int32_t* d
   // the coincident vertices (the shares of the exact start)
   if ((st = devAlloc(ctx, (void**)&d.coincIds, std::max<int64_t>(d.numVerts, 1) * 8)) != ITS_OK) return st;
   if ((st = coincidentIds(ctx, d, d.coincIds, &d.numCoinc)) != ITS_OK) return st;
+  // the row parameters of the matrix-free kernels, on the device for the octree's lifetime
+  const RowParams hp = rowParams(d);
+  if ((st = devAlloc(ctx, &d.rowParams, sizeof(RowParams))) != ITS_OK) return st;
+  ITS_CU(ctx, cudaMemcpyAsync(d.rowParams, &hp, sizeof(RowParams), cudaMemcpyHostToDevice, ctx->stream));
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   return ITS_OK;
 }
