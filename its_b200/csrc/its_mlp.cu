@@ -30,11 +30,28 @@ constexpr int kSplitK = 128;  // weight-gradient partial sums per layer
 
 using bf16 = __nv_bfloat16;
 
-__device__ __forceinline__ float geluF(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+// GELU in its tanh form (Hendrycks & Gimpel, "Gaussian Error Linear Units", 2016):
+//   gelu(z) = z/2 (1 + tanh(u)),  u = sqrt(2/pi) (z + 0.044715 z^3),
+// with the tanh from the hardware's approximate unit: a handful of instructions where the
+// erf form costs a few dozen, in the epilogues that bound the network's kernels.
+constexpr float kGeluK0 = 0.7978845608028654f;  // sqrt(2 / pi)
+constexpr float kGeluK1 = 0.044715f;
+__device__ __forceinline__ float tanhApprox(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float geluF(float z) {
+  const float u = z * fmaf(kGeluK0 * kGeluK1, z * z, kGeluK0);
+  const float h = 0.5f * z;
+  return fmaf(h, tanhApprox(u), h);
+}
+// d gelu / dz = (1 + t)/2 + z/2 (1 - t^2) sqrt(2/pi) (1 + 3 * 0.044715 z^2), t = tanh(u)
 __device__ __forceinline__ float geluGrad(float z) {
-  const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
-  const float pdf = 0.39894228040143268f * expf(-0.5f * z * z);
-  return cdf + z * pdf;
+  const float z2 = z * z;
+  const float t = tanhApprox(z * fmaf(kGeluK0 * kGeluK1, z2, kGeluK0));
+  const float du = fmaf(3.0f * kGeluK0 * kGeluK1, z2, kGeluK0);
+  return fmaf(0.5f * z * du, fmaf(-t, t, 1.0f), 0.5f * (1.0f + t));
 }
 
 // ---- one tcgen05 GEMM: C[m][n] = sum_k A[m][k] B[n][k] over this CTA's K range -------------
@@ -212,8 +229,9 @@ struct EpiPartial {
 // straight back into shared memory as the next layer's A operand -- nothing but the features
 // and the outputs touches global memory. The MMA sequence and the epilogue arithmetic are
 // those of the layer-by-layer kernels, so the outputs are identical.
-constexpr int kFusedGroups = 2;  // two 128-row tiles in flight per CTA (one per warp group)
-constexpr int kFusedSmem = 16384 /*W1*/ + 32768 /*W2*/ + 32768 /*W3*/ + kFusedGroups * (16384 /*X*/ + 32768 /*H*/) +
+constexpr int kFusedSlots = 2;                   // 128-row tiles in flight per CTA
+constexpr int kFusedThreads = 256 * kFusedSlots;  // two warp groups per tile, one per half of the columns
+constexpr int kFusedSmem = 16384 /*W1*/ + 32768 /*W2*/ + 32768 /*W3*/ + kFusedSlots * (16384 /*X*/ + 32768 /*H*/) +
                            64 + 1024;
 
 __device__ __forceinline__ void loadWeightTile(uint8_t* dst, const bf16* __restrict__ W, int K, int tid, int nthreads) {
@@ -224,10 +242,16 @@ __device__ __forceinline__ void loadWeightTile(uint8_t* dst, const bf16* __restr
   }
 }
 
-// Barrier of one warp group (128 threads), ids 1 and 2 (0 is __syncthreads').
-__device__ __forceinline__ void groupSync(int g) { asm volatile("bar.sync %0, 128;" ::"r"(1 + g) : "memory"); }
+// Barrier of one tile slot (256 threads), ids 1 and 2 (0 is __syncthreads').
+__device__ __forceinline__ void slotSync(int s) { asm volatile("bar.sync %0, 256;" ::"r"(1 + s) : "memory"); }
 
-__global__ void __launch_bounds__(128 * kFusedGroups, 1)
+// Share-network inference: persistent, one CTA per SM, two 128-row tiles in flight. A tile's
+// 256 threads load its features, one of them issues each layer's MMAs, and the two warp groups
+// run the epilogue of one half of the 128 columns each (thread = row, the TMEM lane of its
+// warp). The output unit sums the columns in order: the second half's activations (BF16, as
+// the sum uses them) go through shared memory to the first half's threads, so the result is
+// the layer-by-layer kernels' bit for bit.
+__global__ void __launch_bounds__(kFusedThreads, 1)
     kMlpForwardFused(const float* __restrict__ X, int64_t n, const bf16* __restrict__ W1, const bf16* __restrict__ W2,
                      const bf16* __restrict__ W3, const float* __restrict__ P, const float* __restrict__ w4r,
                      float* __restrict__ out, int* __restrict__ err) {
@@ -237,24 +261,25 @@ __global__ void __launch_bounds__(128 * kFusedGroups, 1)
   uint8_t* sW1 = smem;
   uint8_t* sW2 = sW1 + 16384;
   uint8_t* sW3 = sW2 + 32768;
-  const int tid = threadIdx.x, g = tid >> 7, row = tid & 127, warp = tid >> 5;
-  uint8_t* sX = sW3 + 32768 + g * (16384 + 32768);
+  const int tid = threadIdx.x, s = tid >> 8, st = tid & 255, half = st >> 7, row = tid & 127, warp = tid >> 5;
+  uint8_t* sX = sW3 + 32768 + s * (16384 + 32768);
   uint8_t* sH = sX + 16384;
-  uint64_t* mbar = (uint64_t*)(sW3 + 32768 + kFusedGroups * (16384 + 32768));
-  uint32_t* slot = (uint32_t*)(mbar + kFusedGroups);
-  if (warp == 0) tmemAlloc(smemAddr(slot), 128 * kFusedGroups);
+  constexpr int kOutStride = 144;  // bytes per row of the second half's output activations in sH
+  uint64_t* mbar = (uint64_t*)(sW3 + 32768 + kFusedSlots * (16384 + 32768));
+  uint32_t* tslot = (uint32_t*)(mbar + kFusedSlots);
+  if (warp == 0) tmemAlloc(smemAddr(tslot), 128 * kFusedSlots);
   if (tid == 0)
-    for (int k = 0; k < kFusedGroups; ++k) mbarInit(smemAddr(mbar + k), 1);
+    for (int k = 0; k < kFusedSlots; ++k) mbarInit(smemAddr(mbar + k), 1);
   loadWeightTile(sW1, W1, kIn, tid, blockDim.x);
   loadWeightTile(sW2, W2, kHid, tid, blockDim.x);
   loadWeightTile(sW3, W3, kHid, tid, blockDim.x);
   fenceBefore();
   __syncthreads();
   fenceAfter();
-  const uint32_t tmem = *slot + 128u * g;                 // this group's 128 columns
+  const uint32_t tmem = *tslot + 128u * s;                 // this tile slot's 128 columns
   const uint32_t lane = (uint32_t)((warp & 3) * 32) << 16;  // the warp's TMEM lanes
   constexpr uint32_t idesc = idescBf16(128, kHid);
-  const uint32_t bar = smemAddr(mbar + g);
+  const uint32_t bar = smemAddr(mbar + s);
   uint32_t phase = 0;
   bool ok = true;
   const float* b1 = P + kOffB1;
@@ -262,12 +287,12 @@ __global__ void __launch_bounds__(128 * kFusedGroups, 1)
   const float* b3 = P + kOffB3;
   const int64_t tiles = (n + 127) / 128;
   const bool xVec = ((uintptr_t)X & 15) == 0;  // rows are 256 B apart: 16-byte loads when the base allows
-  for (int64_t t = (int64_t)blockIdx.x * kFusedGroups + g; t < tiles; t += (int64_t)gridDim.x * kFusedGroups) {
+  for (int64_t t = (int64_t)blockIdx.x * kFusedSlots + s; t < tiles; t += (int64_t)gridDim.x * kFusedSlots) {
     const int64_t m = t * 128 + row;
     // features -> BF16: the tile's 128 rows x 256 B read in coalesced 32-byte pieces, each one
     // 16-byte chunk of a row in the swizzled A tile
 #pragma unroll 2
-    for (int p = row; p < 128 * 8; p += 128) {
+    for (int p = st; p < 128 * 8; p += 256) {
       const int pr = p >> 3, pc = p & 7;
       const int64_t mr = t * 128 + pr;
       float4 f0 = make_float4(0.f, 0.f, 0.f, 0.f), f1 = f0;
@@ -290,8 +315,8 @@ __global__ void __launch_bounds__(128 * kFusedGroups, 1)
     for (int layer = 0; layer < 3; ++layer) {
       fenceProxyAsync();
       fenceBefore();
-      groupSync(g);
-      if (row == 0) {
+      slotSync(s);
+      if (st == 0) {
         fenceAfter();
         if (layer == 0) {
           const uint64_t da = descSw128(smemAddr(sX)), db = descSw128(smemAddr(sW1));
@@ -311,10 +336,10 @@ __global__ void __launch_bounds__(128 * kFusedGroups, 1)
       ok = mbarWait(bar, phase) && ok;
       phase ^= 1u;
       fenceAfter();
-      // epilogue, 16 accumulator columns at a time (a rolled loop keeps the code small)
+      // epilogue of this half's 64 columns, 16 at a time (a rolled loop keeps the code small)
       const float* bias = layer == 0 ? b1 : (layer == 1 ? b2 : b3);
 #pragma unroll 1
-      for (int n0 = 0; n0 < kHid; n0 += 16) {
+      for (int n0 = 64 * half; n0 < 64 * half + 64; n0 += 16) {
         float v[16];
         tmemLoad16(tmem + lane + (uint32_t)n0, v);
         if (layer < 2) {  // hidden layer: the next layer's A operand
@@ -326,21 +351,34 @@ __global__ void __launch_bounds__(128 * kFusedGroups, 1)
             const int c = (n0 >> 3) + h;
             *(uint4*)(sH + (c >> 3) * 16384 + swizzledChunk(row, c & 7)) = *(const uint4*)q;
           }
-        } else {  // output unit, columns in order
+        } else if (half == 0) {  // output unit, columns in order
 #pragma unroll
           for (int j = 0; j < 16; ++j)
             o += __bfloat162float(__float2bfloat16_rn(geluF(v[j] + bias[n0 + j]))) * w4r[n0 + j];
+        } else {  // the second half's activations for the first half's sum (layer 2 has read sH)
+          __align__(16) bf16 q[16];
+#pragma unroll
+          for (int j = 0; j < 16; ++j) q[j] = __float2bfloat16_rn(geluF(v[j] + bias[n0 + j]));
+          uint4* dst = (uint4*)(sH + row * kOutStride + (n0 - 64) * 2);
+          dst[0] = ((const uint4*)q)[0];
+          dst[1] = ((const uint4*)q)[1];
         }
       }
     }
-    if (m < n && ok) out[m] = o + P[kOffB4];
+    slotSync(s);
+    if (half == 0) {
+      const bf16* a = (const bf16*)(sH + row * kOutStride);
+#pragma unroll 8
+      for (int j = 0; j < 64; ++j) o += __bfloat162float(a[j]) * w4r[64 + j];
+      if (m < n && ok) out[m] = o + P[kOffB4];
+    }
     fenceBefore();
-    groupSync(g);  // every lane has read TMEM before the next tile's first MMA
+    slotSync(s);  // TMEM read and sH free before the next tile
   }
   fenceBefore();
   __syncthreads();
-  if (warp == 0) tmemFree(*slot, 128 * kFusedGroups);
-  if (!ok && tid == 0) atomicExch(err, 1);
+  if (warp == 0) tmemFree(*tslot, 128 * kFusedSlots);
+  if (!ok) atomicExch(err, 1);
 }
 
 // ---- small kernels ----------------------------------------------------------------------
@@ -602,10 +640,10 @@ its_status mlpInfer(its_mlp* h, const float* X, int64_t n, float* out) {
     ITS_CU(ctx, cudaFuncSetAttribute(kMlpForwardFused, cudaFuncAttributeMaxDynamicSharedMemorySize, kFusedSmem));
     configured = true;
   }
-  const int64_t tiles = (n + 127) / 128, ctas = (tiles + kFusedGroups - 1) / kFusedGroups;
+  const int64_t tiles = (n + 127) / 128, ctas = (tiles + kFusedSlots - 1) / kFusedSlots;
   const unsigned grid = (unsigned)(ctas < ctx->numSMs ? ctas : ctx->numSMs);
-  kMlpForwardFused<<<grid, 128 * kFusedGroups, kFusedSmem, ctx->stream>>>(X, n, h->W1, h->W2, h->W3, h->P, h->w4r, out,
-                                                                           h->err);
+  kMlpForwardFused<<<grid, kFusedThreads, kFusedSmem, ctx->stream>>>(X, n, h->W1, h->W2, h->W3, h->P, h->w4r, out,
+                                                                      h->err);
   ITS_LAUNCHED(ctx);
   return ITS_OK;
 }

@@ -9,7 +9,6 @@ backward products) and accumulate in float64; with ``bf16=False`` everything is 
 which is what the finite-difference check in the CPU tests differentiates.
 """
 import numpy as np
-from scipy.special import erf
 
 N_IN, N_HID = 64, 128
 SHAPES = [("W1", (N_HID, N_IN)), ("b1", (N_HID,)), ("W2", (N_HID, N_HID)), ("b2", (N_HID,)),
@@ -38,12 +37,17 @@ def bf16(x):
     return u.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
+K0, K1 = np.sqrt(2.0 / np.pi), 0.044715
+
+
 def gelu(z):
-    return 0.5 * z * (1.0 + erf(z / np.sqrt(2.0)))
+    """GELU, tanh form (Hendrycks & Gimpel 2016): z/2 (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3)))."""
+    return 0.5 * z * (1.0 + np.tanh(K0 * (z + K1 * z ** 3)))
 
 
 def gelu_grad(z):
-    return 0.5 * (1.0 + erf(z / np.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / np.sqrt(2.0 * np.pi)
+    t = np.tanh(K0 * (z + K1 * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * K0 * (1.0 + 3.0 * K1 * z * z)
 
 
 def init_params(seed=0):
