@@ -189,9 +189,10 @@ its_status its_lscg_solve_batch(its_op* const* ops, int64_t count, const double*
    identical rows, so A lambda = b is consistent and its exact solutions differ only in how
    each point's value is split among its coincident vertices. This pass fixes the split
    (vertices whose lattice coordinates are all even below the root depth take shares[v],
-   or 0 when shares is NULL) and solves every other row, coarse depths first, as
-   lambda_v = b_v - sum_{u != v} A(v,u) lambda_u: one matrix-free pass over the rows of A
-   (generated from the octree), one launch per depth. The result is an exact solution;
+   or 0 when shares is NULL) and gives every other row its surplus in explicit form,
+   lambda_v = G_v - sum_c A(v,c) G_c over the corners c of the owner's parent cell, with
+   G = b less the shares of the finer coincident vertices at each point: one matrix-free
+   pass over the rows (generated from the octree), one or two launches. The result is an exact solution;
    its_lscg_solve with it as x0 stops at its residual test. No counterpart in the reference
    (which starts Eigen's CGLS from zero, src/ThinShells.cpp:615-617). Vectors may be host or
    device memory. */
@@ -318,6 +319,17 @@ its_status its_learned_start(its_svo* svo, its_mlp* mlp, const double* b, const 
 /* The same for count octrees of one context (one network pass over all of them). */
 its_status its_learned_start_batch(its_svo* const* svos, int64_t count, its_mlp* mlp, const double* const* b,
                                    const float* norm, double* const* lambda);
+/* The learned fit of one octree, in place of ThinShells::creatShell's LSCG from zero
+   (src/ThinShells.cpp:608-653): its_learned_start, then ||b - A lambda|| / ||b|| (as
+   its_fit_residual), then, when that exceeds tol, its_lscg_solve (FP64, ITS_STOP_RESIDUAL)
+   from the learned start. The start and the check run as a CUDA graph captured on the first
+   call and replayed while the network, norm, the context's stream and the device addresses of
+   b and lambda stay the same (host vectors go through buffers of the octree's own, so their
+   addresses always match); the graph reads b and the network's parameters afresh every time.
+   Complete on return. report (may be NULL): iterations = LSCG iterations after the start (0
+   when the start passed), converged, rel_residual, ms = device time of the call. */
+its_status its_learned_fit(its_svo* svo, its_mlp* mlp, const double* b, const float* norm, double tol,
+                           double* lambda, its_solve_report* report);
 
 #ifdef __cplusplus
 }

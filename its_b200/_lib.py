@@ -80,6 +80,7 @@ SIGNATURES = {
     "its_share_features": (st, [vp, vp, vp, vp, i64, vp, C.POINTER(i64)]),
     "its_learned_start": (st, [vp, vp, vp, vp, vp]),
     "its_learned_start_batch": (st, [vp, i64, vp, vp, vp, vp]),
+    "its_learned_fit": (st, [vp, vp, vp, vp, dbl, vp, C.POINTER(SolveReport)]),
     "its_eval_points": (st, [vp, vp, vp, i64, vp, vp]),
     "its_shell_iso_values": (st, [vp, vp, vp, i64, C.POINTER(dbl), C.POINTER(dbl), C.POINTER(i64)]),
     "its_eval_grid": (st, [vp, vp, vp, vp, i32, vp]),

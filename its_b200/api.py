@@ -466,6 +466,20 @@ def learned_start_batch(svos, net, bs, norm, outs=None):
     return outs
 
 
+def learned_fit(svo, net, b, norm, tol, out=None):
+    """The learned fit of one octree (its_learned_fit): learned start, FP64 residual check,
+    plain LSCG from the start when the residual misses tol. Returns (lambda, report dict)."""
+    b = _f64(b)
+    norm = np.ascontiguousarray(norm, np.float32)
+    if out is None:
+        out = np.zeros(svo.num_verts)
+    rep = SolveReport()
+    svo.ctx.check(lib().its_learned_fit(svo.h, net.h, _addr(b), _ptr(norm), tol, _addr(out), C.byref(rep)),
+                  "its_learned_fit")
+    return out, dict(iterations=rep.iterations, converged=bool(rep.converged), rel_residual=rep.rel_residual,
+                     ms=rep.ms)
+
+
 def _f32(a):
     if isinstance(a, np.ndarray) or not hasattr(a, "data_ptr"):
         return np.ascontiguousarray(a, dtype=np.float32)

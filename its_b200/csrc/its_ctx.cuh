@@ -21,6 +21,10 @@ struct its_ctx {
   int autotune = 0;                  // 0: built-in defaults, 1: measure candidates on first use
   std::map<std::string, int> tuned;  // shape key -> chosen candidate
   std::string tuneCache;             // file the choices persist to ("" = none)
+  // while a CUDA graph is captured, device buffers come from this bump arena (owned by the
+  // graph's plan) instead of the pool, so the graph holds no allocation nodes
+  uint8_t* arena = nullptr;
+  size_t arenaCap = 0, arenaOff = 0;
 };
 
 namespace its {
@@ -36,6 +40,13 @@ namespace its {
 inline its_status devAlloc(its_ctx* ctx, void** p, size_t bytes) {
   *p = nullptr;
   if (bytes == 0) return ITS_OK;
+  if (ctx->arena) {
+    const size_t off = (ctx->arenaOff + 255) & ~(size_t)255;
+    if (off + bytes > ctx->arenaCap) return setError(ctx, ITS_ERR_OOM, "capture arena exhausted");
+    *p = ctx->arena + off;
+    ctx->arenaOff = off + bytes;
+    return ITS_OK;
+  }
   cudaError_t e = ctx->pool ? cudaMallocFromPoolAsync(p, bytes, ctx->pool, ctx->stream)
                             : cudaMallocAsync(p, bytes, ctx->stream);
   if (e != cudaSuccess) {
@@ -48,6 +59,7 @@ inline its_status devAlloc(its_ctx* ctx, void** p, size_t bytes) {
   return ITS_OK;
 }
 inline void devFree(its_ctx* ctx, void* p) {
+  if (ctx->arena && (uint8_t*)p >= ctx->arena && (uint8_t*)p < ctx->arena + ctx->arenaCap) return;
   if (p) cudaFreeAsync(p, ctx->stream);
 }
 

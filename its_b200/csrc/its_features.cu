@@ -432,6 +432,64 @@ its_status mlpInfer(its_mlp* mlp, const float* X, int64_t n, float* out);
 its_status mlpCheck(its_mlp* mlp);
 }  // namespace its
 
+namespace its {
+
+// The 130 normalisation values in host memory (norm may be host or device memory).
+its_status hostNorm(its_ctx* ctx, const float* norm, float* hn) {
+  if (isDevicePtr(norm)) {
+    ITS_CU(ctx, cudaMemcpyAsync(hn, norm, (2 * kFeat + 2) * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  } else {
+    std::memcpy(hn, norm, (2 * kFeat + 2) * sizeof(float));
+  }
+  return ITS_OK;
+}
+
+// Learned starts of count octrees, device vectors, everything queued on the context's stream
+// without a host wait or a copy from host memory (norm hn is passed with the launches): the
+// zero-share starts (feature inputs), the features of every mesh into one array, one network
+// pass, the shares, the exact starts with them.
+its_status learnedStart(its_ctx* ctx, its_svo* const* svos, int64_t count, its_mlp* mlp, const double* const* b,
+                        const float* hn, double* const* lam) {
+  its_status st;
+  std::vector<DevBuf<double>> lam0(count), shares(count);
+  std::vector<const double*> sp(count);
+  std::vector<double*> l0(count);
+  std::vector<int64_t> cnt(count);
+  int64_t total = 0;
+  for (int64_t m = 0; m < count; ++m) {
+    const int64_t n = svos[m]->d.numVerts;
+    if ((st = lam0[m].alloc(ctx, n)) != ITS_OK || (st = shares[m].alloc(ctx, n)) != ITS_OK) return st;
+    l0[m] = lam0[m].p;
+    sp[m] = shares[m].p;
+    cnt[m] = svos[m]->d.numCoinc;
+    total += cnt[m];
+  }
+  if ((st = exactStart(ctx, svos, count, b, nullptr, l0.data())) != ITS_OK) return st;
+  DevBuf<float> feat, pred;
+  if ((st = feat.alloc(ctx, std::max<int64_t>(total, 1) * kFeat)) != ITS_OK ||
+      (st = pred.alloc(ctx, std::max<int64_t>(total, 1))) != ITS_OK)
+    return st;
+  int64_t off = 0;
+  for (int64_t m = 0; m < count; ++m) {
+    if ((st = shareFeatures(ctx, svos[m]->d, b[m], l0[m], svos[m]->d.coincIds, cnt[m], hn, feat.p + off * kFeat)) !=
+        ITS_OK)
+      return st;
+    off += cnt[m];
+  }
+  if (total > 0 && (st = mlpInfer(mlp, feat.p, total, pred.p)) != ITS_OK) return st;
+  off = 0;
+  for (int64_t m = 0; m < count; ++m) {
+    if ((st = scatterShares(ctx, svos[m]->d.coincIds, cnt[m], pred.p + off, hn[2 * kFeat + 1], hn[2 * kFeat],
+                            shares[m].p)) != ITS_OK)
+      return st;
+    off += cnt[m];
+  }
+  return exactStart(ctx, svos, count, b, sp.data(), lam);
+}
+
+}  // namespace its
+
 extern "C" {
 
 its_status its_share_features(its_svo* svo, const double* b, const float* norm, float* features, int64_t capacity,
@@ -480,55 +538,19 @@ its_status its_learned_start_batch(its_svo* const* svos, int64_t count, its_mlp*
       return setError(ctx, ITS_ERR_INVALID, "its_learned_start: bad octree or vector");
   ITS_CU(ctx, cudaSetDevice(ctx->device));
   its_status st;
-  // host norm: input mean[64], input scale[64], output mean, output scale
   float hn[2 * kFeat + 2];
-  if (isDevicePtr(norm)) {
-    ITS_CU(ctx, cudaMemcpyAsync(hn, norm, sizeof(hn), cudaMemcpyDeviceToHost, ctx->stream));
-    ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
-  } else {
-    std::memcpy(hn, norm, sizeof(hn));
-  }
+  if ((st = hostNorm(ctx, norm, hn)) != ITS_OK) return st;
   std::vector<InArg<double>> B(count);
   std::vector<OutArg<double>> L(count);
-  std::vector<DevBuf<double>> lam0(count), shares(count);
-  std::vector<const double*> bp(count), sp(count);
-  std::vector<double*> l0(count), lp(count);
-  std::vector<int64_t> cnt(count);
-  int64_t total = 0;
+  std::vector<const double*> bp(count);
+  std::vector<double*> lp(count);
   for (int64_t m = 0; m < count; ++m) {
     const int64_t n = svos[m]->d.numVerts;
-    if ((st = B[m].stage(ctx, b[m], n)) != ITS_OK || (st = L[m].stage(ctx, lambda[m], n)) != ITS_OK ||
-        (st = lam0[m].alloc(ctx, n)) != ITS_OK || (st = shares[m].alloc(ctx, n)) != ITS_OK)
-      return st;
+    if ((st = B[m].stage(ctx, b[m], n)) != ITS_OK || (st = L[m].stage(ctx, lambda[m], n)) != ITS_OK) return st;
     bp[m] = B[m].d;
-    l0[m] = lam0[m].p;
     lp[m] = L[m].d;
-    sp[m] = shares[m].p;
-    cnt[m] = svos[m]->d.numCoinc;
-    total += cnt[m];
   }
-  // zero-share starts (features), features of every mesh into one array, one network pass
-  if ((st = exactStart(ctx, svos, count, bp.data(), nullptr, l0.data())) != ITS_OK) return st;
-  DevBuf<float> feat, pred;
-  if ((st = feat.alloc(ctx, std::max<int64_t>(total, 1) * kFeat)) != ITS_OK ||
-      (st = pred.alloc(ctx, std::max<int64_t>(total, 1))) != ITS_OK)
-    return st;
-  int64_t off = 0;
-  for (int64_t m = 0; m < count; ++m) {
-    if ((st = shareFeatures(ctx, svos[m]->d, bp[m], l0[m], svos[m]->d.coincIds, cnt[m], hn,
-                            feat.p + off * kFeat)) != ITS_OK)
-      return st;
-    off += cnt[m];
-  }
-  if (total > 0 && (st = mlpInfer(mlp, feat.p, total, pred.p)) != ITS_OK) return st;
-  off = 0;
-  for (int64_t m = 0; m < count; ++m) {
-    if ((st = scatterShares(ctx, svos[m]->d.coincIds, cnt[m], pred.p + off, hn[2 * kFeat + 1], hn[2 * kFeat],
-                            shares[m].p)) != ITS_OK)
-      return st;
-    off += cnt[m];
-  }
-  if ((st = exactStart(ctx, svos, count, bp.data(), sp.data(), lp.data())) != ITS_OK) return st;
+  if ((st = learnedStart(ctx, svos, count, mlp, bp.data(), hn, lp.data())) != ITS_OK) return st;
   bool host = false;
   for (int64_t m = 0; m < count; ++m) {
     host = host || L[m].host;

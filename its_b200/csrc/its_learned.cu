@@ -1,0 +1,218 @@
+// The learned fit as one call: learned start, FP64 residual check, plain LSCG fallback.
+//
+// ThinShells::creatShell (ThinShells.cpp:608-653) assembles the operator and runs Eigen's
+// LSCG from zero. Here the fit is the learned start (zero-share start, features, share
+// network, exact start with the predicted shares), judged by the matrix-free residual
+// ||b - A lambda|| / ||b||; when that misses tol, the plain FP64 LSCG continues from it.
+//
+// The start and the check are a fixed sequence of about a dozen short launches per octree,
+// so their launch and host costs rival the kernels. The sequence is captured once into a CUDA
+// graph per octree (its "plan") and replayed while the octree, the network, the vectors'
+// device addresses and the normalisation stay the same; any change captures a new one. The
+// graph reads the inputs' memory at every replay, so new values of b (or of the network's
+// parameters) are always used. Scratch buffers of the captured sequence live in an arena the
+// plan owns (the graph holds no allocation nodes); host vectors are staged through plan-owned
+// device buffers around the replay.
+#include <cstring>
+#include <vector>
+
+#include "its_op.cuh"
+#include "its_svo.cuh"
+
+struct its_mlp;
+
+namespace its {
+
+its_status learnedStart(its_ctx* ctx, its_svo* const* svos, int64_t count, its_mlp* mlp, const double* const* b,
+                        const float* hn, double* const* lam);
+its_status fitResidualEnqueue(its_ctx* ctx, its_svo* const* svos, int64_t count, const double* const* b,
+                              const double* const* lam, double* relDev);
+its_status hostNorm(its_ctx* ctx, const float* norm, float* hn);
+its_status mlpCheck(its_mlp* mlp);
+
+constexpr int kNormValues = 130;
+
+struct LearnedPlan {
+  its_ctx* ctx = nullptr;
+  // what the graph was captured for
+  its_mlp* mlp = nullptr;
+  const double* b = nullptr;
+  double* lam = nullptr;
+  cudaStream_t stream = nullptr;
+  float norm[kNormValues];
+  cudaGraphExec_t exec = nullptr;
+  int64_t launches = 0;     // kernels per replay
+  // owned memory
+  uint8_t* arena = nullptr; // scratch of the captured sequence
+  size_t arenaCap = 0;
+  double* relDev = nullptr;
+  double* relHost = nullptr;  // pinned
+  double* bStage = nullptr;   // device copies of host vectors
+  double* lamStage = nullptr;
+};
+
+static void dropGraph(LearnedPlan* p) {
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  p->exec = nullptr;
+}
+
+void destroyPlan(LearnedPlan* p) {
+  if (!p) return;
+  cudaStreamSynchronize(p->ctx->stream);
+  dropGraph(p);
+  cudaFree(p->arena);
+  cudaFree(p->relDev);
+  cudaFree(p->bStage);
+  cudaFree(p->lamStage);
+  cudaFreeHost(p->relHost);
+  delete p;
+}
+
+static its_status planFor(its_svo* svo, LearnedPlan** out) {
+  its_ctx* ctx = svo->ctx;
+  if (!svo->plan) {
+    LearnedPlan* p = new LearnedPlan;
+    p->ctx = ctx;
+    const int64_t n = svo->d.numVerts, c = svo->d.numCoinc;
+    // the captured sequence's buffers: zero-share start, shares, G, H (8 B per vertex each),
+    // features and predictions (260 B per coincident vertex), chunk sums, 256-byte alignment
+    p->arenaCap = (size_t)(40 * n + 264 * c + 16 * (n / 256 + 64) + (1 << 16));
+    cudaError_t e = cudaMalloc(&p->arena, p->arenaCap);
+    if (e == cudaSuccess) e = cudaMalloc(&p->relDev, 64);
+    if (e == cudaSuccess) e = cudaMallocHost(&p->relHost, 64);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      destroyPlan(p);
+      return setError(ctx, ITS_ERR_OOM, "learned fit: plan buffers");
+    }
+    svo->plan = p;
+  }
+  *out = svo->plan;
+  return ITS_OK;
+}
+
+// Queue the learned start and the residual check of one octree (device vectors).
+static its_status enqueueFit(its_svo* svo, its_mlp* mlp, const double* b, const float* hn, double* lam,
+                             double* relDev) {
+  its_status st;
+  if ((st = learnedStart(svo->ctx, &svo, 1, mlp, &b, hn, &lam)) != ITS_OK) return st;
+  return fitResidualEnqueue(svo->ctx, &svo, 1, &b, &lam, relDev);
+}
+
+// Capture the sequence for (mlp, b, lam, norm) into p->exec.
+static its_status capture(its_svo* svo, LearnedPlan* p, its_mlp* mlp, const double* b, const float* hn, double* lam) {
+  its_ctx* ctx = svo->ctx;
+  dropGraph(p);
+  const int64_t launches0 = ctx->launches;
+  ctx->arena = p->arena;
+  ctx->arenaCap = p->arenaCap;
+  ctx->arenaOff = 0;
+  cudaGraph_t graph = nullptr;
+  its_status st = ITS_OK;
+  cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    st = enqueueFit(svo, mlp, b, hn, lam, p->relDev);
+    if (st == ITS_OK)
+      e = cudaMemcpyAsync(p->relHost, p->relDev, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    const cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &graph);
+    if (e == cudaSuccess) e = e2;
+  }
+  ctx->arena = nullptr;
+  ctx->arenaCap = ctx->arenaOff = 0;
+  p->launches = ctx->launches - launches0;
+  ctx->launches = launches0;  // nothing ran yet
+  if (st == ITS_OK && e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  if (st != ITS_OK) return st;
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    p->exec = nullptr;
+    return cudaFail(ctx, e, "learned fit: graph capture");
+  }
+  p->mlp = mlp;
+  p->b = b;
+  p->lam = lam;
+  p->stream = ctx->stream;
+  std::memcpy(p->norm, hn, sizeof(p->norm));
+  return ITS_OK;
+}
+
+}  // namespace its
+
+using namespace its;
+
+extern "C" {
+
+its_status its_learned_fit(its_svo* svo, its_mlp* mlp, const double* b, const float* norm, double tol,
+                           double* lambda, its_solve_report* report) {
+  if (!svo || !mlp || !b || !norm || !lambda) return ITS_ERR_INVALID;
+  its_ctx* ctx = svo->ctx;
+  ITS_CU(ctx, cudaSetDevice(ctx->device));
+  its_status st;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  if (report) {
+    std::memset(report, 0, sizeof(*report));
+    ITS_CU(ctx, cudaEventCreate(&t0));
+    ITS_CU(ctx, cudaEventCreate(&t1));
+    ITS_CU(ctx, cudaEventRecord(t0, ctx->stream));
+  }
+  float hn[kNormValues];
+  if ((st = hostNorm(ctx, norm, hn)) != ITS_OK) return st;
+  LearnedPlan* p = nullptr;
+  if ((st = planFor(svo, &p)) != ITS_OK) return st;
+  const int64_t n = svo->d.numVerts;
+  // device addresses of the vectors: the caller's, or the plan's copies of host vectors
+  const bool bHost = !isDevicePtr(b), lamHost = !isDevicePtr(lambda);
+  if ((bHost && !p->bStage && cudaMalloc(&p->bStage, std::max<int64_t>(n, 1) * 8) != cudaSuccess) ||
+      (lamHost && !p->lamStage && cudaMalloc(&p->lamStage, std::max<int64_t>(n, 1) * 8) != cudaSuccess)) {
+    cudaGetLastError();
+    return setError(ctx, ITS_ERR_OOM, "learned fit: staging buffers");
+  }
+  const double* bd = bHost ? p->bStage : b;
+  double* ld = lamHost ? p->lamStage : lambda;
+  if (bHost) ITS_CU(ctx, cudaMemcpyAsync(p->bStage, b, n * 8, cudaMemcpyHostToDevice, ctx->stream));
+  if (!p->exec || p->mlp != mlp || p->b != bd || p->lam != ld || p->stream != ctx->stream ||
+      std::memcmp(p->norm, hn, sizeof(hn)) != 0)
+    if ((st = capture(svo, p, mlp, bd, hn, ld)) != ITS_OK) return st;
+  ITS_CU(ctx, cudaGraphLaunch(p->exec, ctx->stream));
+  ctx->launches += p->launches;
+  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  if ((st = mlpCheck(mlp)) != ITS_OK) return st;
+  double rel = *p->relHost;
+  int64_t iters = 0;
+  int converged = rel <= tol;
+  if (!converged) {  // the plain FP64 LSCG from the learned start
+    its_op* op = nullptr;
+    if ((st = its_operator_build(svo, 0, &op)) != ITS_OK) return st;
+    its_solve_opts o;
+    its_solve_opts_default(&o);
+    o.tol = tol;
+    o.stop_rule = ITS_STOP_RESIDUAL;
+    o.x0 = ld;
+    its_solve_report r;
+    st = its_lscg_solve(op, bd, ld, &o, &r);
+    its_operator_free(op);
+    if (st != ITS_OK) return st;
+    rel = r.rel_residual;
+    iters = r.iterations;
+    converged = r.converged;
+  }
+  if (lamHost) ITS_CU(ctx, cudaMemcpyAsync(lambda, ld, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  if (report) {
+    ITS_CU(ctx, cudaEventRecord(t1, ctx->stream));
+    ITS_CU(ctx, cudaEventSynchronize(t1));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    report->iterations = iters;
+    report->converged = converged;
+    report->rel_residual = rel;
+    report->ms = ms;
+  } else if (lamHost) {
+    ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  return ITS_OK;
+}
+
+}  // extern "C"

@@ -635,11 +635,6 @@ static its_status checkErr(its_mlp* h) {
 its_status mlpInfer(its_mlp* h, const float* X, int64_t n, float* out) {
   its_ctx* ctx = h->ctx;
   if (n <= 0) return ITS_OK;
-  static bool configured = false;
-  if (!configured) {
-    ITS_CU(ctx, cudaFuncSetAttribute(kMlpForwardFused, cudaFuncAttributeMaxDynamicSharedMemorySize, kFusedSmem));
-    configured = true;
-  }
   const int64_t tiles = (n + 127) / 128, ctas = (tiles + kFusedSlots - 1) / kFusedSlots;
   const unsigned grid = (unsigned)(ctas < ctx->numSMs ? ctas : ctx->numSMs);
   kMlpForwardFused<<<grid, kFusedThreads, kFusedSmem, ctx->stream>>>(X, n, h->W1, h->W2, h->W3, h->P, h->w4r, out,
@@ -682,6 +677,8 @@ its_status its_mlp_create(its_ctx* ctx, int64_t batch, its_mlp** out) {
   cudaMemsetAsync(h->Mo, 0, kNumParams * 4, ctx->stream);
   cudaMemsetAsync(h->Ve, 0, kNumParams * 4, ctx->stream);
   cudaMemsetAsync(h->err, 0, 4, ctx->stream);
+  // the fused inference kernel's shared memory, set here once (not inside a graph capture)
+  ITS_CU(ctx, cudaFuncSetAttribute(kMlpForwardFused, cudaFuncAttributeMaxDynamicSharedMemorySize, kFusedSmem));
   *out = h;
   return ITS_OK;
 }

@@ -43,7 +43,7 @@
 
 namespace its {
 
-// One octree (exact start) or one chunk of rows of an octree (residual).
+// One octree of an exact start.
 struct RowSeg {
   const RowParams* P;    // the octree's row parameters (device)
   int64_t rowBegin, rows;
@@ -53,24 +53,63 @@ struct RowSeg {
   double* lam;
 };
 
-__device__ __forceinline__ int findSeg(const int64_t* __restrict__ prefix, int nseg, int64_t i) {
-  int lo = 0, hi = nseg - 1;  // last segment with prefix[seg] <= i
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (prefix[mid] <= i) lo = mid;
-    else hi = mid - 1;
+// A segment table and its prefix. Up to kInlineSegs segments travel with the launch as a
+// kernel parameter (no copy, nothing to wait for); a larger table is copied to the device once
+// (from pageable memory, staged at the call) into keep, which the caller holds until the
+// launches are queued.
+constexpr int kInlineSegs = 16;
+template <class Seg>
+struct SegArgs {
+  int nseg = 0;
+  const Seg* dsegs = nullptr;
+  const int64_t* dprefix = nullptr;
+  Seg segs[kInlineSegs];
+  int64_t prefix[kInlineSegs + 1];
+  __device__ __forceinline__ const Seg& seg(int k) const { return dsegs ? dsegs[k] : segs[k]; }
+  __device__ __forceinline__ int64_t pre(int k) const { return dsegs ? dprefix[k] : prefix[k]; }
+  // last segment whose first item is <= i
+  __device__ __forceinline__ int find(int64_t i) const {
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (pre(mid) <= i) lo = mid;
+      else hi = mid - 1;
+    }
+    return lo;
   }
-  return lo;
+};
+
+template <class Seg>
+static its_status makeSegArgs(its_ctx* ctx, const std::vector<Seg>& segs, const std::vector<int64_t>& prefix,
+                              SegArgs<Seg>& A, DevBuf<uint8_t>& keep) {
+  A.nseg = (int)segs.size();
+  if (A.nseg <= kInlineSegs) {
+    for (int k = 0; k < A.nseg; ++k) {
+      A.segs[k] = segs[k];
+      A.prefix[k] = prefix[k];
+    }
+    A.prefix[A.nseg] = prefix[A.nseg];
+    return ITS_OK;
+  }
+  const size_t a = segs.size() * sizeof(Seg), b = (segs.size() + 1) * sizeof(int64_t);
+  std::vector<uint8_t> h(a + b);
+  std::memcpy(h.data(), segs.data(), a);
+  std::memcpy(h.data() + a, prefix.data(), b);
+  its_status st;
+  if ((st = keep.alloc(ctx, a + b)) != ITS_OK) return st;
+  ITS_CU(ctx, cudaMemcpyAsync(keep.p, h.data(), a + b, cudaMemcpyHostToDevice, ctx->stream));
+  A.dsegs = (const Seg*)keep.p;
+  A.dprefix = (const int64_t*)(keep.p + a);
+  return ITS_OK;
 }
 
 // G_r = b_r - the shares of the finer coincident vertices at r's point (finest first).
-__global__ void __launch_bounds__(256) kStartValues(const RowSeg* __restrict__ segs, const int64_t* __restrict__ prefix,
-                                                    int nseg, int64_t total) {
+__global__ void __launch_bounds__(256) kStartValues(const __grid_constant__ SegArgs<RowSeg> A, int64_t total) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= total) return;
-  const int k = findSeg(prefix, nseg, i);
-  const RowSeg& s = segs[k];
-  const int64_t r = s.rowBegin + (i - prefix[k]);
+  const int k = A.find(i);
+  const RowSeg& s = A.seg(k);
+  const int64_t r = s.rowBegin + (i - A.pre(k));
   const RowParams& P = *s.P;
   double acc = 0.0;
   if (s.shares) {
@@ -82,13 +121,12 @@ __global__ void __launch_bounds__(256) kStartValues(const RowSeg* __restrict__ s
 
 // lambda_r: the share of a coincident vertex; otherwise G_r less the interpolant of G over
 // the corners of the owner's parent cell (the row's hats of that depth, in column order).
-__global__ void __launch_bounds__(256) kStartInterp(const RowSeg* __restrict__ segs, const int64_t* __restrict__ prefix,
-                                                    int nseg, int64_t total) {
+__global__ void __launch_bounds__(256) kStartInterp(const __grid_constant__ SegArgs<RowSeg> A, int64_t total) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= total) return;
-  const int k = findSeg(prefix, nseg, i);
-  const RowSeg& s = segs[k];
-  const int64_t r = s.rowBegin + (i - prefix[k]);
+  const int k = A.find(i);
+  const RowSeg& s = A.seg(k);
+  const int64_t r = s.rowBegin + (i - A.pre(k));
   const RowParams& P = *s.P;
   const VertCoord v = vertCoord(P, r);
   if (coordCoincident(P, v)) {
@@ -105,15 +143,15 @@ __global__ void __launch_bounds__(256) kStartInterp(const RowSeg* __restrict__ s
 
 // ---- residual ||b - A lambda|| ---------------------------------------------------------
 // (A lambda)_v = (the finer coincident columns: their lambdas) + H_v, where H_v = lambda_v +
-// F_{>d}(v) is the field of v's own and the coarser depths at v. For the vertices above the
-// finest depth, H_v is summed as row v has it (the hats of every ancestor's corners). For the
-// finest vertices -- most of the rows, and the most ancestors each -- F_{>0} is trilinear on
-// the owner's parent cell (the argument of the exact start), so
+// F_{>d}(v) is the field of v's own and the coarser depths at v. F_{>d} is trilinear on the
+// owner's parent cell (the argument of the exact start), so
 //   H_v = lambda_v + sum_{corners c of the parent cell} hat_c(v) H_c:
-// the same operator with 8 hats per row instead of 8 per ancestor. Two launches (the coarse
-// band, then the finest depth) over 256-row chunks; every chunk leaves its sums of e^2 and b^2
-// in a slot of its own, a mesh's slots contiguous, and kResidualFinish adds a mesh's slots in
-// a fixed order.
+// the same operator with 8 hats per row instead of 8 per ancestor. Two bands, each one launch
+// for all octrees: the vertices above the finest depth sum H_v as row v has it (the hats of
+// every ancestor's corners); then the finest depth -- most of the rows, with the most
+// ancestors -- interpolates H from the band above. Every 256-row chunk leaves its sums of
+// e^2 and b^2 in a slot of its own, a mesh's slots contiguous, and kResidualFinish adds a
+// mesh's slots in a fixed order.
 constexpr int kResThreads = 256;
 
 struct ResSeg {
@@ -125,13 +163,12 @@ struct ResSeg {
   int64_t slot;            // slot of the segment's first chunk
 };
 
-template <bool kFine>
-__global__ void __launch_bounds__(kResThreads) kResidualBand(const ResSeg* __restrict__ segs,
-                                                            const int64_t* __restrict__ chunkFirst, int nseg,
+template <bool kInterp>
+__global__ void __launch_bounds__(kResThreads) kResidualBand(const __grid_constant__ SegArgs<ResSeg> A,
                                                             double* __restrict__ part) {
-  const int k = findSeg(chunkFirst, nseg, blockIdx.x);
-  const ResSeg& s = segs[k];
-  const int64_t j = blockIdx.x - chunkFirst[k];
+  const int k = A.find(blockIdx.x);
+  const ResSeg& s = A.seg(k);
+  const int64_t j = blockIdx.x - A.pre(k);
   const RowParams& P = *s.P;
   const int64_t i = j * kResThreads + threadIdx.x;
   double rr = 0.0, bb = 0.0;
@@ -141,15 +178,15 @@ __global__ void __launch_bounds__(kResThreads) kResidualBand(const ResSeg* __res
     const double* __restrict__ lam = s.lam;
     const double qx = P.vertPos[3 * r], qy = P.vertPos[3 * r + 1], qz = P.vertPos[3 * r + 2];
     double acc = 0.0;
-    if (kFine) {  // interpolate H from the parent cell's corners
+    if (kInterp) {  // interpolate H from the parent cell's corners
       const double* __restrict__ H = s.H;
       if (v.d + 1 < P.depth) walkAncestor(P, v, v.d + 1, qx, qy, qz, [&](int32_t c, double h) { acc += h * H[c]; });
-    } else {      // the row's own ancestors
+    } else {        // the row's own ancestors
       for (int dd = v.d + 1; dd < P.depth; ++dd)
         walkAncestor(P, v, dd, qx, qy, qz, [&](int32_t c, double h) { acc += h * lam[c]; });
     }
     const double h = lam[r] + acc;
-    if (!kFine) s.H[r] = h;
+    if (v.d > 0) s.H[r] = h;  // the finest depth's H is read by no one
     double chain = 0.0;
     walkChain(P, v.d, v.X, v.Y, v.Z, [&](int32_t c) { chain += lam[c]; });
     const double e = s.b[r] - (chain + h);
@@ -177,14 +214,21 @@ __global__ void __launch_bounds__(kResThreads) kResidualBand(const ResSeg* __res
   }
 }
 
+// Slot ranges of the meshes for kResidualFinish (inline up to kInlineSegs meshes).
+struct SlotArgs {
+  const int64_t* dfirst = nullptr;
+  int64_t first[kInlineSegs + 1];
+  __device__ __forceinline__ int64_t at(int64_t m) const { return dfirst ? dfirst[m] : first[m]; }
+};
+
 // One block per mesh: the mesh's chunk partials in a fixed order (strided per thread, then a
 // fixed tree), so the result does not depend on timing.
 __global__ void __launch_bounds__(kResThreads) kResidualFinish(const double* __restrict__ part,
-                                                               const int64_t* __restrict__ first,
+                                                               const __grid_constant__ SlotArgs F,
                                                                double* __restrict__ rel) {
   const int64_t m = blockIdx.x;
   double a = 0.0, c = 0.0;
-  for (int64_t k = first[m] + threadIdx.x; k < first[m + 1]; k += kResThreads) {
+  for (int64_t k = F.at(m) + threadIdx.x; k < F.at(m + 1); k += kResThreads) {
     a += part[2 * k];
     c += part[2 * k + 1];
   }
@@ -201,27 +245,6 @@ __global__ void __launch_bounds__(kResThreads) kResidualFinish(const double* __r
   }
   if (threadIdx.x == 0) rel[m] = sc[0] > 0.0 ? sqrt(sa[0] / sc[0]) : sqrt(sa[0]);
 }
-
-// A segment table and its prefix in one device buffer (one copy from pageable memory, staged
-// at the call, so the host vectors may go away on return).
-template <class Seg>
-struct SegTable {
-  DevBuf<uint8_t> buf;
-  const Seg* segs = nullptr;
-  const int64_t* prefix = nullptr;
-  its_status upload(its_ctx* ctx, const std::vector<Seg>& s, const std::vector<int64_t>& pre) {
-    const size_t a = s.size() * sizeof(Seg), b = pre.size() * sizeof(int64_t);
-    std::vector<uint8_t> h(a + b);
-    std::memcpy(h.data(), s.data(), a);
-    std::memcpy(h.data() + a, pre.data(), b);
-    its_status st;
-    if ((st = buf.alloc(ctx, std::max<size_t>(a + b, 8))) != ITS_OK) return st;
-    ITS_CU(ctx, cudaMemcpyAsync(buf.p, h.data(), a + b, cudaMemcpyHostToDevice, ctx->stream));
-    segs = (const Seg*)buf.p;
-    prefix = (const int64_t*)(buf.p + a);
-    return ITS_OK;
-  }
-};
 
 static const RowParams* rowParamsOf(its_svo* s) { return (const RowParams*)s->d.rowParams; }
 
@@ -256,43 +279,47 @@ its_status exactStart(its_ctx* ctx, its_svo* const* svos, int64_t count, const d
     prefix.push_back(acc);
     acc += n;
   }
-  const int nseg = (int)segs.size();
-  if (!nseg) return ITS_OK;
-  SegTable<RowSeg> T;
-  if ((st = T.upload(ctx, segs, prefix)) != ITS_OK) return st;
+  if (segs.empty()) return ITS_OK;
+  prefix.push_back(acc);
+  SegArgs<RowSeg> A;
+  DevBuf<uint8_t> keep;
+  if ((st = makeSegArgs(ctx, segs, prefix, A, keep)) != ITS_OK) return st;
   if (anyShares) {
-    kStartValues<<<gridFor(total, 256), 256, 0, ctx->stream>>>(T.segs, T.prefix, nseg, total);
+    kStartValues<<<gridFor(total, 256), 256, 0, ctx->stream>>>(A, total);
     ITS_LAUNCHED(ctx);
   }
-  kStartInterp<<<gridFor(total, 256), 256, 0, ctx->stream>>>(T.segs, T.prefix, nseg, total);
+  kStartInterp<<<gridFor(total, 256), 256, 0, ctx->stream>>>(A, total);
   ITS_LAUNCHED(ctx);
-  return ITS_OK;  // the tables were copied from pageable memory (staged at the call)
+  return ITS_OK;  // a copied table came from pageable memory (staged at the call)
 }
 
-// ||b - A lambda|| / ||b|| of count octrees (device vectors), matrix-free, into rel[count]
-// (host), each mesh's sum in a fixed order: the coarse band, the finest depth, the sums.
-its_status fitResidual(its_ctx* ctx, its_svo* const* svos, int64_t count, const double* const* b,
-                       const double* const* lam, double* rel) {
+// ||b - A lambda|| / ||b|| of count octrees (device vectors), matrix-free, into relDev[count]
+// (device), each mesh's sum in a fixed order: two bands, then the sums; queued on the
+// context's stream without a host wait.
+its_status fitResidualEnqueue(its_ctx* ctx, its_svo* const* svos, int64_t count, const double* const* b,
+                              const double* const* lam, double* relDev) {
   its_status st;
   int64_t total = 0;
   for (int64_t m = 0; m < count; ++m) total += svos[m]->d.numVerts;
   DevBuf<double> H;
   if ((st = H.alloc(ctx, std::max<int64_t>(total, 1))) != ITS_OK) return st;
-  // band 0: depths 1.. (rows vertStart[1]..numVerts-1); band 1: the finest depth. Mesh m owns
-  // slots [mFirst[m], mFirst[m+1]): its coarse band's chunks, then its finest depth's.
-  std::vector<ResSeg> segs[2];
-  std::vector<int64_t> cf[2];
-  int64_t chunks[2] = {0, 0};
+  // band 0: depths >= 1; band 1: the finest depth. Mesh m owns slots [mFirst[m], mFirst[m+1]):
+  // its band 0 chunks, then band 1's.
+  constexpr int kBands = 2;
+  std::vector<ResSeg> segs[kBands];
+  std::vector<int64_t> cf[kBands];
+  int64_t chunks[kBands] = {0, 0};
   std::vector<int64_t> mFirst(count + 1, 0);
   for (int64_t m = 0, h = 0; m < count; ++m) {
     const SvoDevice& d = svos[m]->d;
+    auto vs = [&](int k) { return d.vertStart[k < d.depth ? k : d.depth]; };
+    const int64_t lo[kBands] = {vs(1), 0}, hi[kBands] = {d.numVerts, vs(1)};
     int64_t slot = mFirst[m];
-    for (int band = 0; band < 2; ++band) {
+    for (int band = 0; band < kBands; ++band) {
       ResSeg s;
       s.P = rowParamsOf(svos[m]);
-      const int64_t fine = d.vertStart[1 < d.depth ? 1 : d.depth];  // rows of the finest depth
-      s.rowBegin = band == 0 ? fine : 0;
-      s.rows = band == 0 ? d.numVerts - fine : fine;
+      s.rowBegin = lo[band];
+      s.rows = hi[band] - lo[band];
       s.b = b[m];
       s.lam = lam[m];
       s.H = H.p + h;
@@ -307,34 +334,45 @@ its_status fitResidual(its_ctx* ctx, its_svo* const* svos, int64_t count, const 
     mFirst[m + 1] = slot;
     h += d.numVerts;
   }
-  // one upload: both bands' segments, then their chunk prefixes and the mesh slot starts
-  std::vector<ResSeg> allSegs(segs[0]);
-  allSegs.insert(allSegs.end(), segs[1].begin(), segs[1].end());
-  std::vector<int64_t> tail(cf[0]);
-  tail.push_back(chunks[0]);
-  const size_t cf1 = tail.size();
-  tail.insert(tail.end(), cf[1].begin(), cf[1].end());
-  tail.push_back(chunks[1]);
-  const size_t mfOff = tail.size();
-  tail.insert(tail.end(), mFirst.begin(), mFirst.end());
   const int64_t slots = mFirst[count];
-  SegTable<ResSeg> T;
-  DevBuf<double> part, dRel;
-  if ((st = T.upload(ctx, allSegs, tail)) != ITS_OK || (st = part.alloc(ctx, 2 * std::max<int64_t>(slots, 1))) != ITS_OK ||
-      (st = dRel.alloc(ctx, count)) != ITS_OK)
-    return st;
-  const int n0 = (int)segs[0].size(), n1 = (int)segs[1].size();
+  SegArgs<ResSeg> A[kBands];
+  DevBuf<uint8_t> keep[kBands + 1];
+  for (int band = 0; band < kBands; ++band) {
+    cf[band].push_back(chunks[band]);
+    if ((st = makeSegArgs(ctx, segs[band], cf[band], A[band], keep[band])) != ITS_OK) return st;
+  }
+  SlotArgs F;
+  if (count <= kInlineSegs) {
+    for (int64_t m = 0; m <= count; ++m) F.first[m] = mFirst[m];
+  } else {
+    if ((st = keep[kBands].alloc(ctx, (count + 1) * 8)) != ITS_OK) return st;
+    ITS_CU(ctx, cudaMemcpyAsync(keep[kBands].p, mFirst.data(), (count + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+    F.dfirst = (const int64_t*)keep[kBands].p;
+  }
+  DevBuf<double> part;
+  if ((st = part.alloc(ctx, 2 * std::max<int64_t>(slots, 1))) != ITS_OK) return st;
   if (chunks[0]) {
-    kResidualBand<false><<<(unsigned)chunks[0], kResThreads, 0, ctx->stream>>>(T.segs, T.prefix, n0, part.p);
+    kResidualBand<false><<<(unsigned)chunks[0], kResThreads, 0, ctx->stream>>>(A[0], part.p);
     ITS_LAUNCHED(ctx);
   }
-  if (chunks[1]) {
-    kResidualBand<true><<<(unsigned)chunks[1], kResThreads, 0, ctx->stream>>>(T.segs + n0, T.prefix + cf1, n1, part.p);
+  for (int band = 1; band < kBands; ++band) {
+    if (!chunks[band]) continue;
+    kResidualBand<true><<<(unsigned)chunks[band], kResThreads, 0, ctx->stream>>>(A[band], part.p);
     ITS_LAUNCHED(ctx);
   }
   if (!slots) ITS_CU(ctx, cudaMemsetAsync(part.p, 0, 16, ctx->stream));
-  kResidualFinish<<<(unsigned)count, kResThreads, 0, ctx->stream>>>(part.p, T.prefix + mfOff, dRel.p);
+  kResidualFinish<<<(unsigned)count, kResThreads, 0, ctx->stream>>>(part.p, F, relDev);
   ITS_LAUNCHED(ctx);
+  return ITS_OK;
+}
+
+// The same into rel[count] in host memory (complete on return).
+its_status fitResidual(its_ctx* ctx, its_svo* const* svos, int64_t count, const double* const* b,
+                       const double* const* lam, double* rel) {
+  its_status st;
+  DevBuf<double> dRel;
+  if ((st = dRel.alloc(ctx, count)) != ITS_OK) return st;
+  if ((st = fitResidualEnqueue(ctx, svos, count, b, lam, dRel.p)) != ITS_OK) return st;
   ITS_CU(ctx, cudaMemcpyAsync(rel, dRel.p, count * 8, cudaMemcpyDeviceToHost, ctx->stream));
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   return ITS_OK;

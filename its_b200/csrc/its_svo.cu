@@ -309,6 +309,8 @@ using namespace its;
 
 static void svoRelease(its_svo* s) {
   if (!s) return;
+  its::destroyPlan(s->plan);
+  s->plan = nullptr;
   its_ctx* c = s->ctx;
   SvoDevice& d = s->d;
   void* ptrs[] = {d.voxels, d.nodeMorton, d.nodeParent, d.nodeChild0, d.nodeLeaf, d.nodeNb, d.vertLin, d.vertKey,

@@ -2,9 +2,15 @@
 #pragma once
 #include "its_ctx.cuh"
 
+namespace its {
+struct LearnedPlan;  // the captured learned fit of an octree (its_learned.cu)
+void destroyPlan(LearnedPlan* p);
+}  // namespace its
+
 struct its_svo {
   its_ctx* ctx = nullptr;
   its::SvoDevice d;
+  its::LearnedPlan* plan = nullptr;
 };
 
 namespace its {

@@ -253,3 +253,10 @@ def test_exact_start_batch_matches_single(ctx):
     for svo, b, s, x, r in zip(svos, bs, shares, outs, rels):
         assert np.array_equal(x, svo.exact_start(b, shares=s))
         assert r == svo.residual(b, x) and r <= 1e-14
+    # more octrees than a launch carries inline (16): the tables go through device memory
+    many = [(svos[k % 4], bs[k % 4], shares[k % 4]) for k in range(19)]
+    outs = exact_start_batch([m[0] for m in many], [m[1] for m in many], [m[2] for m in many])
+    rels = fit_residual_batch([m[0] for m in many], [m[1] for m in many], outs)
+    for (svo, b, s), x, r in zip(many, outs, rels):
+        assert np.array_equal(x, svo.exact_start(b, shares=s))
+        assert r == svo.residual(b, x)

@@ -91,3 +91,40 @@ def test_trained_network_gain_on_held_out_meshes(ctx):
         svo.close()
     assert np.mean(err["learned"]) <= 0.25 * np.mean(err["zero"]), err
     net.close()
+
+
+@pytest.mark.gpu
+def test_learned_fit_graph_equals_start_and_check(ctx):
+    # its_learned_fit (captured once, then replayed) gives the learned start bit for bit and
+    # the matrix-free residual; new values of b are read at every replay, new addresses
+    # re-capture, host vectors are staged; a tolerance below the start's residual runs the
+    # plain LSCG from the start
+    import torch
+    from its_b200 import Svo
+    from its_b200.api import ShareNet, learned_fit, learned_start_batch
+    net = ShareNet(ctx, batch=4096, params=omlp.init_params(7) * np.float32(0.1))
+    rng = np.random.default_rng(1)
+    norm = np.concatenate([rng.standard_normal(64) * 0.01, np.ones(64), [0.001, 0.01]]).astype(np.float32)
+    V, F, o, w = prepared_mesh("torus", R=0.7, r=0.25, rings=48, segs=24)
+    s = Svo(ctx, V, F, 32, o, w)
+    b = ctx.signed_distance(s.vertices()[0], V, F)
+    ref = learned_start_batch([s], net, [b], norm)[0]
+    b_dev = torch.from_numpy(b).cuda()
+    lam_dev = torch.empty_like(b_dev)
+    for _ in range(3):
+        lam_dev.zero_()
+        _, rep = learned_fit(s, net, b_dev, norm, 1e-6, out=lam_dev)
+        assert np.array_equal(lam_dev.cpu().numpy(), ref)
+        assert rep["iterations"] == 0 and rep["converged"] and rep["rel_residual"] == s.residual(b, ref)
+    b_dev.mul_(0.5)  # same address, new values
+    learned_fit(s, net, b_dev, norm, 1e-6, out=lam_dev)
+    assert np.array_equal(lam_dev.cpu().numpy(), learned_start_batch([s], net, [0.5 * b], norm)[0])
+    lam_host, rep = learned_fit(s, net, b, norm, 1e-6)  # host vectors
+    assert np.array_equal(lam_host, ref) and rep["iterations"] == 0
+    norm2 = norm.copy()
+    norm2[128] += 0.001  # another normalisation: another graph
+    lam2, _ = learned_fit(s, net, b, norm2, 1e-6)
+    assert np.array_equal(lam2, learned_start_batch([s], net, [b], norm2)[0])
+    x, rep = learned_fit(s, net, b, norm, 0.1 * rep["rel_residual"])
+    assert rep["iterations"] > 0 and np.isfinite(rep["rel_residual"])
+    net.close()
