@@ -28,7 +28,7 @@ its_status learnedStart(its_ctx* ctx, its_svo* const* svos, int64_t count, its_m
 its_status fitResidualEnqueue(its_ctx* ctx, its_svo* const* svos, int64_t count, const double* const* b,
                               const double* const* lam, double* relDev);
 its_status hostNorm(its_ctx* ctx, const float* norm, float* hn);
-its_status mlpCheck(its_mlp* mlp);
+const int* mlpErrFlag(its_mlp* mlp);
 
 constexpr int kNormValues = 130;
 
@@ -46,7 +46,8 @@ struct LearnedPlan {
   uint8_t* arena = nullptr; // scratch of the captured sequence
   size_t arenaCap = 0;
   double* relDev = nullptr;
-  double* relHost = nullptr;  // pinned
+  double* relHost = nullptr;  // pinned: the residual, then the network's error flag (as int)
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
   double* bStage = nullptr;   // device copies of host vectors
   double* lamStage = nullptr;
 };
@@ -60,6 +61,8 @@ void destroyPlan(LearnedPlan* p) {
   if (!p) return;
   cudaStreamSynchronize(p->ctx->stream);
   dropGraph(p);
+  if (p->t0) cudaEventDestroy(p->t0);
+  if (p->t1) cudaEventDestroy(p->t1);
   cudaFree(p->arena);
   cudaFree(p->relDev);
   cudaFree(p->bStage);
@@ -80,6 +83,8 @@ static its_status planFor(its_svo* svo, LearnedPlan** out) {
     cudaError_t e = cudaMalloc(&p->arena, p->arenaCap);
     if (e == cudaSuccess) e = cudaMalloc(&p->relDev, 64);
     if (e == cudaSuccess) e = cudaMallocHost(&p->relHost, 64);
+    if (e == cudaSuccess) e = cudaEventCreate(&p->t0);
+    if (e == cudaSuccess) e = cudaEventCreate(&p->t1);
     if (e != cudaSuccess) {
       cudaGetLastError();
       destroyPlan(p);
@@ -114,6 +119,8 @@ static its_status capture(its_svo* svo, LearnedPlan* p, its_mlp* mlp, const doub
     st = enqueueFit(svo, mlp, b, hn, lam, p->relDev);
     if (st == ITS_OK)
       e = cudaMemcpyAsync(p->relHost, p->relDev, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    if (st == ITS_OK && e == cudaSuccess)
+      e = cudaMemcpyAsync(p->relHost + 1, mlpErrFlag(mlp), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
     const cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &graph);
     if (e == cudaSuccess) e = e2;
   }
@@ -149,17 +156,14 @@ its_status its_learned_fit(its_svo* svo, its_mlp* mlp, const double* b, const fl
   its_ctx* ctx = svo->ctx;
   ITS_CU(ctx, cudaSetDevice(ctx->device));
   its_status st;
-  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  LearnedPlan* p = nullptr;
+  if ((st = planFor(svo, &p)) != ITS_OK) return st;
   if (report) {
     std::memset(report, 0, sizeof(*report));
-    ITS_CU(ctx, cudaEventCreate(&t0));
-    ITS_CU(ctx, cudaEventCreate(&t1));
-    ITS_CU(ctx, cudaEventRecord(t0, ctx->stream));
+    ITS_CU(ctx, cudaEventRecord(p->t0, ctx->stream));
   }
   float hn[kNormValues];
   if ((st = hostNorm(ctx, norm, hn)) != ITS_OK) return st;
-  LearnedPlan* p = nullptr;
-  if ((st = planFor(svo, &p)) != ITS_OK) return st;
   const int64_t n = svo->d.numVerts;
   // device addresses of the vectors: the caller's, or the plan's copies of host vectors
   const bool bHost = !isDevicePtr(b), lamHost = !isDevicePtr(lambda);
@@ -177,7 +181,9 @@ its_status its_learned_fit(its_svo* svo, its_mlp* mlp, const double* b, const fl
   ITS_CU(ctx, cudaGraphLaunch(p->exec, ctx->stream));
   ctx->launches += p->launches;
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
-  if ((st = mlpCheck(mlp)) != ITS_OK) return st;
+  int netErr = 0;
+  std::memcpy(&netErr, p->relHost + 1, sizeof(int));
+  if (netErr) return setError(ctx, ITS_ERR_TIMEOUT, "share network: a tensor-core wait ran out");
   double rel = *p->relHost;
   int64_t iters = 0;
   int converged = rel <= tol;
@@ -199,12 +205,10 @@ its_status its_learned_fit(its_svo* svo, its_mlp* mlp, const double* b, const fl
   }
   if (lamHost) ITS_CU(ctx, cudaMemcpyAsync(lambda, ld, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
   if (report) {
-    ITS_CU(ctx, cudaEventRecord(t1, ctx->stream));
-    ITS_CU(ctx, cudaEventSynchronize(t1));
+    ITS_CU(ctx, cudaEventRecord(p->t1, ctx->stream));
+    ITS_CU(ctx, cudaEventSynchronize(p->t1));
     float ms = 0.0f;
-    cudaEventElapsedTime(&ms, t0, t1);
-    cudaEventDestroy(t0);
-    cudaEventDestroy(t1);
+    cudaEventElapsedTime(&ms, p->t0, p->t1);
     report->iterations = iters;
     report->converged = converged;
     report->rel_residual = rel;

@@ -644,6 +644,8 @@ its_status mlpInfer(its_mlp* h, const float* X, int64_t n, float* out) {
 }
 
 its_status mlpCheck(its_mlp* h) { return checkErr(h); }
+// The network's (sticky) error flag in device memory, for callers that read it with their own copy.
+const int* mlpErrFlag(its_mlp* h) { return h->err; }
 
 }  // namespace its
 

@@ -149,9 +149,9 @@ __global__ void __launch_bounds__(256) kStartInterp(const __grid_constant__ SegA
 // the same operator with 8 hats per row instead of 8 per ancestor. Two bands, each one launch
 // for all octrees: the vertices above the finest depth sum H_v as row v has it (the hats of
 // every ancestor's corners); then the finest depth -- most of the rows, with the most
-// ancestors -- interpolates H from the band above. Every 256-row chunk leaves its sums of
-// e^2 and b^2 in a slot of its own, a mesh's slots contiguous, and kResidualFinish adds a
-// mesh's slots in a fixed order.
+// ancestors -- interpolates H from the band above. Every chunk of rows (32 in the coarse band,
+// 256 at the finest depth) leaves its sums of e^2 and b^2 in a slot of its own, a mesh's slots
+// contiguous, and kResidualFinish adds a mesh's slots in a fixed order.
 constexpr int kResThreads = 256;
 
 struct ResSeg {
@@ -163,8 +163,8 @@ struct ResSeg {
   int64_t slot;            // slot of the segment's first chunk
 };
 
-template <bool kInterp>
-__global__ void __launch_bounds__(kResThreads) kResidualBand(const __grid_constant__ SegArgs<ResSeg> A,
+// The finest depth: one row per thread, H interpolated from the parent cell's corners.
+__global__ void __launch_bounds__(kResThreads) kResidualFine(const __grid_constant__ SegArgs<ResSeg> A,
                                                             double* __restrict__ part) {
   const int k = A.find(blockIdx.x);
   const ResSeg& s = A.seg(k);
@@ -176,17 +176,12 @@ __global__ void __launch_bounds__(kResThreads) kResidualBand(const __grid_consta
     const int64_t r = s.rowBegin + i;
     const VertCoord v = vertCoord(P, r);
     const double* __restrict__ lam = s.lam;
-    const double qx = P.vertPos[3 * r], qy = P.vertPos[3 * r + 1], qz = P.vertPos[3 * r + 2];
+    const double* __restrict__ H = s.H;
     double acc = 0.0;
-    if (kInterp) {  // interpolate H from the parent cell's corners
-      const double* __restrict__ H = s.H;
-      if (v.d + 1 < P.depth) walkAncestor(P, v, v.d + 1, qx, qy, qz, [&](int32_t c, double h) { acc += h * H[c]; });
-    } else {        // the row's own ancestors
-      for (int dd = v.d + 1; dd < P.depth; ++dd)
-        walkAncestor(P, v, dd, qx, qy, qz, [&](int32_t c, double h) { acc += h * lam[c]; });
-    }
+    if (v.d + 1 < P.depth)
+      walkAncestor(P, v, v.d + 1, P.vertPos[3 * r], P.vertPos[3 * r + 1], P.vertPos[3 * r + 2],
+                   [&](int32_t c, double h) { acc += h * H[c]; });
     const double h = lam[r] + acc;
-    if (v.d > 0) s.H[r] = h;  // the finest depth's H is read by no one
     double chain = 0.0;
     walkChain(P, v.d, v.X, v.Y, v.Z, [&](int32_t c) { chain += lam[c]; });
     const double e = s.b[r] - (chain + h);
@@ -211,6 +206,61 @@ __global__ void __launch_bounds__(kResThreads) kResidualBand(const __grid_consta
     }
     part[2 * (s.slot + j)] = a;
     part[2 * (s.slot + j) + 1] = c;
+  }
+}
+
+// The coarse band: 32 rows per block, lane l of every warp on row l, warp w summing the hats
+// of the ancestors at depths d+1+w, d+9+w, ... (a warp's loads stay on one depth of
+// neighbouring rows; these rows are few, so the ancestors, not the rows, fill the GPU). Warp 0
+// also takes the row's finer coincident columns; the parts are added in warp order.
+constexpr int kResCoarseRows = 32;
+constexpr int kResWarps = kResThreads / 32;
+__global__ void __launch_bounds__(kResThreads) kResidualCoarse(const __grid_constant__ SegArgs<ResSeg> A,
+                                                              double* __restrict__ part) {
+  __shared__ double sacc[kResWarps][kResCoarseRows];
+  const int k = A.find(blockIdx.x);
+  const ResSeg& s = A.seg(k);
+  const int64_t j = blockIdx.x - A.pre(k);
+  const RowParams& P = *s.P;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t i = j * kResCoarseRows + lane;
+  const double* __restrict__ lam = s.lam;
+  double acc = 0.0;
+  if (i < s.rows) {
+    const int64_t r = s.rowBegin + i;
+    const VertCoord v = vertCoord(P, r);
+    if (v.d + 1 + warp < P.depth) {
+      const double qx = P.vertPos[3 * r], qy = P.vertPos[3 * r + 1], qz = P.vertPos[3 * r + 2];
+      for (int dd = v.d + 1 + warp; dd < P.depth; dd += kResWarps)
+        walkAncestor(P, v, dd, qx, qy, qz, [&](int32_t c, double h) { acc += h * lam[c]; });
+    }
+  }
+  sacc[warp][lane] = acc;
+  __syncthreads();
+  if (warp == 0) {
+    double rr = 0.0, bb = 0.0;
+    if (i < s.rows) {
+      const int64_t r = s.rowBegin + i;
+      double t = 0.0;
+#pragma unroll
+      for (int w = 0; w < kResWarps; ++w) t += sacc[w][lane];
+      const double h = lam[r] + t;
+      s.H[r] = h;
+      const VertCoord v = vertCoord(P, r);
+      double chain = 0.0;
+      walkChain(P, v.d, v.X, v.Y, v.Z, [&](int32_t c) { chain += lam[c]; });
+      const double e = s.b[r] - (chain + h);
+      rr = e * e;
+      bb = s.b[r] * s.b[r];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      rr += __shfl_down_sync(0xffffffffu, rr, o);
+      bb += __shfl_down_sync(0xffffffffu, bb, o);
+    }
+    if (lane == 0) {
+      part[2 * (s.slot + j)] = rr;
+      part[2 * (s.slot + j) + 1] = bb;
+    }
   }
 }
 
@@ -324,7 +374,8 @@ its_status fitResidualEnqueue(its_ctx* ctx, its_svo* const* svos, int64_t count,
       s.lam = lam[m];
       s.H = H.p + h;
       s.slot = slot;
-      const int64_t c = (s.rows + kResThreads - 1) / kResThreads;
+      const int64_t per = band == 0 ? kResCoarseRows : kResThreads;  // rows per chunk
+      const int64_t c = (s.rows + per - 1) / per;
       if (!c) continue;
       segs[band].push_back(s);
       cf[band].push_back(chunks[band]);
@@ -352,12 +403,12 @@ its_status fitResidualEnqueue(its_ctx* ctx, its_svo* const* svos, int64_t count,
   DevBuf<double> part;
   if ((st = part.alloc(ctx, 2 * std::max<int64_t>(slots, 1))) != ITS_OK) return st;
   if (chunks[0]) {
-    kResidualBand<false><<<(unsigned)chunks[0], kResThreads, 0, ctx->stream>>>(A[0], part.p);
+    kResidualCoarse<<<(unsigned)chunks[0], kResThreads, 0, ctx->stream>>>(A[0], part.p);
     ITS_LAUNCHED(ctx);
   }
   for (int band = 1; band < kBands; ++band) {
     if (!chunks[band]) continue;
-    kResidualBand<true><<<(unsigned)chunks[band], kResThreads, 0, ctx->stream>>>(A[band], part.p);
+    kResidualFine<<<(unsigned)chunks[band], kResThreads, 0, ctx->stream>>>(A[band], part.p);
     ITS_LAUNCHED(ctx);
   }
   if (!slots) ITS_CU(ctx, cudaMemsetAsync(part.p, 0, 16, ctx->stream));
