@@ -12,7 +12,8 @@
 // graph reads the inputs' memory at every replay, so new values of b (or of the network's
 // parameters) are always used. Scratch buffers of the captured sequence live in an arena the
 // plan owns (the graph holds no allocation nodes); host vectors are staged through plan-owned
-// device buffers around the replay.
+// device buffers around the replay. The residual's last kernel writes its result straight to
+// the plan's mapped pinned memory; the network's error flag is copied beside it.
 #include <cstring>
 #include <vector>
 
@@ -45,8 +46,9 @@ struct LearnedPlan {
   // owned memory
   uint8_t* arena = nullptr; // scratch of the captured sequence
   size_t arenaCap = 0;
-  double* relDev = nullptr;
-  double* relHost = nullptr;  // pinned: the residual, then the network's error flag (as int)
+  double* relHost = nullptr;  // pinned: the residual (written by the residual's last kernel
+                              // through the mapped address), then the network's error flag
+  double* relMapped = nullptr;  // relHost's device address
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   double* bStage = nullptr;   // device copies of host vectors
   double* lamStage = nullptr;
@@ -64,7 +66,6 @@ void destroyPlan(LearnedPlan* p) {
   if (p->t0) cudaEventDestroy(p->t0);
   if (p->t1) cudaEventDestroy(p->t1);
   cudaFree(p->arena);
-  cudaFree(p->relDev);
   cudaFree(p->bStage);
   cudaFree(p->lamStage);
   cudaFreeHost(p->relHost);
@@ -81,8 +82,8 @@ static its_status planFor(its_svo* svo, LearnedPlan** out) {
     // features and predictions (260 B per coincident vertex), chunk sums, 256-byte alignment
     p->arenaCap = (size_t)(40 * n + 264 * c + 16 * (n / 256 + 64) + (1 << 16));
     cudaError_t e = cudaMalloc(&p->arena, p->arenaCap);
-    if (e == cudaSuccess) e = cudaMalloc(&p->relDev, 64);
-    if (e == cudaSuccess) e = cudaMallocHost(&p->relHost, 64);
+    if (e == cudaSuccess) e = cudaHostAlloc(&p->relHost, 64, cudaHostAllocMapped);
+    if (e == cudaSuccess) e = cudaHostGetDevicePointer(&p->relMapped, p->relHost, 0);
     if (e == cudaSuccess) e = cudaEventCreate(&p->t0);
     if (e == cudaSuccess) e = cudaEventCreate(&p->t1);
     if (e != cudaSuccess) {
@@ -116,10 +117,8 @@ static its_status capture(its_svo* svo, LearnedPlan* p, its_mlp* mlp, const doub
   its_status st = ITS_OK;
   cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    st = enqueueFit(svo, mlp, b, hn, lam, p->relDev);
+    st = enqueueFit(svo, mlp, b, hn, lam, p->relMapped);
     if (st == ITS_OK)
-      e = cudaMemcpyAsync(p->relHost, p->relDev, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
-    if (st == ITS_OK && e == cudaSuccess)
       e = cudaMemcpyAsync(p->relHost + 1, mlpErrFlag(mlp), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
     const cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &graph);
     if (e == cudaSuccess) e = e2;
@@ -180,6 +179,7 @@ its_status its_learned_fit(its_svo* svo, its_mlp* mlp, const double* b, const fl
     if ((st = capture(svo, p, mlp, bd, hn, ld)) != ITS_OK) return st;
   ITS_CU(ctx, cudaGraphLaunch(p->exec, ctx->stream));
   ctx->launches += p->launches;
+  if (report) ITS_CU(ctx, cudaEventRecord(p->t1, ctx->stream));
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   int netErr = 0;
   std::memcpy(&netErr, p->relHost + 1, sizeof(int));
@@ -202,10 +202,13 @@ its_status its_learned_fit(its_svo* svo, its_mlp* mlp, const double* b, const fl
     rel = r.rel_residual;
     iters = r.iterations;
     converged = r.converged;
+    if (report) ITS_CU(ctx, cudaEventRecord(p->t1, ctx->stream));
   }
-  if (lamHost) ITS_CU(ctx, cudaMemcpyAsync(lambda, ld, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  if (lamHost) {
+    ITS_CU(ctx, cudaMemcpyAsync(lambda, ld, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    if (report) ITS_CU(ctx, cudaEventRecord(p->t1, ctx->stream));
+  }
   if (report) {
-    ITS_CU(ctx, cudaEventRecord(p->t1, ctx->stream));
     ITS_CU(ctx, cudaEventSynchronize(p->t1));
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, p->t0, p->t1);
