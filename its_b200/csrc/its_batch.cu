@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(kSpmvThreads) kBatchSpmv(const BatchOp* __rest
   if (b < L.blockStart[2]) return batchClass<2>(ops, L, 1, b - L.blockStart[1], tr, x, y, S);
   if (b < L.blockStart[3]) return batchClass<4>(ops, L, 2, b - L.blockStart[2], tr, x, y, S);
   if (b < L.blockStart[4]) return batchClass<8>(ops, L, 3, b - L.blockStart[3], tr, x, y, S);
-  if (b < L.blockStart[5]) return batchClass<16>(ops, L, 4, b - L.blockStart[4], tr, x, y, S);
+  if (b < L.blockStart[5]) return batchClass<classLanes(4)>(ops, L, 4, b - L.blockStart[4], tr, x, y, S);
   if (b < L.blockStart[6]) return batchClass<32>(ops, L, 5, b - L.blockStart[5], tr, x, y, S);
   const int64_t seg = b - L.blockStart[6];
   if (seg >= L.nSeg) return;

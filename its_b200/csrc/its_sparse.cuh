@@ -4,9 +4,11 @@
 // nine entries (fine-level columns) with a few enormous ones (a corner of the root cell is
 // touched by almost every row of A). Rows are therefore classed once per matrix by length and
 // each class gets the lane count that keeps every lane busy with a few entries:
-//   class 0..5: 1, 2, 4, 8, 16, 32 lanes for rows of <= 4, 8, 16, 32, 64, 4096 entries;
-//   class 6:    rows above 4096 entries, cut into 4096-entry segments (one block each) whose
+//   class 0..5: 1, 2, 4, 8, 8, 32 lanes for rows of <= 4, 8, 16, 32, 64, 512 entries;
+//   class 6:    rows above 512 entries, cut into 4096-entry segments (one block each) whose
 //               partial sums a second pass adds in segment order.
+// (A warp per row up to 4096 entries left the longest of those rows -- 128 entries per lane
+// -- as the launch's stragglers: A^T took 79 us at 1e7 entries; cut at 512, 48 us.)
 // Each lane keeps two accumulators (alternate entries) so that two loads are in flight.
 // Every sum has a fixed order, so results are bit-reproducible run to run. All classes run in
 // one launch (block ranges pick the class); long rows need one extra combine launch.
@@ -17,11 +19,13 @@ namespace its {
 
 constexpr int kNumClasses = 7;  // 6 lane widths + long rows
 constexpr int kLongClass = 6;
-constexpr int kMidMax = 4096;
+constexpr int kMidMax = 512;
 constexpr int kSegLen = 4096;
 constexpr int kSpmvThreads = 256;
 
-__host__ __device__ constexpr int classLanes(int c) { return 1 << c; }     // classes 0..5
+// lanes per row of classes 0..5: 33..64-entry rows take 8 lanes (4 to 8 entries each, two in
+// flight per lane), which measured faster than 16 for A's dominant class (43 vs 48 us)
+__host__ __device__ constexpr int classLanes(int c) { return c == 4 ? 8 : 1 << c; }
 __host__ __device__ constexpr int classMaxLen(int c) { return c == 5 ? kMidMax : 4 << c; }
 
 struct SpmvPlan {
@@ -92,7 +96,7 @@ __global__ void __launch_bounds__(kSpmvThreads) kSpmvBinned(CsrView<VT, XT> A, S
   if (b < P.blockStart[2]) return spmvClass<2>(A, P, 1, b - P.blockStart[1], x, y);
   if (b < P.blockStart[3]) return spmvClass<4>(A, P, 2, b - P.blockStart[2], x, y);
   if (b < P.blockStart[4]) return spmvClass<8>(A, P, 3, b - P.blockStart[3], x, y);
-  if (b < P.blockStart[5]) return spmvClass<16>(A, P, 4, b - P.blockStart[4], x, y);
+  if (b < P.blockStart[5]) return spmvClass<classLanes(4)>(A, P, 4, b - P.blockStart[4], x, y);
   if (b < P.blockStart[6]) return spmvClass<32>(A, P, 5, b - P.blockStart[5], x, y);
   // one long-row segment per block
   const int64_t seg = b - P.blockStart[6];
