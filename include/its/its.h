@@ -262,6 +262,20 @@ its_status its_marching_cubes_mesh(its_ctx* ctx, const double* field, int res, c
    values (vertex positions in FP64). No counterpart in the reference (FP64 only). */
 its_status its_eval_grid_f32(its_svo* svo, const double* lambda, const double origin[3], const double width[3],
                              int res, float* field);
+/* The dense field of its_eval_grid (FP64) / its_eval_grid_f32 (FP32) on a lattice aligned with
+   the octree -- origin and width the octree's box (to 1e-6 of a cell), res = the octree's res
+   * 1, 2, 4 or 8 (the marching-cubes grids of ThinShells::mcVisualization,
+   src/ThinShells.cpp:1086-1129) -- built coarse to fine by trilinear prolongation over dense
+   per-depth lattices: the cost of writing the field once instead of evaluating every point at
+   every depth. Not bit for bit its_eval_grid: the hats sit on the octree's exact lattice
+   points, where the reference's corner positions and a single-precision-padded box differ by
+   ~1e-9 (field within ~1e-7 of max |field|, tested); any other lattice falls back to
+   its_eval_grid / its_eval_grid_f32. Scratch: 8 (FP32: 4) bytes per point of every depth's
+   lattice, ((res_octree + 1)^3 * 8 / 7 points). */
+its_status its_eval_grid_fast(its_svo* svo, const double* lambda, const double origin[3], const double width[3],
+                              int res, double* field);
+its_status its_eval_grid_fast_f32(its_svo* svo, const double* lambda, const double origin[3], const double width[3],
+                                  int res, float* field);
 its_status its_marching_cubes_f32(its_ctx* ctx, const float* field, int res, const double origin[3],
                                   const double width[3], double iso, uint8_t* cube_index, double* tri_verts,
                                   int64_t capacity, int64_t* num_verts);

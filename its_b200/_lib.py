@@ -89,6 +89,8 @@ SIGNATURES = {
     "its_marching_cubes": (st, [vp, vp, i32, vp, vp, dbl, vp, vp, i64, C.POINTER(i64)]),
     "its_marching_cubes_f32": (st, [vp, vp, i32, vp, vp, dbl, vp, vp, i64, C.POINTER(i64)]),
     "its_eval_grid_f32": (st, [vp, vp, vp, vp, i32, vp]),
+    "its_eval_grid_fast": (st, [vp, vp, vp, vp, i32, vp]),
+    "its_eval_grid_fast_f32": (st, [vp, vp, vp, vp, i32, vp]),
     "its_marching_cubes_mesh": (st, [vp, vp, i32, vp, vp, dbl, vp, i64, C.POINTER(i64), vp, i64, C.POINTER(i64)]),
 }
 

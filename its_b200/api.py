@@ -321,6 +321,17 @@ class Svo:
                        "its_eval_grid_f32")
         return out
 
+    def eval_grid_fast(self, lam, origin, width, res, out=None, fp32=False):
+        """Dense field by prolongation on a lattice aligned with the octree (its_eval_grid_fast,
+        its_eval_grid_fast_f32); other lattices fall back to the point-by-point forms."""
+        lam = _f64(lam)
+        o, w = np.ascontiguousarray(origin, np.float64), np.ascontiguousarray(width, np.float64)
+        if out is None:
+            out = np.zeros((res + 1) ** 3, np.float32 if fp32 else np.float64)
+        fn = lib().its_eval_grid_fast_f32 if fp32 else lib().its_eval_grid_fast
+        self.ctx.check(fn(self.h, _ptr(lam), _ptr(o), _ptr(w), res, _ptr(out)), "its_eval_grid_fast")
+        return out
+
     def vertex_sdf(self, V, F):
         """Right-hand side b: signed distance of every corner vertex (ThinShells::cpSDFOfTreeNodes)."""
         pos, _ = self.vertices()

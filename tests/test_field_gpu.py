@@ -234,3 +234,54 @@ def test_point_value_gradient_matches_oracle(ctx):
         ok = (mp == 0) & (mm == 0)
         fd = (fp - fm) / (2 * h)
         assert np.median(np.abs(fd[ok] - g[inside][ok, a])) <= 1e-5 * np.abs(g[inside]).max()
+
+
+def _cascade_numpy(pos, lam, depth_counts, o, unit, res, f):
+    """The prolongation cascade restated in numpy (hats on the exact lattice points)."""
+    D = len(depth_counts)
+    depth = np.repeat(np.arange(D), depth_counts)
+    acc = None
+    for d in range(D - 1, -1, -1):
+        M = (res >> d) + 1
+        A = np.zeros((M, M, M))
+        sel = depth == d
+        X = np.rint((pos[sel] - o) / (unit * 2 ** d)).astype(int)
+        A[X[:, 0], X[:, 1], X[:, 2]] = lam[sel]
+        acc = A if acc is None else A + _prolong(acc, 2)
+    return acc if f == 1 else _prolong(acc, f)
+
+
+def _prolong(C, f):
+    Mc = C.shape[0]
+    idx = np.arange((Mc - 1) * f + 1)
+    c0, r = idx // f, idx % f
+    c1 = np.minimum(c0 + 1, Mc - 1)
+    w1 = r / f
+    w0 = 1 - w1
+    X = w0[:, None, None] * C[c0] + w1[:, None, None] * C[c1]
+    Y = w0[None, :, None] * X[:, c0] + w1[None, :, None] * X[:, c1]
+    return w0[None, None, :] * Y[:, :, c0] + w1[None, None, :] * Y[:, :, c1]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("f", [1, 2, 4])
+def test_grid_field_by_prolongation(fitted, f):
+    # on the octree's own lattice (res * f): the cascade equals its numpy restatement to
+    # rounding, and the point-by-point field to the geometry's single-precision offsets (corner
+    # positions and a float-padded box a few 1e-9 off the lattice: ~1e-8 of max |field|); FP32
+    # within FP32 rounding; a lattice off the octree's falls back to the exact evaluator
+    V, F, o, w, ref, gpu, pos, b, lam = fitted
+    res = 32
+    R = res * f
+    M = R + 1
+    exact = gpu.eval_grid(lam, o, w, R)
+    fast = gpu.eval_grid_fast(lam, o, w, R)
+    scale = np.abs(exact).max()
+    assert np.abs(fast - exact).max() <= 1e-6 * scale
+    unit = np.full(3, np.asarray(w, float)[0] / res)  # the octree sizes its cells by its first axis
+    cas = _cascade_numpy(pos, lam, gpu.depth_counts()[1], np.asarray(o, float), unit, res, f)
+    assert np.abs(fast.reshape(M, M, M).transpose(2, 1, 0) - cas).max() <= 1e-13 * scale
+    f32 = gpu.eval_grid_fast(lam, o, w, R, fp32=True)
+    assert np.abs(f32.astype(np.float64) - exact).max() <= 1e-5 * scale
+    shifted = np.asarray(o, float) + 0.25 * unit
+    assert np.array_equal(gpu.eval_grid_fast(lam, shifted, w, R), gpu.eval_grid(lam, shifted, w, R))
