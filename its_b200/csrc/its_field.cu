@@ -402,6 +402,50 @@ __global__ void __launch_bounds__(kScanThreads) kMcClassify(const T* __restrict_
   if (threadIdx.x == 0) blockSums[blockIdx.x] = total;
 }
 
+// kMcClassify for R a multiple of 256 (tiles of 8 voxels per thread): the same case bytes and
+// block sums with coalesced loads. A warp takes 256 consecutive voxels of one row, lane l the
+// voxels x0 + l + 32 j; each of the 4 corner rows is read 32 values per load, and the x+1
+// corners come from the next lane (lane 31 from lane 0 of the next round, or one extra load).
+template <typename T>
+__global__ void __launch_bounds__(kScanThreads) kMcClassifyRows(const T* __restrict__ field, int R, double iso,
+                                                               uint8_t* __restrict__ cube,
+                                                               unsigned long long* __restrict__ blockSums) {
+  const int64_t M = (int64_t)R + 1;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t s = (int64_t)blockIdx.x * (kScanThreads * 8) + (int64_t)warp * 256;  // the warp's first voxel
+  int64_t x0, y, z;
+  voxelXYZ(s, R, x0, y, z);
+  const int64_t r[4] = {(z * M + y) * M + x0, (z * M + y + 1) * M + x0, ((z + 1) * M + y) * M + x0,
+                        ((z + 1) * M + y + 1) * M + x0};
+  double v[4][9];  // corner rows: v[k][j] at x0 + lane + 32 j; v[k][8] at x0 + 256 (all lanes)
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v[k][j] = (double)field[r[k] + lane + 32 * j];
+    v[k][8] = (double)field[r[k] + 256];
+  }
+  unsigned long long cnt = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    double n[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const double down = __shfl_down_sync(0xffffffffu, v[k][j], 1);
+      const double wrap = __shfl_sync(0xffffffffu, v[k][j < 7 ? j + 1 : 0], 0);
+      n[k] = lane < 31 ? down : (j < 7 ? wrap : v[k][8]);
+    }
+    // corner order 0 (0,0,0) 1 (0,1,0) 2 (1,1,0) 3 (1,0,0) 4 (0,0,1) 5 (0,1,1) 6 (1,1,1) 7 (1,0,1)
+    const unsigned ci = (unsigned)(v[0][j] < iso) | (unsigned)(v[1][j] < iso) << 1 | (unsigned)(n[1] < iso) << 2 |
+                        (unsigned)(n[0] < iso) << 3 | (unsigned)(v[2][j] < iso) << 4 |
+                        (unsigned)(v[3][j] < iso) << 5 | (unsigned)(n[3] < iso) << 6 | (unsigned)(n[2] < iso) << 7;
+    cube[s + lane + 32 * j] = (uint8_t)ci;
+    cnt += cMcCase[ci] & 15ull;
+  }
+  unsigned long long total;
+  blockExclusiveScan<unsigned long long>(cnt, total);
+  if (threadIdx.x == 0) blockSums[blockIdx.x] = total;
+}
+
 template <typename T, int ITEMS>
 __global__ void __launch_bounds__(kScanThreads) kMcEmit(McCaseT<T> mc, double3 o, double3 vs,
                                                          const uint8_t* __restrict__ cube,
@@ -775,6 +819,8 @@ its_status marchingCubesT(its_ctx* ctx, const FT* field, int res, const double o
       kMcClassify<FT, 16><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(F.d, res, iso, cubeD, sums.p);
     else if (items == 4)
       kMcClassify<FT, 4><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(F.d, res, iso, cubeD, sums.p);
+    else if (res % 256 == 0)
+      kMcClassifyRows<FT><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(F.d, res, iso, cubeD, sums.p);
     else
       kMcClassify<FT, 8><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(F.d, res, iso, cubeD, sums.p);
     ITS_LAUNCHED(ctx);

@@ -285,3 +285,29 @@ def test_grid_field_by_prolongation(fitted, f):
     assert np.abs(f32.astype(np.float64) - exact).max() <= 1e-5 * scale
     shifted = np.asarray(o, float) + 0.25 * unit
     assert np.array_equal(gpu.eval_grid_fast(lam, shifted, w, R), gpu.eval_grid(lam, shifted, w, R))
+
+
+@pytest.mark.gpu
+def test_marching_cubes_row_tiles_bit_exact(ctx, fitted):
+    # grids whose side is a multiple of 256 classify with row tiles (coalesced loads, lanes on
+    # interleaved voxels): the same case bytes and triangles as the oracle, FP64 and FP32
+    import ctypes as C
+    from its_b200 import lib
+    V, F, o, w, ref, gpu, pos, b, lam = fitted
+    R = 256
+    field = gpu.eval_grid_fast(lam, o, w, R)
+    iso = float(np.median(b[np.abs(b) < 0.05]))
+    cube_g, tri_g, n_g = ctx.marching_cubes(field, R, o, w, iso)
+    cube_r, tri_r, n_r = oracle.marching_cubes(field, R, o, w, iso)
+    assert n_g == n_r and n_g > 0
+    assert np.array_equal(cube_g, cube_r)
+    assert np.array_equal(tri_g, tri_r)
+    f32 = field.astype(np.float32)
+    cube = np.zeros(R ** 3, np.uint8)
+    n = C.c_int64(0)
+    o_, w_ = np.ascontiguousarray(o, np.float64), np.ascontiguousarray(w, np.float64)
+    ctx.check(lib().its_marching_cubes_f32(ctx.h, f32.ctypes.data_as(C.c_void_p), R, o_.ctypes.data_as(C.c_void_p),
+                                           w_.ctypes.data_as(C.c_void_p), iso, cube.ctypes.data_as(C.c_void_p), None, 0,
+                                           C.byref(n)), "mc f32")
+    cube_r32, _, n_r32 = oracle.marching_cubes(f32.astype(np.float64), R, o, w, iso)
+    assert np.array_equal(cube, cube_r32) and n.value == n_r32
