@@ -33,56 +33,44 @@ __global__ void kScatterCorners(int64_t n, const uint64_t* __restrict__ vertKey,
   D[off[c.d] + c.X + M * (c.Y + M * (int64_t)c.Z)] = (T)lambda[v];
 }
 
-// One axis of the prolongation by a factor 2^s: the coarse points around fine coordinate y
-// and their weights.
-struct Axis {
-  int64_t c0, c1;
-  int two;  // 1: c0 only (weight 1); 2: c0 and c1 (weights w0, w1)
-  double w0, w1;
-};
-__device__ __forceinline__ Axis axisOf(int64_t y, int s) {
-  Axis a;
-  const int64_t f = (int64_t)1 << s, r = y & (f - 1);
-  a.c0 = y >> s;
-  a.c1 = a.c0 + 1;
-  a.two = r ? 2 : 1;
-  a.w1 = (double)r / (double)f;
-  a.w0 = 1.0 - a.w1;
-  return a;
-}
-
 // fine = (accumulate ? fine : 0) + the trilinear prolongation of coarse by the factor 2^s
 // (fine has Mf = (Mc - 1) 2^s + 1 points per axis, x fastest). One thread per coarse x
 // interval and fine (y, z): it reads the interval's ends on the <= 4 coarse rows around
 // (y, z) and writes the 2^s fine points of the interval (the last coarse point: one), so a
-// warp's stores are contiguous. Launch: x-y pairs flattened over blockIdx.x, z in blockIdx.y.
+// warp's stores are contiguous. Blocks of 32 intervals x 8 fine rows; z per block.
 template <typename T, int S>
-__global__ void __launch_bounds__(256) kProlong(const T* __restrict__ coarse, int64_t Mc, T* __restrict__ fine,
+__global__ void __launch_bounds__(256) kProlong(const T* __restrict__ coarse, int Mc, T* __restrict__ fine,
                                                 int accumulate) {
   constexpr int F = 1 << S;
-  const int64_t Mf = (Mc - 1) * F + 1;
-  const uint32_t t = blockIdx.x * 256u + threadIdx.x;
-  const uint32_t xc = t % (uint32_t)Mc, y = t / (uint32_t)Mc;
-  if (y >= Mf) return;
-  const int64_t z = blockIdx.y;
-  const Axis ay = axisOf(y, S), az = axisOf(z, S);
-  const bool xr = xc + 1 < Mc;  // the interval has a right end
-  T a0 = T(0), a1 = T(0);       // the coarse field at x = xc and xc + 1, interpolated in y, z
-  for (int k = 0; k < az.two; ++k) {
-    const T wz = (T)(k ? az.w1 : az.w0);
-    const int64_t cz = k ? az.c1 : az.c0;
-    for (int j = 0; j < ay.two; ++j) {
-      const T w = wz * (T)(j ? ay.w1 : ay.w0);
-      const T* row = coarse + Mc * ((j ? ay.c1 : ay.c0) + Mc * cz);
-      a0 += w * row[xc];
-      if (xr) a1 += w * row[xc + 1];
-    }
+  const int Mf = (Mc - 1) * F + 1;
+  const int xc = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+  if (xc >= Mc || y >= Mf) return;
+  const int ry = y & (F - 1), rz = z & (F - 1);
+  const int cy = y >> S, cz = z >> S;
+  const T wy1 = (T)ry / (T)F, wz1 = (T)rz / (T)F;  // exact: F is a power of two
+  const bool xr = xc + 1 < Mc;                       // the interval has a right end
+  const T* base = coarse + ((int64_t)cz * Mc + cy) * Mc + xc;
+  const int64_t rowY = Mc, rowZ = (int64_t)Mc * Mc;
+  // the coarse field at x = xc and xc + 1, interpolated in y and z
+  T a0 = base[0], a1 = xr ? base[1] : T(0);
+  if (ry) {
+    a0 = (T(1) - wy1) * a0 + wy1 * base[rowY];
+    if (xr) a1 = (T(1) - wy1) * a1 + wy1 * base[rowY + 1];
   }
-  T* out = fine + Mf * (y + Mf * z) + (int64_t)xc * F;
+  if (rz) {
+    T b0 = base[rowZ], b1 = xr ? base[rowZ + 1] : T(0);
+    if (ry) {
+      b0 = (T(1) - wy1) * b0 + wy1 * base[rowZ + rowY];
+      if (xr) b1 = (T(1) - wy1) * b1 + wy1 * base[rowZ + rowY + 1];
+    }
+    a0 = (T(1) - wz1) * a0 + wz1 * b0;
+    a1 = (T(1) - wz1) * a1 + wz1 * b1;
+  }
+  T* out = fine + ((int64_t)z * Mf + y) * Mf + (int64_t)xc * F;
 #pragma unroll
   for (int r = 0; r < F; ++r) {
     if (r > 0 && !xr) break;
-    const T w1 = (T)r / (T)F;  // exact: F is a power of two
+    const T w1 = (T)r / (T)F;
     const T v = r ? (T(1) - w1) * a0 + w1 * a1 : a0;
     out[r] = accumulate ? out[r] + v : v;
   }
@@ -91,11 +79,11 @@ __global__ void __launch_bounds__(256) kProlong(const T* __restrict__ coarse, in
 template <typename T>
 static its_status prolong(its_ctx* ctx, const T* coarse, int64_t Mc, T* fine, int s, int accumulate) {
   const int64_t Mf = (Mc - 1) * ((int64_t)1 << s) + 1;
-  const dim3 grid((unsigned)((Mc * Mf + 255) / 256), (unsigned)Mf);
+  const dim3 grid((unsigned)((Mc + 31) / 32), (unsigned)((Mf + 7) / 8), (unsigned)Mf), block(32, 8);
   switch (s) {
-    case 1: kProlong<T, 1><<<grid, 256, 0, ctx->stream>>>(coarse, Mc, fine, accumulate); break;
-    case 2: kProlong<T, 2><<<grid, 256, 0, ctx->stream>>>(coarse, Mc, fine, accumulate); break;
-    default: kProlong<T, 3><<<grid, 256, 0, ctx->stream>>>(coarse, Mc, fine, accumulate); break;
+    case 1: kProlong<T, 1><<<grid, block, 0, ctx->stream>>>(coarse, (int)Mc, fine, accumulate); break;
+    case 2: kProlong<T, 2><<<grid, block, 0, ctx->stream>>>(coarse, (int)Mc, fine, accumulate); break;
+    default: kProlong<T, 3><<<grid, block, 0, ctx->stream>>>(coarse, (int)Mc, fine, accumulate); break;
   }
   ITS_LAUNCHED(ctx);
   return ITS_OK;

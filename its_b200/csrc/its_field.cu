@@ -404,8 +404,9 @@ __global__ void __launch_bounds__(kScanThreads) kMcClassify(const T* __restrict_
 
 // kMcClassify for R a multiple of 256 (tiles of 8 voxels per thread): the same case bytes and
 // block sums with coalesced loads. A warp takes 256 consecutive voxels of one row, lane l the
-// voxels x0 + l + 32 j; each of the 4 corner rows is read 32 values per load, and the x+1
-// corners come from the next lane (lane 31 from lane 0 of the next round, or one extra load).
+// voxels x0 + l + 32 j; each of the 4 corner rows is read 32 values per load, compared with
+// the iso level, and the comparison of the x+1 corner comes from the next lane's bit of the
+// row's ballot (lane 31: the next round's bit 0, or one extra value).
 template <typename T>
 __global__ void __launch_bounds__(kScanThreads) kMcClassifyRows(const T* __restrict__ field, int R, double iso,
                                                                uint8_t* __restrict__ cube,
@@ -424,20 +425,27 @@ __global__ void __launch_bounds__(kScanThreads) kMcClassifyRows(const T* __restr
     for (int j = 0; j < 8; ++j) v[k][j] = (double)field[r[k] + lane + 32 * j];
     v[k][8] = (double)field[r[k] + 256];
   }
+  // each corner row's comparisons as warp ballots: the x+1 corner of lane l is bit l+1 (lane
+  // 31: bit 0 of the next round, or the extra value)
+  unsigned bal[4][8];
+  unsigned ext = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) bal[k][j] = __ballot_sync(0xffffffffu, v[k][j] < iso);
+    ext |= (unsigned)(v[k][8] < iso) << k;
+  }
   unsigned long long cnt = 0;
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
-    double n[4];
+    unsigned c[4], n[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      const double down = __shfl_down_sync(0xffffffffu, v[k][j], 1);
-      const double wrap = __shfl_sync(0xffffffffu, v[k][j < 7 ? j + 1 : 0], 0);
-      n[k] = lane < 31 ? down : (j < 7 ? wrap : v[k][8]);
+      c[k] = (bal[k][j] >> lane) & 1u;
+      n[k] = lane < 31 ? (bal[k][j] >> (lane + 1)) & 1u : (j < 7 ? bal[k][j < 7 ? j + 1 : 0] & 1u : (ext >> k) & 1u);
     }
     // corner order 0 (0,0,0) 1 (0,1,0) 2 (1,1,0) 3 (1,0,0) 4 (0,0,1) 5 (0,1,1) 6 (1,1,1) 7 (1,0,1)
-    const unsigned ci = (unsigned)(v[0][j] < iso) | (unsigned)(v[1][j] < iso) << 1 | (unsigned)(n[1] < iso) << 2 |
-                        (unsigned)(n[0] < iso) << 3 | (unsigned)(v[2][j] < iso) << 4 |
-                        (unsigned)(v[3][j] < iso) << 5 | (unsigned)(n[3] < iso) << 6 | (unsigned)(n[2] < iso) << 7;
+    const unsigned ci = c[0] | c[1] << 1 | n[1] << 2 | n[0] << 3 | c[2] << 4 | c[3] << 5 | n[3] << 6 | n[2] << 7;
     cube[s + lane + 32 * j] = (uint8_t)ci;
     cnt += cMcCase[ci] & 15ull;
   }
