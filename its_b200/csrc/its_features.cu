@@ -251,12 +251,22 @@ __global__ void __launch_bounds__(kFeatThreads) kShareFeatures(const __grid_cons
         }
       }
     }
-    // samples in the owner's 27-neighbourhood, strided over the lanes
+    // samples in the owner's 27-neighbourhood, strided over the lanes: the neighbour ids
+    // first, then their sums (independent loads in flight together), added in order
     const uint32_t o = P.vertOwner[v];
-    for (int k = sub; k < 27; k += kFeatLanes) {
-      const uint32_t t = P.nodeNb[27 * (int64_t)o + k];
+    constexpr int kPer = (27 + kFeatLanes - 1) / kFeatLanes;
+    uint32_t nb[kPer];
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+      const int k = sub + kFeatLanes * i;
+      nb[i] = k < 27 ? P.nodeNb[27 * (int64_t)o + k] : kNone;
+    }
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+      const uint32_t t = nb[i];
       if (t == kNone) continue;
       c += (double)S.cnt[t];
+#pragma unroll
       for (int a = 0; a < 3; ++a) {
         p[a] += S.sp[3 * (int64_t)t + a];
         q[a] += S.sn[3 * (int64_t)t + a];

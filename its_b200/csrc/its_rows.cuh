@@ -83,6 +83,17 @@ __device__ __forceinline__ void walkChain(const RowParams& P, int d, uint32_t X,
   }
 }
 
+// hat1r(x, b, w) and hat1r(x, b + w, w) for a coordinate x of a point in the cell [b, b + w]
+// (to rounding: the point is a corner of a node inside it). Of hat1r's four zero tests, two
+// per corner can only hold a cell width away from the cell, so only the others are made; the
+// values are hat1r's bit for bit.
+__device__ __forceinline__ void hatPair(double x, double b, double w, double wi, double h[2]) {
+  const double b1 = b + w;
+  const double e0 = b + w, e1 = b1 - w;  // hat1r's far support ends of the two corners
+  h[0] = (fabs(x - e0) < 1e-9 || x > e0) ? 0.0 : (x <= b ? 1 + divRn(x - b, w, wi) : 1 - divRn(x - b, w, wi));
+  h[1] = (fabs(x - e1) < 1e-9 || x < e1) ? 0.0 : (x <= b1 ? 1 + divRn(x - b1, w, wi) : 1 - divRn(x - b1, w, wi));
+}
+
 // visit(col, val) for the non-zero hats at (qx, qy, qz) of the 8 corners of the depth-dd
 // ancestor of the depth-d vertex c's owner, corners in x-major order. (Corner positions are
 // the cell's origin (+ w), as the reference forms them, so the cell must be the owner's
@@ -96,9 +107,10 @@ __device__ __forceinline__ void walkAncestor(const RowParams& P, const VertCoord
   const double w = P.w0 * (double)(1u << dd), wi = P.winv[dd];
   const double bx = latticePos(P.g.x, w, Xa), by = latticePos(P.g.y, w, Ya), bz = latticePos(P.g.z, w, Za);
   // the six axis factors once (the corners share them)
-  const double hxs[2] = {hat1r(qx, bx, w, wi), hat1r(qx, bx + w, w, wi)};
-  const double hys[2] = {hat1r(qy, by, w, wi), hat1r(qy, by + w, w, wi)};
-  const double hzs[2] = {hat1r(qz, bz, w, wi), hat1r(qz, bz + w, w, wi)};
+  double hxs[2], hys[2], hzs[2];
+  hatPair(qx, bx, w, wi, hxs);
+  hatPair(qy, by, w, wi, hys);
+  hatPair(qz, bz, w, wi, hzs);
 #pragma unroll
   for (int ox = 0; ox < 2; ++ox) {
     const double hx = hxs[ox];
