@@ -211,13 +211,14 @@ __global__ void __launch_bounds__(kResThreads) kResidualFine(const __grid_consta
 
 // The coarse band: 32 rows per block, lane l of every warp on row l, warp w summing the hats
 // of the ancestors at depths d+1+w, d+9+w, ... (a warp's loads stay on one depth of
-// neighbouring rows; these rows are few, so the ancestors, not the rows, fill the GPU). Warp 0
-// also takes the row's finer coincident columns; the parts are added in warp order.
+// neighbouring rows; these rows are few, so the ancestors, not the rows, fill the GPU). The
+// last warp also takes the row's finer coincident columns; the parts are added in warp order.
 constexpr int kResCoarseRows = 32;
 constexpr int kResWarps = kResThreads / 32;
 __global__ void __launch_bounds__(kResThreads) kResidualCoarse(const __grid_constant__ SegArgs<ResSeg> A,
                                                               double* __restrict__ part) {
   __shared__ double sacc[kResWarps][kResCoarseRows];
+  __shared__ double schain[kResCoarseRows];
   const int k = A.find(blockIdx.x);
   const ResSeg& s = A.seg(k);
   const int64_t j = blockIdx.x - A.pre(k);
@@ -234,6 +235,11 @@ __global__ void __launch_bounds__(kResThreads) kResidualCoarse(const __grid_cons
       for (int dd = v.d + 1 + warp; dd < P.depth; dd += kResWarps)
         walkAncestor(P, v, dd, qx, qy, qz, [&](int32_t c, double h) { acc += h * lam[c]; });
     }
+    if (warp == kResWarps - 1) {  // the last warp has the fewest ancestors: it walks the chain too
+      double chain = 0.0;
+      walkChain(P, v.d, v.X, v.Y, v.Z, [&](int32_t c) { chain += lam[c]; });
+      schain[lane] = chain;
+    }
   }
   sacc[warp][lane] = acc;
   __syncthreads();
@@ -246,10 +252,7 @@ __global__ void __launch_bounds__(kResThreads) kResidualCoarse(const __grid_cons
       for (int w = 0; w < kResWarps; ++w) t += sacc[w][lane];
       const double h = lam[r] + t;
       s.H[r] = h;
-      const VertCoord v = vertCoord(P, r);
-      double chain = 0.0;
-      walkChain(P, v.d, v.X, v.Y, v.Z, [&](int32_t c) { chain += lam[c]; });
-      const double e = s.b[r] - (chain + h);
+      const double e = s.b[r] - (schain[lane] + h);
       rr = e * e;
       bb = s.b[r] * s.b[r];
     }
