@@ -12,8 +12,8 @@
 // graph reads the inputs' memory at every replay, so new values of b (or of the network's
 // parameters) are always used. Scratch buffers of the captured sequence live in an arena the
 // plan owns (the graph holds no allocation nodes); host vectors are staged through plan-owned
-// device buffers around the replay. The residual's last kernel writes its result straight to
-// the plan's mapped pinned memory; the network's error flag is copied beside it.
+// device buffers around the replay. The residual's last kernel writes its result, and the
+// network's error flag beside it, straight to the plan's mapped pinned memory.
 #include <cstring>
 #include <vector>
 
@@ -27,7 +27,7 @@ namespace its {
 its_status learnedStart(its_ctx* ctx, its_svo* const* svos, int64_t count, its_mlp* mlp, const double* const* b,
                         const float* hn, double* const* lam);
 its_status fitResidualEnqueue(its_ctx* ctx, its_svo* const* svos, int64_t count, const double* const* b,
-                              const double* const* lam, double* relDev);
+                              const double* const* lam, double* relDev, const int* flagSrc, int* flagDst);
 its_status hostNorm(its_ctx* ctx, const float* norm, float* hn);
 const int* mlpErrFlag(its_mlp* mlp);
 
@@ -98,11 +98,12 @@ static its_status planFor(its_svo* svo, LearnedPlan** out) {
 }
 
 // Queue the learned start and the residual check of one octree (device vectors).
+// (the residual's last kernel also copies the network's error flag beside the result)
 static its_status enqueueFit(its_svo* svo, its_mlp* mlp, const double* b, const float* hn, double* lam,
                              double* relDev) {
   its_status st;
   if ((st = learnedStart(svo->ctx, &svo, 1, mlp, &b, hn, &lam)) != ITS_OK) return st;
-  return fitResidualEnqueue(svo->ctx, &svo, 1, &b, &lam, relDev);
+  return fitResidualEnqueue(svo->ctx, &svo, 1, &b, &lam, relDev, mlpErrFlag(mlp), (int*)(relDev + 1));
 }
 
 // Capture the sequence for (mlp, b, lam, norm) into p->exec.
@@ -118,8 +119,6 @@ static its_status capture(its_svo* svo, LearnedPlan* p, its_mlp* mlp, const doub
   cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
     st = enqueueFit(svo, mlp, b, hn, lam, p->relMapped);
-    if (st == ITS_OK)
-      e = cudaMemcpyAsync(p->relHost + 1, mlpErrFlag(mlp), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
     const cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &graph);
     if (e == cudaSuccess) e = e2;
   }

@@ -271,6 +271,8 @@ __global__ void __launch_bounds__(kResThreads) kResidualCoarse(const __grid_cons
 struct SlotArgs {
   const int64_t* dfirst = nullptr;
   int64_t first[kInlineSegs + 1];
+  const int* flagSrc = nullptr;  // optional: one flag copied to flagDst with the results
+  int* flagDst = nullptr;
   __device__ __forceinline__ int64_t at(int64_t m) const { return dfirst ? dfirst[m] : first[m]; }
 };
 
@@ -280,6 +282,7 @@ __global__ void __launch_bounds__(kResThreads) kResidualFinish(const double* __r
                                                                const __grid_constant__ SlotArgs F,
                                                                double* __restrict__ rel) {
   const int64_t m = blockIdx.x;
+  if (m == 0 && threadIdx.x == 0 && F.flagSrc) *F.flagDst = *F.flagSrc;
   double a = 0.0, c = 0.0;
   for (int64_t k = F.at(m) + threadIdx.x; k < F.at(m + 1); k += kResThreads) {
     a += part[2 * k];
@@ -350,7 +353,7 @@ its_status exactStart(its_ctx* ctx, its_svo* const* svos, int64_t count, const d
 // (device), each mesh's sum in a fixed order: two bands, then the sums; queued on the
 // context's stream without a host wait.
 its_status fitResidualEnqueue(its_ctx* ctx, its_svo* const* svos, int64_t count, const double* const* b,
-                              const double* const* lam, double* relDev) {
+                              const double* const* lam, double* relDev, const int* flagSrc, int* flagDst) {
   its_status st;
   int64_t total = 0;
   for (int64_t m = 0; m < count; ++m) total += svos[m]->d.numVerts;
@@ -396,6 +399,8 @@ its_status fitResidualEnqueue(its_ctx* ctx, its_svo* const* svos, int64_t count,
     if ((st = makeSegArgs(ctx, segs[band], cf[band], A[band], keep[band])) != ITS_OK) return st;
   }
   SlotArgs F;
+  F.flagSrc = flagSrc;
+  F.flagDst = flagDst;
   if (count <= kInlineSegs) {
     for (int64_t m = 0; m <= count; ++m) F.first[m] = mFirst[m];
   } else {
@@ -426,7 +431,7 @@ its_status fitResidual(its_ctx* ctx, its_svo* const* svos, int64_t count, const 
   its_status st;
   DevBuf<double> dRel;
   if ((st = dRel.alloc(ctx, count)) != ITS_OK) return st;
-  if ((st = fitResidualEnqueue(ctx, svos, count, b, lam, dRel.p)) != ITS_OK) return st;
+  if ((st = fitResidualEnqueue(ctx, svos, count, b, lam, dRel.p, nullptr, nullptr)) != ITS_OK) return st;
   ITS_CU(ctx, cudaMemcpyAsync(rel, dRel.p, count * 8, cudaMemcpyDeviceToHost, ctx->stream));
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   return ITS_OK;
