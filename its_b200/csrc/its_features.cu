@@ -15,6 +15,8 @@
 // Samples are the mesh's face centroids with unit face normals; their per-node sums are
 // formed finest depth first (a stable sort of the samples by fine node, a segmented sum in
 // sample order, then each node sums its 8 children), so the features are deterministic.
+// Features 38-45 depend on the octree and the mesh only and are computed with the octree
+// (its_svo_build); the rest, which depend on b, with every fit.
 // Features are optionally normalised, (f - mean) * scale, as the network was trained.
 #include <algorithm>
 #include <cmath>
@@ -174,13 +176,14 @@ constexpr int kFeatThreads = 128;
 constexpr int kFeatRows = kFeatThreads / kFeatLanes;  // vertices per block
 
 // Four lanes per vertex: lane 0 the coincident copies above and the scalar features, lane 1
-// the copies below, the face neighbours split over the lanes, the owner's 27-neighbourhood
-// sample sums strided over the lanes and added by a fixed shuffle tree. The block's rows go
+// the copies below, the face neighbours split over the lanes, lane 3 also the sample features
+// of the owner's 27-neighbourhood (computed with the octree, kCoincGeom). The block's rows go
 // through shared memory so that the normalised features leave in coalesced stores.
 __global__ void __launch_bounds__(kFeatThreads) kShareFeatures(const __grid_constant__ FeatParams P,
                                                                const int64_t* __restrict__ ids, int64_t count,
                                                                const double* __restrict__ b,
-                                                               const double* __restrict__ lam0, NodeStats S,
+                                                               const double* __restrict__ lam0,
+                                                               const float* __restrict__ geom,
                                                                const __grid_constant__ FeatNorm norm,
                                                                float* __restrict__ out) {
   __shared__ __align__(16) float sf[kFeatRows][kFeat];
@@ -191,7 +194,6 @@ __global__ void __launch_bounds__(kFeatThreads) kShareFeatures(const __grid_cons
   for (int k = 0; k < kFeat / kFeatLanes; ++k) f[sub * (kFeat / kFeatLanes) + k] = 0.0f;
   __syncwarp();
   const bool valid = i < count;
-  double c = 0.0, p[3] = {0, 0, 0}, q[3] = {0, 0, 0};
   int64_t v = 0;
   int d = 0;
   double w = 0.0;
@@ -251,49 +253,10 @@ __global__ void __launch_bounds__(kFeatThreads) kShareFeatures(const __grid_cons
         }
       }
     }
-    // samples in the owner's 27-neighbourhood, strided over the lanes: the neighbour ids
-    // first, then their sums (independent loads in flight together), added in order
-    const uint32_t o = P.vertOwner[v];
-    constexpr int kPer = (27 + kFeatLanes - 1) / kFeatLanes;
-    uint32_t nb[kPer];
+    // the samples around the owner (octree and mesh only): computed with the octree
+    if (sub == 3) {
 #pragma unroll
-    for (int i = 0; i < kPer; ++i) {
-      const int k = sub + kFeatLanes * i;
-      nb[i] = k < 27 ? P.nodeNb[27 * (int64_t)o + k] : kNone;
-    }
-#pragma unroll
-    for (int i = 0; i < kPer; ++i) {
-      const uint32_t t = nb[i];
-      if (t == kNone) continue;
-      c += (double)S.cnt[t];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        p[a] += S.sp[3 * (int64_t)t + a];
-        q[a] += S.sn[3 * (int64_t)t + a];
-      }
-    }
-  }
-#pragma unroll
-  for (int off = kFeatLanes / 2; off > 0; off >>= 1) {
-    c += __shfl_down_sync(0xffffffffu, c, off, kFeatLanes);
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      p[a] += __shfl_down_sync(0xffffffffu, p[a], off, kFeatLanes);
-      q[a] += __shfl_down_sync(0xffffffffu, q[a], off, kFeatLanes);
-    }
-  }
-  if (valid && sub == 0) {
-    f[38] = (float)log1p(c);
-    if (c > 0.0) {
-      const double* x = P.vertPos + 3 * v;
-      double nn = 0.0;
-      for (int a = 0; a < 3; ++a) {
-        f[39 + a] = (float)((p[a] / c - x[a]) / w);
-        const double m = q[a] / c;
-        f[42 + a] = (float)m;
-        nn += m * m;
-      }
-      f[45] = (float)(1.0 - sqrt(nn));
+      for (int k = 0; k < 8; ++k) f[38 + k] = geom[8 * i + k];
     }
   }
   __syncthreads();
@@ -362,6 +325,54 @@ its_status coincidentIds(its_ctx* ctx, const SvoDevice& d, int64_t* ids, int64_t
   return readScalar(ctx, tot.p, count);
 }
 
+// Features 38-45 of coincident vertex i (one thread each): the samples of the 27 nodes around
+// its owner, summed in neighbour order.
+__global__ void kCoincGeom(const __grid_constant__ FeatParams P, const int64_t* __restrict__ ids, int64_t count,
+                           NodeStats S, float* __restrict__ geom) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const int64_t v = ids[i];
+  const VertCoord vc = decodeVertKey(P.vertKey[v]);
+  const double w = P.w0 * (double)(1u << vc.d);
+  const uint32_t o = P.vertOwner[v];
+  double c = 0.0, p[3] = {0, 0, 0}, q[3] = {0, 0, 0};
+  for (int k = 0; k < 27; ++k) {
+    const uint32_t t = P.nodeNb[27 * (int64_t)o + k];
+    if (t == kNone) continue;
+    c += (double)S.cnt[t];
+    for (int a = 0; a < 3; ++a) {
+      p[a] += S.sp[3 * (int64_t)t + a];
+      q[a] += S.sn[3 * (int64_t)t + a];
+    }
+  }
+  float f[8] = {(float)log1p(c), 0, 0, 0, 0, 0, 0, 0};
+  if (c > 0.0) {
+    const double* x = P.vertPos + 3 * v;
+    double nn = 0.0;
+    for (int a = 0; a < 3; ++a) {
+      f[1 + a] = (float)((p[a] / c - x[a]) / w);
+      const double m = q[a] / c;
+      f[4 + a] = (float)m;
+      nn += m * m;
+    }
+    f[7] = (float)(1.0 - sqrt(nn));
+  }
+  for (int k = 0; k < 8; ++k) geom[8 * i + k] = f[k];
+}
+
+its_status coincidentGeometry(its_ctx* ctx, SvoDevice& d) {
+  its_status st;
+  if ((st = devAlloc(ctx, (void**)&d.coincGeom, std::max<int64_t>(d.numCoinc, 1) * 8 * sizeof(float))) != ITS_OK)
+    return st;
+  if (d.numCoinc > 0) {
+    NodeStats S{d.nodeSampleCnt, d.nodeSamplePos, d.nodeSampleNrm};
+    kCoincGeom<<<gridFor(d.numCoinc, 128), 128, 0, ctx->stream>>>(featParams(d), d.coincIds, d.numCoinc, S,
+                                                                  d.coincGeom);
+    ITS_LAUNCHED(ctx);
+  }
+  return ITS_OK;
+}
+
 its_status nodeSampleStats(its_ctx* ctx, SvoDevice& d, const double* V, const int32_t* F, int64_t nf) {
   its_status st;
   const int64_t nn = d.numNodes;
@@ -402,17 +413,18 @@ its_status nodeSampleStats(its_ctx* ctx, SvoDevice& d, const double* V, const in
   return ITS_OK;
 }
 
-// Features of the coincident vertices ids[0..count) (see the file comment); hostNorm (host
-// memory, may be null) the normalisation.
+// Features of the octree's coincident vertices (ids = d.coincIds, count = d.numCoinc: row i
+// is coincident vertex i) (see the file comment); hostNorm (host memory, may be null) the
+// normalisation.
 its_status shareFeatures(its_ctx* ctx, const SvoDevice& d, const double* b, const double* lam0, const int64_t* ids,
                          int64_t count, const float* hostNorm, float* out) {
   const FeatParams P = featParams(d);
-  NodeStats S{d.nodeSampleCnt, d.nodeSamplePos, d.nodeSampleNrm};
   FeatNorm norm;
   norm.on = hostNorm != nullptr;
   for (int k = 0; k < 2 * kFeat; ++k) norm.v[k] = hostNorm ? hostNorm[k] : 0.0f;
   if (count > 0) {
-    kShareFeatures<<<gridFor(count, kFeatRows), kFeatThreads, 0, ctx->stream>>>(P, ids, count, b, lam0, S, norm, out);
+    kShareFeatures<<<gridFor(count, kFeatRows), kFeatThreads, 0, ctx->stream>>>(P, ids, count, b, lam0, d.coincGeom,
+                                                                                norm, out);
     ITS_LAUNCHED(ctx);
   }
   return ITS_OK;

@@ -157,6 +157,8 @@ struct SvoDevice {
   double* nodeSampleNrm = nullptr; // 3 per node: sum of unit normals
   int64_t* coincIds = nullptr;     // vertices coincident with a coarser corner, ascending
   int64_t numCoinc = 0;
+  float* coincGeom = nullptr;      // share-network features 38-45 of each coincident vertex (the
+                                   // face samples around its owner: octree and mesh only)
   void* rowParams = nullptr;       // device copy of the octree's RowParams (its_rows.cuh)
   LatticeIndex lattice(int d) const {
     LatticeIndex L;

@@ -315,7 +315,7 @@ static void svoRelease(its_svo* s) {
   SvoDevice& d = s->d;
   void* ptrs[] = {d.voxels, d.nodeMorton, d.nodeParent, d.nodeChild0, d.nodeLeaf, d.nodeNb, d.vertLin, d.vertKey,
                   d.vertOwner, d.vertPos, d.ebits, d.erank, d.edgeKey, d.edgeOwner, d.fineOcc,
-                  d.nodeSampleCnt, d.nodeSamplePos, d.nodeSampleNrm, d.coincIds, d.rowParams};
+                  d.nodeSampleCnt, d.nodeSamplePos, d.nodeSampleNrm, d.coincIds, d.rowParams, d.coincGeom};
   for (void* p : ptrs) devFree(c, p);
   for (int i = 0; i < kMaxDepth; ++i) { devFree(c, d.vbits[i]); devFree(c, d.vrank[i]); }
   d = SvoDevice();
@@ -521,6 +521,7 @@ its_status svoBuild(its_ctx* ctx, const double* dV, int64_t nv, const int32_t* d
   // the coincident vertices (the shares of the exact start)
   if ((st = devAlloc(ctx, (void**)&d.coincIds, std::max<int64_t>(d.numVerts, 1) * 8)) != ITS_OK) return st;
   if ((st = coincidentIds(ctx, d, d.coincIds, &d.numCoinc)) != ITS_OK) return st;
+  if ((st = coincidentGeometry(ctx, d)) != ITS_OK) return st;
   // the row parameters of the matrix-free kernels, on the device for the octree's lifetime
   const RowParams hp = rowParams(d);
   if ((st = devAlloc(ctx, &d.rowParams, sizeof(RowParams))) != ITS_OK) return st;

@@ -24,4 +24,7 @@ its_status nodeSampleStats(its_ctx* ctx, SvoDevice& d, const double* dV, const i
 // The vertices coincident with a coarser corner (lattice coordinates all even below the
 // root depth), ascending, into ids (capacity numVerts); *count their number.
 its_status coincidentIds(its_ctx* ctx, const SvoDevice& d, int64_t* ids, int64_t* count);
+// Features 38-45 of the share network for every coincident vertex into d.coincGeom: they
+// depend on the octree and the mesh's face samples only (its_features.cu).
+its_status coincidentGeometry(its_ctx* ctx, SvoDevice& d);
 }  // namespace its
