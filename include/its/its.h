@@ -337,8 +337,9 @@ its_status its_learned_start_batch(its_svo* const* svos, int64_t count, its_mlp*
    (src/ThinShells.cpp:608-653): its_learned_start, then ||b - A lambda|| / ||b|| (as
    its_fit_residual), then, when that exceeds tol, its_lscg_solve (FP64, ITS_STOP_RESIDUAL)
    from the learned start. The start and the check run as a CUDA graph captured on the first
-   call and replayed while the network, norm, the context's stream and the device addresses of
-   b and lambda stay the same (host vectors go through buffers of the octree's own, so their
+   call and replayed while the network (the same its_mlp, not another made since), norm, the
+   context's stream and the device addresses of b and lambda stay the same (host vectors go
+   through buffers of the octree's own, so their
    addresses always match); the graph reads b and the network's parameters afresh every time.
    Complete on return. report (may be NULL): iterations = LSCG iterations after the start (0
    when the start passed), converged, rel_residual, ms = device time of the call. */

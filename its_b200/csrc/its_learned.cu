@@ -30,6 +30,7 @@ its_status fitResidualEnqueue(its_ctx* ctx, its_svo* const* svos, int64_t count,
                               const double* const* lam, double* relDev, const int* flagSrc, int* flagDst);
 its_status hostNorm(its_ctx* ctx, const float* norm, float* hn);
 const int* mlpErrFlag(its_mlp* mlp);
+uint64_t mlpUid(const its_mlp* mlp);
 
 constexpr int kNormValues = 130;
 
@@ -37,6 +38,7 @@ struct LearnedPlan {
   its_ctx* ctx = nullptr;
   // what the graph was captured for
   its_mlp* mlp = nullptr;
+  uint64_t mlpUid = 0;  // the network's identity (its address may be reused after a free)
   const double* b = nullptr;
   double* lam = nullptr;
   cudaStream_t stream = nullptr;
@@ -135,6 +137,7 @@ static its_status capture(its_svo* svo, LearnedPlan* p, its_mlp* mlp, const doub
     return cudaFail(ctx, e, "learned fit: graph capture");
   }
   p->mlp = mlp;
+  p->mlpUid = mlpUid(mlp);
   p->b = b;
   p->lam = lam;
   p->stream = ctx->stream;
@@ -173,7 +176,8 @@ its_status its_learned_fit(its_svo* svo, its_mlp* mlp, const double* b, const fl
   const double* bd = bHost ? p->bStage : b;
   double* ld = lamHost ? p->lamStage : lambda;
   if (bHost) ITS_CU(ctx, cudaMemcpyAsync(p->bStage, b, n * 8, cudaMemcpyHostToDevice, ctx->stream));
-  if (!p->exec || p->mlp != mlp || p->b != bd || p->lam != ld || p->stream != ctx->stream ||
+  if (!p->exec || p->mlp != mlp || p->mlpUid != mlpUid(mlp) || p->b != bd || p->lam != ld ||
+      p->stream != ctx->stream ||
       std::memcmp(p->norm, hn, sizeof(hn)) != 0)
     if ((st = capture(svo, p, mlp, bd, hn, ld)) != ITS_OK) return st;
   ITS_CU(ctx, cudaGraphLaunch(p->exec, ctx->stream));

@@ -13,6 +13,7 @@
 //
 // Parameters (flat FP32): W1[128x64] b1[128] W2[128x128] b2[128] W3[128x128] b3[128]
 // w4[128] b4[1] (W[o][i]: output o, input i).
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -229,8 +230,11 @@ struct EpiPartial {
 // straight back into shared memory as the next layer's A operand -- nothing but the features
 // and the outputs touches global memory. The MMA sequence and the epilogue arithmetic are
 // those of the layer-by-layer kernels, so the outputs are identical.
-constexpr int kFusedSlots = 2;                   // 128-row tiles in flight per CTA
-constexpr int kFusedThreads = 256 * kFusedSlots;  // two warp groups per tile, one per half of the columns
+constexpr int kFusedSlots = 2;                                 // 128-row tiles in flight per CTA
+constexpr int kFusedGroups = 4;                                // warp groups per tile, one per quarter of the columns
+constexpr int kSlotThreads = 128 * kFusedGroups;
+constexpr int kFusedThreads = kSlotThreads * kFusedSlots;
+constexpr int kGroupCols = 128 / kFusedGroups;
 constexpr int kFusedSmem = 16384 /*W1*/ + 32768 /*W2*/ + 32768 /*W3*/ + kFusedSlots * (16384 /*X*/ + 32768 /*H*/) +
                            64 + 1024;
 
@@ -243,14 +247,16 @@ __device__ __forceinline__ void loadWeightTile(uint8_t* dst, const bf16* __restr
 }
 
 // Barrier of one tile slot (256 threads), ids 1 and 2 (0 is __syncthreads').
-__device__ __forceinline__ void slotSync(int s) { asm volatile("bar.sync %0, 256;" ::"r"(1 + s) : "memory"); }
+__device__ __forceinline__ void slotSync(int s) {
+  asm volatile("bar.sync %0, %1;" ::"r"(1 + s), "n"(kSlotThreads) : "memory");
+}
 
 // Share-network inference: persistent, one CTA per SM, two 128-row tiles in flight. A tile's
-// 256 threads load its features, one of them issues each layer's MMAs, and the two warp groups
-// run the epilogue of one half of the 128 columns each (thread = row, the TMEM lane of its
-// warp). The output unit sums the columns in order: the second half's activations (BF16, as
-// the sum uses them) go through shared memory to the first half's threads, so the result is
-// the layer-by-layer kernels' bit for bit.
+// 512 threads load its features, one of them issues each layer's MMAs, and the four warp
+// groups run the epilogue of a quarter of the 128 columns each (thread = row, the TMEM lane of
+// its warp). The output unit sums the columns in order: the later quarters' activations (BF16,
+// as the sum uses them) go through shared memory to the first group's threads, so the result
+// is the layer-by-layer kernels' bit for bit.
 __global__ void __launch_bounds__(kFusedThreads, 1)
     kMlpForwardFused(const float* __restrict__ X, int64_t n, const bf16* __restrict__ W1, const bf16* __restrict__ W2,
                      const bf16* __restrict__ W3, const float* __restrict__ P, const float* __restrict__ w4r,
@@ -261,10 +267,11 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   uint8_t* sW1 = smem;
   uint8_t* sW2 = sW1 + 16384;
   uint8_t* sW3 = sW2 + 32768;
-  const int tid = threadIdx.x, s = tid >> 8, st = tid & 255, half = st >> 7, row = tid & 127, warp = tid >> 5;
+  const int tid = threadIdx.x, s = tid / kSlotThreads, st = tid % kSlotThreads, grp = st >> 7, row = tid & 127,
+            warp = tid >> 5;
   uint8_t* sX = sW3 + 32768 + s * (16384 + 32768);
   uint8_t* sH = sX + 16384;
-  constexpr int kOutStride = 144;  // bytes per row of the second half's output activations in sH
+  constexpr int kOutStride = 2 * (128 - kGroupCols) + 16;  // bytes per row of the later groups' output activations
   uint64_t* mbar = (uint64_t*)(sW3 + 32768 + kFusedSlots * (16384 + 32768));
   uint32_t* tslot = (uint32_t*)(mbar + kFusedSlots);
   if (warp == 0) tmemAlloc(smemAddr(tslot), 128 * kFusedSlots);
@@ -292,7 +299,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
     // features -> BF16: the tile's 128 rows x 256 B read in coalesced 32-byte pieces, each one
     // 16-byte chunk of a row in the swizzled A tile
 #pragma unroll 2
-    for (int p = st; p < 128 * 8; p += 256) {
+    for (int p = st; p < 128 * 8; p += kSlotThreads) {
       const int pr = p >> 3, pc = p & 7;
       const int64_t mr = t * 128 + pr;
       float4 f0 = make_float4(0.f, 0.f, 0.f, 0.f), f1 = f0;
@@ -336,10 +343,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
       ok = mbarWait(bar, phase) && ok;
       phase ^= 1u;
       fenceAfter();
-      // epilogue of this half's 64 columns, 16 at a time (a rolled loop keeps the code small)
+      // epilogue of this group's columns, 16 at a time (a rolled loop keeps the code small)
       const float* bias = layer == 0 ? b1 : (layer == 1 ? b2 : b3);
 #pragma unroll 1
-      for (int n0 = 64 * half; n0 < 64 * half + 64; n0 += 16) {
+      for (int n0 = kGroupCols * grp; n0 < kGroupCols * grp + kGroupCols; n0 += 16) {
         float v[16];
         tmemLoad16(tmem + lane + (uint32_t)n0, v);
         if (layer < 2) {  // hidden layer: the next layer's A operand
@@ -351,25 +358,25 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
             const int c = (n0 >> 3) + h;
             *(uint4*)(sH + (c >> 3) * 16384 + swizzledChunk(row, c & 7)) = *(const uint4*)q;
           }
-        } else if (half == 0) {  // output unit, columns in order
+        } else if (grp == 0) {  // output unit, columns in order
 #pragma unroll
           for (int j = 0; j < 16; ++j)
             o += __bfloat162float(__float2bfloat16_rn(geluF(v[j] + bias[n0 + j]))) * w4r[n0 + j];
-        } else {  // the second half's activations for the first half's sum (layer 2 has read sH)
+        } else {  // the later groups' activations for the first group's sum (layer 2 has read sH)
           __align__(16) bf16 q[16];
 #pragma unroll
           for (int j = 0; j < 16; ++j) q[j] = __float2bfloat16_rn(geluF(v[j] + bias[n0 + j]));
-          uint4* dst = (uint4*)(sH + row * kOutStride + (n0 - 64) * 2);
+          uint4* dst = (uint4*)(sH + row * kOutStride + (n0 - kGroupCols) * 2);
           dst[0] = ((const uint4*)q)[0];
           dst[1] = ((const uint4*)q)[1];
         }
       }
     }
     slotSync(s);
-    if (half == 0) {
+    if (grp == 0) {
       const bf16* a = (const bf16*)(sH + row * kOutStride);
 #pragma unroll 8
-      for (int j = 0; j < 64; ++j) o += __bfloat162float(a[j]) * w4r[64 + j];
+      for (int j = 0; j < 128 - kGroupCols; ++j) o += __bfloat162float(a[j]) * w4r[kGroupCols + j];
       if (m < n && ok) out[m] = o + P[kOffB4];
     }
     fenceBefore();
@@ -541,6 +548,7 @@ using namespace its;
 
 struct its_mlp {
   its_ctx* ctx = nullptr;
+  uint64_t uid = 0;  // distinct for every network made (a later one may reuse a freed address)
   int64_t cap = 0;  // rows per batch
   float* P = nullptr;
   float* Mo = nullptr;
@@ -646,6 +654,7 @@ its_status mlpInfer(its_mlp* h, const float* X, int64_t n, float* out) {
 its_status mlpCheck(its_mlp* h) { return checkErr(h); }
 // The network's (sticky) error flag in device memory, for callers that read it with their own copy.
 const int* mlpErrFlag(its_mlp* h) { return h->err; }
+uint64_t mlpUid(const its_mlp* h) { return h->uid; }
 
 }  // namespace its
 
@@ -656,6 +665,8 @@ its_status its_mlp_create(its_ctx* ctx, int64_t batch, its_mlp** out) {
   ITS_CU(ctx, cudaSetDevice(ctx->device));
   its_mlp* h = new its_mlp;
   h->ctx = ctx;
+  static std::atomic<uint64_t> made{0};
+  h->uid = ++made;
   h->cap = batch;
   const int64_t B = batch;
   its_status s = ITS_OK;

@@ -128,3 +128,8 @@ def test_learned_fit_graph_equals_start_and_check(ctx):
     x, rep = learned_fit(s, net, b, norm, 0.1 * rep["rel_residual"])
     assert rep["iterations"] > 0 and np.isfinite(rep["rel_residual"])
     net.close()
+    # another network (perhaps at the freed one's address): captured anew
+    net2 = ShareNet(ctx, batch=4096, params=omlp.init_params(9) * np.float32(0.1))
+    lam3, _ = learned_fit(s, net2, b, norm, 1e-6)
+    assert np.array_equal(lam3, learned_start_batch([s], net2, [b], norm)[0])
+    net2.close()
