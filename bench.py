@@ -449,7 +449,10 @@ def run_ours(args):
                       "rel_residual": rep_box["mixed"]["rel_residual"]},
             "learned_breakdown_ms": {"features": round(t_features, 4), "network": round(t_net, 4),
                                      "exact_start": round(t_start, 4), "residual": round(t_resid, 4),
-                                     "rows": int(feats.shape[0])},
+                                     "rows": int(feats.shape[0]),
+                                     "note": "each part called alone through its own C-ABI entry (host staging and "
+                                             "a synchronisation included); inside its_learned_fit they run back to "
+                                             "back as one captured graph"},
             "field_error": field,
             "e2e": {"value": round(e2e_ms, 4), "unit": "ms", "h2d_bytes_per_step": 8 * n,
                     "d2h_bytes_per_step": 8 * n},
