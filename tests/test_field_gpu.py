@@ -10,6 +10,7 @@ import numpy as np
 import pytest
 
 import oracle
+from cascade_np import cascade_numpy as _cascade_numpy
 from conftest import prepared_mesh
 
 
@@ -234,33 +235,6 @@ def test_point_value_gradient_matches_oracle(ctx):
         ok = (mp == 0) & (mm == 0)
         fd = (fp - fm) / (2 * h)
         assert np.median(np.abs(fd[ok] - g[inside][ok, a])) <= 1e-5 * np.abs(g[inside]).max()
-
-
-def _cascade_numpy(pos, lam, depth_counts, o, unit, res, f):
-    """The prolongation cascade restated in numpy (hats on the exact lattice points)."""
-    D = len(depth_counts)
-    depth = np.repeat(np.arange(D), depth_counts)
-    acc = None
-    for d in range(D - 1, -1, -1):
-        M = (res >> d) + 1
-        A = np.zeros((M, M, M))
-        sel = depth == d
-        X = np.rint((pos[sel] - o) / (unit * 2 ** d)).astype(int)
-        A[X[:, 0], X[:, 1], X[:, 2]] = lam[sel]
-        acc = A if acc is None else A + _prolong(acc, 2)
-    return acc if f == 1 else _prolong(acc, f)
-
-
-def _prolong(C, f):
-    Mc = C.shape[0]
-    idx = np.arange((Mc - 1) * f + 1)
-    c0, r = idx // f, idx % f
-    c1 = np.minimum(c0 + 1, Mc - 1)
-    w1 = r / f
-    w0 = 1 - w1
-    X = w0[:, None, None] * C[c0] + w1[:, None, None] * C[c1]
-    Y = w0[None, :, None] * X[:, c0] + w1[None, :, None] * X[:, c1]
-    return w0[None, None, :] * Y[:, :, c0] + w1[None, None, :] * Y[:, :, c1]
 
 
 @pytest.mark.gpu
