@@ -197,12 +197,14 @@ its_status its_lscg_solve_batch(its_op* const* ops, int64_t count, const double*
    (which starts Eigen's CGLS from zero, src/ThinShells.cpp:615-617). Vectors may be host or
    device memory. */
 its_status its_exact_start(its_svo* svo, const double* b, const double* shares, double* lambda);
-/* The same for count octrees of one context (one launch per depth for all of them); shares
+/* The same for count octrees of one context (one or two launches for all of them); shares
    may be NULL or hold NULL entries. */
 its_status its_exact_start_batch(its_svo* const* svos, int64_t count, const double* const* b,
                                  const double* const* shares, double* const* lambda);
-/* ||b - A lambda|| / ||b|| without an assembled operator (rows generated from the octree,
-   summed in a fixed order). */
+/* ||b - A lambda|| / ||b|| without an assembled operator: rows above the finest depth summed
+   as A has them (generated from the octree), finest rows through their parent cell's
+   trilinear interpolant of the coarser field -- the same A lambda, to rounding -- every sum in
+   a fixed order. */
 its_status its_fit_residual(its_svo* svo, const double* b, const double* lambda, double* rel_residual);
 its_status its_fit_residual_batch(its_svo* const* svos, int64_t count, const double* const* b,
                                   const double* const* lambda, double* rel_residual);
