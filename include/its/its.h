@@ -341,8 +341,9 @@ its_status its_learned_start_batch(its_svo* const* svos, int64_t count, its_mlp*
    from the learned start. The start and the check run as a CUDA graph captured on the first
    call and replayed while the network (the same its_mlp, not another made since), norm, the
    context's stream and the device addresses of b and lambda stay the same (host vectors go
-   through buffers of the octree's own, so their
-   addresses always match); the graph reads b and the network's parameters afresh every time.
+   through buffers of the octree's own; page-locked ones are copied by the graph itself, lambda
+   while the residual runs, so their addresses are part of what must stay the same); the graph
+   reads b and the network's parameters afresh every time.
    Complete on return. report (may be NULL): iterations = LSCG iterations after the start (0
    when the start passed), converged, rel_residual, ms = device time of the call. */
 its_status its_learned_fit(its_svo* svo, its_mlp* mlp, const double* b, const float* norm, double tol,

@@ -110,6 +110,17 @@ inline bool isDevicePtr(const void* p) {
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+// True when p is page-locked host memory the GPU can copy from and to asynchronously.
+inline bool isPinnedHostPtr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
 // A read-only argument on the device: the caller's pointer if it already is device
 // memory, else a staged copy.
 template <typename T>

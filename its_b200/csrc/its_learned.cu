@@ -41,6 +41,8 @@ struct LearnedPlan {
   uint64_t mlpUid = 0;  // the network's identity (its address may be reused after a free)
   const double* b = nullptr;
   double* lam = nullptr;
+  const double* bHost = nullptr;  // pinned host vectors copied inside the graph (or null)
+  double* lamHost = nullptr;
   cudaStream_t stream = nullptr;
   float norm[kNormValues];
   cudaGraphExec_t exec = nullptr;
@@ -52,6 +54,8 @@ struct LearnedPlan {
                               // through the mapped address), then the network's error flag
   double* relMapped = nullptr;  // relHost's device address
   cudaEvent_t t0 = nullptr, t1 = nullptr;
+  cudaStream_t side = nullptr;  // the copy of lambda to pinned host memory, beside the residual
+  cudaEvent_t fork = nullptr, join = nullptr;
   double* bStage = nullptr;   // device copies of host vectors
   double* lamStage = nullptr;
 };
@@ -67,6 +71,9 @@ void destroyPlan(LearnedPlan* p) {
   dropGraph(p);
   if (p->t0) cudaEventDestroy(p->t0);
   if (p->t1) cudaEventDestroy(p->t1);
+  if (p->fork) cudaEventDestroy(p->fork);
+  if (p->join) cudaEventDestroy(p->join);
+  if (p->side) cudaStreamDestroy(p->side);
   cudaFree(p->arena);
   cudaFree(p->bStage);
   cudaFree(p->lamStage);
@@ -88,6 +95,9 @@ static its_status planFor(its_svo* svo, LearnedPlan** out) {
     if (e == cudaSuccess) e = cudaHostGetDevicePointer(&p->relMapped, p->relHost, 0);
     if (e == cudaSuccess) e = cudaEventCreate(&p->t0);
     if (e == cudaSuccess) e = cudaEventCreate(&p->t1);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
       cudaGetLastError();
       destroyPlan(p);
@@ -99,17 +109,33 @@ static its_status planFor(its_svo* svo, LearnedPlan** out) {
   return ITS_OK;
 }
 
-// Queue the learned start and the residual check of one octree (device vectors).
-// (the residual's last kernel also copies the network's error flag beside the result)
-static its_status enqueueFit(its_svo* svo, its_mlp* mlp, const double* b, const float* hn, double* lam,
-                             double* relDev) {
+// Queue the learned start and the residual check of one octree (device vectors), with the
+// copies of pinned host vectors when given: b in first, lambda out on the side stream while
+// the residual runs (the residual's last kernel also copies the network's error flag beside
+// its result).
+static its_status enqueueFit(its_svo* svo, LearnedPlan* p, its_mlp* mlp, const double* b, const float* hn, double* lam,
+                             const double* bHost, double* lamHost) {
+  its_ctx* ctx = svo->ctx;
+  const int64_t n = svo->d.numVerts;
   its_status st;
-  if ((st = learnedStart(svo->ctx, &svo, 1, mlp, &b, hn, &lam)) != ITS_OK) return st;
-  return fitResidualEnqueue(svo->ctx, &svo, 1, &b, &lam, relDev, mlpErrFlag(mlp), (int*)(relDev + 1));
+  if (bHost) ITS_CU(ctx, cudaMemcpyAsync(const_cast<double*>(b), bHost, n * 8, cudaMemcpyHostToDevice, ctx->stream));
+  if ((st = learnedStart(ctx, &svo, 1, mlp, &b, hn, &lam)) != ITS_OK) return st;
+  if (lamHost) {
+    ITS_CU(ctx, cudaEventRecord(p->fork, ctx->stream));
+    ITS_CU(ctx, cudaStreamWaitEvent(p->side, p->fork, 0));
+    ITS_CU(ctx, cudaMemcpyAsync(lamHost, lam, n * 8, cudaMemcpyDeviceToHost, p->side));
+    ITS_CU(ctx, cudaEventRecord(p->join, p->side));
+  }
+  if ((st = fitResidualEnqueue(ctx, &svo, 1, &b, &lam, p->relMapped, mlpErrFlag(mlp), (int*)(p->relMapped + 1))) !=
+      ITS_OK)
+    return st;
+  if (lamHost) ITS_CU(ctx, cudaStreamWaitEvent(ctx->stream, p->join, 0));
+  return ITS_OK;
 }
 
-// Capture the sequence for (mlp, b, lam, norm) into p->exec.
-static its_status capture(its_svo* svo, LearnedPlan* p, its_mlp* mlp, const double* b, const float* hn, double* lam) {
+// Capture the sequence for (mlp, b, lam, norm, pinned host vectors) into p->exec.
+static its_status capture(its_svo* svo, LearnedPlan* p, its_mlp* mlp, const double* b, const float* hn, double* lam,
+                          const double* bHost, double* lamHost) {
   its_ctx* ctx = svo->ctx;
   dropGraph(p);
   const int64_t launches0 = ctx->launches;
@@ -120,7 +146,7 @@ static its_status capture(its_svo* svo, LearnedPlan* p, its_mlp* mlp, const doub
   its_status st = ITS_OK;
   cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    st = enqueueFit(svo, mlp, b, hn, lam, p->relMapped);
+    st = enqueueFit(svo, p, mlp, b, hn, lam, bHost, lamHost);
     const cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &graph);
     if (e == cudaSuccess) e = e2;
   }
@@ -140,6 +166,8 @@ static its_status capture(its_svo* svo, LearnedPlan* p, its_mlp* mlp, const doub
   p->mlpUid = mlpUid(mlp);
   p->b = b;
   p->lam = lam;
+  p->bHost = bHost;
+  p->lamHost = lamHost;
   p->stream = ctx->stream;
   std::memcpy(p->norm, hn, sizeof(p->norm));
   return ITS_OK;
@@ -175,11 +203,14 @@ its_status its_learned_fit(its_svo* svo, its_mlp* mlp, const double* b, const fl
   }
   const double* bd = bHost ? p->bStage : b;
   double* ld = lamHost ? p->lamStage : lambda;
-  if (bHost) ITS_CU(ctx, cudaMemcpyAsync(p->bStage, b, n * 8, cudaMemcpyHostToDevice, ctx->stream));
-  if (!p->exec || p->mlp != mlp || p->mlpUid != mlpUid(mlp) || p->b != bd || p->lam != ld ||
-      p->stream != ctx->stream ||
-      std::memcmp(p->norm, hn, sizeof(hn)) != 0)
-    if ((st = capture(svo, p, mlp, bd, hn, ld)) != ITS_OK) return st;
+  // page-locked host vectors are copied by the graph itself (lambda beside the residual);
+  // pageable ones around it
+  const double* bPin = bHost && isPinnedHostPtr(b) ? b : nullptr;
+  double* lamPin = lamHost && isPinnedHostPtr(lambda) ? lambda : nullptr;
+  if (bHost && !bPin) ITS_CU(ctx, cudaMemcpyAsync(p->bStage, b, n * 8, cudaMemcpyHostToDevice, ctx->stream));
+  if (!p->exec || p->mlp != mlp || p->mlpUid != mlpUid(mlp) || p->b != bd || p->lam != ld || p->bHost != bPin ||
+      p->lamHost != lamPin || p->stream != ctx->stream || std::memcmp(p->norm, hn, sizeof(hn)) != 0)
+    if ((st = capture(svo, p, mlp, bd, hn, ld, bPin, lamPin)) != ITS_OK) return st;
   ITS_CU(ctx, cudaGraphLaunch(p->exec, ctx->stream));
   ctx->launches += p->launches;
   if (report) ITS_CU(ctx, cudaEventRecord(p->t1, ctx->stream));
@@ -190,7 +221,8 @@ its_status its_learned_fit(its_svo* svo, its_mlp* mlp, const double* b, const fl
   double rel = *p->relHost;
   int64_t iters = 0;
   int converged = rel <= tol;
-  if (!converged) {  // the plain FP64 LSCG from the learned start
+  const bool fellBack = !converged;
+  if (fellBack) {  // the plain FP64 LSCG from the learned start
     its_op* op = nullptr;
     if ((st = its_operator_build(svo, 0, &op)) != ITS_OK) return st;
     its_solve_opts o;
@@ -207,7 +239,7 @@ its_status its_learned_fit(its_svo* svo, its_mlp* mlp, const double* b, const fl
     converged = r.converged;
     if (report) ITS_CU(ctx, cudaEventRecord(p->t1, ctx->stream));
   }
-  if (lamHost) {
+  if (lamHost && (!lamPin || fellBack)) {  // not copied by the graph, or changed since
     ITS_CU(ctx, cudaMemcpyAsync(lambda, ld, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
     if (report) ITS_CU(ctx, cudaEventRecord(p->t1, ctx->stream));
   }

@@ -121,6 +121,12 @@ def test_learned_fit_graph_equals_start_and_check(ctx):
     assert np.array_equal(lam_dev.cpu().numpy(), learned_start_batch([s], net, [0.5 * b], norm)[0])
     lam_host, rep = learned_fit(s, net, b, norm, 1e-6)  # host vectors
     assert np.array_equal(lam_host, ref) and rep["iterations"] == 0
+    b_pin = torch.from_numpy(b).pin_memory()  # page-locked host vectors: copied by the graph
+    lam_pin = torch.zeros(s.num_verts, dtype=torch.float64).pin_memory()
+    for k in range(2):
+        lam_pin.zero_()
+        learned_fit(s, net, b_pin.numpy(), norm, 1e-6, out=lam_pin.numpy())
+        assert np.array_equal(lam_pin.numpy(), ref)
     norm2 = norm.copy()
     norm2[128] += 0.001  # another normalisation: another graph
     lam2, _ = learned_fit(s, net, b, norm2, 1e-6)
