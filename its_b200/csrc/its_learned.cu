@@ -2,7 +2,7 @@
 //
 // ThinShells::creatShell (ThinShells.cpp:608-653) assembles the operator and runs Eigen's
 // LSCG from zero. Here the fit is the learned start (zero-share start, features, share
-// network, exact start with the predicted shares), judged by the matrix-free residual
+// network, exact start with the predicted shares), checked by the matrix-free residual
 // ||b - A lambda|| / ||b||; when that misses tol, the plain FP64 LSCG continues from it.
 //
 // The start and the check are a fixed sequence of about a dozen short launches per octree,
