@@ -282,11 +282,13 @@ its_status its_marching_cubes_f32(its_ctx* ctx, const float* field, int res, con
                                   const double width[3], double iso, uint8_t* cube_index, double* tri_verts,
                                   int64_t capacity, int64_t* num_verts);
 /* No counterpart in the reference. The same results as its_marching_cubes for callers that
-   cannot allocate device memory while they run (work replayed in a caller-captured CUDA
-   graph, a fixed memory budget): no cudaMalloc/cudaFree, the scan scratch is a fixed 64 KiB
-   file-scope device array. field, cube_index and tri_verts must be device memory; res <= 256
-   (ITS_ERR_INVALID beyond). Calls on one device share the array (overlapping calls race) and
-   the first call on a device looks up its address: make it before any stream capture. */
+   cannot let the library allocate device memory (an application that holds the GPU's memory in
+   its own fixed budget, a frame loop that cudaMalloc's implicit synchronisation would stall):
+   no cudaMalloc/cudaFree, the scan scratch is a fixed 64 KiB file-scope device array.
+   field, cube_index and tri_verts must be device memory of the context's GPU; res <= 256
+   (ITS_ERR_INVALID beyond). Calls on one device share the array (overlapping calls race); the
+   call waits on its stream for num_verts. The first call on a device looks up the array's
+   address and keeps it: cudaDeviceReset of that device afterwards is not supported. */
 its_status its_marching_cubes_noalloc(its_ctx* ctx, const double* field, int res, const double origin[3],
                                       const double width[3], double iso, uint8_t* cube_index, double* tri_verts,
                                       int64_t capacity, int64_t* num_verts);

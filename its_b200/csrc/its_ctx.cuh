@@ -99,15 +99,25 @@ struct DevBuf {
   T* release() { T* q = p; p = nullptr; n = 0; return q; }
 };
 
-// True when p is device (or managed) memory of some GPU.
-inline bool isDevicePtr(const void* p) {
-  if (!p) return false;
+// Where an argument lives, seen from the context's device: its own device memory (or managed
+// memory, which every GPU can reach), host memory, or device memory of another GPU -- which a
+// kernel of this device may not be able to read, so callers reject it.
+enum class MemKind { Host, Device, OtherDevice };
+inline MemKind memKind(const void* p, int device) {
+  if (!p) return MemKind::Host;
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
-    return false;
+    return MemKind::Host;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (a.type == cudaMemoryTypeManaged) return MemKind::Device;
+  if (a.type == cudaMemoryTypeDevice) return a.device == device ? MemKind::Device : MemKind::OtherDevice;
+  return MemKind::Host;
+}
+// True when p is device (or managed) memory the context's device can use directly.
+inline bool isDevicePtr(const its_ctx* ctx, const void* p) { return memKind(p, ctx->device) == MemKind::Device; }
+inline its_status otherDeviceError(its_ctx* ctx) {
+  return setError(ctx, ITS_ERR_INVALID, "an argument is device memory of another GPU than the context's");
 }
 
 // True when p is page-locked host memory the GPU can copy from and to asynchronously.
@@ -129,7 +139,9 @@ struct InArg {
   DevBuf<T> tmp;
   its_status stage(its_ctx* ctx, const T* src, size_t count) {
     if (!src || count == 0) { d = nullptr; return ITS_OK; }
-    if (isDevicePtr(src)) { d = src; return ITS_OK; }
+    const MemKind k = memKind(src, ctx->device);
+    if (k == MemKind::OtherDevice) return otherDeviceError(ctx);
+    if (k == MemKind::Device) { d = src; return ITS_OK; }
     its_status s = tmp.alloc(ctx, count);
     if (s != ITS_OK) return s;
     ITS_CU(ctx, cudaMemcpyAsync(tmp.p, src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
@@ -148,7 +160,9 @@ struct OutArg {
     count = n;
     host = nullptr;
     if (!dst || n == 0) { d = nullptr; return ITS_OK; }
-    if (isDevicePtr(dst)) { d = dst; return ITS_OK; }
+    const MemKind k = memKind(dst, ctx->device);
+    if (k == MemKind::OtherDevice) return otherDeviceError(ctx);
+    if (k == MemKind::Device) { d = dst; return ITS_OK; }
     its_status s = tmp.alloc(ctx, n);
     if (s != ITS_OK) return s;
     d = tmp.p;

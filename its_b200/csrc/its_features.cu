@@ -458,7 +458,9 @@ namespace its {
 
 // The 130 normalisation values in host memory (norm may be host or device memory).
 its_status hostNorm(its_ctx* ctx, const float* norm, float* hn) {
-  if (isDevicePtr(norm)) {
+  const MemKind k = memKind(norm, ctx->device);
+  if (k == MemKind::OtherDevice) return otherDeviceError(ctx);
+  if (k == MemKind::Device) {
     ITS_CU(ctx, cudaMemcpyAsync(hn, norm, (2 * kFeat + 2) * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
     ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   } else {
@@ -525,7 +527,8 @@ its_status its_share_features(its_svo* svo, const double* b, const float* norm, 
   InArg<double> db;
   if ((st = db.stage(ctx, b, n)) != ITS_OK) return st;
   float hn[2 * kFeat];
-  if (norm && isDevicePtr(norm)) {
+  if (norm && memKind(norm, ctx->device) == MemKind::OtherDevice) return otherDeviceError(ctx);
+  if (norm && isDevicePtr(ctx, norm)) {
     ITS_CU(ctx, cudaMemcpyAsync(hn, norm, sizeof(hn), cudaMemcpyDeviceToHost, ctx->stream));
     ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   } else if (norm) {

@@ -195,7 +195,9 @@ its_status its_learned_fit(its_svo* svo, its_mlp* mlp, const double* b, const fl
   if ((st = hostNorm(ctx, norm, hn)) != ITS_OK) return st;
   const int64_t n = svo->d.numVerts;
   // device addresses of the vectors: the caller's, or the plan's copies of host vectors
-  const bool bHost = !isDevicePtr(b), lamHost = !isDevicePtr(lambda);
+  if (memKind(b, ctx->device) == MemKind::OtherDevice || memKind(lambda, ctx->device) == MemKind::OtherDevice)
+    return otherDeviceError(ctx);
+  const bool bHost = !isDevicePtr(ctx, b), lamHost = !isDevicePtr(ctx, lambda);
   if ((bHost && !p->bStage && cudaMalloc(&p->bStage, std::max<int64_t>(n, 1) * 8) != cudaSuccess) ||
       (lamHost && !p->lamStage && cudaMalloc(&p->lamStage, std::max<int64_t>(n, 1) * 8) != cudaSuccess)) {
     cudaGetLastError();

@@ -1,21 +1,27 @@
 // its_marching_cubes_noalloc: marching cubes that allocates no device memory.
 //
-// Some callers cannot call cudaMalloc while they run: code replayed inside a CUDA graph that
-// the caller captured around its own work, a renderer's frame loop that runs under a fixed
-// memory budget, or a host that must not grow the device heap after start-up. For them this
-// entry point computes the same case indices and triangle soup as its_marching_cubes, but
-// its scan scratch (one block sum per 2,048 voxels plus the grand total) lives in a fixed
-// file-scope device array instead of being allocated per call.
+// Some callers of this library cannot let it call cudaMalloc: a host application that
+// reserves the GPU's memory for its own allocator at start-up and runs every later frame
+// inside that fixed budget (an allocation there can fail, or take memory the application has
+// promised elsewhere), and a frame loop that must not stall, since cudaMalloc and cudaFree can
+// synchronise the device. For them this entry point computes the same case indices and
+// triangle soup as its_marching_cubes, but its scan scratch (one block sum per 2,048 voxels
+// plus the grand total) lives in a fixed file-scope device array instead of being allocated
+// per call.
 //
 // Limits and rules:
 //   * res <= 256 (16,777,216 voxels): the array holds 8,193 64-bit words (64 KiB) and every
 //     GPU that loads libits keeps it until the process exits;
-//   * field, cube_index and tri_verts must already be device memory (a host pointer would
-//     need a staging allocation) -- they are rejected with ITS_ERR_INVALID otherwise;
-//   * every call on a device shares the one array, which keeps the last call's contents;
-//     calls that overlap on the GPU (two streams, two host threads) race on it;
+//   * field, cube_index and tri_verts must already be device memory of the context's GPU (a
+//     host pointer would need a staging allocation) -- anything else is rejected with
+//     ITS_ERR_INVALID;
+//   * every call on a device shares the one array, which keeps the last call's contents (each
+//     call rewrites every word it reads); calls that overlap on the GPU (two streams, two host
+//     threads) race on it;
+//   * the call waits for its stream to read the vertex count back to the host;
 //   * the first call on a device looks up the array's device address (cudaGetSymbolAddress,
-//     with that device current) and caches it; make that first call before any stream capture.
+//     with that device current) and keeps it for the life of the process: calling
+//     cudaDeviceReset on that device afterwards is not supported.
 #include <mutex>
 
 #include "its_mc.cuh"
@@ -67,8 +73,17 @@ its_status its_marching_cubes_noalloc(its_ctx* ctx, const double* field, int res
     return setError(ctx, ITS_ERR_INVALID,
                     "its_marching_cubes_noalloc: res " + std::to_string(res) + " exceeds the maximum of 256 "
                     "(fixed scratch of 8,193 words); use its_marching_cubes");
-  if (!isDevicePtr(field) || (cube_index && !isDevicePtr(cube_index)) || (tri_verts && !isDevicePtr(tri_verts)))
-    return setError(ctx, ITS_ERR_INVALID, "its_marching_cubes_noalloc: field and outputs must be device memory");
+  if (!isDevicePtr(ctx, field) || (cube_index && !isDevicePtr(ctx, cube_index)) ||
+      (tri_verts && !isDevicePtr(ctx, tri_verts)))
+    return setError(ctx, ITS_ERR_INVALID,
+                    "its_marching_cubes_noalloc: field and outputs must be device memory of the context's GPU");
+  // the vertex count is read back with a stream synchronisation, which a capturing stream
+  // does not allow: refuse before anything is queued rather than break the caller's capture
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  ITS_CU(ctx, cudaStreamIsCapturing(ctx->stream, &cap));
+  if (cap != cudaStreamCaptureStatusNone)
+    return setError(ctx, ITS_ERR_INVALID,
+                    "its_marching_cubes_noalloc: the stream is capturing; this call waits for the vertex count");
   unsigned long long* scratch = nullptr;
   its_status st = scratchFor(ctx, &scratch);
   if (st != ITS_OK) return st;

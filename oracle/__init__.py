@@ -39,6 +39,7 @@ def _declare(L):
         "orc_morton_encode": (None, [vp, i64, vp]),
         "orc_morton_decode": (None, [vp, i64, vp]),
         "orc_luts": (None, [vp, vp, vp, vp]),
+        "orc_hat": (None, [vp, vp, vp, i64, vp, vp]),
         "orc_svo_build": (vp, [vp, i64, vp, i64, i32, vp, vp]),
         "orc_svo_free": (None, [vp]),
         "orc_svo_counts": (None, [vp, vp]),
@@ -123,6 +124,14 @@ def luts():
     v, e = np.zeros(64, np.int16), np.zeros(48, np.int16)
     lib().orc_luts(_p(p), _p(c), _p(v), _p(e))
     return p, c, v, e
+
+
+def hat(p, w, q):
+    """Hat value and gradient of the corner at p (width w) at the points q (BSpline.hpp:4-57)."""
+    p, q, w = _f64(p, (-1, 3)), _f64(q, (-1, 3)), _f64(w)
+    val, grad = np.zeros(p.shape[0]), np.zeros((p.shape[0], 3))
+    lib().orc_hat(_p(p), _p(w), _p(q), p.shape[0], _p(val), _p(grad))
+    return val, grad
 
 
 class Svo:

@@ -24,6 +24,21 @@ void orc_morton_encode(const uint32_t* xyz, int64_t n, uint32_t* out) {
 void orc_morton_decode(const uint32_t* m, int64_t n, uint32_t* xyz) {
   for (int64_t i = 0; i < n; ++i) mortonDecode(m[i], xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
 }
+// The hat basis at single points: value (baseFunction4Point) and gradient as
+// de_BaseFunction4Point forms it (BSpline.hpp:37-57), for the known-answer pin against the
+// reference's own BSpline.hpp.
+void orc_hat(const double* p, const double* w, const double* q, int64_t n, double* val, double* grad) {
+  for (int64_t i = 0; i < n; ++i) {
+    const V3 c{p[3 * i], p[3 * i + 1], p[3 * i + 2]}, x{q[3 * i], q[3 * i + 1], q[3 * i + 2]};
+    const double wd = w[i];
+    val[i] = baseFunction4Point(c, wd, x);
+    const double bx = baseFunction(x.x, c.x, wd), by = baseFunction(x.y, c.y, wd), bz = baseFunction(x.z, c.z, wd);
+    grad[3 * i] = deBaseFunction(x.x, c.x, wd) * by * bz;
+    grad[3 * i + 1] = bx * deBaseFunction(x.y, c.y, wd) * bz;
+    grad[3 * i + 2] = bx * by * deBaseFunction(x.z, c.z, wd);
+  }
+}
+
 void orc_luts(int16_t* parent, int16_t* child, int16_t* vert, int16_t* edge) {
   short p[8][27], c[8][27], v[64], e[48];
   neighborLUTs(p, c);

@@ -6,6 +6,9 @@ Writes tests/golden/ref_tables.json with:
   * the marching-cubes case tables of the reference's LookTable.h;
   * the neighbour / shared-corner / shared-edge LUTs of the reference's SVO.cu,
     read as text (SVO.cu needs Eigen and Thrust and cannot be compiled here).
+Writes tests/golden/ref_bspline.json: the reference's own hat values and gradients
+(src/BSpline.hpp, BaseFunction4Point and de_BaseFunction4Point, compiled by
+oracle/build_ref.py) at known-answer and pseudo-random points.
 Also writes its_b200/csrc/mc_tables.inc: the same case table repacked as one
 64-bit word per case (low nibble = vertex count, nibble k+1 = k-th edge index),
 which the CUDA product and the oracle include. The standard Lorensen/Bourke case
@@ -19,9 +22,9 @@ import sys
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
-from oracle.build_ref import build  # noqa: E402
+from oracle.build_ref import REF, bspline_harness, build  # noqa: E402
 
-SVO_CU = "/root/reference/src/cuAcc/SVO.cu"
+SVO_CU = os.path.join(REF, "cuAcc", "SVO.cu")
 
 
 def parse_table(src, name):
@@ -69,7 +72,12 @@ def main():
                 "// tests/golden/make_ref_tables.py; corner/edge numbering follows MarchingCubes.cu:233-262.\n")
         for i in range(0, 256, 4):
             f.write("  " + ", ".join("0x%016xull" % w for w in words[i:i + 4]) + ",\n")
-    print("wrote", out, "and", inc)
+    hats = json.loads(subprocess.run([bspline_harness()], check=True, capture_output=True, text=True).stdout)
+    hats["source"] = "src/BSpline.hpp:4-57 (compiled): rows p.x p.y p.z w q.x q.y q.z value grad.x grad.y grad.z"
+    out2 = os.path.join(ROOT, "tests", "golden", "ref_bspline.json")
+    with open(out2, "w") as f:
+        json.dump(hats, f, separators=(",", ":"))
+    print("wrote", out, out2, "and", inc)
 
 
 if __name__ == "__main__":

@@ -1,6 +1,7 @@
-"""Pins the oracle's Morton codes, octree LUTs and MC table against the reference's own
-headers (tests/golden/ref_tables.json, made by tests/golden/make_ref_tables.py from the
-reference's MortonLUT.h, LookTable.h and SVO.cu)."""
+"""Pins the oracle's Morton codes, octree LUTs, MC table and hat basis against the reference's
+own headers (tests/golden/ref_tables.json and ref_bspline.json, made by
+tests/golden/make_ref_tables.py from the reference's MortonLUT.h, LookTable.h, SVO.cu and
+BSpline.hpp)."""
 import json
 import os
 
@@ -9,6 +10,7 @@ import numpy as np
 import oracle
 
 GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "ref_tables.json")))
+HATS = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "ref_bspline.json")))
 
 
 def test_morton_encode_decode_match_reference_tables():
@@ -58,3 +60,21 @@ def test_share_network_oracle_gradient_finite_differences():
         lm = np.mean((mlp.forward(Pm, X, False) - y) ** 2)
         fd = (lp - lm) / (2 * h)
         assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(fd)), (i, fd, g[i])
+
+
+def test_hat_basis_matches_reference_bspline():
+    # BaseFunction4Point / de_BaseFunction4Point of the reference's own BSpline.hpp (compiled),
+    # at the node, the support ends (the 1e-9 cut), half-way and arbitrary points: bit-exact
+    rows = np.array(HATS["hat"], dtype=np.float64)
+    assert rows.shape[0] >= 700
+    val, grad = oracle.hat(rows[:, 0:3], rows[:, 3], rows[:, 4:7])
+    assert np.array_equal(val, rows[:, 7])
+    assert np.array_equal(grad, rows[:, 8:11])
+    # the known answers of the hat: 1 at the node, 0 at the support ends, 1/2 half-way
+    on_axis = rows[:144]
+    w = on_axis[:, 3]
+    a = (on_axis[:, 4] - on_axis[:, 0]) / w
+    b = (on_axis[:, 5] - on_axis[:, 1]) / w
+    want = np.where((np.abs(a) < 1) & (np.abs(b) < 1), (1 - np.abs(a)) * (1 - np.abs(b)) * 0.75, 0.0)
+    ends = (np.abs(np.abs(a) - 1) < 1e-6) | (np.abs(np.abs(b) - 1) < 1e-6)
+    assert np.allclose(on_axis[~ends, 7], want[~ends], atol=1e-12)
