@@ -195,11 +195,11 @@ class ThinShells {
 
  private:
   void marchingCubes(double iso, int res, const std::string& filename, bool welded) const {
-    const int64_t M = (int64_t)res + 1;
-    std::vector<double> field(M * M * M);
-    check(its_eval_grid(svo_, lambda_.data(), origin_.data(), width_.data(), res, field.data()), ctx_, "MC field");
     std::ofstream out(filename);
     if (welded) {
+      const int64_t M = (int64_t)res + 1;
+      std::vector<double> field(M * M * M);
+      check(its_eval_grid(svo_, lambda_.data(), origin_.data(), width_.data(), res, field.data()), ctx_, "MC field");
       int64_t nvt = 0, ntr = 0;
       check(its_marching_cubes_mesh(ctx_, field.data(), res, origin_.data(), width_.data(), iso, nullptr, 0, &nvt,
                                     nullptr, 0, &ntr),
@@ -215,12 +215,15 @@ class ThinShells {
         out << "f " << tris[3 * t] + 1 << ' ' << tris[3 * t + 1] + 1 << ' ' << tris[3 * t + 2] + 1 << '\n';
       return;
     }
+    // the soup: field and marching cubes on the device, only the triangles come back
     int64_t n = 0;
-    check(its_marching_cubes(ctx_, field.data(), res, origin_.data(), width_.data(), iso, nullptr, nullptr, 0, &n), ctx_,
-          "marching_cubes");
-    std::vector<double> tri(3 * n);
-    check(its_marching_cubes(ctx_, field.data(), res, origin_.data(), width_.data(), iso, nullptr, tri.data(), n, &n),
+    check(its_eval_grid_mc(svo_, lambda_.data(), origin_.data(), width_.data(), res, 0, &iso, 1, nullptr, nullptr, &n),
           ctx_, "marching_cubes");
+    std::vector<double> tri(3 * n);
+    double* tp = tri.data();
+    const int64_t cap = n;
+    check(its_eval_grid_mc(svo_, lambda_.data(), origin_.data(), width_.data(), res, 0, &iso, 1, &tp, &cap, &n), ctx_,
+          "marching_cubes");
     for (int64_t i = 0; i < n; ++i) out << "v " << tri[3 * i] << ' ' << tri[3 * i + 1] << ' ' << tri[3 * i + 2] << '\n';
     for (int64_t i = 0; i + 2 < n; i += 3) out << "f " << i + 1 << ' ' << i + 2 << ' ' << i + 3 << '\n';
   }

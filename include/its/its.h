@@ -250,6 +250,16 @@ its_status its_eval_grid(its_svo* svo, const double* lambda, const double origin
 its_status its_marching_cubes(its_ctx* ctx, const double* field, int res, const double origin[3],
                               const double width[3], double iso, uint8_t* cube_index, double* tri_verts,
                               int64_t capacity, int64_t* num_verts);
+/* The marching-cubes driver of ThinShells::mcVisualization (src/ThinShells.cpp:1086-1129 ->
+   MC::marching_cubes, src/cuAcc/MarchingCubes/MarchingCubes.cu:672-714) in one call: the field
+   of lambda on the (res+1)^3 lattice is evaluated once into device scratch (field_mode 0:
+   its_eval_grid, bit-exact; 1: its_eval_grid_fast) and stays on the device while marching
+   cubes runs at each of the n_iso levels. Level k writes up to capacity[k] vertices to
+   tri_verts[k] (host or device; tri_verts NULL or a NULL entry: count only) and its total
+   vertex count to num_verts[k]. */
+its_status its_eval_grid_mc(its_svo* svo, const double* lambda, const double origin[3], const double width[3], int res,
+                            int field_mode, const double* iso, int n_iso, double* const* tri_verts,
+                            const int64_t* capacity, int64_t* num_verts);
 /* Welded, indexed form of MC::marching_cubes' triangle soup (writeToOBJFile,
    src/cuAcc/MarchingCubes/MarchingCubes.cu:635-661, emits 3 fresh vertices per triangle): one
    vertex per active lattice edge (numbered in edge-id order, id = 3*((z*(res+1)+y)*(res+1)+x)+axis)
@@ -310,6 +320,12 @@ its_status its_mlp_set_params(its_mlp* mlp, const float* params);
 its_status its_mlp_get_params(its_mlp* mlp, float* params);
 /* Predictions: one persistent kernel for all layers (weights and activations in shared memory). */
 its_status its_mlp_forward(its_mlp* mlp, const float* features, int64_t n, float* out);
+/* The same predictions for device features and output, queued on the context's stream
+   without waiting (for callers that pipeline inference with their own work); a tensor-core
+   wait that ran out sets a sticky flag that its_mlp_check reports. */
+its_status its_mlp_forward_async(its_mlp* mlp, const float* features, int64_t n, float* out);
+/* Waits for the context's stream; ITS_ERR_TIMEOUT if a network kernel's bounded wait ran out. */
+its_status its_mlp_check(its_mlp* mlp);
 /* The same predictions layer by layer through the training kernels (bit-identical). */
 its_status its_mlp_forward_layers(its_mlp* mlp, const float* features, int64_t n, float* out);
 /* Gradient of mean((out - y)^2) over n rows (n <= batch, a multiple of 64), no update. */

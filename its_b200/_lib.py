@@ -72,6 +72,8 @@ SIGNATURES = {
     "its_mlp_set_params": (st, [vp, vp]),
     "its_mlp_get_params": (st, [vp, vp]),
     "its_mlp_forward": (st, [vp, vp, i64, vp]),
+    "its_mlp_forward_async": (st, [vp, vp, i64, vp]),
+    "its_mlp_check": (st, [vp]),
     "its_mlp_forward_layers": (st, [vp, vp, i64, vp]),
     "its_mlp_gradient": (st, [vp, vp, vp, i64, vp, vp]),
     "its_mlp_train": (st, [vp, vp, vp, i64, i64, C.c_float, C.c_uint64, vp]),
@@ -90,6 +92,7 @@ SIGNATURES = {
     "its_marching_cubes_f32": (st, [vp, vp, i32, vp, vp, dbl, vp, vp, i64, C.POINTER(i64)]),
     "its_eval_grid_f32": (st, [vp, vp, vp, vp, i32, vp]),
     "its_eval_grid_fast": (st, [vp, vp, vp, vp, i32, vp]),
+    "its_eval_grid_mc": (st, [vp, vp, vp, vp, i32, i32, vp, i32, vp, vp, vp]),
     "its_eval_grid_fast_f32": (st, [vp, vp, vp, vp, i32, vp]),
     "its_marching_cubes_mesh": (st, [vp, vp, i32, vp, vp, dbl, vp, i64, C.POINTER(i64), vp, i64, C.POINTER(i64)]),
 }

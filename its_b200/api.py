@@ -332,6 +332,27 @@ class Svo:
         self.ctx.check(fn(self.h, _ptr(lam), _ptr(o), _ptr(w), res, _ptr(out)), "its_eval_grid_fast")
         return out
 
+    def grid_mc(self, lam, origin, width, res, isos, fast=False, triangles=True):
+        """Field once on the device, then marching cubes at every iso level (its_eval_grid_mc,
+        ThinShells::mcVisualization's driver). Returns one (num_verts x 3) soup per level (or the
+        counts with triangles=False)."""
+        lam = _f64(lam)
+        o, w = np.ascontiguousarray(origin, np.float64), np.ascontiguousarray(width, np.float64)
+        iso = np.ascontiguousarray(isos, np.float64)
+        k = int(iso.shape[0])
+        cnt = np.zeros(k, np.int64)
+        L = lib()
+        self.ctx.check(L.its_eval_grid_mc(self.h, _ptr(lam), _ptr(o), _ptr(w), res, 1 if fast else 0, _ptr(iso), k,
+                                          None, None, _ptr(cnt)), "its_eval_grid_mc")
+        if not triangles:
+            return cnt
+        outs = [np.zeros((max(int(c), 1), 3)) for c in cnt]
+        P = (C.c_void_p * k)(*[o_.ctypes.data for o_ in outs])
+        cap = cnt.copy()
+        self.ctx.check(L.its_eval_grid_mc(self.h, _ptr(lam), _ptr(o), _ptr(w), res, 1 if fast else 0, _ptr(iso), k,
+                                          P, _ptr(cap), _ptr(cnt)), "its_eval_grid_mc")
+        return [x[:int(c)] for x, c in zip(outs, cnt)]
+
     def vertex_sdf(self, V, F):
         """Right-hand side b: signed distance of every corner vertex (ThinShells::cpSDFOfTreeNodes)."""
         pos, _ = self.vertices()
@@ -537,6 +558,14 @@ class ShareNet:
             out = np.zeros(n, np.float32)
         self.ctx.check(lib().its_mlp_forward(self.h, _ptr(X), n, _ptr(out)), "its_mlp_forward")
         return out
+
+    def forward_async(self, X, out):
+        """Predictions for device (torch CUDA) features into a device output, queued without waiting."""
+        self.ctx.check(lib().its_mlp_forward_async(self.h, _ptr(X), _n(X), _ptr(out)), "its_mlp_forward_async")
+        return out
+
+    def check(self):
+        self.ctx.check(lib().its_mlp_check(self.h), "its_mlp_check")
 
     def forward_layers(self, X, out=None):
         X = _f32(X)

@@ -740,6 +740,24 @@ its_status its_mlp_forward(its_mlp* h, const float* X, int64_t n, float* out) {
   return checkErr(h);
 }
 
+// The same predictions for device rows, queued on the context's stream without waiting; a
+// tensor-core wait that ran out is reported by the next its_mlp_check (the flag is sticky).
+its_status its_mlp_forward_async(its_mlp* h, const float* X, int64_t n, float* out) {
+  if (!h || (n > 0 && (!X || !out)) || n < 0) return ITS_ERR_INVALID;
+  its_ctx* ctx = h->ctx;
+  if (n > 0 && (!isDevicePtr(ctx, X) || !isDevicePtr(ctx, out)))
+    return setError(ctx, ITS_ERR_INVALID, "its_mlp_forward_async: features and output must be device memory");
+  ITS_CU(ctx, cudaSetDevice(ctx->device));
+  return mlpInfer(h, X, n, out);
+}
+
+// Waits for the context's stream and reports the network's error flag.
+its_status its_mlp_check(its_mlp* h) {
+  if (!h) return ITS_ERR_INVALID;
+  ITS_CU(h->ctx, cudaSetDevice(h->ctx->device));
+  return checkErr(h);
+}
+
 // The same predictions layer by layer (the training kernels' forward); identical to
 // its_mlp_forward bit for bit (a test hook).
 its_status its_mlp_forward_layers(its_mlp* h, const float* X, int64_t n, float* out) {

@@ -259,3 +259,9 @@ def config_mesh(name, seed=None):
     if name == "small":
         return sphere_mesh(3, amp=0.1, seed=0 if seed is None else seed)
     raise KeyError(name)
+
+
+def batch_face_counts(count=256, seed=3, **kw):
+    """Face counts of batch_meshes(count, seed) in generation order (what the batch's
+    sharding over ranks is decided by)."""
+    return [m["faces"] for m in batch_meshes(count, seed, **kw)]

@@ -63,6 +63,7 @@ def _declare(L):
         "orc_points_get": (None, [vp, vp]),
         "orc_points_free": (None, [vp]),
         "orc_signed_distance": (None, [vp, i64, vp, vp, i64, vp]),
+        "orc_signed_distance_bvh": (None, [vp, i64, vp, vp, i64, vp]),
         "orc_eval_points": (None, [vp, vp, vp, i64, vp, vp]),
         "orc_eval_brute": (None, [vp, vp, vp, i64, vp]),
         "orc_eval_grid": (None, [vp, vp, vp, vp, i32, vp]),
@@ -275,6 +276,14 @@ def signed_distance(P, V, F):
     P, V, F = _f64(P), _f64(V), _i32(F)
     out = np.zeros(P.shape[0])
     lib().orc_signed_distance(_p(P), P.shape[0], _p(V), _p(F), F.shape[0], _p(out))
+    return out
+
+
+def signed_distance_bvh(P, V, F):
+    """The signed distance as libits computes it: linear BVH, exact distance, fast winding number."""
+    P, V, F = _f64(P), _f64(V), _i32(F)
+    out = np.zeros(P.shape[0])
+    lib().orc_signed_distance_bvh(_p(P), P.shape[0], _p(V), _p(F), F.shape[0], _p(out))
     return out
 
 

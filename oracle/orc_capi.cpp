@@ -167,6 +167,10 @@ void orc_points_free(void* p) { delete static_cast<Points*>(p); }
 void orc_signed_distance(const double* P, int64_t m, const double* V, const int32_t* F, int64_t nf, double* out) {
   signedDistance(P, m, V, F, nf, out);
 }
+void orc_signed_distance_bvh(const double* P, int64_t m, const double* V, const int32_t* F, int64_t nf,
+                             double* out) {
+  signedDistanceBvh(P, m, V, F, nf, out);
+}
 void orc_eval_points(void* h, const double* lambda, const double* P, int64_t m, double* out, uint8_t* missing) {
   evalPoints(*static_cast<Svo*>(h), lambda, P, m, out, missing);
 }

@@ -173,7 +173,7 @@ std::vector<V3> intersections(const Svo& s, const double* V, int64_t nv, const i
 // libigl's signed_distance(FAST_WINDING_NUMBER) is not available; this restates it as the
 // exact point-triangle distance (Ericson, Real-Time Collision Detection 5.1.5) with the
 // sign of the exact generalised winding number (Jacobson et al. 2013): inside if w > 0.5.
-static double pointTriSqDist(const V3& p, const V3& a, const V3& b, const V3& c) {
+double pointTriSqDist(const V3& p, const V3& a, const V3& b, const V3& c) {
   const V3 ab = b - a, ac = c - a, ap = p - a;
   const double d1 = dot3(ab, ap), d2 = dot3(ac, ap);
   if (d1 <= 0.0 && d2 <= 0.0) return dot3(ap, ap);
@@ -207,7 +207,7 @@ static double pointTriSqDist(const V3& p, const V3& a, const V3& b, const V3& c)
   return dot3(q, q);
 }
 // Solid angle of triangle (a,b,c) seen from p (Van Oosterom & Strackee 1983).
-static double solidAngle(const V3& p, const V3& a0, const V3& b0, const V3& c0) {
+double solidAngle(const V3& p, const V3& a0, const V3& b0, const V3& c0) {
   const V3 a = a0 - p, b = b0 - p, c = c0 - p;
   const double la = std::sqrt(dot3(a, a)), lb = std::sqrt(dot3(b, b)), lc = std::sqrt(dot3(c, c));
   const double num = dot3(a, cross3(b, c));

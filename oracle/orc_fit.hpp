@@ -21,6 +21,11 @@ struct CglsReport {
 std::vector<V3> intersections(const Svo& s, const double* V, int64_t nv, const int32_t* F, int64_t nf,
                               size_t* nEdgePoints);
 void signedDistance(const double* P, int64_t m, const double* V, const int32_t* F, int64_t nf, double* out);
+// The same signed distance accelerated as libits computes it (orc_bvh.cpp): a linear BVH,
+// exact nearest-triangle distance, the sign from the fast winding number.
+void signedDistanceBvh(const double* P, int64_t m, const double* V, const int32_t* F, int64_t nf, double* out);
+double pointTriSqDist(const V3& p, const V3& a, const V3& b, const V3& c);
+double solidAngle(const V3& p, const V3& a0, const V3& b0, const V3& c0);
 Csr assemble(const Svo& s);
 Csr transpose(const Csr& A);
 CglsReport cgls(const Csr& A, const Csr& T, const double* b, double* x, double tol, int64_t maxIters, int stop);

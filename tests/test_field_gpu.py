@@ -285,3 +285,20 @@ def test_marching_cubes_row_tiles_bit_exact(ctx, fitted):
                                            C.byref(n)), "mc f32")
     cube_r32, _, n_r32 = oracle.marching_cubes(f32.astype(np.float64), R, o, w, iso)
     assert np.array_equal(cube, cube_r32) and n.value == n_r32
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fast", [False, True])
+def test_grid_mc_driver_matches_field_then_marching_cubes(ctx, fitted, fast):
+    # its_eval_grid_mc (the mcVisualization driver, field kept on the device) gives exactly the
+    # soups of its_eval_grid / its_eval_grid_fast followed by its_marching_cubes per level
+    V, F, o, w, ref, gpu, pos, b, lam = fitted
+    R = 64  # 2 x the octree's res: the prolongation lattice
+    field = gpu.eval_grid_fast(lam, o, w, R) if fast else gpu.eval_grid(lam, o, w, R)
+    isos = [float(np.quantile(field, 0.4)), float(np.quantile(field, 0.6)), 0.0]
+    soups = gpu.grid_mc(lam, o, w, R, isos, fast=fast)
+    counts = gpu.grid_mc(lam, o, w, R, isos, fast=fast, triangles=False)
+    for iso, soup, cnt in zip(isos, soups, counts):
+        _, tri, n = ctx.marching_cubes(field, R, o, w, iso)
+        assert n == cnt == soup.shape[0] and n > 0
+        assert np.array_equal(soup, tri)
