@@ -136,6 +136,22 @@ typedef enum its_op_mode { ITS_OP_FP64 = 0, ITS_OP_FP32_VALUES = 1 } its_op_mode
    columns plus its transpose; ITS_OP_FP32_VALUES also keeps float copies of the values for
    the mixed-precision solver. */
 its_status its_operator_build(its_svo* svo, int mode, its_op** out);
+/* Basis options of its_operator_build_ex. No counterpart in the reference: its basis is the
+   degree-1 hat (src/BSpline.hpp:4-22) and its fit samples are the corner vertices
+   (src/ThinShells.cpp:481-606); extra sample rows follow the uncompiled
+   src/ThinShellsOctree.deprecated.cpp:139-187, which appends one row per sample point. */
+typedef struct its_basis_opts {
+  int degree;              /* 1: the reference's hats (its_operator_build); 3: cubic B-splines */
+  const double* samples;   /* extra fit points, 3 per point, rows after the corner vertices' */
+  int64_t num_samples;     /* (cubic basis only; 0 for none) */
+} its_basis_opts;
+/* The fit system in the chosen basis. Cubic: vertex v at depth d, lattice point (X,Y,Z), carries
+   the tensor product of uniform cubic B-splines of width w_d = unit * 2^d centred at
+   origin + (X,Y,Z) w_d; row r < num_vertices is the basis at corner vertex r (its exact lattice
+   point), row num_vertices + i at samples[i]. With extra samples the system is stored square
+   (rows x rows, the columns past the vertices empty): its_lscg_solve then takes b and lambda
+   with rows entries, lambda's entries past the vertices staying 0. */
+its_status its_operator_build_ex(its_svo* svo, int mode, const its_basis_opts* opts, its_op** out);
 its_status its_operator_free(its_op* op);
 its_status its_operator_info(const its_op* op, int64_t* rows, int64_t* nnz);
 its_status its_operator_get_csr(its_op* op, int64_t* rowptr, int32_t* col, double* val);
@@ -237,6 +253,22 @@ its_status its_point_query(its_svo* svo, const double* lambda, const double* poi
 its_status its_point_value_gradient(its_svo* svo, const double* lambda, const double* points, const double* before,
                                    int64_t npoints, const double box_origin[3], const double box_end[3], double* values,
                                    double* gradients, uint8_t* missing);
+
+/* ---- cubic basis: field, and the offset shell samples ----------------------------------
+   No counterpart in the reference (see its_basis_opts). Field of cubic coefficients (one per
+   corner vertex) at points / on the (res+1)^3 lattice origin + i*width/res (x fastest): the sum
+   over every depth and every vertex whose support holds the point, in the order the rows of
+   its_operator_build_ex use, so A lambda equals the field at the rows' points bit for bit. */
+its_status its_eval_points_cubic(its_svo* svo, const double* lambda, const double* points, int64_t npoints,
+                                 double* out);
+its_status its_eval_grid_cubic(its_svo* svo, const double* lambda, const double origin[3], const double width[3],
+                               int res, double* field);
+/* Offset shell samples: at every mesh vertex the unit area-weighted normal n (the sum of the
+   unnormalised normals (p1-p0)x(p2-p0) of its faces, in face order, made unit) and the points
+   v + eps n (target +eps) for all vertices, then v - eps n (target -eps): points 6*nverts
+   doubles, targets 2*nverts (either may be NULL). A vertex with no face gets both points at v. */
+its_status its_offset_samples(its_ctx* ctx, const double* verts, int64_t nverts, const int32_t* faces, int64_t nfaces,
+                              double eps, double* points, double* targets);
 
 /* ---- a14-a15: dense field and marching cubes -------------------------------------------- */
 /* The field of MC::launch_computSDFKernel (src/cuAcc/MarchingCubes/MarchingCubes.cu:464-536,

@@ -21,6 +21,10 @@ class SvoInfo(C.Structure):
                 ("origin", C.c_double * 3), ("unit", C.c_double * 3)]
 
 
+class BasisOpts(C.Structure):
+    _fields_ = [("degree", C.c_int), ("samples", C.c_void_p), ("num_samples", C.c_int64)]
+
+
 class SolveOpts(C.Structure):
     _fields_ = [("tol", C.c_double), ("max_iters", C.c_int64), ("stop_rule", C.c_int), ("precision", C.c_int),
                 ("ir_steps", C.c_int), ("inner_tol", C.c_double), ("x0", C.c_void_p), ("check_every", C.c_int)]
@@ -93,6 +97,10 @@ SIGNATURES = {
     "its_eval_grid_f32": (st, [vp, vp, vp, vp, i32, vp]),
     "its_eval_grid_fast": (st, [vp, vp, vp, vp, i32, vp]),
     "its_eval_grid_mc": (st, [vp, vp, vp, vp, i32, i32, vp, i32, vp, vp, vp]),
+    "its_operator_build_ex": (st, [vp, i32, vp, C.POINTER(vp)]),
+    "its_eval_points_cubic": (st, [vp, vp, vp, i64, vp]),
+    "its_eval_grid_cubic": (st, [vp, vp, vp, vp, i32, vp]),
+    "its_offset_samples": (st, [vp, vp, i64, vp, i64, dbl, vp, vp]),
     "its_eval_grid_fast_f32": (st, [vp, vp, vp, vp, i32, vp]),
     "its_marching_cubes_mesh": (st, [vp, vp, i32, vp, vp, dbl, vp, i64, C.POINTER(i64), vp, i64, C.POINTER(i64)]),
 }

@@ -113,6 +113,16 @@ class Context:
                    "its_signed_distance")
         return out
 
+    def offset_samples(self, V, F, eps):
+        """Offset shell samples v + eps n, then v - eps n (n the unit area-weighted vertex
+        normal), and their targets +eps / -eps (its_offset_samples)."""
+        V, F = _f64(V), _i32(F)
+        nv = _n(V)
+        pts, tgt = np.zeros((2 * nv, 3)), np.zeros(2 * nv)
+        self.check(lib().its_offset_samples(self.h, _ptr(V), nv, _ptr(F), _n(F), float(eps), _ptr(pts), _ptr(tgt)),
+                   "its_offset_samples")
+        return pts, tgt
+
     def marching_cubes(self, field, res, origin, width, iso, triangles=True):
         field = _f64(field)
         o, w = np.ascontiguousarray(origin, np.float64), np.ascontiguousarray(width, np.float64)
@@ -332,6 +342,25 @@ class Svo:
         self.ctx.check(fn(self.h, _ptr(lam), _ptr(o), _ptr(w), res, _ptr(out)), "its_eval_grid_fast")
         return out
 
+    def eval_points_cubic(self, lam, P, out=None):
+        """Field of cubic-basis coefficients at points (its_eval_points_cubic)."""
+        lam, P = _f64(lam), _f64(P)
+        m = _n(P)
+        if out is None:
+            out = np.zeros(m)
+        self.ctx.check(lib().its_eval_points_cubic(self.h, _ptr(lam), _ptr(P), m, _ptr(out)), "its_eval_points_cubic")
+        return out
+
+    def eval_grid_cubic(self, lam, origin, width, res, out=None):
+        """Field of cubic-basis coefficients on the (res+1)^3 lattice (its_eval_grid_cubic)."""
+        lam = _f64(lam)
+        o, w = np.ascontiguousarray(origin, np.float64), np.ascontiguousarray(width, np.float64)
+        if out is None:
+            out = np.zeros((res + 1) ** 3)
+        self.ctx.check(lib().its_eval_grid_cubic(self.h, _ptr(lam), _ptr(o), _ptr(w), res, _ptr(out)),
+                       "its_eval_grid_cubic")
+        return out
+
     def grid_mc(self, lam, origin, width, res, isos, fast=False, triangles=True):
         """Field once on the device, then marching cubes at every iso level (its_eval_grid_mc,
         ThinShells::mcVisualization's driver). Returns one (num_verts x 3) soup per level (or the
@@ -360,12 +389,23 @@ class Svo:
 
 
 class Operator:
-    """An its_op: the assembled basis matrix A and its transpose."""
+    """An its_op: the assembled basis matrix A and its transpose.
 
-    def __init__(self, svo, mode=OP_FP64):
+    degree 1 is the reference's hat basis; degree 3 the cubic B-spline basis, optionally with
+    extra sample rows (samples, m x 3) after the corner vertices' rows (its_operator_build_ex);
+    such a system is square-padded: b and the solution then have rows entries."""
+
+    def __init__(self, svo, mode=OP_FP64, degree=1, samples=None):
         self.ctx, self.svo = svo.ctx, svo
+        self.degree = degree
         h = C.c_void_p()
-        svo.ctx.check(lib().its_operator_build(svo.h, mode, C.byref(h)), "its_operator_build")
+        if degree == 1 and samples is None:
+            svo.ctx.check(lib().its_operator_build(svo.h, mode, C.byref(h)), "its_operator_build")
+        else:
+            from ._lib import BasisOpts
+            S = None if samples is None else _f64(samples)
+            opts = BasisOpts(degree, None if S is None else _ptr(S).value, 0 if S is None else _n(S))
+            svo.ctx.check(lib().its_operator_build_ex(svo.h, mode, C.byref(opts), C.byref(h)), "its_operator_build_ex")
         self.h = h
         svo.ctx._adopt(self)
         r, z = C.c_int64(0), C.c_int64(0)

@@ -7,18 +7,26 @@
 // transpose is a stable radix sort of the entries by column.
 #include <cmath>
 
+#include "its_cubic.cuh"
 #include "its_op.cuh"
 #include "its_rows.cuh"
 
 namespace its {
 
-template <bool FILL>
-__global__ void kAssembleRows(const __grid_constant__ RowParams P, int64_t n, int64_t* __restrict__ rowptrOrCount,
+// Rows of the reference's hat-basis system (walkRow).
+struct HatGen {
+  RowParams P;
+  template <typename E>
+  __device__ void operator()(int64_t r, E emit) const { walkRow(P, r, emit); }
+};
+
+template <bool FILL, typename Gen>
+__global__ void kAssembleRows(const __grid_constant__ Gen gen, int64_t n, int64_t* __restrict__ rowptrOrCount,
                               int32_t* __restrict__ col, double* __restrict__ val, uint32_t* __restrict__ rowIdx) {
   const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (r >= n) return;
   int64_t k = FILL ? rowptrOrCount[r] : 0;
-  walkRow(P, r, [&](int32_t c, double v) {
+  gen(r, [&](int32_t c, double v) {
     if (FILL) {
       col[k] = c;
       val[k] = v;
@@ -76,15 +84,15 @@ static void opRelease(its_op* op) {
   releasePlan(c, &op->planT);
 }
 
-static its_status opBuild(its_op* op) {
+// Assembles the n x n system whose rows gen generates (columns < n; a system with more rows
+// than unknowns is stored square, its columns past the unknowns empty).
+template <typename Gen>
+static its_status opBuild(its_op* op, int64_t n, const Gen& P) {
   its_ctx* ctx = op->ctx;
-  const SvoDevice& d = op->svo->d;
-  const int64_t n = d.numVerts;
   op->n = n;
-  const RowParams P = rowParams(d);
   its_status st;
   if ((st = devAlloc(ctx, (void**)&op->rowptr, (n + 1) * 8)) != ITS_OK) return st;
-  kAssembleRows<false><<<gridFor(n, 128), 128, 0, ctx->stream>>>(P, n, op->rowptr, nullptr, nullptr, nullptr);
+  kAssembleRows<false, Gen><<<gridFor(n, 128), 128, 0, ctx->stream>>>(P, n, op->rowptr, nullptr, nullptr, nullptr);
   ITS_LAUNCHED(ctx);
   DevBuf<int64_t> tot;
   if ((st = tot.alloc(ctx, 1)) != ITS_OK) return st;
@@ -102,7 +110,7 @@ static its_status opBuild(its_op* op) {
   if ((st = devAlloc(ctx, (void**)&op->val, nnz * 8)) != ITS_OK) return st;
   DevBuf<uint32_t> rowIdx;
   if ((st = rowIdx.alloc(ctx, nnz)) != ITS_OK) return st;
-  kAssembleRows<true><<<gridFor(n, 128), 128, 0, ctx->stream>>>(P, n, op->rowptr, op->col, op->val, rowIdx.p);
+  kAssembleRows<true, Gen><<<gridFor(n, 128), 128, 0, ctx->stream>>>(P, n, op->rowptr, op->col, op->val, rowIdx.p);
   ITS_LAUNCHED(ctx);
 
   // transpose: stable sort of the entries by column keeps rows ascending within a column
@@ -175,7 +183,42 @@ its_status its_operator_build(its_svo* svo, int mode, its_op** out) {
   op->ctx = ctx;
   op->svo = svo;
   op->mode = mode;
-  its_status st = opBuild(op);
+  op->unknowns = svo->d.numVerts;
+  its_status st = opBuild(op, svo->d.numVerts, HatGen{rowParams(svo->d)});
+  if (st != ITS_OK) {
+    opRelease(op);
+    cudaStreamSynchronize(ctx->stream);
+    delete op;
+    return st;
+  }
+  *out = op;
+  return ITS_OK;
+}
+
+its_status its_operator_build_ex(its_svo* svo, int mode, const its_basis_opts* opts, its_op** out) {
+  if (!svo || !out) return ITS_ERR_INVALID;
+  *out = nullptr;
+  its_ctx* ctx = svo->ctx;
+  const int degree = opts ? opts->degree : 1;
+  const int64_t m = opts ? opts->num_samples : 0;
+  if (mode != ITS_OP_FP64 && mode != ITS_OP_FP32_VALUES) return setError(ctx, ITS_ERR_INVALID, "unknown operator mode");
+  if (degree != 1 && degree != 3) return setError(ctx, ITS_ERR_INVALID, "basis degree must be 1 or 3");
+  if (m < 0 || (m > 0 && !opts->samples)) return setError(ctx, ITS_ERR_INVALID, "bad extra samples");
+  if (degree == 1 && m > 0)
+    return setError(ctx, ITS_ERR_INVALID, "extra sample rows need the cubic basis (degree 3)");
+  if (degree == 1) return its_operator_build(svo, mode, out);
+  if (svo->d.numVerts + m >= (1ll << 31)) return setError(ctx, ITS_ERR_INVALID, "too many rows");
+  ITS_CU(ctx, cudaSetDevice(ctx->device));
+  InArg<double> S;
+  its_status st;
+  if ((st = S.stage(ctx, m > 0 ? opts->samples : nullptr, 3 * m)) != ITS_OK) return st;
+  its_op* op = new its_op;
+  op->ctx = ctx;
+  op->svo = svo;
+  op->mode = mode;
+  op->degree = 3;
+  op->unknowns = svo->d.numVerts;
+  st = opBuild(op, svo->d.numVerts + m, cubicGen(svo->d, S.d));
   if (st != ITS_OK) {
     opRelease(op);
     cudaStreamSynchronize(ctx->stream);

@@ -9,7 +9,9 @@ struct its_op {
   its_ctx* ctx = nullptr;
   its_svo* svo = nullptr;
   int mode = 0;
-  int64_t n = 0, nnz = 0;
+  int degree = 1;          // basis degree: 1 (the reference's hats) or 3 (cubic B-splines)
+  int64_t n = 0, nnz = 0;  // rows (= stored columns: a system with extra sample rows is square-padded)
+  int64_t unknowns = 0;    // columns that are corner vertices (the rest are empty padding)
   int64_t* rowptr = nullptr;
   int32_t* col = nullptr;
   double* val = nullptr;

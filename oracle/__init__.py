@@ -64,6 +64,11 @@ def _declare(L):
         "orc_points_free": (None, [vp]),
         "orc_signed_distance": (None, [vp, i64, vp, vp, i64, vp]),
         "orc_signed_distance_bvh": (None, [vp, i64, vp, vp, i64, vp]),
+        "orc_cubic_assemble": (vp, [vp, vp, i64]),
+        "orc_cubic_eval": (None, [vp, vp, vp, i64, vp]),
+        "orc_cubic_eval_grid": (None, [vp, vp, vp, vp, i32, vp]),
+        "orc_offset_samples": (None, [vp, i64, vp, i64, dbl, vp, vp]),
+        "orc_bspline3": (None, [vp, i64, vp]),
         "orc_eval_points": (None, [vp, vp, vp, i64, vp, vp]),
         "orc_eval_brute": (None, [vp, vp, vp, i64, vp]),
         "orc_eval_grid": (None, [vp, vp, vp, vp, i32, vp]),
@@ -249,6 +254,31 @@ class Svo:
                               float(inner), float(outer), _p(vals), _p(labels))
         return vals, labels
 
+    def cubic_assemble(self, samples=None):
+        """CSR of the cubic B-spline system: one row per corner vertex, then one per extra sample
+        point; square, padded with empty columns past the last vertex."""
+        S = np.zeros((0, 3)) if samples is None else _f64(samples, (-1, 3))
+        h = lib().orc_cubic_assemble(self.h, _p(S), S.shape[0])
+        try:
+            n, nnz = lib().orc_csr_rows(h), lib().orc_csr_nnz(h)
+            rp, col, val = np.zeros(n + 1, np.int64), np.zeros(nnz, np.int32), np.zeros(nnz)
+            lib().orc_csr_get(h, _p(rp), _p(col), _p(val))
+        finally:
+            lib().orc_csr_free(h)
+        return rp, col, val
+
+    def cubic_eval(self, lam, P):
+        lam, P = _f64(lam), _f64(P, (-1, 3))
+        out = np.zeros(P.shape[0])
+        lib().orc_cubic_eval(self.h, _p(lam), _p(P), P.shape[0], _p(out))
+        return out
+
+    def cubic_eval_grid(self, lam, origin, width, R):
+        lam = _f64(lam)
+        out = np.zeros((R + 1) ** 3)
+        lib().orc_cubic_eval_grid(self.h, _p(lam), _p(_f64(origin)), _p(_f64(width)), R, _p(out))
+        return out
+
     def eval_grid(self, lam, origin, width, R):
         lam = _f64(lam)
         out = np.zeros((R + 1) ** 3)
@@ -284,6 +314,23 @@ def signed_distance_bvh(P, V, F):
     P, V, F = _f64(P), _f64(V), _i32(F)
     out = np.zeros(P.shape[0])
     lib().orc_signed_distance_bvh(_p(P), P.shape[0], _p(V), _p(F), F.shape[0], _p(out))
+    return out
+
+
+def offset_samples(V, F, eps):
+    """Offset shell samples (v + eps n, then v - eps n, n the unit area-weighted vertex normal)
+    and their targets (+eps, -eps)."""
+    V, F = _f64(V), _i32(F)
+    nv = V.shape[0]
+    pts, tgt = np.zeros((2 * nv, 3)), np.zeros(2 * nv)
+    lib().orc_offset_samples(_p(V), nv, _p(F), F.shape[0], float(eps), _p(pts), _p(tgt))
+    return pts, tgt
+
+
+def bspline3(t):
+    t = _f64(t)
+    out = np.zeros(t.shape[0])
+    lib().orc_bspline3(_p(t), t.shape[0], _p(out))
     return out
 
 

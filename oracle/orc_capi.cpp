@@ -167,6 +167,23 @@ void orc_points_free(void* p) { delete static_cast<Points*>(p); }
 void orc_signed_distance(const double* P, int64_t m, const double* V, const int32_t* F, int64_t nf, double* out) {
   signedDistance(P, m, V, F, nf, out);
 }
+void* orc_cubic_assemble(void* h, const double* samples, int64_t m) {
+  return new Csr(cubicAssemble(*static_cast<Svo*>(h), samples, m));
+}
+void orc_cubic_eval(void* h, const double* lambda, const double* P, int64_t m, double* out) {
+  cubicEval(*static_cast<Svo*>(h), lambda, P, m, out);
+}
+void orc_cubic_eval_grid(void* h, const double* lambda, const double* origin, const double* width, int R,
+                         double* out) {
+  cubicEvalGrid(*static_cast<Svo*>(h), lambda, origin, width, R, out);
+}
+void orc_offset_samples(const double* V, int64_t nv, const int32_t* F, int64_t nf, double eps, double* pts,
+                        double* tgt) {
+  offsetSamples(V, nv, F, nf, eps, pts, tgt);
+}
+void orc_bspline3(const double* t, int64_t n, double* out) {
+  for (int64_t i = 0; i < n; ++i) out[i] = bspline3(t[i]);
+}
 void orc_signed_distance_bvh(const double* P, int64_t m, const double* V, const int32_t* F, int64_t nf,
                              double* out) {
   signedDistanceBvh(P, m, V, F, nf, out);

@@ -25,6 +25,13 @@ void signedDistance(const double* P, int64_t m, const double* V, const int32_t* 
 // exact nearest-triangle distance, the sign from the fast winding number.
 void signedDistanceBvh(const double* P, int64_t m, const double* V, const int32_t* F, int64_t nf, double* out);
 double pointTriSqDist(const V3& p, const V3& a, const V3& b, const V3& c);
+// Cubic B-spline basis over the corner vertices and offset shell samples (orc_cubic.cpp).
+double bspline3(double t);
+Csr cubicAssemble(const Svo& s, const double* samples, int64_t m);
+void cubicEval(const Svo& s, const double* lambda, const double* P, int64_t m, double* out);
+void cubicEvalGrid(const Svo& s, const double* lambda, const double origin[3], const double width[3], int R,
+                   double* out);
+void offsetSamples(const double* V, int64_t nv, const int32_t* F, int64_t nf, double eps, double* pts, double* tgt);
 double solidAngle(const V3& p, const V3& a0, const V3& b0, const V3& c0);
 Csr assemble(const Svo& s);
 Csr transpose(const Csr& A);
