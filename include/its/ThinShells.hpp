@@ -67,11 +67,17 @@ class ThinShells {
   // from that start as the fallback; without it, the reference's LSCG from zero.
   void creatShell(double tol = 1e-6, int stopRule = ITS_STOP_RESIDUAL, const std::string& shareNetFile = "") {
     const int64_t nv = (int64_t)V_.size() / 3, nf = (int64_t)F_.size() / 3;
-    int64_t nPts = 0, nEdge = 0;  // cpIntersectionPoints
-    check(its_shell_samples(svo_, V_.data(), nv, F_.data(), nf, nullptr, 0, &nPts, &nEdge), ctx_, "cpIntersectionPoints");
-    interPoints_.assign(3 * nPts, 0.0);
-    check(its_shell_samples(svo_, V_.data(), nv, F_.data(), nf, interPoints_.data(), nPts, &nPts, &nEdge), ctx_,
+    int64_t nPts = 0, nEdge = 0;  // cpIntersectionPoints: one call into a generous buffer, a
+    const int64_t cap = 2 * nf + nv + 1024;  // second only when the samples exceed it
+    interPoints_.assign(3 * cap, 0.0);
+    check(its_shell_samples(svo_, V_.data(), nv, F_.data(), nf, interPoints_.data(), cap, &nPts, &nEdge), ctx_,
           "cpIntersectionPoints");
+    if (nPts > cap) {
+      interPoints_.assign(3 * nPts, 0.0);
+      check(its_shell_samples(svo_, V_.data(), nv, F_.data(), nf, interPoints_.data(), nPts, &nPts, &nEdge), ctx_,
+            "cpIntersectionPoints");
+    }
+    interPoints_.resize(3 * nPts);
     std::vector<double> pos(3 * numNodeVerts_);  // cpSDFOfTreeNodes
     check(its_svo_get_vertices(svo_, pos.data(), nullptr), ctx_, "nodeVertexArray");
     sdfVal_.assign(numNodeVerts_, 0.0);

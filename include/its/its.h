@@ -116,7 +116,9 @@ its_status its_svo_get_edges(its_svo* svo, double* p0, double* p1, uint32_t* own
 /* ---- a9: shell samples --------------------------------------------------------------- */
 /* ThinShells::cpIntersectionPoints (src/ThinShells.cpp:38-479): mesh-edge x fine-node-face
    points (sorted, unique) followed by fine-node-edge x triangle points. With out_points NULL
-   only the counts are returned; otherwise up to capacity points are written. */
+   only the counts are returned; otherwise the first min(capacity, *num_points) points are
+   written (a caller can pass a generous buffer once and call again only when *num_points
+   exceeds it). */
 its_status its_shell_samples(its_svo* svo, const double* verts, int64_t nverts, const int32_t* faces,
                              int64_t nfaces, double* out_points, int64_t capacity, int64_t* num_points,
                              int64_t* num_edge_points);

@@ -278,13 +278,18 @@ class Svo:
         return p0, p1, own
 
     def shell_samples(self, V, F):
+        """Shell samples (its_shell_samples): one call into a buffer sized for typical meshes
+        (about one sample per face), a second only when the samples exceed it."""
         V, F = _f64(V), _i32(F)
         n, ne = C.c_int64(0), C.c_int64(0)
-        self.ctx.check(lib().its_shell_samples(self.h, _ptr(V), _n(V), _ptr(F), _n(F), None, 0, C.byref(n),
+        cap = 2 * _n(F) + _n(V) + 1024
+        out = np.empty((cap, 3))
+        self.ctx.check(lib().its_shell_samples(self.h, _ptr(V), _n(V), _ptr(F), _n(F), _ptr(out), cap, C.byref(n),
                                                C.byref(ne)), "its_shell_samples")
-        out = np.zeros((max(n.value, 1), 3))
-        self.ctx.check(lib().its_shell_samples(self.h, _ptr(V), _n(V), _ptr(F), _n(F), _ptr(out), n.value,
-                                               C.byref(n), C.byref(ne)), "its_shell_samples")
+        if n.value > cap:
+            out = np.empty((n.value, 3))
+            self.ctx.check(lib().its_shell_samples(self.h, _ptr(V), _n(V), _ptr(F), _n(F), _ptr(out), n.value,
+                                                   C.byref(n), C.byref(ne)), "its_shell_samples")
         return out[:n.value], int(ne.value)
 
     def eval_points(self, lam, P, out=None):

@@ -177,4 +177,37 @@ struct OutArg {
 
 inline unsigned gridFor(int64_t n, int block) { return (unsigned)((n + block - 1) / block); }
 
+// Programmatic dependent launch: a kernel launched by launchDependent may be scheduled while
+// the kernel before it in the stream is still running, once every block of that kernel has
+// passed gridDependents(). It must call gridDependencyWait() before it reads anything earlier
+// work writes or writes anything earlier work reads; past that call all earlier work is
+// complete and visible. (Launched the ordinary way, both calls return at once.)
+__device__ __forceinline__ void gridDependencyWait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void gridDependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// dependent = false launches the ordinary way. Only a launch whose previous operation in the
+// stream is a kernel may be dependent: the relaxed ordering does not cover copies, memsets,
+// event waits or stream-ordered allocations in between.
+template <typename... KArgs, typename... Args>
+its_status launchDependent(its_ctx* ctx, bool dependent, void (*kernel)(KArgs...), dim3 grid, dim3 block,
+                           size_t smem, cudaStream_t stream, Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = dependent ? 1 : 0;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+  ctx->launches++;
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return cudaFail(ctx, e, "kernel launch");
+  }
+  return ITS_OK;
+}
+
 }  // namespace its

@@ -186,6 +186,8 @@ __global__ void __launch_bounds__(kFeatThreads) kShareFeatures(const __grid_cons
                                                                const float* __restrict__ geom,
                                                                const __grid_constant__ FeatNorm norm,
                                                                float* __restrict__ out) {
+  gridDependencyWait();
+  gridDependents();
   __shared__ __align__(16) float sf[kFeatRows][kFeat];
   const int sub = threadIdx.x & (kFeatLanes - 1), slot = threadIdx.x / kFeatLanes;
   const int64_t i0 = (int64_t)blockIdx.x * kFeatRows, i = i0 + slot;
@@ -286,6 +288,8 @@ __global__ void __launch_bounds__(kFeatThreads) kShareFeatures(const __grid_cons
 // Learned shares of the coincident vertices: share[ids[i]] = pred[i] * scale + mean.
 __global__ void kScatterShares(const int64_t* __restrict__ ids, int64_t count, const float* __restrict__ pred,
                                float scale, float mean, double* __restrict__ shares) {
+  gridDependencyWait();
+  gridDependents();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= count) return;
   shares[ids[i]] = (double)pred[i] * (double)scale + (double)mean;
@@ -417,15 +421,15 @@ its_status nodeSampleStats(its_ctx* ctx, SvoDevice& d, const double* V, const in
 // is coincident vertex i) (see the file comment); hostNorm (host memory, may be null) the
 // normalisation.
 its_status shareFeatures(its_ctx* ctx, const SvoDevice& d, const double* b, const double* lam0, const int64_t* ids,
-                         int64_t count, const float* hostNorm, float* out) {
+                         int64_t count, const float* hostNorm, float* out, bool afterKernel) {
   const FeatParams P = featParams(d);
   FeatNorm norm;
   norm.on = hostNorm != nullptr;
   for (int k = 0; k < 2 * kFeat; ++k) norm.v[k] = hostNorm ? hostNorm[k] : 0.0f;
   if (count > 0) {
-    kShareFeatures<<<gridFor(count, kFeatRows), kFeatThreads, 0, ctx->stream>>>(P, ids, count, b, lam0, d.coincGeom,
-                                                                                norm, out);
-    ITS_LAUNCHED(ctx);
+    its_status st = launchDependent(ctx, afterKernel, kShareFeatures, gridFor(count, kFeatRows), kFeatThreads, 0, ctx->stream, P, ids,
+                                    count, b, lam0, (const float*)d.coincGeom, norm, out);
+    if (st != ITS_OK) return st;
   }
   return ITS_OK;
 }
@@ -434,8 +438,9 @@ its_status shareFeatures(its_ctx* ctx, const SvoDevice& d, const double* b, cons
 its_status scatterShares(its_ctx* ctx, const int64_t* ids, int64_t count, const float* pred, float scale, float mean,
                          double* shares) {
   if (count > 0) {
-    kScatterShares<<<gridFor(count, 256), 256, 0, ctx->stream>>>(ids, count, pred, scale, mean, shares);
-    ITS_LAUNCHED(ctx);
+    its_status st = launchDependent(ctx, true, kScatterShares, gridFor(count, 256), 256, 0, ctx->stream, ids, count, pred, scale,
+                                    mean, shares);
+    if (st != ITS_OK) return st;
   }
   return ITS_OK;
 }
@@ -444,13 +449,15 @@ its_status scatterShares(its_ctx* ctx, const int64_t* ids, int64_t count, const 
 
 namespace its {
 its_status exactStart(its_ctx* ctx, its_svo* const* svos, int64_t count, const double* const* b,
-                      const double* const* shares, double* const* lam);
+                      const double* const* shares, double* const* lam, bool afterKernel, double* gScratch);
 }
 
 using namespace its;
 
 namespace its {
-its_status mlpInfer(its_mlp* mlp, const float* X, int64_t n, float* out);
+its_status mlpInfer(its_mlp* mlp, const float* X, int64_t n, float* out, bool afterKernel);
+its_status mlpInferShares(its_mlp* h, const float* X, int64_t n, const int64_t* ids, float scale, float mean,
+                          double* shares, bool afterKernel);
 its_status mlpCheck(its_mlp* mlp);
 }  // namespace its
 
@@ -480,7 +487,7 @@ its_status learnedStart(its_ctx* ctx, its_svo* const* svos, int64_t count, its_m
   std::vector<const double*> sp(count);
   std::vector<double*> l0(count);
   std::vector<int64_t> cnt(count);
-  int64_t total = 0;
+  int64_t total = 0, verts = 0;
   for (int64_t m = 0; m < count; ++m) {
     const int64_t n = svos[m]->d.numVerts;
     if ((st = lam0[m].alloc(ctx, n)) != ITS_OK || (st = shares[m].alloc(ctx, n)) != ITS_OK) return st;
@@ -488,28 +495,39 @@ its_status learnedStart(its_ctx* ctx, its_svo* const* svos, int64_t count, its_m
     sp[m] = shares[m].p;
     cnt[m] = svos[m]->d.numCoinc;
     total += cnt[m];
+    verts += n;
   }
-  if ((st = exactStart(ctx, svos, count, b, nullptr, l0.data())) != ITS_OK) return st;
+  // every buffer up front: from the first kernel on, each launch follows a kernel (dependent
+  // launches, gridDependencyWait at the top of each kernel)
   DevBuf<float> feat, pred;
+  DevBuf<double> G;
   if ((st = feat.alloc(ctx, std::max<int64_t>(total, 1) * kFeat)) != ITS_OK ||
-      (st = pred.alloc(ctx, std::max<int64_t>(total, 1))) != ITS_OK)
+      (st = pred.alloc(ctx, std::max<int64_t>(total, 1))) != ITS_OK ||
+      (st = G.alloc(ctx, std::max<int64_t>(verts, 1))) != ITS_OK)
     return st;
+  if ((st = exactStart(ctx, svos, count, b, nullptr, l0.data(), false, nullptr)) != ITS_OK) return st;
   int64_t off = 0;
   for (int64_t m = 0; m < count; ++m) {
-    if ((st = shareFeatures(ctx, svos[m]->d, b[m], l0[m], svos[m]->d.coincIds, cnt[m], hn, feat.p + off * kFeat)) !=
-        ITS_OK)
+    if ((st = shareFeatures(ctx, svos[m]->d, b[m], l0[m], svos[m]->d.coincIds, cnt[m], hn, feat.p + off * kFeat,
+                            true)) != ITS_OK)
       return st;
     off += cnt[m];
   }
-  if (total > 0 && (st = mlpInfer(mlp, feat.p, total, pred.p)) != ITS_OK) return st;
-  off = 0;
-  for (int64_t m = 0; m < count; ++m) {
-    if ((st = scatterShares(ctx, svos[m]->d.coincIds, cnt[m], pred.p + off, hn[2 * kFeat + 1], hn[2 * kFeat],
-                            shares[m].p)) != ITS_OK)
+  if (count == 1) {  // one octree: the network writes the shares itself
+    if (total > 0 && (st = mlpInferShares(mlp, feat.p, total, svos[0]->d.coincIds, hn[2 * kFeat + 1], hn[2 * kFeat],
+                                          shares[0].p, true)) != ITS_OK)
       return st;
-    off += cnt[m];
+  } else {
+    if (total > 0 && (st = mlpInfer(mlp, feat.p, total, pred.p, true)) != ITS_OK) return st;
+    off = 0;
+    for (int64_t m = 0; m < count; ++m) {
+      if ((st = scatterShares(ctx, svos[m]->d.coincIds, cnt[m], pred.p + off, hn[2 * kFeat + 1], hn[2 * kFeat],
+                              shares[m].p)) != ITS_OK)
+        return st;
+      off += cnt[m];
+    }
   }
-  return exactStart(ctx, svos, count, b, sp.data(), lam);
+  return exactStart(ctx, svos, count, b, sp.data(), lam, total > 0, G.p);
 }
 
 }  // namespace its
@@ -543,10 +561,10 @@ its_status its_share_features(its_svo* svo, const double* b, const float* norm, 
   if ((st = lam0.alloc(ctx, n)) != ITS_OK) return st;
   const double* bp = db.d;
   double* lp = lam0.p;
-  if ((st = exactStart(ctx, &svo, 1, &bp, nullptr, &lp)) != ITS_OK) return st;
+  if ((st = exactStart(ctx, &svo, 1, &bp, nullptr, &lp, false, nullptr)) != ITS_OK) return st;
   OutArg<float> out;
   if ((st = out.stage(ctx, features, cnt * kFeat)) != ITS_OK) return st;
-  if ((st = shareFeatures(ctx, d, db.d, lam0.p, dIds, cnt, norm ? hn : nullptr, out.d)) != ITS_OK) return st;
+  if ((st = shareFeatures(ctx, d, db.d, lam0.p, dIds, cnt, norm ? hn : nullptr, out.d, false)) != ITS_OK) return st;
   if ((st = out.finish(ctx)) != ITS_OK) return st;
   if (ids) ITS_CU(ctx, cudaMemcpyAsync(ids, dIds, cnt * 8, cudaMemcpyDefault, ctx->stream));
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));

@@ -27,7 +27,8 @@ namespace its {
 its_status learnedStart(its_ctx* ctx, its_svo* const* svos, int64_t count, its_mlp* mlp, const double* const* b,
                         const float* hn, double* const* lam);
 its_status fitResidualEnqueue(its_ctx* ctx, its_svo* const* svos, int64_t count, const double* const* b,
-                              const double* const* lam, double* relDev, const int* flagSrc, int* flagDst);
+                              const double* const* lam, double* relDev, const int* flagSrc, int* flagDst,
+                              bool afterKernel);
 its_status hostNorm(its_ctx* ctx, const float* norm, float* hn);
 const int* mlpErrFlag(its_mlp* mlp);
 uint64_t mlpUid(const its_mlp* mlp);
@@ -126,8 +127,9 @@ static its_status enqueueFit(its_svo* svo, LearnedPlan* p, its_mlp* mlp, const d
     ITS_CU(ctx, cudaMemcpyAsync(lamHost, lam, n * 8, cudaMemcpyDeviceToHost, p->side));
     ITS_CU(ctx, cudaEventRecord(p->join, p->side));
   }
-  if ((st = fitResidualEnqueue(ctx, &svo, 1, &b, &lam, p->relMapped, mlpErrFlag(mlp), (int*)(p->relMapped + 1))) !=
-      ITS_OK)
+  // the residual follows the start's last kernel directly unless lambda's copy forks off first
+  if ((st = fitResidualEnqueue(ctx, &svo, 1, &b, &lam, p->relMapped, mlpErrFlag(mlp), (int*)(p->relMapped + 1),
+                               lamHost == nullptr)) != ITS_OK)
     return st;
   if (lamHost) ITS_CU(ctx, cudaStreamWaitEvent(ctx->stream, p->join, 0));
   return ITS_OK;

@@ -153,6 +153,8 @@ struct EpiHidden {
   }
 };
 
+constexpr int kOutParts = 4;  // partial sums of the output unit (one per quarter of the columns)
+
 // Last hidden layer plus the output unit. Inference: out = sum_j h_j w4_j + b4. Training also
 // forms the loss gradient d = scale (out - y) and dZ3 = d w4 gelu'(z3), the stored H3 (for
 // the w4 gradient) and the per-row squared error.
@@ -171,14 +173,25 @@ struct EpiOutput {
   float* dOut;
   float* sqErr;
   __device__ void operator()(int64_t m, float (&acc)[kHid]) const {
-    float o = 0.0f;
+    // the output unit sums each quarter of the columns in order, then the four partial sums
+    // in order (the fused inference kernel's per-warp-group split; both give the same bits)
+    float part[kOutParts];
 #pragma unroll
-    for (int j = 0; j < kHid; ++j) {
-      acc[j] += bias[j];
-      const float h = __bfloat162float(__float2bfloat16_rn(geluF(acc[j])));
-      if (H3) H3[m * kHid + j] = __float2bfloat16_rn(h);
-      o += h * w4[j];
+    for (int g = 0; g < kOutParts; ++g) {
+      float o = 0.0f;
+#pragma unroll
+      for (int jj = 0; jj < kHid / kOutParts; ++jj) {
+        const int j = g * (kHid / kOutParts) + jj;
+        acc[j] += bias[j];
+        const float h = __bfloat162float(__float2bfloat16_rn(geluF(acc[j])));
+        if (H3) H3[m * kHid + j] = __float2bfloat16_rn(h);
+        o += h * w4[j];
+      }
+      part[g] = o;
     }
+    float o = part[0];
+#pragma unroll
+    for (int g = 1; g < kOutParts; ++g) o += part[g];
     o += b4[0];
     if (out) out[m] = o;
     if (!y) return;
@@ -235,8 +248,10 @@ constexpr int kFusedGroups = 4;                                // warp groups pe
 constexpr int kSlotThreads = 128 * kFusedGroups;
 constexpr int kFusedThreads = kSlotThreads * kFusedSlots;
 constexpr int kGroupCols = 128 / kFusedGroups;
+static_assert(kFusedGroups == kOutParts, "the output unit's partial sums follow the warp groups");
 constexpr int kFusedSmem = 16384 /*W1*/ + 32768 /*W2*/ + 32768 /*W3*/ + kFusedSlots * (16384 /*X*/ + 32768 /*H*/) +
-                           64 + 1024;
+                           4 * 128 * 4 /*b1 b2 b3 w4*/ + kFusedSlots * kFusedGroups * 128 * 4 /*partial sums*/ + 64 +
+                           1024;
 
 __device__ __forceinline__ void loadWeightTile(uint8_t* dst, const bf16* __restrict__ W, int K, int tid, int nthreads) {
   // W: 128 rows x K bf16, row-major (K-major B operand); K/64 swizzled blocks of 128 x 128 B
@@ -254,13 +269,14 @@ __device__ __forceinline__ void slotSync(int s) {
 // Share-network inference: persistent, one CTA per SM, two 128-row tiles in flight. A tile's
 // 512 threads load its features, one of them issues each layer's MMAs, and the four warp
 // groups run the epilogue of a quarter of the 128 columns each (thread = row, the TMEM lane of
-// its warp). The output unit sums the columns in order: the later quarters' activations (BF16,
-// as the sum uses them) go through shared memory to the first group's threads, so the result
-// is the layer-by-layer kernels' bit for bit.
+// its warp). Biases and output weights sit in shared memory. The output unit sums each
+// group's quarter of the columns in order and the first group adds the four partial sums in
+// order, as the layer-by-layer kernels do, so the result is theirs bit for bit.
 __global__ void __launch_bounds__(kFusedThreads, 1)
     kMlpForwardFused(const float* __restrict__ X, int64_t n, const bf16* __restrict__ W1, const bf16* __restrict__ W2,
                      const bf16* __restrict__ W3, const float* __restrict__ P, const float* __restrict__ w4r,
-                     float* __restrict__ out, int* __restrict__ err) {
+                     float* __restrict__ out, int* __restrict__ err, const int64_t* __restrict__ shareIds,
+                     double* __restrict__ shares, float shareScale, float shareMean) {
   using namespace umma;
   extern __shared__ uint8_t smemRaw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smemRaw + 1023) & ~(uintptr_t)1023);
@@ -271,15 +287,21 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
             warp = tid >> 5;
   uint8_t* sX = sW3 + 32768 + s * (16384 + 32768);
   uint8_t* sH = sX + 16384;
-  constexpr int kOutStride = 2 * (128 - kGroupCols) + 16;  // bytes per row of the later groups' output activations
-  uint64_t* mbar = (uint64_t*)(sW3 + 32768 + kFusedSlots * (16384 + 32768));
+  float* sBias = (float*)(sW3 + 32768 + kFusedSlots * (16384 + 32768));  // b1, b2, b3, w4 (128 each)
+  float* sPart = sBias + 4 * 128 + s * kFusedGroups * 128;               // [group][row] partial sums
+  uint64_t* mbar = (uint64_t*)(sBias + 4 * 128 + kFusedSlots * kFusedGroups * 128);
   uint32_t* tslot = (uint32_t*)(mbar + kFusedSlots);
   if (warp == 0) tmemAlloc(smemAddr(tslot), 128 * kFusedSlots);
   if (tid == 0)
     for (int k = 0; k < kFusedSlots; ++k) mbarInit(smemAddr(mbar + k), 1);
+  for (int i = tid; i < 4 * 128; i += blockDim.x)
+    sBias[i] = i < 384 ? P[(i < 128 ? kOffB1 : (i < 256 ? kOffB2 : kOffB3)) + (i & 127)] : w4r[i - 384];
   loadWeightTile(sW1, W1, kIn, tid, blockDim.x);
   loadWeightTile(sW2, W2, kHid, tid, blockDim.x);
   loadWeightTile(sW3, W3, kHid, tid, blockDim.x);
+  // the weights were written before the previous kernel started; the features are its output
+  gridDependencyWait();
+  gridDependents();
   fenceBefore();
   __syncthreads();
   fenceAfter();
@@ -289,9 +311,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   const uint32_t bar = smemAddr(mbar + s);
   uint32_t phase = 0;
   bool ok = true;
-  const float* b1 = P + kOffB1;
-  const float* b2 = P + kOffB2;
-  const float* b3 = P + kOffB3;
+  const float* b1 = sBias;
+  const float* b2 = sBias + 128;
+  const float* b3 = sBias + 256;
+  const float* w4 = sBias + 384;
   const int64_t tiles = (n + 127) / 128;
   const bool xVec = ((uintptr_t)X & 15) == 0;  // rows are 256 B apart: 16-byte loads when the base allows
   for (int64_t t = (int64_t)blockIdx.x * kFusedSlots + s; t < tiles; t += (int64_t)gridDim.x * kFusedSlots) {
@@ -358,26 +381,25 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
             const int c = (n0 >> 3) + h;
             *(uint4*)(sH + (c >> 3) * 16384 + swizzledChunk(row, c & 7)) = *(const uint4*)q;
           }
-        } else if (grp == 0) {  // output unit, columns in order
+        } else {  // output unit: this group's quarter of the columns, in order
 #pragma unroll
           for (int j = 0; j < 16; ++j)
-            o += __bfloat162float(__float2bfloat16_rn(geluF(v[j] + bias[n0 + j]))) * w4r[n0 + j];
-        } else {  // the later groups' activations for the first group's sum (layer 2 has read sH)
-          __align__(16) bf16 q[16];
-#pragma unroll
-          for (int j = 0; j < 16; ++j) q[j] = __float2bfloat16_rn(geluF(v[j] + bias[n0 + j]));
-          uint4* dst = (uint4*)(sH + row * kOutStride + (n0 - kGroupCols) * 2);
-          dst[0] = ((const uint4*)q)[0];
-          dst[1] = ((const uint4*)q)[1];
+            o += __bfloat162float(__float2bfloat16_rn(geluF(v[j] + bias[n0 + j]))) * w4[n0 + j];
         }
       }
     }
+    if (grp > 0) sPart[grp * 128 + row] = o;
     slotSync(s);
     if (grp == 0) {
-      const bf16* a = (const bf16*)(sH + row * kOutStride);
-#pragma unroll 8
-      for (int j = 0; j < 128 - kGroupCols; ++j) o += __bfloat162float(a[j]) * w4r[kGroupCols + j];
-      if (m < n && ok) out[m] = o + P[kOffB4];
+#pragma unroll
+      for (int g = 1; g < kFusedGroups; ++g) o += sPart[g * 128 + row];
+      if (m < n && ok) {
+        const float pred = o + P[kOffB4];
+        if (shares)  // the learned start's share of coincident vertex shareIds[m], de-normalised
+          shares[shareIds[m]] = (double)pred * (double)shareScale + (double)shareMean;
+        else
+          out[m] = pred;
+      }
     }
     fenceBefore();
     slotSync(s);  // TMEM read and sH free before the next tile
@@ -640,15 +662,24 @@ static its_status checkErr(its_mlp* h) {
 
 // Predictions for n device rows into device out, launched on the context's stream without
 // waiting (the caller checks the error flag at its next synchronisation).
-its_status mlpInfer(its_mlp* h, const float* X, int64_t n, float* out) {
+static its_status launchFused(its_mlp* h, const float* X, int64_t n, float* out, const int64_t* ids, double* shares,
+                              float scale, float mean, bool afterKernel) {
   its_ctx* ctx = h->ctx;
   if (n <= 0) return ITS_OK;
   const int64_t tiles = (n + 127) / 128, ctas = (tiles + kFusedSlots - 1) / kFusedSlots;
   const unsigned grid = (unsigned)(ctas < ctx->numSMs ? ctas : ctx->numSMs);
-  kMlpForwardFused<<<grid, kFusedThreads, kFusedSmem, ctx->stream>>>(X, n, h->W1, h->W2, h->W3, h->P, h->w4r, out,
-                                                                      h->err);
-  ITS_LAUNCHED(ctx);
-  return ITS_OK;
+  return launchDependent(ctx, afterKernel, kMlpForwardFused, grid, kFusedThreads, kFusedSmem, ctx->stream, X, n,
+                         (const bf16*)h->W1, (const bf16*)h->W2, (const bf16*)h->W3, (const float*)h->P,
+                         (const float*)h->w4r, out, h->err, ids, shares, scale, mean);
+}
+its_status mlpInfer(its_mlp* h, const float* X, int64_t n, float* out, bool afterKernel) {
+  return launchFused(h, X, n, out, nullptr, nullptr, 0.0f, 0.0f, afterKernel);
+}
+// The same predictions written as shares: shares[ids[m]] = pred[m] * scale + mean (in FP64,
+// as the share scatter of the learned start computes it).
+its_status mlpInferShares(its_mlp* h, const float* X, int64_t n, const int64_t* ids, float scale, float mean,
+                          double* shares, bool afterKernel) {
+  return launchFused(h, X, n, nullptr, ids, shares, scale, mean, afterKernel);
 }
 
 its_status mlpCheck(its_mlp* h) { return checkErr(h); }
@@ -735,7 +766,7 @@ its_status its_mlp_forward(its_mlp* h, const float* X, int64_t n, float* out) {
   its_status st;
   if ((st = x.stage(ctx, X, n * kIn)) != ITS_OK) return st;
   if ((st = o.stage(ctx, out, n)) != ITS_OK) return st;
-  if ((st = mlpInfer(h, x.d, n, o.d)) != ITS_OK) return st;
+  if ((st = mlpInfer(h, x.d, n, o.d, false)) != ITS_OK) return st;
   if ((st = o.finish(ctx)) != ITS_OK) return st;
   return checkErr(h);
 }
@@ -748,7 +779,7 @@ its_status its_mlp_forward_async(its_mlp* h, const float* X, int64_t n, float* o
   if (n > 0 && (!isDevicePtr(ctx, X) || !isDevicePtr(ctx, out)))
     return setError(ctx, ITS_ERR_INVALID, "its_mlp_forward_async: features and output must be device memory");
   ITS_CU(ctx, cudaSetDevice(ctx->device));
-  return mlpInfer(h, X, n, out);
+  return mlpInfer(h, X, n, out, false);
 }
 
 // Waits for the context's stream and reports the network's error flag.

@@ -11,6 +11,7 @@
 // coordinates lie in the triangle's box; candidates are therefore enumerated on the fine
 // lattice around the box (one cell of margin) and checked against the fine-edge bitmap, then
 // the reference's own window and intersection tests decide. Same points, no slab sweep.
+#include <algorithm>
 #include <cmath>
 
 #include "its_scan.cuh"
@@ -373,12 +374,24 @@ its_status its_shell_samples(its_svo* s, const double* verts, int64_t nverts, co
   *num_points = total;
   if (num_edge_points) *num_edge_points = nEdge;
   if (!out_points) return ITS_OK;
-  if (capacity < total) return setError(ctx, ITS_ERR_INVALID, "its_shell_samples: capacity too small");
+  if (capacity < 0) return setError(ctx, ITS_ERR_INVALID, "its_shell_samples: negative capacity");
+  // the first min(capacity, total) points: straight into the output when it holds them all,
+  // else through a full-size scratch
+  const int64_t keep = std::min<int64_t>(capacity, total);
   OutArg<double> O;
-  if ((st = O.stage(ctx, out_points, 3 * total)) != ITS_OK) return st;
-  if (nEdge) ITS_CU(ctx, cudaMemcpyAsync(O.d, edgePts.p, (size_t)nEdge * 24, cudaMemcpyDeviceToDevice, ctx->stream));
-  if ((st = scanExclusiveAlloc<uint32_t>(ctx, fs, nfaces, FaceEmit{fs, O.d + 3 * (int64_t)nEdge}, tot.p + 2)) != ITS_OK)
+  if ((st = O.stage(ctx, out_points, 3 * keep)) != ITS_OK) return st;
+  DevBuf<double> all;
+  double* dst = O.d;
+  if (keep < total) {
+    if ((st = all.alloc(ctx, 3 * total)) != ITS_OK) return st;
+    dst = all.p;
+  }
+  if (nEdge && dst) ITS_CU(ctx, cudaMemcpyAsync(dst, edgePts.p, (size_t)nEdge * 24, cudaMemcpyDeviceToDevice, ctx->stream));
+  if (dst && (st = scanExclusiveAlloc<uint32_t>(ctx, fs, nfaces, FaceEmit{fs, dst + 3 * (int64_t)nEdge}, tot.p + 2)) !=
+                 ITS_OK)
     return st;
+  if (keep < total && keep > 0)
+    ITS_CU(ctx, cudaMemcpyAsync(O.d, all.p, (size_t)keep * 24, cudaMemcpyDeviceToDevice, ctx->stream));
   if ((st = O.finish(ctx)) != ITS_OK) return st;
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   return ITS_OK;

@@ -105,6 +105,8 @@ static its_status makeSegArgs(its_ctx* ctx, const std::vector<Seg>& segs, const 
 
 // G_r = b_r - the shares of the finer coincident vertices at r's point (finest first).
 __global__ void __launch_bounds__(256) kStartValues(const __grid_constant__ SegArgs<RowSeg> A, int64_t total) {
+  gridDependencyWait();
+  gridDependents();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= total) return;
   const int k = A.find(i);
@@ -122,6 +124,8 @@ __global__ void __launch_bounds__(256) kStartValues(const __grid_constant__ SegA
 // lambda_r: the share of a coincident vertex; otherwise G_r less the interpolant of G over
 // the corners of the owner's parent cell (the row's hats of that depth, in column order).
 __global__ void __launch_bounds__(256) kStartInterp(const __grid_constant__ SegArgs<RowSeg> A, int64_t total) {
+  gridDependencyWait();
+  gridDependents();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= total) return;
   const int k = A.find(i);
@@ -166,6 +170,8 @@ struct ResSeg {
 // The finest depth: one row per thread, H interpolated from the parent cell's corners.
 __global__ void __launch_bounds__(kResThreads) kResidualFine(const __grid_constant__ SegArgs<ResSeg> A,
                                                             double* __restrict__ part) {
+  gridDependencyWait();
+  gridDependents();
   const int k = A.find(blockIdx.x);
   const ResSeg& s = A.seg(k);
   const int64_t j = blockIdx.x - A.pre(k);
@@ -217,6 +223,8 @@ constexpr int kResCoarseRows = 32;
 constexpr int kResWarps = kResThreads / 32;
 __global__ void __launch_bounds__(kResThreads) kResidualCoarse(const __grid_constant__ SegArgs<ResSeg> A,
                                                               double* __restrict__ part) {
+  gridDependencyWait();
+  gridDependents();
   __shared__ double sacc[kResWarps][kResCoarseRows];
   __shared__ double schain[kResCoarseRows];
   const int k = A.find(blockIdx.x);
@@ -281,6 +289,8 @@ struct SlotArgs {
 __global__ void __launch_bounds__(kResThreads) kResidualFinish(const double* __restrict__ part,
                                                                const __grid_constant__ SlotArgs F,
                                                                double* __restrict__ rel) {
+  gridDependencyWait();
+  gridDependents();
   const int64_t m = blockIdx.x;
   if (m == 0 && threadIdx.x == 0 && F.flagSrc) *F.flagDst = *F.flagSrc;
   double a = 0.0, c = 0.0;
@@ -307,7 +317,7 @@ static const RowParams* rowParamsOf(its_svo* s) { return (const RowParams*)s->d.
 // Exact starts of count octrees (device vectors), matrix-free: G (when there are shares),
 // then lambda, each one launch for all octrees together.
 its_status exactStart(its_ctx* ctx, its_svo* const* svos, int64_t count, const double* const* b,
-                      const double* const* shares, double* const* lam) {
+                      const double* const* shares, double* const* lam, bool afterKernel, double* gScratch) {
   its_status st;
   bool anyShares = false;
   int64_t total = 0;
@@ -316,7 +326,8 @@ its_status exactStart(its_ctx* ctx, its_svo* const* svos, int64_t count, const d
     total += svos[m]->d.numVerts;
   }
   DevBuf<double> G;
-  if (anyShares && (st = G.alloc(ctx, std::max<int64_t>(total, 1))) != ITS_OK) return st;
+  if (anyShares && !gScratch && (st = G.alloc(ctx, std::max<int64_t>(total, 1))) != ITS_OK) return st;
+  double* g = gScratch ? gScratch : G.p;
   std::vector<RowSeg> segs;
   std::vector<int64_t> prefix;
   int64_t acc = 0;
@@ -329,7 +340,7 @@ its_status exactStart(its_ctx* ctx, its_svo* const* svos, int64_t count, const d
     s.rows = n;
     s.b = b[m];
     s.shares = shares ? shares[m] : nullptr;
-    s.g = anyShares ? G.p + acc : const_cast<double*>(b[m]);  // no shares anywhere: G = b
+    s.g = anyShares ? g + acc : const_cast<double*>(b[m]);  // no shares anywhere: G = b
     s.lam = lam[m];
     segs.push_back(s);
     prefix.push_back(acc);
@@ -340,12 +351,15 @@ its_status exactStart(its_ctx* ctx, its_svo* const* svos, int64_t count, const d
   SegArgs<RowSeg> A;
   DevBuf<uint8_t> keep;
   if ((st = makeSegArgs(ctx, segs, prefix, A, keep)) != ITS_OK) return st;
+  // dependent launches only straight after a kernel (no segment table copied in between)
+  const bool dep = afterKernel && !A.dsegs;
   if (anyShares) {
-    kStartValues<<<gridFor(total, 256), 256, 0, ctx->stream>>>(A, total);
-    ITS_LAUNCHED(ctx);
+    if ((st = launchDependent(ctx, dep, kStartValues, gridFor(total, 256), 256, 0, ctx->stream, A, total)) != ITS_OK)
+      return st;
   }
-  kStartInterp<<<gridFor(total, 256), 256, 0, ctx->stream>>>(A, total);
-  ITS_LAUNCHED(ctx);
+  if ((st = launchDependent(ctx, anyShares || dep, kStartInterp, gridFor(total, 256), 256, 0, ctx->stream, A,
+                            total)) != ITS_OK)
+    return st;
   return ITS_OK;  // a copied table came from pageable memory (staged at the call)
 }
 
@@ -353,7 +367,8 @@ its_status exactStart(its_ctx* ctx, its_svo* const* svos, int64_t count, const d
 // (device), each mesh's sum in a fixed order: two bands, then the sums; queued on the
 // context's stream without a host wait.
 its_status fitResidualEnqueue(its_ctx* ctx, its_svo* const* svos, int64_t count, const double* const* b,
-                              const double* const* lam, double* relDev, const int* flagSrc, int* flagDst) {
+                              const double* const* lam, double* relDev, const int* flagSrc, int* flagDst,
+                              bool afterKernel) {
   its_status st;
   int64_t total = 0;
   for (int64_t m = 0; m < count; ++m) total += svos[m]->d.numVerts;
@@ -410,18 +425,24 @@ its_status fitResidualEnqueue(its_ctx* ctx, its_svo* const* svos, int64_t count,
   }
   DevBuf<double> part;
   if ((st = part.alloc(ctx, 2 * std::max<int64_t>(slots, 1))) != ITS_OK) return st;
+  // the coarse band first: the finest rows interpolate the H values it writes
   if (chunks[0]) {
-    kResidualCoarse<<<(unsigned)chunks[0], kResThreads, 0, ctx->stream>>>(A[0], part.p);
-    ITS_LAUNCHED(ctx);
+    // dependent only straight after the caller's kernel (no table copied in between)
+    const bool dep = afterKernel && !A[0].dsegs && !F.dfirst;
+    if ((st = launchDependent(ctx, dep, kResidualCoarse, (unsigned)chunks[0], kResThreads, 0, ctx->stream, A[0],
+                              part.p)) != ITS_OK)
+      return st;
   }
   for (int band = 1; band < kBands; ++band) {
     if (!chunks[band]) continue;
-    kResidualFine<<<(unsigned)chunks[band], kResThreads, 0, ctx->stream>>>(A[band], part.p);
-    ITS_LAUNCHED(ctx);
+    if ((st = launchDependent(ctx, chunks[0] > 0, kResidualFine, (unsigned)chunks[band], kResThreads, 0, ctx->stream,
+                              A[band], part.p)) != ITS_OK)
+      return st;
   }
   if (!slots) ITS_CU(ctx, cudaMemsetAsync(part.p, 0, 16, ctx->stream));
-  kResidualFinish<<<(unsigned)count, kResThreads, 0, ctx->stream>>>(part.p, F, relDev);
-  ITS_LAUNCHED(ctx);
+  if ((st = launchDependent(ctx, slots > 0, kResidualFinish, (unsigned)count, kResThreads, 0, ctx->stream, (const double*)part.p,
+                            F, relDev)) != ITS_OK)
+    return st;
   return ITS_OK;
 }
 
@@ -431,7 +452,7 @@ its_status fitResidual(its_ctx* ctx, its_svo* const* svos, int64_t count, const 
   its_status st;
   DevBuf<double> dRel;
   if ((st = dRel.alloc(ctx, count)) != ITS_OK) return st;
-  if ((st = fitResidualEnqueue(ctx, svos, count, b, lam, dRel.p, nullptr, nullptr)) != ITS_OK) return st;
+  if ((st = fitResidualEnqueue(ctx, svos, count, b, lam, dRel.p, nullptr, nullptr, false)) != ITS_OK) return st;
   ITS_CU(ctx, cudaMemcpyAsync(rel, dRel.p, count * 8, cudaMemcpyDeviceToHost, ctx->stream));
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   return ITS_OK;
@@ -478,7 +499,7 @@ its_status its_exact_start_batch(its_svo* const* svos, int64_t count, const doub
     db[m] = B[m].d;
     dl[m] = L[m].d;
   }
-  if ((st = exactStart(ctx, svos, count, db.data(), ds.data(), dl.data())) != ITS_OK) return st;
+  if ((st = exactStart(ctx, svos, count, db.data(), ds.data(), dl.data(), false, nullptr)) != ITS_OK) return st;
   bool host = false;
   for (int64_t m = 0; m < count; ++m) {
     host = host || L[m].host;
