@@ -34,6 +34,26 @@ struct BvhDevice {
   unsigned* flag = nullptr;
 };
 
+// The traversal's view of the tree: one 128-byte record per node, so a visit touches one
+// cache line. Internal nodes carry their box, the fast winding number's expansion centre
+// (area-weighted centroid sum / area), squared radius, normal sum and area, and the children;
+// leaves carry their box and their triangle's corners. The values are those the traversal
+// used to form per visit from the build's arrays (same operations), so results are unchanged.
+struct __align__(128) BvhNode {
+  double lo[3], hi[3];
+  union {
+    struct {
+      double c[3];
+      double r2;
+      double an[3];
+      double area;
+      int32_t left, right;
+    } in;
+    double tri[9];
+  };
+};
+static_assert(sizeof(BvhNode) == 128, "one cache line per node");
+
 __global__ void kCentroidBounds(const double* __restrict__ V, const int32_t* __restrict__ F, int64_t nf,
                                 double* __restrict__ partial) {
   double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
@@ -160,6 +180,42 @@ __global__ void kBottomUp(const double* __restrict__ V, const int32_t* __restric
   }
 }
 
+__global__ void kPackNodes(const double* __restrict__ V, const int32_t* __restrict__ F, BvhDevice B,
+                           BvhNode* __restrict__ out) {
+  const int64_t n = B.nf;
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= 2 * n - 1) return;
+  BvhNode r;
+  for (int a = 0; a < 3; ++a) {
+    r.lo[a] = B.lo[3 * k + a];
+    r.hi[a] = B.hi[3 * k + a];
+  }
+  if (k >= n - 1) {  // leaf: its triangle's corners
+    const uint32_t t = B.leafTri[k - (n - 1)];
+    for (int c = 0; c < 3; ++c)
+      for (int a = 0; a < 3; ++a) r.tri[3 * c + a] = V[3 * (int64_t)F[3 * t + c] + a];
+  } else {
+    const double A = B.area[k];
+    r.in.area = A;
+    r.in.r2 = 0.0;
+    for (int a = 0; a < 3; ++a) {
+      r.in.an[a] = B.an[3 * k + a];
+      r.in.c[a] = A > 0.0 ? B.ac[3 * k + a] / A : 0.0;
+    }
+    if (A > 0.0) {
+      double r2 = 0.0;
+      for (int a = 0; a < 3; ++a) {
+        const double e = fmax(r.in.c[a] - r.lo[a], r.hi[a] - r.in.c[a]);
+        r2 += e * e;
+      }
+      r.in.r2 = r2;
+    }
+    r.in.left = B.left[k];
+    r.in.right = B.right[k];
+  }
+  out[k] = r;
+}
+
 __device__ inline double boxDist2(const double* lo, const double* hi, const double* q) {
   double s = 0.0;
   for (int a = 0; a < 3; ++a) {
@@ -169,21 +225,16 @@ __device__ inline double boxDist2(const double* lo, const double* hi, const doub
   return s;
 }
 
-__global__ void __launch_bounds__(128) kSdfBvh(const double* __restrict__ P, int64_t m, const double* __restrict__ V,
-                                               const int32_t* __restrict__ F, BvhDevice B, double* __restrict__ out,
-                                               unsigned* __restrict__ overflow) {
+__global__ void __launch_bounds__(128) kSdfBvh(const double* __restrict__ P, int64_t m, const BvhNode* __restrict__ N,
+                                               int64_t n, double* __restrict__ out, unsigned* __restrict__ overflow) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= m) return;
-  const int64_t n = B.nf;
   const double q[3] = {P[3 * i], P[3 * i + 1], P[3 * i + 2]};
   const D3 qd{q[0], q[1], q[2]};
   auto nodeOf = [n](int32_t c) -> int64_t { return c < 0 ? (n - 1) + (-c - 1) : c; };
   auto tri = [&](int64_t node, D3* t) {
-    const uint32_t ti = B.leafTri[node - (n - 1)];
-    for (int c = 0; c < 3; ++c) {
-      const int32_t vi = F[3 * ti + c];
-      t[c] = D3{V[3 * vi], V[3 * vi + 1], V[3 * vi + 2]};
-    }
+    const double* v = N[node].tri;
+    for (int c = 0; c < 3; ++c) t[c] = D3{v[3 * c], v[3 * c + 1], v[3 * c + 2]};
   };
   // exact unsigned distance
   double best = 1.7976931348623157e308;
@@ -197,12 +248,12 @@ __global__ void __launch_bounds__(128) kSdfBvh(const double* __restrict__ P, int
     stack[sp++] = 0;
     while (sp > 0) {
       const int64_t node = stack[--sp];
-      if (boxDist2(B.lo + 3 * node, B.hi + 3 * node, q) > best * (1.0 + 1e-12)) continue;
-      const int32_t c[2] = {B.left[node], B.right[node]};
+      if (boxDist2(N[node].lo, N[node].hi, q) > best * (1.0 + 1e-12)) continue;
+      const int32_t c[2] = {N[node].in.left, N[node].in.right};
       double dc[2];
       for (int k = 0; k < 2; ++k) {
         const int64_t cn = nodeOf(c[k]);
-        dc[k] = boxDist2(B.lo + 3 * cn, B.hi + 3 * cn, q);
+        dc[k] = boxDist2(N[cn].lo, N[cn].hi, q);
       }
       const int first = dc[1] < dc[0] ? 1 : 0;
       for (int kk = 1; kk >= 0; --kk) {  // push the farther child first
@@ -232,27 +283,19 @@ __global__ void __launch_bounds__(128) kSdfBvh(const double* __restrict__ P, int
       w += solidAngle(qd, t[0], t[1], t[2]);
       continue;
     }
-    const double A = B.area[node];
-    const double* lo = B.lo + 3 * node;
-    const double* hi = B.hi + 3 * node;
-    if (A > 0.0) {
-      const double c[3] = {B.ac[3 * node] / A, B.ac[3 * node + 1] / A, B.ac[3 * node + 2] / A};
-      double r2 = 0.0;
-      for (int a = 0; a < 3; ++a) {
-        const double e = fmax(c[a] - lo[a], hi[a] - c[a]);
-        r2 += e * e;
-      }
-      const double d[3] = {c[0] - q[0], c[1] - q[1], c[2] - q[2]};
+    const BvhNode& nd = N[node];
+    if (nd.in.area > 0.0) {
+      const double d[3] = {nd.in.c[0] - q[0], nd.in.c[1] - q[1], nd.in.c[2] - q[2]};
       const double R2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
-      if (R2 > kFwnBeta * kFwnBeta * r2) {
+      if (R2 > kFwnBeta * kFwnBeta * nd.in.r2) {
         const double R = sqrt(R2);
-        w += (B.an[3 * node] * d[0] + B.an[3 * node + 1] * d[1] + B.an[3 * node + 2] * d[2]) / (R2 * R);
+        w += (nd.in.an[0] * d[0] + nd.in.an[1] * d[1] + nd.in.an[2] * d[2]) / (R2 * R);
         continue;
       }
     }
     if (sp + 2 > kBvhStack) { atomicOr(overflow, 1u); continue; }
-    stack[sp++] = B.left[node];
-    stack[sp++] = B.right[node];
+    stack[sp++] = nd.in.left;
+    stack[sp++] = nd.in.right;
   }
   const double wn = w / (4.0 * 3.14159265358979323846);
   const double dist = sqrt(best);
@@ -312,7 +355,11 @@ its_status sdfBvh(its_ctx* ctx, const double* dP, int64_t m, const double* dV, c
   }
   kBottomUp<<<gridFor(nf, 256), 256, 0, ctx->stream>>>(dV, dF, nf, leafTri.p, B);
   ITS_LAUNCHED(ctx);
-  kSdfBvh<<<gridFor(m, 128), 128, 0, ctx->stream>>>(dP, m, dV, dF, B, dOut, overflow.p);
+  DevBuf<BvhNode> packed;
+  if ((st = packed.alloc(ctx, nodes)) != ITS_OK) return st;
+  kPackNodes<<<gridFor(nodes, 128), 128, 0, ctx->stream>>>(dV, dF, B, packed.p);
+  ITS_LAUNCHED(ctx);
+  kSdfBvh<<<gridFor(m, 128), 128, 0, ctx->stream>>>(dP, m, packed.p, nf, dOut, overflow.p);
   ITS_LAUNCHED(ctx);
   unsigned ov = 0;
   ITS_CU(ctx, cudaMemcpyAsync(&ov, overflow.p, 4, cudaMemcpyDeviceToHost, ctx->stream));

@@ -366,26 +366,24 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
       ok = mbarWait(bar, phase) && ok;
       phase ^= 1u;
       fenceAfter();
-      // epilogue of this group's columns, 16 at a time (a rolled loop keeps the code small)
+      // epilogue of this group's 32 columns: one TMEM load, one wait
       const float* bias = layer == 0 ? b1 : (layer == 1 ? b2 : b3);
-#pragma unroll 1
-      for (int n0 = kGroupCols * grp; n0 < kGroupCols * grp + kGroupCols; n0 += 16) {
-        float v[16];
-        tmemLoad16(tmem + lane + (uint32_t)n0, v);
-        if (layer < 2) {  // hidden layer: the next layer's A operand
+      const int n0 = kGroupCols * grp;
+      float v[kGroupCols];
+      tmemLoad32(tmem + lane + (uint32_t)n0, v);
+      if (layer < 2) {  // hidden layer: the next layer's A operand
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            __align__(16) bf16 q[8];
+        for (int h = 0; h < kGroupCols / 8; ++h) {
+          __align__(16) bf16 q[8];
 #pragma unroll
-            for (int e = 0; e < 8; ++e) q[e] = __float2bfloat16_rn(geluF(v[h * 8 + e] + bias[n0 + h * 8 + e]));
-            const int c = (n0 >> 3) + h;
-            *(uint4*)(sH + (c >> 3) * 16384 + swizzledChunk(row, c & 7)) = *(const uint4*)q;
-          }
-        } else {  // output unit: this group's quarter of the columns, in order
-#pragma unroll
-          for (int j = 0; j < 16; ++j)
-            o += __bfloat162float(__float2bfloat16_rn(geluF(v[j] + bias[n0 + j]))) * w4[n0 + j];
+          for (int e = 0; e < 8; ++e) q[e] = __float2bfloat16_rn(geluF(v[h * 8 + e] + bias[n0 + h * 8 + e]));
+          const int c = (n0 >> 3) + h;
+          *(uint4*)(sH + (c >> 3) * 16384 + swizzledChunk(row, c & 7)) = *(const uint4*)q;
         }
+      } else {  // output unit: this group's quarter of the columns, in order
+#pragma unroll
+        for (int j = 0; j < kGroupCols; ++j)
+          o += __bfloat162float(__float2bfloat16_rn(geluF(v[j] + bias[n0 + j]))) * w4[n0 + j];
       }
     }
     if (grp > 0) sPart[grp * 128 + row] = o;
