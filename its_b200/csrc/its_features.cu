@@ -25,6 +25,7 @@
 
 #include "its_op.cuh"
 #include "its_scan.cuh"
+#include "its_umma.cuh"
 
 namespace its {
 
@@ -185,7 +186,8 @@ __global__ void __launch_bounds__(kFeatThreads) kShareFeatures(const __grid_cons
                                                                const double* __restrict__ lam0,
                                                                const float* __restrict__ geom,
                                                                const __grid_constant__ FeatNorm norm,
-                                                               float* __restrict__ out) {
+                                                               float* __restrict__ out, __nv_bfloat16* __restrict__ tiles,
+                                                               int64_t tileRow0) {
   gridDependencyWait();
   gridDependents();
   __shared__ __align__(16) float sf[kFeatRows][kFeat];
@@ -262,8 +264,26 @@ __global__ void __launch_bounds__(kFeatThreads) kShareFeatures(const __grid_cons
     }
   }
   __syncthreads();
-  // the block's rows are consecutive in out: float4 stores over all of them
   const int64_t rows = count - i0 < kFeatRows ? count - i0 : kFeatRows;
+  if (tiles) {
+    // the network's input tiles: row R = tileRow0 + i of 128-row tile R / 128, 64 BF16 (128 B)
+    // per row in 16-byte chunks at their 128-byte-swizzled places (umma::swizzledChunk)
+    for (int e = threadIdx.x; e < rows * 8; e += kFeatThreads) {
+      const int r = e >> 3, c = e & 7;
+      const int64_t R = tileRow0 + i0 + r;
+      __align__(16) __nv_bfloat16 q[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        float x = sf[r][8 * c + k];
+        if (norm.on) x = (x - norm.v[8 * c + k]) * norm.v[kFeat + 8 * c + k];
+        q[k] = __float2bfloat16_rn(x);
+      }
+      *(uint4*)((uint8_t*)tiles + (R >> 7) * 16384 + umma::swizzledChunk((uint32_t)(R & 127), (uint32_t)c)) =
+          *(const uint4*)q;
+    }
+    return;
+  }
+  // the block's rows are consecutive in out: float4 stores over all of them
   for (int e = threadIdx.x; e < rows * (kFeat / 4); e += kFeatThreads) {
     const int r = e / (kFeat / 4), k = 4 * (e % (kFeat / 4));
     float4 x = *(const float4*)&sf[r][k];
@@ -421,14 +441,15 @@ its_status nodeSampleStats(its_ctx* ctx, SvoDevice& d, const double* V, const in
 // is coincident vertex i) (see the file comment); hostNorm (host memory, may be null) the
 // normalisation.
 its_status shareFeatures(its_ctx* ctx, const SvoDevice& d, const double* b, const double* lam0, const int64_t* ids,
-                         int64_t count, const float* hostNorm, float* out, bool afterKernel) {
+                         int64_t count, const float* hostNorm, float* out, bool afterKernel, __nv_bfloat16* tiles,
+                         int64_t tileRow0) {
   const FeatParams P = featParams(d);
   FeatNorm norm;
   norm.on = hostNorm != nullptr;
   for (int k = 0; k < 2 * kFeat; ++k) norm.v[k] = hostNorm ? hostNorm[k] : 0.0f;
   if (count > 0) {
     its_status st = launchDependent(ctx, afterKernel, kShareFeatures, gridFor(count, kFeatRows), kFeatThreads, 0, ctx->stream, P, ids,
-                                    count, b, lam0, (const float*)d.coincGeom, norm, out);
+                                    count, b, lam0, (const float*)d.coincGeom, norm, out, tiles, tileRow0);
     if (st != ITS_OK) return st;
   }
   return ITS_OK;
@@ -456,8 +477,8 @@ using namespace its;
 
 namespace its {
 its_status mlpInfer(its_mlp* mlp, const float* X, int64_t n, float* out, bool afterKernel);
-its_status mlpInferShares(its_mlp* h, const float* X, int64_t n, const int64_t* ids, float scale, float mean,
-                          double* shares, bool afterKernel);
+its_status mlpInferTiles(its_mlp* h, const __nv_bfloat16* tiles, int64_t n, float* out, const int64_t* ids,
+                         float scale, float mean, double* shares, bool afterKernel);
 its_status mlpCheck(its_mlp* mlp);
 }  // namespace its
 
@@ -499,26 +520,30 @@ its_status learnedStart(its_ctx* ctx, its_svo* const* svos, int64_t count, its_m
   }
   // every buffer up front: from the first kernel on, each launch follows a kernel (dependent
   // launches, gridDependencyWait at the top of each kernel)
-  DevBuf<float> feat, pred;
+  // the features go straight into the network's BF16 input tiles (128 rows x 128 B each)
+  DevBuf<__nv_bfloat16> feat;
+  DevBuf<float> pred;
   DevBuf<double> G;
-  if ((st = feat.alloc(ctx, std::max<int64_t>(total, 1) * kFeat)) != ITS_OK ||
+  if ((st = feat.alloc(ctx, std::max<int64_t>((total + 127) / 128, 1) * 128 * kFeat)) != ITS_OK ||
       (st = pred.alloc(ctx, std::max<int64_t>(total, 1))) != ITS_OK ||
       (st = G.alloc(ctx, std::max<int64_t>(verts, 1))) != ITS_OK)
     return st;
   if ((st = exactStart(ctx, svos, count, b, nullptr, l0.data(), false, nullptr)) != ITS_OK) return st;
   int64_t off = 0;
   for (int64_t m = 0; m < count; ++m) {
-    if ((st = shareFeatures(ctx, svos[m]->d, b[m], l0[m], svos[m]->d.coincIds, cnt[m], hn, feat.p + off * kFeat,
-                            true)) != ITS_OK)
+    if ((st = shareFeatures(ctx, svos[m]->d, b[m], l0[m], svos[m]->d.coincIds, cnt[m], hn, nullptr, true, feat.p,
+                            off)) != ITS_OK)
       return st;
     off += cnt[m];
   }
   if (count == 1) {  // one octree: the network writes the shares itself
-    if (total > 0 && (st = mlpInferShares(mlp, feat.p, total, svos[0]->d.coincIds, hn[2 * kFeat + 1], hn[2 * kFeat],
-                                          shares[0].p, true)) != ITS_OK)
+    if (total > 0 && (st = mlpInferTiles(mlp, feat.p, total, nullptr, svos[0]->d.coincIds, hn[2 * kFeat + 1],
+                                         hn[2 * kFeat], shares[0].p, true)) != ITS_OK)
       return st;
   } else {
-    if (total > 0 && (st = mlpInfer(mlp, feat.p, total, pred.p, true)) != ITS_OK) return st;
+    if (total > 0 &&
+        (st = mlpInferTiles(mlp, feat.p, total, pred.p, nullptr, 0.0f, 0.0f, nullptr, true)) != ITS_OK)
+      return st;
     off = 0;
     for (int64_t m = 0; m < count; ++m) {
       if ((st = scatterShares(ctx, svos[m]->d.coincIds, cnt[m], pred.p + off, hn[2 * kFeat + 1], hn[2 * kFeat],
@@ -564,7 +589,8 @@ its_status its_share_features(its_svo* svo, const double* b, const float* norm, 
   if ((st = exactStart(ctx, &svo, 1, &bp, nullptr, &lp, false, nullptr)) != ITS_OK) return st;
   OutArg<float> out;
   if ((st = out.stage(ctx, features, cnt * kFeat)) != ITS_OK) return st;
-  if ((st = shareFeatures(ctx, d, db.d, lam0.p, dIds, cnt, norm ? hn : nullptr, out.d, false)) != ITS_OK) return st;
+  if ((st = shareFeatures(ctx, d, db.d, lam0.p, dIds, cnt, norm ? hn : nullptr, out.d, false, nullptr, 0)) != ITS_OK)
+    return st;
   if ((st = out.finish(ctx)) != ITS_OK) return st;
   if (ids) ITS_CU(ctx, cudaMemcpyAsync(ids, dIds, cnt * 8, cudaMemcpyDefault, ctx->stream));
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));

@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
     kMlpForwardFused(const float* __restrict__ X, int64_t n, const bf16* __restrict__ W1, const bf16* __restrict__ W2,
                      const bf16* __restrict__ W3, const float* __restrict__ P, const float* __restrict__ w4r,
                      float* __restrict__ out, int* __restrict__ err, const int64_t* __restrict__ shareIds,
-                     double* __restrict__ shares, float shareScale, float shareMean) {
+                     double* __restrict__ shares, float shareScale, float shareMean, const bf16* __restrict__ Xt) {
   using namespace umma;
   extern __shared__ uint8_t smemRaw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smemRaw + 1023) & ~(uintptr_t)1023);
@@ -289,11 +289,11 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   uint8_t* sH = sX + 16384;
   float* sBias = (float*)(sW3 + 32768 + kFusedSlots * (16384 + 32768));  // b1, b2, b3, w4 (128 each)
   float* sPart = sBias + 4 * 128 + s * kFusedGroups * 128;               // [group][row] partial sums
-  uint64_t* mbar = (uint64_t*)(sBias + 4 * 128 + kFusedSlots * kFusedGroups * 128);
-  uint32_t* tslot = (uint32_t*)(mbar + kFusedSlots);
+  uint64_t* mbar = (uint64_t*)(sBias + 4 * 128 + kFusedSlots * kFusedGroups * 128);  // MMA, then input loads
+  uint32_t* tslot = (uint32_t*)(mbar + 2 * kFusedSlots);
   if (warp == 0) tmemAlloc(smemAddr(tslot), 128 * kFusedSlots);
   if (tid == 0)
-    for (int k = 0; k < kFusedSlots; ++k) mbarInit(smemAddr(mbar + k), 1);
+    for (int k = 0; k < 2 * kFusedSlots; ++k) mbarInit(smemAddr(mbar + k), 1);
   for (int i = tid; i < 4 * 128; i += blockDim.x)
     sBias[i] = i < 384 ? P[(i < 128 ? kOffB1 : (i < 256 ? kOffB2 : kOffB3)) + (i & 127)] : w4r[i - 384];
   loadWeightTile(sW1, W1, kIn, tid, blockDim.x);
@@ -308,8 +308,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   const uint32_t tmem = *tslot + 128u * s;                 // this tile slot's 128 columns
   const uint32_t lane = (uint32_t)((warp & 3) * 32) << 16;  // the warp's TMEM lanes
   constexpr uint32_t idesc = idescBf16(128, kHid);
-  const uint32_t bar = smemAddr(mbar + s);
-  uint32_t phase = 0;
+  const uint32_t bar = smemAddr(mbar + s), barX = smemAddr(mbar + kFusedSlots + s);
+  uint32_t phase = 0, phaseX = 0;
   bool ok = true;
   const float* b1 = sBias;
   const float* b2 = sBias + 128;
@@ -319,10 +319,18 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   const bool xVec = ((uintptr_t)X & 15) == 0;  // rows are 256 B apart: 16-byte loads when the base allows
   for (int64_t t = (int64_t)blockIdx.x * kFusedSlots + s; t < tiles; t += (int64_t)gridDim.x * kFusedSlots) {
     const int64_t m = t * 128 + row;
+    if (Xt) {  // the tile already in BF16 and swizzled: one bulk copy by the TMA engine
+      if (st == 0) {
+        mbarArriveExpectTx(barX, 16384);
+        bulkLoad(smemAddr(sX), (const uint8_t*)Xt + t * 16384, 16384, barX);
+      }
+      ok = mbarWait(barX, phaseX) && ok;
+      phaseX ^= 1u;
+    }
     // features -> BF16: the tile's 128 rows x 256 B read in coalesced 32-byte pieces, each one
     // 16-byte chunk of a row in the swizzled A tile
 #pragma unroll 2
-    for (int p = st; p < 128 * 8; p += kSlotThreads) {
+    for (int p = st; p < (Xt ? 0 : 128 * 8); p += kSlotThreads) {
       const int pr = p >> 3, pc = p & 7;
       const int64_t mr = t * 128 + pr;
       float4 f0 = make_float4(0.f, 0.f, 0.f, 0.f), f1 = f0;
@@ -661,23 +669,26 @@ static its_status checkErr(its_mlp* h) {
 // Predictions for n device rows into device out, launched on the context's stream without
 // waiting (the caller checks the error flag at its next synchronisation).
 static its_status launchFused(its_mlp* h, const float* X, int64_t n, float* out, const int64_t* ids, double* shares,
-                              float scale, float mean, bool afterKernel) {
+                              float scale, float mean, bool afterKernel, const bf16* Xt = nullptr) {
   its_ctx* ctx = h->ctx;
   if (n <= 0) return ITS_OK;
   const int64_t tiles = (n + 127) / 128, ctas = (tiles + kFusedSlots - 1) / kFusedSlots;
   const unsigned grid = (unsigned)(ctas < ctx->numSMs ? ctas : ctx->numSMs);
   return launchDependent(ctx, afterKernel, kMlpForwardFused, grid, kFusedThreads, kFusedSmem, ctx->stream, X, n,
                          (const bf16*)h->W1, (const bf16*)h->W2, (const bf16*)h->W3, (const float*)h->P,
-                         (const float*)h->w4r, out, h->err, ids, shares, scale, mean);
+                         (const float*)h->w4r, out, h->err, ids, shares, scale, mean, Xt);
 }
 its_status mlpInfer(its_mlp* h, const float* X, int64_t n, float* out, bool afterKernel) {
   return launchFused(h, X, n, out, nullptr, nullptr, 0.0f, 0.0f, afterKernel);
 }
 // The same predictions written as shares: shares[ids[m]] = pred[m] * scale + mean (in FP64,
 // as the share scatter of the learned start computes it).
-its_status mlpInferShares(its_mlp* h, const float* X, int64_t n, const int64_t* ids, float scale, float mean,
-                          double* shares, bool afterKernel) {
-  return launchFused(h, X, n, nullptr, ids, shares, scale, mean, afterKernel);
+// Predictions from input tiles that are already BF16 and swizzled (128 rows x 128 B each,
+// whole tiles): into out, or, with shares set, as shares[ids[m]] = pred[m] * scale + mean (in
+// FP64, as the share scatter of the learned start computes it).
+its_status mlpInferTiles(its_mlp* h, const bf16* tiles, int64_t n, float* out, const int64_t* ids, float scale,
+                         float mean, double* shares, bool afterKernel) {
+  return launchFused(h, nullptr, n, out, ids, shares, scale, mean, afterKernel, tiles);
 }
 
 its_status mlpCheck(its_mlp* h) { return checkErr(h); }

@@ -100,6 +100,18 @@ __device__ __forceinline__ void mbarInit(uint32_t mbar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count));
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
+// Arrive on an mbarrier and add bytes to the transaction count its phase waits for.
+__device__ __forceinline__ void mbarArriveExpectTx(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+// Bulk copy (the TMA engine, no tensor map) of bytes from global to this CTA's shared memory,
+// completing as a transaction on mbar. Both addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulkLoad(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(mbar)
+               : "memory");
+}
+
 // Bounded wait for the given phase parity; false when the bound ran out.
 __device__ __forceinline__ bool mbarWait(uint32_t mbar, uint32_t parity, uint32_t maxTries = 1u << 22) {
   for (uint32_t i = 0; i < maxTries; ++i) {
