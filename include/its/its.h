@@ -90,6 +90,9 @@ typedef struct its_svo_info {
   int64_t nodes_per_depth[16];
   int64_t vertices_per_depth[16];
   double origin[3], unit[3];
+  double build_ms;           /* device time of its_svo_build (from the voxelisation on) */
+  double learned_tables_ms;  /* of which the learned fit's octree-only tables: per-node face-sample
+                                sums, coincident vertices and their geometric features */
 } its_svo_info;
 /* SparseVoxelOctree::createOctree (src/SVO.h:104, src/cuAcc/SVO.cu:674-856) together with
    constructNodeAtrributes (SVO.cu:1112-1118): voxelises the triangles at res^3 (res a power

@@ -18,7 +18,8 @@ class SvoInfo(C.Structure):
     _fields_ = [("res", C.c_int), ("depth", C.c_int), ("num_voxels", C.c_int64), ("num_fine_nodes", C.c_int64),
                 ("num_nodes", C.c_int64), ("num_vertices", C.c_int64), ("num_edges", C.c_int64),
                 ("nodes_per_depth", C.c_int64 * 16), ("vertices_per_depth", C.c_int64 * 16),
-                ("origin", C.c_double * 3), ("unit", C.c_double * 3)]
+                ("origin", C.c_double * 3), ("unit", C.c_double * 3), ("build_ms", C.c_double),
+                ("learned_tables_ms", C.c_double)]
 
 
 class BasisOpts(C.Structure):

@@ -160,6 +160,8 @@ struct SvoDevice {
   float* coincGeom = nullptr;      // share-network features 38-45 of each coincident vertex (the
                                    // face samples around its owner: octree and mesh only)
   void* rowParams = nullptr;       // device copy of the octree's RowParams (its_rows.cuh)
+  float buildMs = 0.0f;            // device time of the whole build
+  float learnedTablesMs = 0.0f;    // of which the learned fit's octree-only tables
   LatticeIndex lattice(int d) const {
     LatticeIndex L;
     L.bits = vbits[d];

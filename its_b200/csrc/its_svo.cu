@@ -334,6 +334,14 @@ its_status svoBuild(its_ctx* ctx, const double* dV, int64_t nv, const int32_t* d
   const int64_t gridBits = (int64_t)res * res * res;
   const int64_t gridWords = (gridBits + 63) / 64;
   its_status st;
+  // device time of the build and of the learned fit's tables (reported by its_svo_get_info)
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  for (auto& e : ev) ITS_CU(ctx, cudaEventCreate(&e));
+  struct EvFree {
+    cudaEvent_t* e;
+    ~EvFree() { for (int k = 0; k < 3; ++k) if (e[k]) cudaEventDestroy(e[k]); }
+  } evFree{ev};
+  ITS_CU(ctx, cudaEventRecord(ev[0], ctx->stream));
 
   // 1. voxelise into the Morton bitset
   DevBuf<unsigned long long> occ;
@@ -517,6 +525,7 @@ its_status svoBuild(its_ctx* ctx, const double* dV, int64_t nv, const int32_t* d
     ITS_LAUNCHED(ctx);
   }
   // per-node sums of the face samples (features of the share network)
+  ITS_CU(ctx, cudaEventRecord(ev[1], ctx->stream));
   if ((st = nodeSampleStats(ctx, d, dV, dF, nf)) != ITS_OK) return st;
   // the coincident vertices (the shares of the exact start)
   if ((st = devAlloc(ctx, (void**)&d.coincIds, std::max<int64_t>(d.numVerts, 1) * 8)) != ITS_OK) return st;
@@ -526,7 +535,10 @@ its_status svoBuild(its_ctx* ctx, const double* dV, int64_t nv, const int32_t* d
   const RowParams hp = rowParams(d);
   if ((st = devAlloc(ctx, &d.rowParams, sizeof(RowParams))) != ITS_OK) return st;
   ITS_CU(ctx, cudaMemcpyAsync(d.rowParams, &hp, sizeof(RowParams), cudaMemcpyHostToDevice, ctx->stream));
+  ITS_CU(ctx, cudaEventRecord(ev[2], ctx->stream));
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  cudaEventElapsedTime(&d.buildMs, ev[0], ev[2]);
+  cudaEventElapsedTime(&d.learnedTablesMs, ev[1], ev[2]);
   return ITS_OK;
 }
 
@@ -590,6 +602,8 @@ its_status its_svo_get_info(const its_svo* s, its_svo_info* info) {
     info->vertices_per_depth[L] = d.vertCount[L];
   }
   for (int a = 0; a < 3; ++a) { info->origin[a] = d.origin[a]; info->unit[a] = d.unit[a]; }
+  info->build_ms = d.buildMs;
+  info->learned_tables_ms = d.learnedTablesMs;
   return ITS_OK;
 }
 

@@ -34,3 +34,20 @@ def test_host_preprocessing_matches_oracle():
     assert np.array_equal(a, b)
     for x, y in zip(api.uniform_bbox(a), oracle.uniform_bbox(b)):
         assert np.array_equal(x, y)
+
+
+def test_ctypes_structs_match_the_header(tmp_path):
+    # the Python binding's structs have the C layout of include/its/its.h (sizes and offsets)
+    import subprocess
+    from its_b200 import _lib
+    src = tmp_path / "sizes.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "its/its.h"\n'
+                   'int main(void) { printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(its_svo_info), '
+                   'offsetof(its_svo_info, learned_tables_ms), sizeof(its_solve_opts), sizeof(its_solve_report), '
+                   'sizeof(its_basis_opts), offsetof(its_basis_opts, num_samples)); return 0; }\n')
+    exe = tmp_path / "sizes"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = [ctypes.sizeof(_lib.SvoInfo), _lib.SvoInfo.learned_tables_ms.offset, ctypes.sizeof(_lib.SolveOpts),
+            ctypes.sizeof(_lib.SolveReport), ctypes.sizeof(_lib.BasisOpts), _lib.BasisOpts.num_samples.offset]
+    assert got == want
