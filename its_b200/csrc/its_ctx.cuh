@@ -114,6 +114,19 @@ inline MemKind memKind(const void* p, int device) {
   if (a.type == cudaMemoryTypeDevice) return a.device == device ? MemKind::Device : MemKind::OtherDevice;
   return MemKind::Host;
 }
+// The same with host memory split into page-locked and pageable, from one attribute query.
+enum class PtrClass { Pageable, Pinned, Device, OtherDevice };
+inline PtrClass ptrClass(const void* p, int device) {
+  if (!p) return PtrClass::Pageable;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return PtrClass::Pageable;
+  }
+  if (a.type == cudaMemoryTypeManaged) return PtrClass::Device;
+  if (a.type == cudaMemoryTypeDevice) return a.device == device ? PtrClass::Device : PtrClass::OtherDevice;
+  return a.type == cudaMemoryTypeHost ? PtrClass::Pinned : PtrClass::Pageable;
+}
 // True when p is device (or managed) memory the context's device can use directly.
 inline bool isDevicePtr(const its_ctx* ctx, const void* p) { return memKind(p, ctx->device) == MemKind::Device; }
 inline its_status otherDeviceError(its_ctx* ctx) {

@@ -196,10 +196,11 @@ its_status its_learned_fit(its_svo* svo, its_mlp* mlp, const double* b, const fl
   float hn[kNormValues];
   if ((st = hostNorm(ctx, norm, hn)) != ITS_OK) return st;
   const int64_t n = svo->d.numVerts;
-  // device addresses of the vectors: the caller's, or the plan's copies of host vectors
-  if (memKind(b, ctx->device) == MemKind::OtherDevice || memKind(lambda, ctx->device) == MemKind::OtherDevice)
-    return otherDeviceError(ctx);
-  const bool bHost = !isDevicePtr(ctx, b), lamHost = !isDevicePtr(ctx, lambda);
+  // device addresses of the vectors: the caller's, or the plan's copies of host vectors (one
+  // attribute query per vector)
+  const PtrClass cb = ptrClass(b, ctx->device), cl = ptrClass(lambda, ctx->device);
+  if (cb == PtrClass::OtherDevice || cl == PtrClass::OtherDevice) return otherDeviceError(ctx);
+  const bool bHost = cb != PtrClass::Device, lamHost = cl != PtrClass::Device;
   if ((bHost && !p->bStage && cudaMalloc(&p->bStage, std::max<int64_t>(n, 1) * 8) != cudaSuccess) ||
       (lamHost && !p->lamStage && cudaMalloc(&p->lamStage, std::max<int64_t>(n, 1) * 8) != cudaSuccess)) {
     cudaGetLastError();
@@ -209,8 +210,8 @@ its_status its_learned_fit(its_svo* svo, its_mlp* mlp, const double* b, const fl
   double* ld = lamHost ? p->lamStage : lambda;
   // page-locked host vectors are copied by the graph itself (lambda beside the residual);
   // pageable ones around it
-  const double* bPin = bHost && isPinnedHostPtr(b) ? b : nullptr;
-  double* lamPin = lamHost && isPinnedHostPtr(lambda) ? lambda : nullptr;
+  const double* bPin = cb == PtrClass::Pinned ? b : nullptr;
+  double* lamPin = cl == PtrClass::Pinned ? lambda : nullptr;
   if (bHost && !bPin) ITS_CU(ctx, cudaMemcpyAsync(p->bStage, b, n * 8, cudaMemcpyHostToDevice, ctx->stream));
   if (!p->exec || p->mlp != mlp || p->mlpUid != mlpUid(mlp) || p->b != bd || p->lam != ld || p->bHost != bPin ||
       p->lamHost != lamPin || p->stream != ctx->stream || std::memcmp(p->norm, hn, sizeof(hn)) != 0)
