@@ -54,7 +54,8 @@ struct LearnedPlan {
   double* relHost = nullptr;  // pinned: the residual (written by the residual's last kernel
                               // through the mapped address), then the network's error flag
   double* relMapped = nullptr;  // relHost's device address
-  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;      // recorded by the graph itself: its start and end
+  cudaEvent_t tPre = nullptr, tPost = nullptr;  // recorded by the call around work outside the graph
   cudaStream_t side = nullptr;  // the copy of lambda to pinned host memory, beside the residual
   cudaEvent_t fork = nullptr, join = nullptr;
   double* bStage = nullptr;   // device copies of host vectors
@@ -70,8 +71,8 @@ void destroyPlan(LearnedPlan* p) {
   if (!p) return;
   cudaStreamSynchronize(p->ctx->stream);
   dropGraph(p);
-  if (p->t0) cudaEventDestroy(p->t0);
-  if (p->t1) cudaEventDestroy(p->t1);
+  for (cudaEvent_t e : {p->t0, p->t1, p->tPre, p->tPost})
+    if (e) cudaEventDestroy(e);
   if (p->fork) cudaEventDestroy(p->fork);
   if (p->join) cudaEventDestroy(p->join);
   if (p->side) cudaStreamDestroy(p->side);
@@ -96,6 +97,8 @@ static its_status planFor(its_svo* svo, LearnedPlan** out) {
     if (e == cudaSuccess) e = cudaHostGetDevicePointer(&p->relMapped, p->relHost, 0);
     if (e == cudaSuccess) e = cudaEventCreate(&p->t0);
     if (e == cudaSuccess) e = cudaEventCreate(&p->t1);
+    if (e == cudaSuccess) e = cudaEventCreate(&p->tPre);
+    if (e == cudaSuccess) e = cudaEventCreate(&p->tPost);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking);
@@ -148,7 +151,10 @@ static its_status capture(its_svo* svo, LearnedPlan* p, its_mlp* mlp, const doub
   its_status st = ITS_OK;
   cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    st = enqueueFit(svo, p, mlp, b, hn, lam, bHost, lamHost);
+    // the graph's own start and end timestamps (the report's device time, no host calls)
+    e = cudaEventRecordWithFlags(p->t0, ctx->stream, cudaEventRecordExternal);
+    if (e == cudaSuccess) st = enqueueFit(svo, p, mlp, b, hn, lam, bHost, lamHost);
+    if (e == cudaSuccess && st == ITS_OK) e = cudaEventRecordWithFlags(p->t1, ctx->stream, cudaEventRecordExternal);
     const cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &graph);
     if (e == cudaSuccess) e = e2;
   }
@@ -189,10 +195,7 @@ its_status its_learned_fit(its_svo* svo, its_mlp* mlp, const double* b, const fl
   its_status st;
   LearnedPlan* p = nullptr;
   if ((st = planFor(svo, &p)) != ITS_OK) return st;
-  if (report) {
-    std::memset(report, 0, sizeof(*report));
-    ITS_CU(ctx, cudaEventRecord(p->t0, ctx->stream));
-  }
+  if (report) std::memset(report, 0, sizeof(*report));
   float hn[kNormValues];
   if ((st = hostNorm(ctx, norm, hn)) != ITS_OK) return st;
   const int64_t n = svo->d.numVerts;
@@ -212,14 +215,17 @@ its_status its_learned_fit(its_svo* svo, its_mlp* mlp, const double* b, const fl
   // pageable ones around it
   const double* bPin = cb == PtrClass::Pinned ? b : nullptr;
   double* lamPin = cl == PtrClass::Pinned ? lambda : nullptr;
-  if (bHost && !bPin) ITS_CU(ctx, cudaMemcpyAsync(p->bStage, b, n * 8, cudaMemcpyHostToDevice, ctx->stream));
+  // the report's device time runs from the graph's start, or from the copy of a pageable b
+  const bool preCopy = bHost && !bPin;
+  if (report && preCopy) ITS_CU(ctx, cudaEventRecord(p->tPre, ctx->stream));
+  if (preCopy) ITS_CU(ctx, cudaMemcpyAsync(p->bStage, b, n * 8, cudaMemcpyHostToDevice, ctx->stream));
   if (!p->exec || p->mlp != mlp || p->mlpUid != mlpUid(mlp) || p->b != bd || p->lam != ld || p->bHost != bPin ||
       p->lamHost != lamPin || p->stream != ctx->stream || std::memcmp(p->norm, hn, sizeof(hn)) != 0)
     if ((st = capture(svo, p, mlp, bd, hn, ld, bPin, lamPin)) != ITS_OK) return st;
   ITS_CU(ctx, cudaGraphLaunch(p->exec, ctx->stream));
   ctx->launches += p->launches;
-  if (report) ITS_CU(ctx, cudaEventRecord(p->t1, ctx->stream));
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  bool post = false;  // work after the graph (fallback, copy of a pageable lambda) ends at tPost
   int netErr = 0;
   std::memcpy(&netErr, p->relHost + 1, sizeof(int));
   if (netErr) return setError(ctx, ITS_ERR_TIMEOUT, "share network: a tensor-core wait ran out");
@@ -242,16 +248,17 @@ its_status its_learned_fit(its_svo* svo, its_mlp* mlp, const double* b, const fl
     rel = r.rel_residual;
     iters = r.iterations;
     converged = r.converged;
-    if (report) ITS_CU(ctx, cudaEventRecord(p->t1, ctx->stream));
+    post = true;
   }
   if (lamHost && (!lamPin || fellBack)) {  // not copied by the graph, or changed since
     ITS_CU(ctx, cudaMemcpyAsync(lambda, ld, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
-    if (report) ITS_CU(ctx, cudaEventRecord(p->t1, ctx->stream));
+    post = true;
   }
+  if (report && post) ITS_CU(ctx, cudaEventRecord(p->tPost, ctx->stream));
   if (report) {
-    ITS_CU(ctx, cudaEventSynchronize(p->t1));
+    ITS_CU(ctx, cudaEventSynchronize(post ? p->tPost : p->t1));
     float ms = 0.0f;
-    cudaEventElapsedTime(&ms, p->t0, p->t1);
+    cudaEventElapsedTime(&ms, preCopy ? p->tPre : p->t0, post ? p->tPost : p->t1);
     report->iterations = iters;
     report->converged = converged;
     report->rel_residual = rel;
