@@ -400,7 +400,9 @@ its_status its_learned_start_batch(its_svo* const* svos, int64_t count, its_mlp*
    while the residual runs, so their addresses are part of what must stay the same); the graph
    reads b and the network's parameters afresh every time.
    Complete on return. report (may be NULL): iterations = LSCG iterations after the start (0
-   when the start passed), converged, rel_residual, ms = device time of the call. */
+   when the start passed), converged, rel_residual, ms = device time from the start's first
+   kernel to the end of the residual check (the device clock, read by those kernels), plus the
+   fallback LSCG's when it runs; copies of host vectors are not included. */
 its_status its_learned_fit(its_svo* svo, its_mlp* mlp, const double* b, const float* norm, double tol,
                            double* lambda, its_solve_report* report);
 

@@ -195,6 +195,12 @@ inline unsigned gridFor(int64_t n, int block) { return (unsigned)((n + block - 1
 // passed gridDependents(). It must call gridDependencyWait() before it reads anything earlier
 // work writes or writes anything earlier work reads; past that call all earlier work is
 // complete and visible. (Launched the ordinary way, both calls return at once.)
+// The device's global nanosecond clock.
+__device__ __forceinline__ unsigned long long globalTimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 __device__ __forceinline__ void gridDependencyWait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void gridDependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 

@@ -470,7 +470,8 @@ its_status scatterShares(its_ctx* ctx, const int64_t* ids, int64_t count, const 
 
 namespace its {
 its_status exactStart(its_ctx* ctx, its_svo* const* svos, int64_t count, const double* const* b,
-                      const double* const* shares, double* const* lam, bool afterKernel, double* gScratch);
+                      const double* const* shares, double* const* lam, bool afterKernel, double* gScratch,
+                      unsigned long long* stamp);
 }
 
 using namespace its;
@@ -502,7 +503,7 @@ its_status hostNorm(its_ctx* ctx, const float* norm, float* hn) {
 // zero-share starts (feature inputs), the features of every mesh into one array, one network
 // pass, the shares, the exact starts with them.
 its_status learnedStart(its_ctx* ctx, its_svo* const* svos, int64_t count, its_mlp* mlp, const double* const* b,
-                        const float* hn, double* const* lam) {
+                        const float* hn, double* const* lam, unsigned long long* stamp) {
   its_status st;
   std::vector<DevBuf<double>> lam0(count), shares(count);
   std::vector<const double*> sp(count);
@@ -528,7 +529,7 @@ its_status learnedStart(its_ctx* ctx, its_svo* const* svos, int64_t count, its_m
       (st = pred.alloc(ctx, std::max<int64_t>(total, 1))) != ITS_OK ||
       (st = G.alloc(ctx, std::max<int64_t>(verts, 1))) != ITS_OK)
     return st;
-  if ((st = exactStart(ctx, svos, count, b, nullptr, l0.data(), false, nullptr)) != ITS_OK) return st;
+  if ((st = exactStart(ctx, svos, count, b, nullptr, l0.data(), false, nullptr, stamp)) != ITS_OK) return st;
   int64_t off = 0;
   for (int64_t m = 0; m < count; ++m) {
     if ((st = shareFeatures(ctx, svos[m]->d, b[m], l0[m], svos[m]->d.coincIds, cnt[m], hn, nullptr, true, feat.p,
@@ -552,7 +553,7 @@ its_status learnedStart(its_ctx* ctx, its_svo* const* svos, int64_t count, its_m
       off += cnt[m];
     }
   }
-  return exactStart(ctx, svos, count, b, sp.data(), lam, total > 0, G.p);
+  return exactStart(ctx, svos, count, b, sp.data(), lam, total > 0, G.p, nullptr);
 }
 
 }  // namespace its
@@ -586,7 +587,7 @@ its_status its_share_features(its_svo* svo, const double* b, const float* norm, 
   if ((st = lam0.alloc(ctx, n)) != ITS_OK) return st;
   const double* bp = db.d;
   double* lp = lam0.p;
-  if ((st = exactStart(ctx, &svo, 1, &bp, nullptr, &lp, false, nullptr)) != ITS_OK) return st;
+  if ((st = exactStart(ctx, &svo, 1, &bp, nullptr, &lp, false, nullptr, nullptr)) != ITS_OK) return st;
   OutArg<float> out;
   if ((st = out.stage(ctx, features, cnt * kFeat)) != ITS_OK) return st;
   if ((st = shareFeatures(ctx, d, db.d, lam0.p, dIds, cnt, norm ? hn : nullptr, out.d, false, nullptr, 0)) != ITS_OK)
@@ -619,7 +620,7 @@ its_status its_learned_start_batch(its_svo* const* svos, int64_t count, its_mlp*
     bp[m] = B[m].d;
     lp[m] = L[m].d;
   }
-  if ((st = learnedStart(ctx, svos, count, mlp, bp.data(), hn, lp.data())) != ITS_OK) return st;
+  if ((st = learnedStart(ctx, svos, count, mlp, bp.data(), hn, lp.data(), nullptr)) != ITS_OK) return st;
   bool host = false;
   for (int64_t m = 0; m < count; ++m) {
     host = host || L[m].host;

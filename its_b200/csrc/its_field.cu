@@ -1,3 +1,4 @@
+#include <cmath>
 // Field evaluation and marching cubes.
 //
 // * Points (ThinShells::cpLatentBSplineValue, ThinShells.cpp:655-755): a point's fine node
@@ -31,6 +32,7 @@ struct EvalParams {
   const uint32_t* morton;
   const uint32_t* parent;
   const double* vertPos;
+  const uint64_t* vertKey;  // packed lattice coordinates and the vertex's corner of its owner
   double winv[kMaxDepth];  // RN(1 / w_d), for divRn
 };
 
@@ -45,6 +47,7 @@ static EvalParams evalParams(const SvoDevice& d) {
   P.morton = d.nodeMorton;
   P.parent = d.nodeParent;
   P.vertPos = d.vertPos;
+  P.vertKey = d.vertKey;
   for (int L = 0; L < kMaxDepth; ++L) P.winv[L] = 1.0 / (P.w0 * (double)(1u << L));
   return P;
 }
@@ -322,6 +325,146 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
   }
 }
 
+// The FP64 field again, separably. A corner vertex's position along one axis is one of two
+// values: g + w X (the owner node's corner bit is 0 on that axis) or (g + w (X - 1)) + w (the
+// bit is 1; SVO.cu:573-576 forms corners from the owner's origin). So the hat factor of a
+// point and a corner along an axis is one of two values that depend only on the point's
+// coordinate on that axis, the corner's lattice coordinate and that bit. Per brick and depth
+// the kernel tabulates them (the reference's hat arithmetic, quotients by divRn) for the
+// brick's x, y and z coordinates, and stages each corner of the brick's cell box as its
+// coefficient and a flag byte (present, the three corner bits). A point then sums, for
+// d = 0..D-1 and k = x|y<<1|z<<2, lambda * ((hx * hy) * hz) over its present corners with
+// positive factors -- fieldAt's additions in fieldAt's order, so the field is bit-identical,
+// at a few table reads and four FP64 operations per term.
+constexpr int kSepX = 32, kSepY = 8, kSepZ = 4, kSepThreads = kSepX * kSepY, kSepTileCap = 512;
+
+__global__ void __launch_bounds__(kSepThreads) kEvalGridSep(const __grid_constant__ EvalParams P,
+                                                            const double* __restrict__ lambda, double3 o, double3 vs,
+                                                            int R, double* __restrict__ field) {
+  __shared__ double tLam[kSepTileCap];
+  __shared__ unsigned char tFlag[kSepTileCap];
+  __shared__ double hX[kSepX][4], hY[kSepY][4], hZ[kSepZ][4];  // [coordinate][corner side * 2 + corner bit]
+  __shared__ int cX[kSepX], cY[kSepY], cZ[kSepZ];
+  const int64_t M = (int64_t)R + 1;
+  const int tid = threadIdx.x, tx = tid % kSepX, ty = tid / kSepX;
+  const int64_t x0 = (int64_t)blockIdx.x * kSepX, y0 = (int64_t)blockIdx.y * kSepY, z0 = (int64_t)blockIdx.z * kSepZ;
+  const int64_t xi = x0 + tx, yj = y0 + ty;
+  const bool inXY = xi < M && yj < M;
+  double sum[kSepZ];
+#pragma unroll
+  for (int q = 0; q < kSepZ; ++q) sum[q] = 0.0;
+  for (int d = 0; d < P.depth; ++d) {
+    const double w = P.w0 * (double)(1u << d), wi = P.winv[d];
+    const LatticeIndex& L = P.lat[d];
+    const int64_t lim = (int64_t)(P.res >> d);
+    // cells and hat tables of the brick's coordinates (clamped to the grid)
+    if (tid < kSepX + kSepY + kSepZ) {
+      const int a = tid < kSepX ? 0 : (tid < kSepX + kSepY ? 1 : 2);
+      const int k = a == 0 ? tid : (a == 1 ? tid - kSepX : tid - kSepX - kSepY);
+      int64_t idx = (a == 0 ? x0 : a == 1 ? y0 : z0) + k;
+      if (idx > M - 1) idx = M - 1;
+      const double oa = a == 0 ? o.x : a == 1 ? o.y : o.z, va = a == 0 ? vs.x : a == 1 ? vs.y : vs.z;
+      const double ga = a == 0 ? P.g.x : a == 1 ? P.g.y : P.g.z;
+      const double pa = oa + (double)idx * va;
+      const int64_t c = (int64_t)floor(divRn(pa - ga, w, wi));
+      double h[4];
+#pragma unroll
+      for (int side = 0; side < 2; ++side) {
+        const int64_t X = c + side;
+        const double pA = latticePos(ga, w, (uint32_t)(X < 0 ? 0 : X));
+        const double pB = X >= 1 ? latticePos(ga, w, (uint32_t)(X - 1)) + w : pA;
+        h[2 * side] = hat1r(pa, pA, w, wi);
+        h[2 * side + 1] = hat1r(pa, pB, w, wi);
+      }
+      double* dst = a == 0 ? hX[k] : (a == 1 ? hY[k] : hZ[k]);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) dst[e] = h[e];
+      (a == 0 ? cX : a == 1 ? cY : cZ)[k] = (int)c;
+    }
+    __syncthreads();
+    const int64_t cx0 = cX[0], cy0 = cY[0], cz0 = cZ[0];
+    const int nx = cX[kSepX - 1] - (int)cx0 + 2, ny = cY[kSepY - 1] - (int)cy0 + 2, nz = cZ[kSepZ - 1] - (int)cz0 + 2;
+    if (nx * ny * nz > kSepTileCap) {  // block-uniform: the box does not fit, per-point lookups
+      if (inXY) {
+        const double px = o.x + (double)xi * vs.x, py = o.y + (double)yj * vs.y;
+#pragma unroll
+        for (int q = 0; q < kSepZ; ++q) {
+          const double pz = o.z + (double)(z0 + q) * vs.z;
+          const int64_t cx = cX[tx], cy = cY[ty], cz = cZ[q];
+          double s = sum[q];
+          for (int k = 0; k < 8; ++k) {
+            const int64_t Lx = cx + (k & 1), Ly = cy + ((k >> 1) & 1), Lz = cz + ((k >> 2) & 1);
+            if (Lx < 0 || Ly < 0 || Lz < 0 || Lx > lim || Ly > lim || Lz > lim) continue;
+            const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
+            if (!latticeHas(L, lin)) continue;
+            const uint32_t v = latticeRank(L, lin);
+            const double fx = hat1r(px, P.vertPos[3 * (int64_t)v], w, wi);
+            if (fx <= 0.0) continue;
+            const double fy = hat1r(py, P.vertPos[3 * (int64_t)v + 1], w, wi);
+            if (fy <= 0.0) continue;
+            const double fz = hat1r(pz, P.vertPos[3 * (int64_t)v + 2], w, wi);
+            if (fz <= 0.0) continue;
+            s += lambda[v] * (fx * fy * fz);
+          }
+          sum[q] = s;
+        }
+      }
+      __syncthreads();
+      continue;
+    }
+    int mine = 0;
+    for (int t = tid; t < nx * ny * nz; t += kSepThreads) {
+      const int64_t Lx = cx0 + t / (ny * nz), Ly = cy0 + (t / nz) % ny, Lz = cz0 + t % nz;
+      unsigned char f = 0;
+      if (Lx >= 0 && Ly >= 0 && Lz >= 0 && Lx <= lim && Ly <= lim && Lz <= lim) {
+        const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
+        if (latticeHas(L, lin)) {
+          const uint32_t v = latticeRank(L, lin);
+          tLam[t] = lambda[v];
+          f = (unsigned char)(1u | (((uint32_t)(P.vertKey[v] >> 37) & 7u) << 1));
+        }
+      }
+      tFlag[t] = f;
+      mine |= f;
+    }
+    if (__syncthreads_or(mine) && inXY) {
+      const int rx = cX[tx] - (int)cx0, ry = cY[ty] - (int)cy0;
+      double hx[4], hy[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        hx[e] = hX[tx][e];
+        hy[e] = hY[ty][e];
+      }
+#pragma unroll
+      for (int q = 0; q < kSepZ; ++q) {
+        const int rz = cZ[q] - (int)cz0;
+        double s = sum[q];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
+          const int t = ((rx + ox) * ny + (ry + oy)) * nz + (rz + oz);
+          const unsigned f = tFlag[t];
+          if (!(f & 1u)) continue;
+          const double fx = (f & 2u) ? hx[2 * ox + 1] : hx[2 * ox];
+          if (fx <= 0.0) continue;
+          const double fy = (f & 4u) ? hy[2 * oy + 1] : hy[2 * oy];
+          if (fy <= 0.0) continue;
+          const double fz = hZ[q][2 * oz + ((f >> 3) & 1u)];
+          if (fz <= 0.0) continue;
+          s += tLam[t] * (fx * fy * fz);
+        }
+        sum[q] = s;
+      }
+    }
+    __syncthreads();
+  }
+  if (inXY) {
+#pragma unroll
+    for (int q = 0; q < kSepZ; ++q)
+      if (z0 + q < M) field[xi + M * (yj + M * (z0 + q))] = sum[q];
+  }
+}
+
 // ---- marching cubes in three launches -----------------------------------------------------
 // Classify: each thread takes 8 consecutive voxels (x fastest) and slides along x, loading one
 // column of 4 corner values per voxel (each field value is read about once), writes the case
@@ -491,10 +634,23 @@ static its_status launchBricks(its_ctx* ctx, const EvalParams& P, const double* 
   return ITS_OK;
 }
 
+// Corners per axis of the cell box that n consecutive lattice points span at the finest depth
+// (one more than the exact bound, for the rounding of the cell quotients).
+static int64_t boxCorners(int n, double v, double w0) { return (int64_t)std::floor((n - 1) * v / w0) + 3; }
+
 template <typename T>
 static its_status evalGridTuned(its_ctx* ctx, const SvoDevice& d, const double* lam, double3 o, double3 vs, int res,
                                 T* field) {
   const EvalParams P = evalParams(d);
+  if (sizeof(T) == 8 && boxCorners(kSepX, vs.x, d.unit[0]) * boxCorners(kSepY, vs.y, d.unit[0]) *
+                                boxCorners(kSepZ, vs.z, d.unit[0]) <= kSepTileCap) {
+    const int64_t M = (int64_t)res + 1;
+    const dim3 grid((unsigned)((M + kSepX - 1) / kSepX), (unsigned)((M + kSepY - 1) / kSepY),
+                    (unsigned)((M + kSepZ - 1) / kSepZ));
+    kEvalGridSep<<<grid, kSepThreads, 0, ctx->stream>>>(P, lam, o, vs, res, (double*)field);
+    ITS_LAUNCHED(ctx);
+    return ITS_OK;
+  }
   auto run = [&](int i) -> its_status {
     switch (i) {
       case 1: return launchBricks<T, 32, 8, 2>(ctx, P, lam, o, vs, res, field);

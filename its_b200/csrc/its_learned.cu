@@ -25,10 +25,10 @@ struct its_mlp;
 namespace its {
 
 its_status learnedStart(its_ctx* ctx, its_svo* const* svos, int64_t count, its_mlp* mlp, const double* const* b,
-                        const float* hn, double* const* lam);
+                        const float* hn, double* const* lam, unsigned long long* stamp);
 its_status fitResidualEnqueue(its_ctx* ctx, its_svo* const* svos, int64_t count, const double* const* b,
                               const double* const* lam, double* relDev, const int* flagSrc, int* flagDst,
-                              bool afterKernel);
+                              bool afterKernel, unsigned long long* stampEnd);
 its_status hostNorm(its_ctx* ctx, const float* norm, float* hn);
 const int* mlpErrFlag(its_mlp* mlp);
 uint64_t mlpUid(const its_mlp* mlp);
@@ -54,8 +54,7 @@ struct LearnedPlan {
   double* relHost = nullptr;  // pinned: the residual (written by the residual's last kernel
                               // through the mapped address), then the network's error flag
   double* relMapped = nullptr;  // relHost's device address
-  cudaEvent_t t0 = nullptr, t1 = nullptr;      // recorded by the graph itself: its start and end
-  cudaEvent_t tPre = nullptr, tPost = nullptr;  // recorded by the call around work outside the graph
+
   cudaStream_t side = nullptr;  // the copy of lambda to pinned host memory, beside the residual
   cudaEvent_t fork = nullptr, join = nullptr;
   double* bStage = nullptr;   // device copies of host vectors
@@ -71,8 +70,7 @@ void destroyPlan(LearnedPlan* p) {
   if (!p) return;
   cudaStreamSynchronize(p->ctx->stream);
   dropGraph(p);
-  for (cudaEvent_t e : {p->t0, p->t1, p->tPre, p->tPost})
-    if (e) cudaEventDestroy(e);
+
   if (p->fork) cudaEventDestroy(p->fork);
   if (p->join) cudaEventDestroy(p->join);
   if (p->side) cudaStreamDestroy(p->side);
@@ -95,10 +93,7 @@ static its_status planFor(its_svo* svo, LearnedPlan** out) {
     cudaError_t e = cudaMalloc(&p->arena, p->arenaCap);
     if (e == cudaSuccess) e = cudaHostAlloc(&p->relHost, 64, cudaHostAllocMapped);
     if (e == cudaSuccess) e = cudaHostGetDevicePointer(&p->relMapped, p->relHost, 0);
-    if (e == cudaSuccess) e = cudaEventCreate(&p->t0);
-    if (e == cudaSuccess) e = cudaEventCreate(&p->t1);
-    if (e == cudaSuccess) e = cudaEventCreate(&p->tPre);
-    if (e == cudaSuccess) e = cudaEventCreate(&p->tPost);
+
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking);
@@ -123,7 +118,9 @@ static its_status enqueueFit(its_svo* svo, LearnedPlan* p, its_mlp* mlp, const d
   const int64_t n = svo->d.numVerts;
   its_status st;
   if (bHost) ITS_CU(ctx, cudaMemcpyAsync(const_cast<double*>(b), bHost, n * 8, cudaMemcpyHostToDevice, ctx->stream));
-  if ((st = learnedStart(ctx, &svo, 1, mlp, &b, hn, &lam)) != ITS_OK) return st;
+  // the plan's mapped words: residual, the network's error flag, first-kernel and last-kernel clocks
+  unsigned long long* stamps = (unsigned long long*)(p->relMapped + 2);
+  if ((st = learnedStart(ctx, &svo, 1, mlp, &b, hn, &lam, stamps)) != ITS_OK) return st;
   if (lamHost) {
     ITS_CU(ctx, cudaEventRecord(p->fork, ctx->stream));
     ITS_CU(ctx, cudaStreamWaitEvent(p->side, p->fork, 0));
@@ -132,7 +129,7 @@ static its_status enqueueFit(its_svo* svo, LearnedPlan* p, its_mlp* mlp, const d
   }
   // the residual follows the start's last kernel directly unless lambda's copy forks off first
   if ((st = fitResidualEnqueue(ctx, &svo, 1, &b, &lam, p->relMapped, mlpErrFlag(mlp), (int*)(p->relMapped + 1),
-                               lamHost == nullptr)) != ITS_OK)
+                               lamHost == nullptr, stamps + 1)) != ITS_OK)
     return st;
   if (lamHost) ITS_CU(ctx, cudaStreamWaitEvent(ctx->stream, p->join, 0));
   return ITS_OK;
@@ -151,10 +148,7 @@ static its_status capture(its_svo* svo, LearnedPlan* p, its_mlp* mlp, const doub
   its_status st = ITS_OK;
   cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    // the graph's own start and end timestamps (the report's device time, no host calls)
-    e = cudaEventRecordWithFlags(p->t0, ctx->stream, cudaEventRecordExternal);
-    if (e == cudaSuccess) st = enqueueFit(svo, p, mlp, b, hn, lam, bHost, lamHost);
-    if (e == cudaSuccess && st == ITS_OK) e = cudaEventRecordWithFlags(p->t1, ctx->stream, cudaEventRecordExternal);
+    st = enqueueFit(svo, p, mlp, b, hn, lam, bHost, lamHost);
     const cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &graph);
     if (e == cudaSuccess) e = e2;
   }
@@ -215,17 +209,17 @@ its_status its_learned_fit(its_svo* svo, its_mlp* mlp, const double* b, const fl
   // pageable ones around it
   const double* bPin = cb == PtrClass::Pinned ? b : nullptr;
   double* lamPin = cl == PtrClass::Pinned ? lambda : nullptr;
-  // the report's device time runs from the graph's start, or from the copy of a pageable b
-  const bool preCopy = bHost && !bPin;
-  if (report && preCopy) ITS_CU(ctx, cudaEventRecord(p->tPre, ctx->stream));
-  if (preCopy) ITS_CU(ctx, cudaMemcpyAsync(p->bStage, b, n * 8, cudaMemcpyHostToDevice, ctx->stream));
+  if (bHost && !bPin) ITS_CU(ctx, cudaMemcpyAsync(p->bStage, b, n * 8, cudaMemcpyHostToDevice, ctx->stream));
   if (!p->exec || p->mlp != mlp || p->mlpUid != mlpUid(mlp) || p->b != bd || p->lam != ld || p->bHost != bPin ||
       p->lamHost != lamPin || p->stream != ctx->stream || std::memcmp(p->norm, hn, sizeof(hn)) != 0)
     if ((st = capture(svo, p, mlp, bd, hn, ld, bPin, lamPin)) != ITS_OK) return st;
   ITS_CU(ctx, cudaGraphLaunch(p->exec, ctx->stream));
   ctx->launches += p->launches;
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
-  bool post = false;  // work after the graph (fallback, copy of a pageable lambda) ends at tPost
+  // device time of the start and the check: from the first kernel's start to the residual's end
+  // (the device clock, written by those kernels to the plan's mapped words)
+  const unsigned long long* stamps = (const unsigned long long*)(p->relHost + 2);
+  double ms = stamps[1] > stamps[0] ? (double)(stamps[1] - stamps[0]) * 1e-6 : 0.0;
   int netErr = 0;
   std::memcpy(&netErr, p->relHost + 1, sizeof(int));
   if (netErr) return setError(ctx, ITS_ERR_TIMEOUT, "share network: a tensor-core wait ran out");
@@ -248,23 +242,17 @@ its_status its_learned_fit(its_svo* svo, its_mlp* mlp, const double* b, const fl
     rel = r.rel_residual;
     iters = r.iterations;
     converged = r.converged;
-    post = true;
+    ms += r.ms;
   }
   if (lamHost && (!lamPin || fellBack)) {  // not copied by the graph, or changed since
     ITS_CU(ctx, cudaMemcpyAsync(lambda, ld, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
-    post = true;
+    ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   }
-  if (report && post) ITS_CU(ctx, cudaEventRecord(p->tPost, ctx->stream));
   if (report) {
-    ITS_CU(ctx, cudaEventSynchronize(post ? p->tPost : p->t1));
-    float ms = 0.0f;
-    cudaEventElapsedTime(&ms, preCopy ? p->tPre : p->t0, post ? p->tPost : p->t1);
     report->iterations = iters;
     report->converged = converged;
     report->rel_residual = rel;
     report->ms = ms;
-  } else if (lamHost) {
-    ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   }
   return ITS_OK;
 }

@@ -63,6 +63,7 @@ struct SegArgs {
   int nseg = 0;
   const Seg* dsegs = nullptr;
   const int64_t* dprefix = nullptr;
+  unsigned long long* stamp = nullptr;  // when set: the device clock (ns) at the kernel's start
   Seg segs[kInlineSegs];
   int64_t prefix[kInlineSegs + 1];
   __device__ __forceinline__ const Seg& seg(int k) const { return dsegs ? dsegs[k] : segs[k]; }
@@ -126,6 +127,7 @@ __global__ void __launch_bounds__(256) kStartValues(const __grid_constant__ SegA
 __global__ void __launch_bounds__(256) kStartInterp(const __grid_constant__ SegArgs<RowSeg> A, int64_t total) {
   gridDependencyWait();
   gridDependents();
+  if (A.stamp && blockIdx.x == 0 && threadIdx.x == 0) *A.stamp = globalTimer();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= total) return;
   const int k = A.find(i);
@@ -281,6 +283,7 @@ struct SlotArgs {
   int64_t first[kInlineSegs + 1];
   const int* flagSrc = nullptr;  // optional: one flag copied to flagDst with the results
   int* flagDst = nullptr;
+  unsigned long long* stampEnd = nullptr;  // optional: the device clock (ns) when the results are out
   __device__ __forceinline__ int64_t at(int64_t m) const { return dfirst ? dfirst[m] : first[m]; }
 };
 
@@ -309,7 +312,10 @@ __global__ void __launch_bounds__(kResThreads) kResidualFinish(const double* __r
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) rel[m] = sc[0] > 0.0 ? sqrt(sa[0] / sc[0]) : sqrt(sa[0]);
+  if (threadIdx.x == 0) {
+    rel[m] = sc[0] > 0.0 ? sqrt(sa[0] / sc[0]) : sqrt(sa[0]);
+    if (m == 0 && F.stampEnd) *F.stampEnd = globalTimer();
+  }
 }
 
 static const RowParams* rowParamsOf(its_svo* s) { return (const RowParams*)s->d.rowParams; }
@@ -317,7 +323,8 @@ static const RowParams* rowParamsOf(its_svo* s) { return (const RowParams*)s->d.
 // Exact starts of count octrees (device vectors), matrix-free: G (when there are shares),
 // then lambda, each one launch for all octrees together.
 its_status exactStart(its_ctx* ctx, its_svo* const* svos, int64_t count, const double* const* b,
-                      const double* const* shares, double* const* lam, bool afterKernel, double* gScratch) {
+                      const double* const* shares, double* const* lam, bool afterKernel, double* gScratch,
+                      unsigned long long* stamp) {
   its_status st;
   bool anyShares = false;
   int64_t total = 0;
@@ -351,6 +358,7 @@ its_status exactStart(its_ctx* ctx, its_svo* const* svos, int64_t count, const d
   SegArgs<RowSeg> A;
   DevBuf<uint8_t> keep;
   if ((st = makeSegArgs(ctx, segs, prefix, A, keep)) != ITS_OK) return st;
+  A.stamp = stamp;
   // dependent launches only straight after a kernel (no segment table copied in between)
   const bool dep = afterKernel && !A.dsegs;
   if (anyShares) {
@@ -368,7 +376,7 @@ its_status exactStart(its_ctx* ctx, its_svo* const* svos, int64_t count, const d
 // context's stream without a host wait.
 its_status fitResidualEnqueue(its_ctx* ctx, its_svo* const* svos, int64_t count, const double* const* b,
                               const double* const* lam, double* relDev, const int* flagSrc, int* flagDst,
-                              bool afterKernel) {
+                              bool afterKernel, unsigned long long* stampEnd) {
   its_status st;
   int64_t total = 0;
   for (int64_t m = 0; m < count; ++m) total += svos[m]->d.numVerts;
@@ -416,6 +424,7 @@ its_status fitResidualEnqueue(its_ctx* ctx, its_svo* const* svos, int64_t count,
   SlotArgs F;
   F.flagSrc = flagSrc;
   F.flagDst = flagDst;
+  F.stampEnd = stampEnd;
   if (count <= kInlineSegs) {
     for (int64_t m = 0; m <= count; ++m) F.first[m] = mFirst[m];
   } else {
@@ -452,7 +461,8 @@ its_status fitResidual(its_ctx* ctx, its_svo* const* svos, int64_t count, const 
   its_status st;
   DevBuf<double> dRel;
   if ((st = dRel.alloc(ctx, count)) != ITS_OK) return st;
-  if ((st = fitResidualEnqueue(ctx, svos, count, b, lam, dRel.p, nullptr, nullptr, false)) != ITS_OK) return st;
+  if ((st = fitResidualEnqueue(ctx, svos, count, b, lam, dRel.p, nullptr, nullptr, false, nullptr)) != ITS_OK)
+    return st;
   ITS_CU(ctx, cudaMemcpyAsync(rel, dRel.p, count * 8, cudaMemcpyDeviceToHost, ctx->stream));
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
   return ITS_OK;
@@ -499,7 +509,8 @@ its_status its_exact_start_batch(its_svo* const* svos, int64_t count, const doub
     db[m] = B[m].d;
     dl[m] = L[m].d;
   }
-  if ((st = exactStart(ctx, svos, count, db.data(), ds.data(), dl.data(), false, nullptr)) != ITS_OK) return st;
+  if ((st = exactStart(ctx, svos, count, db.data(), ds.data(), dl.data(), false, nullptr, nullptr)) != ITS_OK)
+    return st;
   bool host = false;
   for (int64_t m = 0; m < count; ++m) {
     host = host || L[m].host;
