@@ -642,27 +642,30 @@ template <typename T>
 static its_status evalGridTuned(its_ctx* ctx, const SvoDevice& d, const double* lam, double3 o, double3 vs, int res,
                                 T* field) {
   const EvalParams P = evalParams(d);
-  if (sizeof(T) == 8 && boxCorners(kSepX, vs.x, d.unit[0]) * boxCorners(kSepY, vs.y, d.unit[0]) *
-                                boxCorners(kSepZ, vs.z, d.unit[0]) <= kSepTileCap) {
-    const int64_t M = (int64_t)res + 1;
-    const dim3 grid((unsigned)((M + kSepX - 1) / kSepX), (unsigned)((M + kSepY - 1) / kSepY),
-                    (unsigned)((M + kSepZ - 1) / kSepZ));
-    kEvalGridSep<<<grid, kSepThreads, 0, ctx->stream>>>(P, lam, o, vs, res, (double*)field);
-    ITS_LAUNCHED(ctx);
-    return ITS_OK;
-  }
+  // the separable kernel (FP64, when the brick's cell box fits its tile) and four brick shapes
+  // of the point-wise kernel: every candidate computes the same bits
+  const bool sep = sizeof(T) == 8 && boxCorners(kSepX, vs.x, d.unit[0]) * boxCorners(kSepY, vs.y, d.unit[0]) *
+                                             boxCorners(kSepZ, vs.z, d.unit[0]) <= kSepTileCap;
   auto run = [&](int i) -> its_status {
     switch (i) {
       case 1: return launchBricks<T, 32, 8, 2>(ctx, P, lam, o, vs, res, field);
       case 2: return launchBricks<T, 64, 4, 2>(ctx, P, lam, o, vs, res, field);
       case 3: return launchBricks<T, 16, 4, 4>(ctx, P, lam, o, vs, res, field);
+      case 4: {
+        const int64_t M = (int64_t)res + 1;
+        const dim3 grid((unsigned)((M + kSepX - 1) / kSepX), (unsigned)((M + kSepY - 1) / kSepY),
+                        (unsigned)((M + kSepZ - 1) / kSepZ));
+        kEvalGridSep<<<grid, kSepThreads, 0, ctx->stream>>>(P, lam, o, vs, res, (double*)field);
+        ITS_LAUNCHED(ctx);
+        return ITS_OK;
+      }
       default: return launchBricks<T, 32, 4, 4>(ctx, P, lam, o, vs, res, field);
     }
   };
   const std::string key = std::string("eval_grid/") + (sizeof(T) == 8 ? "f64" : "f32") + "/grid=" +
                           std::to_string(res) + "/octree=" + std::to_string(d.res) + "/depth=" + std::to_string(d.depth);
   int choice = 0;
-  its_status st = tuneChoice(ctx, key, 4, 0, run, &choice);
+  its_status st = tuneChoice(ctx, key, sep ? 5 : 4, sep ? 4 : 0, run, &choice);
   if (st != ITS_OK) return st;
   return run(choice);
 }
