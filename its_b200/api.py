@@ -271,18 +271,36 @@ class Svo:
         self.ctx.check(lib().its_svo_get_vertices(self.h, _ptr(pos), _ptr(own)), "its_svo_get_vertices")
         return pos, own
 
+    def vertex_positions_device(self):
+        """The corner vertices' positions as a torch CUDA tensor (n x 3), copied on the device."""
+        import torch
+        pos = torch.empty((self.num_verts, 3), dtype=torch.float64, device="cuda")
+        self.ctx.check(lib().its_svo_get_vertices(self.h, _ptr(pos), None), "its_svo_get_vertices")
+        return pos
+
     def edges(self):
         E = self.num_edges
         p0, p1, own = np.zeros((E, 3)), np.zeros((E, 3)), np.zeros(E, np.uint32)
         self.ctx.check(lib().its_svo_get_edges(self.h, _ptr(p0), _ptr(p1), _ptr(own)), "its_svo_get_edges")
         return p0, p1, own
 
-    def shell_samples(self, V, F):
+    def shell_samples(self, V, F, device=False):
         """Shell samples (its_shell_samples): one call into a buffer sized for typical meshes
-        (about one sample per face), a second only when the samples exceed it."""
+        (about one sample per face), a second only when the samples exceed it. device=True
+        returns them in a torch CUDA tensor (V and F may be CUDA tensors as well)."""
         V, F = _f64(V), _i32(F)
         n, ne = C.c_int64(0), C.c_int64(0)
         cap = 2 * _n(F) + _n(V) + 1024
+        if device:
+            import torch
+            out = torch.empty((cap, 3), dtype=torch.float64, device="cuda")
+            self.ctx.check(lib().its_shell_samples(self.h, _ptr(V), _n(V), _ptr(F), _n(F), _ptr(out), cap, C.byref(n),
+                                                   C.byref(ne)), "its_shell_samples")
+            if n.value > cap:
+                out = torch.empty((n.value, 3), dtype=torch.float64, device="cuda")
+                self.ctx.check(lib().its_shell_samples(self.h, _ptr(V), _n(V), _ptr(F), _n(F), _ptr(out), n.value,
+                                                       C.byref(n), C.byref(ne)), "its_shell_samples")
+            return out[:n.value], int(ne.value)
         out = np.empty((cap, 3))
         self.ctx.check(lib().its_shell_samples(self.h, _ptr(V), _n(V), _ptr(F), _n(F), _ptr(out), cap, C.byref(n),
                                                C.byref(ne)), "its_shell_samples")

@@ -160,6 +160,19 @@ __device__ __forceinline__ int64_t latticeVertex(const FeatParams& P, int d, int
   return latticeHas(L, lin) ? (int64_t)latticeRank(L, lin) : -1;
 }
 
+// latticeVertex with both words (presence bits and rank) loaded up front, so that independent
+// lookups issued together overlap their memory latency; -1 where no vertex is.
+__device__ __forceinline__ int64_t latticeVertexIlp(const FeatParams& P, int d, int64_t X, int64_t Y, int64_t Z) {
+  if (d < 0 || d >= P.depth) return -1;
+  const LatticeIndex& L = P.lat[d];
+  if (X < 0 || Y < 0 || Z < 0 || X >= L.M || Y >= L.M || Z >= L.M) return -1;
+  const uint32_t lin = (uint32_t)((X * L.M + Y) * L.M + Z);
+  const unsigned long long word = L.bits[lin >> 6];
+  const uint32_t rank = L.rank[lin >> 6];
+  if (!((word >> (lin & 63)) & 1ull)) return -1;
+  return (int64_t)(L.base + rank + (uint32_t)__popcll(word & ((1ull << (lin & 63)) - 1ull)));
+}
+
 __global__ void kMarkCoincident(const __grid_constant__ FeatParams P, int64_t n, uint32_t* __restrict__ flag) {
   const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (v >= n) return;
@@ -209,20 +222,25 @@ __global__ void __launch_bounds__(kFeatThreads) kShareFeatures(const __grid_cons
     w = P.w0 * (double)(1u << d);
     const double bv = b[v];
     if (sub == 0) {  // the coincident copies above
+      // depth d + k holds a copy while the low k bits of X, Y and Z are all zero and every
+      // depth in between has one: the candidates' lookups are independent, so they are issued
+      // together and the chain is cut at the first missing copy afterwards
+      const uint64_t xyz = (uint64_t)(X | Y | Z);
+      const int even = xyz ? __ffsll((long long)xyz) - 1 : kMaxDepth;  // trailing zeros
+      const int maxUp = min(even, P.depth - 1 - d);
+      int64_t cand[kMaxDepth];
+#pragma unroll
+      for (int k = 1; k < kMaxDepth; ++k)
+        cand[k] = k <= maxUp ? latticeVertexIlp(P, d + k, X >> k, Y >> k, Z >> k) : -1;
       int up = 0;
-      int64_t top = v, X1 = X, Y1 = Y, Z1 = Z;
-      double oneUp = 0.0;
-      for (int dd = d + 1; dd < P.depth; ++dd) {
-        if ((X1 | Y1 | Z1) & 1) break;
-        X1 >>= 1;
-        Y1 >>= 1;
-        Z1 >>= 1;
-        const int64_t u = latticeVertex(P, dd, X1, Y1, Z1);
-        if (u < 0) break;
-        if (dd == d + 1) oneUp = lam0[u];
-        top = u;
-        ++up;
-      }
+      int64_t top = v;
+#pragma unroll
+      for (int k = 1; k < kMaxDepth; ++k)
+        if (up == k - 1 && cand[k] >= 0) {
+          up = k;
+          top = cand[k];
+        }
+      const double oneUp = up >= 1 ? lam0[cand[1]] : 0.0;
       f[0] = (float)bv;
       f[1] = (float)lam0[top];
       f[2] = (float)oneUp;
@@ -230,13 +248,14 @@ __global__ void __launch_bounds__(kFeatThreads) kShareFeatures(const __grid_cons
       f[4] = (float)up / (float)P.depth;
       f[36] = (float)w;
       f[37] = (float)(bv / w);
-    } else if (sub == 1) {  // the coincident copies below
+    } else if (sub == 1) {  // the coincident copies below: independent lookups, then the chain
+      bool has[kMaxDepth];
+#pragma unroll
+      for (int s = 1; s < kMaxDepth; ++s) has[s] = s <= d && latticeVertexIlp(P, d - s, X << s, Y << s, Z << s) >= 0;
       int down = 0;
-      for (int dd = d - 1; dd >= 0; --dd) {
-        const int s = d - dd;
-        if (latticeVertex(P, dd, X << s, Y << s, Z << s) < 0) break;
-        ++down;
-      }
+#pragma unroll
+      for (int s = 1; s < kMaxDepth; ++s)
+        if (down == s - 1 && has[s]) down = s;
       f[5] = (float)down / (float)P.depth;
     }
     // face neighbours: lanes 0, 1 one each, lanes 2, 3 two each
