@@ -336,8 +336,9 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
 // d = 0..D-1 and k = x|y<<1|z<<2, lambda * ((hx * hy) * hz) over its present corners with
 // positive factors -- fieldAt's additions in fieldAt's order, so the field is bit-identical,
 // at a few table reads and four FP64 operations per term.
-constexpr int kSepX = 32, kSepY = 8, kSepZ = 4, kSepThreads = kSepX * kSepY, kSepTileCap = 512;
+constexpr int kSepX = 32, kSepY = 8, kSepThreads = kSepX * kSepY, kSepTileCap = 1024;
 
+template <int kSepZ>  // points per thread along z (the brick's depth)
 __global__ void __launch_bounds__(kSepThreads) kEvalGridSep(const __grid_constant__ EvalParams P,
                                                             const double* __restrict__ lambda, double3 o, double3 vs,
                                                             int R, double* __restrict__ field) {
@@ -642,20 +643,27 @@ template <typename T>
 static its_status evalGridTuned(its_ctx* ctx, const SvoDevice& d, const double* lam, double3 o, double3 vs, int res,
                                 T* field) {
   const EvalParams P = evalParams(d);
-  // the separable kernel (FP64, when the brick's cell box fits its tile) and four brick shapes
-  // of the point-wise kernel: every candidate computes the same bits
-  const bool sep = sizeof(T) == 8 && boxCorners(kSepX, vs.x, d.unit[0]) * boxCorners(kSepY, vs.y, d.unit[0]) *
-                                             boxCorners(kSepZ, vs.z, d.unit[0]) <= kSepTileCap;
+  // four brick shapes of the point-wise kernel and the separable kernel with 4 or 8 points per
+  // thread along z (FP64, when the brick's cell box fits its tile): every candidate computes
+  // the same bits
+  auto sepFits = [&](int z) {
+    return sizeof(T) == 8 && boxCorners(kSepX, vs.x, d.unit[0]) * boxCorners(kSepY, vs.y, d.unit[0]) *
+                                     boxCorners(z, vs.z, d.unit[0]) <= kSepTileCap;
+  };
+  const bool sep4 = sepFits(4), sep8 = sepFits(8);
   auto run = [&](int i) -> its_status {
     switch (i) {
       case 1: return launchBricks<T, 32, 8, 2>(ctx, P, lam, o, vs, res, field);
       case 2: return launchBricks<T, 64, 4, 2>(ctx, P, lam, o, vs, res, field);
       case 3: return launchBricks<T, 16, 4, 4>(ctx, P, lam, o, vs, res, field);
-      case 4: {
+      case 4:
+      case 5: {
+        const int z = i == 5 ? 8 : 4;
         const int64_t M = (int64_t)res + 1;
         const dim3 grid((unsigned)((M + kSepX - 1) / kSepX), (unsigned)((M + kSepY - 1) / kSepY),
-                        (unsigned)((M + kSepZ - 1) / kSepZ));
-        kEvalGridSep<<<grid, kSepThreads, 0, ctx->stream>>>(P, lam, o, vs, res, (double*)field);
+                        (unsigned)((M + z - 1) / z));
+        if (z == 8) kEvalGridSep<8><<<grid, kSepThreads, 0, ctx->stream>>>(P, lam, o, vs, res, (double*)field);
+        else kEvalGridSep<4><<<grid, kSepThreads, 0, ctx->stream>>>(P, lam, o, vs, res, (double*)field);
         ITS_LAUNCHED(ctx);
         return ITS_OK;
       }
@@ -665,7 +673,7 @@ static its_status evalGridTuned(its_ctx* ctx, const SvoDevice& d, const double* 
   const std::string key = std::string("eval_grid/") + (sizeof(T) == 8 ? "f64" : "f32") + "/grid=" +
                           std::to_string(res) + "/octree=" + std::to_string(d.res) + "/depth=" + std::to_string(d.depth);
   int choice = 0;
-  its_status st = tuneChoice(ctx, key, sep ? 5 : 4, sep ? 4 : 0, run, &choice);
+  its_status st = tuneChoice(ctx, key, sep8 ? 6 : (sep4 ? 5 : 4), sep8 ? 5 : (sep4 ? 4 : 0), run, &choice);
   if (st != ITS_OK) return st;
   return run(choice);
 }
