@@ -3,10 +3,12 @@
 //   * the exact unsigned distance: nearest-first traversal with box lower bounds; a node is
 //     skipped only when its box is farther than the best squared distance times (1 + 1e-12),
 //     so the minimum is the same IEEE value the brute force finds (same per-triangle code);
-//   * the sign from the fast winding number (Barill et al. 2018): far nodes contribute their
-//     area-weighted normal as a dipole at their area centroid, near nodes recurse, leaves add
-//     the exact solid angle. libigl's signed_distance(FAST_WINDING_NUMBER), which the reference
-//     calls (ThinShells.cpp:501), uses the same approximation; inside if w > 1/2.
+//   * the sign from the fast winding number (Barill et al. 2018): a node farther than beta = 2
+//     times its radius contributes the second-order expansion of its triangles' solid angles
+//     about its area centroid (the area-weighted normal sum as a dipole, plus the tensor
+//     M = sum_t an_t (c_t - c)^T), nearer nodes recurse, leaves add the exact solid angle.
+//     libigl's signed_distance(FAST_WINDING_NUMBER), which the reference calls
+//     (ThinShells.cpp:501), uses the same expansion order and accuracy scale; inside if w > 1/2.
 #include <cmath>
 
 #include "its_scan.cuh"
@@ -18,7 +20,7 @@
 namespace its {
 
 constexpr int kBvhStack = 64;
-constexpr double kFwnBeta = 3.0;  // far-field test |q - c| > beta * r
+constexpr double kFwnBeta = 2.0;  // far-field test |q - c| > beta * r
 
 struct BvhDevice {
   int64_t nf = 0;
@@ -30,6 +32,7 @@ struct BvhDevice {
   double* hi = nullptr;
   double* an = nullptr;      // area-weighted normal sum (3 per node)
   double* ac = nullptr;      // area-weighted centroid sum (3 per node)
+  double* sm = nullptr;      // sum over the node's triangles of an_t c_t^T (9 per node, row-major)
   double* area = nullptr;
   unsigned* flag = nullptr;
 };
@@ -39,7 +42,7 @@ struct BvhDevice {
 // (area-weighted centroid sum / area), squared radius, normal sum and area, and the children;
 // leaves carry their box and their triangle's corners. The values are those the traversal
 // used to form per visit from the build's arrays (same operations), so results are unchanged.
-struct __align__(128) BvhNode {
+struct __align__(64) BvhNode {
   double lo[3], hi[3];
   union {
     struct {
@@ -47,12 +50,13 @@ struct __align__(128) BvhNode {
       double r2;
       double an[3];
       double area;
+      double m[9];  // sum_t an_t (c_t - c)^T about the node's centre c
       int32_t left, right;
     } in;
     double tri[9];
   };
 };
-static_assert(sizeof(BvhNode) == 128, "one cache line per node");
+static_assert(sizeof(BvhNode) == 192, "three 64-byte lines per node");
 
 __global__ void kCentroidBounds(const double* __restrict__ V, const int32_t* __restrict__ F, int64_t nf,
                                 double* __restrict__ partial) {
@@ -155,6 +159,9 @@ __global__ void kBottomUp(const double* __restrict__ V, const int32_t* __restric
       B.hi[3 * node + a] = fmax(p[0][a], fmax(p[1][a], p[2][a]));
       B.ac[3 * node + a] = ar * (p[0][a] + p[1][a] + p[2][a]) / 3.0;
     }
+    const double an3[3] = {nx, ny, nz};
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) B.sm[9 * node + 3 * i + j] = an3[i] * ((p[0][j] + p[1][j] + p[2][j]) / 3.0);
     B.an[3 * node] = nx;
     B.an[3 * node + 1] = ny;
     B.an[3 * node + 2] = nz;
@@ -175,6 +182,8 @@ __global__ void kBottomUp(const double* __restrict__ V, const int32_t* __restric
       B.ac[3 * par + c] = ((volatile double*)B.ac)[3 * a + c] + ((volatile double*)B.ac)[3 * b + c];
     }
     B.area[par] = ((volatile double*)B.area)[a] + ((volatile double*)B.area)[b];
+    for (int e = 0; e < 9; ++e)
+      B.sm[9 * par + e] = ((volatile double*)B.sm)[9 * a + e] + ((volatile double*)B.sm)[9 * b + e];
     __threadfence();
     node = par;
   }
@@ -210,6 +219,8 @@ __global__ void kPackNodes(const double* __restrict__ V, const int32_t* __restri
       }
       r.in.r2 = r2;
     }
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) r.in.m[3 * i + j] = B.sm[9 * k + 3 * i + j] - r.in.an[i] * r.in.c[j];
     r.in.left = B.left[k];
     r.in.right = B.right[k];
   }
@@ -289,7 +300,13 @@ __global__ void __launch_bounds__(128) kSdfBvh(const double* __restrict__ P, int
       const double R2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
       if (R2 > kFwnBeta * kFwnBeta * nd.in.r2) {
         const double R = sqrt(R2);
-        w += (nd.in.an[0] * d[0] + nd.in.an[1] * d[1] + nd.in.an[2] * d[2]) / (R2 * R);
+        const double R3 = R2 * R, R5 = R3 * R2;
+        const double* m = nd.in.m;
+        const double tr = m[0] + m[4] + m[8];
+        const double dmd = d[0] * (m[0] * d[0] + m[1] * d[1] + m[2] * d[2]) +
+                           d[1] * (m[3] * d[0] + m[4] * d[1] + m[5] * d[2]) +
+                           d[2] * (m[6] * d[0] + m[7] * d[1] + m[8] * d[2]);
+        w += (nd.in.an[0] * d[0] + nd.in.an[1] * d[1] + nd.in.an[2] * d[2]) / R3 + (tr / R3 - 3.0 * dmd / R5);
         continue;
       }
     }
@@ -309,7 +326,7 @@ its_status sdfBvh(its_ctx* ctx, const double* dP, int64_t m, const double* dV, c
   B.nf = nf;
   DevBuf<int32_t> left, right, parent;
   DevBuf<uint32_t> codes, idx, sc, leafTri, tk, tv;
-  DevBuf<double> lo, hi, an, ac, area;
+  DevBuf<double> lo, hi, an, ac, area, smom;
   DevBuf<unsigned> flag, overflow;
   if ((st = left.alloc(ctx, nf)) != ITS_OK || (st = right.alloc(ctx, nf)) != ITS_OK ||
       (st = parent.alloc(ctx, nodes)) != ITS_OK || (st = codes.alloc(ctx, nf)) != ITS_OK ||
@@ -318,6 +335,7 @@ its_status sdfBvh(its_ctx* ctx, const double* dP, int64_t m, const double* dV, c
       (st = tv.alloc(ctx, nf)) != ITS_OK || (st = lo.alloc(ctx, 3 * nodes)) != ITS_OK ||
       (st = hi.alloc(ctx, 3 * nodes)) != ITS_OK || (st = an.alloc(ctx, 3 * nodes)) != ITS_OK ||
       (st = ac.alloc(ctx, 3 * nodes)) != ITS_OK || (st = area.alloc(ctx, nodes)) != ITS_OK ||
+      (st = smom.alloc(ctx, 9 * nodes)) != ITS_OK ||
       (st = flag.zeros(ctx, nf)) != ITS_OK || (st = overflow.zeros(ctx, 1)) != ITS_OK)
     return st;
   // centroid bounds for the Morton quantisation
@@ -347,6 +365,7 @@ its_status sdfBvh(its_ctx* ctx, const double* dP, int64_t m, const double* dV, c
   B.an = an.p;
   B.ac = ac.p;
   B.area = area.p;
+  B.sm = smom.p;
   B.flag = flag.p;
   ITS_CU(ctx, cudaMemsetAsync(parent.p, 0xFF, nodes * 4, ctx->stream));
   if (nf > 1) {

@@ -8,9 +8,11 @@
 //   * distance: the exact minimum over all triangles of the per-triangle squared distance
 //     (pointTriSqDist, Ericson 5.1.5); subtrees whose box is farther than the best so far
 //     (times 1 + 1e-12) are skipped, so the minimum is the brute force's IEEE value;
-//   * sign: the fast winding number (Barill et al. 2018): a node whose area centroid is farther
-//     than beta = 3 times its box radius contributes its normal sum as a dipole, nearer nodes
-//     recurse (right child first), leaves add the exact solid angle; inside if w > 1/2.
+//   * sign: the fast winding number (Barill et al. 2018): a node whose area centroid c is
+//     farther than beta = 2 times its box radius contributes the second-order expansion of its
+//     triangles' solid angles about c -- the normal sum as a dipole plus the tensor
+//     M = sum_t an_t (c_t - c)^T (formed as sum_t an_t c_t^T - AN c^T) -- nearer nodes recurse
+//     (right child first), leaves add the exact solid angle; inside if w > 1/2.
 // The same tree, the same traversal order and the same IEEE operations as libits' kSdfBvh, so
 // distances are bit-identical and the winding numbers agree to the last bits of atan2.
 #include <omp.h>
@@ -25,13 +27,14 @@
 namespace orc {
 namespace {
 
-constexpr double kBeta = 3.0;
+constexpr double kBeta = 2.0;
 
 struct Bvh {
   int64_t n = 0;
   std::vector<int32_t> left, right;  // internal nodes; child >= 0 internal, < 0 leaf -(k+1)
   std::vector<uint32_t> leafTri;
   std::vector<double> lo, hi, an, ac, area;  // 2n-1 nodes: internal 0..n-2, leaves n-1..2n-2
+  std::vector<double> sm;                    // sum_t an_t c_t^T, 9 per node (row-major)
   int64_t nodeOf(int32_t c) const { return c < 0 ? (n - 1) + (-c - 1) : c; }
 };
 
@@ -104,6 +107,7 @@ Bvh build(const double* V, const int32_t* F, int64_t nf) {
   B.an.assign(3 * nodes, 0.0);
   B.ac.assign(3 * nodes, 0.0);
   B.area.assign(nodes, 0.0);
+  B.sm.assign(9 * nodes, 0.0);
   for (int64_t k = 0; k < nf; ++k) {
     const int64_t node = (nf - 1) + k;
     const uint32_t t = B.leafTri[k];
@@ -124,6 +128,9 @@ Bvh build(const double* V, const int32_t* F, int64_t nf) {
     B.an[3 * node + 1] = ny;
     B.an[3 * node + 2] = nz;
     B.area[node] = ar;
+    const double an3[3] = {nx, ny, nz};
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) B.sm[9 * node + 3 * i + j] = an3[i] * ((p[0][j] + p[1][j] + p[2][j]) / 3.0);
   }
   // internal nodes bottom-up (children before parents: a post-order walk from the root)
   if (nf > 1) {
@@ -147,6 +154,7 @@ Bvh build(const double* V, const int32_t* F, int64_t nf) {
         B.ac[3 * i + c] = B.ac[3 * a + c] + B.ac[3 * b + c];
       }
       B.area[i] = B.area[a] + B.area[b];
+      for (int e = 0; e < 9; ++e) B.sm[9 * i + e] = B.sm[9 * a + e] + B.sm[9 * b + e];
     }
   }
   return B;
@@ -227,7 +235,16 @@ double queryOne(const Bvh& B, const double* V, const int32_t* F, const double* q
       const double R2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
       if (R2 > kBeta * kBeta * r2) {
         const double R = std::sqrt(R2);
-        w += (B.an[3 * node] * d[0] + B.an[3 * node + 1] * d[1] + B.an[3 * node + 2] * d[2]) / (R2 * R);
+        const double R3 = R2 * R, R5 = R3 * R2;
+        double m[9];
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) m[3 * i + j] = B.sm[9 * node + 3 * i + j] - B.an[3 * node + i] * c[j];
+        const double tr = m[0] + m[4] + m[8];
+        const double dmd = d[0] * (m[0] * d[0] + m[1] * d[1] + m[2] * d[2]) +
+                           d[1] * (m[3] * d[0] + m[4] * d[1] + m[5] * d[2]) +
+                           d[2] * (m[6] * d[0] + m[7] * d[1] + m[8] * d[2]);
+        w += (B.an[3 * node] * d[0] + B.an[3 * node + 1] * d[1] + B.an[3 * node + 2] * d[2]) / R3 +
+             (tr / R3 - 3.0 * dmd / R5);
         continue;
       }
     }
