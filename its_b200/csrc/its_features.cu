@@ -39,7 +39,8 @@ struct NodeStats {
 
 // Face centroid, unit normal and fine node (fineCount when no fine node holds the centroid).
 __global__ void kFaceSamples(const double* __restrict__ V, const int32_t* __restrict__ F, int64_t nf, double3 g,
-                             double w0, int res, const uint32_t* __restrict__ morton, int64_t fineCount,
+                             double w0, int res, const unsigned long long* __restrict__ occ,
+                             const uint32_t* __restrict__ occRank, int64_t fineCount,
                              double* __restrict__ cent, double* __restrict__ nrm, uint32_t* __restrict__ node,
                              uint32_t* __restrict__ ids) {
   const int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -67,14 +68,8 @@ __global__ void kFaceSamples(const double* __restrict__ V, const int32_t* __rest
   uint32_t t = (uint32_t)fineCount;  // "no fine node" sorts after every node
   const int dx = (int)((cx - g.x) / w0), dy = (int)((cy - g.y) / w0), dz = (int)((cz - g.z) / w0);
   if (dx >= 0 && dy >= 0 && dz >= 0 && dx < res && dy < res && dz < res) {
-    const uint32_t m = mortonEncode((uint32_t)dx, (uint32_t)dy, (uint32_t)dz);
-    int64_t lo = 0, hi = fineCount;
-    while (lo < hi) {
-      const int64_t mid = (lo + hi) >> 1;
-      if (morton[mid] < m) lo = mid + 1;
-      else hi = mid;
-    }
-    if (lo < fineCount && morton[lo] == m) t = (uint32_t)lo;
+    const uint32_t k = fineNodeOf(occ, occRank, mortonEncode((uint32_t)dx, (uint32_t)dy, (uint32_t)dz));
+    if (k != kNone) t = k;
   }
   node[f] = t;
 }
@@ -436,7 +431,8 @@ its_status nodeSampleStats(its_ctx* ctx, SvoDevice& d, const double* V, const in
     return st;
   const int64_t fineCount = d.levelCount[0];
   kFaceSamples<<<gridFor(nf, 256), 256, 0, ctx->stream>>>(V, F, nf, make_double3(d.origin[0], d.origin[1], d.origin[2]),
-                                                         d.unit[0], d.res, d.nodeMorton, fineCount, cent.p, nrm.p,
+                                                         d.unit[0], d.res, (const unsigned long long*)d.fineOcc,
+                                                         d.fineRank, fineCount, cent.p, nrm.p,
                                                          node.p, fid.p);
   ITS_LAUNCHED(ctx);
   // stable sort by fine node ("none" = fineCount sorts last)

@@ -33,6 +33,8 @@ struct EvalParams {
   const uint32_t* parent;
   const double* vertPos;
   const uint64_t* vertKey;  // packed lattice coordinates and the vertex's corner of its owner
+  const unsigned long long* fineOcc;  // depth-0 nodes: Morton bitset and its word ranks
+  const uint32_t* fineRank;
   double winv[kMaxDepth];  // RN(1 / w_d), for divRn
 };
 
@@ -48,6 +50,8 @@ static EvalParams evalParams(const SvoDevice& d) {
   P.parent = d.nodeParent;
   P.vertPos = d.vertPos;
   P.vertKey = d.vertKey;
+  P.fineOcc = (const unsigned long long*)d.fineOcc;
+  P.fineRank = d.fineRank;
   for (int L = 0; L < kMaxDepth; ++L) P.winv[L] = 1.0 / (P.w0 * (double)(1u << L));
   return P;
 }
@@ -57,15 +61,8 @@ __device__ inline bool evalChain(const EvalParams& P, const double* __restrict__
                                  double pz, double& out) {
   const int dx = (int)((px - P.g.x) / P.w0), dy = (int)((py - P.g.y) / P.w0), dz = (int)((pz - P.g.z) / P.w0);
   if (dx < 0 || dy < 0 || dz < 0 || dx >= P.res || dy >= P.res || dz >= P.res) return false;
-  const uint32_t m = mortonEncode((uint32_t)dx, (uint32_t)dy, (uint32_t)dz);
-  int64_t lo = 0, hi = P.fineCount;  // first index with morton >= m
-  while (lo < hi) {
-    const int64_t mid = (lo + hi) >> 1;
-    if (P.morton[mid] < m) lo = mid + 1;
-    else hi = mid;
-  }
-  if (lo >= P.fineCount || P.morton[lo] != m) return false;
-  uint32_t t = (uint32_t)lo;
+  uint32_t t = fineNodeOf(P.fineOcc, P.fineRank, mortonEncode((uint32_t)dx, (uint32_t)dy, (uint32_t)dz));
+  if (t == kNone) return false;
   double sum = 0.0;
   for (int d = 0; d < P.depth && t != kNone; ++d) {
     uint32_t X, Y, Z;
@@ -718,16 +715,10 @@ __global__ void kPointGradient(const __grid_constant__ EvalParams P, const doubl
   bool found = false;
   const int dx = (int)((px - P.g.x) / P.w0), dy = (int)((py - P.g.y) / P.w0), dz = (int)((pz - P.g.z) / P.w0);
   if (dx >= 0 && dy >= 0 && dz >= 0 && dx < P.res && dy < P.res && dz < P.res) {
-    const uint32_t mc = mortonEncode((uint32_t)dx, (uint32_t)dy, (uint32_t)dz);
-    int64_t a = 0, b = P.fineCount;
-    while (a < b) {
-      const int64_t mid = (a + b) >> 1;
-      if (P.morton[mid] < mc) a = mid + 1;
-      else b = mid;
-    }
-    if (a < P.fineCount && P.morton[a] == mc) {
+    const uint32_t t0 = fineNodeOf(P.fineOcc, P.fineRank, mortonEncode((uint32_t)dx, (uint32_t)dy, (uint32_t)dz));
+    if (t0 != kNone) {
       found = true;
-      uint32_t t = (uint32_t)a;
+      uint32_t t = t0;
       for (int d = 0; d < P.depth && t != kNone; ++d) {
         uint32_t X, Y, Z;
         mortonDecode(P.morton[t], X, Y, Z);

@@ -151,6 +151,7 @@ struct SvoDevice {
   uint32_t* edgeKey = nullptr;
   uint32_t* edgeOwner = nullptr;
   uint64_t* fineOcc = nullptr;     // res^3-bit Morton bitset of depth-0 nodes
+  uint32_t* fineRank = nullptr;    // exclusive popcount prefix per word of fineOcc: node index by rank
   // face samples (centroids, unit normals) summed per node, finest depth first
   float* nodeSampleCnt = nullptr;  // per node
   double* nodeSamplePos = nullptr; // 3 per node: sum of centroids
@@ -171,6 +172,14 @@ struct SvoDevice {
     return L;
   }
 };
+
+// Index of the depth-0 node with Morton code m (depth-0 nodes are stored in Morton order), or
+// kNone: a bit test and a rank in the fine-node bitset instead of a binary search.
+__device__ __forceinline__ uint32_t fineNodeOf(const unsigned long long* occ, const uint32_t* rank, uint32_t m) {
+  const unsigned long long w = occ[m >> 6];
+  if (!((w >> (m & 63)) & 1ull)) return kNone;
+  return rank[m >> 6] + (uint32_t)__popcll(w & ((1ull << (m & 63)) - 1ull));
+}
 
 // Lattice position g + w*X per axis (createNode_1/2, SVO.cu:573-576).
 __host__ __device__ inline double latticePos(double g, double w, uint32_t X) { return g + w * (double)X; }

@@ -314,7 +314,7 @@ static void svoRelease(its_svo* s) {
   its_ctx* c = s->ctx;
   SvoDevice& d = s->d;
   void* ptrs[] = {d.voxels, d.nodeMorton, d.nodeParent, d.nodeChild0, d.nodeLeaf, d.nodeNb, d.vertLin, d.vertKey,
-                  d.vertOwner, d.vertPos, d.ebits, d.erank, d.edgeKey, d.edgeOwner, d.fineOcc,
+                  d.vertOwner, d.vertPos, d.ebits, d.erank, d.edgeKey, d.edgeOwner, d.fineOcc, d.fineRank,
                   d.nodeSampleCnt, d.nodeSamplePos, d.nodeSampleNrm, d.coincIds, d.rowParams, d.coincGeom};
   for (void* p : ptrs) devFree(c, p);
   for (int i = 0; i < kMaxDepth; ++i) { devFree(c, d.vbits[i]); devFree(c, d.vrank[i]); }
@@ -523,6 +523,12 @@ its_status svoBuild(its_ctx* ctx, const double* dV, int64_t nv, const int32_t* d
     ITS_CU(ctx, cudaMemsetAsync(d.fineOcc, 0, gridWords * 8, ctx->stream));
     kMarkFine<<<gridFor(nf0, 256), 256, 0, ctx->stream>>>(nf0, d.nodeMorton, (unsigned long long*)d.fineOcc);
     ITS_LAUNCHED(ctx);
+    if ((st = devAlloc(ctx, (void**)&d.fineRank, gridWords * 4)) != ITS_OK) return st;
+    const unsigned long long* occBits = (const unsigned long long*)d.fineOcc;
+    auto pc = [occBits] __device__(int64_t i) -> uint32_t { return (uint32_t)__popcll(occBits[i]); };
+    if ((st = scanExclusiveAlloc<uint32_t>(ctx, pc, gridWords, StorePrefix<uint32_t>{d.fineRank}, (uint32_t*)nullptr)) !=
+        ITS_OK)
+      return st;
   }
   // per-node sums of the face samples (features of the share network)
   ITS_CU(ctx, cudaEventRecord(ev[1], ctx->stream));
