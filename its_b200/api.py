@@ -394,15 +394,23 @@ class Svo:
         k = int(iso.shape[0])
         cnt = np.zeros(k, np.int64)
         L = lib()
-        self.ctx.check(L.its_eval_grid_mc(self.h, _ptr(lam), _ptr(o), _ptr(w), res, 1 if fast else 0, _ptr(iso), k,
-                                          None, None, _ptr(cnt)), "its_eval_grid_mc")
         if not triangles:
+            self.ctx.check(L.its_eval_grid_mc(self.h, _ptr(lam), _ptr(o), _ptr(w), res, 1 if fast else 0, _ptr(iso),
+                                              k, None, None, _ptr(cnt)), "its_eval_grid_mc")
             return cnt
-        outs = [np.zeros((max(int(c), 1), 3)) for c in cnt]
+        # one call into buffers sized for a surface crossing the grid (12 vertices per R^2 and
+        # level, pages committed only where written), a second only for levels that exceed them
+        cap = np.full(k, 12 * res * res + 1024, np.int64)
+        outs = [np.empty((int(c), 3)) for c in cap]
         P = (C.c_void_p * k)(*[o_.ctypes.data for o_ in outs])
-        cap = cnt.copy()
         self.ctx.check(L.its_eval_grid_mc(self.h, _ptr(lam), _ptr(o), _ptr(w), res, 1 if fast else 0, _ptr(iso), k,
                                           P, _ptr(cap), _ptr(cnt)), "its_eval_grid_mc")
+        if np.any(cnt > cap):
+            outs = [np.empty((max(int(c), 1), 3)) for c in cnt]
+            P = (C.c_void_p * k)(*[o_.ctypes.data for o_ in outs])
+            cap = cnt.copy()
+            self.ctx.check(L.its_eval_grid_mc(self.h, _ptr(lam), _ptr(o), _ptr(w), res, 1 if fast else 0, _ptr(iso),
+                                              k, P, _ptr(cap), _ptr(cnt)), "its_eval_grid_mc")
         return [x[:int(c)] for x, c in zip(outs, cnt)]
 
     def vertex_sdf(self, V, F):
