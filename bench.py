@@ -293,6 +293,19 @@ def run_ours(args):
     def max_ranks(v):
         return max_over_ranks(v, pg, "cuda")
 
+    if args.only == "pipeline":  # the facade-order pipeline alone (for profiling its stages)
+        from its_b200 import sharenet as _sn
+        params, norm = _sn.load()
+        net = ShareNet(ctx, batch=65536, params=params)
+        pipe = run_pipeline(ctx, net, norm, V, F, o, w, wl, timed, reps=max(1, args.steps))
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "only": "pipeline", "pipeline": pipe}), flush=True)
+        net.close()
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
+
     # ---- setup: octree and right-hand side (signed distance at the corner vertices) ------
     # the octree build timed warm from a device-resident mesh (the host arrays' upload apart)
     Vd, Fd = torch.from_numpy(np.ascontiguousarray(V)).cuda(), torch.from_numpy(np.ascontiguousarray(F, np.int32)).cuda()
@@ -926,7 +939,8 @@ def main():
     ap.add_argument("--config", default="c1", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline legs")
     ap.add_argument("--no-batch", action="store_true", help="skip the multi-mesh batch leg")
-    ap.add_argument("--only", default="all", choices=["all", "fit"], help="fit: time the fit steps only")
+    ap.add_argument("--only", default="all", choices=["all", "fit", "pipeline"],
+                    help="fit: time the fit steps only; pipeline: the facade-order pipeline only")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.gpus > 1 and "RANK" not in os.environ:
