@@ -14,6 +14,7 @@
 //   the reference's corner order, vertex counts from the case table, an exclusive scan of the
 //   counts, and the triangle soup written in voxel order by the scan's own downsweep (no
 //   compaction pass, no 18 R^3 preallocation).
+#include <algorithm>
 #include <cfloat>
 #include <vector>
 
@@ -335,22 +336,24 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
 // at a few table reads and four FP64 operations per term.
 constexpr int kSepX = 32, kSepY = 8, kSepThreads = kSepX * kSepY, kSepTileCap = 1024;
 
-template <int kSepZ>  // points per thread along z (the brick's depth)
+// T = float is the precision form's FP32 field: the same tables (formed in FP64, rounded once)
+// and the same terms, summed in FP32.
+template <typename T, int kSepZ>  // points per thread along z (the brick's depth)
 __global__ void __launch_bounds__(kSepThreads) kEvalGridSep(const __grid_constant__ EvalParams P,
                                                             const double* __restrict__ lambda, double3 o, double3 vs,
-                                                            int R, double* __restrict__ field) {
-  __shared__ double tLam[kSepTileCap];
+                                                            int R, T* __restrict__ field) {
+  __shared__ T tLam[kSepTileCap];
   __shared__ unsigned char tFlag[kSepTileCap];
-  __shared__ double hX[kSepX][4], hY[kSepY][4], hZ[kSepZ][4];  // [coordinate][corner side * 2 + corner bit]
+  __shared__ T hX[kSepX][4], hY[kSepY][4], hZ[kSepZ][4];  // [coordinate][corner side * 2 + corner bit]
   __shared__ int cX[kSepX], cY[kSepY], cZ[kSepZ];
   const int64_t M = (int64_t)R + 1;
   const int tid = threadIdx.x, tx = tid % kSepX, ty = tid / kSepX;
   const int64_t x0 = (int64_t)blockIdx.x * kSepX, y0 = (int64_t)blockIdx.y * kSepY, z0 = (int64_t)blockIdx.z * kSepZ;
   const int64_t xi = x0 + tx, yj = y0 + ty;
   const bool inXY = xi < M && yj < M;
-  double sum[kSepZ];
+  T sum[kSepZ];
 #pragma unroll
-  for (int q = 0; q < kSepZ; ++q) sum[q] = 0.0;
+  for (int q = 0; q < kSepZ; ++q) sum[q] = T(0);
   for (int d = 0; d < P.depth; ++d) {
     const double w = P.w0 * (double)(1u << d), wi = P.winv[d];
     const LatticeIndex& L = P.lat[d];
@@ -374,9 +377,9 @@ __global__ void __launch_bounds__(kSepThreads) kEvalGridSep(const __grid_constan
         h[2 * side] = hat1r(pa, pA, w, wi);
         h[2 * side + 1] = hat1r(pa, pB, w, wi);
       }
-      double* dst = a == 0 ? hX[k] : (a == 1 ? hY[k] : hZ[k]);
+      T* dst = a == 0 ? hX[k] : (a == 1 ? hY[k] : hZ[k]);
 #pragma unroll
-      for (int e = 0; e < 4; ++e) dst[e] = h[e];
+      for (int e = 0; e < 4; ++e) dst[e] = (T)h[e];
       (a == 0 ? cX : a == 1 ? cY : cZ)[k] = (int)c;
     }
     __syncthreads();
@@ -389,7 +392,7 @@ __global__ void __launch_bounds__(kSepThreads) kEvalGridSep(const __grid_constan
         for (int q = 0; q < kSepZ; ++q) {
           const double pz = o.z + (double)(z0 + q) * vs.z;
           const int64_t cx = cX[tx], cy = cY[ty], cz = cZ[q];
-          double s = sum[q];
+          T s = sum[q];
           for (int k = 0; k < 8; ++k) {
             const int64_t Lx = cx + (k & 1), Ly = cy + ((k >> 1) & 1), Lz = cz + ((k >> 2) & 1);
             if (Lx < 0 || Ly < 0 || Lz < 0 || Lx > lim || Ly > lim || Lz > lim) continue;
@@ -402,7 +405,7 @@ __global__ void __launch_bounds__(kSepThreads) kEvalGridSep(const __grid_constan
             if (fy <= 0.0) continue;
             const double fz = hat1r(pz, P.vertPos[3 * (int64_t)v + 2], w, wi);
             if (fz <= 0.0) continue;
-            s += lambda[v] * (fx * fy * fz);
+            s += (T)lambda[v] * ((T)fx * (T)fy * (T)fz);
           }
           sum[q] = s;
         }
@@ -418,7 +421,7 @@ __global__ void __launch_bounds__(kSepThreads) kEvalGridSep(const __grid_constan
         const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
         if (latticeHas(L, lin)) {
           const uint32_t v = latticeRank(L, lin);
-          tLam[t] = lambda[v];
+          tLam[t] = (T)lambda[v];
           f = (unsigned char)(1u | (((uint32_t)(P.vertKey[v] >> 37) & 7u) << 1));
         }
       }
@@ -427,31 +430,45 @@ __global__ void __launch_bounds__(kSepThreads) kEvalGridSep(const __grid_constan
     }
     if (__syncthreads_or(mine) && inXY) {
       const int rx = cX[tx] - (int)cx0, ry = cY[ty] - (int)cy0;
-      double hx[4], hy[4];
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        hx[e] = hX[tx][e];
-        hy[e] = hY[ty][e];
-      }
-#pragma unroll
-      for (int q = 0; q < kSepZ; ++q) {
-        const int rz = cZ[q] - (int)cz0;
-        double s = sum[q];
+      const T* hx = hX[tx];
+      const T* hy = hY[ty];
+      // A present corner adds lambda * ((hx * hy) * hz) even where a factor is 0: the term is
+      // then +-0 (NaN for a non-finite coefficient), as fieldAt's sum over the corners adds it,
+      // and a running sum that starts at +0 is never -0, so a +-0 term leaves it unchanged.
+      if (nz == 2) {
+        // Every point of the brick's z run lies in one cell (block-uniform): a corner is the
+        // same vertex for all of the thread's points, so its coefficient, bits and x*y factor
+        // are read once and its terms cost two products and a sum per point.
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
           const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
-          const int t = ((rx + ox) * ny + (ry + oy)) * nz + (rz + oz);
+          const int t = ((rx + ox) * ny + (ry + oy)) * 2 + oz;
           const unsigned f = tFlag[t];
           if (!(f & 1u)) continue;
-          const double fx = (f & 2u) ? hx[2 * ox + 1] : hx[2 * ox];
-          if (fx <= 0.0) continue;
-          const double fy = (f & 4u) ? hy[2 * oy + 1] : hy[2 * oy];
-          if (fy <= 0.0) continue;
-          const double fz = hZ[q][2 * oz + ((f >> 3) & 1u)];
-          if (fz <= 0.0) continue;
-          s += tLam[t] * (fx * fy * fz);
+          const T lam = tLam[t];
+          const T fxy = hx[2 * ox + ((f >> 1) & 1u)] * hy[2 * oy + ((f >> 2) & 1u)];
+          const int e = 2 * oz + (int)((f >> 3) & 1u);
+#pragma unroll
+          for (int q = 0; q < kSepZ; ++q) sum[q] += lam * (fxy * hZ[q][e]);
         }
-        sum[q] = s;
+      } else {
+#pragma unroll
+        for (int q = 0; q < kSepZ; ++q) {
+          const int rz = cZ[q] - (int)cz0;
+          T s = sum[q];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
+            const int t = ((rx + ox) * ny + (ry + oy)) * nz + (rz + oz);
+            const unsigned f = tFlag[t];
+            if (!(f & 1u)) continue;
+            const T fx = hx[2 * ox + ((f >> 1) & 1u)];
+            const T fy = hy[2 * oy + ((f >> 2) & 1u)];
+            const T fz = hZ[q][2 * oz + ((f >> 3) & 1u)];
+            s += tLam[t] * (fx * fy * fz);
+          }
+          sum[q] = s;
+        }
       }
     }
     __syncthreads();
@@ -644,23 +661,30 @@ static its_status evalGridTuned(its_ctx* ctx, const SvoDevice& d, const double* 
   // thread along z (FP64, when the brick's cell box fits its tile): every candidate computes
   // the same bits
   auto sepFits = [&](int z) {
-    return sizeof(T) == 8 && boxCorners(kSepX, vs.x, d.unit[0]) * boxCorners(kSepY, vs.y, d.unit[0]) *
-                                     boxCorners(z, vs.z, d.unit[0]) <= kSepTileCap;
+    return boxCorners(kSepX, vs.x, d.unit[0]) * boxCorners(kSepY, vs.y, d.unit[0]) * boxCorners(z, vs.z, d.unit[0]) <=
+           kSepTileCap;
   };
-  const bool sep4 = sepFits(4), sep8 = sepFits(8);
-  auto run = [&](int i) -> its_status {
-    switch (i) {
+  // Candidates, each computing the same bits for its type: FP64, four brick shapes of the
+  // point-wise kernel and the separable kernel with 4 or 8 points per thread along z (when the
+  // brick's cell box fits its tile); FP32, the separable kernel's two shapes where it fits (its
+  // rounding differs from the point-wise FP32 kernel's), else the brick shapes.
+  std::vector<int> cand;
+  if (sizeof(T) == 8 || !sepFits(4)) cand = {0, 1, 2, 3};
+  if (sepFits(4)) cand.push_back(4);
+  if (sepFits(8)) cand.push_back(5);
+  auto run = [&](int j) -> its_status {
+    switch (cand[j]) {
       case 1: return launchBricks<T, 32, 8, 2>(ctx, P, lam, o, vs, res, field);
       case 2: return launchBricks<T, 64, 4, 2>(ctx, P, lam, o, vs, res, field);
       case 3: return launchBricks<T, 16, 4, 4>(ctx, P, lam, o, vs, res, field);
       case 4:
       case 5: {
-        const int z = i == 5 ? 8 : 4;
+        const int z = cand[j] == 5 ? 8 : 4;
         const int64_t M = (int64_t)res + 1;
         const dim3 grid((unsigned)((M + kSepX - 1) / kSepX), (unsigned)((M + kSepY - 1) / kSepY),
                         (unsigned)((M + z - 1) / z));
-        if (z == 8) kEvalGridSep<8><<<grid, kSepThreads, 0, ctx->stream>>>(P, lam, o, vs, res, (double*)field);
-        else kEvalGridSep<4><<<grid, kSepThreads, 0, ctx->stream>>>(P, lam, o, vs, res, (double*)field);
+        if (z == 8) kEvalGridSep<T, 8><<<grid, kSepThreads, 0, ctx->stream>>>(P, lam, o, vs, res, field);
+        else kEvalGridSep<T, 4><<<grid, kSepThreads, 0, ctx->stream>>>(P, lam, o, vs, res, field);
         ITS_LAUNCHED(ctx);
         return ITS_OK;
       }
@@ -670,7 +694,7 @@ static its_status evalGridTuned(its_ctx* ctx, const SvoDevice& d, const double* 
   const std::string key = std::string("eval_grid/") + (sizeof(T) == 8 ? "f64" : "f32") + "/grid=" +
                           std::to_string(res) + "/octree=" + std::to_string(d.res) + "/depth=" + std::to_string(d.depth);
   int choice = 0;
-  its_status st = tuneChoice(ctx, key, sep8 ? 6 : (sep4 ? 5 : 4), sep8 ? 5 : (sep4 ? 4 : 0), run, &choice);
+  its_status st = tuneChoice(ctx, key, (int)cand.size(), cand.back() >= 4 ? (int)cand.size() - 1 : 0, run, &choice);
   if (st != ITS_OK) return st;
   return run(choice);
 }
@@ -1012,6 +1036,8 @@ its_status marchingCubesT(its_ctx* ctx, const FT* field, int res, const double o
   unsigned long long total = 0;
   if ((st = readScalar(ctx, tot.p, &total)) != ITS_OK) return st;
   *num_verts = (int64_t)total;
+  // only the vertices written leave the device (the rest of a host buffer is left untouched)
+  T.count = 3 * (size_t)std::min<int64_t>(capacity, (int64_t)total);
   if ((st = Cb.finish(ctx)) != ITS_OK) return st;
   if ((st = T.finish(ctx)) != ITS_OK) return st;
   ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));

@@ -198,10 +198,11 @@ def test_autotuner_changes_speed_not_bits(tmp_path):
         lam = svo.exact_start(b)
         field = svo.eval_grid(lam, o, w, 80)
         cube, tri, n = ctx.marching_cubes(field, 80, o, w, float(np.median(b)))
-        outs[mode] = (field, cube, tri, ctx.autotune_choices())
+        field32 = svo.eval_grid_f32(lam, o, w, 80)
+        outs[mode] = (field, cube, tri, ctx.autotune_choices(), field32)
         ctx.close()
     for mode in (1, 2):
-        assert np.array_equal(outs[mode][0], outs[0][0])
+        assert np.array_equal(outs[mode][0], outs[0][0]) and np.array_equal(outs[mode][4], outs[0][4])
         assert np.array_equal(outs[mode][1], outs[0][1]) and np.array_equal(outs[mode][2], outs[0][2])
     choices = outs[1][3]
     assert any(k.startswith("eval_grid/f64") for k in choices) and any(k.startswith("marching_cubes/f64") for k in choices)
