@@ -9,8 +9,10 @@
 // edge whose axial span overlaps the triangle's box (within 1e-9) and keeps plane hits that
 // pass the inside-triangle test. A hit lies inside the triangle, so the edge's two lateral
 // coordinates lie in the triangle's box; candidates are therefore enumerated on the fine
-// lattice around the box (one cell of margin) and checked against the fine-edge bitmap, then
-// the reference's own window and intersection tests decide. Same points, no slab sweep.
+// lattice lines of the box (and along the axis one cell either side of it, for the sweep's
+// tolerance) and checked against the fine-edge bitmap, then the reference's own window and
+// intersection tests decide. Same points, no slab sweep. Each step tests every item once to
+// count its hits and again only where it has hits, to write them.
 #include <algorithm>
 #include <cmath>
 
@@ -218,10 +220,10 @@ __device__ int faceHits(const SampleParams& S, const double* V, const int32_t* F
   }
   const double org[3] = {S.g.x, S.g.y, S.g.z};
   const uint32_t M = (uint32_t)S.res + 1u;
-  int cl[3], ch[3];
+  int fl[3], fh[3];
   for (int a = 0; a < 3; ++a) {
-    cl[a] = (int)floor((lo[a] - org[a]) / S.w0) - 1;
-    ch[a] = (int)floor((hi[a] - org[a]) / S.w0) + 2;
+    fl[a] = (int)floor((lo[a] - org[a]) / S.w0);
+    fh[a] = (int)floor((hi[a] - org[a]) / S.w0);
   }
   auto dot3 = [](const double* a, const double* b) {
     double s = a[0] * b[0];
@@ -236,10 +238,16 @@ __device__ int faceHits(const SampleParams& S, const double* V, const int32_t* F
   int n = 0;
   for (int axis = 0; axis < 3; ++axis) {
     const uint32_t ord = axis == 2 ? 0u : (axis == 1 ? 1u : 2u);
+    // Candidate fine edges along the axis. Along it: those whose span can meet the sweep window
+    // [lo - 1e-9, hi + 1e-9] (start cells floor(lo) - 1 .. floor(hi) + 1). Across it: a hit is
+    // the edge's own lateral coordinates (the edge direction has no lateral component) and lies
+    // in the triangle, so the lattice lines in [lo, hi] to rounding: floor(lo) .. floor(hi) + 1.
+    // (A cell quotient's rounding moves a floor by at most one, toward lines a cell outside.)
     int l0[3], l1[3];
     for (int a = 0; a < 3; ++a) {
-      l0[a] = cl[a] < 0 ? 0 : cl[a];
-      l1[a] = ch[a] > S.res ? S.res : ch[a];
+      const int c0 = a == axis ? fl[a] - 1 : fl[a], c1 = fh[a] + 1;
+      l0[a] = c0 < 0 ? 0 : c0;
+      l1[a] = c1 > S.res ? S.res : c1;
     }
     if (l1[axis] > S.res - 1) l1[axis] = S.res - 1;  // edge start along its axis
     for (int X = l0[0]; X <= l1[0]; ++X)
@@ -281,6 +289,18 @@ struct FaceEmit {
   __device__ void operator()(int64_t t, uint32_t prefix, uint32_t count) const {
     if (count) faceHits(fs.S, fs.V, fs.F, t, out + 3 * (int64_t)prefix);
   }
+};
+
+// The hit count of every item, evaluated once and stored; the compaction's two scans read the
+// stored counts and the emitting pass re-runs the hit test only for items that have hits.
+template <class Step>
+__global__ void __launch_bounds__(128) kCountHits(Step f, int64_t n, uint32_t* __restrict__ cnt) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) cnt[i] = f(i);
+}
+struct StoredCount {
+  const uint32_t* cnt;
+  __device__ uint32_t operator()(int64_t i) const { return cnt[i]; }
 };
 
 static uint64_t tableSize(int64_t keys) {
@@ -333,15 +353,19 @@ its_status its_shell_samples(its_svo* s, const double* verts, int64_t nverts, co
   kEdgeInsert<<<gridFor(slots, 256), 256, 0, ctx->stream>>>(F.d, slots, ekeys.p, eown.p, tsz - 1);
   ITS_LAUNCHED(ctx);
   EdgeStep es{S, V.d, F.d, ekeys.p, eown.p, tsz - 1};
-  DevBuf<uint32_t> tot;
-  if ((st = tot.zeros(ctx, 3)) != ITS_OK) return st;
+  DevBuf<uint32_t> tot, ecnt;
+  if ((st = tot.zeros(ctx, 3)) != ITS_OK || (st = ecnt.alloc(ctx, slots)) != ITS_OK) return st;
+  kCountHits<<<gridFor(slots, 128), 128, 0, ctx->stream>>>(es, slots, ecnt.p);
+  ITS_LAUNCHED(ctx);
   auto nowrite = [] __device__(int64_t, uint32_t, uint32_t) {};
-  if ((st = scanExclusiveAlloc<uint32_t>(ctx, es, slots, nowrite, tot.p)) != ITS_OK) return st;
+  if ((st = scanExclusiveAlloc<uint32_t>(ctx, StoredCount{ecnt.p}, slots, nowrite, tot.p)) != ITS_OK) return st;
   uint32_t nRaw = 0;
   if ((st = readScalar(ctx, tot.p, &nRaw)) != ITS_OK) return st;
   DevBuf<double> raw;
   if ((st = raw.alloc(ctx, 3 * (size_t)(nRaw ? nRaw : 1))) != ITS_OK) return st;
-  if ((st = scanExclusiveAlloc<uint32_t>(ctx, es, slots, EdgeEmit{es, raw.p}, tot.p)) != ITS_OK) return st;
+  if ((st = scanExclusiveAlloc<uint32_t>(ctx, StoredCount{ecnt.p}, slots, EdgeEmit{es, raw.p}, tot.p)) != ITS_OK)
+    return st;
+  ecnt.reset();
   ekeys.reset();
   eown.reset();
   // exact-duplicate removal
@@ -367,7 +391,11 @@ its_status its_shell_samples(its_svo* s, const double* verts, int64_t nverts, co
   raw.reset();
   // face step
   FaceStep fs{S, V.d, F.d};
-  if ((st = scanExclusiveAlloc<uint32_t>(ctx, fs, nfaces, nowrite, tot.p + 2)) != ITS_OK) return st;
+  DevBuf<uint32_t> fcnt;
+  if ((st = fcnt.alloc(ctx, nfaces)) != ITS_OK) return st;
+  kCountHits<<<gridFor(nfaces, 128), 128, 0, ctx->stream>>>(fs, nfaces, fcnt.p);
+  ITS_LAUNCHED(ctx);
+  if ((st = scanExclusiveAlloc<uint32_t>(ctx, StoredCount{fcnt.p}, nfaces, nowrite, tot.p + 2)) != ITS_OK) return st;
   uint32_t nFace = 0;
   if ((st = readScalar(ctx, tot.p + 2, &nFace)) != ITS_OK) return st;
   const int64_t total = (int64_t)nEdge + nFace;
@@ -387,8 +415,8 @@ its_status its_shell_samples(its_svo* s, const double* verts, int64_t nverts, co
     dst = all.p;
   }
   if (nEdge && dst) ITS_CU(ctx, cudaMemcpyAsync(dst, edgePts.p, (size_t)nEdge * 24, cudaMemcpyDeviceToDevice, ctx->stream));
-  if (dst && (st = scanExclusiveAlloc<uint32_t>(ctx, fs, nfaces, FaceEmit{fs, dst + 3 * (int64_t)nEdge}, tot.p + 2)) !=
-                 ITS_OK)
+  if (dst && (st = scanExclusiveAlloc<uint32_t>(ctx, StoredCount{fcnt.p}, nfaces, FaceEmit{fs, dst + 3 * (int64_t)nEdge},
+                                                tot.p + 2)) != ITS_OK)
     return st;
   if (keep < total && keep > 0)
     ITS_CU(ctx, cudaMemcpyAsync(O.d, all.p, (size_t)keep * 24, cudaMemcpyDeviceToDevice, ctx->stream));

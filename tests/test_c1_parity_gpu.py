@@ -3,6 +3,7 @@ depth 9 (res 256), marching cubes at 512^3.
 
 Bars:
   * octree, occupancy, neighbours, corner vertices and fine edges: bit-exact with the oracle;
+  * shell samples (edge and face intersections): the same point set as the oracle's;
   * right-hand side: distances bit-exact with the oracle's BVH signed distance, and the same
     signs (both take the sign from the same fast winding number over the same tree);
   * the 513^3 FP64 lattice field of the FP64 LSCG fit: bit-exact with the oracle's, and the
@@ -50,6 +51,20 @@ def test_c1_octree_bit_exact(c1):
     assert np.array_equal(go, ro) and np.array_equal(gp, rp)
     for a, b in zip(gpu.edges(), ref.edges()):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.gpu
+def test_c1_shell_samples_same_point_set(c1):
+    # edge and face intersections (ThinShells::cpIntersectionPoints): the same points, the
+    # same split between the two kinds; the GPU emits them in mesh order, the oracle in the
+    # reference's sweep order
+    V, F, o, w, gpu, ref = c1
+    pts_ref, ne_ref = ref.intersections()
+    pts_gpu, ne_gpu = gpu.shell_samples(V, F)
+    assert ne_gpu == ne_ref and len(pts_gpu) == len(pts_ref)
+    key = lambda P: P[np.lexsort((P[:, 2], P[:, 1], P[:, 0]))]  # noqa: E731
+    assert np.array_equal(key(pts_gpu[:ne_gpu]), key(pts_ref[:ne_ref]))
+    assert np.array_equal(key(pts_gpu[ne_gpu:]), key(pts_ref[ne_ref:]))
 
 
 @pytest.mark.gpu
