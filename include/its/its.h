@@ -282,7 +282,8 @@ its_status its_eval_grid(its_svo* svo, const double* lambda, const double origin
                          int res, double* field);
 /* MC::marching_cubes (src/cuAcc/MarchingCubes/MarchingCubes.h:136-139) on a lattice field:
    cube_index (res^3 bytes, NULL allowed) with bit i = field[corner i] < iso in the corner
-   order of MarchingCubes.cu:233-241; triangle vertices (3 doubles each) in voxel order.
+   order of MarchingCubes.cu:233-241; triangle vertices (3 doubles each) in voxel order: the
+   first min(capacity, num_verts) are written, the rest of tri_verts is left as it was.
    With tri_verts NULL only num_verts is returned. */
 its_status its_marching_cubes(its_ctx* ctx, const double* field, int res, const double origin[3],
                               const double width[3], double iso, uint8_t* cube_index, double* tri_verts,

@@ -130,6 +130,7 @@ its_status its_destroy(its_ctx* c) {
   if (!c) return ITS_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  its::hostIoRelease(c);
   if (c->ownStream) cudaStreamDestroy(c->ownStream);
   if (c->pool) cudaMemPoolDestroy(c->pool);  // released once nothing allocated from it is live
   if (c->pinned) cudaFreeHost(c->pinned);

@@ -8,6 +8,10 @@
 
 #include "its_internal.cuh"
 
+namespace its {
+struct HostIo;  // pinned staging and host threads for large copies into pageable memory (its_hostio.cu)
+}
+
 struct its_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -25,6 +29,7 @@ struct its_ctx {
   // graph's plan) instead of the pool, so the graph holds no allocation nodes
   uint8_t* arena = nullptr;
   size_t arenaCap = 0, arenaOff = 0;
+  its::HostIo* hostio = nullptr;  // created on the first large copy into pageable memory
 };
 
 namespace its {
@@ -162,6 +167,12 @@ struct InArg {
     return ITS_OK;
   }
 };
+// Device-to-host copy of bytes into pageable dst through pinned chunks, the chunks copied on
+// by several host threads; returns with the data in dst (its_hostio.cu).
+constexpr size_t kStagedCopyMin = 8u << 20;
+its_status copyToHostStaged(its_ctx* ctx, void* dst, const void* src, size_t bytes);
+void hostIoRelease(its_ctx* ctx);
+
 // A written argument: device scratch copied back to a host destination by finish().
 template <typename T>
 struct OutArg {
@@ -182,8 +193,14 @@ struct OutArg {
     host = dst;
     return ITS_OK;
   }
+  // Large results into pageable memory go through copyToHostStaged (synchronous), the rest
+  // by one asynchronous copy that the caller's stream synchronisation completes.
   its_status finish(its_ctx* ctx) {
-    if (host && count) ITS_CU(ctx, cudaMemcpyAsync(host, d, count * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+    if (!host || !count) return ITS_OK;
+    const size_t bytes = count * sizeof(T);
+    if (bytes >= kStagedCopyMin && !ctx->arena && ptrClass(host, ctx->device) == PtrClass::Pageable)
+      return copyToHostStaged(ctx, host, d, bytes);
+    ITS_CU(ctx, cudaMemcpyAsync(host, d, bytes, cudaMemcpyDeviceToHost, ctx->stream));
     return ITS_OK;
   }
 };
