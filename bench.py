@@ -81,13 +81,14 @@ def load_peaks():
         return 6650.0, 1590.0, "fallback"
 
 
-def profile_traffic(name):
-    """DRAM bytes per launch of a kernel from its committed ncu summary (a line
-    `traffic_bytes_per_launch: N` in profiles/<name>*.md), or None."""
+def profile_traffic(name, cfg):
+    """DRAM bytes per launch of a kernel on workload `cfg` from its committed ncu summary (a
+    line `traffic_bytes_per_launch: N` in profiles/<name>_<cfg>_*.md), or None when no capture
+    of that kernel on that workload is committed."""
     pdir = os.path.join(ROOT, "profiles")
     try:
         for fn in sorted(os.listdir(pdir)):
-            if fn.startswith(name) and fn.endswith(".md"):
+            if fn.startswith(name + "_" + cfg + "_") and fn.endswith(".md"):
                 for line in open(os.path.join(pdir, fn)):
                     if line.strip().startswith("traffic_bytes_per_launch:"):
                         return int(float(line.split(":", 1)[1].strip().split()[0]))
@@ -404,7 +405,7 @@ def run_ours(args):
     hbm_peak, tensor_peak, peak_kind = load_peaks()
     mlp_flop = 2.0 * rows * MLP_MACS_PER_ROW
     mlp_tflops = mlp_flop / (mlp_ms * 1e-3) / 1e12
-    traffic = profile_traffic("kMlpForwardFused")
+    traffic = profile_traffic("kMlpForwardFused", wl["mesh"])
 
     # ---- breakdown of the learned fit ----------------------------------------------------
     learned_bytes = 3 * 48 * n + 2 * 256 * rows
@@ -618,7 +619,7 @@ def run_ours(args):
                               "achieved": round(spmv_achieved, 1), "peak": hbm_peak, "unit": "GB/s",
                               "frac": round(spmv_achieved / hbm_peak, 4), "peak_kind": peak_kind,
                               "bytes_per_launch": spmv_bytes, "launch_ms": round(spmv[dom], 5),
-                              "traffic": profile_traffic("kSpmvBinned")},
+                              "traffic": profile_traffic("kSpmvBinned", wl["mesh"])},
             "roofline_learned_step": {"bound": "hbm", "kernel": "the learned fit step as a whole (its 9 kernels)",
                                       "achieved": round(learned_bytes / (fit_ms * 1e-3) / 1e9, 1), "peak": hbm_peak,
                                       "unit": "GB/s", "frac": round(learned_bytes / (fit_ms * 1e-3) / 1e9 / hbm_peak, 4),
@@ -634,7 +635,7 @@ def run_ours(args):
                                "achieved": round(8 * M ** 3 / (field_ms * 1e-3) / 1e9, 1), "peak": hbm_peak,
                                "unit": "GB/s", "frac": round(8 * M ** 3 / (field_ms * 1e-3) / 1e9 / hbm_peak, 4),
                                "bytes_per_launch": 8 * M ** 3, "launch_ms": round(field_ms, 4),
-                               "traffic": profile_traffic("kEvalGridSep")},
+                               "traffic": profile_traffic("kEvalGridSep", wl["mesh"])},
             "mc_f32": mc32,
             "mc_fast": mc_fast,
             "pipeline": pipeline,
