@@ -47,6 +47,15 @@ __device__ __forceinline__ float geluF(float z) {
   const float h = 0.5f * z;
   return fmaf(h, tanhApprox(u), h);
 }
+// Two lanes of geluF with the packed FP32 instructions (each lane one IEEE FP32 operation of
+// geluF's, in geluF's order: the same bits at half the instructions).
+__device__ __forceinline__ float2 geluF2(float2 z) {
+  const float2 p = __ffma2_rn(make_float2(kGeluK0 * kGeluK1, kGeluK0 * kGeluK1), __fmul2_rn(z, z),
+                              make_float2(kGeluK0, kGeluK0));
+  const float2 u = __fmul2_rn(z, p);
+  const float2 h = __fmul2_rn(make_float2(0.5f, 0.5f), z);
+  return __ffma2_rn(h, make_float2(tanhApprox(u.x), tanhApprox(u.y)), h);
+}
 // d gelu / dz = (1 + t)/2 + z/2 (1 - t^2) sqrt(2/pi) (1 + 3 * 0.044715 z^2), t = tanh(u)
 __device__ __forceinline__ float geluGrad(float z) {
   const float z2 = z * z;
@@ -253,11 +262,25 @@ constexpr int kFusedSmem = 16384 /*W1*/ + 32768 /*W2*/ + 32768 /*W3*/ + kFusedSl
                            4 * 128 * 4 /*b1 b2 b3 w4*/ + kFusedSlots * kFusedGroups * 128 * 4 /*partial sums*/ + 64 +
                            1024;
 
-__device__ __forceinline__ void loadWeightTile(uint8_t* dst, const bf16* __restrict__ W, int K, int tid, int nthreads) {
-  // W: 128 rows x K bf16, row-major (K-major B operand); K/64 swizzled blocks of 128 x 128 B
-  for (int i = tid; i < 128 * (K / 8); i += nthreads) {
-    const int r = i / (K / 8), c = i % (K / 8);
-    *(uint4*)(dst + (c >> 3) * 16384 + umma::swizzledChunk(r, c & 7)) = __ldg((const uint4*)(W + (int64_t)r * K + c * 8));
+// The fused kernel's shared-memory image of the weights, built once per parameter update:
+// W1 (16 KB), W2 and W3 (32 KB each) as 128 x K bf16 K-major B operands in 128-byte-swizzled
+// blocks of 128 x 64, then b1, b2, b3 and the BF16-rounded w4 (512 floats). A CTA fetches it
+// with a few bulk copies.
+constexpr int kImgWeights = 16384 + 32768 + 32768, kImgBytes = kImgWeights + 4 * 128 * 4;
+__global__ void kPackFusedImage(const float* __restrict__ P, const bf16* __restrict__ W1, const bf16* __restrict__ W2,
+                                const bf16* __restrict__ W3, const float* __restrict__ w4r, uint8_t* __restrict__ img) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;  // one 16-byte chunk of a weight row
+  if (i < 128 * 8 + 2 * 128 * 16) {
+    const bf16* W = i < 1024 ? W1 : (i < 1024 + 2048 ? W2 : W3);
+    const int K = i < 1024 ? kIn : kHid;
+    const int j = i < 1024 ? i : (i - 1024) % 2048;
+    const int r = j / (K / 8), c = j % (K / 8);
+    uint8_t* dst = img + (i < 1024 ? 0 : (i < 1024 + 2048 ? 16384 : 16384 + 32768));
+    *(uint4*)(dst + (c >> 3) * 16384 + umma::swizzledChunk(r, c & 7)) = *(const uint4*)(W + (int64_t)r * K + c * 8);
+  }
+  if (i < 512) {
+    float* b = (float*)(img + kImgWeights);
+    b[i] = i < 384 ? P[(i < 128 ? kOffB1 : (i < 256 ? kOffB2 : kOffB3)) + (i & 127)] : w4r[i - 384];
   }
 }
 
@@ -273,9 +296,8 @@ __device__ __forceinline__ void slotSync(int s) {
 // group's quarter of the columns in order and the first group adds the four partial sums in
 // order, as the layer-by-layer kernels do, so the result is theirs bit for bit.
 __global__ void __launch_bounds__(kFusedThreads, 1)
-    kMlpForwardFused(const float* __restrict__ X, int64_t n, const bf16* __restrict__ W1, const bf16* __restrict__ W2,
-                     const bf16* __restrict__ W3, const float* __restrict__ P, const float* __restrict__ w4r,
-                     float* __restrict__ out, int* __restrict__ err, const int64_t* __restrict__ shareIds,
+    kMlpForwardFused(const float* __restrict__ X, int64_t n, const uint8_t* __restrict__ img,
+                     const float* __restrict__ P, float* __restrict__ out, int* __restrict__ err, const int64_t* __restrict__ shareIds,
                      double* __restrict__ shares, float shareScale, float shareMean, const bf16* __restrict__ Xt) {
   using namespace umma;
   extern __shared__ uint8_t smemRaw[];
@@ -289,28 +311,30 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   uint8_t* sH = sX + 16384;
   float* sBias = (float*)(sW3 + 32768 + kFusedSlots * (16384 + 32768));  // b1, b2, b3, w4 (128 each)
   float* sPart = sBias + 4 * 128 + s * kFusedGroups * 128;               // [group][row] partial sums
-  uint64_t* mbar = (uint64_t*)(sBias + 4 * 128 + kFusedSlots * kFusedGroups * 128);  // MMA, then input loads
-  uint32_t* tslot = (uint32_t*)(mbar + 2 * kFusedSlots);
+  uint64_t* mbar = (uint64_t*)(sBias + 4 * 128 + kFusedSlots * kFusedGroups * 128);  // MMA, input loads, weights
+  uint32_t* tslot = (uint32_t*)(mbar + 2 * kFusedSlots + 1);
+  const uint32_t barW = smemAddr(mbar + 2 * kFusedSlots);
   if (warp == 0) tmemAlloc(smemAddr(tslot), 128 * kFusedSlots);
-  if (tid == 0)
-    for (int k = 0; k < 2 * kFusedSlots; ++k) mbarInit(smemAddr(mbar + k), 1);
-  for (int i = tid; i < 4 * 128; i += blockDim.x)
-    sBias[i] = i < 384 ? P[(i < 128 ? kOffB1 : (i < 256 ? kOffB2 : kOffB3)) + (i & 127)] : w4r[i - 384];
-  loadWeightTile(sW1, W1, kIn, tid, blockDim.x);
-  loadWeightTile(sW2, W2, kHid, tid, blockDim.x);
-  loadWeightTile(sW3, W3, kHid, tid, blockDim.x);
-  // the weights were written before the previous kernel started; the features are its output
+  if (tid == 0) {
+    for (int k = 0; k < 2 * kFusedSlots + 1; ++k) mbarInit(smemAddr(mbar + k), 1);
+    // the weight image in five 16 KB bulk copies and the biases in one; the image was written
+    // before the previous kernel started (only the features are its output)
+    mbarArriveExpectTx(barW, kImgBytes);
+#pragma unroll
+    for (int k = 0; k < kImgWeights / 16384; ++k) bulkLoad(smemAddr(sW1 + k * 16384), img + k * 16384, 16384, barW);
+    bulkLoad(smemAddr(sBias), img + kImgWeights, kImgBytes - kImgWeights, barW);
+  }
   gridDependencyWait();
   gridDependents();
   fenceBefore();
   __syncthreads();
   fenceAfter();
+  bool ok = mbarWait(barW, 0);
   const uint32_t tmem = *tslot + 128u * s;                 // this tile slot's 128 columns
   const uint32_t lane = (uint32_t)((warp & 3) * 32) << 16;  // the warp's TMEM lanes
   constexpr uint32_t idesc = idescBf16(128, kHid);
   const uint32_t bar = smemAddr(mbar + s), barX = smemAddr(mbar + kFusedSlots + s);
   uint32_t phase = 0, phaseX = 0;
-  bool ok = true;
   const float* b1 = sBias;
   const float* b2 = sBias + 128;
   const float* b3 = sBias + 256;
@@ -379,19 +403,29 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
       const int n0 = kGroupCols * grp;
       float v[kGroupCols];
       tmemLoad32(tmem + lane + (uint32_t)n0, v);
+      // two columns per packed FP32 instruction; the output unit's sum stays in column order
       if (layer < 2) {  // hidden layer: the next layer's A operand
 #pragma unroll
         for (int h = 0; h < kGroupCols / 8; ++h) {
-          __align__(16) bf16 q[8];
+          __align__(16) __nv_bfloat162 q[4];
 #pragma unroll
-          for (int e = 0; e < 8; ++e) q[e] = __float2bfloat16_rn(geluF(v[h * 8 + e] + bias[n0 + h * 8 + e]));
+          for (int e = 0; e < 4; ++e) {
+            const int j = h * 8 + 2 * e;
+            const float2 b = *(const float2*)(bias + n0 + j);
+            q[e] = __float22bfloat162_rn(geluF2(__fadd2_rn(make_float2(v[j], v[j + 1]), b)));
+          }
           const int c = (n0 >> 3) + h;
           *(uint4*)(sH + (c >> 3) * 16384 + swizzledChunk(row, c & 7)) = *(const uint4*)q;
         }
       } else {  // output unit: this group's quarter of the columns, in order
 #pragma unroll
-        for (int j = 0; j < kGroupCols; ++j)
-          o += __bfloat162float(__float2bfloat16_rn(geluF(v[j] + bias[n0 + j]))) * w4[n0 + j];
+        for (int j = 0; j < kGroupCols; j += 2) {
+          const float2 b = *(const float2*)(bias + n0 + j);
+          const float2 g = __bfloat1622float2(__float22bfloat162_rn(geluF2(__fadd2_rn(make_float2(v[j], v[j + 1]), b))));
+          const float2 t = __fmul2_rn(g, *(const float2*)(w4 + n0 + j));
+          o += t.x;
+          o += t.y;
+        }
       }
     }
     if (grp > 0) sPart[grp * 128 + row] = o;
@@ -586,6 +620,7 @@ struct its_mlp {
   int64_t step = 0;
   bf16 *W1, *W1t, *W2, *W2t, *W3, *W3t;
   float* w4r;
+  uint8_t* img;  // the fused inference kernel's shared-memory image of the parameters
   // batch buffers
   bf16 *Xb, *Xt, *H1, *H1t, *H2, *H2t, *H3, *dZ3, *dZ3t, *dZ2, *dZ2t, *dZ1t;
   float *Z1, *Z2, *yb, *dOut, *sqErr, *out, *part1, *part2, *part3;
@@ -604,6 +639,9 @@ namespace its {
 static its_status mlpCast(its_mlp* h) {
   kCastWeights<<<gridFor(kHid * kHid, 256), 256, 0, h->ctx->stream>>>(h->P, h->W1, h->W1t, h->W2, h->W2t, h->W3,
                                                                       h->W3t, h->w4r);
+  ITS_LAUNCHED(h->ctx);
+  kPackFusedImage<<<gridFor(128 * 8 + 2 * 128 * 16, 256), 256, 0, h->ctx->stream>>>(h->P, h->W1, h->W2, h->W3, h->w4r,
+                                                                                    h->img);
   ITS_LAUNCHED(h->ctx);
   return ITS_OK;
 }
@@ -675,8 +713,7 @@ static its_status launchFused(its_mlp* h, const float* X, int64_t n, float* out,
   const int64_t tiles = (n + 127) / 128, ctas = (tiles + kFusedSlots - 1) / kFusedSlots;
   const unsigned grid = (unsigned)(ctas < ctx->numSMs ? ctas : ctx->numSMs);
   return launchDependent(ctx, afterKernel, kMlpForwardFused, grid, kFusedThreads, kFusedSmem, ctx->stream, X, n,
-                         (const bf16*)h->W1, (const bf16*)h->W2, (const bf16*)h->W3, (const float*)h->P,
-                         (const float*)h->w4r, out, h->err, ids, shares, scale, mean, Xt);
+                         (const uint8_t*)h->img, (const float*)h->P, out, h->err, ids, shares, scale, mean, Xt);
 }
 its_status mlpInfer(its_mlp* h, const float* X, int64_t n, float* out, bool afterKernel) {
   return launchFused(h, X, n, out, nullptr, nullptr, 0.0f, 0.0f, afterKernel);
@@ -715,7 +752,7 @@ its_status its_mlp_create(its_ctx* ctx, int64_t batch, its_mlp** out) {
   };
   A(&h->P, kNumParams); A(&h->Mo, kNumParams); A(&h->Ve, kNumParams); A(&h->G, kNumParams); A(&h->loss, 1);
   A(&h->W1, kHid * kIn); A(&h->W1t, kHid * kIn); A(&h->W2, kHid * kHid); A(&h->W2t, kHid * kHid);
-  A(&h->W3, kHid * kHid); A(&h->W3t, kHid * kHid); A(&h->w4r, kHid);
+  A(&h->W3, kHid * kHid); A(&h->W3t, kHid * kHid); A(&h->w4r, kHid); A(&h->img, kImgBytes);
   A(&h->Xb, B * kIn); A(&h->Xt, B * kIn); A(&h->H1, B * kHid); A(&h->H1t, B * kHid); A(&h->H2, B * kHid);
   A(&h->H2t, B * kHid); A(&h->H3, B * kHid); A(&h->dZ3, B * kHid); A(&h->dZ3t, B * kHid); A(&h->dZ2, B * kHid);
   A(&h->dZ2t, B * kHid); A(&h->dZ1t, B * kHid); A(&h->Z1, B * kHid); A(&h->Z2, B * kHid); A(&h->yb, B);
@@ -730,6 +767,7 @@ its_status its_mlp_create(its_ctx* ctx, int64_t batch, its_mlp** out) {
   cudaMemsetAsync(h->Mo, 0, kNumParams * 4, ctx->stream);
   cudaMemsetAsync(h->Ve, 0, kNumParams * 4, ctx->stream);
   cudaMemsetAsync(h->err, 0, 4, ctx->stream);
+  cudaMemsetAsync(h->img, 0, kImgBytes, ctx->stream);
   // the fused inference kernel's shared memory, set here once (not inside a graph capture)
   ITS_CU(ctx, cudaFuncSetAttribute(kMlpForwardFused, cudaFuncAttributeMaxDynamicSharedMemorySize, kFusedSmem));
   *out = h;
