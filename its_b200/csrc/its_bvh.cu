@@ -37,21 +37,22 @@ struct BvhDevice {
   unsigned* flag = nullptr;
 };
 
-// The traversal's view of the tree: one 128-byte record per node, so a visit touches one
-// cache line. Internal nodes carry their box, the fast winding number's expansion centre
-// (area-weighted centroid sum / area), squared radius, normal sum and area, and the children;
-// leaves carry their box and their triangle's corners. The values are those the traversal
-// used to form per visit from the build's arrays (same operations), so results are unchanged.
+// The traversal's view of the tree: one 192-byte record per node in three 64-byte lines. Line 0
+// holds what every visit reads -- the box, the children and the area; lines 1-2 hold what only
+// some visits read: for an internal node the fast winding number's expansion centre
+// (area-weighted centroid sum / area), squared radius, normal sum and second-order tensor, for
+// a leaf its triangle's corners. The values are those the traversal used to form per visit
+// from the build's arrays (same operations), so results are unchanged.
 struct __align__(64) BvhNode {
   double lo[3], hi[3];
+  int32_t left, right;  // internal nodes: child index; >= 0 internal, < 0 leaf -(k+1)
+  double area;
   union {
     struct {
       double c[3];
       double r2;
       double an[3];
-      double area;
       double m[9];  // sum_t an_t (c_t - c)^T about the node's centre c
-      int32_t left, right;
     } in;
     double tri[9];
   };
@@ -203,9 +204,11 @@ __global__ void kPackNodes(const double* __restrict__ V, const int32_t* __restri
     const uint32_t t = B.leafTri[k - (n - 1)];
     for (int c = 0; c < 3; ++c)
       for (int a = 0; a < 3; ++a) r.tri[3 * c + a] = V[3 * (int64_t)F[3 * t + c] + a];
+    r.left = r.right = 0;
+    r.area = 0.0;
   } else {
     const double A = B.area[k];
-    r.in.area = A;
+    r.area = A;
     r.in.r2 = 0.0;
     for (int a = 0; a < 3; ++a) {
       r.in.an[a] = B.an[3 * k + a];
@@ -221,8 +224,8 @@ __global__ void kPackNodes(const double* __restrict__ V, const int32_t* __restri
     }
     for (int i = 0; i < 3; ++i)
       for (int j = 0; j < 3; ++j) r.in.m[3 * i + j] = B.sm[9 * k + 3 * i + j] - r.in.an[i] * r.in.c[j];
-    r.in.left = B.left[k];
-    r.in.right = B.right[k];
+    r.left = B.left[k];
+    r.right = B.right[k];
   }
   out[k] = r;
 }
@@ -236,10 +239,14 @@ __device__ inline double boxDist2(const double* lo, const double* hi, const doub
   return s;
 }
 
-__global__ void __launch_bounds__(128) kSdfBvh(const double* __restrict__ P, int64_t m, const BvhNode* __restrict__ N,
+// One query per thread, queries taken in the Morton order of their positions (order[i] is the
+// i-th query), so that a warp's traversals follow nearby paths through the tree.
+__global__ void __launch_bounds__(128) kSdfBvh(const double* __restrict__ P, int64_t m,
+                                               const uint32_t* __restrict__ order, const BvhNode* __restrict__ N,
                                                int64_t n, double* __restrict__ out, unsigned* __restrict__ overflow) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= m) return;
+  const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= m) return;
+  const int64_t i = order[s];
   const double q[3] = {P[3 * i], P[3 * i + 1], P[3 * i + 2]};
   const D3 qd{q[0], q[1], q[2]};
   auto nodeOf = [n](int32_t c) -> int64_t { return c < 0 ? (n - 1) + (-c - 1) : c; };
@@ -247,20 +254,25 @@ __global__ void __launch_bounds__(128) kSdfBvh(const double* __restrict__ P, int
     const double* v = N[node].tri;
     for (int c = 0; c < 3; ++c) t[c] = D3{v[3 * c], v[3 * c + 1], v[3 * c + 2]};
   };
-  // exact unsigned distance
+  // exact unsigned distance: nearest-first, each stacked node with its box distance (tested
+  // again against the best distance when popped)
   double best = 1.7976931348623157e308;
   int32_t stack[kBvhStack];
+  double sdist[kBvhStack];
   int sp = 0;
   if (n == 1) {
     D3 t[3];
     tri(0, t);
     best = pointTriSqDist(qd, t[0], t[1], t[2]);
   } else {
-    stack[sp++] = 0;
+    stack[0] = 0;
+    sdist[0] = boxDist2(N[0].lo, N[0].hi, q);
+    sp = 1;
     while (sp > 0) {
-      const int64_t node = stack[--sp];
-      if (boxDist2(N[node].lo, N[node].hi, q) > best * (1.0 + 1e-12)) continue;
-      const int32_t c[2] = {N[node].in.left, N[node].in.right};
+      --sp;
+      if (sdist[sp] > best * (1.0 + 1e-12)) continue;
+      const int64_t node = stack[sp];
+      const int32_t c[2] = {N[node].left, N[node].right};
       double dc[2];
       for (int k = 0; k < 2; ++k) {
         const int64_t cn = nodeOf(c[k]);
@@ -276,7 +288,9 @@ __global__ void __launch_bounds__(128) kSdfBvh(const double* __restrict__ P, int
           best = fmin(best, pointTriSqDist(qd, t[0], t[1], t[2]));
         } else {
           if (sp >= kBvhStack) { atomicOr(overflow, 1u); continue; }
-          stack[sp++] = c[k];
+          stack[sp] = c[k];
+          sdist[sp] = dc[k];
+          ++sp;
         }
       }
     }
@@ -295,28 +309,43 @@ __global__ void __launch_bounds__(128) kSdfBvh(const double* __restrict__ P, int
       continue;
     }
     const BvhNode& nd = N[node];
-    if (nd.in.area > 0.0) {
+    if (nd.area > 0.0) {
       const double d[3] = {nd.in.c[0] - q[0], nd.in.c[1] - q[1], nd.in.c[2] - q[2]};
       const double R2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
       if (R2 > kFwnBeta * kFwnBeta * nd.in.r2) {
         const double R = sqrt(R2);
         const double R3 = R2 * R, R5 = R3 * R2;
-        const double* m = nd.in.m;
-        const double tr = m[0] + m[4] + m[8];
-        const double dmd = d[0] * (m[0] * d[0] + m[1] * d[1] + m[2] * d[2]) +
-                           d[1] * (m[3] * d[0] + m[4] * d[1] + m[5] * d[2]) +
-                           d[2] * (m[6] * d[0] + m[7] * d[1] + m[8] * d[2]);
+        const double* mm = nd.in.m;
+        const double tr = mm[0] + mm[4] + mm[8];
+        const double dmd = d[0] * (mm[0] * d[0] + mm[1] * d[1] + mm[2] * d[2]) +
+                           d[1] * (mm[3] * d[0] + mm[4] * d[1] + mm[5] * d[2]) +
+                           d[2] * (mm[6] * d[0] + mm[7] * d[1] + mm[8] * d[2]);
         w += (nd.in.an[0] * d[0] + nd.in.an[1] * d[1] + nd.in.an[2] * d[2]) / R3 + (tr / R3 - 3.0 * dmd / R5);
         continue;
       }
     }
     if (sp + 2 > kBvhStack) { atomicOr(overflow, 1u); continue; }
-    stack[sp++] = nd.in.left;
-    stack[sp++] = nd.in.right;
+    stack[sp++] = nd.left;
+    stack[sp++] = nd.right;
   }
   const double wn = w / (4.0 * 3.14159265358979323846);
   const double dist = sqrt(best);
   out[i] = (wn > 0.5) ? -dist : dist;
+}
+
+// Morton code of a query position in the triangles' centroid box (clamped), for the traversal order.
+__global__ void kQueryCodes(const double* __restrict__ P, int64_t m, double3 lo, double3 inv,
+                            uint32_t* __restrict__ codes, uint32_t* __restrict__ idx) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const double L[3] = {lo.x, lo.y, lo.z}, I[3] = {inv.x, inv.y, inv.z};
+  uint32_t qc[3];
+  for (int a = 0; a < 3; ++a) {
+    const double u = (P[3 * i + a] - L[a]) * I[a];
+    qc[a] = (uint32_t)fmin(fmax(u * 1024.0, 0.0), 1023.0);
+  }
+  codes[i] = mortonEncode(qc[0], qc[1], qc[2]);
+  idx[i] = (uint32_t)i;
 }
 
 its_status sdfBvh(its_ctx* ctx, const double* dP, int64_t m, const double* dV, const int32_t* dF, int64_t nf, double* dOut) {
@@ -378,7 +407,16 @@ its_status sdfBvh(its_ctx* ctx, const double* dP, int64_t m, const double* dV, c
   if ((st = packed.alloc(ctx, nodes)) != ITS_OK) return st;
   kPackNodes<<<gridFor(nodes, 128), 128, 0, ctx->stream>>>(dV, dF, B, packed.p);
   ITS_LAUNCHED(ctx);
-  kSdfBvh<<<gridFor(m, 128), 128, 0, ctx->stream>>>(dP, m, packed.p, nf, dOut, overflow.p);
+  // the queries in Morton order (the tree's build buffers are reused for the sort)
+  DevBuf<uint32_t> qc, qi, qsc, qorder, qtk, qtv;
+  if ((st = qc.alloc(ctx, m)) != ITS_OK || (st = qi.alloc(ctx, m)) != ITS_OK || (st = qsc.alloc(ctx, m)) != ITS_OK ||
+      (st = qorder.alloc(ctx, m)) != ITS_OK || (st = qtk.alloc(ctx, m)) != ITS_OK || (st = qtv.alloc(ctx, m)) != ITS_OK)
+    return st;
+  kQueryCodes<<<gridFor(m, 256), 256, 0, ctx->stream>>>(dP, m, make_double3(bl[0], bl[1], bl[2]),
+                                                       make_double3(inv[0], inv[1], inv[2]), qc.p, qi.p);
+  ITS_LAUNCHED(ctx);
+  if ((st = radixSortPairs(ctx, qc.p, qi.p, qsc.p, qorder.p, qtk.p, qtv.p, m, 30)) != ITS_OK) return st;
+  kSdfBvh<<<gridFor(m, 128), 128, 0, ctx->stream>>>(dP, m, qorder.p, packed.p, nf, dOut, overflow.p);
   ITS_LAUNCHED(ctx);
   unsigned ov = 0;
   ITS_CU(ctx, cudaMemcpyAsync(&ov, overflow.p, 4, cudaMemcpyDeviceToHost, ctx->stream));

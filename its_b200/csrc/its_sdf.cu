@@ -20,6 +20,7 @@ its_status its_signed_distance(its_ctx* ctx, const double* points, int64_t npoin
   if (!points || !verts || !faces || !out || npoints < 0 || nverts <= 0 || nfaces <= 0)
     return setError(ctx, ITS_ERR_INVALID, "its_signed_distance: bad arguments");
   if (nfaces >= (1ll << 31)) return setError(ctx, ITS_ERR_INVALID, "its_signed_distance: too many faces");
+  if (npoints >= (1ll << 32)) return setError(ctx, ITS_ERR_INVALID, "its_signed_distance: too many points");
   if (npoints == 0) return ITS_OK;
   ITS_CU(ctx, cudaSetDevice(ctx->device));
   InArg<double> P, V;
