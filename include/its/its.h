@@ -362,6 +362,14 @@ its_status its_mlp_forward(its_mlp* mlp, const float* features, int64_t n, float
    without waiting (for callers that pipeline inference with their own work); a tensor-core
    wait that ran out sets a sticky flag that its_mlp_check reports. */
 its_status its_mlp_forward_async(its_mlp* mlp, const float* features, int64_t n, float* out);
+/* The same from features already in the kernel's input form, as the learned fit's features
+   kernel writes them: ceil(n / 128) tiles of 128 rows x 64 BF16 features (16 KB each, device
+   memory, 16-byte aligned), rows of 128 bytes, the 16-byte chunk c of row r stored at chunk
+   position c ^ (r % 8) of its row (128-byte swizzle, 8-row atoms of 1 KB). after_kernel != 0
+   declares that the previous operation on the context's stream is a kernel launch: the
+   network's blocks may then be scheduled while that kernel drains (programmatic dependent
+   launch; the network reads its input only after that kernel has completed). */
+its_status its_mlp_forward_tiles_async(its_mlp* mlp, const void* tiles, int64_t n, float* out, int after_kernel);
 /* Waits for the context's stream; ITS_ERR_TIMEOUT if a network kernel's bounded wait ran out. */
 its_status its_mlp_check(its_mlp* mlp);
 /* The same predictions layer by layer through the training kernels (bit-identical). */

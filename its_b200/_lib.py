@@ -78,6 +78,7 @@ SIGNATURES = {
     "its_mlp_get_params": (st, [vp, vp]),
     "its_mlp_forward": (st, [vp, vp, i64, vp]),
     "its_mlp_forward_async": (st, [vp, vp, i64, vp]),
+    "its_mlp_forward_tiles_async": (st, [vp, vp, i64, vp, C.c_int]),
     "its_mlp_check": (st, [vp]),
     "its_mlp_forward_layers": (st, [vp, vp, i64, vp]),
     "its_mlp_gradient": (st, [vp, vp, vp, i64, vp, vp]),

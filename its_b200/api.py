@@ -590,6 +590,24 @@ def _f32(a):
     return a
 
 
+def feature_tiles(X):
+    """FP32 features (n x 64) as the network kernel's input tiles (its_mlp_forward_tiles_async):
+    BF16 (round to nearest even), 128-row tiles of 128-byte rows, the 16-byte chunk c of row r
+    at chunk position c ^ (r % 8). Returns a uint8 array of ceil(n / 128) * 16384 bytes."""
+    X = np.ascontiguousarray(X, np.float32)
+    n = X.shape[0]
+    tiles = (n + 127) // 128
+    bits = np.zeros((tiles * 128, 64), np.uint32)
+    bits[:n] = X.view(np.uint32)
+    bf = ((bits + 0x7FFF + ((bits >> 16) & 1)) >> 16).astype(np.uint16)  # RN-even to BF16
+    rows = bf.reshape(tiles * 128, 8, 8)  # [row][chunk][8 values]
+    r = np.arange(tiles * 128)
+    out = np.empty_like(rows)
+    for c in range(8):
+        out[r, c ^ (r % 8)] = rows[:, c]
+    return out.reshape(-1).view(np.uint8)
+
+
 class ShareNet:
     """The share network (its_mlp): predicts minimum-norm shares from 64 vertex features."""
 
@@ -633,6 +651,13 @@ class ShareNet:
     def forward_async(self, X, out):
         """Predictions for device (torch CUDA) features into a device output, queued without waiting."""
         self.ctx.check(lib().its_mlp_forward_async(self.h, _ptr(X), _n(X), _ptr(out)), "its_mlp_forward_async")
+        return out
+
+    def forward_tiles_async(self, tiles, n, out, after_kernel=False):
+        """Predictions for n rows from device input tiles (feature_tiles' layout) into a device
+        output, queued without waiting (its_mlp_forward_tiles_async)."""
+        self.ctx.check(lib().its_mlp_forward_tiles_async(self.h, _ptr(tiles), int(n), _ptr(out), 1 if after_kernel else 0),
+                       "its_mlp_forward_tiles_async")
         return out
 
     def check(self):

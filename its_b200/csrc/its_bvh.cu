@@ -37,27 +37,31 @@ struct BvhDevice {
   unsigned* flag = nullptr;
 };
 
-// The traversal's view of the tree: one 192-byte record per node in three 64-byte lines. Line 0
-// holds what every visit reads -- the box, the children and the area; lines 1-2 hold what only
-// some visits read: for an internal node the fast winding number's expansion centre
-// (area-weighted centroid sum / area), squared radius, normal sum and second-order tensor, for
-// a leaf its triangle's corners. The values are those the traversal used to form per visit
-// from the build's arrays (same operations), so results are unchanged.
-struct __align__(64) BvhNode {
-  double lo[3], hi[3];
-  int32_t left, right;  // internal nodes: child index; >= 0 internal, < 0 leaf -(k+1)
-  double area;
-  union {
-    struct {
-      double c[3];
-      double r2;
-      double an[3];
-      double m[9];  // sum_t an_t (c_t - c)^T about the node's centre c
-    } in;
-    double tri[9];
-  };
+// The traversal's view of the tree, in three arrays:
+//   * TravNode, one 64-byte line per internal node: both children's boxes (FP32, rounded
+//     outward, so a box distance from them is a lower bound of the exact box's) and the
+//     children. A nearest-distance visit reads this one line; for 10^6 triangles the array
+//     (64 MB) stays in L2.
+//   * FwnNode, two lines per internal node: the fast winding number's expansion centre
+//     (area-weighted centroid sum / area), squared radius (+inf for a node without area, which
+//     the far-field test then never accepts), normal sum and second-order tensor.
+//   * the leaves' triangles (9 doubles each, in leaf order).
+// The FP64 values are those the traversal used to form per visit from the build's arrays
+// (same operations), and a pruned node is one whose exact box is also beyond the best
+// distance, so results are unchanged.
+struct __align__(64) TravNode {
+  float lo[2][3], hi[2][3];
+  int32_t child[2];  // >= 0 internal, < 0 leaf -(k+1)
+  int32_t pad[2];
 };
-static_assert(sizeof(BvhNode) == 192, "three 64-byte lines per node");
+static_assert(sizeof(TravNode) == 64, "one line per node");
+struct __align__(64) FwnNode {
+  double c[3];
+  double r2;
+  double an[3];
+  double m[9];  // sum_t an_t (c_t - c)^T about the node's centre c
+};
+static_assert(sizeof(FwnNode) == 128, "two lines per node");
 
 __global__ void kCentroidBounds(const double* __restrict__ V, const int32_t* __restrict__ F, int64_t nf,
                                 double* __restrict__ partial) {
@@ -191,43 +195,49 @@ __global__ void kBottomUp(const double* __restrict__ V, const int32_t* __restric
 }
 
 __global__ void kPackNodes(const double* __restrict__ V, const int32_t* __restrict__ F, BvhDevice B,
-                           BvhNode* __restrict__ out) {
+                           TravNode* __restrict__ trav, FwnNode* __restrict__ fwn, double* __restrict__ tris) {
   const int64_t n = B.nf;
   const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (k >= 2 * n - 1) return;
-  BvhNode r;
-  for (int a = 0; a < 3; ++a) {
-    r.lo[a] = B.lo[3 * k + a];
-    r.hi[a] = B.hi[3 * k + a];
-  }
   if (k >= n - 1) {  // leaf: its triangle's corners
     const uint32_t t = B.leafTri[k - (n - 1)];
+    double* dst = tris + 9 * (k - (n - 1));
     for (int c = 0; c < 3; ++c)
-      for (int a = 0; a < 3; ++a) r.tri[3 * c + a] = V[3 * (int64_t)F[3 * t + c] + a];
-    r.left = r.right = 0;
-    r.area = 0.0;
-  } else {
-    const double A = B.area[k];
-    r.area = A;
-    r.in.r2 = 0.0;
-    for (int a = 0; a < 3; ++a) {
-      r.in.an[a] = B.an[3 * k + a];
-      r.in.c[a] = A > 0.0 ? B.ac[3 * k + a] / A : 0.0;
-    }
-    if (A > 0.0) {
-      double r2 = 0.0;
-      for (int a = 0; a < 3; ++a) {
-        const double e = fmax(r.in.c[a] - r.lo[a], r.hi[a] - r.in.c[a]);
-        r2 += e * e;
-      }
-      r.in.r2 = r2;
-    }
-    for (int i = 0; i < 3; ++i)
-      for (int j = 0; j < 3; ++j) r.in.m[3 * i + j] = B.sm[9 * k + 3 * i + j] - r.in.an[i] * r.in.c[j];
-    r.left = B.left[k];
-    r.right = B.right[k];
+      for (int a = 0; a < 3; ++a) dst[3 * c + a] = V[3 * (int64_t)F[3 * t + c] + a];
+    return;
   }
-  out[k] = r;
+  TravNode r;
+  const int32_t ch[2] = {B.left[k], B.right[k]};
+  for (int j = 0; j < 2; ++j) {
+    const int64_t cn = ch[j] < 0 ? (n - 1) + (-ch[j] - 1) : ch[j];
+    for (int a = 0; a < 3; ++a) {
+      r.lo[j][a] = __double2float_rd(B.lo[3 * cn + a]);
+      r.hi[j][a] = __double2float_ru(B.hi[3 * cn + a]);
+    }
+    r.child[j] = ch[j];
+  }
+  r.pad[0] = r.pad[1] = 0;
+  trav[k] = r;
+  FwnNode f;
+  const double A = B.area[k];
+  const double lo[3] = {B.lo[3 * k], B.lo[3 * k + 1], B.lo[3 * k + 2]};
+  const double hi[3] = {B.hi[3 * k], B.hi[3 * k + 1], B.hi[3 * k + 2]};
+  for (int a = 0; a < 3; ++a) {
+    f.an[a] = B.an[3 * k + a];
+    f.c[a] = A > 0.0 ? B.ac[3 * k + a] / A : 0.0;
+  }
+  f.r2 = __longlong_as_double(0x7ff0000000000000ll);  // +inf: no far-field term without area
+  if (A > 0.0) {
+    double r2 = 0.0;
+    for (int a = 0; a < 3; ++a) {
+      const double e = fmax(f.c[a] - lo[a], hi[a] - f.c[a]);
+      r2 += e * e;
+    }
+    f.r2 = r2;
+  }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) f.m[3 * i + j] = B.sm[9 * k + 3 * i + j] - f.an[i] * f.c[j];
+  fwn[k] = f;
 }
 
 __device__ inline double boxDist2(const double* lo, const double* hi, const double* q) {
@@ -239,19 +249,30 @@ __device__ inline double boxDist2(const double* lo, const double* hi, const doub
   return s;
 }
 
+// Squared distance from q to a box given in FP32 (promoted exactly to FP64).
+__device__ inline double boxDist2f(const float* lo, const float* hi, const double* q) {
+  double s = 0.0;
+  for (int a = 0; a < 3; ++a) {
+    const double l = lo[a], h = hi[a];
+    const double d = q[a] < l ? l - q[a] : (q[a] > h ? q[a] - h : 0.0);
+    s = s + d * d;
+  }
+  return s;
+}
+
 // One query per thread, queries taken in the Morton order of their positions (order[i] is the
 // i-th query), so that a warp's traversals follow nearby paths through the tree.
 __global__ void __launch_bounds__(128) kSdfBvh(const double* __restrict__ P, int64_t m,
-                                               const uint32_t* __restrict__ order, const BvhNode* __restrict__ N,
+                                               const uint32_t* __restrict__ order, const TravNode* __restrict__ T,
+                                               const FwnNode* __restrict__ W, const double* __restrict__ tris,
                                                int64_t n, double* __restrict__ out, unsigned* __restrict__ overflow) {
   const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (s >= m) return;
   const int64_t i = order[s];
   const double q[3] = {P[3 * i], P[3 * i + 1], P[3 * i + 2]};
   const D3 qd{q[0], q[1], q[2]};
-  auto nodeOf = [n](int32_t c) -> int64_t { return c < 0 ? (n - 1) + (-c - 1) : c; };
-  auto tri = [&](int64_t node, D3* t) {
-    const double* v = N[node].tri;
+  auto tri = [&](int32_t leafCode, D3* t) {
+    const double* v = tris + 9 * (int64_t)(-leafCode - 1);
     for (int c = 0; c < 3; ++c) t[c] = D3{v[3 * c], v[3 * c + 1], v[3 * c + 2]};
   };
   // exact unsigned distance: nearest-first, each stacked node with its box distance (tested
@@ -262,29 +283,25 @@ __global__ void __launch_bounds__(128) kSdfBvh(const double* __restrict__ P, int
   int sp = 0;
   if (n == 1) {
     D3 t[3];
-    tri(0, t);
+    tri(-1, t);
     best = pointTriSqDist(qd, t[0], t[1], t[2]);
   } else {
     stack[0] = 0;
-    sdist[0] = boxDist2(N[0].lo, N[0].hi, q);
+    sdist[0] = 0.0;
     sp = 1;
     while (sp > 0) {
       --sp;
       if (sdist[sp] > best * (1.0 + 1e-12)) continue;
-      const int64_t node = stack[sp];
-      const int32_t c[2] = {N[node].left, N[node].right};
-      double dc[2];
-      for (int k = 0; k < 2; ++k) {
-        const int64_t cn = nodeOf(c[k]);
-        dc[k] = boxDist2(N[cn].lo, N[cn].hi, q);
-      }
+      const TravNode& nd = T[stack[sp]];
+      const double dc[2] = {boxDist2f(nd.lo[0], nd.hi[0], q), boxDist2f(nd.lo[1], nd.hi[1], q)};
+      const int32_t c[2] = {nd.child[0], nd.child[1]};
       const int first = dc[1] < dc[0] ? 1 : 0;
       for (int kk = 1; kk >= 0; --kk) {  // push the farther child first
         const int k = kk == 1 ? 1 - first : first;
         if (dc[k] > best * (1.0 + 1e-12)) continue;
         if (c[k] < 0) {
           D3 t[3];
-          tri(nodeOf(c[k]), t);
+          tri(c[k], t);
           best = fmin(best, pointTriSqDist(qd, t[0], t[1], t[2]));
         } else {
           if (sp >= kBvhStack) { atomicOr(overflow, 1u); continue; }
@@ -301,32 +318,29 @@ __global__ void __launch_bounds__(128) kSdfBvh(const double* __restrict__ P, int
   stack[sp++] = n == 1 ? -1 : 0;
   while (sp > 0) {
     const int32_t cur = stack[--sp];
-    const int64_t node = nodeOf(cur);
     if (cur < 0) {
       D3 t[3];
-      tri(node, t);
+      tri(cur, t);
       w += solidAngle(qd, t[0], t[1], t[2]);
       continue;
     }
-    const BvhNode& nd = N[node];
-    if (nd.area > 0.0) {
-      const double d[3] = {nd.in.c[0] - q[0], nd.in.c[1] - q[1], nd.in.c[2] - q[2]};
-      const double R2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
-      if (R2 > kFwnBeta * kFwnBeta * nd.in.r2) {
-        const double R = sqrt(R2);
-        const double R3 = R2 * R, R5 = R3 * R2;
-        const double* mm = nd.in.m;
-        const double tr = mm[0] + mm[4] + mm[8];
-        const double dmd = d[0] * (mm[0] * d[0] + mm[1] * d[1] + mm[2] * d[2]) +
-                           d[1] * (mm[3] * d[0] + mm[4] * d[1] + mm[5] * d[2]) +
-                           d[2] * (mm[6] * d[0] + mm[7] * d[1] + mm[8] * d[2]);
-        w += (nd.in.an[0] * d[0] + nd.in.an[1] * d[1] + nd.in.an[2] * d[2]) / R3 + (tr / R3 - 3.0 * dmd / R5);
-        continue;
-      }
+    const FwnNode& nd = W[cur];
+    const double d[3] = {nd.c[0] - q[0], nd.c[1] - q[1], nd.c[2] - q[2]};
+    const double R2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+    if (R2 > kFwnBeta * kFwnBeta * nd.r2) {
+      const double R = sqrt(R2);
+      const double R3 = R2 * R, R5 = R3 * R2;
+      const double* mm = nd.m;
+      const double tr = mm[0] + mm[4] + mm[8];
+      const double dmd = d[0] * (mm[0] * d[0] + mm[1] * d[1] + mm[2] * d[2]) +
+                         d[1] * (mm[3] * d[0] + mm[4] * d[1] + mm[5] * d[2]) +
+                         d[2] * (mm[6] * d[0] + mm[7] * d[1] + mm[8] * d[2]);
+      w += (nd.an[0] * d[0] + nd.an[1] * d[1] + nd.an[2] * d[2]) / R3 + (tr / R3 - 3.0 * dmd / R5);
+      continue;
     }
     if (sp + 2 > kBvhStack) { atomicOr(overflow, 1u); continue; }
-    stack[sp++] = nd.left;
-    stack[sp++] = nd.right;
+    stack[sp++] = T[cur].child[0];
+    stack[sp++] = T[cur].child[1];
   }
   const double wn = w / (4.0 * 3.14159265358979323846);
   const double dist = sqrt(best);
@@ -403,9 +417,13 @@ its_status sdfBvh(its_ctx* ctx, const double* dP, int64_t m, const double* dV, c
   }
   kBottomUp<<<gridFor(nf, 256), 256, 0, ctx->stream>>>(dV, dF, nf, leafTri.p, B);
   ITS_LAUNCHED(ctx);
-  DevBuf<BvhNode> packed;
-  if ((st = packed.alloc(ctx, nodes)) != ITS_OK) return st;
-  kPackNodes<<<gridFor(nodes, 128), 128, 0, ctx->stream>>>(dV, dF, B, packed.p);
+  DevBuf<TravNode> trav;
+  DevBuf<FwnNode> fwn;
+  DevBuf<double> tris;
+  if ((st = trav.alloc(ctx, nf > 1 ? nf - 1 : 1)) != ITS_OK || (st = fwn.alloc(ctx, nf > 1 ? nf - 1 : 1)) != ITS_OK ||
+      (st = tris.alloc(ctx, 9 * nf)) != ITS_OK)
+    return st;
+  kPackNodes<<<gridFor(nodes, 128), 128, 0, ctx->stream>>>(dV, dF, B, trav.p, fwn.p, tris.p);
   ITS_LAUNCHED(ctx);
   // the queries in Morton order (the tree's build buffers are reused for the sort)
   DevBuf<uint32_t> qc, qi, qsc, qorder, qtk, qtv;
@@ -416,7 +434,8 @@ its_status sdfBvh(its_ctx* ctx, const double* dP, int64_t m, const double* dV, c
                                                        make_double3(inv[0], inv[1], inv[2]), qc.p, qi.p);
   ITS_LAUNCHED(ctx);
   if ((st = radixSortPairs(ctx, qc.p, qi.p, qsc.p, qorder.p, qtk.p, qtv.p, m, 30)) != ITS_OK) return st;
-  kSdfBvh<<<gridFor(m, 128), 128, 0, ctx->stream>>>(dP, m, qorder.p, packed.p, nf, dOut, overflow.p);
+  kSdfBvh<<<gridFor(m, 128), 128, 0, ctx->stream>>>(dP, m, qorder.p, trav.p, fwn.p, tris.p, nf, dOut,
+                                                   overflow.p);
   ITS_LAUNCHED(ctx);
   unsigned ov = 0;
   ITS_CU(ctx, cudaMemcpyAsync(&ov, overflow.p, 4, cudaMemcpyDeviceToHost, ctx->stream));

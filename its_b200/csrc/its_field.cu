@@ -68,14 +68,20 @@ __device__ inline bool evalChain(const EvalParams& P, const double* __restrict__
   for (int d = 0; d < P.depth && t != kNone; ++d) {
     uint32_t X, Y, Z;
     mortonDecode(P.morton[t], X, Y, Z);
-    const double w = P.w0 * (double)(1u << d);
+    const double w = P.w0 * (double)(1u << d), wi = P.winv[d];
     const double bx = latticePos(P.g.x, w, X), by = latticePos(P.g.y, w, Y), bz = latticePos(P.g.z, w, Z);
     const LatticeIndex& L = P.lat[d];
+    // hat3's three factors for the cell's two corner positions per axis (the 8 corners share
+    // them); each term is hat3's value: 0 once a factor is not positive, else x * y * z
+    const double fx[2] = {hat1r(px, bx, w, wi), hat1r(px, bx + w, w, wi)};
+    const double fy[2] = {hat1r(py, by, w, wi), hat1r(py, by + w, w, wi)};
+    const double fz[2] = {hat1r(pz, bz, w, wi), hat1r(pz, bz + w, w, wi)};
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
       const uint32_t col = latticeRank(L, ((X + ox) * L.M + (Y + oy)) * L.M + (Z + oz));
-      sum += lambda[col] * hat3(ox ? bx + w : bx, oy ? by + w : by, oz ? bz + w : bz, w, px, py, pz);
+      const double h = (fx[ox] <= 0.0 || fy[oy] <= 0.0 || fz[oz] <= 0.0) ? 0.0 : fx[ox] * fy[oy] * fz[oz];
+      sum += lambda[col] * h;
     }
     t = P.parent[t];
   }
@@ -138,11 +144,11 @@ __device__ inline double fieldAt(const EvalParams& P, const double* __restrict__
                                  double pz) {
   double sum = 0.0;
   for (int d = 0; d < P.depth; ++d) {
-    const double w = P.w0 * (double)(1u << d);
+    const double w = P.w0 * (double)(1u << d), wi = P.winv[d];
     const LatticeIndex& L = P.lat[d];
     const int64_t lim = (int64_t)(P.res >> d);
-    const int64_t cx = (int64_t)floor((px - P.g.x) / w), cy = (int64_t)floor((py - P.g.y) / w),
-                  cz = (int64_t)floor((pz - P.g.z) / w);
+    const int64_t cx = (int64_t)floor(divRn(px - P.g.x, w, wi)), cy = (int64_t)floor(divRn(py - P.g.y, w, wi)),
+                  cz = (int64_t)floor(divRn(pz - P.g.z, w, wi));
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const int64_t Lx = cx + (k & 1), Ly = cy + ((k >> 1) & 1), Lz = cz + ((k >> 2) & 1);
@@ -150,7 +156,7 @@ __device__ inline double fieldAt(const EvalParams& P, const double* __restrict__
       const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
       if (!latticeHas(L, lin)) continue;
       const uint32_t v = latticeRank(L, lin);
-      sum += lambda[v] * hat3(P.vertPos[3 * v], P.vertPos[3 * v + 1], P.vertPos[3 * v + 2], w, px, py, pz);
+      sum += lambda[v] * hat3r(P.vertPos[3 * v], P.vertPos[3 * v + 1], P.vertPos[3 * v + 2], w, wi, px, py, pz);
     }
   }
   return sum;
@@ -342,56 +348,94 @@ template <typename T, int kSepZ>  // points per thread along z (the brick's dept
 __global__ void __launch_bounds__(kSepThreads) kEvalGridSep(const __grid_constant__ EvalParams P,
                                                             const double* __restrict__ lambda, double3 o, double3 vs,
                                                             int R, T* __restrict__ field) {
-  __shared__ T tLam[kSepTileCap];
-  __shared__ unsigned char tFlag[kSepTileCap];
-  __shared__ T hX[kSepX][4], hY[kSepY][4], hZ[kSepZ][4];  // [coordinate][corner side * 2 + corner bit]
-  __shared__ int cX[kSepX], cY[kSepY], cZ[kSepZ];
+  // hat tables and cells of the brick's coordinates for every depth ([corner side * 2 + corner
+  // bit]), and two corner tiles: depth d+1's is staged while depth d's is summed
+  __shared__ T hX[kMaxDepth][kSepX][4], hY[kMaxDepth][kSepY][4], hZ[kMaxDepth][kSepZ][4];
+  __shared__ int cX[kMaxDepth][kSepX], cY[kMaxDepth][kSepY], cZ[kMaxDepth][kSepZ];
+  __shared__ T tLam[2][kSepTileCap];
+  __shared__ unsigned char tFlag[2][kSepTileCap];
   const int64_t M = (int64_t)R + 1;
   const int tid = threadIdx.x, tx = tid % kSepX, ty = tid / kSepX;
   const int64_t x0 = (int64_t)blockIdx.x * kSepX, y0 = (int64_t)blockIdx.y * kSepY, z0 = (int64_t)blockIdx.z * kSepZ;
   const int64_t xi = x0 + tx, yj = y0 + ty;
   const bool inXY = xi < M && yj < M;
+  const int D = P.depth;
+  constexpr int kCoords = kSepX + kSepY + kSepZ;
+  for (int item = tid; item < kCoords * D; item += kSepThreads) {
+    const int d = item / kCoords, j = item % kCoords;
+    const double w = P.w0 * (double)(1u << d), wi = P.winv[d];
+    const int a = j < kSepX ? 0 : (j < kSepX + kSepY ? 1 : 2);
+    const int k = a == 0 ? j : (a == 1 ? j - kSepX : j - kSepX - kSepY);
+    int64_t idx = (a == 0 ? x0 : a == 1 ? y0 : z0) + k;
+    if (idx > M - 1) idx = M - 1;  // clamped to the grid
+    const double oa = a == 0 ? o.x : a == 1 ? o.y : o.z, va = a == 0 ? vs.x : a == 1 ? vs.y : vs.z;
+    const double ga = a == 0 ? P.g.x : a == 1 ? P.g.y : P.g.z;
+    const double pa = oa + (double)idx * va;
+    const int64_t c = (int64_t)floor(divRn(pa - ga, w, wi));
+    double h[4];
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      const int64_t X = c + side;
+      const double pA = latticePos(ga, w, (uint32_t)(X < 0 ? 0 : X));
+      const double pB = X >= 1 ? latticePos(ga, w, (uint32_t)(X - 1)) + w : pA;
+      h[2 * side] = hat1r(pa, pA, w, wi);
+      h[2 * side + 1] = hat1r(pa, pB, w, wi);
+    }
+    T* dst = a == 0 ? hX[d][k] : (a == 1 ? hY[d][k] : hZ[d][k]);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) dst[e] = (T)h[e];
+    (a == 0 ? cX[d] : a == 1 ? cY[d] : cZ[d])[k] = (int)c;
+  }
+  __syncthreads();
+  auto boxOf = [&](int d, int& nx, int& ny, int& nz) {
+    nx = cX[d][kSepX - 1] - cX[d][0] + 2;
+    ny = cY[d][kSepY - 1] - cY[d][0] + 2;
+    nz = cZ[d][kSepZ - 1] - cZ[d][0] + 2;
+    return nx * ny * nz <= kSepTileCap;  // block-uniform
+  };
+  // the corners of depth d's cell box: coefficient and flag byte (bit 0 present, bits 1-3 the
+  // owner corner bits); returns whether this thread found any
+  auto stage = [&](int d, int b) -> int {
+    int nx, ny, nz;
+    if (!boxOf(d, nx, ny, nz)) return 0;
+    const LatticeIndex& L = P.lat[d];
+    const int64_t lim = (int64_t)(P.res >> d);
+    const int64_t cx0 = cX[d][0], cy0 = cY[d][0], cz0 = cZ[d][0];
+    int mine = 0;
+    for (int t = tid; t < nx * ny * nz; t += kSepThreads) {
+      const int64_t Lx = cx0 + t / (ny * nz), Ly = cy0 + (t / nz) % ny, Lz = cz0 + t % nz;
+      unsigned char f = 0;
+      if (Lx >= 0 && Ly >= 0 && Lz >= 0 && Lx <= lim && Ly <= lim && Lz <= lim) {
+        const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
+        if (latticeHas(L, lin)) {
+          const uint32_t v = latticeRank(L, lin);
+          tLam[b][t] = (T)lambda[v];
+          f = (unsigned char)(1u | (((uint32_t)(P.vertKey[v] >> 37) & 7u) << 1));
+        }
+      }
+      tFlag[b][t] = f;
+      mine |= f;
+    }
+    return mine;
+  };
   T sum[kSepZ];
 #pragma unroll
   for (int q = 0; q < kSepZ; ++q) sum[q] = T(0);
-  for (int d = 0; d < P.depth; ++d) {
+  int anyCur = __syncthreads_or(stage(0, 0));
+  for (int d = 0; d < D; ++d) {
+    const int b = d & 1;
+    const int anyNext = d + 1 < D ? stage(d + 1, b ^ 1) : 0;
     const double w = P.w0 * (double)(1u << d), wi = P.winv[d];
-    const LatticeIndex& L = P.lat[d];
-    const int64_t lim = (int64_t)(P.res >> d);
-    // cells and hat tables of the brick's coordinates (clamped to the grid)
-    if (tid < kSepX + kSepY + kSepZ) {
-      const int a = tid < kSepX ? 0 : (tid < kSepX + kSepY ? 1 : 2);
-      const int k = a == 0 ? tid : (a == 1 ? tid - kSepX : tid - kSepX - kSepY);
-      int64_t idx = (a == 0 ? x0 : a == 1 ? y0 : z0) + k;
-      if (idx > M - 1) idx = M - 1;
-      const double oa = a == 0 ? o.x : a == 1 ? o.y : o.z, va = a == 0 ? vs.x : a == 1 ? vs.y : vs.z;
-      const double ga = a == 0 ? P.g.x : a == 1 ? P.g.y : P.g.z;
-      const double pa = oa + (double)idx * va;
-      const int64_t c = (int64_t)floor(divRn(pa - ga, w, wi));
-      double h[4];
-#pragma unroll
-      for (int side = 0; side < 2; ++side) {
-        const int64_t X = c + side;
-        const double pA = latticePos(ga, w, (uint32_t)(X < 0 ? 0 : X));
-        const double pB = X >= 1 ? latticePos(ga, w, (uint32_t)(X - 1)) + w : pA;
-        h[2 * side] = hat1r(pa, pA, w, wi);
-        h[2 * side + 1] = hat1r(pa, pB, w, wi);
-      }
-      T* dst = a == 0 ? hX[k] : (a == 1 ? hY[k] : hZ[k]);
-#pragma unroll
-      for (int e = 0; e < 4; ++e) dst[e] = (T)h[e];
-      (a == 0 ? cX : a == 1 ? cY : cZ)[k] = (int)c;
-    }
-    __syncthreads();
-    const int64_t cx0 = cX[0], cy0 = cY[0], cz0 = cZ[0];
-    const int nx = cX[kSepX - 1] - (int)cx0 + 2, ny = cY[kSepY - 1] - (int)cy0 + 2, nz = cZ[kSepZ - 1] - (int)cz0 + 2;
-    if (nx * ny * nz > kSepTileCap) {  // block-uniform: the box does not fit, per-point lookups
+    int nx, ny, nz;
+    if (!boxOf(d, nx, ny, nz)) {  // the box does not fit the tile: per-point lookups
       if (inXY) {
+        const LatticeIndex& L = P.lat[d];
+        const int64_t lim = (int64_t)(P.res >> d);
         const double px = o.x + (double)xi * vs.x, py = o.y + (double)yj * vs.y;
 #pragma unroll
         for (int q = 0; q < kSepZ; ++q) {
           const double pz = o.z + (double)(z0 + q) * vs.z;
-          const int64_t cx = cX[tx], cy = cY[ty], cz = cZ[q];
+          const int64_t cx = cX[d][tx], cy = cY[d][ty], cz = cZ[d][q];
           T s = sum[q];
           for (int k = 0; k < 8; ++k) {
             const int64_t Lx = cx + (k & 1), Ly = cy + ((k >> 1) & 1), Lz = cz + ((k >> 2) & 1);
@@ -410,28 +454,12 @@ __global__ void __launch_bounds__(kSepThreads) kEvalGridSep(const __grid_constan
           sum[q] = s;
         }
       }
-      __syncthreads();
-      continue;
-    }
-    int mine = 0;
-    for (int t = tid; t < nx * ny * nz; t += kSepThreads) {
-      const int64_t Lx = cx0 + t / (ny * nz), Ly = cy0 + (t / nz) % ny, Lz = cz0 + t % nz;
-      unsigned char f = 0;
-      if (Lx >= 0 && Ly >= 0 && Lz >= 0 && Lx <= lim && Ly <= lim && Lz <= lim) {
-        const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
-        if (latticeHas(L, lin)) {
-          const uint32_t v = latticeRank(L, lin);
-          tLam[t] = (T)lambda[v];
-          f = (unsigned char)(1u | (((uint32_t)(P.vertKey[v] >> 37) & 7u) << 1));
-        }
-      }
-      tFlag[t] = f;
-      mine |= f;
-    }
-    if (__syncthreads_or(mine) && inXY) {
-      const int rx = cX[tx] - (int)cx0, ry = cY[ty] - (int)cy0;
-      const T* hx = hX[tx];
-      const T* hy = hY[ty];
+    } else if (anyCur && inXY) {
+      const int rx = cX[d][tx] - cX[d][0], ry = cY[d][ty] - cY[d][0];
+      const T* hx = hX[d][tx];
+      const T* hy = hY[d][ty];
+      const T* lamT = tLam[b];
+      const unsigned char* flagT = tFlag[b];
       // A present corner adds lambda * ((hx * hy) * hz) even where a factor is 0: the term is
       // then +-0 (NaN for a non-finite coefficient), as fieldAt's sum over the corners adds it,
       // and a running sum that starts at +0 is never -0, so a +-0 term leaves it unchanged.
@@ -443,35 +471,36 @@ __global__ void __launch_bounds__(kSepThreads) kEvalGridSep(const __grid_constan
         for (int k = 0; k < 8; ++k) {
           const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
           const int t = ((rx + ox) * ny + (ry + oy)) * 2 + oz;
-          const unsigned f = tFlag[t];
+          const unsigned f = flagT[t];
           if (!(f & 1u)) continue;
-          const T lam = tLam[t];
+          const T lam = lamT[t];
           const T fxy = hx[2 * ox + ((f >> 1) & 1u)] * hy[2 * oy + ((f >> 2) & 1u)];
           const int e = 2 * oz + (int)((f >> 3) & 1u);
 #pragma unroll
-          for (int q = 0; q < kSepZ; ++q) sum[q] += lam * (fxy * hZ[q][e]);
+          for (int q = 0; q < kSepZ; ++q) sum[q] += lam * (fxy * hZ[d][q][e]);
         }
       } else {
 #pragma unroll
         for (int q = 0; q < kSepZ; ++q) {
-          const int rz = cZ[q] - (int)cz0;
+          const int rz = cZ[d][q] - cZ[d][0];
           T s = sum[q];
 #pragma unroll
           for (int k = 0; k < 8; ++k) {
             const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
             const int t = ((rx + ox) * ny + (ry + oy)) * nz + (rz + oz);
-            const unsigned f = tFlag[t];
+            const unsigned f = flagT[t];
             if (!(f & 1u)) continue;
             const T fx = hx[2 * ox + ((f >> 1) & 1u)];
             const T fy = hy[2 * oy + ((f >> 2) & 1u)];
-            const T fz = hZ[q][2 * oz + ((f >> 3) & 1u)];
-            s += tLam[t] * (fx * fy * fz);
+            const T fz = hZ[d][q][2 * oz + ((f >> 3) & 1u)];
+            s += lamT[t] * (fx * fy * fz);
           }
           sum[q] = s;
         }
       }
     }
-    __syncthreads();
+    // publishes depth d+1's tile and frees depth d's buffer for depth d+2
+    anyCur = __syncthreads_or(anyNext);
   }
   if (inXY) {
 #pragma unroll
@@ -616,7 +645,11 @@ template <typename T, int ITEMS>
 __global__ void __launch_bounds__(kScanThreads) kMcEmit(McCaseT<T> mc, double3 o, double3 vs,
                                                          const uint8_t* __restrict__ cube,
                                                          const unsigned long long* __restrict__ blockOffsets,
+                                                         const unsigned long long* __restrict__ grandTotal,
                                                          double* __restrict__ tri, unsigned long long capacity) {
+  // a block whose voxels emit nothing (most of them: the surface crosses few tiles) leaves at once
+  const unsigned long long next = blockIdx.x + 1 < gridDim.x ? blockOffsets[blockIdx.x + 1] : *grandTotal;
+  if (next == blockOffsets[blockIdx.x]) return;
   const int64_t nvox = (int64_t)mc.R * mc.R * mc.R;
   const int64_t base = (int64_t)blockIdx.x * (kScanThreads * ITEMS) + (int64_t)threadIdx.x * ITEMS;
   unsigned char ci[ITEMS];
@@ -1019,11 +1052,11 @@ its_status marchingCubesT(its_ctx* ctx, const FT* field, int res, const double o
     if (T.d) {
       const unsigned long long cap = (unsigned long long)capacity;
       if (items == 16)
-        kMcEmit<FT, 16><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(mc, o3, v3, cubeD, sums.p, T.d, cap);
+        kMcEmit<FT, 16><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(mc, o3, v3, cubeD, sums.p, tot.p, T.d, cap);
       else if (items == 4)
-        kMcEmit<FT, 4><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(mc, o3, v3, cubeD, sums.p, T.d, cap);
+        kMcEmit<FT, 4><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(mc, o3, v3, cubeD, sums.p, tot.p, T.d, cap);
       else
-        kMcEmit<FT, 8><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(mc, o3, v3, cubeD, sums.p, T.d, cap);
+        kMcEmit<FT, 8><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(mc, o3, v3, cubeD, sums.p, tot.p, T.d, cap);
       ITS_LAUNCHED(ctx);
     }
     return ITS_OK;

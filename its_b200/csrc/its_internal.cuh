@@ -73,6 +73,17 @@ __device__ __forceinline__ double hat1r(double x, double p, double w, double win
   if (x <= p) return 1 + divRn(x - p, w, winv);
   return 1 - divRn(x - p, w, winv);
 }
+// hat3 with the quotients formed by divRn (same result bit for bit).
+__device__ __forceinline__ double hat3r(double px, double py, double pz, double w, double winv, double qx, double qy,
+                                        double qz) {
+  const double x = hat1r(qx, px, w, winv);
+  if (x <= 0.0) return 0.0;
+  const double y = hat1r(qy, py, w, winv);
+  if (y <= 0.0) return 0.0;
+  const double z = hat1r(qz, pz, w, winv);
+  if (z <= 0.0) return 0.0;
+  return x * y * z;
+}
 __host__ __device__ inline double hat3(double px, double py, double pz, double w, double qx, double qy,
                                        double qz) {
   const double x = hat1(qx, px, w);

@@ -20,6 +20,7 @@
 
 #include "its_ctx.cuh"
 #include "its_umma.cuh"
+#include <cuda_fp16.h>
 
 namespace its {
 
@@ -34,7 +35,10 @@ using bf16 = __nv_bfloat16;
 // GELU in its tanh form (Hendrycks & Gimpel, "Gaussian Error Linear Units", 2016):
 //   gelu(z) = z/2 (1 + tanh(u)),  u = sqrt(2/pi) (z + 0.044715 z^3),
 // with the tanh from the hardware's approximate unit: a handful of instructions where the
-// erf form costs a few dozen, in the epilogues that bound the network's kernels.
+// erf form costs a few dozen. The epilogues that bound the network's kernels are bound by
+// that unit, so it evaluates two tanh per instruction in half precision (tanh.approx.f16x2:
+// u rounded to FP16, a result within about 2^-10 of tanh(u), the accuracy of tanh.approx.f32
+// itself); the rest of the GELU is FP32, two lanes per packed instruction.
 constexpr float kGeluK0 = 0.7978845608028654f;  // sqrt(2 / pi)
 constexpr float kGeluK1 = 0.044715f;
 __device__ __forceinline__ float tanhApprox(float x) {
@@ -42,20 +46,22 @@ __device__ __forceinline__ float tanhApprox(float x) {
   asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
-__device__ __forceinline__ float geluF(float z) {
-  const float u = z * fmaf(kGeluK0 * kGeluK1, z * z, kGeluK0);
-  const float h = 0.5f * z;
-  return fmaf(h, tanhApprox(u), h);
+__device__ __forceinline__ float2 tanhApprox2(float2 u) {
+  const __half2 hu = __float22half2_rn(u);
+  uint32_t t;
+  asm("tanh.approx.f16x2 %0, %1;" : "=r"(t) : "r"(*(const uint32_t*)&hu));
+  return __half22float2(*(const __half2*)&t);
 }
-// Two lanes of geluF with the packed FP32 instructions (each lane one IEEE FP32 operation of
-// geluF's, in geluF's order: the same bits at half the instructions).
 __device__ __forceinline__ float2 geluF2(float2 z) {
   const float2 p = __ffma2_rn(make_float2(kGeluK0 * kGeluK1, kGeluK0 * kGeluK1), __fmul2_rn(z, z),
                               make_float2(kGeluK0, kGeluK0));
   const float2 u = __fmul2_rn(z, p);
   const float2 h = __fmul2_rn(make_float2(0.5f, 0.5f), z);
-  return __ffma2_rn(h, make_float2(tanhApprox(u.x), tanhApprox(u.y)), h);
+  return __ffma2_rn(h, tanhApprox2(u), h);
 }
+// One lane of geluF2 (the same instructions, so the layer-by-layer training kernels and the
+// fused inference kernel compute the same bits).
+__device__ __forceinline__ float geluF(float z) { return geluF2(make_float2(z, z)).x; }
 // d gelu / dz = (1 + t)/2 + z/2 (1 - t^2) sqrt(2/pi) (1 + 3 * 0.044715 z^2), t = tanh(u)
 __device__ __forceinline__ float geluGrad(float z) {
   const float z2 = z * z;
@@ -326,6 +332,15 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   }
   gridDependencyWait();
   gridDependents();
+  const int64_t tiles = (n + 127) / 128;
+  if (tid == 0 && Xt)  // each slot's first input tile (the previous kernel's output), beside the weights
+    for (int s2 = 0; s2 < kFusedSlots; ++s2) {
+      const int64_t t0 = (int64_t)blockIdx.x * kFusedSlots + s2;
+      if (t0 >= tiles) break;
+      const uint32_t b2 = smemAddr(mbar + kFusedSlots + s2);
+      mbarArriveExpectTx(b2, 16384);
+      bulkLoad(smemAddr(sW3 + 32768 + s2 * (16384 + 32768)), (const uint8_t*)Xt + t0 * 16384, 16384, b2);
+    }
   fenceBefore();
   __syncthreads();
   fenceAfter();
@@ -339,12 +354,11 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   const float* b2 = sBias + 128;
   const float* b3 = sBias + 256;
   const float* w4 = sBias + 384;
-  const int64_t tiles = (n + 127) / 128;
   const bool xVec = ((uintptr_t)X & 15) == 0;  // rows are 256 B apart: 16-byte loads when the base allows
   for (int64_t t = (int64_t)blockIdx.x * kFusedSlots + s; t < tiles; t += (int64_t)gridDim.x * kFusedSlots) {
     const int64_t m = t * 128 + row;
     if (Xt) {  // the tile already in BF16 and swizzled: one bulk copy by the TMA engine
-      if (st == 0) {
+      if (st == 0 && t != (int64_t)blockIdx.x * kFusedSlots + s) {  // (the first was issued above)
         mbarArriveExpectTx(barX, 16384);
         bulkLoad(smemAddr(sX), (const uint8_t*)Xt + t * 16384, 16384, barX);
       }
@@ -827,6 +841,16 @@ its_status its_mlp_forward_async(its_mlp* h, const float* X, int64_t n, float* o
     return setError(ctx, ITS_ERR_INVALID, "its_mlp_forward_async: features and output must be device memory");
   ITS_CU(ctx, cudaSetDevice(ctx->device));
   return mlpInfer(h, X, n, out, false);
+}
+
+its_status its_mlp_forward_tiles_async(its_mlp* h, const void* tiles, int64_t n, float* out, int after_kernel) {
+  if (!h || (n > 0 && (!tiles || !out)) || n < 0) return ITS_ERR_INVALID;
+  its_ctx* ctx = h->ctx;
+  if (n > 0 && (!isDevicePtr(ctx, tiles) || !isDevicePtr(ctx, out) || ((uintptr_t)tiles & 15)))
+    return setError(ctx, ITS_ERR_INVALID,
+                    "its_mlp_forward_tiles_async: tiles (16-byte aligned) and output must be device memory");
+  ITS_CU(ctx, cudaSetDevice(ctx->device));
+  return mlpInferTiles(h, (const bf16*)tiles, n, out, nullptr, 0.0f, 0.0f, nullptr, after_kernel != 0);
 }
 
 // Waits for the context's stream and reports the network's error flag.

@@ -52,19 +52,24 @@ __global__ void kScanUpsweep(F f, int64_t n, T* blockSums) {
   if (threadIdx.x == 0) blockSums[blockIdx.x] = total;
 }
 
-// Single block: exclusive scan of the block sums in place; grand total to *total.
+// Single block: exclusive scan of the block sums in place; grand total to *total. Thread t
+// takes the t-th contiguous run of ceil(nb / threads) sums: it adds them, the block scans the
+// run totals once, and the thread writes its run's prefixes (integer sums: any grouping gives
+// the same values).
 template <typename T>
 __global__ void kScanSpine(T* blockSums, int64_t nb, T* total) {
-  T carry = 0;
-  for (int64_t c = 0; c < nb; c += kScanThreads) {
-    const int64_t i = c + threadIdx.x;
-    const T v = (i < nb) ? blockSums[i] : T(0);
-    T t;
-    const T e = blockExclusiveScan<T>(v, t);
-    if (i < nb) blockSums[i] = carry + e;
-    carry += t;
+  const int64_t per = (nb + kScanThreads - 1) / kScanThreads;
+  const int64_t b0 = (int64_t)threadIdx.x * per, b1 = b0 + per < nb ? b0 + per : nb;
+  T s = 0;
+  for (int64_t i = b0; i < b1; ++i) s += blockSums[i];
+  T tot;
+  T run = blockExclusiveScan<T>(s, tot);
+  for (int64_t i = b0; i < b1; ++i) {
+    const T v = blockSums[i];
+    blockSums[i] = run;
+    run += v;
   }
-  if (threadIdx.x == 0 && total) *total = carry;
+  if (threadIdx.x == 0 && total) *total = tot;
 }
 
 template <typename T, typename F, typename W>

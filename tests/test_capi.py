@@ -51,3 +51,22 @@ def test_ctypes_structs_match_the_header(tmp_path):
     want = [ctypes.sizeof(_lib.SvoInfo), _lib.SvoInfo.learned_tables_ms.offset, ctypes.sizeof(_lib.SolveOpts),
             ctypes.sizeof(_lib.SolveReport), ctypes.sizeof(_lib.BasisOpts), _lib.BasisOpts.num_samples.offset]
     assert got == want
+
+
+def test_feature_tiles_layout():
+    import numpy as np
+    # the network kernel's input tiles: BF16 (round to nearest even), row r at byte 128 r of
+    # its tile, 16-byte chunk c at chunk position c ^ (r % 8)
+    from its_b200.api import feature_tiles
+    rng = np.random.default_rng(5)
+    X = rng.standard_normal((300, 64)).astype(np.float32)
+    t = feature_tiles(X)
+    assert t.size == 3 * 16384
+    words = t.view(np.uint16)
+    bits = X.view(np.uint32).astype(np.uint64)
+    bf = ((bits + 0x7FFF + ((bits >> 16) & 1)) >> 16).astype(np.uint16)
+    for r in (0, 5, 127, 128, 201, 299):
+        for c in range(8):
+            base = (r // 128) * 8192 + (r % 128) * 64 + ((c ^ (r % 8)) & 7) * 8
+            assert np.array_equal(words[base:base + 8], bf[r, 8 * c:8 * c + 8])
+    assert not words[(300 % 128) * 64 + 2 * 8192:].any()  # rows past n are zero

@@ -34,6 +34,25 @@ def test_forward_matches_oracle(ctx, n):
 
 
 @pytest.mark.gpu
+def test_forward_from_tiles_matches_forward(ctx):
+    # the input in the kernel's own tile form (as the learned fit's features kernel writes it)
+    # gives the predictions of the FP32-feature path bit for bit, launched as a dependent
+    # launch or not
+    import torch
+    from its_b200.api import ShareNet, feature_tiles
+    net = ShareNet(ctx, batch=65536, params=ref.init_params(3))
+    X, _ = _data(33505, 4)
+    want = net.forward(X)
+    tiles = torch.from_numpy(feature_tiles(X)).cuda()
+    out = torch.zeros(len(X), dtype=torch.float32, device="cuda")
+    net.forward_tiles_async(tiles, len(X), out)
+    net.forward_tiles_async(tiles, len(X), out, after_kernel=True)
+    net.check()
+    assert np.array_equal(out.cpu().numpy(), want)
+    net.close()
+
+
+@pytest.mark.gpu
 def test_gradient_matches_oracle(ctx):
     from its_b200.api import ShareNet
     P = ref.init_params(4)
