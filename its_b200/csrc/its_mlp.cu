@@ -20,7 +20,6 @@
 
 #include "its_ctx.cuh"
 #include "its_umma.cuh"
-#include <cuda_fp16.h>
 
 namespace its {
 
@@ -35,10 +34,7 @@ using bf16 = __nv_bfloat16;
 // GELU in its tanh form (Hendrycks & Gimpel, "Gaussian Error Linear Units", 2016):
 //   gelu(z) = z/2 (1 + tanh(u)),  u = sqrt(2/pi) (z + 0.044715 z^3),
 // with the tanh from the hardware's approximate unit: a handful of instructions where the
-// erf form costs a few dozen. The epilogues that bound the network's kernels are bound by
-// that unit, so it evaluates two tanh per instruction in half precision (tanh.approx.f16x2:
-// u rounded to FP16, a result within about 2^-10 of tanh(u), the accuracy of tanh.approx.f32
-// itself); the rest of the GELU is FP32, two lanes per packed instruction.
+// erf form costs a few dozen, in the epilogues that bound the network's kernels.
 constexpr float kGeluK0 = 0.7978845608028654f;  // sqrt(2 / pi)
 constexpr float kGeluK1 = 0.044715f;
 __device__ __forceinline__ float tanhApprox(float x) {
@@ -46,22 +42,20 @@ __device__ __forceinline__ float tanhApprox(float x) {
   asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
-__device__ __forceinline__ float2 tanhApprox2(float2 u) {
-  const __half2 hu = __float22half2_rn(u);
-  uint32_t t;
-  asm("tanh.approx.f16x2 %0, %1;" : "=r"(t) : "r"(*(const uint32_t*)&hu));
-  return __half22float2(*(const __half2*)&t);
+__device__ __forceinline__ float geluF(float z) {
+  const float u = z * fmaf(kGeluK0 * kGeluK1, z * z, kGeluK0);
+  const float h = 0.5f * z;
+  return fmaf(h, tanhApprox(u), h);
 }
+// Two lanes of geluF with the packed FP32 instructions (each lane one IEEE FP32 operation of
+// geluF's, in geluF's order: the same bits at half the instructions).
 __device__ __forceinline__ float2 geluF2(float2 z) {
   const float2 p = __ffma2_rn(make_float2(kGeluK0 * kGeluK1, kGeluK0 * kGeluK1), __fmul2_rn(z, z),
                               make_float2(kGeluK0, kGeluK0));
   const float2 u = __fmul2_rn(z, p);
   const float2 h = __fmul2_rn(make_float2(0.5f, 0.5f), z);
-  return __ffma2_rn(h, tanhApprox2(u), h);
+  return __ffma2_rn(h, make_float2(tanhApprox(u.x), tanhApprox(u.y)), h);
 }
-// One lane of geluF2 (the same instructions, so the layer-by-layer training kernels and the
-// fused inference kernel compute the same bits).
-__device__ __forceinline__ float geluF(float z) { return geluF2(make_float2(z, z)).x; }
 // d gelu / dz = (1 + t)/2 + z/2 (1 - t^2) sqrt(2/pi) (1 + 3 * 0.044715 z^2), t = tanh(u)
 __device__ __forceinline__ float geluGrad(float z) {
   const float z2 = z * z;
@@ -148,6 +142,16 @@ __global__ void __launch_bounds__(128) kUmmaGemm(const bf16* __restrict__ A, int
 }
 
 // ---- epilogues ----------------------------------------------------------------------------
+// A thread owns one row (its TMEM lane), so its row-major stores go out in 16-byte pieces
+// (eight BF16 or four FP32 values per store); the transposed copies are coalesced as they are.
+__device__ __forceinline__ uint4 packBf16x8(const float* v) {
+  uint4 r;
+  __nv_bfloat162* q = (__nv_bfloat162*)&r;
+#pragma unroll
+  for (int e = 0; e < 4; ++e) q[e] = __floats2bfloat162_rn(v[2 * e], v[2 * e + 1]);
+  return r;
+}
+
 // Hidden layer: z = acc + b, h = gelu(z); Z (FP32, for the backward pass), H row-major and
 // its transpose (the operands of the next layer and of the weight gradient).
 struct EpiHidden {
@@ -158,12 +162,24 @@ struct EpiHidden {
   int64_t ldt;
   __device__ void operator()(int64_t m, float (&acc)[kHid]) const {
 #pragma unroll
-    for (int j = 0; j < kHid; ++j) {
-      const float z = acc[j] + bias[j];
-      const bf16 h = __float2bfloat16_rn(geluF(z));
-      if (Z) Z[m * kHid + j] = z;
-      H[m * kHid + j] = h;
-      if (Ht) Ht[(int64_t)j * ldt + m] = h;
+    for (int j0 = 0; j0 < kHid; j0 += 8) {
+      float z[8], h[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        z[e] = acc[j0 + e] + bias[j0 + e];
+        h[e] = geluF(z[e]);
+      }
+      if (Z) {
+        *(float4*)(Z + m * kHid + j0) = make_float4(z[0], z[1], z[2], z[3]);
+        *(float4*)(Z + m * kHid + j0 + 4) = make_float4(z[4], z[5], z[6], z[7]);
+      }
+      const uint4 hb = packBf16x8(h);
+      *(uint4*)(H + m * kHid + j0) = hb;
+      if (Ht) {
+        const bf16* hv = (const bf16*)&hb;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) Ht[(int64_t)(j0 + e) * ldt + m] = hv[e];
+      }
     }
   }
 };
@@ -195,12 +211,16 @@ struct EpiOutput {
     for (int g = 0; g < kOutParts; ++g) {
       float o = 0.0f;
 #pragma unroll
-      for (int jj = 0; jj < kHid / kOutParts; ++jj) {
-        const int j = g * (kHid / kOutParts) + jj;
-        acc[j] += bias[j];
-        const float h = __bfloat162float(__float2bfloat16_rn(geluF(acc[j])));
-        if (H3) H3[m * kHid + j] = __float2bfloat16_rn(h);
-        o += h * w4[j];
+      for (int j0 = g * (kHid / kOutParts); j0 < (g + 1) * (kHid / kOutParts); j0 += 8) {
+        float h[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          const int j = j0 + e;
+          acc[j] += bias[j];
+          h[e] = __bfloat162float(__float2bfloat16_rn(geluF(acc[j])));
+          o += h[e] * w4[j];
+        }
+        if (H3) *(uint4*)(H3 + m * kHid + j0) = packBf16x8(h);
       }
       part[g] = o;
     }
@@ -215,10 +235,15 @@ struct EpiOutput {
     dOut[m] = d;
     sqErr[m] = e * e;
 #pragma unroll
-    for (int j = 0; j < kHid; ++j) {
-      const bf16 g = __float2bfloat16_rn(d * w4[j] * geluGrad(acc[j]));
-      dZ[m * kHid + j] = g;
-      dZt[(int64_t)j * ldt + m] = g;
+    for (int j0 = 0; j0 < kHid; j0 += 8) {
+      float g[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) g[k] = d * w4[j0 + k] * geluGrad(acc[j0 + k]);
+      const uint4 gb = packBf16x8(g);
+      *(uint4*)(dZ + m * kHid + j0) = gb;
+      const bf16* gv = (const bf16*)&gb;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) dZt[(int64_t)(j0 + k) * ldt + m] = gv[k];
     }
   }
 };
@@ -231,10 +256,17 @@ struct EpiBack {
   int64_t ldt;
   __device__ void operator()(int64_t m, float (&acc)[kHid]) const {
 #pragma unroll
-    for (int j = 0; j < kHid; ++j) {
-      const bf16 g = __float2bfloat16_rn(acc[j] * geluGrad(Z[m * kHid + j]));
-      if (dZ) dZ[m * kHid + j] = g;
-      dZt[(int64_t)j * ldt + m] = g;
+    for (int j0 = 0; j0 < kHid; j0 += 8) {
+      const float4 z0 = *(const float4*)(Z + m * kHid + j0), z1 = *(const float4*)(Z + m * kHid + j0 + 4);
+      const float z[8] = {z0.x, z0.y, z0.z, z0.w, z1.x, z1.y, z1.z, z1.w};
+      float g[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) g[k] = acc[j0 + k] * geluGrad(z[k]);
+      const uint4 gb = packBf16x8(g);
+      if (dZ) *(uint4*)(dZ + m * kHid + j0) = gb;
+      const bf16* gv = (const bf16*)&gb;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) dZt[(int64_t)(j0 + k) * ldt + m] = gv[k];
     }
   }
 };
@@ -247,7 +279,7 @@ struct EpiPartial {
   __device__ void operator()(int64_t m, float (&acc)[N]) const {
     float* p = partial + ((int64_t)blockIdx.z * rows + m) * N;
 #pragma unroll
-    for (int j = 0; j < N; ++j) p[j] = acc[j];
+    for (int j = 0; j < N; j += 4) *(float4*)(p + j) = make_float4(acc[j], acc[j + 1], acc[j + 2], acc[j + 3]);
   }
 };
 
@@ -319,9 +351,11 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   float* sPart = sBias + 4 * 128 + s * kFusedGroups * 128;               // [group][row] partial sums
   uint64_t* mbar = (uint64_t*)(sBias + 4 * 128 + kFusedSlots * kFusedGroups * 128);  // MMA, input loads, weights
   uint32_t* tslot = (uint32_t*)(mbar + 2 * kFusedSlots + 1);
+  volatile uint32_t* slot0Started = tslot + 1;  // set once slot 0's first layer-1 product is done
   const uint32_t barW = smemAddr(mbar + 2 * kFusedSlots);
   if (warp == 0) tmemAlloc(smemAddr(tslot), 128 * kFusedSlots);
   if (tid == 0) {
+    *slot0Started = 0;
     for (int k = 0; k < 2 * kFusedSlots + 1; ++k) mbarInit(smemAddr(mbar + k), 1);
     // the weight image in five 16 KB bulk copies and the biases in one; the image was written
     // before the previous kernel started (only the features are its output)
@@ -387,6 +421,11 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
                                  __float2bfloat16_rn(f1.z), __float2bfloat16_rn(f1.w)};
       *(uint4*)(sX + swizzledChunk(pr, pc)) = *(const uint4*)v;
     }
+    // The two slots start half a layer apart: slot 1 begins once slot 0's first product is
+    // done, so that one slot's epilogue (bound by the tanh unit and the issue rate) runs while
+    // the other's MMA does. A bounded wait: past the bound slot 1 simply goes on.
+    if (s == 1 && t == (int64_t)blockIdx.x * kFusedSlots + s)
+      for (int spin = 0; spin < 20000 && *slot0Started == 0; ++spin) __nanosleep(32);
     float o = 0.0f;
     for (int layer = 0; layer < 3; ++layer) {
       fenceProxyAsync();
@@ -412,6 +451,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
       ok = mbarWait(bar, phase) && ok;
       phase ^= 1u;
       fenceAfter();
+      if (s == 0 && st == 0 && layer == 0) *slot0Started = 1;
       // epilogue of this group's 32 columns: one TMEM load, one wait
       const float* bias = layer == 0 ? b1 : (layer == 1 ? b2 : b3);
       const int n0 = kGroupCols * grp;
