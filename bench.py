@@ -72,6 +72,41 @@ def config_of(wl, n, nnz):
             "l2": "the operator (A and A^T, 12 B per entry each) exceeds the 126 MB L2 at this size"}
 
 
+def field_terms(pos, depth_counts, o, w, res, R):
+    """Terms of the bit-exact dense field on the (R+1)^3 MC lattice over the octree's own box
+    (R a multiple of res): every corner vertex at depth d adds one term to each lattice point of
+    the cells it is a corner of -- points i with floor(i / s) in {X - 1, X} per axis,
+    s = R / (res >> d)."""
+    terms = 0
+    w0 = float(w[0]) / res
+    start = 0
+    for d, cnt in enumerate(depth_counts):
+        P = pos[start:start + cnt]
+        start += cnt
+        if cnt == 0:
+            continue
+        s = R // (res >> d)
+        X = np.rint((P - np.asarray(o)[None, :]) / (w0 * (1 << d))).astype(np.int64)
+        lo = np.maximum(0, s * (X - 1))
+        hi = np.minimum(R, s * (X + 1) - 1)
+        c = np.clip(hi - lo + 1, 0, None)
+        terms += int(np.sum(c[:, 0] * c[:, 1] * c[:, 2]))
+    return terms
+
+
+def fp64_peak():
+    """Nominal FP64 vector rate of the device (64 operations per SM per clock at the maximum
+    SM clock; no measured FP64 figure is available): operations per second."""
+    import torch
+    props = torch.cuda.get_device_properties(0)
+    try:
+        mhz = float(subprocess.run(["nvidia-smi", "--query-gpu=clocks.max.sm", "--format=csv,noheader,nounits",
+                                    "-i", "0"], capture_output=True, text=True, timeout=20).stdout.split()[0])
+    except Exception:
+        mhz = 1965.0
+    return 64.0 * props.multi_processor_count * mhz * 1e6
+
+
 def load_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -520,6 +555,26 @@ def run_ours(args):
     mc_mvox = R ** 3 / ((field_ms + mc_ms) * 1e-3) / 1e6
     mc_verts = int(nv.value)
 
+    # the bit-exact field is bound by FP64 arithmetic (three operations per term, the terms in
+    # the reference's order), not by its writes: both rooflines are reported
+    f_terms = field_terms(pos, svo.depth_counts()[1], o, w, wl["res"], R) if R % wl["res"] == 0 else None
+    f_bytes = 8 * M ** 3
+    f_hbm = f_bytes / (field_ms * 1e-3) / 1e9
+    field_roof = {"bound": "fp64", "kernel": "the bit-exact FP64 field of the MC grid (its_eval_grid: kEvalGridSep, "
+                                             "lambda * ((hx * hy) * hz) summed in the reference's order)",
+                  "launch_ms": round(field_ms, 4), "terms_per_launch": f_terms,
+                  "traffic": profile_traffic("kEvalGridSep", wl["mesh"]),
+                  "hbm": {"achieved": round(f_hbm, 1), "peak": hbm_peak, "unit": "GB/s",
+                          "frac": round(f_hbm / hbm_peak, 4), "bytes_per_launch": f_bytes}}
+    if f_terms:
+        ops = 3.0 * f_terms
+        peak64 = fp64_peak()
+        field_roof.update({"achieved": round(ops / (field_ms * 1e-3) / 1e12, 3), "peak": round(peak64 / 1e12, 3),
+                           "unit": "T FP64 op/s", "frac": round(ops / (field_ms * 1e-3) / peak64, 4),
+                           "peak_kind": "nominal (64 FP64 operations per SM per clock at the maximum SM clock)",
+                           "note": "3 FP64 operations (two multiplies, one add) per term; every term a corner "
+                                   "vertex contributes to a lattice point of its cells"})
+
     # ---- FP32 field + marching cubes (the precision mode) ------------------------------------
     field32 = torch.empty(M ** 3, dtype=torch.float32, device="cuda")
 
@@ -647,12 +702,7 @@ def run_ours(args):
             "gpu_launches": launches,
             "mc": {"res": R, "mvox_s": round(mc_mvox, 1), "field_ms": round(field_ms, 3), "mc_ms": round(mc_ms, 3),
                    "iso": ol, "tri_vertices": mc_verts, "field": "FP64, bit-exact with the oracle"},
-            "roofline_field": {"bound": "hbm", "kernel": "the bit-exact FP64 field of the MC grid (its_eval_grid: "
-                                                       "kEvalGridSep, the FP64 terms in the reference's order)",
-                               "achieved": round(8 * M ** 3 / (field_ms * 1e-3) / 1e9, 1), "peak": hbm_peak,
-                               "unit": "GB/s", "frac": round(8 * M ** 3 / (field_ms * 1e-3) / 1e9 / hbm_peak, 4),
-                               "bytes_per_launch": 8 * M ** 3, "launch_ms": round(field_ms, 4),
-                               "traffic": profile_traffic("kEvalGridSep", wl["mesh"])},
+            "roofline_field": field_roof,
             "mc_f32": mc32,
             "mc_fast": mc_fast,
             "pipeline": pipeline,
