@@ -56,15 +56,34 @@ __global__ void kScanUpsweep(F f, int64_t n, T* blockSums) {
 // takes the t-th contiguous run of ceil(nb / threads) sums: it adds them, the block scans the
 // run totals once, and the thread writes its run's prefixes (integer sums: any grouping gives
 // the same values).
+// Both passes read eight sums per step, so that the loads of a run are in flight together.
 template <typename T>
 __global__ void kScanSpine(T* blockSums, int64_t nb, T* total) {
   const int64_t per = (nb + kScanThreads - 1) / kScanThreads;
   const int64_t b0 = (int64_t)threadIdx.x * per, b1 = b0 + per < nb ? b0 + per : nb;
   T s = 0;
-  for (int64_t i = b0; i < b1; ++i) s += blockSums[i];
+  int64_t i = b0;
+  for (; i + 8 <= b1; i += 8) {
+    T v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = blockSums[i + k];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += v[k];
+  }
+  for (; i < b1; ++i) s += blockSums[i];
   T tot;
   T run = blockExclusiveScan<T>(s, tot);
-  for (int64_t i = b0; i < b1; ++i) {
+  for (i = b0; i + 8 <= b1; i += 8) {
+    T v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = blockSums[i + k];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      blockSums[i + k] = run;
+      run += v[k];
+    }
+  }
+  for (; i < b1; ++i) {
     const T v = blockSums[i];
     blockSums[i] = run;
     run += v;
