@@ -340,7 +340,7 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
 // d = 0..D-1 and k = x|y<<1|z<<2, lambda * ((hx * hy) * hz) over its present corners with
 // positive factors -- fieldAt's additions in fieldAt's order, so the field is bit-identical,
 // at a few table reads and four FP64 operations per term.
-constexpr int kSepX = 32, kSepY = 8, kSepThreads = kSepX * kSepY, kSepTileCap = 1024;
+constexpr int kSepX = 32, kSepY = 8, kSepThreads = kSepX * kSepY, kSepTileCap = 1024, kSepStageCap = 2048;
 
 // T = float is the precision form's FP32 field: the same tables (formed in FP64, rounded once)
 // and the same terms, summed in FP32.
@@ -349,11 +349,14 @@ __global__ void __launch_bounds__(kSepThreads) kEvalGridSep(const __grid_constan
                                                             const double* __restrict__ lambda, double3 o, double3 vs,
                                                             int R, T* __restrict__ field) {
   // hat tables and cells of the brick's coordinates for every depth ([corner side * 2 + corner
-  // bit]), and two corner tiles: depth d+1's is staged while depth d's is summed
+  // bit]), and the corner boxes of every depth, staged together in one pass (their lattice
+  // lookups are dependent loads: in one pass their latencies overlap)
   __shared__ T hX[kMaxDepth][kSepX][4], hY[kMaxDepth][kSepY][4], hZ[kMaxDepth][kSepZ][4];
   __shared__ int cX[kMaxDepth][kSepX], cY[kMaxDepth][kSepY], cZ[kMaxDepth][kSepZ];
-  __shared__ T tLam[2][kSepTileCap];
-  __shared__ unsigned char tFlag[2][kSepTileCap];
+  __shared__ T tLam[kSepStageCap];
+  __shared__ unsigned char tFlag[kSepStageCap];
+  __shared__ int tOff[kMaxDepth], tEnd[kMaxDepth];  // depth d's tile: [tOff[d], tEnd[d]); tOff -1: per-point
+  __shared__ int tAny[kMaxDepth], tTotal;
   const int64_t M = (int64_t)R + 1;
   const int tid = threadIdx.x, tx = tid % kSepX, ty = tid / kSepX;
   const int64_t x0 = (int64_t)blockIdx.x * kSepX, y0 = (int64_t)blockIdx.y * kSepY, z0 = (int64_t)blockIdx.z * kSepZ;
@@ -391,43 +394,54 @@ __global__ void __launch_bounds__(kSepThreads) kEvalGridSep(const __grid_constan
     nx = cX[d][kSepX - 1] - cX[d][0] + 2;
     ny = cY[d][kSepY - 1] - cY[d][0] + 2;
     nz = cZ[d][kSepZ - 1] - cZ[d][0] + 2;
-    return nx * ny * nz <= kSepTileCap;  // block-uniform
+    return nx * ny * nz;
   };
-  // the corners of depth d's cell box: coefficient and flag byte (bit 0 present, bits 1-3 the
-  // owner corner bits); returns whether this thread found any
-  auto stage = [&](int d, int b) -> int {
+  if (tid == 0) {  // where each depth's box goes (a box over the capacity: per-point lookups)
+    int off = 0;
+    for (int d = 0; d < D; ++d) {
+      int nx, ny, nz;
+      const int n = boxOf(d, nx, ny, nz);
+      const bool fits = n <= kSepTileCap && off + n <= kSepStageCap;
+      tOff[d] = fits ? off : -1;
+      if (fits) off += n;
+      tEnd[d] = off;
+      tAny[d] = 0;
+    }
+    tTotal = off;
+  }
+  __syncthreads();
+  // the corners of every depth's cell box: coefficient and flag byte (bit 0 present, bits 1-3
+  // the owner corner bits); tAny[d]: whether depth d has any
+  for (int e = tid; e < tTotal; e += kSepThreads) {
+    int d = 0;
+    while (e >= tEnd[d]) ++d;  // the tiles lie in depth order (a depth without one: an empty range)
     int nx, ny, nz;
-    if (!boxOf(d, nx, ny, nz)) return 0;
+    boxOf(d, nx, ny, nz);
+    const int t = e - tOff[d];
     const LatticeIndex& L = P.lat[d];
     const int64_t lim = (int64_t)(P.res >> d);
-    const int64_t cx0 = cX[d][0], cy0 = cY[d][0], cz0 = cZ[d][0];
-    int mine = 0;
-    for (int t = tid; t < nx * ny * nz; t += kSepThreads) {
-      const int64_t Lx = cx0 + t / (ny * nz), Ly = cy0 + (t / nz) % ny, Lz = cz0 + t % nz;
-      unsigned char f = 0;
-      if (Lx >= 0 && Ly >= 0 && Lz >= 0 && Lx <= lim && Ly <= lim && Lz <= lim) {
-        const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
-        if (latticeHas(L, lin)) {
-          const uint32_t v = latticeRank(L, lin);
-          tLam[b][t] = (T)lambda[v];
-          f = (unsigned char)(1u | (((uint32_t)(P.vertKey[v] >> 37) & 7u) << 1));
-        }
+    const int64_t Lx = cX[d][0] + t / (ny * nz), Ly = cY[d][0] + (t / nz) % ny, Lz = cZ[d][0] + t % nz;
+    unsigned char f = 0;
+    if (Lx >= 0 && Ly >= 0 && Lz >= 0 && Lx <= lim && Ly <= lim && Lz <= lim) {
+      const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
+      if (latticeHas(L, lin)) {
+        const uint32_t v = latticeRank(L, lin);
+        tLam[e] = (T)lambda[v];
+        f = (unsigned char)(1u | (((uint32_t)(P.vertKey[v] >> 37) & 7u) << 1));
       }
-      tFlag[b][t] = f;
-      mine |= f;
     }
-    return mine;
-  };
+    tFlag[e] = f;
+    if (f) tAny[d] = 1;  // benign race: every writer stores 1
+  }
+  __syncthreads();
   T sum[kSepZ];
 #pragma unroll
   for (int q = 0; q < kSepZ; ++q) sum[q] = T(0);
-  int anyCur = __syncthreads_or(stage(0, 0));
   for (int d = 0; d < D; ++d) {
-    const int b = d & 1;
-    const int anyNext = d + 1 < D ? stage(d + 1, b ^ 1) : 0;
     const double w = P.w0 * (double)(1u << d), wi = P.winv[d];
     int nx, ny, nz;
-    if (!boxOf(d, nx, ny, nz)) {  // the box does not fit the tile: per-point lookups
+    boxOf(d, nx, ny, nz);
+    if (tOff[d] < 0) {  // the box does not fit the tile: per-point lookups
       if (inXY) {
         const LatticeIndex& L = P.lat[d];
         const int64_t lim = (int64_t)(P.res >> d);
@@ -454,12 +468,12 @@ __global__ void __launch_bounds__(kSepThreads) kEvalGridSep(const __grid_constan
           sum[q] = s;
         }
       }
-    } else if (anyCur && inXY) {
+    } else if (tAny[d] && inXY) {
       const int rx = cX[d][tx] - cX[d][0], ry = cY[d][ty] - cY[d][0];
       const T* hx = hX[d][tx];
       const T* hy = hY[d][ty];
-      const T* lamT = tLam[b];
-      const unsigned char* flagT = tFlag[b];
+      const T* lamT = tLam + tOff[d];
+      const unsigned char* flagT = tFlag + tOff[d];
       // A present corner adds lambda * ((hx * hy) * hz) even where a factor is 0: the term is
       // then +-0 (NaN for a non-finite coefficient), as fieldAt's sum over the corners adds it,
       // and a running sum that starts at +0 is never -0, so a +-0 term leaves it unchanged.
@@ -499,8 +513,6 @@ __global__ void __launch_bounds__(kSepThreads) kEvalGridSep(const __grid_constan
         }
       }
     }
-    // publishes depth d+1's tile and frees depth d's buffer for depth d+2
-    anyCur = __syncthreads_or(anyNext);
   }
   if (inXY) {
 #pragma unroll
