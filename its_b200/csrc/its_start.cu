@@ -40,6 +40,7 @@
 
 #include "its_op.cuh"
 #include "its_rows.cuh"
+#include "its_tune.cuh"
 
 namespace its {
 
@@ -359,16 +360,32 @@ its_status exactStart(its_ctx* ctx, its_svo* const* svos, int64_t count, const d
   DevBuf<uint8_t> keep;
   if ((st = makeSegArgs(ctx, segs, prefix, A, keep)) != ITS_OK) return st;
   A.stamp = stamp;
-  // dependent launches only straight after a kernel (no segment table copied in between)
+  // dependent launches only straight after a kernel (no segment table copied in between; not
+  // while the autotuner times candidates, which records events between them)
+  bool timing = true;
   const bool dep = afterKernel && !A.dsegs;
-  if (anyShares) {
-    if ((st = launchDependent(ctx, dep, kStartValues, gridFor(total, 256), 256, 0, ctx->stream, A, total)) != ITS_OK)
+  // a thread per row, no block-level sums: the block size is result-neutral and tuned
+  static const int kStartBlocks[3] = {256, 128, 64};
+  auto run = [&](int c) -> its_status {
+    const int bs = kStartBlocks[c];
+    if (anyShares &&
+        (st = launchDependent(ctx, dep && !timing, kStartValues, gridFor(total, bs), bs, 0, ctx->stream, A, total)) !=
+            ITS_OK)
       return st;
-  }
-  if ((st = launchDependent(ctx, anyShares || dep, kStartInterp, gridFor(total, 256), 256, 0, ctx->stream, A,
-                            total)) != ITS_OK)
-    return st;
-  return ITS_OK;  // a copied table came from pageable memory (staged at the call)
+    return launchDependent(ctx, anyShares || (dep && !timing), kStartInterp, gridFor(total, bs), bs, 0, ctx->stream, A,
+                           total);
+  };
+  const std::string key = std::string("exact_start/rows=") + std::to_string(total) + "/octrees=" +
+                          std::to_string(count) + (anyShares ? "/shares" : "/zero");
+  // the tuner measures on the first uncaptured call of a key when tuning is on; its last
+  // stream operation is then an event, so the launch that follows is not a dependent one
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(ctx->stream, &cs) != cudaSuccess) cudaGetLastError();
+  const bool measures = ctx->autotune && cs == cudaStreamCaptureStatusNone && ctx->tuned.find(key) == ctx->tuned.end();
+  int choice = 0;
+  if ((st = tuneChoice(ctx, key, 3, 0, run, &choice)) != ITS_OK) return st;
+  timing = measures;
+  return run(choice);  // a copied table came from pageable memory (staged at the call)
 }
 
 // ||b - A lambda|| / ||b|| of count octrees (device vectors), matrix-free, into relDev[count]

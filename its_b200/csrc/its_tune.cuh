@@ -29,6 +29,13 @@ its_status tuneChoice(its_ctx* ctx, const std::string& key, int n, int def, Run&
     *choice = def;
     return ITS_OK;
   }
+  // inside a stream capture nothing can be timed: the default, until an uncaptured call tunes
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(ctx->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+    cudaGetLastError();
+    *choice = def;
+    return ITS_OK;
+  }
   cudaEvent_t e0, e1;
   ITS_CU(ctx, cudaEventCreate(&e0));
   ITS_CU(ctx, cudaEventCreate(&e1));

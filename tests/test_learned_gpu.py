@@ -139,3 +139,37 @@ def test_learned_fit_graph_equals_start_and_check(ctx):
     lam3, _ = learned_fit(s, net2, b, norm, 1e-6)
     assert np.array_equal(lam3, learned_start_batch([s], net2, [b], norm)[0])
     net2.close()
+
+
+@pytest.mark.gpu
+def test_tuned_fit_launches_change_speed_not_bits():
+    # with tuning on, the exact start's block size is measured (before the learned fit's graph
+    # is captured) and kept; the start, the learned fit and the batched start are the untuned
+    # ones bit for bit
+    import torch
+    from its_b200 import Context, Svo
+    from its_b200.api import ShareNet, learned_fit, learned_start_batch
+    rng = np.random.default_rng(1)
+    norm = np.concatenate([rng.standard_normal(64) * 0.01, np.ones(64), [0.001, 0.01]]).astype(np.float32)
+    V, F, o, w = prepared_mesh("torus", R=0.7, r=0.25, rings=48, segs=24)
+    outs = []
+    for tuned in (False, True):
+        ctx = Context(0)
+        if tuned:
+            ctx.set_autotune(True)
+        net = ShareNet(ctx, batch=4096, params=omlp.init_params(7) * np.float32(0.1))
+        s = Svo(ctx, V, F, 32, o, w)
+        b = ctx.signed_distance(s.vertices()[0], V, F)
+        zero = s.exact_start(b)
+        start = learned_start_batch([s], net, [b], norm)[0]
+        b_dev = torch.from_numpy(b).cuda()
+        lam_dev = torch.zeros_like(b_dev)
+        learned_fit(s, net, b_dev, norm, 1e-6, out=lam_dev)
+        learned_fit(s, net, b_dev, norm, 1e-6, out=lam_dev)  # the replay
+        outs.append((zero, start, lam_dev.cpu().numpy(), ctx.autotune_choices()))
+        net.close()
+        s.close()
+        ctx.close()
+    for a, b_ in zip(outs[0][:3], outs[1][:3]):
+        assert np.array_equal(a, b_)
+    assert any(k.startswith("exact_start/") for k in outs[1][3])
