@@ -4,6 +4,7 @@ Arrays may be numpy arrays (host) or torch CUDA tensors (device); results come b
 numpy arrays unless a device output is passed. Every entry point goes through libits.so.
 """
 import ctypes as C
+import mmap
 import weakref
 
 import numpy as np
@@ -14,6 +15,24 @@ from ._lib import ItsError, SolveOpts, SolveReport, SvoInfo, lib
 STOP_NORMAL, STOP_RESIDUAL = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
 OP_FP64, OP_FP32_VALUES = 0, 1
+
+
+def _host_array(shape, dtype=np.float64):
+    """A zero-filled host array for a large result copied from the device. Large ones live in
+    anonymous memory advised for transparent huge pages, so that the copy that first writes
+    them takes one page fault per 2 MB instead of one per 4 KB; small ones are plain numpy."""
+    dtype = np.dtype(dtype)
+    count = int(np.prod(shape))
+    nbytes = count * dtype.itemsize
+    if nbytes < (8 << 20) or not hasattr(mmap, "MADV_HUGEPAGE"):
+        return np.zeros(shape, dtype)
+    huge = 2 << 20
+    mm = mmap.mmap(-1, (nbytes + huge - 1) // huge * huge, flags=mmap.MAP_PRIVATE | mmap.MAP_ANONYMOUS)
+    try:
+        mm.madvise(mmap.MADV_HUGEPAGE)
+    except OSError:
+        pass
+    return np.frombuffer(mm, dtype=dtype, count=count).reshape(shape)
 
 
 def _ptr(a):
@@ -132,7 +151,7 @@ class Context:
                                             C.byref(n)), "its_marching_cubes")
         tri = None
         if triangles:
-            tri = np.zeros((max(n.value, 1), 3))
+            tri = _host_array((max(n.value, 1), 3))
             self.check(lib().its_marching_cubes(self.h, _ptr(field), res, _ptr(o), _ptr(w), float(iso), None,
                                                 _ptr(tri), n.value, C.byref(n)), "its_marching_cubes")
             tri = tri[:n.value]
@@ -301,11 +320,11 @@ class Svo:
                 self.ctx.check(lib().its_shell_samples(self.h, _ptr(V), _n(V), _ptr(F), _n(F), _ptr(out), n.value,
                                                        C.byref(n), C.byref(ne)), "its_shell_samples")
             return out[:n.value], int(ne.value)
-        out = np.empty((cap, 3))
+        out = _host_array((cap, 3))
         self.ctx.check(lib().its_shell_samples(self.h, _ptr(V), _n(V), _ptr(F), _n(F), _ptr(out), cap, C.byref(n),
                                                C.byref(ne)), "its_shell_samples")
         if n.value > cap:
-            out = np.empty((n.value, 3))
+            out = _host_array((n.value, 3))
             self.ctx.check(lib().its_shell_samples(self.h, _ptr(V), _n(V), _ptr(F), _n(F), _ptr(out), n.value,
                                                    C.byref(n), C.byref(ne)), "its_shell_samples")
         return out[:n.value], int(ne.value)
@@ -340,7 +359,7 @@ class Svo:
         lam = _f64(lam)
         o, w = np.ascontiguousarray(origin, np.float64), np.ascontiguousarray(width, np.float64)
         if out is None:
-            out = np.zeros((res + 1) ** 3)
+            out = _host_array((res + 1) ** 3)
         self.ctx.check(lib().its_eval_grid(self.h, _ptr(lam), _ptr(o), _ptr(w), res, _ptr(out)), "its_eval_grid")
         return out
 
@@ -349,7 +368,7 @@ class Svo:
         lam = _f64(lam)
         o, w = np.ascontiguousarray(origin, np.float64), np.ascontiguousarray(width, np.float64)
         if out is None:
-            out = np.zeros((res + 1) ** 3, np.float32)
+            out = _host_array((res + 1) ** 3, np.float32)
         self.ctx.check(lib().its_eval_grid_f32(self.h, _ptr(lam), _ptr(o), _ptr(w), res, _ptr(out)),
                        "its_eval_grid_f32")
         return out
@@ -360,7 +379,7 @@ class Svo:
         lam = _f64(lam)
         o, w = np.ascontiguousarray(origin, np.float64), np.ascontiguousarray(width, np.float64)
         if out is None:
-            out = np.zeros((res + 1) ** 3, np.float32 if fp32 else np.float64)
+            out = _host_array((res + 1) ** 3, np.float32 if fp32 else np.float64)
         fn = lib().its_eval_grid_fast_f32 if fp32 else lib().its_eval_grid_fast
         self.ctx.check(fn(self.h, _ptr(lam), _ptr(o), _ptr(w), res, _ptr(out)), "its_eval_grid_fast")
         return out
@@ -379,7 +398,7 @@ class Svo:
         lam = _f64(lam)
         o, w = np.ascontiguousarray(origin, np.float64), np.ascontiguousarray(width, np.float64)
         if out is None:
-            out = np.zeros((res + 1) ** 3)
+            out = _host_array((res + 1) ** 3)
         self.ctx.check(lib().its_eval_grid_cubic(self.h, _ptr(lam), _ptr(o), _ptr(w), res, _ptr(out)),
                        "its_eval_grid_cubic")
         return out
@@ -401,12 +420,12 @@ class Svo:
         # one call into buffers sized for a surface crossing the grid (12 vertices per R^2 and
         # level, pages committed only where written), a second only for levels that exceed them
         cap = np.full(k, 12 * res * res + 1024, np.int64)
-        outs = [np.empty((int(c), 3)) for c in cap]
+        outs = [_host_array((int(c), 3)) for c in cap]
         P = (C.c_void_p * k)(*[o_.ctypes.data for o_ in outs])
         self.ctx.check(L.its_eval_grid_mc(self.h, _ptr(lam), _ptr(o), _ptr(w), res, 1 if fast else 0, _ptr(iso), k,
                                           P, _ptr(cap), _ptr(cnt)), "its_eval_grid_mc")
         if np.any(cnt > cap):
-            outs = [np.empty((max(int(c), 1), 3)) for c in cnt]
+            outs = [_host_array((max(int(c), 1), 3)) for c in cnt]
             P = (C.c_void_p * k)(*[o_.ctypes.data for o_ in outs])
             cap = cnt.copy()
             self.ctx.check(L.its_eval_grid_mc(self.h, _ptr(lam), _ptr(o), _ptr(w), res, 1 if fast else 0, _ptr(iso),

@@ -131,6 +131,7 @@ its_status its_destroy(its_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   its::hostIoRelease(c);
+  if (c->mapSlab) cudaFreeHost(c->mapSlab);
   if (c->ownStream) cudaStreamDestroy(c->ownStream);
   if (c->pool) cudaMemPoolDestroy(c->pool);  // released once nothing allocated from it is live
   if (c->pinned) cudaFreeHost(c->pinned);

@@ -30,6 +30,9 @@ struct its_ctx {
   uint8_t* arena = nullptr;
   size_t arenaCap = 0, arenaOff = 0;
   its::HostIo* hostio = nullptr;  // created on the first large copy into pageable memory
+  // mapped pinned words handed out in 64-byte slots (learned-fit plans: residual, flags, clocks)
+  double* mapSlab = nullptr;
+  uint64_t mapUsed = 0;  // one bit per slot
 };
 
 namespace its {

@@ -59,6 +59,7 @@ struct LearnedPlan {
   cudaEvent_t fork = nullptr, join = nullptr;
   double* bStage = nullptr;   // device copies of host vectors
   double* lamStage = nullptr;
+  int mapSlot = -1;            // relHost's slot in the context's mapped slab (-1: its own allocation)
 };
 
 static void dropGraph(LearnedPlan* p) {
@@ -74,10 +75,11 @@ void destroyPlan(LearnedPlan* p) {
   if (p->fork) cudaEventDestroy(p->fork);
   if (p->join) cudaEventDestroy(p->join);
   if (p->side) cudaStreamDestroy(p->side);
-  cudaFree(p->arena);
-  cudaFree(p->bStage);
-  cudaFree(p->lamStage);
-  cudaFreeHost(p->relHost);
+  devFree(p->ctx, p->arena);
+  devFree(p->ctx, p->bStage);
+  devFree(p->ctx, p->lamStage);
+  if (p->mapSlot >= 0) p->ctx->mapUsed &= ~(1ull << p->mapSlot);
+  else if (p->relHost) cudaFreeHost(p->relHost);
   delete p;
 }
 
@@ -90,8 +92,23 @@ static its_status planFor(its_svo* svo, LearnedPlan** out) {
     // the captured sequence's buffers: zero-share start, shares, G, H (8 B per vertex each),
     // features and predictions (260 B per coincident vertex), chunk sums, 256-byte alignment
     p->arenaCap = (size_t)(40 * n + 264 * c + 16 * (n / 256 + 64) + (1 << 16));
-    cudaError_t e = cudaMalloc(&p->arena, p->arenaCap);
-    if (e == cudaSuccess) e = cudaHostAlloc(&p->relHost, 64, cudaHostAllocMapped);
+    // from the context's stream-ordered pool (a plan per octree: cudaMalloc's device-wide
+    // synchronisation and its cost on a busy device stay out of the fit's first call)
+    its_status st = devAlloc(ctx, (void**)&p->arena, p->arenaCap);
+    if (st != ITS_OK) {
+      delete p;
+      return st;
+    }
+    cudaError_t e = cudaSuccess;
+    if (!ctx->mapSlab) e = cudaHostAlloc((void**)&ctx->mapSlab, 64 * 64, cudaHostAllocMapped);
+    if (e == cudaSuccess && ctx->mapUsed != ~0ull) {  // a free 64-byte slot of the mapped slab
+      const int slot = __builtin_ctzll(~ctx->mapUsed);
+      ctx->mapUsed |= 1ull << slot;
+      p->mapSlot = slot;
+      p->relHost = ctx->mapSlab + 8 * slot;
+    } else if (e == cudaSuccess) {
+      e = cudaHostAlloc(&p->relHost, 64, cudaHostAllocMapped);
+    }
     if (e == cudaSuccess) e = cudaHostGetDevicePointer(&p->relMapped, p->relHost, 0);
 
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming);
@@ -102,6 +119,7 @@ static its_status planFor(its_svo* svo, LearnedPlan** out) {
       destroyPlan(p);
       return setError(ctx, ITS_ERR_OOM, "learned fit: plan buffers");
     }
+    ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));  // the pool memory usable from any stream
     svo->plan = p;
   }
   *out = svo->plan;
@@ -204,11 +222,9 @@ its_status its_learned_fit(its_svo* svo, its_mlp* mlp, const double* b, const fl
   const PtrClass cb = ptrClass(b, ctx->device), cl = ptrClass(lambda, ctx->device);
   if (cb == PtrClass::OtherDevice || cl == PtrClass::OtherDevice) return otherDeviceError(ctx);
   const bool bHost = cb != PtrClass::Device, lamHost = cl != PtrClass::Device;
-  if ((bHost && !p->bStage && cudaMalloc(&p->bStage, std::max<int64_t>(n, 1) * 8) != cudaSuccess) ||
-      (lamHost && !p->lamStage && cudaMalloc(&p->lamStage, std::max<int64_t>(n, 1) * 8) != cudaSuccess)) {
-    cudaGetLastError();
-    return setError(ctx, ITS_ERR_OOM, "learned fit: staging buffers");
-  }
+  if ((bHost && !p->bStage && (st = devAlloc(ctx, (void**)&p->bStage, std::max<int64_t>(n, 1) * 8)) != ITS_OK) ||
+      (lamHost && !p->lamStage && (st = devAlloc(ctx, (void**)&p->lamStage, std::max<int64_t>(n, 1) * 8)) != ITS_OK))
+    return st;
   const double* bd = bHost ? p->bStage : b;
   double* ld = lamHost ? p->lamStage : lambda;
   // page-locked host vectors are copied by the graph itself (lambda beside the residual);
