@@ -35,6 +35,7 @@ struct BvhDevice {
   double* sm = nullptr;      // sum over the node's triangles of an_t c_t^T (9 per node, row-major)
   double* area = nullptr;
   unsigned* flag = nullptr;
+  int32_t* range = nullptr;  // internal node i covers sorted leaves range[2i] .. range[2i+1]
 };
 
 // The traversal's view of the tree, in three arrays:
@@ -49,10 +50,11 @@ struct BvhDevice {
 // The FP64 values are those the traversal used to form per visit from the build's arrays
 // (same operations), and a pruned node is one whose exact box is also beyond the best
 // distance, so results are unchanged.
+constexpr int kBucket = 4;  // a child whose subtree holds at most this many leaves is tested leaf by leaf
 struct __align__(64) TravNode {
   float lo[2][3], hi[2][3];
-  int32_t child[2];  // >= 0 internal, < 0 leaf -(k+1)
-  int32_t pad[2];
+  int32_t child[2];   // >= 0 internal, < 0 leaf -(k+1)
+  uint32_t bucket[2]; // an internal child of <= kBucket leaves: (count << 29) | first leaf; else 0
 };
 static_assert(sizeof(TravNode) == 64, "one line per node");
 struct __align__(64) FwnNode {
@@ -116,7 +118,7 @@ __device__ inline int delta(const uint32_t* codes, int64_t n, int64_t i, int64_t
 }
 
 __global__ void kBuildInternal(const uint32_t* __restrict__ codes, int64_t n, int32_t* __restrict__ left,
-                               int32_t* __restrict__ right, int32_t* __restrict__ parent) {
+                               int32_t* __restrict__ right, int32_t* __restrict__ parent, int32_t* __restrict__ range) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n - 1) return;
   const int d = delta(codes, n, i, i + 1) - delta(codes, n, i, i - 1) >= 0 ? 1 : -1;
@@ -139,6 +141,8 @@ __global__ void kBuildInternal(const uint32_t* __restrict__ codes, int64_t n, in
   const int32_t R = (hi == g + 1) ? -(int32_t)(g + 2) : (int32_t)(g + 1);
   left[i] = L;
   right[i] = R;
+  range[2 * i] = (int32_t)lo;
+  range[2 * i + 1] = (int32_t)hi;
   parent[L < 0 ? (n - 1) + (-L - 1) : L] = (int32_t)i;
   parent[R < 0 ? (n - 1) + (-R - 1) : R] = (int32_t)i;
 }
@@ -215,8 +219,12 @@ __global__ void kPackNodes(const double* __restrict__ V, const int32_t* __restri
       r.hi[j][a] = __double2float_ru(B.hi[3 * cn + a]);
     }
     r.child[j] = ch[j];
+    r.bucket[j] = 0;
+    if (ch[j] >= 0) {
+      const int32_t first = B.range[2 * ch[j]], count = B.range[2 * ch[j] + 1] - first + 1;
+      if (count <= kBucket && first < (1 << 29)) r.bucket[j] = ((uint32_t)count << 29) | (uint32_t)first;
+    }
   }
-  r.pad[0] = r.pad[1] = 0;
   trav[k] = r;
   FwnNode f;
   const double A = B.area[k];
@@ -295,6 +303,7 @@ __global__ void __launch_bounds__(128) kSdfBvh(const double* __restrict__ P, int
       const TravNode& nd = T[stack[sp]];
       const double dc[2] = {boxDist2f(nd.lo[0], nd.hi[0], q), boxDist2f(nd.lo[1], nd.hi[1], q)};
       const int32_t c[2] = {nd.child[0], nd.child[1]};
+      const uint32_t bk[2] = {nd.bucket[0], nd.bucket[1]};
       const int first = dc[1] < dc[0] ? 1 : 0;
       for (int kk = 1; kk >= 0; --kk) {  // push the farther child first
         const int k = kk == 1 ? 1 - first : first;
@@ -303,6 +312,13 @@ __global__ void __launch_bounds__(128) kSdfBvh(const double* __restrict__ P, int
           D3 t[3];
           tri(c[k], t);
           best = fmin(best, pointTriSqDist(qd, t[0], t[1], t[2]));
+        } else if (bk[k]) {  // a small subtree: its leaves' triangles directly
+          const int32_t f0 = (int32_t)(bk[k] & ((1u << 29) - 1u)), cnt = (int32_t)(bk[k] >> 29);
+          for (int32_t l = 0; l < cnt; ++l) {
+            D3 t[3];
+            tri(-(f0 + l) - 1, t);
+            best = fmin(best, pointTriSqDist(qd, t[0], t[1], t[2]));
+          }
         } else {
           if (sp >= kBvhStack) { atomicOr(overflow, 1u); continue; }
           stack[sp] = c[k];
@@ -371,6 +387,7 @@ its_status sdfBvh(its_ctx* ctx, const double* dP, int64_t m, const double* dV, c
   DevBuf<uint32_t> codes, idx, sc, leafTri, tk, tv;
   DevBuf<double> lo, hi, an, ac, area, smom;
   DevBuf<unsigned> flag, overflow;
+  DevBuf<int32_t> range;
   if ((st = left.alloc(ctx, nf)) != ITS_OK || (st = right.alloc(ctx, nf)) != ITS_OK ||
       (st = parent.alloc(ctx, nodes)) != ITS_OK || (st = codes.alloc(ctx, nf)) != ITS_OK ||
       (st = idx.alloc(ctx, nf)) != ITS_OK || (st = sc.alloc(ctx, nf)) != ITS_OK ||
@@ -379,7 +396,8 @@ its_status sdfBvh(its_ctx* ctx, const double* dP, int64_t m, const double* dV, c
       (st = hi.alloc(ctx, 3 * nodes)) != ITS_OK || (st = an.alloc(ctx, 3 * nodes)) != ITS_OK ||
       (st = ac.alloc(ctx, 3 * nodes)) != ITS_OK || (st = area.alloc(ctx, nodes)) != ITS_OK ||
       (st = smom.alloc(ctx, 9 * nodes)) != ITS_OK ||
-      (st = flag.zeros(ctx, nf)) != ITS_OK || (st = overflow.zeros(ctx, 1)) != ITS_OK)
+      (st = flag.zeros(ctx, nf)) != ITS_OK || (st = overflow.zeros(ctx, 1)) != ITS_OK ||
+      (st = range.alloc(ctx, 2 * nf)) != ITS_OK)
     return st;
   // centroid bounds for the Morton quantisation
   const unsigned pb = 256;
@@ -410,9 +428,10 @@ its_status sdfBvh(its_ctx* ctx, const double* dP, int64_t m, const double* dV, c
   B.area = area.p;
   B.sm = smom.p;
   B.flag = flag.p;
+  B.range = range.p;
   ITS_CU(ctx, cudaMemsetAsync(parent.p, 0xFF, nodes * 4, ctx->stream));
   if (nf > 1) {
-    kBuildInternal<<<gridFor(nf - 1, 256), 256, 0, ctx->stream>>>(sc.p, nf, left.p, right.p, parent.p);
+    kBuildInternal<<<gridFor(nf - 1, 256), 256, 0, ctx->stream>>>(sc.p, nf, left.p, right.p, parent.p, range.p);
     ITS_LAUNCHED(ctx);
   }
   kBottomUp<<<gridFor(nf, 256), 256, 0, ctx->stream>>>(dV, dF, nf, leafTri.p, B);
