@@ -343,15 +343,15 @@ __global__ void __launch_bounds__(128) kSdfBvh(const double* __restrict__ P, int
     const FwnNode& nd = W[cur];
     const double d[3] = {nd.c[0] - q[0], nd.c[1] - q[1], nd.c[2] - q[2]};
     const double R2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
-    if (R2 > kFwnBeta * kFwnBeta * nd.r2) {
-      const double R = sqrt(R2);
-      const double R3 = R2 * R, R5 = R3 * R2;
+    if (R2 > kFwnBeta * kFwnBeta * nd.r2) {  // the powers of 1/R from one reciprocal
+      const double iR = 1.0 / sqrt(R2);
+      const double iR2 = iR * iR, iR3 = iR2 * iR, iR5 = iR3 * iR2;
       const double* mm = nd.m;
       const double tr = mm[0] + mm[4] + mm[8];
       const double dmd = d[0] * (mm[0] * d[0] + mm[1] * d[1] + mm[2] * d[2]) +
                          d[1] * (mm[3] * d[0] + mm[4] * d[1] + mm[5] * d[2]) +
                          d[2] * (mm[6] * d[0] + mm[7] * d[1] + mm[8] * d[2]);
-      w += (nd.an[0] * d[0] + nd.an[1] * d[1] + nd.an[2] * d[2]) / R3 + (tr / R3 - 3.0 * dmd / R5);
+      w += (nd.an[0] * d[0] + nd.an[1] * d[1] + nd.an[2] * d[2]) * iR3 + (tr * iR3 - 3.0 * dmd * iR5);
       continue;
     }
     if (sp + 2 > kBvhStack) { atomicOr(overflow, 1u); continue; }

@@ -11,7 +11,8 @@
 //   * sign: the fast winding number (Barill et al. 2018): a node whose area centroid c is
 //     farther than beta = 2 times its box radius contributes the second-order expansion of its
 //     triangles' solid angles about c -- the normal sum as a dipole plus the tensor
-//     M = sum_t an_t (c_t - c)^T (formed as sum_t an_t c_t^T - AN c^T) -- nearer nodes recurse
+//     M = sum_t an_t (c_t - c)^T (formed as sum_t an_t c_t^T - AN c^T), the powers of 1/R from
+//     one reciprocal of sqrt(R^2) -- nearer nodes recurse
 //     (right child first), leaves add the exact solid angle; inside if w > 1/2.
 // The same tree, the same traversal order and the same IEEE operations as libits' kSdfBvh, so
 // distances are bit-identical and the winding numbers agree to the last bits of atan2.
@@ -234,8 +235,8 @@ double queryOne(const Bvh& B, const double* V, const int32_t* F, const double* q
       const double d[3] = {c[0] - q[0], c[1] - q[1], c[2] - q[2]};
       const double R2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
       if (R2 > kBeta * kBeta * r2) {
-        const double R = std::sqrt(R2);
-        const double R3 = R2 * R, R5 = R3 * R2;
+        const double iR = 1.0 / std::sqrt(R2);
+        const double iR2 = iR * iR, iR3 = iR2 * iR, iR5 = iR3 * iR2;
         double m[9];
         for (int i = 0; i < 3; ++i)
           for (int j = 0; j < 3; ++j) m[3 * i + j] = B.sm[9 * node + 3 * i + j] - B.an[3 * node + i] * c[j];
@@ -243,8 +244,8 @@ double queryOne(const Bvh& B, const double* V, const int32_t* F, const double* q
         const double dmd = d[0] * (m[0] * d[0] + m[1] * d[1] + m[2] * d[2]) +
                            d[1] * (m[3] * d[0] + m[4] * d[1] + m[5] * d[2]) +
                            d[2] * (m[6] * d[0] + m[7] * d[1] + m[8] * d[2]);
-        w += (B.an[3 * node] * d[0] + B.an[3 * node + 1] * d[1] + B.an[3 * node + 2] * d[2]) / R3 +
-             (tr / R3 - 3.0 * dmd / R5);
+        w += (B.an[3 * node] * d[0] + B.an[3 * node + 1] * d[1] + B.an[3 * node + 2] * d[2]) * iR3 +
+             (tr * iR3 - 3.0 * dmd * iR5);
         continue;
       }
     }
