@@ -767,7 +767,7 @@ def run_pipeline(ctx, net, norm, V, F, o, w, wl, timed, reps=3):
     R = wl["mc_res"]
     stages = {k: [] for k in ("upload", "octree", "samples", "signed_distance", "fit", "iso", "field_mc")}
     walls, tris = [], None
-    Vh, Fh = torch.from_numpy(np.ascontiguousarray(V)), torch.from_numpy(np.ascontiguousarray(F, np.int32))
+    Vh, Fh = np.ascontiguousarray(V), np.ascontiguousarray(F, np.int32)
     for _ in range(reps + 1):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -780,7 +780,7 @@ def run_pipeline(ctx, net, norm, V, F, o, w, wl, timed, reps=3):
             stages[name].append((now - t) * 1e3)
             t = now
 
-        Vd, Fd = Vh.cuda(), Fh.cuda()
+        Vd, Fd = ctx.to_device(Vh), ctx.to_device(Fh)  # its_copy_to_device
         lap("upload")
         svo = Svo(ctx, Vd, Fd, wl["res"], o, w)
         lap("octree")

@@ -56,9 +56,15 @@ its_status its_synchronize(its_ctx* ctx);
 const char* its_version(void);
 /* Number of kernels this context has launched so far (a diagnostic counter). */
 int64_t its_kernel_launches(const its_ctx* ctx);
+/* Copies bytes of host memory (pageable or page-locked) to device memory of the context's GPU
+   and waits for the copy. A pageable source of 32 MB or more goes through two page-locked
+   chunks that several host threads fill while the previous chunk is in flight (the same path
+   every entry point takes for large pageable inputs). No counterpart in the reference, which
+   copies its arrays with cudaMemcpy. */
+its_status its_copy_to_device(its_ctx* ctx, void* dst, const void* src, int64_t bytes);
 /* The autotuner. With enable = 1 the first call of a tunable launch (the dense field's brick
-   shape, the marching-cubes tile) for a given shape key times every candidate on the context's
-   stream and keeps the fastest; later calls reuse the choice. Every candidate computes the
+   shape, the marching-cubes tile, the exact start's block size) for a given shape key times
+   every candidate on the context's stream and keeps the fastest; later calls reuse the choice. Every candidate computes the
    same bits, so tuning changes speed only. cache_path (NULL: none) persists the choices as
    "key value" lines and is read here. No counterpart in the reference. */
 its_status its_set_autotune(its_ctx* ctx, int enable, const char* cache_path);

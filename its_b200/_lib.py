@@ -48,6 +48,7 @@ SIGNATURES = {
     "its_kernel_launches": (i64, [vp]),
     "its_check_division": (st, [vp, vp, vp, i64, C.POINTER(i64)]),
     "its_set_autotune": (st, [vp, i32, C.c_char_p]),
+    "its_copy_to_device": (st, [vp, vp, vp, i64]),
     "its_autotune_choices": (st, [vp, C.c_char_p, i64, C.POINTER(i64)]),
     "its_model_to_unit_cube": (st, [vp, i64, dbl]),
     "its_uniform_bbox": (st, [vp, i64, vp, vp, vp]),

@@ -104,6 +104,16 @@ class Context:
         self.check(lib().its_set_autotune(self.h, 1 if enable else 0,
                                           None if cache_path is None else cache_path.encode()), "its_set_autotune")
 
+    def to_device(self, a):
+        """A torch CUDA tensor holding a copy of host array a (its_copy_to_device: large
+        pageable arrays go through page-locked chunks filled by host threads)."""
+        import torch
+        a = np.ascontiguousarray(a)
+        out = torch.empty(a.shape, dtype=getattr(torch, a.dtype.name), device="cuda")
+        self.check(lib().its_copy_to_device(self.h, C.c_void_p(out.data_ptr()), a.ctypes.data_as(C.c_void_p),
+                                            a.nbytes), "its_copy_to_device")
+        return out
+
     def autotune_choices(self):
         n = C.c_int64(0)
         self.check(lib().its_autotune_choices(self.h, None, 0, C.byref(n)), "its_autotune_choices")

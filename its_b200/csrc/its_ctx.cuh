@@ -154,6 +154,16 @@ inline bool isPinnedHostPtr(const void* p) {
 
 // A read-only argument on the device: the caller's pointer if it already is device
 // memory, else a staged copy.
+// Large copies between pageable host memory and the device through two pinned chunks, the
+// host side of each chunk copied by several host threads (its_hostio.cu). To the host: returns
+// with the data in dst. To the device: returns once the last chunk is queued on the context's
+// stream (later work on the stream sees the data).
+constexpr size_t kStagedCopyMin = 8u << 20;     // to the host: parallel first touch of the pages
+constexpr size_t kStagedUploadMin = 32u << 20;  // to the device: below this the driver's path is as fast
+its_status copyToHostStaged(its_ctx* ctx, void* dst, const void* src, size_t bytes);
+its_status copyToDeviceStaged(its_ctx* ctx, void* dst, const void* src, size_t bytes);
+void hostIoRelease(its_ctx* ctx);
+
 template <typename T>
 struct InArg {
   const T* d = nullptr;
@@ -165,16 +175,13 @@ struct InArg {
     if (k == MemKind::Device) { d = src; return ITS_OK; }
     its_status s = tmp.alloc(ctx, count);
     if (s != ITS_OK) return s;
-    ITS_CU(ctx, cudaMemcpyAsync(tmp.p, src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
     d = tmp.p;
+    if (count * sizeof(T) >= kStagedUploadMin && !ctx->arena && ptrClass(src, ctx->device) == PtrClass::Pageable)
+      return copyToDeviceStaged(ctx, tmp.p, src, count * sizeof(T));
+    ITS_CU(ctx, cudaMemcpyAsync(tmp.p, src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
     return ITS_OK;
   }
 };
-// Device-to-host copy of bytes into pageable dst through pinned chunks, the chunks copied on
-// by several host threads; returns with the data in dst (its_hostio.cu).
-constexpr size_t kStagedCopyMin = 8u << 20;
-its_status copyToHostStaged(its_ctx* ctx, void* dst, const void* src, size_t bytes);
-void hostIoRelease(its_ctx* ctx);
 
 // A written argument: device scratch copied back to a host destination by finish().
 template <typename T>

@@ -157,4 +157,57 @@ its_status copyToHostStaged(its_ctx* ctx, void* dst, const void* src, size_t byt
   return ITS_OK;
 }
 
+its_status copyToDeviceStaged(its_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  its_status st = hostIoInit(ctx);
+  if (st != ITS_OK) return st;
+  HostIo* h = ctx->hostio;
+  // pieces of a quarter of the copy (at least 4 MB, at most a chunk), so that the host's copy
+  // into one buffer overlaps the transfer from the other
+  size_t piece = bytes / 4;
+  piece = piece < (4u << 20) ? (4u << 20) : (piece > kChunk ? kChunk : piece);
+  const size_t chunks = (bytes + piece - 1) / piece;
+  for (size_t c = 0; c < chunks; ++c) {
+    const int b = (int)(c & 1);
+    // the buffer's previous transfer (of this call or an earlier one) has left it
+    ITS_CU(ctx, cudaEventSynchronize(h->ready[b]));
+    const size_t off = c * piece, len = bytes - off < piece ? bytes - off : piece;
+    const uint8_t* from = (const uint8_t*)src + off;
+    uint8_t* to = h->stage[b];
+    const int parts = h->pool->size();
+    const size_t per = ((len + parts - 1) / parts + kPage - 1) / kPage * kPage;
+    h->pool->run(parts, [&](int p) {
+      const size_t a = (size_t)p * per;
+      if (a >= len) return;
+      const size_t n = len - a < per ? len - a : per;
+      memcpy(to + a, from + a, n);
+    });
+    ITS_CU(ctx, cudaMemcpyAsync((uint8_t*)dst + off, to, len, cudaMemcpyHostToDevice, ctx->stream));
+    ITS_CU(ctx, cudaEventRecord(h->ready[b], ctx->stream));
+  }
+  return ITS_OK;
+}
+
 }  // namespace its
+
+using namespace its;
+
+extern "C" {
+
+its_status its_copy_to_device(its_ctx* ctx, void* dst, const void* src, int64_t bytes) {
+  if (!ctx || bytes < 0 || (bytes > 0 && (!dst || !src))) return ITS_ERR_INVALID;
+  if (bytes == 0) return ITS_OK;
+  ITS_CU(ctx, cudaSetDevice(ctx->device));
+  if (ptrClass(dst, ctx->device) != PtrClass::Device)
+    return setError(ctx, ITS_ERR_INVALID, "its_copy_to_device: the destination must be device memory of the context's GPU");
+  const PtrClass k = ptrClass(src, ctx->device);
+  its_status st = ITS_OK;
+  if (k == PtrClass::Pageable && (size_t)bytes >= kStagedUploadMin)
+    st = copyToDeviceStaged(ctx, dst, src, (size_t)bytes);
+  else
+    ITS_CU(ctx, cudaMemcpyAsync(dst, src, (size_t)bytes, cudaMemcpyDefault, ctx->stream));
+  if (st != ITS_OK) return st;
+  ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  return ITS_OK;
+}
+
+}  // extern "C"

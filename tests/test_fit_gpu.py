@@ -260,3 +260,15 @@ def test_exact_start_batch_matches_single(ctx):
     for (svo, b, s), x, r in zip(many, outs, rels):
         assert np.array_equal(x, svo.exact_start(b, shares=s))
         assert r == svo.residual(b, x)
+
+
+@pytest.mark.gpu
+def test_copy_to_device_small_and_staged(ctx):
+    # its_copy_to_device: a small array by one copy, a large pageable one through the pinned
+    # chunks filled by host threads (also the path of every large host input)
+    rng = np.random.default_rng(3)
+    for n in (1000, 5_000_001, 9_000_001):  # 8 KB, 40 MB (below the staged size), 72 MB (pieces, odd tail)
+        a = rng.standard_normal(n)
+        assert np.array_equal(ctx.to_device(a).cpu().numpy(), a)
+    f = rng.integers(0, 1 << 30, size=(6_000_000, 3)).astype(np.int32)
+    assert np.array_equal(ctx.to_device(f).cpu().numpy(), f)
