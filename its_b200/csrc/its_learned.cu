@@ -60,6 +60,10 @@ struct LearnedPlan {
   double* bStage = nullptr;   // device copies of host vectors
   double* lamStage = nullptr;
   int mapSlot = -1;            // relHost's slot in the context's mapped slab (-1: its own allocation)
+  // the kinds of the last call's norm, b and lambda addresses (the graph is reused only for
+  // the same addresses, so the kinds are looked up again only when an address changes)
+  const void* kindOf[3] = {nullptr, nullptr, nullptr};
+  PtrClass kind[3] = {PtrClass::Pageable, PtrClass::Pageable, PtrClass::Pageable};
 };
 
 static void dropGraph(LearnedPlan* p) {
@@ -214,13 +218,26 @@ its_status its_learned_fit(its_svo* svo, its_mlp* mlp, const double* b, const fl
   LearnedPlan* p = nullptr;
   if ((st = planFor(svo, &p)) != ITS_OK) return st;
   if (report) std::memset(report, 0, sizeof(*report));
+  const void* addr[3] = {norm, b, lambda};
+  for (int k = 0; k < 3; ++k)
+    if (p->kindOf[k] != addr[k]) {
+      p->kind[k] = ptrClass(addr[k], ctx->device);
+      p->kindOf[k] = addr[k];
+    }
+  const PtrClass cn = p->kind[0], cb = p->kind[1], cl = p->kind[2];
+  if (cn == PtrClass::OtherDevice || cb == PtrClass::OtherDevice || cl == PtrClass::OtherDevice) {
+    p->kindOf[0] = p->kindOf[1] = p->kindOf[2] = nullptr;
+    return otherDeviceError(ctx);
+  }
   float hn[kNormValues];
-  if ((st = hostNorm(ctx, norm, hn)) != ITS_OK) return st;
+  if (cn == PtrClass::Device) {
+    ITS_CU(ctx, cudaMemcpyAsync(hn, norm, sizeof(hn), cudaMemcpyDeviceToHost, ctx->stream));
+    ITS_CU(ctx, cudaStreamSynchronize(ctx->stream));
+  } else {
+    std::memcpy(hn, norm, sizeof(hn));
+  }
   const int64_t n = svo->d.numVerts;
-  // device addresses of the vectors: the caller's, or the plan's copies of host vectors (one
-  // attribute query per vector)
-  const PtrClass cb = ptrClass(b, ctx->device), cl = ptrClass(lambda, ctx->device);
-  if (cb == PtrClass::OtherDevice || cl == PtrClass::OtherDevice) return otherDeviceError(ctx);
+  // device addresses of the vectors: the caller's, or the plan's copies of host vectors
   const bool bHost = cb != PtrClass::Device, lamHost = cl != PtrClass::Device;
   if ((bHost && !p->bStage && (st = devAlloc(ctx, (void**)&p->bStage, std::max<int64_t>(n, 1) * 8)) != ITS_OK) ||
       (lamHost && !p->lamStage && (st = devAlloc(ctx, (void**)&p->lamStage, std::max<int64_t>(n, 1) * 8)) != ITS_OK))
