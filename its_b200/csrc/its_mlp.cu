@@ -65,76 +65,122 @@ __device__ __forceinline__ float geluGrad(float z) {
 }
 
 // ---- one tcgen05 GEMM: C[m][n] = sum_k A[m][k] B[n][k] over this CTA's K range -------------
+// 128 rows per CTA and four warp groups: 64-wide K chunks are fetched by all 512 threads with
+// cp.async into one of two stages while the tensor core multiplies the other; the accumulator
+// (TMEM) is read back by each warp group for a quarter of the columns (thread = row, the TMEM
+// lane of its warp) and handed to the epilogue functor with that quarter.
+constexpr int kGemmGroups = 4;
+constexpr int kGemmThreads = 128 * kGemmGroups;
 template <int N>
 struct GemmSmem {
-  static constexpr int kA = 128 * 128, kB = N * 128;
-  static constexpr int kBytes = kA + kB + 64 + 1024;  // + mbarrier, TMEM slot, alignment slack
+  static constexpr int kA = 128 * 128, kB = N * 128, kStage = kA + kB;
+  // two stages, the epilogue's per-group row partials and per-row value, mbarriers, TMEM slot
+  static constexpr int kBytes = 2 * kStage + (kGemmGroups + 1) * 128 * 4 + 64 + 1024;
 };
 
+// 16 bytes global -> shared without staging through registers; bytes < 16 zero-fills the rest.
+__device__ __forceinline__ void cpAsync16(uint32_t dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int Pending>
+__device__ __forceinline__ void cpAsyncWait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(Pending) : "memory");
+}
+
 template <int N, class Epi>
-__global__ void __launch_bounds__(128) kUmmaGemm(const bf16* __restrict__ A, int64_t lda, int64_t M,
-                                                 const bf16* __restrict__ B, int64_t ldb, int64_t K,
-                                                 int64_t kPerSplit, Epi epi, int* __restrict__ err) {
+__global__ void __launch_bounds__(kGemmThreads, 1) kUmmaGemm(const bf16* __restrict__ A, int64_t lda, int64_t M,
+                                                             const bf16* __restrict__ B, int64_t ldb, int64_t K,
+                                                             int64_t kPerSplit, Epi epi, int* __restrict__ err) {
   using namespace umma;
   extern __shared__ uint8_t smemRaw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smemRaw + 1023) & ~(uintptr_t)1023);
-  uint8_t* sA = smem;
-  uint8_t* sB = smem + GemmSmem<N>::kA;
-  uint64_t* mbar = (uint64_t*)(sB + GemmSmem<N>::kB);
-  uint32_t* slot = (uint32_t*)(mbar + 1);
-  const int tid = threadIdx.x, warp = tid >> 5;
+  float* sPart = (float*)(smem + 2 * GemmSmem<N>::kStage);  // [group][row]
+  float* sRow = sPart + kGemmGroups * 128;                  // [row]
+  uint64_t* mbar = (uint64_t*)(sRow + 128);                 // one per stage
+  uint32_t* slot = (uint32_t*)(mbar + 2);
+  const int tid = threadIdx.x, warp = tid >> 5, grp = tid >> 7, row = tid & 127;
   const int64_t m0 = (int64_t)blockIdx.x * 128;
   const int64_t k0 = (int64_t)blockIdx.z * kPerSplit;
   const int64_t k1 = k0 + kPerSplit < K ? k0 + kPerSplit : K;
   constexpr uint32_t kCols = N < 32 ? 32 : N;
   if (warp == 0) tmemAlloc(smemAddr(slot), kCols);
-  if (tid == 0) mbarInit(smemAddr(mbar), 1);
+  if (tid == 0) {
+    mbarInit(smemAddr(mbar), 1);
+    mbarInit(smemAddr(mbar + 1), 1);
+  }
   fenceBefore();
   __syncthreads();
   fenceAfter();
   const uint32_t tmem = *slot;
   constexpr uint32_t idesc = idescBf16(128, N);
-  uint32_t phase = 0;
-  bool ok = true;
-  for (int64_t kc = k0; kc < k1; kc += 64) {
-    for (int i = tid; i < 128 * 8; i += 128) {
+  // chunk kc into stage st; columns past the split's end (and rows past M) read as zeros
+  auto load = [&](int st, int64_t kc) {
+    uint8_t* sA = smem + st * GemmSmem<N>::kStage;
+    uint8_t* sB = sA + GemmSmem<N>::kA;
+    for (int i = tid; i < 128 * 8; i += kGemmThreads) {
       const int r = i >> 3, c = i & 7;
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if (m0 + r < M) v = __ldg((const uint4*)(A + (m0 + r) * lda + kc + c * 8));
-      *(uint4*)(sA + swizzledChunk(r, c)) = v;
+      const int64_t col = kc + c * 8, left = k1 - col;
+      const uint32_t bytes = (m0 + r < M && left > 0) ? (uint32_t)(left >= 8 ? 16 : 2 * left) : 0u;
+      cpAsync16(smemAddr(sA + swizzledChunk(r, c)), bytes ? (const void*)(A + (m0 + r) * lda + col) : (const void*)A,
+                bytes);
     }
-    for (int i = tid; i < N * 8; i += 128) {
+    for (int i = tid; i < N * 8; i += kGemmThreads) {
       const int r = i >> 3, c = i & 7;
-      *(uint4*)(sB + swizzledChunk(r, c)) = __ldg((const uint4*)(B + (int64_t)r * ldb + kc + c * 8));
+      const int64_t col = kc + c * 8, left = k1 - col;
+      const uint32_t bytes = left > 0 ? (uint32_t)(left >= 8 ? 16 : 2 * left) : 0u;
+      cpAsync16(smemAddr(sB + swizzledChunk(r, c)), bytes ? (const void*)(B + (int64_t)r * ldb + col) : (const void*)B,
+                bytes);
+    }
+    cpAsyncCommit();
+  };
+  const int nk = k1 > k0 ? (int)((k1 - k0 + 63) / 64) : 0;
+  uint32_t ph[2] = {0u, 0u};
+  bool ok = true;
+  if (nk > 0) load(0, k0);
+  for (int c = 0; c < nk; ++c) {
+    const int st = c & 1;
+    if (c + 1 < nk) {
+      if (c >= 1) {  // the products of chunk c - 1 have read the stage chunk c + 1 goes into
+        ok = mbarWait(smemAddr(mbar + (st ^ 1)), ph[st ^ 1]) && ok;
+        ph[st ^ 1] ^= 1u;
+      }
+      load(st ^ 1, k0 + (int64_t)(c + 1) * 64);
+      cpAsyncWait<1>();  // this chunk's copies (the next chunk's may still be in flight)
+    } else {
+      cpAsyncWait<0>();
     }
     fenceProxyAsync();
     __syncthreads();
     if (tid == 0) {
       fenceAfter();
-      const uint64_t da = descSw128(smemAddr(sA)), db = descSw128(smemAddr(sB));
+      const uint8_t* sA = smem + st * GemmSmem<N>::kStage;
+      const uint64_t da = descSw128(smemAddr(sA)), db = descSw128(smemAddr(sA + GemmSmem<N>::kA));
 #pragma unroll
-      for (int k = 0; k < 4; ++k) mma(tmem, da + 2 * k, db + 2 * k, idesc, (kc > k0 || k > 0) ? 1u : 0u);
-      commit(smemAddr(mbar));
+      for (int k = 0; k < 4; ++k) mma(tmem, da + 2 * k, db + 2 * k, idesc, (c > 0 || k > 0) ? 1u : 0u);
+      commit(smemAddr(mbar + st));
     }
-    ok = mbarWait(smemAddr(mbar), phase) && ok;
-    phase ^= 1u;
+  }
+  if (nk > 0) {  // the last chunk's products (and with them every earlier one)
+    const int st = (nk - 1) & 1;
+    ok = mbarWait(smemAddr(mbar + st), ph[st]) && ok;
   }
   fenceAfter();
-  float acc[N];
-  const uint32_t lane = (uint32_t)(warp * 32) << 16;
-#pragma unroll
-  for (int n0 = 0; n0 < N; n0 += 16) {
-    float v[16];
-    tmemLoad16(tmem + lane + (uint32_t)n0, v);
-#pragma unroll
-    for (int j = 0; j < 16; ++j) acc[n0 + j] = v[j];
+  constexpr int C = N / kGemmGroups;
+  static_assert(C == 16 || C == 32, "a quarter of the columns per warp group");
+  float v[C];
+  const uint32_t lane = (uint32_t)((warp & 3) * 32) << 16;
+  if constexpr (C == 32) {
+    tmemLoad32(tmem + lane + (uint32_t)(grp * C), v);
+  } else {
+    tmemLoad16(tmem + lane + (uint32_t)(grp * C), v);
   }
   if (k1 <= k0) {  // an empty split contributes zeros
 #pragma unroll
-    for (int j = 0; j < N; ++j) acc[j] = 0.0f;
+    for (int j = 0; j < C; ++j) v[j] = 0.0f;
   }
-  const int64_t m = m0 + tid;
-  if (ok && m < M) epi(m, acc);
+  const int64_t m = m0 + row;
+  epi(m, ok && m < M, grp * C, v, sPart, sRow, grp);
   fenceBefore();
   __syncthreads();
   if (warp == 0) tmemFree(tmem, kCols);
@@ -142,8 +188,10 @@ __global__ void __launch_bounds__(128) kUmmaGemm(const bf16* __restrict__ A, int
 }
 
 // ---- epilogues ----------------------------------------------------------------------------
-// A thread owns one row (its TMEM lane), so its row-major stores go out in 16-byte pieces
-// (eight BF16 or four FP32 values per store); the transposed copies are coalesced as they are.
+// Each is called by every thread with its row m, whether the row is written (valid), the first
+// column j0 of its warp group's quarter and that quarter's accumulators. The row-major stores
+// go out in 16-byte pieces (eight BF16 or four FP32 values per store); the transposed copies are
+// coalesced across the warp as they are.
 __device__ __forceinline__ uint4 packBf16x8(const float* v) {
   uint4 r;
   __nv_bfloat162* q = (__nv_bfloat162*)&r;
@@ -160,35 +208,41 @@ struct EpiHidden {
   bf16* H;
   bf16* Ht;
   int64_t ldt;
-  __device__ void operator()(int64_t m, float (&acc)[kHid]) const {
+  template <int C>
+  __device__ void operator()(int64_t m, bool valid, int j0, float (&v)[C], float*, float*, int) const {
+    if (!valid) return;
 #pragma unroll
-    for (int j0 = 0; j0 < kHid; j0 += 8) {
+    for (int jb = 0; jb < C; jb += 8) {
+      const int j = j0 + jb;
       float z[8], h[8];
 #pragma unroll
       for (int e = 0; e < 8; ++e) {
-        z[e] = acc[j0 + e] + bias[j0 + e];
+        z[e] = v[jb + e] + bias[j + e];
         h[e] = geluF(z[e]);
       }
       if (Z) {
-        *(float4*)(Z + m * kHid + j0) = make_float4(z[0], z[1], z[2], z[3]);
-        *(float4*)(Z + m * kHid + j0 + 4) = make_float4(z[4], z[5], z[6], z[7]);
+        *(float4*)(Z + m * kHid + j) = make_float4(z[0], z[1], z[2], z[3]);
+        *(float4*)(Z + m * kHid + j + 4) = make_float4(z[4], z[5], z[6], z[7]);
       }
       const uint4 hb = packBf16x8(h);
-      *(uint4*)(H + m * kHid + j0) = hb;
+      *(uint4*)(H + m * kHid + j) = hb;
       if (Ht) {
         const bf16* hv = (const bf16*)&hb;
 #pragma unroll
-        for (int e = 0; e < 8; ++e) Ht[(int64_t)(j0 + e) * ldt + m] = hv[e];
+        for (int e = 0; e < 8; ++e) Ht[(int64_t)(j + e) * ldt + m] = hv[e];
       }
     }
   }
 };
 
 constexpr int kOutParts = 4;  // partial sums of the output unit (one per quarter of the columns)
+static_assert(kOutParts == kGemmGroups, "the output unit's partial sums follow the warp groups");
 
 // Last hidden layer plus the output unit. Inference: out = sum_j h_j w4_j + b4. Training also
 // forms the loss gradient d = scale (out - y) and dZ3 = d w4 gelu'(z3), the stored H3 (for
-// the w4 gradient) and the per-row squared error.
+// the w4 gradient) and the per-row squared error. The output unit sums each quarter of the
+// columns in order (one per warp group), then the four partial sums in order -- the fused
+// inference kernel's split, so both give the same bits.
 struct EpiOutput {
   const float* bias;
   const float* w4;  // BF16-rounded values
@@ -203,47 +257,57 @@ struct EpiOutput {
   int64_t ldt;
   float* dOut;
   float* sqErr;
-  __device__ void operator()(int64_t m, float (&acc)[kHid]) const {
-    // the output unit sums each quarter of the columns in order, then the four partial sums
-    // in order (the fused inference kernel's per-warp-group split; both give the same bits)
-    float part[kOutParts];
+  template <int C>
+  __device__ void operator()(int64_t m, bool valid, int j0, float (&v)[C], float* sPart, float* sRow, int grp) const {
+    const int row = threadIdx.x & 127;
+    float o = 0.0f;
+    if (valid) {
 #pragma unroll
-    for (int g = 0; g < kOutParts; ++g) {
-      float o = 0.0f;
-#pragma unroll
-      for (int j0 = g * (kHid / kOutParts); j0 < (g + 1) * (kHid / kOutParts); j0 += 8) {
+      for (int jb = 0; jb < C; jb += 8) {
         float h[8];
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
-          const int j = j0 + e;
-          acc[j] += bias[j];
-          h[e] = __bfloat162float(__float2bfloat16_rn(geluF(acc[j])));
+          const int j = j0 + jb + e;
+          v[jb + e] += bias[j];
+          h[e] = __bfloat162float(__float2bfloat16_rn(geluF(v[jb + e])));
           o += h[e] * w4[j];
         }
-        if (H3) *(uint4*)(H3 + m * kHid + j0) = packBf16x8(h);
+        if (H3) *(uint4*)(H3 + m * kHid + j0 + jb) = packBf16x8(h);
       }
-      part[g] = o;
     }
-    float o = part[0];
+    sPart[grp * 128 + row] = o;
+    __syncthreads();
+    if (grp == 0) {
+      float d = 0.0f;
+      if (valid) {
+        float oo = sPart[row];
 #pragma unroll
-    for (int g = 1; g < kOutParts; ++g) o += part[g];
-    o += b4[0];
-    if (out) out[m] = o;
-    if (!y) return;
-    const float e = o - y[m];
-    const float d = scale * e;
-    dOut[m] = d;
-    sqErr[m] = e * e;
+        for (int g = 1; g < kOutParts; ++g) oo += sPart[g * 128 + row];
+        oo += b4[0];
+        if (out) out[m] = oo;
+        if (y) {
+          const float e = oo - y[m];
+          d = scale * e;
+          dOut[m] = d;
+          sqErr[m] = e * e;
+        }
+      }
+      sRow[row] = d;
+    }
+    __syncthreads();
+    if (!valid || !y) return;
+    const float d = sRow[row];
 #pragma unroll
-    for (int j0 = 0; j0 < kHid; j0 += 8) {
+    for (int jb = 0; jb < C; jb += 8) {
+      const int j = j0 + jb;
       float g[8];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) g[k] = d * w4[j0 + k] * geluGrad(acc[j0 + k]);
+      for (int k = 0; k < 8; ++k) g[k] = d * w4[j + k] * geluGrad(v[jb + k]);
       const uint4 gb = packBf16x8(g);
-      *(uint4*)(dZ + m * kHid + j0) = gb;
+      *(uint4*)(dZ + m * kHid + j) = gb;
       const bf16* gv = (const bf16*)&gb;
 #pragma unroll
-      for (int k = 0; k < 8; ++k) dZt[(int64_t)(j0 + k) * ldt + m] = gv[k];
+      for (int k = 0; k < 8; ++k) dZt[(int64_t)(j + k) * ldt + m] = gv[k];
     }
   }
 };
@@ -254,19 +318,22 @@ struct EpiBack {
   bf16* dZ;
   bf16* dZt;
   int64_t ldt;
-  __device__ void operator()(int64_t m, float (&acc)[kHid]) const {
+  template <int C>
+  __device__ void operator()(int64_t m, bool valid, int j0, float (&v)[C], float*, float*, int) const {
+    if (!valid) return;
 #pragma unroll
-    for (int j0 = 0; j0 < kHid; j0 += 8) {
-      const float4 z0 = *(const float4*)(Z + m * kHid + j0), z1 = *(const float4*)(Z + m * kHid + j0 + 4);
+    for (int jb = 0; jb < C; jb += 8) {
+      const int j = j0 + jb;
+      const float4 z0 = *(const float4*)(Z + m * kHid + j), z1 = *(const float4*)(Z + m * kHid + j + 4);
       const float z[8] = {z0.x, z0.y, z0.z, z0.w, z1.x, z1.y, z1.z, z1.w};
       float g[8];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) g[k] = acc[j0 + k] * geluGrad(z[k]);
+      for (int k = 0; k < 8; ++k) g[k] = v[jb + k] * geluGrad(z[k]);
       const uint4 gb = packBf16x8(g);
-      if (dZ) *(uint4*)(dZ + m * kHid + j0) = gb;
+      if (dZ) *(uint4*)(dZ + m * kHid + j) = gb;
       const bf16* gv = (const bf16*)&gb;
 #pragma unroll
-      for (int k = 0; k < 8; ++k) dZt[(int64_t)(j0 + k) * ldt + m] = gv[k];
+      for (int k = 0; k < 8; ++k) dZt[(int64_t)(j + k) * ldt + m] = gv[k];
     }
   }
 };
@@ -276,10 +343,12 @@ template <int N>
 struct EpiPartial {
   float* partial;
   int64_t rows;
-  __device__ void operator()(int64_t m, float (&acc)[N]) const {
-    float* p = partial + ((int64_t)blockIdx.z * rows + m) * N;
+  template <int C>
+  __device__ void operator()(int64_t m, bool valid, int j0, float (&v)[C], float*, float*, int) const {
+    if (!valid) return;
+    float* p = partial + ((int64_t)blockIdx.z * rows + m) * N + j0;
 #pragma unroll
-    for (int j = 0; j < N; j += 4) *(float4*)(p + j) = make_float4(acc[j], acc[j + 1], acc[j + 2], acc[j + 3]);
+    for (int j = 0; j < C; j += 4) *(float4*)(p + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
   }
 };
 
@@ -295,7 +364,7 @@ constexpr int kFusedGroups = 4;                                // warp groups pe
 constexpr int kSlotThreads = 128 * kFusedGroups;
 constexpr int kFusedThreads = kSlotThreads * kFusedSlots;
 constexpr int kGroupCols = 128 / kFusedGroups;
-static_assert(kFusedGroups == kOutParts, "the output unit's partial sums follow the warp groups");
+static_assert(kFusedGroups == kOutParts, "the output unit's partial sums follow the warp groups in both kernels");
 constexpr int kFusedSmem = 16384 /*W1*/ + 32768 /*W2*/ + 32768 /*W3*/ + kFusedSlots * (16384 /*X*/ + 32768 /*H*/) +
                            4 * 128 * 4 /*b1 b2 b3 w4*/ + kFusedSlots * kFusedGroups * 128 * 4 /*partial sums*/ + 64 +
                            1024;
@@ -653,7 +722,7 @@ static its_status gemm(its_ctx* ctx, const bf16* A, int64_t lda, int64_t M, cons
   }
   const int64_t kPer = ((K / splits + 63) / 64) * 64;
   dim3 grid((unsigned)((M + 127) / 128), 1, (unsigned)splits);
-  kUmmaGemm<N, Epi><<<grid, 128, GemmSmem<N>::kBytes, ctx->stream>>>(A, lda, M, B, ldb, K, kPer, epi, err);
+  kUmmaGemm<N, Epi><<<grid, kGemmThreads, GemmSmem<N>::kBytes, ctx->stream>>>(A, lda, M, B, ldb, K, kPer, epi, err);
   ITS_LAUNCHED(ctx);
   return ITS_OK;
 }
