@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) kUmmaGemm(const bf16* __restr
     for (int j = 0; j < C; ++j) v[j] = 0.0f;
   }
   const int64_t m = m0 + row;
-  epi(m, ok && m < M, grp * C, v, sPart, sRow, grp);
+  epi(m, ok && m < M, grp * C, v, sPart, sRow, grp, smem, m0, M);  // the stages are free: the products are done
   fenceBefore();
   __syncthreads();
   if (warp == 0) tmemFree(tmem, kCols);
@@ -199,6 +199,27 @@ __device__ __forceinline__ uint4 packBf16x8(const float* v) {
   for (int e = 0; e < 4; ++e) q[e] = __floats2bfloat162_rn(v[2 * e], v[2 * e + 1]);
   return r;
 }
+// The transposed copy of a 128-row tile goes through shared memory (sT[column][row], BF16):
+// each thread stages its row's values, then the block writes whole rows of the transposed
+// matrix (128 consecutive m) in 16-byte pieces.
+__device__ __forceinline__ void stageT(bf16* sT, int row, int j, const uint4& vals) {
+  const bf16* v = (const bf16*)&vals;
+#pragma unroll
+  for (int e = 0; e < 8; ++e) sT[(j + e) * 128 + row] = v[e];
+}
+__device__ __forceinline__ void storeT(const bf16* sT, bf16* dstT, int64_t ldt, int64_t m0, int64_t M) {
+  for (int p = threadIdx.x; p < kHid * 16; p += blockDim.x) {
+    const int j = p >> 4, r8 = (p & 15) * 8;
+    const int64_t m = m0 + r8;
+    bf16* dst = dstT + (int64_t)j * ldt + m;
+    const bf16* src = sT + j * 128 + r8;
+    if (m + 8 <= M) {
+      *(uint4*)dst = *(const uint4*)src;
+    } else {
+      for (int e = 0; e < 8 && m + e < M; ++e) dst[e] = src[e];
+    }
+  }
+}
 
 // Hidden layer: z = acc + b, h = gelu(z); Z (FP32, for the backward pass), H row-major and
 // its transpose (the operands of the next layer and of the weight gradient).
@@ -209,29 +230,31 @@ struct EpiHidden {
   bf16* Ht;
   int64_t ldt;
   template <int C>
-  __device__ void operator()(int64_t m, bool valid, int j0, float (&v)[C], float*, float*, int) const {
-    if (!valid) return;
+  __device__ void operator()(int64_t m, bool valid, int j0, float (&v)[C], float*, float*, int, uint8_t* stage,
+                             int64_t m0, int64_t M) const {
+    bf16* sT = (bf16*)stage;
+    if (valid) {
 #pragma unroll
-    for (int jb = 0; jb < C; jb += 8) {
-      const int j = j0 + jb;
-      float z[8], h[8];
+      for (int jb = 0; jb < C; jb += 8) {
+        const int j = j0 + jb;
+        float z[8], h[8];
 #pragma unroll
-      for (int e = 0; e < 8; ++e) {
-        z[e] = v[jb + e] + bias[j + e];
-        h[e] = geluF(z[e]);
-      }
-      if (Z) {
-        *(float4*)(Z + m * kHid + j) = make_float4(z[0], z[1], z[2], z[3]);
-        *(float4*)(Z + m * kHid + j + 4) = make_float4(z[4], z[5], z[6], z[7]);
-      }
-      const uint4 hb = packBf16x8(h);
-      *(uint4*)(H + m * kHid + j) = hb;
-      if (Ht) {
-        const bf16* hv = (const bf16*)&hb;
-#pragma unroll
-        for (int e = 0; e < 8; ++e) Ht[(int64_t)(j + e) * ldt + m] = hv[e];
+        for (int e = 0; e < 8; ++e) {
+          z[e] = v[jb + e] + bias[j + e];
+          h[e] = geluF(z[e]);
+        }
+        if (Z) {
+          *(float4*)(Z + m * kHid + j) = make_float4(z[0], z[1], z[2], z[3]);
+          *(float4*)(Z + m * kHid + j + 4) = make_float4(z[4], z[5], z[6], z[7]);
+        }
+        const uint4 hb = packBf16x8(h);
+        *(uint4*)(H + m * kHid + j) = hb;
+        if (Ht) stageT(sT, threadIdx.x & 127, j, hb);
       }
     }
+    if (!Ht) return;
+    __syncthreads();
+    storeT(sT, Ht, ldt, m0, M);
   }
 };
 
@@ -239,7 +262,7 @@ constexpr int kOutParts = 4;  // partial sums of the output unit (one per quarte
 static_assert(kOutParts == kGemmGroups, "the output unit's partial sums follow the warp groups");
 
 // Last hidden layer plus the output unit. Inference: out = sum_j h_j w4_j + b4. Training also
-// forms the loss gradient d = scale (out - y) and dZ3 = d w4 gelu'(z3), the stored H3 (for
+// forms the loss gradient d = scale (out - y) and dZ3 = d w4 gelu'(z3), H3 transposed (for
 // the w4 gradient) and the per-row squared error. The output unit sums each quarter of the
 // columns in order (one per warp group), then the four partial sums in order -- the fused
 // inference kernel's split, so both give the same bits.
@@ -251,15 +274,17 @@ struct EpiOutput {
   // training only
   const float* y;
   float scale;
-  bf16* H3;
+  bf16* H3t;  // H3 transposed (for the w4 gradient)
   bf16* dZ;
   bf16* dZt;
   int64_t ldt;
   float* dOut;
   float* sqErr;
   template <int C>
-  __device__ void operator()(int64_t m, bool valid, int j0, float (&v)[C], float* sPart, float* sRow, int grp) const {
+  __device__ void operator()(int64_t m, bool valid, int j0, float (&v)[C], float* sPart, float* sRow, int grp,
+                             uint8_t* stage, int64_t m0, int64_t M) const {
     const int row = threadIdx.x & 127;
+    bf16* sT3 = (bf16*)stage + kHid * 128;  // H3's transposed tile (the stage area's second half)
     float o = 0.0f;
     if (valid) {
 #pragma unroll
@@ -272,11 +297,12 @@ struct EpiOutput {
           h[e] = __bfloat162float(__float2bfloat16_rn(geluF(v[jb + e])));
           o += h[e] * w4[j];
         }
-        if (H3) *(uint4*)(H3 + m * kHid + j0 + jb) = packBf16x8(h);
+        if (H3t) stageT(sT3, row, j0 + jb, packBf16x8(h));
       }
     }
     sPart[grp * 128 + row] = o;
     __syncthreads();
+    if (H3t) storeT(sT3, H3t, ldt, m0, M);
     if (grp == 0) {
       float d = 0.0f;
       if (valid) {
@@ -295,20 +321,23 @@ struct EpiOutput {
       sRow[row] = d;
     }
     __syncthreads();
-    if (!valid || !y) return;
-    const float d = sRow[row];
+    if (!y) return;
+    bf16* sT = (bf16*)stage;
+    if (valid) {
+      const float d = sRow[row];
 #pragma unroll
-    for (int jb = 0; jb < C; jb += 8) {
-      const int j = j0 + jb;
-      float g[8];
+      for (int jb = 0; jb < C; jb += 8) {
+        const int j = j0 + jb;
+        float g[8];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) g[k] = d * w4[j + k] * geluGrad(v[jb + k]);
-      const uint4 gb = packBf16x8(g);
-      *(uint4*)(dZ + m * kHid + j) = gb;
-      const bf16* gv = (const bf16*)&gb;
-#pragma unroll
-      for (int k = 0; k < 8; ++k) dZt[(int64_t)(j + k) * ldt + m] = gv[k];
+        for (int k = 0; k < 8; ++k) g[k] = d * w4[j + k] * geluGrad(v[jb + k]);
+        const uint4 gb = packBf16x8(g);
+        *(uint4*)(dZ + m * kHid + j) = gb;
+        stageT(sT, row, j, gb);
+      }
     }
+    __syncthreads();
+    storeT(sT, dZt, ldt, m0, M);
   }
 };
 
@@ -319,22 +348,25 @@ struct EpiBack {
   bf16* dZt;
   int64_t ldt;
   template <int C>
-  __device__ void operator()(int64_t m, bool valid, int j0, float (&v)[C], float*, float*, int) const {
-    if (!valid) return;
+  __device__ void operator()(int64_t m, bool valid, int j0, float (&v)[C], float*, float*, int, uint8_t* stage,
+                             int64_t m0, int64_t M) const {
+    bf16* sT = (bf16*)stage;
+    if (valid) {
 #pragma unroll
-    for (int jb = 0; jb < C; jb += 8) {
-      const int j = j0 + jb;
-      const float4 z0 = *(const float4*)(Z + m * kHid + j), z1 = *(const float4*)(Z + m * kHid + j + 4);
-      const float z[8] = {z0.x, z0.y, z0.z, z0.w, z1.x, z1.y, z1.z, z1.w};
-      float g[8];
+      for (int jb = 0; jb < C; jb += 8) {
+        const int j = j0 + jb;
+        const float4 z0 = *(const float4*)(Z + m * kHid + j), z1 = *(const float4*)(Z + m * kHid + j + 4);
+        const float z[8] = {z0.x, z0.y, z0.z, z0.w, z1.x, z1.y, z1.z, z1.w};
+        float g[8];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) g[k] = v[jb + k] * geluGrad(z[k]);
-      const uint4 gb = packBf16x8(g);
-      if (dZ) *(uint4*)(dZ + m * kHid + j) = gb;
-      const bf16* gv = (const bf16*)&gb;
-#pragma unroll
-      for (int k = 0; k < 8; ++k) dZt[(int64_t)(j + k) * ldt + m] = gv[k];
+        for (int k = 0; k < 8; ++k) g[k] = v[jb + k] * geluGrad(z[k]);
+        const uint4 gb = packBf16x8(g);
+        if (dZ) *(uint4*)(dZ + m * kHid + j) = gb;
+        stageT(sT, threadIdx.x & 127, j, gb);
+      }
     }
+    __syncthreads();
+    storeT(sT, dZt, ldt, m0, M);
   }
 };
 
@@ -344,7 +376,8 @@ struct EpiPartial {
   float* partial;
   int64_t rows;
   template <int C>
-  __device__ void operator()(int64_t m, bool valid, int j0, float (&v)[C], float*, float*, int) const {
+  __device__ void operator()(int64_t m, bool valid, int j0, float (&v)[C], float*, float*, int, uint8_t*, int64_t,
+                             int64_t) const {
     if (!valid) return;
     float* p = partial + ((int64_t)blockIdx.z * rows + m) * N + j0;
 #pragma unroll
@@ -626,7 +659,7 @@ __device__ __forceinline__ float blockSum256(float v) {
 // weights (H3^T dOut), the output bias (sum dOut) and the loss (mean squared error).
 // Block b: 0..383 hidden biases, 384..511 w4, 512 b4, 513 loss.
 __global__ void __launch_bounds__(256) kSmallGrads(const bf16* __restrict__ dZ1t, const bf16* __restrict__ dZ2t,
-                                                  const bf16* __restrict__ dZ3t, const bf16* __restrict__ H3,
+                                                  const bf16* __restrict__ dZ3t, const bf16* __restrict__ H3t,
                                                   const float* __restrict__ dOut, const float* __restrict__ sqErr,
                                                   int64_t n, int64_t ldt, float* __restrict__ grad,
                                                   float* __restrict__ loss) {
@@ -637,7 +670,7 @@ __global__ void __launch_bounds__(256) kSmallGrads(const bf16* __restrict__ dZ1t
     for (int64_t m = threadIdx.x; m < n; m += 256) s += __bfloat162float(row[m]);
   } else if (b < 4 * kHid) {
     const int j = b - 3 * kHid;
-    for (int64_t m = threadIdx.x; m < n; m += 256) s += dOut[m] * __bfloat162float(H3[m * kHid + j]);
+    for (int64_t m = threadIdx.x; m < n; m += 256) s += dOut[m] * __bfloat162float(H3t[(int64_t)j * ldt + m]);
   } else if (b == 4 * kHid) {
     for (int64_t m = threadIdx.x; m < n; m += 256) s += dOut[m];
   } else {
@@ -704,10 +737,26 @@ __global__ void kGatherBatch(const float* __restrict__ X, const float* __restric
   z ^= z >> 31;
   const int64_t r = (int64_t)(z % (uint64_t)n);
   yb[i] = y[r];
-  for (int k = 0; k < kIn; ++k) {
-    const bf16 v = __float2bfloat16_rn(X[r * kIn + k]);
-    Xb[i * kIn + k] = v;
-    Xt[(int64_t)k * B + i] = v;
+  const float* src = X + r * kIn;
+  if (((uintptr_t)X & 15) == 0) {  // the row in 16-byte pieces, the BF16 row out in 16-byte pieces
+#pragma unroll
+    for (int k = 0; k < kIn; k += 8) {
+      const float4 a = *(const float4*)(src + k), b = *(const float4*)(src + k + 4);
+      const float f[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+      __align__(16) bf16 q[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        q[e] = __float2bfloat16_rn(f[e]);
+        Xt[(int64_t)(k + e) * B + i] = q[e];
+      }
+      *(uint4*)(Xb + i * kIn + k) = *(const uint4*)q;
+    }
+  } else {
+    for (int k = 0; k < kIn; ++k) {
+      const bf16 v = __float2bfloat16_rn(src[k]);
+      Xb[i * kIn + k] = v;
+      Xt[(int64_t)k * B + i] = v;
+    }
   }
 }
 
@@ -745,7 +794,7 @@ struct its_mlp {
   float* w4r;
   uint8_t* img;  // the fused inference kernel's shared-memory image of the parameters
   // batch buffers
-  bf16 *Xb, *Xt, *H1, *H1t, *H2, *H2t, *H3, *dZ3, *dZ3t, *dZ2, *dZ2t, *dZ1t;
+  bf16 *Xb, *Xt, *H1, *H1t, *H2, *H2t, *H3t, *dZ3, *dZ3t, *dZ2, *dZ2t, *dZ1t;
   float *Z1, *Z2, *yb, *dOut, *sqErr, *out, *part1, *part2, *part3;
   int* err;
   std::vector<void*> allocs;
@@ -778,7 +827,7 @@ static its_status mlpForward(its_mlp* h, int64_t n, bool train, const float* y, 
   if ((st = gemm<kHid>(ctx, h->Xb, kIn, n, h->W1, kIn, kIn, 1, e1, h->err)) != ITS_OK) return st;
   EpiHidden e2{h->P + kOffB2, train ? h->Z2 : nullptr, h->H2, train ? h->H2t : nullptr, ldt};
   if ((st = gemm<kHid>(ctx, h->H1, kHid, n, h->W2, kHid, kHid, 1, e2, h->err)) != ITS_OK) return st;
-  EpiOutput e3{h->P + kOffB3, h->w4r, h->P + kOffB4, out, y, 2.0f / (float)n, train ? h->H3 : nullptr,
+  EpiOutput e3{h->P + kOffB3, h->w4r, h->P + kOffB4, out, y, 2.0f / (float)n, train ? h->H3t : nullptr,
                h->dZ3, h->dZ3t, ldt, h->dOut, h->sqErr};
   return gemm<kHid>(ctx, h->H2, kHid, n, h->W3, kHid, kHid, 1, e3, h->err);
 }
@@ -803,7 +852,7 @@ static its_status mlpGradient(its_mlp* h, int64_t n) {
   if ((st = gemm<kIn>(ctx, h->dZ1t, ldt, kHid, h->Xt, ldt, n, kSplitK, p1, h->err)) != ITS_OK) return st;
   kSumPartials<<<gridFor(kHid * kHid, 256), 256, 0, ctx->stream>>>(h->part1, h->part2, h->part3, h->G);
   ITS_LAUNCHED(ctx);
-  kSmallGrads<<<4 * kHid + 2, 256, 0, ctx->stream>>>(h->dZ1t, h->dZ2t, h->dZ3t, h->H3, h->dOut, h->sqErr, n, ldt, h->G,
+  kSmallGrads<<<4 * kHid + 2, 256, 0, ctx->stream>>>(h->dZ1t, h->dZ2t, h->dZ3t, h->H3t, h->dOut, h->sqErr, n, ldt, h->G,
                                                      h->loss);
   ITS_LAUNCHED(ctx);
   return ITS_OK;
@@ -877,7 +926,7 @@ its_status its_mlp_create(its_ctx* ctx, int64_t batch, its_mlp** out) {
   A(&h->W1, kHid * kIn); A(&h->W1t, kHid * kIn); A(&h->W2, kHid * kHid); A(&h->W2t, kHid * kHid);
   A(&h->W3, kHid * kHid); A(&h->W3t, kHid * kHid); A(&h->w4r, kHid); A(&h->img, kImgBytes);
   A(&h->Xb, B * kIn); A(&h->Xt, B * kIn); A(&h->H1, B * kHid); A(&h->H1t, B * kHid); A(&h->H2, B * kHid);
-  A(&h->H2t, B * kHid); A(&h->H3, B * kHid); A(&h->dZ3, B * kHid); A(&h->dZ3t, B * kHid); A(&h->dZ2, B * kHid);
+  A(&h->H2t, B * kHid); A(&h->H3t, B * kHid); A(&h->dZ3, B * kHid); A(&h->dZ3t, B * kHid); A(&h->dZ2, B * kHid);
   A(&h->dZ2t, B * kHid); A(&h->dZ1t, B * kHid); A(&h->Z1, B * kHid); A(&h->Z2, B * kHid); A(&h->yb, B);
   A(&h->dOut, B); A(&h->sqErr, B); A(&h->out, B); A(&h->part1, (int64_t)kSplitK * kHid * kIn);
   A(&h->part2, (int64_t)kSplitK * kHid * kHid); A(&h->part3, (int64_t)kSplitK * kHid * kHid); A(&h->err, 1);
