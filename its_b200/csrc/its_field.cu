@@ -333,170 +333,326 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
 // values: g + w X (the owner node's corner bit is 0 on that axis) or (g + w (X - 1)) + w (the
 // bit is 1; SVO.cu:573-576 forms corners from the owner's origin). So the hat factor of a
 // point and a corner along an axis is one of two values that depend only on the point's
-// coordinate on that axis, the corner's lattice coordinate and that bit. Per brick and depth
-// the kernel tabulates them (the reference's hat arithmetic, quotients by divRn) for the
-// brick's x, y and z coordinates, and stages each corner of the brick's cell box as its
-// coefficient and a flag byte (present, the three corner bits). A point then sums, for
-// d = 0..D-1 and k = x|y<<1|z<<2, lambda * ((hx * hy) * hz) over its present corners with
-// positive factors -- fieldAt's additions in fieldAt's order, so the field is bit-identical,
-// at a few table reads and four FP64 operations per term.
+// coordinate on that axis, the corner's lattice coordinate and that bit. kSepTables forms
+// them once per grid coordinate and depth (the reference's hat arithmetic, quotients by
+// divRn); each block copies its brick's slices and stages each corner of the brick's cell box
+// at every depth as its coefficient and a flag byte (present, the three corner bits). A point
+// then sums, for d = 0..D-1 and k = x|y<<1|z<<2, lambda * ((hx * hy) * hz) over its present
+// corners -- fieldAt's additions in fieldAt's order, so the field is bit-identical, at a few
+// table reads and three FP64 operations per term (the x*y factor is shared by a column's
+// points where they lie in one cell).
 constexpr int kSepX = 32, kSepY = 8, kSepThreads = kSepX * kSepY, kSepTileCap = 1024, kSepStageCap = 2048;
+template <typename T> struct Pair { typedef double2 type; };
+template <> struct Pair<float> { typedef float2 type; };
 
-// T = float is the precision form's FP32 field: the same tables (formed in FP64, rounded once)
-// and the same terms, summed in FP32.
-template <typename T, int kSepZ>  // points per thread along z (the brick's depth)
-__global__ void __launch_bounds__(kSepThreads) kEvalGridSep(const __grid_constant__ EvalParams P,
-                                                            const double* __restrict__ lambda, double3 o, double3 vs,
-                                                            int R, T* __restrict__ field) {
-  // hat tables and cells of the brick's coordinates for every depth ([corner side * 2 + corner
-  // bit]), and the corner boxes of every depth, staged together in one pass (their lattice
-  // lookups are dependent loads: in one pass their latencies overlap)
-  __shared__ T hX[kMaxDepth][kSepX][4], hY[kMaxDepth][kSepY][4], hZ[kMaxDepth][kSepZ][4];
-  __shared__ int cX[kMaxDepth][kSepX], cY[kMaxDepth][kSepY], cZ[kMaxDepth][kSepZ];
-  __shared__ T tLam[kSepStageCap];
-  __shared__ unsigned char tFlag[kSepStageCap];
-  __shared__ int tOff[kMaxDepth], tEnd[kMaxDepth];  // depth d's tile: [tOff[d], tEnd[d]); tOff -1: per-point
-  __shared__ int tAny[kMaxDepth], tTotal;
-  const int64_t M = (int64_t)R + 1;
-  const int tid = threadIdx.x, tx = tid % kSepX, ty = tid / kSepX;
-  const int64_t x0 = (int64_t)blockIdx.x * kSepX, y0 = (int64_t)blockIdx.y * kSepY, z0 = (int64_t)blockIdx.z * kSepZ;
-  const int64_t xi = x0 + tx, yj = y0 + ty;
-  const bool inXY = xi < M && yj < M;
-  const int D = P.depth;
-  constexpr int kCoords = kSepX + kSepY + kSepZ;
-  for (int item = tid; item < kCoords * D; item += kSepThreads) {
-    const int d = item / kCoords, j = item % kCoords;
-    const double w = P.w0 * (double)(1u << d), wi = P.winv[d];
-    const int a = j < kSepX ? 0 : (j < kSepX + kSepY ? 1 : 2);
-    const int k = a == 0 ? j : (a == 1 ? j - kSepX : j - kSepX - kSepY);
-    int64_t idx = (a == 0 ? x0 : a == 1 ? y0 : z0) + k;
-    if (idx > M - 1) idx = M - 1;  // clamped to the grid
-    const double oa = a == 0 ? o.x : a == 1 ? o.y : o.z, va = a == 0 ? vs.x : a == 1 ? vs.y : vs.z;
-    const double ga = a == 0 ? P.g.x : a == 1 ? P.g.y : P.g.z;
-    const double pa = oa + (double)idx * va;
-    const int64_t c = (int64_t)floor(divRn(pa - ga, w, wi));
-    double h[4];
+// The hat tables of every lattice coordinate of the grid, once per depth and axis (a grid of
+// (R+1)^3 points has only 3 (R+1) coordinates per depth, which every brick would otherwise
+// form again): tabC the coordinate's cell c = floor((p - g) / w), tabH its factors
+// [corner side * 2 + corner bit] against the corner at c + side, whose position is g + w X for
+// an owner bit 0 and (g + w (X - 1)) + w for an owner bit 1. Entry ((d * 3 + axis) * M + i).
+__global__ void kSepTables(const __grid_constant__ EvalParams P, double3 o, double3 vs, int64_t M,
+                           double* __restrict__ tabH, int* __restrict__ tabC) {
+  const int64_t item = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (item >= (int64_t)P.depth * 3 * M) return;
+  const int d = (int)(item / (3 * M)), a = (int)((item / M) % 3);
+  const int64_t idx = item % M;
+  const double w = P.w0 * (double)(1u << d), wi = P.winv[d];
+  const double oa = a == 0 ? o.x : a == 1 ? o.y : o.z, va = a == 0 ? vs.x : a == 1 ? vs.y : vs.z;
+  const double ga = a == 0 ? P.g.x : a == 1 ? P.g.y : P.g.z;
+  const double pa = oa + (double)idx * va;
+  const int64_t c = (int64_t)floor(divRn(pa - ga, w, wi));
+  double h[4];
 #pragma unroll
-    for (int side = 0; side < 2; ++side) {
-      const int64_t X = c + side;
-      const double pA = latticePos(ga, w, (uint32_t)(X < 0 ? 0 : X));
-      const double pB = X >= 1 ? latticePos(ga, w, (uint32_t)(X - 1)) + w : pA;
-      h[2 * side] = hat1r(pa, pA, w, wi);
-      h[2 * side + 1] = hat1r(pa, pB, w, wi);
-    }
-    T* dst = a == 0 ? hX[d][k] : (a == 1 ? hY[d][k] : hZ[d][k]);
-#pragma unroll
-    for (int e = 0; e < 4; ++e) dst[e] = (T)h[e];
-    (a == 0 ? cX[d] : a == 1 ? cY[d] : cZ[d])[k] = (int)c;
+  for (int side = 0; side < 2; ++side) {
+    const int64_t X = c + side;
+    const double pA = latticePos(ga, w, (uint32_t)(X < 0 ? 0 : X));
+    const double pB = X >= 1 ? latticePos(ga, w, (uint32_t)(X - 1)) + w : pA;
+    h[2 * side] = hat1r(pa, pA, w, wi);
+    h[2 * side + 1] = hat1r(pa, pB, w, wi);
   }
-  __syncthreads();
-  auto boxOf = [&](int d, int& nx, int& ny, int& nz) {
+  double2* dst = (double2*)(tabH + 4 * item);
+  dst[0] = make_double2(h[0], h[1]);
+  dst[1] = make_double2(h[2], h[3]);
+  tabC[item] = (int)c;
+}
+
+// One brick's hat tables and cell boxes: the hat factors and cells of the brick's coordinates
+// for every depth ([corner side * 2 + corner bit]; hZ is [depth][that index][point], so a
+// corner's factors for a thread's points lie side by side and come in pairs), and the corner
+// boxes of every depth staged together in one pass (their lattice lookups are dependent loads:
+// in one pass their latencies overlap).
+template <typename T, int kSepZ>
+struct alignas(16) SepStage {
+  T hX[kMaxDepth][4][kSepX];  // [depth][corner side * 2 + corner bit][x]: a warp's x run reads side by side
+  T hY[kMaxDepth][kSepY][4];
+  T hZ[kMaxDepth][4][kSepZ];
+  T tLam[kSepStageCap];
+  int cX[kMaxDepth][kSepX], cY[kMaxDepth][kSepY], cZ[kMaxDepth][kSepZ];
+  int tOff[kMaxDepth], tEnd[kMaxDepth];  // depth d's tile: [tOff[d], tEnd[d]); tOff -1: per-point
+  int cOff[kMaxDepth], cEnd[kMaxDepth];  // its (x, y) columns: [cOff[d], cEnd[d])
+  int bny[kMaxDepth], bnz[kMaxDepth];  // the box's corners along y and z
+  int tAny[kMaxDepth], tCols;
+  unsigned char tFlag[kSepStageCap];
+  __device__ int boxOf(int d, int& nx, int& ny, int& nz) const {
     nx = cX[d][kSepX - 1] - cX[d][0] + 2;
     ny = cY[d][kSepY - 1] - cY[d][0] + 2;
     nz = cZ[d][kSepZ - 1] - cZ[d][0] + 2;
     return nx * ny * nz;
-  };
-  if (tid == 0) {  // where each depth's box goes (a box over the capacity: per-point lookups)
-    int off = 0;
-    for (int d = 0; d < D; ++d) {
-      int nx, ny, nz;
-      const int n = boxOf(d, nx, ny, nz);
-      const bool fits = n <= kSepTileCap && off + n <= kSepStageCap;
-      tOff[d] = fits ? off : -1;
-      if (fits) off += n;
-      tEnd[d] = off;
-      tAny[d] = 0;
-    }
-    tTotal = off;
   }
-  __syncthreads();
-  // the corners of every depth's cell box: coefficient and flag byte (bit 0 present, bits 1-3
-  // the owner corner bits); tAny[d]: whether depth d has any
-  for (int e = tid; e < tTotal; e += kSepThreads) {
+};
+
+// The brick's slices of kSepTables' tables (threads i = 0, n, 2n, ... of the calling group).
+template <typename T, int kSepZ>
+__device__ void sepTables(SepStage<T, kSepZ>& S, int D, int64_t M, int64_t x0, int64_t y0, int64_t z0,
+                          const double* __restrict__ tabH, const int* __restrict__ tabC, int i, int n) {
+  constexpr int kCoords = kSepX + kSepY + kSepZ, kBatch = 4;  // a thread's items in batches, loads first
+  const int total = kCoords * D;
+  for (int item0 = i; item0 < total; item0 += kBatch * n) {
+    double2 h01[kBatch], h23[kBatch];
+    int c[kBatch];
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      const int item = item0 + u * n;
+      if (item >= total) break;
+      const int d = item / kCoords, j = item % kCoords;
+      const int a = j < kSepX ? 0 : (j < kSepX + kSepY ? 1 : 2);
+      const int k = a == 0 ? j : (a == 1 ? j - kSepX : j - kSepX - kSepY);
+      int64_t idx = (a == 0 ? x0 : a == 1 ? y0 : z0) + k;
+      if (idx > M - 1) idx = M - 1;  // clamped to the grid
+      const int64_t r = ((int64_t)d * 3 + a) * M + idx;
+      h01[u] = __ldg((const double2*)(tabH + 4 * r));
+      h23[u] = __ldg((const double2*)(tabH + 4 * r) + 1);
+      c[u] = __ldg(tabC + r);
+    }
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      const int item = item0 + u * n;
+      if (item >= total) break;
+      const int d = item / kCoords, j = item % kCoords;
+      const int a = j < kSepX ? 0 : (j < kSepX + kSepY ? 1 : 2);
+      const int k = a == 0 ? j : (a == 1 ? j - kSepX : j - kSepX - kSepY);
+      if (a == 2) {
+        S.hZ[d][0][k] = (T)h01[u].x;
+        S.hZ[d][1][k] = (T)h01[u].y;
+        S.hZ[d][2][k] = (T)h23[u].x;
+        S.hZ[d][3][k] = (T)h23[u].y;
+      } else if (a == 0) {
+        S.hX[d][0][k] = (T)h01[u].x;
+        S.hX[d][1][k] = (T)h01[u].y;
+        S.hX[d][2][k] = (T)h23[u].x;
+        S.hX[d][3][k] = (T)h23[u].y;
+      } else {
+        T* dst = S.hY[d][k];
+        dst[0] = (T)h01[u].x;
+        dst[1] = (T)h01[u].y;
+        dst[2] = (T)h23[u].x;
+        dst[3] = (T)h23[u].y;
+      }
+      (a == 0 ? S.cX[d] : a == 1 ? S.cY[d] : S.cZ[d])[k] = c[u];
+    }
+  }
+}
+
+// Where each depth's box goes (a box over the capacity: per-point lookups), by one warp: lane d
+// sizes depth d's box, then every lane runs the greedy placement in depth order on the
+// shuffled sizes (registers only) and lane d keeps depth d's place.
+template <typename T, int kSepZ>
+__device__ void sepPlace(SepStage<T, kSepZ>& S, int D, int lane) {
+  int n = 0, c = 0, ny = 0, nz = 0;
+  if (lane < D) {
+    int nx;
+    n = S.boxOf(lane, nx, ny, nz);
+    c = nx * ny;
+  }
+  int off = 0, cols = 0, myOff = -1, myCol = 0, myEnd = 0, myColEnd = 0;
+  for (int d = 0; d < D; ++d) {
+    const int nd = __shfl_sync(0xffffffffu, n, d), cd = __shfl_sync(0xffffffffu, c, d);
+    const bool fits = nd <= kSepTileCap && off + nd <= kSepStageCap;
+    if (lane == d) {
+      myOff = fits ? off : -1;
+      myCol = cols;
+    }
+    if (fits) {
+      off += (nd + 1) & ~1;  // boxes start at even entries: a column's z pairs are aligned
+      cols += cd;
+    }
+    if (lane == d) {
+      myEnd = off;
+      myColEnd = cols;
+    }
+  }
+  if (lane < D) {
+    S.tOff[lane] = myOff;
+    S.tEnd[lane] = myEnd;
+    S.cOff[lane] = myCol;
+    S.cEnd[lane] = myColEnd;
+    S.bny[lane] = ny;
+    S.bnz[lane] = nz;
+    S.tAny[lane] = 0;
+  }
+  if (lane == 0) S.tCols = cols;
+}
+
+// The corners of every depth's cell box: coefficient and flag byte (bit 0 present, bits 1-3
+// the owner corner bits); tAny[d]: whether depth d has any. A thread per (x, y) column of a
+// box, eight z entries at a time: their lattice indices are consecutive, so they lie in one or
+// two words of the lattice bits, and the loads of those words, then of the present corners'
+// coefficients and keys, go out together. The box entry (x, y, z) sits at (x ny + y) nz + z.
+template <typename T, int kSepZ>
+__device__ void sepStageBoxes(SepStage<T, kSepZ>& S, const EvalParams& P, const double* __restrict__ lambda, int i,
+                              int n) {
+  for (int e = i; e < S.tCols; e += n) {
+    // the columns lie in depth order (a depth without a tile: an empty range): e's depth is the
+    // number of depths whose columns end at or before it
     int d = 0;
-    while (e >= tEnd[d]) ++d;  // the tiles lie in depth order (a depth without one: an empty range)
-    int nx, ny, nz;
-    boxOf(d, nx, ny, nz);
-    const int t = e - tOff[d];
+#pragma unroll
+    for (int j = 0; j < kMaxDepth; ++j) d += (j < P.depth && e >= S.cEnd[j]) ? 1 : 0;
+    const int ny = S.bny[d], nz = S.bnz[d];
+    const int col = e - S.cOff[d], ix = col / ny, iy = col - ix * ny;
     const LatticeIndex& L = P.lat[d];
     const int64_t lim = (int64_t)(P.res >> d);
-    const int64_t Lx = cX[d][0] + t / (ny * nz), Ly = cY[d][0] + (t / nz) % ny, Lz = cZ[d][0] + t % nz;
-    unsigned char f = 0;
-    if (Lx >= 0 && Ly >= 0 && Lz >= 0 && Lx <= lim && Ly <= lim && Lz <= lim) {
-      const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
-      if (latticeHas(L, lin)) {
-        const uint32_t v = latticeRank(L, lin);
-        tLam[e] = (T)lambda[v];
-        f = (unsigned char)(1u | (((uint32_t)(P.vertKey[v] >> 37) & 7u) << 1));
-      }
-    }
-    tFlag[e] = f;
-    if (f) tAny[d] = 1;  // benign race: every writer stores 1
-  }
-  __syncthreads();
-  T sum[kSepZ];
-#pragma unroll
-  for (int q = 0; q < kSepZ; ++q) sum[q] = T(0);
-  for (int d = 0; d < D; ++d) {
-    const double w = P.w0 * (double)(1u << d), wi = P.winv[d];
-    int nx, ny, nz;
-    boxOf(d, nx, ny, nz);
-    if (tOff[d] < 0) {  // the box does not fit the tile: per-point lookups
-      if (inXY) {
-        const LatticeIndex& L = P.lat[d];
-        const int64_t lim = (int64_t)(P.res >> d);
-        const double px = o.x + (double)xi * vs.x, py = o.y + (double)yj * vs.y;
-#pragma unroll
-        for (int q = 0; q < kSepZ; ++q) {
-          const double pz = o.z + (double)(z0 + q) * vs.z;
-          const int64_t cx = cX[d][tx], cy = cY[d][ty], cz = cZ[d][q];
-          T s = sum[q];
-          for (int k = 0; k < 8; ++k) {
-            const int64_t Lx = cx + (k & 1), Ly = cy + ((k >> 1) & 1), Lz = cz + ((k >> 2) & 1);
-            if (Lx < 0 || Ly < 0 || Lz < 0 || Lx > lim || Ly > lim || Lz > lim) continue;
-            const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
-            if (!latticeHas(L, lin)) continue;
-            const uint32_t v = latticeRank(L, lin);
-            const double fx = hat1r(px, P.vertPos[3 * (int64_t)v], w, wi);
-            if (fx <= 0.0) continue;
-            const double fy = hat1r(py, P.vertPos[3 * (int64_t)v + 1], w, wi);
-            if (fy <= 0.0) continue;
-            const double fz = hat1r(pz, P.vertPos[3 * (int64_t)v + 2], w, wi);
-            if (fz <= 0.0) continue;
-            s += (T)lambda[v] * ((T)fx * (T)fy * (T)fz);
-          }
-          sum[q] = s;
+    const int64_t Lx = S.cX[d][0] + ix, Ly = S.cY[d][0] + iy;
+    const bool inBox = Lx >= 0 && Ly >= 0 && Lx <= lim && Ly <= lim;
+    const int64_t colBase = (Lx * L.M + Ly) * L.M;
+    bool any = false;
+    for (int z8 = 0; z8 < nz; z8 += 8) {
+      const int64_t zA = S.cZ[d][0] + z8;
+      const int64_t zLo = zA < 0 ? 0 : zA, zHi = min(min(zA + 7, (int64_t)S.cZ[d][0] + nz - 1), lim);
+      unsigned long long wLo = 0, wHi = 0;
+      uint32_t rLo = 0, rHi = 0, wIdx = 0;
+      const bool live = inBox && zLo <= zHi;
+      if (live) {
+        wIdx = (uint32_t)((colBase + zLo) >> 6);
+        const uint32_t wLast = (uint32_t)((colBase + zHi) >> 6);
+        wLo = L.bits[wIdx];
+        rLo = L.rank[wIdx];
+        if (wLast != wIdx) {
+          wHi = L.bits[wLast];
+          rHi = L.rank[wLast];
         }
       }
-    } else if (tAny[d] && inXY) {
-      const int rx = cX[d][tx] - cX[d][0], ry = cY[d][ty] - cY[d][0];
-      const T* hx = hX[d][tx];
-      const T* hy = hY[d][ty];
-      const T* lamT = tLam + tOff[d];
-      const unsigned char* flagT = tFlag + tOff[d];
+      uint32_t v[8];
+      unsigned hasMask = 0;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int64_t Lz = zA + j;
+        v[j] = 0;
+        if (live && Lz >= zLo && Lz <= zHi) {
+          const uint32_t lin = (uint32_t)(colBase + Lz);
+          const bool lo = (lin >> 6) == wIdx;
+          const unsigned long long word = lo ? wLo : wHi;
+          if ((word >> (lin & 63)) & 1ull) {  // latticeHas / latticeRank on the kept words
+            v[j] = L.base + (lo ? rLo : rHi) + (uint32_t)__popcll(word & ((1ull << (lin & 63)) - 1ull));
+            hasMask |= 1u << j;
+          }
+        }
+      }
+      double lv[8];
+      uint32_t keyHi[8];  // the key's upper word: the owner corner bits 37-39 are its bits 5-7
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        lv[j] = 0.0;
+        keyHi[j] = 0;
+        if (hasMask >> j & 1u) {
+          lv[j] = lambda[v[j]];
+          keyHi[j] = ((const uint32_t*)P.vertKey)[2 * (size_t)v[j] + 1];
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        if (z8 + j >= nz) break;
+        const int t = S.tOff[d] + col * nz + z8 + j;
+        unsigned char f = 0;
+        if (hasMask >> j & 1u) {
+          S.tLam[t] = (T)lv[j];
+          f = (unsigned char)(1u | (((keyHi[j] >> 5) & 7u) << 1));
+        }
+        S.tFlag[t] = f;
+      }
+      any |= hasMask != 0;
+    }
+    if (any) S.tAny[d] = 1;  // benign race: every writer stores 1
+  }
+}
+
+// The terms of one thread's column of kSepZ points (brick column tx, ty) over every depth, in
+// fieldAt's order: for d = 0..D-1 and k = x|y<<1|z<<2, lambda * ((hx * hy) * hz).
+template <typename T, int kSepZ>
+__device__ void sepTerms(const SepStage<T, kSepZ>& S, const EvalParams& P, const double* __restrict__ lambda,
+                         double3 o, double3 vs, int tx, int ty, int64_t xi, int64_t yj, int64_t z0, T (&sum)[kSepZ]) {
+#pragma unroll
+  for (int q = 0; q < kSepZ; ++q) sum[q] = T(0);
+  for (int d = 0; d < P.depth; ++d) {
+    const double w = P.w0 * (double)(1u << d), wi = P.winv[d];
+    const int ny = S.bny[d], nz = S.bnz[d];
+    if (S.tOff[d] < 0) {  // the box does not fit the tile: per-point lookups
+      const LatticeIndex& L = P.lat[d];
+      const int64_t lim = (int64_t)(P.res >> d);
+      const double px = o.x + (double)xi * vs.x, py = o.y + (double)yj * vs.y;
+#pragma unroll
+      for (int q = 0; q < kSepZ; ++q) {
+        const double pz = o.z + (double)(z0 + q) * vs.z;
+        const int64_t cx = S.cX[d][tx], cy = S.cY[d][ty], cz = S.cZ[d][q];
+        T s = sum[q];
+        for (int k = 0; k < 8; ++k) {
+          const int64_t Lx = cx + (k & 1), Ly = cy + ((k >> 1) & 1), Lz = cz + ((k >> 2) & 1);
+          if (Lx < 0 || Ly < 0 || Lz < 0 || Lx > lim || Ly > lim || Lz > lim) continue;
+          const uint32_t lin = (uint32_t)((Lx * L.M + Ly) * L.M + Lz);
+          if (!latticeHas(L, lin)) continue;
+          const uint32_t v = latticeRank(L, lin);
+          const double fx = hat1r(px, P.vertPos[3 * (int64_t)v], w, wi);
+          if (fx <= 0.0) continue;
+          const double fy = hat1r(py, P.vertPos[3 * (int64_t)v + 1], w, wi);
+          if (fy <= 0.0) continue;
+          const double fz = hat1r(pz, P.vertPos[3 * (int64_t)v + 2], w, wi);
+          if (fz <= 0.0) continue;
+          s += (T)lambda[v] * ((T)fx * (T)fy * (T)fz);
+        }
+        sum[q] = s;
+      }
+    } else if (S.tAny[d]) {
+      const int rx = S.cX[d][tx] - S.cX[d][0], ry = S.cY[d][ty] - S.cY[d][0];
+      const T* hx = &S.hX[d][0][tx];  // hx[kSepX * e]: factor e of the thread's x
+      const T* hy = S.hY[d][ty];
+      const T* lamT = S.tLam + S.tOff[d];
+      const unsigned char* flagT = S.tFlag + S.tOff[d];
       // A present corner adds lambda * ((hx * hy) * hz) even where a factor is 0: the term is
       // then +-0 (NaN for a non-finite coefficient), as fieldAt's sum over the corners adds it,
       // and a running sum that starts at +0 is never -0, so a +-0 term leaves it unchanged.
       if (nz == 2) {
         // Every point of the brick's z run lies in one cell (block-uniform): a corner is the
         // same vertex for all of the thread's points, so its coefficient, bits and x*y factor
-        // are read once and its terms cost two products and a sum per point.
+        // are read once and its terms cost two products and a sum per point. The four (x, y)
+        // corner columns' flag and coefficient pairs (z = 0, 1 side by side, at an even entry)
+        // are read up front.
+        typedef typename Pair<T>::type P2;
+        unsigned fp[4];
+        P2 lp[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const int t0 = ((rx + (c & 1)) * ny + (ry + (c >> 1))) * 2;
+          fp[c] = *(const unsigned short*)(flagT + t0);
+          lp[c] = *(const P2*)(lamT + t0);
+        }
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
           const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
-          const int t = ((rx + ox) * ny + (ry + oy)) * 2 + oz;
-          const unsigned f = flagT[t];
+          const unsigned f = (fp[k & 3] >> (8 * oz)) & 0xffu;
           if (!(f & 1u)) continue;
-          const T lam = lamT[t];
-          const T fxy = hx[2 * ox + ((f >> 1) & 1u)] * hy[2 * oy + ((f >> 2) & 1u)];
-          const int e = 2 * oz + (int)((f >> 3) & 1u);
+          const T lam = oz ? lp[k & 3].y : lp[k & 3].x;
+          const T fxy = hx[kSepX * (2 * ox + ((f >> 1) & 1u))] * hy[2 * oy + ((f >> 2) & 1u)];
+          const T* hz = S.hZ[d][2 * oz + (int)((f >> 3) & 1u)];
 #pragma unroll
-          for (int q = 0; q < kSepZ; ++q) sum[q] += lam * (fxy * hZ[d][q][e]);
+          for (int q = 0; q < kSepZ; q += 2) {
+            const typename Pair<T>::type h2 = *(const typename Pair<T>::type*)(hz + q);
+            sum[q] += lam * (fxy * h2.x);
+            sum[q + 1] += lam * (fxy * h2.y);
+          }
         }
       } else {
 #pragma unroll
         for (int q = 0; q < kSepZ; ++q) {
-          const int rz = cZ[d][q] - cZ[d][0];
+          const int rz = S.cZ[d][q] - S.cZ[d][0];
           T s = sum[q];
 #pragma unroll
           for (int k = 0; k < 8; ++k) {
@@ -504,9 +660,9 @@ __global__ void __launch_bounds__(kSepThreads) kEvalGridSep(const __grid_constan
             const int t = ((rx + ox) * ny + (ry + oy)) * nz + (rz + oz);
             const unsigned f = flagT[t];
             if (!(f & 1u)) continue;
-            const T fx = hx[2 * ox + ((f >> 1) & 1u)];
+            const T fx = hx[kSepX * (2 * ox + ((f >> 1) & 1u))];
             const T fy = hy[2 * oy + ((f >> 2) & 1u)];
-            const T fz = hZ[d][q][2 * oz + ((f >> 3) & 1u)];
+            const T fz = S.hZ[d][2 * oz + ((f >> 3) & 1u)][q];
             s += lamT[t] * (fx * fy * fz);
           }
           sum[q] = s;
@@ -514,7 +670,30 @@ __global__ void __launch_bounds__(kSepThreads) kEvalGridSep(const __grid_constan
       }
     }
   }
-  if (inXY) {
+}
+
+// T = float is the precision form's FP32 field: the same tables (formed in FP64, rounded once)
+// and the same terms, summed in FP32. One block per brick of kSepX x kSepY x kSepZ points.
+template <typename T, int kSepZ>  // points per thread along z (the brick's depth)
+__global__ void __launch_bounds__(kSepThreads, 4) kEvalGridSep(const __grid_constant__ EvalParams P,
+                                                            const double* __restrict__ lambda, double3 o, double3 vs,
+                                                            const double* __restrict__ tabH,
+                                                            const int* __restrict__ tabC, int R,
+                                                            T* __restrict__ field) {
+  __shared__ SepStage<T, kSepZ> S;
+  const int64_t M = (int64_t)R + 1;
+  const int tid = threadIdx.x, tx = tid % kSepX, ty = tid / kSepX;
+  const int64_t x0 = (int64_t)blockIdx.x * kSepX, y0 = (int64_t)blockIdx.y * kSepY, z0 = (int64_t)blockIdx.z * kSepZ;
+  const int64_t xi = x0 + tx, yj = y0 + ty;
+  sepTables(S, P.depth, M, x0, y0, z0, tabH, tabC, tid, kSepThreads);
+  __syncthreads();
+  if (tid < 32) sepPlace(S, P.depth, tid);
+  __syncthreads();
+  sepStageBoxes(S, P, lambda, tid, kSepThreads);
+  __syncthreads();
+  if (xi < M && yj < M) {
+    T sum[kSepZ];
+    sepTerms(S, P, lambda, o, vs, tx, ty, xi, yj, z0, sum);
 #pragma unroll
     for (int q = 0; q < kSepZ; ++q)
       if (z0 + q < M) field[xi + M * (yj + M * (z0 + q))] = sum[q];
@@ -717,6 +896,16 @@ static its_status evalGridTuned(its_ctx* ctx, const SvoDevice& d, const double* 
   if (sizeof(T) == 8 || !sepFits(4)) cand = {0, 1, 2, 3};
   if (sepFits(4)) cand.push_back(4);
   if (sepFits(8)) cand.push_back(5);
+  DevBuf<double> tabH;
+  DevBuf<int> tabC;
+  if (sepFits(4)) {  // the separable kernel's hat tables, formed once for all its launches here
+    const int64_t M = (int64_t)res + 1, n = (int64_t)d.depth * 3 * M;
+    its_status st = tabH.alloc(ctx, 4 * n);
+    if (st == ITS_OK) st = tabC.alloc(ctx, n);
+    if (st != ITS_OK) return st;
+    kSepTables<<<gridFor(n, 256), 256, 0, ctx->stream>>>(P, o, vs, M, tabH.p, tabC.p);
+    ITS_LAUNCHED(ctx);
+  }
   auto run = [&](int j) -> its_status {
     switch (cand[j]) {
       case 1: return launchBricks<T, 32, 8, 2>(ctx, P, lam, o, vs, res, field);
@@ -728,8 +917,10 @@ static its_status evalGridTuned(its_ctx* ctx, const SvoDevice& d, const double* 
         const int64_t M = (int64_t)res + 1;
         const dim3 grid((unsigned)((M + kSepX - 1) / kSepX), (unsigned)((M + kSepY - 1) / kSepY),
                         (unsigned)((M + z - 1) / z));
-        if (z == 8) kEvalGridSep<T, 8><<<grid, kSepThreads, 0, ctx->stream>>>(P, lam, o, vs, res, field);
-        else kEvalGridSep<T, 4><<<grid, kSepThreads, 0, ctx->stream>>>(P, lam, o, vs, res, field);
+        if (z == 8)
+          kEvalGridSep<T, 8><<<grid, kSepThreads, 0, ctx->stream>>>(P, lam, o, vs, tabH.p, tabC.p, res, field);
+        else
+          kEvalGridSep<T, 4><<<grid, kSepThreads, 0, ctx->stream>>>(P, lam, o, vs, tabH.p, tabC.p, res, field);
         ITS_LAUNCHED(ctx);
         return ITS_OK;
       }
