@@ -575,6 +575,28 @@ __device__ void sepStageBoxes(SepStage<T, kSepZ>& S, const EvalParams& P, const 
   }
 }
 
+// The terms of G consecutive points q0.. of a thread's column that lie in one cell (box-relative
+// z cell rz): each present corner's coefficient, bits and x*y factor are read once for them,
+// and each point adds lambda * ((hx * hy) * hz) in corner order. colT[c]: the box entry of the
+// (x, y) corner column c = x | y << 1 at z = 0.
+template <int G, typename T, int kSepZ>
+__device__ __forceinline__ void sepCellTerms(const SepStage<T, kSepZ>& S, int d, const T* hx, const T* hy,
+                                             const T* lamT, const unsigned char* flagT, const int (&colT)[4], int rz,
+                                             int q0, T (&sum)[kSepZ]) {
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int ox = k & 1, oy = (k >> 1) & 1, oz = k >> 2;
+    const int t = colT[k & 3] + rz + oz;
+    const unsigned f = flagT[t];
+    if (!(f & 1u)) continue;
+    const T lam = lamT[t];
+    const T fxy = hx[kSepX * (2 * ox + ((f >> 1) & 1u))] * hy[2 * oy + ((f >> 2) & 1u)];
+    const T* hz = S.hZ[d][2 * oz + ((f >> 3) & 1u)];
+#pragma unroll
+    for (int g = 0; g < G; ++g) sum[q0 + g] += lam * (fxy * hz[q0 + g]);
+  }
+}
+
 // The terms of one thread's column of kSepZ points (brick column tx, ty) over every depth, in
 // fieldAt's order: for d = 0..D-1 and k = x|y<<1|z<<2, lambda * ((hx * hy) * hz).
 template <typename T, int kSepZ>
@@ -650,22 +672,33 @@ __device__ void sepTerms(const SepStage<T, kSepZ>& S, const EvalParams& P, const
           }
         }
       } else {
+        // The thread's z run spans several cells (the finest depths): the points are taken in
+        // runs of four, two or one that lie in one cell (the runs are the same for the whole
+        // block), so a corner's reads and x*y factor serve every point of its run.
+        int colT[4];
 #pragma unroll
-        for (int q = 0; q < kSepZ; ++q) {
-          const int rz = S.cZ[d][q] - S.cZ[d][0];
-          T s = sum[q];
+        for (int c = 0; c < 4; ++c) colT[c] = ((rx + (c & 1)) * ny + (ry + (c >> 1))) * nz;
+        const int zc = S.cZ[d][0];
 #pragma unroll
-          for (int k = 0; k < 8; ++k) {
-            const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
-            const int t = ((rx + ox) * ny + (ry + oy)) * nz + (rz + oz);
-            const unsigned f = flagT[t];
-            if (!(f & 1u)) continue;
-            const T fx = hx[kSepX * (2 * ox + ((f >> 1) & 1u))];
-            const T fy = hy[2 * oy + ((f >> 2) & 1u)];
-            const T fz = S.hZ[d][2 * oz + ((f >> 3) & 1u)][q];
-            s += lamT[t] * (fx * fy * fz);
+        for (int q0 = 0; q0 < kSepZ; q0 += 4) {
+          const int ra = S.cZ[d][q0] - zc, rb = S.cZ[d][q0 + 1] - zc, rc = S.cZ[d][q0 + 2] - zc,
+                    rd = S.cZ[d][q0 + 3] - zc;
+          if (ra == rd) {
+            sepCellTerms<4>(S, d, hx, hy, lamT, flagT, colT, ra, q0, sum);
+          } else {
+            if (ra == rb) {
+              sepCellTerms<2>(S, d, hx, hy, lamT, flagT, colT, ra, q0, sum);
+            } else {
+              sepCellTerms<1>(S, d, hx, hy, lamT, flagT, colT, ra, q0, sum);
+              sepCellTerms<1>(S, d, hx, hy, lamT, flagT, colT, rb, q0 + 1, sum);
+            }
+            if (rc == rd) {
+              sepCellTerms<2>(S, d, hx, hy, lamT, flagT, colT, rc, q0 + 2, sum);
+            } else {
+              sepCellTerms<1>(S, d, hx, hy, lamT, flagT, colT, rc, q0 + 2, sum);
+              sepCellTerms<1>(S, d, hx, hy, lamT, flagT, colT, rd, q0 + 3, sum);
+            }
           }
-          sum[q] = s;
         }
       }
     }
