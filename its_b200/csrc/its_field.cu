@@ -510,20 +510,20 @@ __device__ void sepStageBoxes(SepStage<T, kSepZ>& S, const EvalParams& P, const 
     const int ny = S.bny[d], nz = S.bnz[d];
     const int col = e - S.cOff[d], ix = col / ny, iy = col - ix * ny;
     const LatticeIndex& L = P.lat[d];
-    const int64_t lim = (int64_t)(P.res >> d);
-    const int64_t Lx = S.cX[d][0] + ix, Ly = S.cY[d][0] + iy;
+    const int lim = P.res >> d;
+    const int Lx = S.cX[d][0] + ix, Ly = S.cY[d][0] + iy;
     const bool inBox = Lx >= 0 && Ly >= 0 && Lx <= lim && Ly <= lim;
-    const int64_t colBase = (Lx * L.M + Ly) * L.M;
+    const uint32_t colBase = inBox ? ((uint32_t)Lx * L.M + (uint32_t)Ly) * L.M : 0u;
     bool any = false;
     for (int z8 = 0; z8 < nz; z8 += 8) {
-      const int64_t zA = S.cZ[d][0] + z8;
-      const int64_t zLo = zA < 0 ? 0 : zA, zHi = min(min(zA + 7, (int64_t)S.cZ[d][0] + nz - 1), lim);
+      const int zA = S.cZ[d][0] + z8;
+      const int zLo = zA < 0 ? 0 : zA, zHi = min(min(zA + 7, S.cZ[d][0] + nz - 1), lim);
       unsigned long long wLo = 0, wHi = 0;
       uint32_t rLo = 0, rHi = 0, wIdx = 0;
       const bool live = inBox && zLo <= zHi;
       if (live) {
-        wIdx = (uint32_t)((colBase + zLo) >> 6);
-        const uint32_t wLast = (uint32_t)((colBase + zHi) >> 6);
+        wIdx = (colBase + (uint32_t)zLo) >> 6;
+        const uint32_t wLast = (colBase + (uint32_t)zHi) >> 6;
         wLo = L.bits[wIdx];
         rLo = L.rank[wIdx];
         if (wLast != wIdx) {
@@ -535,10 +535,10 @@ __device__ void sepStageBoxes(SepStage<T, kSepZ>& S, const EvalParams& P, const 
       unsigned hasMask = 0;
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
-        const int64_t Lz = zA + j;
+        const int Lz = zA + j;
         v[j] = 0;
         if (live && Lz >= zLo && Lz <= zHi) {
-          const uint32_t lin = (uint32_t)(colBase + Lz);
+          const uint32_t lin = colBase + (uint32_t)Lz;
           const bool lo = (lin >> 6) == wIdx;
           const unsigned long long word = lo ? wLo : wHi;
           if ((word >> (lin & 63)) & 1ull) {  // latticeHas / latticeRank on the kept words
