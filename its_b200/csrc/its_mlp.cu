@@ -89,7 +89,7 @@ __device__ __forceinline__ void cpAsyncWait() {
 }
 
 template <int N, class Epi>
-__global__ void __launch_bounds__(kGemmThreads, 1) kUmmaGemm(const bf16* __restrict__ A, int64_t lda, int64_t M,
+__global__ void __launch_bounds__(kGemmThreads, 2) kUmmaGemm(const bf16* __restrict__ A, int64_t lda, int64_t M,
                                                              const bf16* __restrict__ B, int64_t ldb, int64_t K,
                                                              int64_t kPerSplit, Epi epi, int* __restrict__ err) {
   using namespace umma;
@@ -221,8 +221,52 @@ __device__ __forceinline__ void storeT(const bf16* sT, bf16* dstT, int64_t ldt, 
   }
 }
 
+// A row-major 128-row tile goes through shared memory too: each thread stages its row's 16-byte
+// pieces (piece c of row r at slot c ^ (r mod pieces per row): no bank conflicts either way),
+// then consecutive threads write consecutive pieces of whole rows, or, for loadRows, read them.
+template <int RowBytes>
+__device__ __forceinline__ void stageRow(uint8_t* sR, int row, int byteCol, const uint4& v) {
+  constexpr int kPieces = RowBytes / 16;
+  *(uint4*)(sR + row * RowBytes + (((byteCol >> 4) ^ (row % kPieces)) << 4)) = v;
+}
+template <int RowBytes>
+__device__ __forceinline__ uint4 rowPiece(const uint8_t* sR, int row, int byteCol) {
+  constexpr int kPieces = RowBytes / 16;
+  return *(const uint4*)(sR + row * RowBytes + (((byteCol >> 4) ^ (row % kPieces)) << 4));
+}
+template <int RowBytes>
+__device__ __forceinline__ void storeRows(const uint8_t* sR, void* dst, int64_t m0, int64_t M) {
+  constexpr int kPieces = RowBytes / 16;
+  for (int p = threadIdx.x; p < 128 * kPieces; p += blockDim.x) {
+    const int row = p / kPieces, c = p % kPieces;
+    if (m0 + row < M)
+      *(uint4*)((uint8_t*)dst + (m0 + row) * RowBytes + c * 16) = rowPiece<RowBytes>(sR, row, c * 16);
+  }
+}
+template <int RowBytes, int kThreads>  // a thread's loads go out four at a time before their shared stores
+__device__ __forceinline__ void loadRows(uint8_t* sR, const void* src, int64_t m0, int64_t M) {
+  constexpr int kPieces = RowBytes / 16, kPer = 128 * kPieces / kThreads, kBatch = 4;
+  static_assert(kPer * kThreads == 128 * kPieces && kPer % kBatch == 0, "whole batches of pieces per thread");
+#pragma unroll
+  for (int i0 = 0; i0 < kPer; i0 += kBatch) {
+    uint4 q[kBatch];
+#pragma unroll
+    for (int i = 0; i < kBatch; ++i) {
+      const int p = threadIdx.x + (i0 + i) * kThreads, row = p / kPieces, c = p % kPieces;
+      q[i] = m0 + row < M ? *(const uint4*)((const uint8_t*)src + (m0 + row) * RowBytes + c * 16)
+                          : make_uint4(0, 0, 0, 0);
+    }
+#pragma unroll
+    for (int i = 0; i < kBatch; ++i) {
+      const int p = threadIdx.x + (i0 + i) * kThreads;
+      stageRow<RowBytes>(sR, p / kPieces, (p % kPieces) * 16, q[i]);
+    }
+  }
+}
+
 // Hidden layer: z = acc + b, h = gelu(z); Z (FP32, for the backward pass), H row-major and
-// its transpose (the operands of the next layer and of the weight gradient).
+// its transpose (the operands of the next layer and of the weight gradient). Ht and H go out
+// through the two halves of the stage area, then Z through all of it.
 struct EpiHidden {
   const float* bias;
   float* Z;
@@ -233,28 +277,37 @@ struct EpiHidden {
   __device__ void operator()(int64_t m, bool valid, int j0, float (&v)[C], float*, float*, int, uint8_t* stage,
                              int64_t m0, int64_t M) const {
     bf16* sT = (bf16*)stage;
+    uint8_t* sH = stage + kHid * 128 * 2;  // the second half: H row-major
+    const int row = threadIdx.x & 127;
     if (valid) {
 #pragma unroll
       for (int jb = 0; jb < C; jb += 8) {
         const int j = j0 + jb;
-        float z[8], h[8];
+        float h[8];
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
-          z[e] = v[jb + e] + bias[j + e];
-          h[e] = geluF(z[e]);
-        }
-        if (Z) {
-          *(float4*)(Z + m * kHid + j) = make_float4(z[0], z[1], z[2], z[3]);
-          *(float4*)(Z + m * kHid + j + 4) = make_float4(z[4], z[5], z[6], z[7]);
+          v[jb + e] += bias[j + e];  // z, kept for Z
+          h[e] = geluF(v[jb + e]);
         }
         const uint4 hb = packBf16x8(h);
-        *(uint4*)(H + m * kHid + j) = hb;
-        if (Ht) stageT(sT, threadIdx.x & 127, j, hb);
+        stageRow<kHid * 2>(sH, row, j * 2, hb);
+        if (Ht) stageT(sT, row, j, hb);
       }
     }
-    if (!Ht) return;
     __syncthreads();
-    storeT(sT, Ht, ldt, m0, M);
+    storeRows<kHid * 2>(sH, H, m0, M);
+    if (Ht) storeT(sT, Ht, ldt, m0, M);
+    if (!Z) return;
+    __syncthreads();
+    if (valid) {
+#pragma unroll
+      for (int jb = 0; jb < C; jb += 4)
+        stageRow<kHid * 4>(stage, row, (j0 + jb) * 4,
+                           make_uint4(__float_as_uint(v[jb]), __float_as_uint(v[jb + 1]), __float_as_uint(v[jb + 2]),
+                                      __float_as_uint(v[jb + 3])));
+    }
+    __syncthreads();
+    storeRows<kHid * 4>(stage, Z, m0, M);
   }
 };
 
@@ -322,7 +375,7 @@ struct EpiOutput {
     }
     __syncthreads();
     if (!y) return;
-    bf16* sT = (bf16*)stage;
+    bf16* sT = (bf16*)stage;  // dZt; dZ row-major in the second half (H3t's copy is out)
     if (valid) {
       const float d = sRow[row];
 #pragma unroll
@@ -332,11 +385,12 @@ struct EpiOutput {
 #pragma unroll
         for (int k = 0; k < 8; ++k) g[k] = d * w4[j + k] * geluGrad(v[jb + k]);
         const uint4 gb = packBf16x8(g);
-        *(uint4*)(dZ + m * kHid + j) = gb;
+        stageRow<kHid * 2>((uint8_t*)sT3, row, j * 2, gb);
         stageT(sT, row, j, gb);
       }
     }
     __syncthreads();
+    storeRows<kHid * 2>((const uint8_t*)sT3, dZ, m0, M);
     storeT(sT, dZt, ldt, m0, M);
   }
 };
@@ -350,22 +404,35 @@ struct EpiBack {
   template <int C>
   __device__ void operator()(int64_t m, bool valid, int j0, float (&v)[C], float*, float*, int, uint8_t* stage,
                              int64_t m0, int64_t M) const {
+    // Z's tile comes in through all of the stage area (whole rows per warp), then dZt and dZ go
+    // out through its two halves
     bf16* sT = (bf16*)stage;
+    uint8_t* sD = stage + kHid * 128 * 2;
+    const int row = threadIdx.x & 127;
+    loadRows<kHid * 4, kGemmThreads>(stage, Z, m0, M);
+    __syncthreads();
+    if (valid) {  // dZ in place of the accumulators
+#pragma unroll
+      for (int jb = 0; jb < C; jb += 4) {
+        const uint4 zq = rowPiece<kHid * 4>(stage, row, (j0 + jb) * 4);
+        v[jb] *= geluGrad(__uint_as_float(zq.x));
+        v[jb + 1] *= geluGrad(__uint_as_float(zq.y));
+        v[jb + 2] *= geluGrad(__uint_as_float(zq.z));
+        v[jb + 3] *= geluGrad(__uint_as_float(zq.w));
+      }
+    }
+    __syncthreads();
     if (valid) {
 #pragma unroll
       for (int jb = 0; jb < C; jb += 8) {
         const int j = j0 + jb;
-        const float4 z0 = *(const float4*)(Z + m * kHid + j), z1 = *(const float4*)(Z + m * kHid + j + 4);
-        const float z[8] = {z0.x, z0.y, z0.z, z0.w, z1.x, z1.y, z1.z, z1.w};
-        float g[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) g[k] = v[jb + k] * geluGrad(z[k]);
-        const uint4 gb = packBf16x8(g);
-        if (dZ) *(uint4*)(dZ + m * kHid + j) = gb;
-        stageT(sT, threadIdx.x & 127, j, gb);
+        const uint4 gb = packBf16x8(v + jb);
+        if (dZ) stageRow<kHid * 2>(sD, row, j * 2, gb);
+        stageT(sT, row, j, gb);
       }
     }
     __syncthreads();
+    if (dZ) storeRows<kHid * 2>(sD, dZ, m0, M);
     storeT(sT, dZt, ldt, m0, M);
   }
 };
