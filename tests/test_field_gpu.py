@@ -210,6 +210,47 @@ def test_autotuner_changes_speed_not_bits(tmp_path):
 
 
 @pytest.mark.gpu
+def test_every_tuned_candidate_computes_the_same_bits(tmp_path):
+    # Each launch shape the autotuner may pick -- the four brick shapes and the two separable
+    # depths of the FP64 field, the two separable depths of the FP32 field, the three
+    # marching-cubes tiles -- forced through the cache file in turn, gives the defaults' bits.
+    from its_b200 import Context, Svo
+    V, F, o, w = prepared_mesh("c0")
+    R = 80
+
+    def run(cache=None):
+        ctx = Context(0)
+        if cache:
+            ctx.set_autotune(True, cache)
+        svo = Svo(ctx, V, F, 32, o, w)
+        b = ctx.signed_distance(svo.vertices()[0], V, F)
+        lam = svo.exact_start(b)
+        field = svo.eval_grid(lam, o, w, R)
+        field32 = svo.eval_grid_f32(lam, o, w, R)
+        cube, tri, n = ctx.marching_cubes(field, R, o, w, float(np.median(b)))
+        out = (field, field32, cube, tri, svo.depth, ctx.autotune_choices())
+        ctx.close()
+        return out
+
+    ref = run()
+    depth = ref[4]
+    for k in range(6):
+        cache = str(tmp_path / ("tune%d.txt" % k))
+        with open(cache, "w") as f:
+            f.write("eval_grid/f64/grid=%d/octree=32/depth=%d %d\n" % (R, depth, k))
+            f.write("eval_grid/f32/grid=%d/octree=32/depth=%d %d\n" % (R, depth, k % 2))
+            f.write("marching_cubes/f64/res=%d/cases %d\n" % (R, k % 3))
+            f.write("marching_cubes/f64/res=%d/soup %d\n" % (R, k % 3))
+        got = run(cache)
+        assert got[5]["eval_grid/f64/grid=%d/octree=32/depth=%d" % (R, depth)] == k
+        assert got[5]["eval_grid/f32/grid=%d/octree=32/depth=%d" % (R, depth)] == k % 2
+        assert got[5]["marching_cubes/f64/res=%d/cases" % R] == got[5]["marching_cubes/f64/res=%d/soup" % R] == k % 3
+        assert np.array_equal(got[0], ref[0]), "FP64 field, candidate %d" % k
+        assert np.array_equal(got[1], ref[1]), "FP32 field, candidate %d" % (k % 2)
+        assert np.array_equal(got[2], ref[2]) and np.array_equal(got[3], ref[3]), "marching cubes, tile %d" % (k % 3)
+
+
+@pytest.mark.gpu
 def test_point_value_gradient_matches_oracle(ctx):
     from its_b200 import Operator, Svo, uniform_bbox
     V, F, o, w = prepared_mesh("c0")
