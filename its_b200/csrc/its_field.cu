@@ -1268,7 +1268,7 @@ its_status marchingCubesT(its_ctx* ctx, const FT* field, int res, const double o
   const int itemsOf[3] = {8, 16, 4};
   const int64_t nbMax = (nvox + kScanThreads * 4 - 1) / (kScanThreads * 4);
   DevBuf<unsigned long long> sums, tot;
-  if ((st = sums.alloc(ctx, nbMax)) != ITS_OK || (st = tot.alloc(ctx, 1)) != ITS_OK) return st;
+  if ((st = sums.alloc(ctx, nbMax + spineTops(nbMax))) != ITS_OK || (st = tot.alloc(ctx, 1)) != ITS_OK) return st;
   const double3 o3 = make_double3(origin[0], origin[1], origin[2]);
   const double3 v3 = make_double3(width[0] / res, width[1] / res, width[2] / res);
   auto run = [&](int i) -> its_status {
@@ -1283,8 +1283,7 @@ its_status marchingCubesT(its_ctx* ctx, const FT* field, int res, const double o
     else
       kMcClassify<FT, 8><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(F.d, res, iso, cubeD, sums.p);
     ITS_LAUNCHED(ctx);
-    kScanSpine<unsigned long long><<<1, kScanThreads, 0, ctx->stream>>>(sums.p, nb, tot.p);
-    ITS_LAUNCHED(ctx);
+    if ((st = scanSpine<unsigned long long>(ctx, sums.p, nb, tot.p, sums.p + nbMax)) != ITS_OK) return st;
     if (T.d) {
       const unsigned long long cap = (unsigned long long)capacity;
       if (items == 16)

@@ -91,6 +91,41 @@ __global__ void kScanSpine(T* blockSums, int64_t nb, T* total) {
   if (threadIdx.x == 0 && total) *total = tot;
 }
 
+// The spine above kSpineOneBlock block sums, in three launches: tiles of kSpineTile sums
+// scanned in place by a block each (eight consecutive sums per thread) with each tile's total
+// in tops; the totals scanned by kScanSpine (one block); each tile's offset added.
+constexpr int64_t kSpineOneBlock = 8192;
+constexpr int kSpineTile = kScanThreads * 8;
+inline int64_t spineTops(int64_t nb) { return nb > kSpineOneBlock ? (nb + kSpineTile - 1) / kSpineTile : 0; }
+template <typename T>
+__global__ void __launch_bounds__(kScanThreads) kSpineTiles(T* __restrict__ sums, int64_t nb, T* __restrict__ tops) {
+  const int64_t i0 = (int64_t)blockIdx.x * kSpineTile + (int64_t)threadIdx.x * 8;
+  T v[8];
+  T s = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    v[k] = i0 + k < nb ? sums[i0 + k] : T(0);
+    s += v[k];
+  }
+  T tot;
+  T run = blockExclusiveScan<T>(s, tot);
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    if (i0 + k < nb) {
+      sums[i0 + k] = run;
+      run += v[k];
+    }
+  if (threadIdx.x == 0) tops[blockIdx.x] = tot;
+}
+template <typename T>
+__global__ void __launch_bounds__(kScanThreads) kSpineAdd(T* __restrict__ sums, int64_t nb,
+                                                         const T* __restrict__ tops) {
+  const T add = tops[blockIdx.x];
+  const int64_t i0 = (int64_t)blockIdx.x * kSpineTile;
+  for (int k = threadIdx.x; k < kSpineTile; k += kScanThreads)
+    if (i0 + k < nb) sums[i0 + k] += add;
+}
+
 template <typename T, typename F, typename W>
 __global__ void kScanDownsweep(F f, int64_t n, const T* blockOffsets, W write) {
   const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
@@ -118,10 +153,33 @@ struct StorePrefix {
   __device__ void operator()(int64_t i, T prefix, T) const { out[i] = prefix; }
 };
 
+// The spine: nb block sums scanned in place (exclusive), their total to *total (may be NULL);
+// above kSpineOneBlock sums tops holds spineTops(nb) elements of scratch.
+template <typename T>
+its_status scanSpine(its_ctx* ctx, T* sums, int64_t nb, T* total, T* tops) {
+  if (nb <= kSpineOneBlock) {
+    kScanSpine<T><<<1, kScanThreads, 0, ctx->stream>>>(sums, nb, total);
+    ITS_LAUNCHED(ctx);
+    return ITS_OK;
+  }
+  const int64_t nt = spineTops(nb);
+  kSpineTiles<T><<<(unsigned)nt, kScanThreads, 0, ctx->stream>>>(sums, nb, tops);
+  ITS_LAUNCHED(ctx);
+  kScanSpine<T><<<1, kScanThreads, 0, ctx->stream>>>(tops, nt, total);
+  ITS_LAUNCHED(ctx);
+  kSpineAdd<T><<<(unsigned)nt, kScanThreads, 0, ctx->stream>>>(sums, nb, tops);
+  ITS_LAUNCHED(ctx);
+  return ITS_OK;
+}
+
 // Exclusive scan of f(0..n-1); write(i, prefix, value) receives each element's prefix.
 // The total lands in *dTotal (device memory, may be NULL). scratch must hold
-// scanScratchSize(n) elements of T.
+// scanScratchSize(n) elements of T (the block sums, then the spine's tile totals).
 inline int64_t scanBlocks(int64_t n) { return (n + kScanTile - 1) / kScanTile; }
+inline int64_t scanScratchSize(int64_t n) {
+  const int64_t nb = scanBlocks(n > 0 ? n : 1);
+  return nb + spineTops(nb);
+}
 template <typename T, typename F, typename W>
 its_status scanExclusive(its_ctx* ctx, F f, int64_t n, W write, T* dTotal, T* scratch) {
   if (n <= 0) {
@@ -131,8 +189,8 @@ its_status scanExclusive(its_ctx* ctx, F f, int64_t n, W write, T* dTotal, T* sc
   const int64_t nb = scanBlocks(n);
   kScanUpsweep<T, F><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(f, n, scratch);
   ITS_LAUNCHED(ctx);
-  kScanSpine<T><<<1, kScanThreads, 0, ctx->stream>>>(scratch, nb, dTotal);
-  ITS_LAUNCHED(ctx);
+  its_status st = scanSpine<T>(ctx, scratch, nb, dTotal, scratch + nb);
+  if (st != ITS_OK) return st;
   kScanDownsweep<T, F, W><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(f, n, scratch, write);
   ITS_LAUNCHED(ctx);
   return ITS_OK;
@@ -141,7 +199,7 @@ its_status scanExclusive(its_ctx* ctx, F f, int64_t n, W write, T* dTotal, T* sc
 template <typename T, typename F, typename W>
 its_status scanExclusiveAlloc(its_ctx* ctx, F f, int64_t n, W write, T* dTotal) {
   DevBuf<T> spine;
-  its_status s = spine.alloc(ctx, (size_t)(scanBlocks(n > 0 ? n : 1)));
+  its_status s = spine.alloc(ctx, (size_t)scanScratchSize(n));
   if (s != ITS_OK) return s;
   return scanExclusive<T>(ctx, f, n, write, dTotal, spine.p);
 }

@@ -189,7 +189,7 @@ its_status radixSortPairs(its_ctx* ctx, const uint32_t* keys, const uint32_t* va
   its_status st;
   DevBuf<uint32_t> hist, spine;
   if ((st = hist.alloc(ctx, 256 * nb)) != ITS_OK) return st;
-  if ((st = spine.alloc(ctx, scanBlocks(256 * nb))) != ITS_OK) return st;
+  if ((st = spine.alloc(ctx, scanScratchSize(256 * nb))) != ITS_OK) return st;
   const uint32_t* sk = keys;
   const uint32_t* sv = vals;
   for (int p = 0; p < passes; ++p) {
