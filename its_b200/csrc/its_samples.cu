@@ -291,12 +291,21 @@ struct FaceEmit {
   }
 };
 
-// The hit count of every item, evaluated once and stored; the compaction's two scans read the
-// stored counts and the emitting pass re-runs the hit test only for items that have hits.
+// The hit count of every item, evaluated once and stored; the scan of the stored counts writes
+// each item's offset, and the emitting pass re-runs the hit test, one thread per item, only for
+// items that have hits, writing them at that offset.
 template <class Step>
 __global__ void __launch_bounds__(128) kCountHits(Step f, int64_t n, uint32_t* __restrict__ cnt) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) cnt[i] = f(i);
+}
+template <class Emit>
+__global__ void __launch_bounds__(128) kEmitHits(Emit e, int64_t n, const uint32_t* __restrict__ cnt,
+                                                 const uint32_t* __restrict__ off) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t c = cnt[i];
+  if (c) e(i, off[i], c);
 }
 struct StoredCount {
   const uint32_t* cnt;
@@ -353,19 +362,23 @@ its_status its_shell_samples(its_svo* s, const double* verts, int64_t nverts, co
   kEdgeInsert<<<gridFor(slots, 256), 256, 0, ctx->stream>>>(F.d, slots, ekeys.p, eown.p, tsz - 1);
   ITS_LAUNCHED(ctx);
   EdgeStep es{S, V.d, F.d, ekeys.p, eown.p, tsz - 1};
-  DevBuf<uint32_t> tot, ecnt;
-  if ((st = tot.zeros(ctx, 3)) != ITS_OK || (st = ecnt.alloc(ctx, slots)) != ITS_OK) return st;
+  DevBuf<uint32_t> tot, ecnt, eoff;
+  if ((st = tot.zeros(ctx, 3)) != ITS_OK || (st = ecnt.alloc(ctx, slots)) != ITS_OK ||
+      (st = eoff.alloc(ctx, slots)) != ITS_OK)
+    return st;
   kCountHits<<<gridFor(slots, 128), 128, 0, ctx->stream>>>(es, slots, ecnt.p);
   ITS_LAUNCHED(ctx);
-  auto nowrite = [] __device__(int64_t, uint32_t, uint32_t) {};
-  if ((st = scanExclusiveAlloc<uint32_t>(ctx, StoredCount{ecnt.p}, slots, nowrite, tot.p)) != ITS_OK) return st;
+  if ((st = scanExclusiveAlloc<uint32_t>(ctx, StoredCount{ecnt.p}, slots, StorePrefix<uint32_t>{eoff.p}, tot.p)) !=
+      ITS_OK)
+    return st;
   uint32_t nRaw = 0;
   if ((st = readScalar(ctx, tot.p, &nRaw)) != ITS_OK) return st;
   DevBuf<double> raw;
   if ((st = raw.alloc(ctx, 3 * (size_t)(nRaw ? nRaw : 1))) != ITS_OK) return st;
-  if ((st = scanExclusiveAlloc<uint32_t>(ctx, StoredCount{ecnt.p}, slots, EdgeEmit{es, raw.p}, tot.p)) != ITS_OK)
-    return st;
+  kEmitHits<<<gridFor(slots, 128), 128, 0, ctx->stream>>>(EdgeEmit{es, raw.p}, slots, ecnt.p, eoff.p);
+  ITS_LAUNCHED(ctx);
   ecnt.reset();
+  eoff.reset();
   ekeys.reset();
   eown.reset();
   // exact-duplicate removal
@@ -391,11 +404,13 @@ its_status its_shell_samples(its_svo* s, const double* verts, int64_t nverts, co
   raw.reset();
   // face step
   FaceStep fs{S, V.d, F.d};
-  DevBuf<uint32_t> fcnt;
-  if ((st = fcnt.alloc(ctx, nfaces)) != ITS_OK) return st;
+  DevBuf<uint32_t> fcnt, foff;
+  if ((st = fcnt.alloc(ctx, nfaces)) != ITS_OK || (st = foff.alloc(ctx, nfaces)) != ITS_OK) return st;
   kCountHits<<<gridFor(nfaces, 128), 128, 0, ctx->stream>>>(fs, nfaces, fcnt.p);
   ITS_LAUNCHED(ctx);
-  if ((st = scanExclusiveAlloc<uint32_t>(ctx, StoredCount{fcnt.p}, nfaces, nowrite, tot.p + 2)) != ITS_OK) return st;
+  if ((st = scanExclusiveAlloc<uint32_t>(ctx, StoredCount{fcnt.p}, nfaces, StorePrefix<uint32_t>{foff.p},
+                                         tot.p + 2)) != ITS_OK)
+    return st;
   uint32_t nFace = 0;
   if ((st = readScalar(ctx, tot.p + 2, &nFace)) != ITS_OK) return st;
   const int64_t total = (int64_t)nEdge + nFace;
@@ -415,9 +430,11 @@ its_status its_shell_samples(its_svo* s, const double* verts, int64_t nverts, co
     dst = all.p;
   }
   if (nEdge && dst) ITS_CU(ctx, cudaMemcpyAsync(dst, edgePts.p, (size_t)nEdge * 24, cudaMemcpyDeviceToDevice, ctx->stream));
-  if (dst && (st = scanExclusiveAlloc<uint32_t>(ctx, StoredCount{fcnt.p}, nfaces, FaceEmit{fs, dst + 3 * (int64_t)nEdge},
-                                                tot.p + 2)) != ITS_OK)
-    return st;
+  if (dst) {
+    kEmitHits<<<gridFor(nfaces, 128), 128, 0, ctx->stream>>>(FaceEmit{fs, dst + 3 * (int64_t)nEdge}, nfaces, fcnt.p,
+                                                             foff.p);
+    ITS_LAUNCHED(ctx);
+  }
   if (keep < total && keep > 0)
     ITS_CU(ctx, cudaMemcpyAsync(O.d, all.p, (size_t)keep * 24, cudaMemcpyDeviceToDevice, ctx->stream));
   if ((st = O.finish(ctx)) != ITS_OK) return st;
