@@ -884,12 +884,31 @@ __global__ void __launch_bounds__(kScanThreads) kMcEmit(McCaseT<T> mc, double3 o
     cnt += cMcCase[ci[j]] & 15ull;
   }
   unsigned long long total;
-  unsigned long long run = blockExclusiveScan<unsigned long long>(cnt, total) + blockOffsets[blockIdx.x];
+  const unsigned long long tileBase = blockOffsets[blockIdx.x];
+  unsigned long long run = blockExclusiveScan<unsigned long long>(cnt, total);  // within the tile
   if (!total || !tri) return;
+  // The tile's voxels with vertices are listed (place in the tile | offset within the tile's
+  // output << 12: at most 15 vertices per voxel, so the offset stays below 2^16) and the block
+  // emits the list round-robin, instead of each thread its own ITEMS voxels one after another.
+  // Every voxel writes at its own offset: the order of the list does not matter.
+  static_assert(kScanThreads * ITEMS <= 4096 && 15 * kScanThreads * ITEMS < 65536, "list entry packing");
+  __shared__ uint32_t sList[kScanThreads * ITEMS];
+  __shared__ unsigned sCount;
+  if (threadIdx.x == 0) sCount = 0;
+  __syncthreads();
+#pragma unroll
   for (int j = 0; j < ITEMS; ++j) {
-    const unsigned long long c = cMcCase[ci[j]] & 15ull;
-    if (c) mcEmitVoxel(mc, o, vs, tri, capacity, base + j, ci[j], run, c);
+    const unsigned c = cMcCase[ci[j]] & 15u;
+    if (c) sList[atomicAdd(&sCount, 1u)] = (uint32_t)(threadIdx.x * ITEMS + j) | (uint32_t)run << 12;
     run += c;
+  }
+  __syncthreads();
+  const int64_t tile0 = (int64_t)blockIdx.x * (kScanThreads * ITEMS);
+  for (unsigned e = threadIdx.x; e < sCount; e += kScanThreads) {
+    const uint32_t item = sList[e];
+    const int64_t v = tile0 + (item & 4095u);
+    const unsigned char c8 = cube[v];
+    mcEmitVoxel(mc, o, vs, tri, capacity, v, c8, tileBase + (item >> 12), cMcCase[c8] & 15ull);
   }
 }
 
