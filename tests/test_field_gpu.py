@@ -124,6 +124,21 @@ def test_marching_cubes_bit_exact(ctx, fitted, R):
 
 
 @pytest.mark.gpu
+def test_marching_cubes_bit_exact_tiled_block_sum_scan(ctx, fitted):
+    # At R = 260 the classify pass leaves 8,583 block sums (2,048 voxels each): above the 8,192
+    # that one block scans, so the spine runs in tiles of 2,048 with a partial last tile; the
+    # cases and the soup stay the oracle's.
+    V, F, o, w, ref, gpu, pos, b, lam = fitted
+    R = 260
+    field = gpu.eval_grid(lam, o, w, R)
+    cube_g, tri_g, n_g = ctx.marching_cubes(field, R, o, w, 0.0)
+    cube_r, tri_r, n_r = oracle.marching_cubes(field, R, o, w, 0.0)
+    assert n_g == n_r and n_g > 0
+    assert np.array_equal(cube_g, cube_r)
+    assert np.array_equal(tri_g, tri_r)
+
+
+@pytest.mark.gpu
 def test_fast_division_is_correctly_rounded(ctx):
     # The field kernels divide by the cell width through RN(1/w) and two FMAs (Markstein);
     # the quotients must equal the GPU's correctly rounded division bit for bit.
