@@ -47,7 +47,8 @@ def _ptr(a):
 def _f64(a):
     if isinstance(a, np.ndarray) or not hasattr(a, "data_ptr"):
         return np.ascontiguousarray(a, dtype=np.float64)
-    assert str(a.dtype) == "torch.float64" and a.is_contiguous()
+    import torch
+    assert a.dtype is torch.float64 and a.is_contiguous()
     return a
 
 
@@ -598,15 +599,31 @@ def learned_start_batch(svos, net, bs, norm, outs=None):
     return outs
 
 
+# The last FP32 normalisation array passed to learned_fit as it is (contiguous float32, no copy
+# made) and its address: the fit is called again and again with the same one, and reading an
+# array's address through ctypes costs more than the rest of the call's Python side.
+_norm_seen = [None, 0]
+
+
+def _norm_arg(norm):
+    if _norm_seen[0] is norm:
+        return norm, _norm_seen[1]
+    a = np.ascontiguousarray(norm, np.float32)
+    addr = a.ctypes.data
+    if a is norm:
+        _norm_seen[0], _norm_seen[1] = a, addr
+    return a, addr
+
+
 def learned_fit(svo, net, b, norm, tol, out=None):
     """The learned fit of one octree (its_learned_fit): learned start, FP64 residual check,
     plain LSCG from the start when the residual misses tol. Returns (lambda, report dict)."""
     b = _f64(b)
-    norm = np.ascontiguousarray(norm, np.float32)
+    norm, norm_addr = _norm_arg(norm)
     if out is None:
         out = np.zeros(svo.num_verts)
     rep = SolveReport()
-    svo.ctx.check(lib().its_learned_fit(svo.h, net.h, _addr(b), _ptr(norm), tol, _addr(out), C.byref(rep)),
+    svo.ctx.check(lib().its_learned_fit(svo.h, net.h, _addr(b), norm_addr, tol, _addr(out), C.byref(rep)),
                   "its_learned_fit")
     return out, dict(iterations=rep.iterations, converged=bool(rep.converged), rel_residual=rep.rel_residual,
                      ms=rep.ms)
