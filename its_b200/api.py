@@ -557,7 +557,15 @@ def solve_batch(ops, bs, tol=None, max_iters=0, stop_rule=STOP_NORMAL, check_eve
 
 
 def _addr(a):
-    return None if a is None else (a.ctypes.data if isinstance(a, np.ndarray) else a.data_ptr())
+    """Address of a contiguous numpy array or a torch tensor (None -> NULL). A writable array's
+    address through the buffer protocol: about half the time of reading it through ctypes."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        if a.flags.writeable and a.size and a.flags.c_contiguous:
+            return C.addressof(C.c_char.from_buffer(a))
+        return a.ctypes.data
+    return a.data_ptr()
 
 
 def exact_start_batch(svos, bs, shares=None, outs=None):
