@@ -342,7 +342,8 @@ its_status its_marching_cubes_f32(its_ctx* ctx, const float* field, int res, con
    field, cube_index and tri_verts must be device memory of the context's GPU; res <= 256
    (ITS_ERR_INVALID beyond). Calls on one device share the array (overlapping calls race); the
    call waits on its stream for num_verts. The first call on a device looks up the array's
-   address and keeps it: cudaDeviceReset of that device afterwards is not supported. */
+   address and keeps it: make that first call before any stream capture, and do not reset the
+   device (cudaDeviceReset) afterwards. */
 its_status its_marching_cubes_noalloc(its_ctx* ctx, const double* field, int res, const double origin[3],
                                       const double width[3], double iso, uint8_t* cube_index, double* tri_verts,
                                       int64_t capacity, int64_t* num_verts);
