@@ -692,7 +692,7 @@ def run_ours(args):
                               "frac": round(spmv_achieved / hbm_peak, 4), "peak_kind": peak_kind,
                               "bytes_per_launch": spmv_bytes, "launch_ms": round(spmv[dom], 5),
                               "traffic": profile_traffic("kSpmvBinned", wl["mesh"])},
-            "roofline_learned_step": {"bound": "hbm", "kernel": "the learned fit step as a whole (its 9 kernels)",
+            "roofline_learned_step": {"bound": "hbm", "kernel": "the learned fit step as a whole (its 8 kernels)",
                                       "achieved": round(learned_bytes / (fit_ms * 1e-3) / 1e9, 1), "peak": hbm_peak,
                                       "unit": "GB/s", "frac": round(learned_bytes / (fit_ms * 1e-3) / 1e9 / hbm_peak, 4),
                                       "bytes_per_launch": learned_bytes, "launch_ms": round(fit_ms, 5)},
